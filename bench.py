@@ -1,0 +1,264 @@
+#!/usr/bin/env python
+"""Benchmark of the CPU-free Jacobi hot path on B200.
+
+Workload (one "step"): 100 persistent FP64 Jacobi 3d7p sweeps of the 512^3
+periodic problem (x faces sin(2 pi y/(ny-1)) sin(2 pi z/(nz-1)), periodic in
+y and z), i.e. one solve of that configuration; successive steps continue
+from the previous grid, which does not change the work.  Metric: GLUP/s
+(interior lattice-point updates per second, 510^3 per sweep).
+
+  value  device-resident throughput: CUDA events on the library's stream
+         around K steps (each step = edge preset + one cooperative launch).
+  e2e    the same metric through the C ABI with pinned host buffers:
+         cfm_jacobi_run_host = H2D of the grid, the sweeps, D2H of the result.
+  roofline  16 algorithmic bytes per LUP over the measured launch time,
+         against MEASURED_PEAKS.json's copy bandwidth.
+  cpu_baseline  the oracle's FP64 sweep loop (C/OpenMP) on the host cores.
+
+--gpus N runs N independent replicas (one per GPU, no data exchange; weak
+scaling); rank 0 prints the JSON line.  --impl reference times the host
+restatement of the reference's single-GPU sweep (the reference ships no CPU
+Jacobi of its own) on the host cores with the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cpu-free-model_b200"))
+
+N = 512
+NITER = 100
+LUP_PER_SWEEP = (N - 2) ** 3
+BYTES_PER_LUP = 16.0  # FP64: one 8-byte read + one 8-byte write per interior point
+FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "jacobi3d_persistent_512_fp64.md")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes per persistent launch from the committed ncu summary, if any."""
+    try:
+        for line in open(TRAFFIC_FILE):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait(timeout=10)
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline():
+    """Oracle FP64 sweep loop on the host cores, sized to ~10 s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    t1 = oracle.jacobi3d_bench(N, 1)
+    k = int(max(1, min(60, 10.0 / max(t1, 1e-3))))
+    t = oracle.jacobi3d_bench(N, k)
+    return {"value": k * LUP_PER_SWEEP / t / 1e9, "unit": "GLUP/s", "cores": oracle.max_threads(),
+            "kind": "port",
+            "sample": f"{k} FP64 sweeps of the 512^3 periodic problem, sweep loop only (OpenMP)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    sweeps = 1
+    for _ in range(args.warmup):
+        oracle.jacobi3d_bench(N, sweeps)
+    t = 0.0
+    for _ in range(args.steps):
+        t += oracle.jacobi3d_bench(N, sweeps)
+    v = args.steps * sweeps * LUP_PER_SWEEP / t / 1e9
+    cores = oracle.max_threads()
+    line = {
+        "impl": "reference", "metric": "Jacobi 3d7p 512^3 FP64 GLUP/s", "value": v, "unit": "GLUP/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "jacobi3d7p_512^3_fp64_periodic", "nx": N, "ny": N, "nz": N,
+                   "sweeps_per_step": sweeps, "impl": "host C/OpenMP restatement of single_gpu()"},
+        "cpu_baseline": {"value": v, "unit": "GLUP/s", "cores": cores, "kind": "port",
+                         "sample": f"{sweeps} sweep(s) of 512^3 per step"},
+        "e2e": {"value": v, "unit": "GLUP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import cfm
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    j = cfm.Jacobi(3, N, N, N, cfm.FP64, 1, cfm.JACOBI_PERSISTENT)
+    stream = torch.cuda.Stream()
+    j.set_stream(stream.cuda_stream)
+    j.load_problem(cfm.PROBLEM_CONFIG)
+    blocks, threads = j.launch_shape()
+    for _ in range(args.warmup):
+        j.run(NITER)
+
+    # ---- device-resident timed region
+    clocks = Clocks(local)
+    time.sleep(0.25)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, kern_s = 0, 0.0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st = j.run(NITER)
+        launches += st.launches
+        kern_s += st.seconds
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) * 1e-3)
+    kern_s = max_over_ranks(kern_s)
+
+    # ---- end-to-end through the C ABI with pinned host buffers
+    host_in = torch.from_numpy(j.problem_host(cfm.PROBLEM_CONFIG).reshape(-1)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    j.run_host(NITER, host_in, host_out)  # warm the copy path
+    e2e_steps = max(3, args.steps // 3)
+    barrier()
+    torch.cuda.synchronize()
+    e2e_s = 0.0
+    h2d = d2h = 0.0
+    for _ in range(e2e_steps):
+        st = j.run_host(NITER, host_in, host_out)
+        e2e_s += st.seconds
+        h2d, d2h = st.h2d_bytes, st.d2h_bytes
+    torch.cuda.synchronize()
+    barrier()
+    e2e_s = max_over_ranks(e2e_s)
+    clk = clocks.stop()
+    j.close()
+
+    lup_step = NITER * LUP_PER_SWEEP
+    value = world * args.steps * lup_step / t_dev / 1e9
+    e2e_value = world * e2e_steps * lup_step / e2e_s / 1e9
+    peak, peak_kind = peak_hbm()
+    per_launch_s = kern_s / args.steps
+    achieved = BYTES_PER_LUP * lup_step / per_launch_s / 1e9
+    traffic = traffic_per_launch()
+    line = {
+        "metric": "Jacobi 3d7p 512^3 FP64 GLUP/s", "value": value, "unit": "GLUP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "jacobi3d7p_512^3_fp64_periodic", "nx": N, "ny": N, "nz": N,
+                   "niter_per_step": NITER, "problem": "config (x faces sin*sin, periodic y,z)",
+                   "impl": "persistent cooperative kernel, grid barrier per sweep",
+                   "launch": f"{blocks}x{threads}", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (two 1.07 GB grids)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": BYTES_PER_LUP * lup_step},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "GLUP/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,301 @@
+"""ctypes binding of libcfm.so (declared in include/cfm.h).
+
+Used by the tests and bench.py to drive the C ABI exactly as a foreign host
+(cgo / JNI / ctypes) would: plain pointers and sizes, integer status codes.
+There is no fallback: if lib/libcfm.so is missing the import of this module
+raises, and every call goes to the CUDA library.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcfm.so")
+
+OK, BAD_ARG, CUDA_ERROR, BARRIER_TIMEOUT, BREAKDOWN, NOT_CONVERGED, NO_DEVICE, UNSUPPORTED, OOM = range(9)
+FP64, FP32 = 0, 1
+PROBLEM_REF, PROBLEM_CONFIG = 0, 1
+JACOBI_HOST_LOOP, JACOBI_HOST_LOOP_INKERNEL_HALO, JACOBI_PERSISTENT, JACOBI_RESIDENT = range(4)
+CG_DISCRETE, CG_PERSISTENT, CG_PERSISTENT_PIPELINED, CG_MIXED = range(4)
+
+# Every function include/cfm.h declares, with (restype, argtypes).
+_c = ctypes
+_vp = _c.c_void_p
+_SIGS = {
+    "cfm_api_version": (_c.c_int, []),
+    "cfm_status_string": (_c.c_char_p, [_c.c_int]),
+    "cfm_last_error": (_c.c_char_p, []),
+    "cfm_set_barrier_timeout_ms": (_c.c_int, [_c.c_double]),
+    "cfm_device_info": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_jacobi_problem_host": (_c.c_int, [_vp, _c.c_int, _vp]),
+    "cfm_jacobi_create": (_c.c_int, [_vp, _vp]),
+    "cfm_jacobi_destroy": (None, [_vp]),
+    "cfm_jacobi_set_stream": (_c.c_int, [_vp, _vp]),
+    "cfm_jacobi_load_problem": (_c.c_int, [_vp, _c.c_int]),
+    "cfm_jacobi_upload": (_c.c_int, [_vp, _vp]),
+    "cfm_jacobi_download": (_c.c_int, [_vp, _vp]),
+    "cfm_jacobi_run": (_c.c_int, [_vp, _c.c_int, _vp]),
+    "cfm_jacobi_run_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
+    "cfm_jacobi_device_grid": (_vp, [_vp]),
+    "cfm_jacobi_launch_shape": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_csr_create": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp]),
+    "cfm_csr_destroy": (None, [_vp]),
+    "cfm_csr_spmv_host": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_cg_create": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_cg_destroy": (None, [_vp]),
+    "cfm_cg_set_stream": (_c.c_int, [_vp, _vp]),
+    "cfm_cg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
+    "cfm_cg_solve_device": (_c.c_int, [_vp, _vp, _vp, _vp]),
+    "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
+    "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
+    "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
+    "cfm_uniform": (_c.c_int, [_c.c_ulonglong, _c.c_longlong, _c.c_double, _c.c_double, _vp]),
+    "cfm_philox4x32_10": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_barrier_selftest": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp]),
+}
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("seconds", ctypes.c_double),
+        ("iterations", ctypes.c_longlong),
+        ("lups", ctypes.c_double),
+        ("glups", ctypes.c_double),
+        ("bytes", ctypes.c_double),
+        ("gbs", ctypes.c_double),
+        ("residual", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_double),
+        ("d2h_bytes", ctypes.c_double),
+        ("launches", ctypes.c_int),
+        ("status", ctypes.c_int),
+        ("refinements", ctypes.c_int),
+        ("pad", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+class JacobiParams(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("dims", "nx", "ny", "nz", "precision", "periodic_y", "impl")]
+
+
+class CGParams(ctypes.Structure):
+    _fields_ = [
+        ("impl", ctypes.c_int),
+        ("maxiter", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("inner_maxiter", ctypes.c_int),
+        ("inner_tol", ctypes.c_double),
+    ]
+
+
+def load_library(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C cpu-free-model_b200` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = load_library()
+
+
+class CfmError(RuntimeError):
+    def __init__(self, what, status):
+        self.status = status
+        msg = lib.cfm_last_error().decode(errors="replace")
+        super().__init__(f"{what}: {lib.cfm_status_string(status).decode()} ({msg})")
+
+
+def check(what, status, allowed=(OK,)):
+    if status not in allowed:
+        raise CfmError(what, status)
+    return status
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def np_dtype(precision):
+    return np.float64 if precision == FP64 else np.float32
+
+
+class Jacobi:
+    """One device grid pair; mirrors cfm_jacobi_* (and the reference's init(argc, argv))."""
+
+    def __init__(self, dims, nx, ny, nz=1, precision=FP64, periodic_y=0, impl=JACOBI_PERSISTENT):
+        self.p = JacobiParams(dims, nx, ny, nz if dims == 3 else 1, precision, periodic_y, impl)
+        self.shape = (nz, ny, nx) if dims == 3 else (ny, nx)
+        self.dtype = np_dtype(precision)
+        h = ctypes.c_void_p()
+        check("cfm_jacobi_create", lib.cfm_jacobi_create(ctypes.byref(self.p), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_jacobi_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def problem_host(self, problem):
+        a = np.empty(self.shape, self.dtype)
+        check("cfm_jacobi_problem_host", lib.cfm_jacobi_problem_host(ctypes.byref(self.p), problem, _ptr(a)))
+        return a
+
+    def load_problem(self, problem):
+        check("cfm_jacobi_load_problem", lib.cfm_jacobi_load_problem(self.h, problem))
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, self.dtype)
+        assert a.shape == self.shape
+        check("cfm_jacobi_upload", lib.cfm_jacobi_upload(self.h, _ptr(a)))
+
+    def download(self):
+        a = np.empty(self.shape, self.dtype)
+        check("cfm_jacobi_download", lib.cfm_jacobi_download(self.h, _ptr(a)))
+        return a
+
+    def run(self, niter, allowed=(OK,)):
+        st = Stats()
+        check("cfm_jacobi_run", lib.cfm_jacobi_run(self.h, niter, ctypes.byref(st)), allowed)
+        return st
+
+    def run_host(self, niter, host_in, host_out):
+        """End-to-end call with caller-owned host buffers (numpy or pinned torch memory)."""
+        st = Stats()
+        pin = host_in.ctypes.data if isinstance(host_in, np.ndarray) else host_in.data_ptr()
+        pout = host_out.ctypes.data if isinstance(host_out, np.ndarray) else host_out.data_ptr()
+        check("cfm_jacobi_run_host",
+              lib.cfm_jacobi_run_host(self.h, niter, ctypes.c_void_p(pin), ctypes.c_void_p(pout), ctypes.byref(st)))
+        return st
+
+    def set_stream(self, stream_handle):
+        check("cfm_jacobi_set_stream", lib.cfm_jacobi_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def device_grid(self):
+        return lib.cfm_jacobi_device_grid(self.h)
+
+    def launch_shape(self):
+        b, t = ctypes.c_int(), ctypes.c_int()
+        check("cfm_jacobi_launch_shape", lib.cfm_jacobi_launch_shape(self.h, ctypes.byref(b), ctypes.byref(t)))
+        return b.value, t.value
+
+
+class CSR:
+    def __init__(self, rowptr, col, val):
+        self.rowptr = np.ascontiguousarray(rowptr, np.int32)
+        self.col = np.ascontiguousarray(col, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+        self.n = len(self.rowptr) - 1
+        h = ctypes.c_void_p()
+        check("cfm_csr_create", lib.cfm_csr_create(self.n, len(self.val), _ptr(self.rowptr), _ptr(self.col),
+                                                   _ptr(self.val), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_csr_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.n)
+        check("cfm_csr_spmv_host", lib.cfm_csr_spmv_host(self.h, _ptr(x), _ptr(y)))
+        return y
+
+
+class CG:
+    def __init__(self, A, impl=CG_PERSISTENT, maxiter=20000, tol=1e-8, inner_maxiter=0, inner_tol=0.0):
+        self.A = A
+        self.p = CGParams(impl, maxiter, tol, inner_maxiter, inner_tol)
+        h = ctypes.c_void_p()
+        check("cfm_cg_create", lib.cfm_cg_create(A.h, ctypes.byref(self.p), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_cg_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def solve(self, b=None, allowed=(OK, NOT_CONVERGED)):
+        x = np.empty(self.A.n)
+        st = Stats()
+        bb = None if b is None else np.ascontiguousarray(b, np.float64)
+        check("cfm_cg_solve", lib.cfm_cg_solve(self.h, _ptr(bb), _ptr(x), ctypes.byref(st)), allowed)
+        return x, st
+
+    def solve_device(self, b_dev_ptr, x_dev_ptr, allowed=(OK, NOT_CONVERGED)):
+        st = Stats()
+        check("cfm_cg_solve_device", lib.cfm_cg_solve_device(self.h, ctypes.c_void_p(b_dev_ptr),
+                                                              ctypes.c_void_p(x_dev_ptr), ctypes.byref(st)), allowed)
+        return st
+
+    def set_stream(self, stream_handle):
+        check("cfm_cg_set_stream", lib.cfm_cg_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+
+def poisson3d(g):
+    nnz = lib.cfm_poisson3d_nnz(g, g, g)
+    n = g * g * g
+    rowptr = np.empty(n + 1, np.int32)
+    col = np.empty(nnz, np.int32)
+    val = np.empty(nnz, np.float64)
+    check("cfm_poisson3d_csr", lib.cfm_poisson3d_csr(g, g, g, _ptr(rowptr), _ptr(col), _ptr(val)))
+    return rowptr, col, val
+
+
+def tridiag(n):
+    nnz = 3 * n - 2
+    rowptr = np.empty(n + 1, np.int32)
+    col = np.empty(nnz, np.int32)
+    val = np.empty(nnz, np.float64)
+    check("cfm_tridiag_csr", lib.cfm_tridiag_csr(n, _ptr(rowptr), _ptr(col), _ptr(val)))
+    return rowptr, col, val
+
+
+def uniform(seed, n, lo=-1.0, hi=1.0):
+    out = np.empty(n)
+    check("cfm_uniform", lib.cfm_uniform(seed, n, lo, hi, _ptr(out)))
+    return out
+
+
+def philox(ctr, key):
+    c = np.asarray(ctr, np.uint32)
+    k = np.asarray(key, np.uint32)
+    o = np.empty(4, np.uint32)
+    check("cfm_philox4x32_10", lib.cfm_philox4x32_10(_ptr(c), _ptr(k), _ptr(o)))
+    return o
+
+
+def device_info():
+    sms, ma, mi = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    st = lib.cfm_device_info(ctypes.byref(sms), ctypes.byref(ma), ctypes.byref(mi))
+    return st, sms.value, ma.value, mi.value
+
+
+def barrier_selftest(blocks=0, rounds=4, drop_block=-1):
+    ms = ctypes.c_double()
+    st = lib.cfm_barrier_selftest(blocks, rounds, drop_block, ctypes.byref(ms))
+    return st, ms.value
+
+
+def set_barrier_timeout_ms(ms):
+    check("cfm_set_barrier_timeout_ms", lib.cfm_set_barrier_timeout_ms(ms))

@@ -1,0 +1,62 @@
+// Internal declarations shared by the libcfm translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "cfm.h"
+
+namespace cfm {
+
+// Records a one-line error message for cfm_last_error() (thread-local).
+void set_error(const char *fmt, ...);
+void clear_error();
+
+// Barrier wait budget in nanoseconds (cfm_set_barrier_timeout_ms).
+unsigned long long barrier_timeout_ns();
+
+struct DeviceInfo {
+    int device = -1;
+    int num_sms = 0;
+    int cc_major = 0, cc_minor = 0;
+    size_t smem_optin = 0;
+};
+// Queries (and caches per device) the current device's properties.
+int current_device_info(DeviceInfo *out);
+
+// Device-side state of one grid barrier; see barrier.cuh.
+struct BarrierState {
+    unsigned int count;   // arrivals in the current generation
+    unsigned int gen;     // generation, bumped by the last arrival
+    int error;            // set to 1 by a wait that ran out of budget
+    int where;            // barrier index at which the first timeout happened
+    unsigned long long timeout_ns;
+};
+
+// Kernel launch helper: cooperative launch so that every block is resident
+// (the barrier needs co-residency).
+cudaError_t launch_cooperative(const void *fn, dim3 grid, dim3 block, void **args, size_t smem,
+                               cudaStream_t s);
+
+}  // namespace cfm
+
+#define CFM_CUDA_TRY(call)                                                                    \
+    do {                                                                                      \
+        cudaError_t cfm_e_ = (call);                                                          \
+        if (cfm_e_ != cudaSuccess) {                                                          \
+            cfm::set_error("%s failed: %s (%d) at %s:%d", #call, cudaGetErrorString(cfm_e_), \
+                           (int)cfm_e_, __FILE__, __LINE__);                                  \
+            return cfm_e_ == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;  \
+        }                                                                                     \
+    } while (0)
+
+#define CFM_ARG_CHECK(cond, msg)                      \
+    do {                                              \
+        if (!(cond)) {                                \
+            cfm::set_error("bad argument: %s", msg);  \
+            return CFM_BAD_ARG;                       \
+        }                                             \
+    } while (0)

@@ -1,0 +1,731 @@
+// Jacobi 2d5p / 3d7p sweeps on one GPU: kernels and the cfm_jacobi handle.
+//
+// Arithmetic (bit-exact with the reference's single-GPU run):
+//   2D  a' = 0.25 * (((a[x+1] + a[x-1]) + a[y+1]) + a[y-1])
+//        Stencil/jacobi2D/src/common.cu:28-42
+//   3D  a' = (T(1)/T(6)) * (((((a[x+1] + a[x-1]) + a[y+1]) + a[y-1]) + a[z+1]) + a[z-1])
+//        Stencil/jacobi3D/src/common.cu:31-57
+// Halo semantics: after every sweep the reference copies row ny-2 -> row 0 and
+// row 1 -> row ny-1 (planes in 3D), full width (Stencil/jacobi2D/src/common.cu:
+// 234-242, Stencil/jacobi3D/src/common.cu:198-207).  The kernels here write
+// each periodic image together with the interior value it copies (as
+// jacobi_kernel_single_gpu_persistent does, Stencil/jacobi3D/src/common.cu:82-88),
+// and the few cells no sweep reads or writes (the box edges of the halo
+// rows/planes) are set to their images once before the first sweep
+// (edge_preset_kernel), which gives the same grid after >= 1 sweeps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "barrier.cuh"
+#include "cfm_internal.h"
+
+namespace cfm {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ T quarter(T s);
+template <>
+__device__ __forceinline__ double quarter<double>(double s) {
+    return __dmul_rn(0.25, s);
+}
+template <>
+__device__ __forceinline__ float quarter<float>(float s) {
+    // The reference multiplies by the double literal 0.25 and stores a float;
+    // scaling by a power of two is exact in double, so the single rounding to
+    // float equals the correctly rounded float product.
+    return __fmul_rn(0.25f, s);
+}
+
+template <typename T>
+__device__ __forceinline__ T add_rn(T a, T b);
+template <>
+__device__ __forceinline__ double add_rn<double>(double a, double b) {
+    return __dadd_rn(a, b);
+}
+template <>
+__device__ __forceinline__ float add_rn<float>(float a, float b) {
+    return __fadd_rn(a, b);
+}
+template <typename T>
+__device__ __forceinline__ T mul_rn(T a, T b);
+template <>
+__device__ __forceinline__ double mul_rn<double>(double a, double b) {
+    return __dmul_rn(a, b);
+}
+template <>
+__device__ __forceinline__ float mul_rn<float>(float a, float b) {
+    return __fmul_rn(a, b);
+}
+
+// ------------------------------------------------------------------ 2D sweep
+// One warp handles one 32-wide segment of one interior row; x neighbours come
+// from warp shuffles, y neighbours from the (L1/L2-resident) rows above/below.
+// Used for the persistent kernel (niter sweeps, barrier between) and, with
+// niter = 1 and a plain launch, for the host-loop comparators.
+template <typename T, bool IMAGES>
+__global__ void __launch_bounds__(256) j2d_sweeps_kernel(T *g0, T *g1, int nx, int ny, int niter,
+                                                         BarrierState *bar) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int ntx = (nx + 31) >> 5;
+    const long long nseg = (long long)ntx * (ny - 2);
+    T *in = g0, *out = g1;
+    for (int it = 0; it < niter; ++it) {
+        for (long long s = warp; s < nseg; s += nwarps) {
+            const int y = 1 + (int)(s / ntx);
+            const int x = (int)(s % ntx) * 32 + lane;
+            const bool ld = x < nx;
+            const size_t idx = (size_t)y * nx + x;
+            T cur = ld ? in[idx] : T(0);
+            T e = __shfl_down_sync(FULL, cur, 1);
+            T w = __shfl_up_sync(FULL, cur, 1);
+            if (lane == 31) e = (x + 1 < nx) ? in[idx + 1] : T(0);
+            if (lane == 0) w = (x >= 1 && ld) ? in[idx - 1] : T(0);
+            if (x >= 1 && x <= nx - 2) {
+                const T n = in[idx + nx];
+                const T so = in[idx - nx];
+                const T v = quarter<T>(add_rn(add_rn(add_rn(e, w), n), so));
+                out[idx] = v;
+                if (IMAGES) {
+                    if (y == 1) out[idx + (size_t)(ny - 2) * nx] = v;
+                    if (y == ny - 2) out[idx - (size_t)(ny - 2) * nx] = v;
+                }
+            }
+        }
+        if (it + 1 < niter) {
+            if (!grid_barrier(bar, gridDim.x, it)) return;
+        }
+        T *t = in;
+        in = out;
+        out = t;
+    }
+}
+
+// ------------------------------------------------------------------ 3D sweep
+// Work unit = (z-chunk, tile) with the tile 32 (x, aligned at x = 0) by TY
+// interior rows; units are ordered chunk-major and every block takes one
+// contiguous, equal-sized range, so blocks owning neighbouring tiles visit the
+// same planes at the same time and the tile-edge rows they share are L2 hits.
+// Inside a unit each thread marches along z keeping the z-1, z, z+1 values in
+// registers: every interior value is read from HBM once per sweep.
+template <typename T, int TY, bool PY, bool IMAGES>
+__global__ void __launch_bounds__(32 * TY) j3d_sweeps_kernel(T *g0, T *g1, int nx, int ny, int nz,
+                                                             int niter, int zchunk,
+                                                             BarrierState *bar) {
+    const int lane = threadIdx.x;
+    const int wy = threadIdx.y;
+    const int ntx = (nx + 31) >> 5;
+    const int nty = (ny - 2 + TY - 1) / TY;
+    const long long ntiles = (long long)ntx * nty;
+    const int nzi = nz - 2;
+    const int nch = (nzi + zchunk - 1) / zchunk;
+    const long long U = ntiles * nch;
+    const long long u0 = (long long)blockIdx.x * U / gridDim.x;
+    const long long u1 = (long long)(blockIdx.x + 1) * U / gridDim.x;
+    const size_t P = (size_t)nx * ny;
+    const T c6 = T(1) / T(6);
+    const size_t zimg = (size_t)(nz - 2) * P;
+    const size_t yimg = (size_t)(ny - 2) * nx;
+    T *in = g0, *out = g1;
+    for (int it = 0; it < niter; ++it) {
+        for (long long u = u0; u < u1; ++u) {
+            const int ch = (int)(u / ntiles);
+            const int tile = (int)(u - (long long)ch * ntiles);
+            const int x = (tile % ntx) * 32 + lane;
+            const int y = 1 + (tile / ntx) * TY + wy;
+            const int z0 = 1 + ch * zchunk;
+            const int z1 = min(z0 + zchunk, nz - 1);
+            const bool ld = (y <= ny - 2) && (x < nx);
+            const bool comp = ld && x >= 1 && x <= nx - 2;
+            size_t idx = ((size_t)z0 * ny + (ld ? y : 1)) * nx + (ld ? x : 0);
+            T prev = ld ? in[idx - P] : T(0);
+            T cur = ld ? in[idx] : T(0);
+            for (int z = z0; z < z1; ++z, idx += P) {
+                const T next = ld ? in[idx + P] : T(0);
+                T e = __shfl_down_sync(FULL, cur, 1);
+                T w = __shfl_up_sync(FULL, cur, 1);
+                if (lane == 31) e = (ld && x + 1 < nx) ? in[idx + 1] : T(0);
+                if (lane == 0) w = (ld && x >= 1) ? in[idx - 1] : T(0);
+                if (comp) {
+                    const T n = in[idx + nx];
+                    const T so = in[idx - nx];
+                    T s = add_rn(add_rn(add_rn(add_rn(add_rn(e, w), n), so), next), prev);
+                    const T v = mul_rn(c6, s);
+                    out[idx] = v;
+                    if (IMAGES) {
+                        const bool zlo = (z == 1), zhi = (z == nz - 2);
+                        if (zlo) out[idx + zimg] = v;
+                        if (zhi) out[idx - zimg] = v;
+                        if (PY) {
+                            if (y == 1) {
+                                out[idx + yimg] = v;
+                                if (zlo) out[idx + yimg + zimg] = v;
+                                if (zhi) out[idx + yimg - zimg] = v;
+                            }
+                            if (y == ny - 2) {
+                                out[idx - yimg] = v;
+                                if (zlo) out[idx - yimg + zimg] = v;
+                                if (zhi) out[idx - yimg - zimg] = v;
+                            }
+                        }
+                    }
+                }
+                prev = cur;
+                cur = next;
+            }
+        }
+        if (it + 1 < niter) {
+            if (!grid_barrier(bar, gridDim.x, it)) return;
+        }
+        T *t = in;
+        in = out;
+        out = t;
+    }
+}
+
+// Cells on the edges of the box (two or more coordinates on the boundary) are
+// neither read nor written by a sweep.  The reference's full-row/plane halo
+// copies leave each such cell equal to its periodic image after the first
+// sweep; set that once in both buffers.  Images always have their periodic
+// coordinates moved inside, so no cell read here is written here.
+template <typename T>
+__global__ void edge_preset_kernel(const T *cur, T *b0, T *b1, int dims, int nx, int ny, int nz,
+                                   int py) {
+    const long long n_edge = 4LL * nx + 4LL * ny + (dims == 3 ? 4LL * nz : 0);
+    const int zmax = dims == 3 ? nz : 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_edge;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        long long k = i;
+        if (k < 4LL * nx) {  // edges running along x
+            const int c = (int)(k / nx);
+            x = (int)(k % nx);
+            y = (c & 1) ? ny - 1 : 0;
+            z = (c & 2) ? zmax - 1 : 0;
+        } else if ((k -= 4LL * nx) < 4LL * ny) {  // edges along y
+            const int c = (int)(k / ny);
+            y = (int)(k % ny);
+            x = (c & 1) ? nx - 1 : 0;
+            z = (c & 2) ? zmax - 1 : 0;
+        } else {  // edges along z (3D only)
+            k -= 4LL * ny;
+            const int c = (int)(k / nz);
+            z = (int)(k % nz);
+            x = (c & 1) ? nx - 1 : 0;
+            y = (c & 2) ? ny - 1 : 0;
+        }
+        const int onb = (x == 0 || x == nx - 1) + (y == 0 || y == ny - 1) +
+                        (dims == 3 && (z == 0 || z == nz - 1));
+        if (onb < 2) continue;
+        int iy = y, iz = z;
+        if (dims == 2 || py) iy = (y == 0) ? ny - 2 : (y == ny - 1 ? 1 : y);
+        if (dims == 3) iz = (z == 0) ? nz - 2 : (z == nz - 1 ? 1 : z);
+        if (iy == y && iz == z) continue;
+        const size_t dst = ((size_t)z * ny + y) * nx + x;
+        const size_t src = ((size_t)iz * ny + iy) * nx + x;
+        const T v = cur[src];
+        b0[dst] = v;
+        b1[dst] = v;
+    }
+}
+
+// Device-side initial state (same values as cfm_jacobi_problem_host):
+// sy/sz hold the host-computed sin(2 pi i/(n-1)) factors.
+template <typename T>
+__global__ void load_problem_kernel(T *a, int dims, int nx, int ny, int nz, int problem,
+                                    const double *sy, const double *sz) {
+    const size_t N = (size_t)nx * ny * (dims == 3 ? nz : 1);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx);
+        const size_t r = i / nx;
+        const int y = (int)(r % ny);
+        const int z = (int)(r / ny);
+        T v = T(0);
+        if (dims == 2) {
+            if (x == 0 || x == nx - 1) v = (T)sy[y];
+        } else if (problem == CFM_PROBLEM_REF) {
+            if (x == 0) v = (T)((T)z - (T)y) - (T)(nx - 1);
+        } else {
+            if (x == 0 || x == nx - 1) v = (T)(sy[y] * sz[z]);
+        }
+        a[i] = v;
+    }
+}
+
+}  // namespace cfm
+
+using namespace cfm;
+
+struct cfm_jacobi {
+    cfm_jacobi_params p;
+    size_t elems = 0, esize = 0;
+    void *buf[2] = {nullptr, nullptr};
+    int cur = 0;
+    BarrierState *bar = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int blocks = 0, threads = 0, zchunk = 0;
+    int num_sms = 0;
+};
+
+namespace {
+
+constexpr int J3_TY = 8;
+
+int check_params(const cfm_jacobi_params *p) {
+    CFM_ARG_CHECK(p, "params is null");
+    CFM_ARG_CHECK(p->dims == 2 || p->dims == 3, "dims must be 2 or 3");
+    CFM_ARG_CHECK(p->nx >= 3 && p->ny >= 3, "nx, ny must be >= 3");
+    CFM_ARG_CHECK(p->dims == 2 || p->nz >= 3, "nz must be >= 3");
+    CFM_ARG_CHECK(p->precision == CFM_FP64 || p->precision == CFM_FP32, "precision");
+    CFM_ARG_CHECK(p->impl >= CFM_JACOBI_HOST_LOOP && p->impl <= CFM_JACOBI_RESIDENT, "impl");
+    const double cells = (double)p->nx * p->ny * (p->dims == 3 ? p->nz : 1);
+    CFM_ARG_CHECK(cells < 9.0e18, "grid too large");
+    CFM_ARG_CHECK((double)p->nx * p->ny < 2.0e9, "plane too large");
+    return CFM_OK;
+}
+
+size_t grid_elems(const cfm_jacobi_params *p) {
+    return (size_t)p->nx * p->ny * (p->dims == 3 ? (size_t)p->nz : 1);
+}
+
+template <typename T>
+const void *sweep_fn(const cfm_jacobi_params &p, bool images) {
+    if (p.dims == 2)
+        return images ? (const void *)j2d_sweeps_kernel<T, true>
+                      : (const void *)j2d_sweeps_kernel<T, false>;
+    if (p.periodic_y)
+        return images ? (const void *)j3d_sweeps_kernel<T, J3_TY, true, true>
+                      : (const void *)j3d_sweeps_kernel<T, J3_TY, true, false>;
+    return images ? (const void *)j3d_sweeps_kernel<T, J3_TY, false, true>
+                  : (const void *)j3d_sweeps_kernel<T, J3_TY, false, false>;
+}
+
+const void *sweep_fn_any(const cfm_jacobi_params &p, bool images) {
+    return p.precision == CFM_FP64 ? sweep_fn<double>(p, images) : sweep_fn<float>(p, images);
+}
+
+dim3 block_of(const cfm_jacobi_params &p) { return p.dims == 2 ? dim3(256) : dim3(32, J3_TY); }
+
+// Host-side sin factors shared by the host and device initial states.
+void sin_factors(int n, std::vector<double> &out) {
+    const double pi = 2.0 * std::asin(1.0);
+    out.resize(n);
+    for (int i = 0; i < n; ++i) out[i] = std::sin(2.0 * pi * (double)i / (double)(n - 1));
+}
+
+template <typename T>
+void host_problem(const cfm_jacobi_params *p, int problem, T *a) {
+    const int nx = p->nx, ny = p->ny, nz = p->dims == 3 ? p->nz : 1;
+    std::memset(a, 0, sizeof(T) * grid_elems(p));
+    if (p->dims == 2) {
+        // 2D: the reference rounds pi to the grid type before the double sin
+        // (Stencil/jacobi2D/include/common.h:24, src/common.cu:19).
+        const T pi = (T)(2.0 * std::asin(1.0));
+        for (int y = 0; y < ny; ++y) {
+            const T v = (T)std::sin(2.0 * (double)pi * (double)y / (double)(ny - 1));
+            a[(size_t)y * nx] = v;
+            a[(size_t)y * nx + nx - 1] = v;
+        }
+        return;
+    }
+    std::vector<double> sy, sz;
+    sin_factors(ny, sy);
+    sin_factors(nz, sz);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y) {
+            const size_t row = ((size_t)z * ny + y) * nx;
+            if (problem == CFM_PROBLEM_REF) {
+                a[row] = (T)((T)z - (T)y) - (T)(nx - 1);
+            } else {
+                const T v = (T)(sy[y] * sz[z]);
+                a[row] = v;
+                a[row + nx - 1] = v;
+            }
+        }
+}
+
+int choose_launch(cfm_jacobi *h) {
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    h->num_sms = di.num_sms;
+    const cfm_jacobi_params &p = h->p;
+    const void *fn = sweep_fn_any(p, true);
+    dim3 b = block_of(p);
+    const int threads = (int)(b.x * b.y);
+    int per_sm = 0;
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0));
+    if (per_sm < 1) {
+        set_error("sweep kernel cannot be resident");
+        return CFM_UNSUPPORTED;
+    }
+    h->threads = threads;
+    h->blocks = per_sm * di.num_sms;
+    if (p.dims == 3) {
+        // Chunk the z range so that every block gets many units (balance to
+        // within one unit) while each unit still streams >= 16 planes.
+        const long long ntiles = (long long)((p.nx + 31) / 32) * ((p.ny - 2 + J3_TY - 1) / J3_TY);
+        const int nzi = p.nz - 2;
+        int zc = 32;
+        while (zc > 8 && ntiles * ((nzi + zc - 1) / zc) < 8LL * h->blocks) zc /= 2;
+        h->zchunk = std::min(zc, nzi);
+        const long long units = ntiles * ((nzi + h->zchunk - 1) / h->zchunk);
+        if (units < h->blocks) h->blocks = (int)std::max(1LL, units);
+    } else {
+        const long long nseg = (long long)((p.nx + 31) / 32) * (p.ny - 2);
+        const long long need = (nseg * 32 + threads - 1) / threads;
+        if (need < h->blocks) h->blocks = (int)std::max(1LL, need);
+    }
+    return CFM_OK;
+}
+
+template <typename T>
+int launch_edge_preset(cfm_jacobi *h) {
+    const cfm_jacobi_params &p = h->p;
+    T *cur = (T *)h->buf[h->cur];
+    const long long n = 4LL * p.nx + 4LL * p.ny + (p.dims == 3 ? 4LL * p.nz : 0);
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 1024);
+    edge_preset_kernel<T><<<blocks, 256, 0, h->stream>>>(cur, (T *)h->buf[0], (T *)h->buf[1],
+                                                         p.dims, p.nx, p.ny, p.dims == 3 ? p.nz : 1,
+                                                         p.periodic_y);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+// Reference single_gpu() host loop: sweep kernel, then the periodic halo
+// copies with cudaMemcpyAsync (Stencil/jacobi3D/src/common.cu:174-215).
+int host_loop_copy(cfm_jacobi *h, int niter, int *launches) {
+    const cfm_jacobi_params &p = h->p;
+    const void *fn = sweep_fn_any(p, false);
+    const size_t es = h->esize;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    int one = 1;
+    const dim3 block = block_of(p);
+    for (int it = 0; it < niter; ++it) {
+        void *in = h->buf[h->cur], *out = h->buf[h->cur ^ 1];
+        void *args3[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &one,
+                         &h->zchunk, &h->bar};
+        void *args2[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, &one, &h->bar};
+        CFM_CUDA_TRY(cudaLaunchKernel(fn, dim3(h->blocks), block, p.dims == 3 ? args3 : args2, 0,
+                                      h->stream));
+        char *o = (char *)out;
+        if (p.dims == 2) {
+            const size_t row = (size_t)nx * es;
+            CFM_CUDA_TRY(cudaMemcpyAsync(o, o + (size_t)(ny - 2) * row, row,
+                                         cudaMemcpyDeviceToDevice, h->stream));
+            CFM_CUDA_TRY(cudaMemcpyAsync(o + (size_t)(ny - 1) * row, o + row, row,
+                                         cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+            const size_t row = (size_t)nx * es, plane = row * ny;
+            if (p.periodic_y) {
+                CFM_CUDA_TRY(cudaMemcpy2DAsync(o + plane, plane, o + plane + (size_t)(ny - 2) * row,
+                                               plane, row, nz - 2, cudaMemcpyDeviceToDevice,
+                                               h->stream));
+                CFM_CUDA_TRY(cudaMemcpy2DAsync(o + plane + (size_t)(ny - 1) * row, plane,
+                                               o + plane + row, plane, row, nz - 2,
+                                               cudaMemcpyDeviceToDevice, h->stream));
+            }
+            CFM_CUDA_TRY(cudaMemcpyAsync(o, o + (size_t)(nz - 2) * plane, plane,
+                                         cudaMemcpyDeviceToDevice, h->stream));
+            CFM_CUDA_TRY(cudaMemcpyAsync(o + (size_t)(nz - 1) * plane, o + plane, plane,
+                                         cudaMemcpyDeviceToDevice, h->stream));
+        }
+        h->cur ^= 1;
+        ++*launches;
+    }
+    return CFM_OK;
+}
+
+int host_loop_images(cfm_jacobi *h, int niter, int *launches) {
+    const cfm_jacobi_params &p = h->p;
+    const void *fn = sweep_fn_any(p, true);
+    int one = 1;
+    const dim3 block = block_of(p);
+    for (int it = 0; it < niter; ++it) {
+        void *in = h->buf[h->cur], *out = h->buf[h->cur ^ 1];
+        void *args3[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &one,
+                         &h->zchunk, &h->bar};
+        void *args2[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, &one, &h->bar};
+        CFM_CUDA_TRY(cudaLaunchKernel(fn, dim3(h->blocks), block, p.dims == 3 ? args3 : args2, 0,
+                                      h->stream));
+        h->cur ^= 1;
+        ++*launches;
+    }
+    return CFM_OK;
+}
+
+int persistent(cfm_jacobi *h, int niter, int *launches) {
+    const cfm_jacobi_params &p = h->p;
+    const void *fn = sweep_fn_any(p, true);
+    void *in = h->buf[h->cur], *out = h->buf[h->cur ^ 1];
+    int n = niter;
+    void *args3[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &n, &h->zchunk,
+                     &h->bar};
+    void *args2[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, &n, &h->bar};
+    CFM_CUDA_TRY(launch_cooperative(fn, dim3(h->blocks), block_of(p),
+                                    p.dims == 3 ? args3 : args2, 0, h->stream));
+    h->cur ^= (niter & 1);
+    ++*launches;
+    return CFM_OK;
+}
+
+int reset_barrier(cfm_jacobi *h) {
+    BarrierState s{};
+    s.timeout_ns = barrier_timeout_ns();
+    CFM_CUDA_TRY(cudaMemcpyAsync(h->bar, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+    return CFM_OK;
+}
+
+// Enqueues the sweeps (no synchronisation).
+int enqueue_sweeps(cfm_jacobi *h, int niter, int *launches) {
+    if (niter == 0) return CFM_OK;
+    int st;
+    if (h->p.impl != CFM_JACOBI_HOST_LOOP) {
+        st = h->p.precision == CFM_FP64 ? launch_edge_preset<double>(h)
+                                        : launch_edge_preset<float>(h);
+        if (st) return st;
+        ++*launches;
+    }
+    switch (h->p.impl) {
+        case CFM_JACOBI_HOST_LOOP: return host_loop_copy(h, niter, launches);
+        case CFM_JACOBI_HOST_LOOP_INKERNEL_HALO: return host_loop_images(h, niter, launches);
+        default: return persistent(h, niter, launches);
+    }
+}
+
+int finish_run(cfm_jacobi *h, int niter, int launches, double extra_h2d, double extra_d2h,
+               cfm_stats *st) {
+    CFM_CUDA_TRY(cudaEventRecord(h->ev1, h->stream));
+    CFM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    BarrierState s{};
+    CFM_CUDA_TRY(cudaMemcpy(&s, h->bar, sizeof(s), cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    CFM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    int status = CFM_OK;
+    if (s.error) {
+        set_error("grid barrier %d timed out", s.where);
+        status = CFM_BARRIER_TIMEOUT;
+    }
+    if (st) {
+        const cfm_jacobi_params &p = h->p;
+        std::memset(st, 0, sizeof(*st));
+        const double lup = (double)(p.nx - 2) * (p.ny - 2) * (p.dims == 3 ? (p.nz - 2) : 1);
+        st->seconds = ms * 1e-3;
+        st->iterations = niter;
+        st->lups = lup * niter;
+        st->glups = st->seconds > 0 ? st->lups / st->seconds * 1e-9 : 0.0;
+        st->bytes = st->lups * 2.0 * (double)h->esize;
+        st->gbs = st->seconds > 0 ? st->bytes / st->seconds * 1e-9 : 0.0;
+        st->h2d_bytes = extra_h2d;
+        st->d2h_bytes = extra_d2h;
+        st->launches = launches;
+        st->status = status;
+    }
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfm_jacobi_problem_host(const cfm_jacobi_params *p, int problem, void *host_grid) {
+    int st = check_params(p);
+    if (st) return st;
+    CFM_ARG_CHECK(host_grid, "host_grid is null");
+    CFM_ARG_CHECK(problem == CFM_PROBLEM_REF || problem == CFM_PROBLEM_CONFIG, "problem");
+    if (p->precision == CFM_FP64)
+        host_problem<double>(p, problem, (double *)host_grid);
+    else
+        host_problem<float>(p, problem, (float *)host_grid);
+    return CFM_OK;
+}
+
+int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out) {
+    clear_error();
+    int st = check_params(p);
+    if (st) return st;
+    CFM_ARG_CHECK(out, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error("no CUDA device visible");
+        return CFM_NO_DEVICE;
+    }
+    cfm_jacobi *h = new cfm_jacobi();
+    h->p = *p;
+    if (h->p.dims == 2) {
+        h->p.nz = 1;
+        h->p.periodic_y = 1;
+    }
+    h->elems = grid_elems(&h->p);
+    h->esize = p->precision == CFM_FP64 ? 8 : 4;
+    auto fail = [&](int s) {
+        cfm_jacobi_destroy(h);
+        return s;
+    };
+    cudaError_t e;
+    for (int i = 0; i < 2; ++i) {
+        if ((e = cudaMalloc(&h->buf[i], h->elems * h->esize)) != cudaSuccess) {
+            set_error("cudaMalloc of %zu bytes failed: %s", h->elems * h->esize,
+                      cudaGetErrorString(e));
+            cudaGetLastError();
+            return fail(e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR);
+        }
+    }
+    if ((e = cudaMalloc(&h->bar, sizeof(BarrierState))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev0)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+        set_error("handle setup failed: %s", cudaGetErrorString(e));
+        return fail(CFM_CUDA_ERROR);
+    }
+    h->own_stream = true;
+    if ((st = choose_launch(h))) return fail(st);
+    for (int i = 0; i < 2; ++i)
+        if ((e = cudaMemset(h->buf[i], 0, h->elems * h->esize)) != cudaSuccess) {
+            set_error("cudaMemset failed: %s", cudaGetErrorString(e));
+            return fail(CFM_CUDA_ERROR);
+        }
+    *out = h;
+    return CFM_OK;
+}
+
+void cfm_jacobi_destroy(cfm_jacobi *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int i = 0; i < 2; ++i)
+        if (h->buf[i]) cudaFree(h->buf[i]);
+    if (h->bar) cudaFree(h->bar);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int cfm_jacobi_set_stream(cfm_jacobi *h, void *cuda_stream) {
+    CFM_ARG_CHECK(h, "handle is null");
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (!cuda_stream) {
+        if (!h->own_stream) {
+            CFM_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            h->own_stream = true;
+        }
+        return CFM_OK;
+    }
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->own_stream = false;
+    h->stream = (cudaStream_t)cuda_stream;
+    return CFM_OK;
+}
+
+int cfm_jacobi_load_problem(cfm_jacobi *h, int problem) {
+    CFM_ARG_CHECK(h, "handle is null");
+    CFM_ARG_CHECK(problem == CFM_PROBLEM_REF || problem == CFM_PROBLEM_CONFIG, "problem");
+    const cfm_jacobi_params &p = h->p;
+    std::vector<double> sy, sz(1, 0.0);
+    if (p.dims == 2) {
+        const double pi_t = p.precision == CFM_FP64 ? 2.0 * std::asin(1.0)
+                                                    : (double)(float)(2.0 * std::asin(1.0));
+        sy.resize(p.ny);
+        for (int y = 0; y < p.ny; ++y) sy[y] = std::sin(2.0 * pi_t * (double)y / (double)(p.ny - 1));
+    } else {
+        sin_factors(p.ny, sy);
+        sin_factors(p.nz, sz);
+    }
+    double *d = nullptr;
+    CFM_CUDA_TRY(cudaMalloc(&d, sizeof(double) * (sy.size() + sz.size())));
+    cudaError_t e = cudaMemcpy(d, sy.data(), sizeof(double) * sy.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d + sy.size(), sz.data(), sizeof(double) * sz.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const int nz = p.dims == 3 ? p.nz : 1;
+        for (int i = 0; i < 2; ++i) {
+            if (p.precision == CFM_FP64)
+                load_problem_kernel<double><<<4 * h->num_sms, 256, 0, h->stream>>>(
+                    (double *)h->buf[i], p.dims, p.nx, p.ny, nz, problem, d, d + sy.size());
+            else
+                load_problem_kernel<float><<<4 * h->num_sms, 256, 0, h->stream>>>(
+                    (float *)h->buf[i], p.dims, p.nx, p.ny, nz, problem, d, d + sy.size());
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(d);
+    CFM_CUDA_TRY(e);
+    h->cur = 0;
+    return CFM_OK;
+}
+
+int cfm_jacobi_upload(cfm_jacobi *h, const void *host_grid) {
+    CFM_ARG_CHECK(h && host_grid, "null argument");
+    const size_t bytes = h->elems * h->esize;
+    CFM_CUDA_TRY(cudaMemcpyAsync(h->buf[0], host_grid, bytes, cudaMemcpyHostToDevice, h->stream));
+    CFM_CUDA_TRY(cudaMemcpyAsync(h->buf[1], h->buf[0], bytes, cudaMemcpyDeviceToDevice, h->stream));
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->cur = 0;
+    return CFM_OK;
+}
+
+int cfm_jacobi_download(cfm_jacobi *h, void *host_grid) {
+    CFM_ARG_CHECK(h && host_grid, "null argument");
+    CFM_CUDA_TRY(cudaMemcpyAsync(host_grid, h->buf[h->cur], h->elems * h->esize,
+                                 cudaMemcpyDeviceToHost, h->stream));
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return CFM_OK;
+}
+
+int cfm_jacobi_run(cfm_jacobi *h, int niter, cfm_stats *st) {
+    CFM_ARG_CHECK(h, "handle is null");
+    CFM_ARG_CHECK(niter >= 0, "niter must be >= 0");
+    clear_error();
+    int s = reset_barrier(h);
+    if (s) return s;
+    int launches = 0;
+    CFM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+    s = enqueue_sweeps(h, niter, &launches);
+    if (s) return s;
+    return finish_run(h, niter, launches, 0, 0, st);
+}
+
+int cfm_jacobi_run_host(cfm_jacobi *h, int niter, const void *host_in, void *host_out,
+                        cfm_stats *st) {
+    CFM_ARG_CHECK(h && host_in && host_out, "null argument");
+    CFM_ARG_CHECK(niter >= 0, "niter must be >= 0");
+    clear_error();
+    int s = reset_barrier(h);
+    if (s) return s;
+    const size_t bytes = h->elems * h->esize;
+    int launches = 0;
+    CFM_CUDA_TRY(cudaEventRecord(h->ev0, h->stream));
+    h->cur = 0;
+    CFM_CUDA_TRY(cudaMemcpyAsync(h->buf[0], host_in, bytes, cudaMemcpyHostToDevice, h->stream));
+    CFM_CUDA_TRY(cudaMemcpyAsync(h->buf[1], h->buf[0], bytes, cudaMemcpyDeviceToDevice, h->stream));
+    s = enqueue_sweeps(h, niter, &launches);
+    if (s) return s;
+    CFM_CUDA_TRY(cudaMemcpyAsync(host_out, h->buf[h->cur], bytes, cudaMemcpyDeviceToHost,
+                                 h->stream));
+    return finish_run(h, niter, launches, (double)bytes, (double)bytes, st);
+}
+
+void *cfm_jacobi_device_grid(cfm_jacobi *h) { return h ? h->buf[h->cur] : nullptr; }
+
+int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads) {
+    CFM_ARG_CHECK(h, "handle is null");
+    if (blocks) *blocks = h->blocks;
+    if (threads) *threads = h->threads;
+    return CFM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+/*
+ * cfm.h -- C ABI of libcfm.so, the single-GPU (B200, sm_100a) CPU-free
+ * iterative-solver library: Jacobi 2d5p / 3d7p sweeps and conjugate
+ * gradient, each run as one persistent kernel that loops on the device
+ * behind grid barriers.
+ *
+ * Conventions
+ *  - Every entry point returns a cfm_status (int); no entry point exits the
+ *    process.  cfm_last_error() gives a one-line description of the last
+ *    failure seen by the calling thread.
+ *  - Grids are row-major with x fastest: a[(z * ny + y) * nx + x].
+ *    Cells x = 0 and x = nx-1 are fixed (Dirichlet) columns/faces.
+ *    Rows y = 0, ny-1 (2D) and planes z = 0, nz-1 (3D) are periodic halo
+ *    copies of rows ny-2, 1 (planes nz-2, 1), exactly as the reference's
+ *    single-GPU run copies them after every sweep.
+ *  - Host buffers passed in are owned by the caller.  Device buffers are
+ *    owned by the library handle unless an entry point says otherwise.
+ *  - Calls on one handle must come from one thread at a time.  Each handle
+ *    issues all its work on one CUDA stream (its own, or the one set with
+ *    the *_set_stream call).
+ *
+ * Reference interfaces these replace (paths within ParCoreLab/CPU-Free-model):
+ *  - Stencil version table entry `int init(int argc, char **argv)`
+ *      Stencil/jacobi2D/include/common.h:20, Stencil/jacobi3D/src/main.cu:31-53
+ *  - single-GPU oracle `double single_gpu(nx, ny, iter_max, real *a_ref_h, ...)`
+ *      Stencil/jacobi2D/src/common.cu:154-273, Stencil/jacobi3D/src/common.cu:110-239
+ *  - CG version table entry `initfunc_t(int *dRowPtr, int *dCol, real *dVal,
+ *      int n, int nnz, bool zero_indexed, int iter_max, real *x_final, ...)`
+ *      CG/include/common.h:122-127
+ */
+#ifndef CFM_H
+#define CFM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFM_API_VERSION 1
+
+typedef enum cfm_status {
+    CFM_OK = 0,
+    CFM_BAD_ARG = 1,          /* invalid sizes, null pointers, unknown enum value */
+    CFM_CUDA_ERROR = 2,       /* a CUDA runtime call failed (see cfm_last_error) */
+    CFM_BARRIER_TIMEOUT = 3,  /* a device grid barrier wait ran out of its time budget */
+    CFM_BREAKDOWN = 4,        /* CG: non-finite or non-positive curvature (alpha/beta) */
+    CFM_NOT_CONVERGED = 5,    /* CG: iteration cap reached before the tolerance */
+    CFM_NO_DEVICE = 6,        /* no CUDA device visible */
+    CFM_UNSUPPORTED = 7,      /* request not supported by this build (e.g. grid too large) */
+    CFM_OUT_OF_MEMORY = 8     /* device allocation failed */
+} cfm_status;
+
+typedef enum cfm_precision { CFM_FP64 = 0, CFM_FP32 = 1 } cfm_precision;
+
+/* Initial-state generators.
+ * CFM_PROBLEM_REF: the reference's own initial grid (2D: x columns at
+ *   sin(2*pi*y/(ny-1)); 3D: x=0 face at z - y - (nx-1), x=nx-1 face 0,
+ *   Stencil/jacobi3D/src/common.cu:15-29).
+ * CFM_PROBLEM_CONFIG: 2D as REF; 3D both x faces at
+ *   sin(2*pi*y/(ny-1)) * sin(2*pi*z/(nz-1)), periodic in y and z. */
+typedef enum cfm_problem { CFM_PROBLEM_REF = 0, CFM_PROBLEM_CONFIG = 1 } cfm_problem;
+
+/* Jacobi implementations, named for the reference version they stand in for
+ * on one GPU. */
+typedef enum cfm_jacobi_impl {
+    /* "Baseline Copy": one kernel launch per sweep plus cudaMemcpyAsync halo
+     * copies, host-controlled (Stencil/jacobi3D/src/baseline/multi-threaded-copy.cu) */
+    CFM_JACOBI_HOST_LOOP = 0,
+    /* "Baseline P2P": one launch per sweep, halos written by the kernel
+     * (Stencil/jacobi3D/src/baseline/multi-threaded-p2p.cu) */
+    CFM_JACOBI_HOST_LOOP_INKERNEL_HALO = 1,
+    /* "Design 1"/"Design 2": CPU-free, one cooperative launch for all sweeps,
+     * device grid barrier between sweeps (Stencil/jacobi2D/src/single-stream/
+     * multi-threaded-two-block-comm.cu:9-105) */
+    CFM_JACOBI_PERSISTENT = 2,
+    /* "PERKS": CPU-free with each block's tile resident on chip across sweeps
+     * (Stencil/jacobi2D/PERKS/jacobi-general-kernel.cuh:22-505) */
+    CFM_JACOBI_RESIDENT = 3
+} cfm_jacobi_impl;
+
+typedef struct cfm_stats {
+    double seconds;       /* device time of the solve, CUDA events on the handle's stream */
+    long long iterations; /* sweeps (Jacobi) or CG iterations performed */
+    double lups;          /* lattice-point updates (Jacobi) */
+    double glups;         /* lups / seconds / 1e9 */
+    double bytes;         /* algorithmic HBM bytes of the solve (16 B/LUP FP64, 8 FP32 for Jacobi) */
+    double gbs;           /* bytes / seconds / 1e9 */
+    double residual;      /* CG: final FP64 true relative residual ||b-Ax||/||b|| */
+    double h2d_bytes;     /* host->device bytes copied inside the call */
+    double d2h_bytes;     /* device->host bytes copied inside the call */
+    int launches;         /* kernel launches issued inside the timed region */
+    int status;           /* cfm_status of the run */
+    int refinements;      /* CG mixed precision: outer refinement sweeps */
+    int pad;
+} cfm_stats;
+
+/* ------------------------------------------------------------------ misc */
+int cfm_api_version(void);
+const char *cfm_status_string(int status);
+const char *cfm_last_error(void);
+/* Budget of every device grid-barrier wait, in milliseconds (default 2000). */
+int cfm_set_barrier_timeout_ms(double ms);
+/* Number of SMs and max co-resident blocks reported for the current device. */
+int cfm_device_info(int *num_sms, int *cc_major, int *cc_minor);
+
+/* --------------------------------------------------------------- Jacobi */
+typedef struct cfm_jacobi_params {
+    int dims;       /* 2 (5-point) or 3 (7-point) */
+    int nx, ny, nz; /* grid including fixed columns and halo rows/planes; nz ignored for 2D */
+    int precision;  /* cfm_precision */
+    int periodic_y; /* 3D only: 1 = rows y=0, ny-1 are periodic halos too (CONFIG problem) */
+    int impl;       /* cfm_jacobi_impl */
+} cfm_jacobi_params;
+
+typedef struct cfm_jacobi cfm_jacobi;
+
+/* Fill a caller-owned host grid (nx*ny*nz elements of the params' precision)
+ * with the initial state of `problem`.  Host-side; needs no GPU.
+ * Replaces initialize_boundaries (Stencil/jacobi2D/src/common.cu:15-26,
+ * Stencil/jacobi3D/src/common.cu:15-29) plus the zero memsets. */
+int cfm_jacobi_problem_host(const cfm_jacobi_params *p, int problem, void *host_grid);
+
+/* Allocate the two device grids of the ping-pong pair and the barrier state. */
+int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out);
+void cfm_jacobi_destroy(cfm_jacobi *h);
+int cfm_jacobi_set_stream(cfm_jacobi *h, void *cuda_stream);
+/* Device-side equivalent of cfm_jacobi_problem_host into the handle's grid. */
+int cfm_jacobi_load_problem(cfm_jacobi *h, int problem);
+/* Copy a caller-owned host grid in / the current grid out (blocking). */
+int cfm_jacobi_upload(cfm_jacobi *h, const void *host_grid);
+int cfm_jacobi_download(cfm_jacobi *h, void *host_grid);
+/* Run `niter` sweeps on the device-resident grid; stats optional.
+ * The result equals the reference single_gpu() run for niter sweeps on the
+ * same initial grid (Stencil/jacobi3D/src/common.cu:110-239). */
+int cfm_jacobi_run(cfm_jacobi *h, int niter, cfm_stats *st);
+/* End-to-end call: upload host_in, run niter sweeps, download into host_out.
+ * stats->seconds covers both copies and the sweeps. */
+int cfm_jacobi_run_host(cfm_jacobi *h, int niter, const void *host_in, void *host_out,
+                        cfm_stats *st);
+/* Device pointer of the current grid (valid until the next run/destroy). */
+void *cfm_jacobi_device_grid(cfm_jacobi *h);
+/* Blocks and threads the persistent kernels launch with on this device. */
+int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads);
+
+/* ------------------------------------------------------------------- CG */
+typedef enum cfm_cg_impl {
+    /* "Single GPU Discrete Standard": kernel per operation, host reads the
+     * dots every iteration (CG/src/common.cu:399-538) */
+    CFM_CG_DISCRETE = 0,
+    /* "Single Stream Standard": whole CG in one persistent kernel
+     * (CG/src/single-stream/standard.cu:158-299) */
+    CFM_CG_PERSISTENT = 1,
+    /* "Single Stream Pipelined" (CG/src/single-stream/pipelined.cu:176-330) */
+    CFM_CG_PERSISTENT_PIPELINED = 2,
+    /* FP32 inner persistent CG inside an FP64 iterative-refinement loop */
+    CFM_CG_MIXED = 3
+} cfm_cg_impl;
+
+typedef struct cfm_csr cfm_csr;
+
+/* Upload a CSR matrix from caller-owned host arrays.  The index base (0 or 1)
+ * is taken from rowptr[0], as the reference's main does (CG/src/main.cu:180-187). */
+int cfm_csr_create(int n, long long nnz, const int *rowptr, const int *col, const double *val,
+                   cfm_csr **out);
+void cfm_csr_destroy(cfm_csr *A);
+/* y = A x with host vectors (FP64, deterministic row order). */
+int cfm_csr_spmv_host(const cfm_csr *A, const double *x, double *y);
+
+typedef struct cfm_cg_params {
+    int impl;          /* cfm_cg_impl */
+    int maxiter;       /* iteration cap; with tol <= 0 exactly maxiter iterations run */
+    double tol;        /* relative residual target ||r||/||b||; <= 0 = fixed count (reference -niter) */
+    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = default 200) */
+    double inner_tol;  /* CFM_CG_MIXED: relative reduction per sweep (0 = default 1e-4) */
+} cfm_cg_params;
+
+typedef struct cfm_cg cfm_cg;
+
+int cfm_cg_create(const cfm_csr *A, const cfm_cg_params *p, cfm_cg **out);
+void cfm_cg_destroy(cfm_cg *h);
+int cfm_cg_set_stream(cfm_cg *h, void *cuda_stream);
+/* Solve A x = b from x0 = 0 with host vectors; b == NULL means b = ones, the
+ * reference's right-hand side (CG/src/common.cu:133-140). */
+int cfm_cg_solve(cfm_cg *h, const double *b_host, double *x_host, cfm_stats *st);
+/* Same with device vectors (length n, FP64). */
+int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st);
+
+/* ------------------------------------------------------------ generators */
+/* Number of nonzeros of the 7-point Dirichlet Poisson matrix on gx*gy*gz cells. */
+long long cfm_poisson3d_nnz(int gx, int gy, int gz);
+/* 7-point Poisson matrix (diagonal 6, off-diagonals -1, Dirichlet boundary
+ * eliminated), 0-based CSR with sorted columns, into caller arrays of size
+ * n+1, nnz, nnz. */
+int cfm_poisson3d_csr(int gx, int gy, int gz, int *rowptr, int *col, double *val);
+/* The reference's random tridiagonal test matrix (CG/src/common.cu:46-76),
+ * drawn from libc rand() in its default state; nnz = 3n-2. */
+int cfm_tridiag_csr(int n, int *rowptr, int *col, double *val);
+/* n doubles uniform in [lo, hi) from a Philox-4x32-10 stream keyed by seed. */
+int cfm_uniform(unsigned long long seed, long long n, double lo, double hi, double *out);
+
+/* One Philox-4x32-10 block (counter, key) -> 4 words; the generator behind
+ * cfm_uniform, exported for its known-answer test. */
+int cfm_philox4x32_10(const unsigned int ctr[4], const unsigned int key[2], unsigned int out[4]);
+
+/* -------------------------------------------------------------- testing */
+/* Launch a persistent kernel of `blocks` blocks (0 = device default) that
+ * meets `rounds` grid barriers; when drop_block >= 0 that block skips its
+ * arrival at the first barrier.  Returns CFM_OK or CFM_BARRIER_TIMEOUT; the
+ * device stays usable either way. elapsed_ms (optional) gets the kernel time. */
+int cfm_barrier_selftest(int blocks, int rounds, int drop_block, double *elapsed_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFM_H */

@@ -1,0 +1,168 @@
+"""ctypes binding of the CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline and
+--impl reference legs, always as the checker or the timed host baseline,
+never as the thing measured.  See cfm_oracle.h for the reference lines each
+function restates.  Also exposes the reference's own single-GPU Jacobi runs
+(oracle/_ref, built from the reference sources) when they were built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF2D_PATH = os.path.join(HERE, "_ref", "libref_jacobi2d.so")
+REF3D_PATH = os.path.join(HERE, "_ref", "libref_jacobi3d.so")
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} missing: run `make -C oracle`")
+    lib = ctypes.CDLL(LIB_PATH)
+    sigs = {
+        "orc_jacobi2d_init_f64": [_i, _i, _vp],
+        "orc_jacobi2d_init_f32": [_i, _i, _vp],
+        "orc_jacobi3d_init_f64": [_i, _i, _i, _i, _vp],
+        "orc_jacobi3d_init_f32": [_i, _i, _i, _i, _vp],
+        "orc_jacobi2d_f64": [_i, _i, _i, _vp, _vp, _i],
+        "orc_jacobi2d_f32": [_i, _i, _i, _vp, _vp, _i],
+        "orc_jacobi3d_f64": [_i, _i, _i, _i, _i, _vp, _vp, _i],
+        "orc_jacobi3d_f32": [_i, _i, _i, _i, _i, _vp, _vp, _i],
+        "orc_jacobi2d_mirror_f32": [_i, _i, _i, _vp, _vp, _i],
+        "orc_cg": [_i, _vp, _vp, _vp, _vp, _i, ctypes.c_double, _vp, _vp, _vp, _i],
+        "orc_spmv": [_i, _vp, _vp, _vp, _vp, _vp, _i],
+        "orc_max_threads": [],
+    }
+    for name, args in sigs.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.orc_dot.argtypes = [ctypes.c_longlong, _vp, _vp, _i]
+    lib.orc_dot.restype = ctypes.c_double
+    lib.orc_jacobi3d_bench_f64.argtypes = [_i, _i, _i, _i, _i]
+    lib.orc_jacobi3d_bench_f64.restype = ctypes.c_double
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _suffix(dtype):
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def max_threads():
+    return lib.orc_max_threads()
+
+
+def jacobi2d_init(nx, ny, dtype=np.float64):
+    a = np.empty((ny, nx), dtype)
+    assert getattr(lib, f"orc_jacobi2d_init_{_suffix(dtype)}")(nx, ny, _p(a)) == 0
+    return a
+
+
+def jacobi3d_init(nx, ny, nz, problem, dtype=np.float64):
+    a = np.empty((nz, ny, nx), dtype)
+    assert getattr(lib, f"orc_jacobi3d_init_{_suffix(dtype)}")(nx, ny, nz, problem, _p(a)) == 0
+    return a
+
+
+def jacobi2d(a, niter, threads=0):
+    a = np.ascontiguousarray(a)
+    ny, nx = a.shape
+    out = np.empty_like(a)
+    assert getattr(lib, f"orc_jacobi2d_{_suffix(a.dtype)}")(nx, ny, niter, _p(a), _p(out), threads) == 0
+    return out
+
+
+def jacobi2d_mirror(a, niter, threads=0):
+    a = np.ascontiguousarray(a, np.float32)
+    ny, nx = a.shape
+    out = np.empty_like(a)
+    assert lib.orc_jacobi2d_mirror_f32(nx, ny, niter, _p(a), _p(out), threads) == 0
+    return out
+
+
+def jacobi3d(a, niter, periodic_y=0, threads=0):
+    a = np.ascontiguousarray(a)
+    nz, ny, nx = a.shape
+    out = np.empty_like(a)
+    fn = getattr(lib, f"orc_jacobi3d_{_suffix(a.dtype)}")
+    assert fn(nx, ny, nz, niter, periodic_y, _p(a), _p(out), threads) == 0
+    return out
+
+
+def jacobi3d_bench(n, niter, threads=0):
+    """Seconds of `niter` FP64 sweeps of the n^3 periodic config problem (loop only)."""
+    return lib.orc_jacobi3d_bench_f64(n, n, n, niter, threads)
+
+
+def dot(a, b, threads=0):
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    return lib.orc_dot(len(a), _p(a), _p(b), threads)
+
+
+def spmv(rowptr, col, val, x, threads=0):
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty(len(rowptr) - 1)
+    assert lib.orc_spmv(len(y), _p(rowptr), _p(col), _p(val), _p(x), _p(y), threads) == 0
+    return y
+
+
+def cg(rowptr, col, val, b, maxiter, tol, threads=0):
+    """Returns (x, status, iterations, true relative residual)."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    n = len(rowptr) - 1
+    x = np.empty(n)
+    it = ctypes.c_longlong()
+    rr = ctypes.c_double()
+    bb = None if b is None else np.ascontiguousarray(b, np.float64)
+    st = lib.orc_cg(n, _p(rowptr), _p(col), _p(val), None if bb is None else _p(bb), maxiter, tol,
+                    _p(x), ctypes.byref(it), ctypes.byref(rr), threads)
+    return x, st, it.value, rr.value
+
+
+# ------------------------------------------------------ the reference itself
+def ref_available():
+    return os.path.exists(REF2D_PATH) and os.path.exists(REF3D_PATH)
+
+
+def _ref_lib(path, names):
+    lib = ctypes.CDLL(path)
+    for name, args in names.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_double
+    return lib
+
+
+def ref_jacobi2d(nx, ny, niter, mirror=False):
+    """The reference's single_gpu() (FP32, its own init) on the current GPU."""
+    lib = _ref_lib(REF2D_PATH, {"ref_jacobi2d_single_gpu": [_i, _i, _i, _vp],
+                                "ref_jacobi2d_single_gpu_mirror": [_i, _i, _i, _vp]})
+    out = np.empty((ny, nx), np.float32)
+    fn = lib.ref_jacobi2d_single_gpu_mirror if mirror else lib.ref_jacobi2d_single_gpu
+    fn(nx, ny, niter, _p(out))
+    return out
+
+
+def ref_jacobi3d(nx, ny, nz, niter):
+    lib = _ref_lib(REF3D_PATH, {"ref_jacobi3d_single_gpu": [_i, _i, _i, _i, _vp]})
+    out = np.empty((nz, ny, nx), np.float32)
+    lib.ref_jacobi3d_single_gpu(nx, ny, nz, niter, _p(out))
+    return out

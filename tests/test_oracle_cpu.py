@@ -1,0 +1,203 @@
+"""The CPU oracle against independent restatements (numpy, SciPy) and against
+the reference's own outputs (golden fixtures).  No GPU needed."""
+import glob
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import oracle
+from conftest import GOLDEN
+
+
+# ---------------------------------------------------------------- numpy restatements
+def np_jacobi2d(a, niter):
+    """Vectorised single_gpu() (Stencil/jacobi2D/src/common.cu:154-273)."""
+    a = a.copy()
+    b = a.copy()
+    q = 0.25 if a.dtype == np.float64 else np.float32(0.25)
+    for _ in range(niter):
+        s = a[1:-1, 2:] + a[1:-1, :-2]
+        s = s + a[2:, 1:-1]
+        s = s + a[:-2, 1:-1]
+        b[1:-1, 1:-1] = q * s
+        b[0, :] = b[-2, :]
+        b[-1, :] = b[1, :]
+        a, b = b, a
+    return a
+
+
+def np_jacobi3d(a, niter, periodic_y):
+    """Vectorised 3D single_gpu() (Stencil/jacobi3D/src/common.cu:110-239)."""
+    a = a.copy()
+    b = a.copy()
+    c6 = a.dtype.type(1) / a.dtype.type(6)
+    for _ in range(niter):
+        s = a[1:-1, 1:-1, 2:] + a[1:-1, 1:-1, :-2]
+        s = s + a[1:-1, 2:, 1:-1]
+        s = s + a[1:-1, :-2, 1:-1]
+        s = s + a[2:, 1:-1, 1:-1]
+        s = s + a[:-2, 1:-1, 1:-1]
+        b[1:-1, 1:-1, 1:-1] = c6 * s
+        if periodic_y:
+            b[1:-1, 0, :] = b[1:-1, -2, :]
+            b[1:-1, -1, :] = b[1:-1, 1, :]
+        b[0] = b[-2]
+        b[-1] = b[1]
+        a, b = b, a
+    return a
+
+
+def rand_grid(shape, dtype, seed):
+    return np.random.default_rng(seed).uniform(-1, 1, shape).astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("shape,niter", [((3, 3), 1), ((9, 7), 5), ((17, 33), 11), ((40, 24), 0)])
+def test_oracle_jacobi2d_matches_numpy(dtype, shape, niter):
+    a = rand_grid(shape, dtype, 1)
+    np.testing.assert_array_equal(oracle.jacobi2d(a, niter), np_jacobi2d(a, niter))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("periodic_y", [0, 1])
+@pytest.mark.parametrize("shape,niter", [((3, 3, 3), 2), ((5, 6, 7), 4), ((9, 17, 12), 9)])
+def test_oracle_jacobi3d_matches_numpy(dtype, periodic_y, shape, niter):
+    a = rand_grid(shape, dtype, 2)
+    np.testing.assert_array_equal(oracle.jacobi3d(a, niter, periodic_y),
+                                  np_jacobi3d(a, niter, periodic_y))
+
+
+def test_oracle_thread_count_does_not_change_results():
+    a = rand_grid((20, 30, 40), np.float64, 3)
+    np.testing.assert_array_equal(oracle.jacobi3d(a, 6, 1, threads=1), oracle.jacobi3d(a, 6, 1, threads=7))
+
+
+def test_oracle_mirror_matches_numpy():
+    a = rand_grid((12, 64), np.float32, 4)
+    ref = a.copy()
+    b = a.copy()
+    for _ in range(5):
+        e = np.concatenate([ref[1:-1, 1:], ref[1:-1, -1:]], axis=1)
+        w = np.concatenate([ref[1:-1, :1], ref[1:-1, :-1]], axis=1)
+        s = ref[2:, :] + ref[:-2, :]
+        s = s + e
+        s = s + w
+        b[1:-1, :] = np.float32(0.25) * s
+        b[0] = b[-2]
+        b[-1] = b[1]
+        ref, b = b, ref
+    np.testing.assert_array_equal(oracle.jacobi2d_mirror(a, 5), ref)
+
+
+def test_oracle_init_3d_reference_quirk():
+    # x = 0 face is z - y - (nx - 1) (last write of the ix loop), x = nx-1 face 0
+    a = oracle.jacobi3d_init(6, 5, 4, 0, np.float32)
+    z, y = np.meshgrid(np.arange(4), np.arange(5), indexing="ij")
+    np.testing.assert_array_equal(a[:, :, 0], (z - y - 5).astype(np.float32))
+    assert not a[:, :, 1:].any()
+
+
+def test_oracle_init_config():
+    nx, ny, nz = 7, 9, 11
+    a = oracle.jacobi3d_init(nx, ny, nz, 1, np.float64)
+    f = np.outer(np.sin(2 * np.pi * np.arange(nz) / (nz - 1)), np.sin(2 * np.pi * np.arange(ny) / (ny - 1)))
+    np.testing.assert_allclose(a[:, :, 0], f, rtol=0, atol=1e-15)
+    np.testing.assert_array_equal(a[:, :, 0], a[:, :, -1])
+    assert not a[:, :, 1:-1].any()
+    b = oracle.jacobi2d_init(8, 10, np.float64)
+    np.testing.assert_allclose(b[:, 0], np.sin(2 * np.pi * np.arange(10) / 9), atol=1e-15)
+
+
+# ------------------------------------------------------------- reference fixtures
+def _fixtures():
+    return sorted(glob.glob(os.path.join(GOLDEN, "ref_jacobi*.npz")))
+
+
+def test_reference_fixtures_present():
+    assert _fixtures(), "tests/golden/ref_jacobi*.npz missing (made by tests/golden/make_ref_fixtures.py)"
+
+
+@pytest.mark.parametrize("path", _fixtures(), ids=os.path.basename)
+def test_oracle_matches_reference_run(path):
+    """Pin: the oracle reproduces grids written by the reference's own
+    single_gpu() bit-for-bit (FP32, reference initial state)."""
+    f = np.load(path)
+    out = f["out"]
+    niter = int(f["niter"])
+    kind = str(f["kind"])
+    if kind == "2d":
+        ny, nx = out.shape
+        a = oracle.jacobi2d_init(nx, ny, np.float32)
+        # the boundary columns were computed by the reference with device sin;
+        # they are never changed by a sweep, so the output carries them
+        np.testing.assert_array_equal(a[1:-1, 0], out[1:-1, 0])
+        np.testing.assert_array_equal(oracle.jacobi2d(a, niter), out)
+    elif kind == "2d_mirror":
+        ny, nx = out.shape
+        a = oracle.jacobi2d_init(nx, ny, np.float32)
+        np.testing.assert_array_equal(oracle.jacobi2d_mirror(a, niter), out)
+    else:
+        nz, ny, nx = out.shape
+        a = oracle.jacobi3d_init(nx, ny, nz, 0, np.float32)
+        np.testing.assert_array_equal(oracle.jacobi3d(a, niter, 0), out)
+
+
+# -------------------------------------------------------------------------- CG
+def poisson_scipy(g):
+    one = sp.diags([-1.0, 2.0, -1.0], [-1, 0, 1], shape=(g, g))
+    eye = sp.identity(g)
+    lap = (sp.kron(sp.kron(eye, eye), one) + sp.kron(sp.kron(eye, one), eye) +
+           sp.kron(sp.kron(one, eye), eye)).tocsr()
+    lap.sum_duplicates()
+    lap.eliminate_zeros()
+    lap.sort_indices()
+    return lap
+
+
+def test_oracle_dot_close_to_numpy():
+    rng = np.random.default_rng(5)
+    for n in (1, 31, 1024, 1025, 5000, 100003):
+        a, b = rng.standard_normal(n), rng.standard_normal(n)
+        d = oracle.dot(a, b)
+        assert abs(d - np.dot(a, b)) <= 1e-12 * np.sum(np.abs(a * b))
+
+
+def test_oracle_spmv_matches_scipy():
+    A = poisson_scipy(6)
+    x = np.random.default_rng(6).uniform(-1, 1, A.shape[0])
+    y = oracle.spmv(A.indptr, A.indices, A.data, x)
+    np.testing.assert_allclose(y, A @ x, rtol=0, atol=1e-13)
+    # 1-based CSR gives the same result
+    y1 = oracle.spmv(A.indptr + 1, A.indices + 1, A.data, x)
+    np.testing.assert_array_equal(y, y1)
+
+
+@pytest.mark.parametrize("g", [4, 12])
+def test_oracle_cg_solves_poisson(g):
+    A = poisson_scipy(g)
+    xs = np.random.default_rng(g).uniform(-1, 1, A.shape[0])
+    b = A @ xs
+    x, st, it, rr = oracle.cg(A.indptr, A.indices, A.data, b, 20000, 1e-10)
+    assert st == 0 and rr <= 1e-10
+    np.testing.assert_allclose(x, xs, rtol=0, atol=1e-8)
+    # SciPy's CG on the same system needs about as many iterations
+    its = []
+    spla.cg(A, b, rtol=1e-10, maxiter=20000, callback=lambda _: its.append(1))
+    assert abs(it - len(its)) <= max(2, 0.05 * len(its))
+
+
+def test_oracle_cg_fixed_count_reference_mode():
+    # reference mode: b = ones, fixed iteration count, no tolerance exit
+    A = poisson_scipy(5)
+    x, st, it, rr = oracle.cg(A.indptr, A.indices, A.data, None, 30, 0.0)
+    assert st == 0 and it == 30
+    np.testing.assert_allclose(A @ x, np.ones(A.shape[0]), atol=1e-9)
+
+
+def test_oracle_cg_breakdown_on_indefinite():
+    A = sp.diags([1.0, -1.0, 2.0]).tocsr()
+    _, st, _, _ = oracle.cg(A.indptr, A.indices, A.data, np.array([1.0, 1.0, 0.0]), 10, 1e-12)
+    assert st == 4
