@@ -190,6 +190,100 @@ __global__ void __launch_bounds__(32 * TY) j3d_sweeps_kernel(T *g0, T *g1, int n
     }
 }
 
+// ---------------------------------------------------------- 2D resident sweep
+// PERKS-style temporal residency (the design of Stencil/jacobi2D/PERKS/
+// jacobi-general-kernel.cuh:22-505, re-derived): block b owns the interior
+// rows [r0, r1) and keeps them, plus one halo row above and below, in shared
+// memory for all sweeps (two copies, ping-pong).  Per sweep the only global
+// traffic is the block's first and last new rows, published to a
+// double-buffered exchange area, and its two halo rows read back from the
+// ring neighbours (b-1, b+1 mod B; the ring closes through the periodic rows,
+// so block 0's upper halo is the last block's last row).  Synchronisation is
+// point-to-point: a per-block sweep counter, bounded waits on the two
+// neighbours only, no grid-wide barrier.
+__device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024, 1)
+    j2d_resident_kernel(const T *in, T *final_out, int nx, int ny, int niter, T *xbuf,
+                        unsigned int *flags, BarrierState *bar) {
+    extern __shared__ __align__(16) unsigned char j2d_smem[];
+    const int B = gridDim.x, b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const int nrows = ny - 2;
+    const int r0 = 1 + (int)((long long)b * nrows / B);
+    const int r1 = 1 + (int)((long long)(b + 1) * nrows / B);
+    const int h = r1 - r0;
+    const int up_blk = (b + B - 1) % B, dn_blk = (b + 1) % B;
+    const size_t band = (size_t)(h + 2) * nx;
+    T *cur = reinterpret_cast<T *>(j2d_smem);
+    T *nxt = cur + band;
+    for (size_t i = tid; i < band; i += nth) {
+        const T v = in[(size_t)(r0 - 1) * nx + i];
+        cur[i] = v;
+        nxt[i] = v;
+    }
+    __syncthreads();
+    __shared__ int s_ok;
+    const int inner = nx - 2;
+    for (int t = 0; t < niter; ++t) {
+        for (int p = tid; p < h * inner; p += nth) {
+            const int r = 1 + p / inner;
+            const int x = 1 + p % inner;
+            const T *c = cur + (size_t)r * nx + x;
+            nxt[(size_t)r * nx + x] = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
+        }
+        __syncthreads();
+        T *xb = xbuf + ((size_t)(t & 1) * B + b) * 2 * nx;
+        for (int x = tid; x < nx; x += nth) {
+            __stcg(xb + x, nxt[(size_t)nx + x]);
+            __stcg(xb + nx + x, nxt[(size_t)h * nx + x]);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int ok = 1;
+            __threadfence();
+            st_release_u32(flags + b, (unsigned)(t + 1));
+            const unsigned long long t0 = global_ns();
+            const unsigned long long budget = bar->timeout_ns;
+            while (ld_acquire_u32(flags + up_blk) < (unsigned)(t + 1) ||
+                   ld_acquire_u32(flags + dn_blk) < (unsigned)(t + 1)) {
+                if (ld_relaxed_i32(&bar->error)) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > budget) {
+                    if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = t;
+                    ok = 0;
+                    break;
+                }
+            }
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        const T *up = xbuf + ((size_t)(t & 1) * B + up_blk) * 2 * nx + nx;  // last row above
+        const T *dn = xbuf + ((size_t)(t & 1) * B + dn_blk) * 2 * nx;       // first row below
+        for (int x = tid; x < nx; x += nth) {
+            nxt[x] = __ldcg(up + x);
+            nxt[(size_t)(h + 1) * nx + x] = __ldcg(dn + x);
+        }
+        __syncthreads();
+        T *tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    // write the band back; the owners of rows 1 and ny-2 also write their
+    // periodic images (full rows, so the corner cells become images too)
+    for (size_t i = tid; i < (size_t)h * nx; i += nth) final_out[(size_t)r0 * nx + i] = cur[nx + i];
+    if (r0 == 1)
+        for (int x = tid; x < nx; x += nth) final_out[(size_t)(ny - 1) * nx + x] = cur[nx + x];
+    if (r1 == ny - 1)
+        for (int x = tid; x < nx; x += nth) final_out[x] = cur[(size_t)h * nx + x];
+}
+
 // Cells on the edges of the box (two or more coordinates on the boundary) are
 // neither read nor written by a sweep.  The reference's full-row/plane halo
 // copies leave each such cell equal to its periodic image after the first
@@ -275,6 +369,12 @@ struct cfm_jacobi {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int blocks = 0, threads = 0, zchunk = 0;
     int num_sms = 0;
+    // 2D resident kernel: exchange rows, per-block sweep counters, shape
+    void *xbuf = nullptr;
+    unsigned int *flags = nullptr;
+    int res_blocks = 0;
+    size_t res_smem = 0;
+    bool resident = false;
 };
 
 namespace {
@@ -386,6 +486,26 @@ int choose_launch(cfm_jacobi *h) {
         const long long need = (nseg * 32 + threads - 1) / threads;
         if (need < h->blocks) h->blocks = (int)std::max(1LL, need);
     }
+    if (p.dims == 2 && p.impl == CFM_JACOBI_RESIDENT) {
+        // One 1024-thread block per SM, each holding its band (+2 halo rows)
+        // twice in shared memory; used only when that fits on chip.
+        const int B = std::min(di.num_sms, p.ny - 2);
+        const int hmax = (p.ny - 2 + B - 1) / B;
+        const size_t smem = 2 * (size_t)(hmax + 2) * p.nx * h->esize;
+        const void *rfn = p.precision == CFM_FP64 ? (const void *)j2d_resident_kernel<double>
+                                                  : (const void *)j2d_resident_kernel<float>;
+        if (smem <= di.smem_optin) {
+            CFM_CUDA_TRY(cudaFuncSetAttribute(rfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+            int rper = 0;
+            CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, rfn, 1024, smem));
+            if (rper >= 1) {
+                h->resident = true;
+                h->res_blocks = B;
+                h->res_smem = smem;
+            }
+        }
+    }
     return CFM_OK;
 }
 
@@ -464,8 +584,26 @@ int host_loop_images(cfm_jacobi *h, int niter, int *launches) {
     return CFM_OK;
 }
 
+int resident2d(cfm_jacobi *h, int niter, int *launches) {
+    const cfm_jacobi_params &p = h->p;
+    CFM_CUDA_TRY(cudaMemsetAsync(h->flags, 0, sizeof(unsigned int) * h->res_blocks, h->stream));
+    const void *in = h->buf[h->cur];
+    void *fin = h->buf[h->cur ^ (niter & 1)];
+    int n = niter;
+    void *args[] = {(void *)&in, &fin, (void *)&p.nx, (void *)&p.ny, &n, &h->xbuf, &h->flags,
+                    &h->bar};
+    const void *fn = p.precision == CFM_FP64 ? (const void *)j2d_resident_kernel<double>
+                                             : (const void *)j2d_resident_kernel<float>;
+    CFM_CUDA_TRY(launch_cooperative(fn, dim3(h->res_blocks), dim3(1024), args, h->res_smem,
+                                    h->stream));
+    h->cur ^= (niter & 1);
+    ++*launches;
+    return CFM_OK;
+}
+
 int persistent(cfm_jacobi *h, int niter, int *launches) {
     const cfm_jacobi_params &p = h->p;
+    if (h->resident) return resident2d(h, niter, launches);
     const void *fn = sweep_fn_any(p, true);
     void *in = h->buf[h->cur], *out = h->buf[h->cur ^ 1];
     int n = niter;
@@ -592,6 +730,14 @@ int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out) {
     }
     h->own_stream = true;
     if ((st = choose_launch(h))) return fail(st);
+    if (h->resident) {
+        const size_t xbytes = 2 * (size_t)h->res_blocks * 2 * h->p.nx * h->esize;
+        if ((e = cudaMalloc(&h->xbuf, xbytes)) != cudaSuccess ||
+            (e = cudaMalloc(&h->flags, sizeof(unsigned int) * h->res_blocks)) != cudaSuccess) {
+            set_error("exchange buffers: %s", cudaGetErrorString(e));
+            return fail(CFM_CUDA_ERROR);
+        }
+    }
     for (int i = 0; i < 2; ++i)
         if ((e = cudaMemset(h->buf[i], 0, h->elems * h->esize)) != cudaSuccess) {
             set_error("cudaMemset failed: %s", cudaGetErrorString(e));
@@ -607,6 +753,8 @@ void cfm_jacobi_destroy(cfm_jacobi *h) {
     for (int i = 0; i < 2; ++i)
         if (h->buf[i]) cudaFree(h->buf[i]);
     if (h->bar) cudaFree(h->bar);
+    if (h->xbuf) cudaFree(h->xbuf);
+    if (h->flags) cudaFree(h->flags);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
