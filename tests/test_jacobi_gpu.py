@@ -48,7 +48,8 @@ def test_jacobi2d_random_bitexact(impl, prec, shape, niter):
 @pytest.mark.parametrize("impl", IMPLS)
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("py", [0, 1])
-@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 6, 7), (17, 9, 33), (16, 40, 64), (20, 11, 131)])
+@pytest.mark.parametrize("shape", [(3, 3, 3), (5, 6, 7), (17, 9, 33), (16, 40, 64), (20, 11, 131),
+                                   (7, 13, 128), (5, 3, 200), (33, 70, 96), (9, 10, 66)])
 @pytest.mark.parametrize("niter", [1, 2, 5])
 def test_jacobi3d_random_bitexact(impl, prec, py, shape, niter):
     a = rand_grid(shape, cfm.np_dtype(prec), 12)
@@ -72,6 +73,8 @@ def test_jacobi2d_config1_problem_1024():
     """1024^2 FP64 problem, 50 sweeps, persistent and resident against the oracle."""
     a = oracle.jacobi2d_init(1024, 1024, np.float64)
     want = oracle.jacobi2d(a, 50)
+    with cfm.Jacobi(2, 1024, 1024, 1, cfm.FP64, 1, cfm.JACOBI_RESIDENT) as j:
+        assert j.launch_shape()[1] == 1024  # the on-chip resident kernel
     for impl in (cfm.JACOBI_PERSISTENT, cfm.JACOBI_RESIDENT):
         got, st = run_gpu(a, 50, impl)
         np.testing.assert_array_equal(got, want)
@@ -83,6 +86,7 @@ def test_jacobi3d_512_fp64_bitexact_and_e2e():
     end-to-end host-buffer call gives the same grid."""
     nx = ny = nz = 512
     with cfm.Jacobi(3, nx, ny, nz, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
+        assert j.launch_shape()[1] == 288  # the TMA-fed pipeline kernel
         a = j.problem_host(cfm.PROBLEM_CONFIG)
         want = oracle.jacobi3d(a, 3, 1)
         j.upload(a)
