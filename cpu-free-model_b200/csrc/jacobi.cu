@@ -113,11 +113,12 @@ __global__ void __launch_bounds__(256) j2d_sweeps_kernel(T *g0, T *g1, int nx, i
 
 // ------------------------------------------------------------------ 3D sweep
 // Work unit = (z-chunk, tile) with the tile 32 (x, aligned at x = 0) by TY
-// interior rows; units are ordered chunk-major and every block takes one
-// contiguous, equal-sized range, so blocks owning neighbouring tiles visit the
-// same planes at the same time and the tile-edge rows they share are L2 hits.
-// Inside a unit each thread marches along z keeping the z-1, z, z+1 values in
-// registers: every interior value is read from HBM once per sweep.
+// interior rows; units are ordered chunk-major and dealt to blocks round-robin
+// (block b takes units b, b + G, b + 2G, ...), so at any moment the G blocks
+// work on G consecutive units -- neighbouring tiles of the same z-chunk at the
+// same plane -- and the tile-edge rows they share are L2 hits.  Inside a unit
+// each thread marches along z keeping the z-1, z, z+1 values in registers:
+// every interior value is read from HBM once per sweep.
 template <typename T, int TY, bool PY, bool IMAGES>
 __global__ void __launch_bounds__(32 * TY) j3d_sweeps_kernel(T *g0, T *g1, int nx, int ny, int nz,
                                                              int niter, int zchunk,
@@ -130,15 +131,13 @@ __global__ void __launch_bounds__(32 * TY) j3d_sweeps_kernel(T *g0, T *g1, int n
     const int nzi = nz - 2;
     const int nch = (nzi + zchunk - 1) / zchunk;
     const long long U = ntiles * nch;
-    const long long u0 = (long long)blockIdx.x * U / gridDim.x;
-    const long long u1 = (long long)(blockIdx.x + 1) * U / gridDim.x;
     const size_t P = (size_t)nx * ny;
     const T c6 = T(1) / T(6);
     const size_t zimg = (size_t)(nz - 2) * P;
     const size_t yimg = (size_t)(ny - 2) * nx;
     T *in = g0, *out = g1;
     for (int it = 0; it < niter; ++it) {
-        for (long long u = u0; u < u1; ++u) {
+        for (long long u = blockIdx.x; u < U; u += gridDim.x) {
             const int ch = (int)(u / ntiles);
             const int tile = (int)(u - (long long)ch * ntiles);
             const int x = (tile % ntx) * 32 + lane;
@@ -255,8 +254,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
     const int nzi = nz - 2;
     const int nch = (nzi + zchunk - 1) / zchunk;
     const long long U = ntiles * nch;
-    const long long u0 = (long long)blockIdx.x * U / gridDim.x;
-    const long long u1 = (long long)(blockIdx.x + 1) * U / gridDim.x;
+    const long long G = gridDim.x;  // units are dealt round-robin (see j3d_sweeps_kernel)
     const unsigned long long budget = bar->timeout_ns;
     const size_t P = (size_t)nx * ny;
     const size_t zimg = (size_t)(nz - 2) * P;
@@ -271,7 +269,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
             // ------------------------------------------------ producer warp
             if (lane == 0) {
                 fence_proxy_async_global();
-                for (long long u = u0; u < u1 && !s_err; ++u) {
+                for (long long u = blockIdx.x; u < U && !s_err; u += G) {
                     const int ch = (int)(u / ntiles);
                     const int tile = (int)(u - (long long)ch * ntiles);
                     const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
@@ -293,7 +291,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
             __syncwarp();
         } else {
             // ------------------------------------------------ consumer warps
-            for (long long u = u0; u < u1; ++u) {
+            for (long long u = blockIdx.x; u < U; u += G) {
                 const int ch = (int)(u / ntiles);
                 const int tile = (int)(u - (long long)ch * ntiles);
                 const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
@@ -616,6 +614,34 @@ struct cfm_jacobi {
 
 namespace {
 
+// Units are dealt round-robin to G blocks, so a sweep takes ceil(U / G)
+// rounds and the last one may leave blocks idle.  Pick the longest z-chunk
+// (fewest pipeline restarts) whose rounds keep >= 97% of the blocks busy;
+// if none does, the chunk with the best efficiency.  Returns the chunk and
+// lowers *blocks when there are fewer units than blocks.
+int pick_zchunk(long long ntiles, int nzi, int *blocks) {
+    int best = 8;
+    double best_eff = -1.0;
+    for (int zc = 128; zc >= 8; zc /= 2) {
+        const int c = std::min(zc, nzi);
+        const long long U = ntiles * ((nzi + c - 1) / c);
+        const long long G = std::min<long long>(*blocks, U);
+        const double eff = (double)U / ((double)((U + G - 1) / G) * (double)G);
+        if (eff >= 0.97 && U >= *blocks) {
+            best = c;
+            best_eff = 2.0;
+            break;
+        }
+        if (eff > best_eff + 1e-9) {
+            best = c;
+            best_eff = eff;
+        }
+    }
+    const long long U = ntiles * ((nzi + best - 1) / best);
+    if (U < *blocks) *blocks = (int)std::max(1LL, U);
+    return best;
+}
+
 constexpr int J3_TY = 8;
 constexpr int TMA_TY = 8;
 constexpr int TMA_STAGES = 8;
@@ -686,12 +712,7 @@ int setup_tma(cfm_jacobi *h) {
     h->tma_blocks = per_sm * h->num_sms;
     const long long ntiles =
         (long long)((p.nx + tma_tile_x(p) - 1) / tma_tile_x(p)) * ((p.ny - 2 + TMA_TY - 1) / TMA_TY);
-    const int nzi = p.nz - 2;
-    int zc = 64;
-    while (zc > 8 && ntiles * ((nzi + zc - 1) / zc) < 8LL * h->tma_blocks) zc /= 2;
-    h->tma_zchunk = std::min(zc, nzi);
-    const long long units = ntiles * ((nzi + h->tma_zchunk - 1) / h->tma_zchunk);
-    if (units < h->tma_blocks) h->tma_blocks = (int)std::max(1LL, units);
+    h->tma_zchunk = pick_zchunk(ntiles, p.nz - 2, &h->tma_blocks);
     h->tma = true;
     return CFM_OK;
 }
@@ -787,15 +808,8 @@ int choose_launch(cfm_jacobi *h) {
     h->threads = threads;
     h->blocks = per_sm * di.num_sms;
     if (p.dims == 3) {
-        // Chunk the z range so that every block gets many units (balance to
-        // within one unit) while each unit still streams >= 16 planes.
         const long long ntiles = (long long)((p.nx + 31) / 32) * ((p.ny - 2 + J3_TY - 1) / J3_TY);
-        const int nzi = p.nz - 2;
-        int zc = 32;
-        while (zc > 8 && ntiles * ((nzi + zc - 1) / zc) < 8LL * h->blocks) zc /= 2;
-        h->zchunk = std::min(zc, nzi);
-        const long long units = ntiles * ((nzi + h->zchunk - 1) / h->zchunk);
-        if (units < h->blocks) h->blocks = (int)std::max(1LL, units);
+        h->zchunk = pick_zchunk(ntiles, p.nz - 2, &h->blocks);
     } else {
         const long long nseg = (long long)((p.nx + 31) / 32) * (p.ny - 2);
         const long long need = (nseg * 32 + threads - 1) / threads;
@@ -1072,11 +1086,17 @@ int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out) {
             return fail(CFM_CUDA_ERROR);
         }
     }
+    // Zero both grids on the handle's own (non-blocking) stream: a legacy-
+    // stream memset would not be ordered before later work on that stream.
     for (int i = 0; i < 2; ++i)
-        if ((e = cudaMemset(h->buf[i], 0, h->elems * h->esize)) != cudaSuccess) {
-            set_error("cudaMemset failed: %s", cudaGetErrorString(e));
+        if ((e = cudaMemsetAsync(h->buf[i], 0, h->elems * h->esize, h->stream)) != cudaSuccess) {
+            set_error("cudaMemsetAsync failed: %s", cudaGetErrorString(e));
             return fail(CFM_CUDA_ERROR);
         }
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
+        set_error("grid zeroing failed: %s", cudaGetErrorString(e));
+        return fail(CFM_CUDA_ERROR);
+    }
     *out = h;
     return CFM_OK;
 }
