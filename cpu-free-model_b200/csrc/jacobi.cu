@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
     const int nzi = nz - 2;
     const int nch = (nzi + zchunk - 1) / zchunk;
     const long long U = ntiles * nch;
-    const long long G = gridDim.x;  // units are dealt round-robin (see j3d_sweeps_kernel)
+    const long long NB = gridDim.x;  // units are dealt round-robin (see j3d_sweeps_kernel)
     const unsigned long long budget = bar->timeout_ns;
     const size_t P = (size_t)nx * ny;
     const size_t zimg = (size_t)(nz - 2) * P;
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
             // ------------------------------------------------ producer warp
             if (lane == 0) {
                 fence_proxy_async_global();
-                for (long long u = blockIdx.x; u < U && !s_err; u += G) {
+                for (long long u = blockIdx.x; u < U && !s_err; u += NB) {
                     const int ch = (int)(u / ntiles);
                     const int tile = (int)(u - (long long)ch * ntiles);
                     const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(32 * (TY + 1))
             __syncwarp();
         } else {
             // ------------------------------------------------ consumer warps
-            for (long long u = blockIdx.x; u < U; u += G) {
+            for (long long u = blockIdx.x; u < U; u += NB) {
                 const int ch = (int)(u / ntiles);
                 const int tile = (int)(u - (long long)ch * ntiles);
                 const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
