@@ -25,6 +25,7 @@
 
 #include "barrier.cuh"
 #include "cfm_internal.h"
+#include "j3d_tma.cuh"
 #include "tma.cuh"
 
 namespace cfm {
@@ -189,235 +190,6 @@ __global__ void __launch_bounds__(32 * TY) j3d_sweeps_kernel(T *g0, T *g1, int n
         T *t = in;
         in = out;
         out = t;
-    }
-}
-
-// ------------------------------------------------------- 3D TMA-fed sweep
-// Same work units and sum order as j3d_sweeps_kernel, but the plane tiles
-// come through a ring of STAGES shared-memory buffers filled by the tensor
-// memory accelerator: one producer warp issues cp.async.bulk.tensor loads of
-// (32*VN + 2*VN) x (TY + 2) x 1 boxes (the tile plus its x and y halos; x
-// starts VN elements early so every box is 16-byte aligned) and TY consumer
-// warps compute one row each, VN points per lane (one 16-byte vector).  Each
-// stage is released (mbarrier) by every consumer warp after its last use, so
-// up to STAGES planes stream in ahead of the compute.  All waits are bounded.
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<double> {
-    using type = double2;
-    static constexpr int N = 2;
-};
-template <>
-struct Vec16<float> {
-    using type = float4;
-    static constexpr int N = 4;
-};
-
-template <typename T, int TY, int STAGES>
-struct TmaGeom {
-    static constexpr int VN = Vec16<T>::N;
-    static constexpr int TX = 32 * VN;
-    static constexpr int BXW = TX + 2 * VN;
-    static constexpr int BYH = TY + 2;
-    static constexpr unsigned TX_BYTES = BXW * BYH * sizeof(T);
-    static constexpr unsigned STRIDE = (TX_BYTES + 127) / 128 * 128;
-    static constexpr size_t SMEM = (size_t)STAGES * STRIDE + 2 * STAGES * sizeof(uint64_t);
-    static constexpr int THREADS = 32 * (TY + 1);
-};
-
-template <typename T, int TY, int STAGES, bool PY>
-__global__ void __launch_bounds__(32 * (TY + 1))
-    j3d_tma_kernel(const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
-                   T *g0, T *g1, int nx, int ny, int nz, int niter, int zchunk, BarrierState *bar) {
-    using G = TmaGeom<T, TY, STAGES>;
-    using V = typename Vec16<T>::type;
-    constexpr int VN = G::VN, TX = G::TX, BXW = G::BXW;
-    extern __shared__ __align__(128) unsigned char tsm[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(tsm + STAGES * G::STRIDE);
-    uint64_t *empty = full + STAGES;
-    __shared__ int s_err;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&empty[s], TY);
-        }
-        s_err = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-
-    const int ntx = (nx + TX - 1) / TX;
-    const int nty = (ny - 2 + TY - 1) / TY;
-    const long long ntiles = (long long)ntx * nty;
-    const int nzi = nz - 2;
-    const int nch = (nzi + zchunk - 1) / zchunk;
-    const long long U = ntiles * nch;
-    const long long NB = gridDim.x;  // units are dealt round-robin (see j3d_sweeps_kernel)
-    const unsigned long long budget = bar->timeout_ns;
-    const size_t P = (size_t)nx * ny;
-    const size_t zimg = (size_t)(nz - 2) * P;
-    const size_t yimg = (size_t)(ny - 2) * nx;
-    const T c6 = T(1) / T(6);
-    unsigned k = 0;  // plane loads issued (producer) / consumed (consumers) so far
-
-    for (int it = 0; it < niter; ++it) {
-        const CUtensorMap *tm = (it & 1) ? &tm1 : &tm0;
-        T *out = (it & 1) ? g0 : g1;
-        if (warp == TY) {
-            // ------------------------------------------------ producer warp
-            if (lane == 0) {
-                fence_proxy_async_global();
-                for (long long u = blockIdx.x; u < U && !s_err; u += NB) {
-                    const int ch = (int)(u / ntiles);
-                    const int tile = (int)(u - (long long)ch * ntiles);
-                    const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
-                    const int z0 = 1 + ch * zchunk, z1 = min(z0 + zchunk, nz - 1);
-                    for (int z = z0 - 1; z <= z1; ++z) {
-                        const int s = k % STAGES;
-                        const unsigned ph = (k / STAGES) & 1;
-                        if (!mbar_wait_bounded(&empty[s], ph ^ 1, budget)) {
-                            if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = 1000000 + it;
-                            s_err = 1;
-                            break;
-                        }
-                        mbar_arrive_expect_tx(&full[s], G::TX_BYTES);
-                        tma_load_3d(tsm + s * G::STRIDE, tm, x0 - VN, y0 - 1, z, &full[s]);
-                        ++k;
-                    }
-                }
-            }
-            __syncwarp();
-        } else {
-            // ------------------------------------------------ consumer warps
-            for (long long u = blockIdx.x; u < U; u += NB) {
-                const int ch = (int)(u / ntiles);
-                const int tile = (int)(u - (long long)ch * ntiles);
-                const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
-                const int z0 = 1 + ch * zchunk, z1 = min(z0 + zchunk, nz - 1);
-                const int y = y0 + warp;
-                const int xb = x0 + lane * VN;
-                const bool row_ok = y <= ny - 2;
-                const int own = (warp + 1) * BXW + VN + lane * VN;
-                T prev[VN], cur[VN], nxt[VN];
-                bool ok = true;
-                // plane z0 - 1: only this thread's own values are needed
-                {
-                    const int s = k % STAGES;
-                    if (!mbar_wait_bounded(&full[s], (k / STAGES) & 1, budget)) ok = false;
-                    if (ok) {
-                        const V v = *reinterpret_cast<const V *>(
-                            reinterpret_cast<const T *>(tsm + s * G::STRIDE) + own);
-                        memcpy(prev, &v, sizeof(v));
-                    }
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty[s]);
-                    ++k;
-                }
-                int scur = k % STAGES;
-                if (ok && !mbar_wait_bounded(&full[scur], (k / STAGES) & 1, budget)) ok = false;
-                if (ok) {
-                    const V v = *reinterpret_cast<const V *>(
-                        reinterpret_cast<const T *>(tsm + scur * G::STRIDE) + own);
-                    memcpy(cur, &v, sizeof(v));
-                }
-                ++k;
-                for (int z = z0; z < z1 && ok; ++z) {
-                    const int snx = k % STAGES;
-                    if (!mbar_wait_bounded(&full[snx], (k / STAGES) & 1, budget)) {
-                        ok = false;
-                        break;
-                    }
-                    ++k;
-                    const T *pc = reinterpret_cast<const T *>(tsm + scur * G::STRIDE);
-                    const T *pn = reinterpret_cast<const T *>(tsm + snx * G::STRIDE);
-                    {
-                        const V v = *reinterpret_cast<const V *>(pn + own);
-                        memcpy(nxt, &v, sizeof(v));
-                    }
-                    T nn[VN], ss[VN];
-                    {
-                        const V vn = *reinterpret_cast<const V *>(pc + own + BXW);
-                        const V vs = *reinterpret_cast<const V *>(pc + own - BXW);
-                        memcpy(nn, &vn, sizeof(vn));
-                        memcpy(ss, &vs, sizeof(vs));
-                    }
-                    T wl = __shfl_up_sync(FULL, cur[VN - 1], 1);
-                    T er = __shfl_down_sync(FULL, cur[0], 1);
-                    if (lane == 0) wl = pc[own - 1];
-                    if (lane == 31) er = pc[own + VN];
-                    T res[VN];
-#pragma unroll
-                    for (int i = 0; i < VN; ++i) {
-                        const T e = (i == VN - 1) ? er : cur[i + 1];
-                        const T w = (i == 0) ? wl : cur[i - 1];
-                        const T s = add_rn(add_rn(add_rn(add_rn(add_rn(e, w), nn[i]), ss[i]), nxt[i]),
-                                           prev[i]);
-                        res[i] = mul_rn(c6, s);
-                    }
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&empty[scur]);
-                    if (row_ok) {
-                        const size_t idx = ((size_t)z * ny + y) * nx + xb;
-                        const bool full_vec = xb >= 1 && xb + VN - 1 <= nx - 2;
-                        const bool zlo = (z == 1), zhi = (z == nz - 2);
-                        const bool ylo = PY && (y == 1), yhi = PY && (y == ny - 2);
-                        auto put = [&](size_t base) {
-                            if (full_vec) {
-                                V v;
-                                memcpy(&v, res, sizeof(v));
-                                *reinterpret_cast<V *>(out + base) = v;
-                            } else {
-#pragma unroll
-                                for (int i = 0; i < VN; ++i) {
-                                    const int x = xb + i;
-                                    if (x >= 1 && x <= nx - 2) out[base + i] = res[i];
-                                }
-                            }
-                        };
-                        put(idx);
-                        if (zlo) put(idx + zimg);
-                        if (zhi) put(idx - zimg);
-                        if (ylo) {
-                            put(idx + yimg);
-                            if (zlo) put(idx + yimg + zimg);
-                            if (zhi) put(idx + yimg - zimg);
-                        }
-                        if (yhi) {
-                            put(idx - yimg);
-                            if (zlo) put(idx - yimg + zimg);
-                            if (zhi) put(idx - yimg - zimg);
-                        }
-                    }
-#pragma unroll
-                    for (int i = 0; i < VN; ++i) {
-                        prev[i] = cur[i];
-                        cur[i] = nxt[i];
-                    }
-                    scur = snx;
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[scur]);
-                if (!ok) {
-                    if (lane == 0) {
-                        if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = 2000000 + it;
-                        s_err = 1;
-                    }
-                    break;
-                }
-            }
-        }
-        if (it + 1 < niter) {
-            if (!grid_barrier(bar, gridDim.x, it)) break;
-        }
-    }
-    // On an error exit, let the loads this block issued land before its
-    // shared memory goes away (bounded).
-    if (warp == TY && lane == 0 && s_err) {
-        const unsigned lo = k > (unsigned)STAGES ? k - STAGES : 0u;
-        for (unsigned j = lo; j < k; ++j)
-            mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, budget);
     }
 }
 
@@ -643,12 +415,16 @@ int pick_zchunk(long long ntiles, int nzi, int *blocks) {
 }
 
 constexpr int J3_TY = 8;
-constexpr int TMA_TY = 8;
+// TMA pipeline shape: 4 consumer warps x 2 rows = 8-row tiles, 8 stages.
+constexpr int TMA_CW = 4;
+constexpr int TMA_RPW = 2;
+constexpr int TMA_TY = TMA_CW * TMA_RPW;
 constexpr int TMA_STAGES = 8;
+constexpr int TMA_THREADS = 32 * (TMA_CW + 1);
 
 template <typename T, bool PY>
 const void *tma_fn() {
-    return (const void *)j3d_tma_kernel<T, TMA_TY, TMA_STAGES, PY>;
+    return (const void *)j3d_tma_kernel<T, TMA_CW, TMA_RPW, TMA_STAGES, PY>;
 }
 
 const void *tma_fn_any(const cfm_jacobi_params &p) {
@@ -657,13 +433,13 @@ const void *tma_fn_any(const cfm_jacobi_params &p) {
 }
 
 size_t tma_smem(const cfm_jacobi_params &p) {
-    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_TY, TMA_STAGES>::SMEM
-                                   : TmaGeom<float, TMA_TY, TMA_STAGES>::SMEM;
+    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_CW, TMA_RPW, TMA_STAGES>::SMEM
+                                   : TmaGeom<float, TMA_CW, TMA_RPW, TMA_STAGES>::SMEM;
 }
 
 int tma_tile_x(const cfm_jacobi_params &p) {
-    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_TY, TMA_STAGES>::TX
-                                   : TmaGeom<float, TMA_TY, TMA_STAGES>::TX;
+    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_CW, TMA_RPW, TMA_STAGES>::TX
+                                   : TmaGeom<float, TMA_CW, TMA_RPW, TMA_STAGES>::TX;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -707,7 +483,7 @@ int setup_tma(cfm_jacobi *h) {
     const size_t smem = tma_smem(p);
     CFM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * (TMA_TY + 1), smem));
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TMA_THREADS, smem));
     if (per_sm < 1) return CFM_OK;
     h->tma_blocks = per_sm * h->num_sms;
     const long long ntiles =
@@ -939,7 +715,7 @@ int persistent_tma(cfm_jacobi *h, int niter, int *launches) {
     int n = niter;
     void *args[] = {(void *)m0, (void *)m1, &g0, &g1, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz,
                     &n, &h->tma_zchunk, &h->bar};
-    CFM_CUDA_TRY(launch_cooperative(tma_fn_any(p), dim3(h->tma_blocks), dim3(32 * (TMA_TY + 1)),
+    CFM_CUDA_TRY(launch_cooperative(tma_fn_any(p), dim3(h->tma_blocks), dim3(TMA_THREADS),
                                     args, tma_smem(p), h->stream));
     h->cur ^= (niter & 1);
     ++*launches;
@@ -1231,7 +1007,7 @@ int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads) {
         t = 1024;
     } else if (h->tma) {
         b = h->tma_blocks;
-        t = 32 * (TMA_TY + 1);
+        t = TMA_THREADS;
     }
     if (blocks) *blocks = b;
     if (threads) *threads = t;
