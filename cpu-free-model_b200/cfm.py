@@ -39,6 +39,8 @@ _SIGS = {
     "cfm_jacobi_run_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_jacobi_device_grid": (_vp, [_vp]),
     "cfm_jacobi_launch_shape": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_jacobi_autotune": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
+    "cfm_jacobi_variant_info": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
     "cfm_csr_create": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp]),
     "cfm_csr_destroy": (None, [_vp]),
     "cfm_csr_spmv_host": (_c.c_int, [_vp, _vp, _vp]),
@@ -193,6 +195,17 @@ class Jacobi:
         b, t = ctypes.c_int(), ctypes.c_int()
         check("cfm_jacobi_launch_shape", lib.cfm_jacobi_launch_shape(self.h, ctypes.byref(b), ctypes.byref(t)))
         return b.value, t.value
+
+    def autotune(self, sweeps=20):
+        v, r = ctypes.c_int(), ctypes.c_double()
+        check("cfm_jacobi_autotune", lib.cfm_jacobi_autotune(self.h, sweeps, ctypes.byref(v), ctypes.byref(r)))
+        return v.value, r.value
+
+
+def variant_info(i):
+    cw, rpw, st = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    s = lib.cfm_jacobi_variant_info(i, ctypes.byref(cw), ctypes.byref(rpw), ctypes.byref(st))
+    return None if s != OK else (cw.value, rpw.value, st.value)
 
 
 class CSR:

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -381,7 +382,10 @@ struct cfm_jacobi {
     // 3D TMA pipeline: tensor maps of the two grids, shape
     bool tma = false;
     CUtensorMap tmap[2];
-    int tma_blocks = 0, tma_zchunk = 0;
+    int tma_blocks = 0, tma_zchunk = 0, tma_var = 0;
+    const void *tma_fn = nullptr;
+    size_t tma_smem = 0;
+    size_t smem_optin = 0;
 };
 
 namespace {
@@ -415,32 +419,48 @@ int pick_zchunk(long long ntiles, int nzi, int *blocks) {
 }
 
 constexpr int J3_TY = 8;
-// TMA pipeline shape: 4 consumer warps x 2 rows = 8-row tiles, 8 stages.
-constexpr int TMA_CW = 4;
-constexpr int TMA_RPW = 2;
-constexpr int TMA_TY = TMA_CW * TMA_RPW;
-constexpr int TMA_STAGES = 8;
-constexpr int TMA_THREADS = 32 * (TMA_CW + 1);
 
-template <typename T, bool PY>
-const void *tma_fn() {
-    return (const void *)j3d_tma_kernel<T, TMA_CW, TMA_RPW, TMA_STAGES, PY>;
+// Shapes of the TMA pipeline compiled into the library: consumer warps, rows
+// per consumer warp, ring stages.  Entry 0 is the default; the autotuner
+// (cfm_jacobi_autotune) times them all; the environment variable
+// CFM_J3D_TMA_VARIANT (an index into this table) overrides the choice.
+struct TmaVariant {
+    int cw, rpw, stages;
+    const void *fn[2][2];  // [precision][periodic_y]
+    size_t smem[2];        // [precision]
+    int tx[2];             // [precision]
+};
+
+template <int CW, int RPW, int S>
+TmaVariant make_tma_variant() {
+    TmaVariant v{CW, RPW, S, {}, {}, {}};
+    v.fn[CFM_FP64][0] = (const void *)j3d_tma_kernel<double, CW, RPW, S, false>;
+    v.fn[CFM_FP64][1] = (const void *)j3d_tma_kernel<double, CW, RPW, S, true>;
+    v.fn[CFM_FP32][0] = (const void *)j3d_tma_kernel<float, CW, RPW, S, false>;
+    v.fn[CFM_FP32][1] = (const void *)j3d_tma_kernel<float, CW, RPW, S, true>;
+    v.smem[CFM_FP64] = TmaGeom<double, CW, RPW, S>::SMEM;
+    v.smem[CFM_FP32] = TmaGeom<float, CW, RPW, S>::SMEM;
+    v.tx[CFM_FP64] = TmaGeom<double, CW, RPW, S>::TX;
+    v.tx[CFM_FP32] = TmaGeom<float, CW, RPW, S>::TX;
+    return v;
 }
 
-const void *tma_fn_any(const cfm_jacobi_params &p) {
-    if (p.precision == CFM_FP64) return p.periodic_y ? tma_fn<double, true>() : tma_fn<double, false>();
-    return p.periodic_y ? tma_fn<float, true>() : tma_fn<float, false>();
+const TmaVariant *tma_variants(int *count) {
+    static const TmaVariant v[] = {
+        make_tma_variant<4, 2, 8>(), make_tma_variant<8, 2, 6>(), make_tma_variant<4, 4, 6>(),
+        make_tma_variant<8, 1, 8>(), make_tma_variant<4, 2, 12>(), make_tma_variant<2, 4, 8>(),
+    };
+    *count = (int)(sizeof(v) / sizeof(v[0]));
+    return v;
 }
 
-size_t tma_smem(const cfm_jacobi_params &p) {
-    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_CW, TMA_RPW, TMA_STAGES>::SMEM
-                                   : TmaGeom<float, TMA_CW, TMA_RPW, TMA_STAGES>::SMEM;
+const TmaVariant &tma_variant(int i) {
+    int n = 0;
+    const TmaVariant *v = tma_variants(&n);
+    return v[(i >= 0 && i < n) ? i : 0];
 }
 
-int tma_tile_x(const cfm_jacobi_params &p) {
-    return p.precision == CFM_FP64 ? TmaGeom<double, TMA_CW, TMA_RPW, TMA_STAGES>::TX
-                                   : TmaGeom<float, TMA_CW, TMA_RPW, TMA_STAGES>::TX;
-}
+int tma_threads(int var) { return 32 * (tma_variant(var).cw + 1); }
 
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -459,16 +479,18 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // Tensor maps over both grids: dims (nx, ny, nz), box (TX + 2 VN, TY + 2, 1),
 // zero fill outside.  Needs the row pitch nx * esize to be a multiple of 16.
-int setup_tma(cfm_jacobi *h) {
+int setup_tma(cfm_jacobi *h, int var) {
     const cfm_jacobi_params &p = h->p;
     h->tma = false;
     if (p.dims != 3 || ((size_t)p.nx * h->esize) % 16 != 0) return CFM_OK;
     auto enc = tensor_map_encoder();
     if (!enc) return CFM_OK;
+    const TmaVariant &V = tma_variant(var);
+    const int ty = V.cw * V.rpw, tx = V.tx[p.precision];
     const int vn = (int)(16 / h->esize);
     const cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
     const cuuint64_t strides[2] = {(cuuint64_t)p.nx * h->esize, (cuuint64_t)p.nx * p.ny * h->esize};
-    const cuuint32_t box[3] = {(cuuint32_t)(tma_tile_x(p) + 2 * vn), (cuuint32_t)(TMA_TY + 2), 1u};
+    const cuuint32_t box[3] = {(cuuint32_t)(tx + 2 * vn), (cuuint32_t)(ty + 2), 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
     for (int i = 0; i < 2; ++i) {
         CUresult r = enc(&h->tmap[i],
@@ -479,18 +501,35 @@ int setup_tma(cfm_jacobi *h) {
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return CFM_OK;  // stay on the register kernel
     }
-    const void *fn = tma_fn_any(p);
-    const size_t smem = tma_smem(p);
+    const void *fn = V.fn[p.precision][p.periodic_y ? 1 : 0];
+    const size_t smem = V.smem[p.precision];
+    if (smem > h->smem_optin) return CFM_OK;
     CFM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, TMA_THREADS, smem));
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tma_threads(var), smem));
     if (per_sm < 1) return CFM_OK;
     h->tma_blocks = per_sm * h->num_sms;
-    const long long ntiles =
-        (long long)((p.nx + tma_tile_x(p) - 1) / tma_tile_x(p)) * ((p.ny - 2 + TMA_TY - 1) / TMA_TY);
+    const long long ntiles = (long long)((p.nx + tx - 1) / tx) * ((p.ny - 2 + ty - 1) / ty);
     h->tma_zchunk = pick_zchunk(ntiles, p.nz - 2, &h->tma_blocks);
+    if (const char *zc = std::getenv("CFM_J3D_ZCHUNK")) {
+        const int z = std::atoi(zc);
+        if (z >= 1) h->tma_zchunk = std::min(z, p.nz - 2);
+    }
+    h->tma_var = var;
+    h->tma_fn = fn;
+    h->tma_smem = smem;
     h->tma = true;
     return CFM_OK;
+}
+
+int default_tma_variant() {
+    int n = 0;
+    tma_variants(&n);
+    if (const char *e = std::getenv("CFM_J3D_TMA_VARIANT")) {
+        const int v = std::atoi(e);
+        if (v >= 0 && v < n) return v;
+    }
+    return 0;
 }
 
 int check_params(const cfm_jacobi_params *p) {
@@ -571,6 +610,7 @@ int choose_launch(cfm_jacobi *h) {
     int st = current_device_info(&di);
     if (st) return st;
     h->num_sms = di.num_sms;
+    h->smem_optin = di.smem_optin;
     const cfm_jacobi_params &p = h->p;
     const void *fn = sweep_fn_any(p, true);
     dim3 b = block_of(p);
@@ -715,8 +755,8 @@ int persistent_tma(cfm_jacobi *h, int niter, int *launches) {
     int n = niter;
     void *args[] = {(void *)m0, (void *)m1, &g0, &g1, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz,
                     &n, &h->tma_zchunk, &h->bar};
-    CFM_CUDA_TRY(launch_cooperative(tma_fn_any(p), dim3(h->tma_blocks), dim3(TMA_THREADS),
-                                    args, tma_smem(p), h->stream));
+    CFM_CUDA_TRY(launch_cooperative(h->tma_fn, dim3(h->tma_blocks), dim3(tma_threads(h->tma_var)),
+                                    args, h->tma_smem, h->stream));
     h->cur ^= (niter & 1);
     ++*launches;
     return CFM_OK;
@@ -853,7 +893,7 @@ int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out) {
     h->own_stream = true;
     if ((st = choose_launch(h))) return fail(st);
     if (h->p.impl == CFM_JACOBI_PERSISTENT || h->p.impl == CFM_JACOBI_RESIDENT)
-        if ((st = setup_tma(h))) return fail(st);
+        if ((st = setup_tma(h, default_tma_variant()))) return fail(st);
     if (h->resident) {
         const size_t xbytes = 2 * (size_t)h->res_blocks * 2 * h->p.nx * h->esize;
         if ((e = cudaMalloc(&h->xbuf, xbytes)) != cudaSuccess ||
@@ -999,6 +1039,63 @@ int cfm_jacobi_run_host(cfm_jacobi *h, int niter, const void *host_in, void *hos
 
 void *cfm_jacobi_device_grid(cfm_jacobi *h) { return h ? h->buf[h->cur] : nullptr; }
 
+int cfm_jacobi_variant_info(int index, int *consumer_warps, int *rows_per_warp, int *stages) {
+    int n = 0;
+    const TmaVariant *v = tma_variants(&n);
+    if (index < 0 || index >= n) return CFM_BAD_ARG;
+    if (consumer_warps) *consumer_warps = v[index].cw;
+    if (rows_per_warp) *rows_per_warp = v[index].rpw;
+    if (stages) *stages = v[index].stages;
+    return CFM_OK;
+}
+
+int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *best_glups) {
+    CFM_ARG_CHECK(h, "handle is null");
+    CFM_ARG_CHECK(sweeps >= 1, "sweeps must be >= 1");
+    if (best_variant) *best_variant = -1;
+    if (best_glups) *best_glups = 0.0;
+    if (!h->tma) return CFM_OK;  // only the TMA pipeline has shapes to choose from
+    const size_t bytes = h->elems * h->esize;
+    void *saved = nullptr;
+    CFM_CUDA_TRY(cudaMalloc(&saved, bytes));
+    auto restore = [&]() -> int {
+        for (int i = 0; i < 2; ++i)
+            CFM_CUDA_TRY(cudaMemcpyAsync(h->buf[i], saved, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->cur = 0;
+        return CFM_OK;
+    };
+    int st = CFM_OK;
+    cudaError_t e = cudaMemcpyAsync(saved, h->buf[h->cur], bytes, cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    int n = 0, best = -1;
+    double best_rate = 0.0;
+    tma_variants(&n);
+    for (int v = 0; v < n && e == cudaSuccess && st == CFM_OK; ++v) {
+        if ((st = setup_tma(h, v)) || !h->tma) {
+            st = CFM_OK;
+            continue;
+        }
+        if ((st = restore())) break;
+        cfm_stats s{};
+        if ((st = cfm_jacobi_run(h, sweeps, &s))) break;
+        if (s.glups > best_rate) {
+            best_rate = s.glups;
+            best = v;
+        }
+    }
+    const int st2 = (best >= 0) ? setup_tma(h, best) : setup_tma(h, default_tma_variant());
+    const int st3 = restore();
+    cudaFree(saved);
+    CFM_CUDA_TRY(e);
+    if (st) return st;
+    if (st2) return st2;
+    if (st3) return st3;
+    if (best_variant) *best_variant = best;
+    if (best_glups) *best_glups = best_rate;
+    return CFM_OK;
+}
+
 int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads) {
     CFM_ARG_CHECK(h, "handle is null");
     int b = h->blocks, t = h->threads;
@@ -1007,7 +1104,7 @@ int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads) {
         t = 1024;
     } else if (h->tma) {
         b = h->tma_blocks;
-        t = TMA_THREADS;
+        t = tma_threads(h->tma_var);
     }
     if (blocks) *blocks = b;
     if (threads) *threads = t;

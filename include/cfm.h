@@ -142,6 +142,15 @@ int cfm_jacobi_run_host(cfm_jacobi *h, int niter, const void *host_in, void *hos
 void *cfm_jacobi_device_grid(cfm_jacobi *h);
 /* Blocks and threads the persistent kernels launch with on this device. */
 int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads);
+/* Autotuner for the 3D TMA pipeline: times every compiled pipeline shape for
+ * `sweeps` sweeps on a saved copy of the current grid, keeps the fastest for
+ * this handle and restores the grid.  best_variant is -1 when the handle does
+ * not use the TMA pipeline (2D, host loops, nx * esize not a multiple of 16).
+ * Tuning knob (no reference counterpart; the reference hard-codes its launch
+ * geometry, Stencil/jacobi3D/src/multi-stream/multi-gpu-peer-tiling.cu:214-220). */
+int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *best_glups);
+/* Shape of compiled pipeline variant `index` (CFM_BAD_ARG past the last). */
+int cfm_jacobi_variant_info(int index, int *consumer_warps, int *rows_per_warp, int *stages);
 
 /* ------------------------------------------------------------------- CG */
 typedef enum cfm_cg_impl {
