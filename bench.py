@@ -185,6 +185,8 @@ def main():
     stream = torch.cuda.Stream()
     j.set_stream(stream.cuda_stream)
     j.load_problem(cfm.PROBLEM_CONFIG)
+    best, _ = j.autotune(20)  # pipeline shape and z-chunk; restores the grid
+    tuned = cfm.variant_info(best) if best >= 0 else None
     blocks, threads = j.launch_shape()
     for _ in range(args.warmup):
         j.run(NITER)
@@ -242,6 +244,8 @@ def main():
                    "niter_per_step": NITER, "problem": "config (x faces sin*sin, periodic y,z)",
                    "impl": "persistent cooperative kernel, grid barrier per sweep",
                    "launch": f"{blocks}x{threads}", "parallelism": f"replicas x{world}",
+                   "tuned": None if tuned is None else
+                   {"variant": best, "consumer_warps": tuned[0], "rows_per_warp": tuned[1], "stages": tuned[2]},
                    "l2": "inputs larger than L2 (two 1.07 GB grids)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,

@@ -391,29 +391,27 @@ struct cfm_jacobi {
 namespace {
 
 // Units are dealt round-robin to G blocks, so a sweep takes ceil(U / G)
-// rounds and the last one may leave blocks idle.  Pick the longest z-chunk
-// (fewest pipeline restarts) whose rounds keep >= 97% of the blocks busy;
-// if none does, the chunk with the best efficiency.  Returns the chunk and
-// lowers *blocks when there are fewer units than blocks.
+// rounds, each as long as one unit: zc planes plus the two planes every unit
+// reloads at its start.  Pick the z-chunk that minimises rounds * (zc + 2)
+// (ties: the longer chunk).  Returns the chunk and lowers *blocks when there
+// are fewer units than blocks.
+long long units_of(long long ntiles, int nzi, int zc) { return ntiles * ((nzi + zc - 1) / zc); }
+
 int pick_zchunk(long long ntiles, int nzi, int *blocks) {
-    int best = 8;
-    double best_eff = -1.0;
-    for (int zc = 128; zc >= 8; zc /= 2) {
-        const int c = std::min(zc, nzi);
-        const long long U = ntiles * ((nzi + c - 1) / c);
+    int best = std::min(8, nzi);
+    double best_cost = 1e300;
+    const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    for (int zc0 : cand) {
+        const int zc = std::min(zc0, nzi);
+        const long long U = units_of(ntiles, nzi, zc);
         const long long G = std::min<long long>(*blocks, U);
-        const double eff = (double)U / ((double)((U + G - 1) / G) * (double)G);
-        if (eff >= 0.97 && U >= *blocks) {
-            best = c;
-            best_eff = 2.0;
-            break;
-        }
-        if (eff > best_eff + 1e-9) {
-            best = c;
-            best_eff = eff;
+        const double cost = (double)((U + G - 1) / G) * (zc + 2) * ((double)*blocks / G);
+        if (cost <= best_cost) {
+            best_cost = cost;
+            best = zc;
         }
     }
-    const long long U = ntiles * ((nzi + best - 1) / best);
+    const long long U = units_of(ntiles, nzi, best);
     if (U < *blocks) *blocks = (int)std::max(1LL, U);
     return best;
 }
@@ -447,7 +445,7 @@ TmaVariant make_tma_variant() {
 
 const TmaVariant *tma_variants(int *count) {
     static const TmaVariant v[] = {
-        make_tma_variant<4, 2, 8>(), make_tma_variant<8, 2, 6>(), make_tma_variant<4, 4, 6>(),
+        make_tma_variant<8, 2, 6>(), make_tma_variant<4, 2, 8>(), make_tma_variant<4, 4, 6>(),
         make_tma_variant<8, 1, 8>(), make_tma_variant<4, 2, 12>(), make_tma_variant<2, 4, 8>(),
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
@@ -479,7 +477,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // Tensor maps over both grids: dims (nx, ny, nz), box (TX + 2 VN, TY + 2, 1),
 // zero fill outside.  Needs the row pitch nx * esize to be a multiple of 16.
-int setup_tma(cfm_jacobi *h, int var) {
+int setup_tma(cfm_jacobi *h, int var, int zchunk = 0) {
     const cfm_jacobi_params &p = h->p;
     h->tma = false;
     if (p.dims != 3 || ((size_t)p.nx * h->esize) % 16 != 0) return CFM_OK;
@@ -510,10 +508,14 @@ int setup_tma(cfm_jacobi *h, int var) {
     if (per_sm < 1) return CFM_OK;
     h->tma_blocks = per_sm * h->num_sms;
     const long long ntiles = (long long)((p.nx + tx - 1) / tx) * ((p.ny - 2 + ty - 1) / ty);
-    h->tma_zchunk = pick_zchunk(ntiles, p.nz - 2, &h->tma_blocks);
-    if (const char *zc = std::getenv("CFM_J3D_ZCHUNK")) {
-        const int z = std::atoi(zc);
-        if (z >= 1) h->tma_zchunk = std::min(z, p.nz - 2);
+    if (zchunk <= 0)
+        if (const char *zc = std::getenv("CFM_J3D_ZCHUNK")) zchunk = std::atoi(zc);
+    if (zchunk >= 1) {
+        h->tma_zchunk = std::min(zchunk, p.nz - 2);
+        const long long U = units_of(ntiles, p.nz - 2, h->tma_zchunk);
+        if (U < h->tma_blocks) h->tma_blocks = (int)std::max(1LL, U);
+    } else {
+        h->tma_zchunk = pick_zchunk(ntiles, p.nz - 2, &h->tma_blocks);
     }
     h->tma_var = var;
     h->tma_fn = fn;
@@ -1068,23 +1070,28 @@ int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *be
     int st = CFM_OK;
     cudaError_t e = cudaMemcpyAsync(saved, h->buf[h->cur], bytes, cudaMemcpyDeviceToDevice, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    int n = 0, best = -1;
+    int n = 0, best = -1, best_zc = 0;
     double best_rate = 0.0;
     tma_variants(&n);
+    const int zcands[] = {0, 16, 32, 64, 128};  // 0: the cost-model choice
     for (int v = 0; v < n && e == cudaSuccess && st == CFM_OK; ++v) {
-        if ((st = setup_tma(h, v)) || !h->tma) {
-            st = CFM_OK;
-            continue;
-        }
-        if ((st = restore())) break;
-        cfm_stats s{};
-        if ((st = cfm_jacobi_run(h, sweeps, &s))) break;
-        if (s.glups > best_rate) {
-            best_rate = s.glups;
-            best = v;
+        for (int zc : zcands) {
+            if ((st = setup_tma(h, v, zc)) || !h->tma) {
+                st = CFM_OK;
+                break;
+            }
+            if ((st = restore())) break;
+            cfm_stats s{};
+            if ((st = cfm_jacobi_run(h, sweeps, &s))) break;
+            if (s.glups > best_rate) {
+                best_rate = s.glups;
+                best = v;
+                best_zc = h->tma_zchunk;
+            }
         }
     }
-    const int st2 = (best >= 0) ? setup_tma(h, best) : setup_tma(h, default_tma_variant());
+    const int st2 =
+        (best >= 0) ? setup_tma(h, best, best_zc) : setup_tma(h, default_tma_variant());
     const int st3 = restore();
     cudaFree(saved);
     CFM_CUDA_TRY(e);

@@ -86,7 +86,7 @@ def test_jacobi3d_512_fp64_bitexact_and_e2e():
     end-to-end host-buffer call gives the same grid."""
     nx = ny = nz = 512
     with cfm.Jacobi(3, nx, ny, nz, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
-        assert j.launch_shape()[1] == 160  # the TMA-fed pipeline kernel (4 consumer warps + producer)
+        assert j.launch_shape()[1] in (96, 160, 288)  # a TMA pipeline kernel (consumer warps + producer)
         a = j.problem_host(cfm.PROBLEM_CONFIG)
         want = oracle.jacobi3d(a, 3, 1)
         j.upload(a)
@@ -97,6 +97,28 @@ def test_jacobi3d_512_fp64_bitexact_and_e2e():
         st2 = j.run_host(3, a, out)
         np.testing.assert_array_equal(out, want)
         assert st2.h2d_bytes == a.nbytes and st2.d2h_bytes == a.nbytes
+
+
+def test_autotune_restores_grid_and_stays_bitexact():
+    a = rand_grid((40, 36, 128), np.float64, 15)
+    with cfm.Jacobi(3, 128, 36, 40, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
+        j.upload(a)
+        best, rate = j.autotune(3)
+        assert best >= 0 and rate > 0 and cfm.variant_info(best) is not None
+        np.testing.assert_array_equal(j.download(), a)
+        j.run(6)
+        np.testing.assert_array_equal(j.download(), oracle.jacobi3d(a, 6, 1))
+    with cfm.Jacobi(2, 64, 64, 1, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
+        assert j.autotune(2)[0] == -1  # nothing to tune outside the 3D TMA pipeline
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_every_pipeline_variant_bitexact(variant, monkeypatch):
+    monkeypatch.setenv("CFM_J3D_TMA_VARIANT", str(variant))
+    for prec, py, shape in ((cfm.FP64, 1, (21, 19, 128)), (cfm.FP32, 0, (13, 40, 136))):
+        a = rand_grid(shape, cfm.np_dtype(prec), 16)
+        got, _ = run_gpu(a, 5, cfm.JACOBI_PERSISTENT, py)
+        np.testing.assert_array_equal(got, oracle.jacobi3d(a, 5, py))
 
 
 def test_jacobi_run_twice_equals_one_long_run():
