@@ -203,11 +203,13 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                             V v;
                             memcpy(&v, res, sizeof(v));
                             if (full_vec) {
-                                *reinterpret_cast<V *>(out + idx) = v;
+                                // evict-first: the output must not push the input
+                                // planes other tiles still need out of L2
+                                __stcs(reinterpret_cast<V *>(out + idx), v);
                             } else {
 #pragma unroll
                                 for (int i = 0; i < VN; ++i)
-                                    if (xb + i >= 1 && xb + i <= nx - 2) out[idx + i] = res[i];
+                                    if (xb + i >= 1 && xb + i <= nx - 2) __stcs(out + idx + i, res[i]);
                             }
                             const int y = y0 + r0 + j;
                             const bool yspecial = PY && (y == 1 || y == ny - 2);

@@ -112,7 +112,7 @@ def test_autotune_restores_grid_and_stays_bitexact():
         assert j.autotune(2)[0] == -1  # nothing to tune outside the 3D TMA pipeline
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(8))
 def test_every_pipeline_variant_bitexact(variant, monkeypatch):
     monkeypatch.setenv("CFM_J3D_TMA_VARIANT", str(variant))
     for prec, py, shape in ((cfm.FP64, 1, (21, 19, 128)), (cfm.FP32, 0, (13, 40, 136))):
