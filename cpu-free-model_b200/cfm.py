@@ -49,6 +49,8 @@ _SIGS = {
     "cfm_cg_set_stream": (_c.c_int, [_vp, _vp]),
     "cfm_cg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_cg_solve_device": (_c.c_int, [_vp, _vp, _vp, _vp]),
+    "cfm_cg_solve_noalloc": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp, _vp, _c.c_int,
+                                        _c.c_double, _vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),

@@ -19,8 +19,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "barrier.cuh"
@@ -651,3 +653,162 @@ int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats
 }
 
 }  // extern "C"
+
+// ------------------------------------------- CG without device allocation
+// cfm_cg_solve_noalloc runs cg_persistent_kernel with its scratch carved out
+// of one fixed device array instead of cudaMalloc'd buffers, for callers
+// that cannot allocate device memory (an outside allocator owns the pool,
+// the memory is reserved up front, or an allocation would synchronise).
+// Layout, in doubles (256-byte aligned pieces):
+//   [0, 32)            header: BarrierState at byte 0, CgResult at byte 64,
+//                      4 reduced scalars at byte 128
+//   [32, 32 + 4T)      dot partials, T = CFM_CG_NOALLOC_MAX_N / 1024 tiles
+//   then 4 N           the vectors r, p, s, t (N = CFM_CG_NOALLOC_MAX_N)
+namespace cfm {
+
+constexpr size_t NA_MAX_N = CFM_CG_NOALLOC_MAX_N;
+constexpr size_t NA_MAX_TILES = NA_MAX_N / CG_TILE;
+constexpr size_t NA_HDR = 32;
+constexpr size_t NA_PART = NA_HDR;
+constexpr size_t NA_VEC = NA_PART + 4 * NA_MAX_TILES;
+constexpr size_t NA_TOTAL = NA_VEC + 4 * NA_MAX_N;
+static_assert(NA_MAX_N % CG_TILE == 0, "whole tiles");
+static_assert(sizeof(BarrierState) <= 64 && sizeof(CgResult) <= 64, "header layout");
+
+// Held by every GPU that loads the library, until the process exits.
+static __device__ __align__(256) double g_cg_noalloc_scratch[NA_TOTAL];
+
+// Zeroes the barrier (the only scratch read before it is written) and sets
+// its wait budget.
+__global__ void k_noalloc_reset(BarrierState *b, unsigned long long timeout_ns) {
+    b->count = 0;
+    b->gen = 0;
+    b->error = 0;
+    b->where = 0;
+    b->timeout_ns = timeout_ns;
+}
+
+namespace {
+
+// Device address of g_cg_noalloc_scratch on the current device.  In host
+// code the symbol names a host-side stand-in, so the address is looked up
+// once per device with that device current and cached.
+int noalloc_scratch(double **out) {
+    static std::mutex mu;
+    static double *addr[64] = {};
+    int dev = 0;
+    CFM_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("device index %d out of range", dev);
+        return CFM_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(g_cg_noalloc_scratch) failed: %s",
+                      cudaGetErrorString(e));
+            return CFM_CUDA_ERROR;
+        }
+        addr[dev] = static_cast<double *>(p);
+    }
+    *out = addr[dev];
+    return CFM_OK;
+}
+
+}  // namespace
+}  // namespace cfm
+
+extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
+                                    const int *col_dev, const double *val_dev,
+                                    const double *b_dev, double *x_dev, int maxiter, double tol,
+                                    void *cuda_stream, cfm_stats *st) {
+    clear_error();
+    CFM_ARG_CHECK(n > 0, "n must be positive");
+    if ((size_t)n > NA_MAX_N) {
+        set_error("bad argument: n = %d exceeds CFM_CG_NOALLOC_MAX_N = %d (the fixed scratch "
+                  "array of cfm_cg_solve_noalloc)", n, (int)NA_MAX_N);
+        return CFM_BAD_ARG;
+    }
+    CFM_ARG_CHECK(nnz >= 0 && nnz < 2147483647LL, "nnz");
+    CFM_ARG_CHECK(rowptr_dev && x_dev && (nnz == 0 || (col_dev && val_dev)), "null argument");
+    CFM_ARG_CHECK(maxiter >= 0, "maxiter");
+    double *scr = nullptr;
+    int e = noalloc_scratch(&scr);
+    if (e) return e;
+    DeviceInfo di;
+    if ((e = current_device_info(&di))) return e;
+    int per_sm = 0;
+    CFM_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent_kernel, CG_TILE, 0));
+    if (per_sm < 1) {
+        set_error("cg kernel cannot be resident");
+        return CFM_UNSUPPORTED;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    CgArgs a{};
+    a.n = n;
+    a.ntiles = (n + CG_TILE - 1) / CG_TILE;
+    a.rowptr = rowptr_dev;
+    a.col = col_dev;
+    a.val = val_dev;
+    a.b = b_dev;
+    a.x = x_dev;
+    a.r = scr + NA_VEC;
+    a.p = a.r + n;
+    a.s = a.p + n;
+    a.t = a.s + n;
+    a.part = scr + NA_PART;
+    a.bar = reinterpret_cast<BarrierState *>(scr);
+    a.res = reinterpret_cast<CgResult *>(reinterpret_cast<char *>(scr) + 64);
+    double *scal = scr + 16;
+    a.maxiter = maxiter;
+    a.tol = tol;
+    const int blocks = std::min(per_sm * di.num_sms, a.ntiles);
+    const auto t0 = std::chrono::steady_clock::now();
+    k_noalloc_reset<<<1, 1, 0, s>>>(a.bar, barrier_timeout_ns());
+    CFM_CUDA_TRY(cudaGetLastError());
+    void *args[] = {&a};
+    CFM_CUDA_TRY(launch_cooperative((const void *)cg_persistent_kernel, dim3(blocks),
+                                    dim3(CG_TILE), args, 0, s));
+    // final FP64 true residual b - A x into partial slot 2, reduced to scal[2]
+    k_true_residual<<<a.ntiles, CG_TILE, 0, s>>>(a);
+    CFM_CUDA_TRY(cudaGetLastError());
+    k_reduce<<<1, CG_TILE, 0, s>>>(a, 2, scal);
+    CFM_CUDA_TRY(cudaGetLastError());
+    double hdr[NA_HDR];
+    CFM_CUDA_TRY(cudaMemcpyAsync(hdr, scr, sizeof(hdr), cudaMemcpyDeviceToHost, s));
+    CFM_CUDA_TRY(cudaStreamSynchronize(s));
+    const double secs =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    BarrierState bs;
+    CgResult r;
+    std::memcpy(&bs, hdr, sizeof(bs));
+    std::memcpy(&r, reinterpret_cast<const char *>(hdr) + 64, sizeof(r));
+    if (bs.error) {
+        set_error("grid barrier %d timed out", bs.where);
+        if (st) {
+            std::memset(st, 0, sizeof(*st));
+            st->status = CFM_BARRIER_TIMEOUT;
+        }
+        return CFM_BARRIER_TIMEOUT;
+    }
+    const double tt = hdr[16 + 2];
+    const double relres = r.bnorm > 0 ? std::sqrt(tt) / r.bnorm : std::sqrt(tt);
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        st->seconds = secs;
+        st->iterations = r.iters;
+        st->residual = relres;
+        st->bytes = (double)r.iters * (12.0 * (double)nnz + 4.0 * (n + 1) + 88.0 * n);
+        st->gbs = secs > 0 ? st->bytes / secs * 1e-9 : 0;
+        st->launches = 4;
+        st->status = r.status;
+        st->refinements = r.restarts;
+    }
+    if (r.status == CFM_NOT_CONVERGED)
+        set_error("not converged after %lld iterations (true relres %.3e)", r.iters, relres);
+    if (r.status == CFM_BREAKDOWN) set_error("CG breakdown at iteration %lld", r.iters);
+    return r.status;
+}

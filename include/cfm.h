@@ -195,6 +195,34 @@ int cfm_cg_solve(cfm_cg *h, const double *b_host, double *x_host, cfm_stats *st)
 /* Same with device vectors (length n, FP64). */
 int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st);
 
+/* Largest system cfm_cg_solve_noalloc accepts (rows). */
+#define CFM_CG_NOALLOC_MAX_N 262144
+
+/* Persistent CG (the CFM_CG_PERSISTENT kernel and arithmetic, so the same x
+ * and iteration count) for callers that cannot allocate device memory: code
+ * that runs inside another framework's memory pool or allocator, in a
+ * process whose device memory is reserved up front, or at a point where an
+ * allocation would synchronise the device.  It calls no cudaMalloc,
+ * cudaFree, stream or event creation.  Its working vectors (r, p, s, t), dot
+ * partials, result word and grid-barrier state live in one fixed device
+ * array inside the library, about 8.0 MiB, that every GPU which loads the
+ * library holds until the process exits.
+ *  - Inputs and outputs are the caller's device memory: a 0-based CSR
+ *    matrix (rowptr n+1, col nnz, val nnz) with n <= CFM_CG_NOALLOC_MAX_N
+ *    (larger n: CFM_BAD_ARG), b (NULL = ones) and x (length n, written).
+ *  - Work goes on `cuda_stream` (NULL = the legacy default stream); the
+ *    call returns when the solve is done.  stats->seconds is host time.
+ *  - The first call on a device looks up the array's device address (with
+ *    that device current); make that first call before any stream capture.
+ *  - All calls share the one array and the call resets what must start at
+ *    zero, so calls whose kernels overlap on the GPU (other threads, other
+ *    streams) race; serialise them.
+ * No counterpart in the reference: its CG versions allocate their vectors
+ * themselves with cudaMalloc. */
+int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev, const int *col_dev,
+                         const double *val_dev, const double *b_dev, double *x_dev, int maxiter,
+                         double tol, void *cuda_stream, cfm_stats *st);
+
 /* ------------------------------------------------------------ generators */
 /* Number of nonzeros of the 7-point Dirichlet Poisson matrix on gx*gy*gz cells. */
 long long cfm_poisson3d_nnz(int gx, int gy, int gz);
