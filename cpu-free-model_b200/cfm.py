@@ -51,6 +51,15 @@ _SIGS = {
     "cfm_cg_solve_device": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_cg_solve_noalloc": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp, _vp, _c.c_int,
                                         _c.c_double, _vp, _vp]),
+    "cfm_stencil_create": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _vp, _vp]),
+    "cfm_stencil_destroy": (None, [_vp]),
+    "cfm_stencil_apply_host": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_cg_create_stencil": (_c.c_int, [_vp, _vp, _vp]),
+    "cfm_normal": (_c.c_int, [_c.c_ulonglong, _c.c_uint, _c.c_longlong, _vp]),
+    "cfm_grf": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_double,
+                           _c.c_double, _vp]),
+    "cfm_varcoef_problem": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_ulonglong, _vp, _vp]),
+    "cfm_varcoef_coeffs": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -235,12 +244,44 @@ class CSR:
         return y
 
 
+class Stencil:
+    """Matrix-free variable-coefficient operator (cfm_stencil) built from k."""
+
+    def __init__(self, k):
+        k = np.ascontiguousarray(k, np.float64)
+        self.dims = k.ndim
+        self.shape = k.shape
+        nz = k.shape[0] if k.ndim == 3 else 1
+        ny, nx = k.shape[-2], k.shape[-1]
+        self.grid = (nx, ny, nz)
+        self.n = k.size
+        h = ctypes.c_void_p()
+        check("cfm_stencil_create", lib.cfm_stencil_create(self.dims, nx, ny, nz, _ptr(k), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_stencil_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def apply(self, x):
+        x = np.ascontiguousarray(x, np.float64).reshape(-1)
+        y = np.empty(self.n)
+        check("cfm_stencil_apply_host", lib.cfm_stencil_apply_host(self.h, _ptr(x), _ptr(y)))
+        return y
+
+
 class CG:
     def __init__(self, A, impl=CG_PERSISTENT, maxiter=20000, tol=1e-8, inner_maxiter=0, inner_tol=0.0):
         self.A = A
         self.p = CGParams(impl, maxiter, tol, inner_maxiter, inner_tol)
         h = ctypes.c_void_p()
-        check("cfm_cg_create", lib.cfm_cg_create(A.h, ctypes.byref(self.p), ctypes.byref(h)))
+        if isinstance(A, Stencil):
+            check("cfm_cg_create_stencil", lib.cfm_cg_create_stencil(A.h, ctypes.byref(self.p), ctypes.byref(h)))
+        else:
+            check("cfm_cg_create", lib.cfm_cg_create(A.h, ctypes.byref(self.p), ctypes.byref(h)))
         self.h = h
 
     def close(self):
@@ -314,3 +355,41 @@ def barrier_selftest(blocks=0, rounds=4, drop_block=-1):
 
 def set_barrier_timeout_ms(ms):
     check("cfm_set_barrier_timeout_ms", lib.cfm_set_barrier_timeout_ms(ms))
+
+
+def normal(seed, n, stream=0):
+    out = np.empty(n)
+    check("cfm_normal", lib.cfm_normal(seed, stream, n, _ptr(out)))
+    return out
+
+
+def _grid_args(shape):
+    if len(shape) == 2:
+        return 2, shape[1], shape[0], 1
+    return 3, shape[2], shape[1], shape[0]
+
+
+def grf(shape, seed, sigma=1.0, corr_len=16.0):
+    dims, nx, ny, nz = _grid_args(shape)
+    out = np.empty(shape)
+    check("cfm_grf", lib.cfm_grf(dims, nx, ny, nz, seed, sigma, corr_len, _ptr(out)))
+    return out
+
+
+def varcoef_problem(shape, seed):
+    """(k, f) of the variable-coefficient diffusion problem on a grid of `shape` (y, x) or (z, y, x)."""
+    dims, nx, ny, nz = _grid_args(shape)
+    k = np.empty(shape)
+    f = np.empty(shape)
+    check("cfm_varcoef_problem", lib.cfm_varcoef_problem(dims, nx, ny, nz, seed, _ptr(k), _ptr(f)))
+    return k, f
+
+
+def varcoef_coeffs(k):
+    """(we, wn, wt, dg) face coefficients of the stencil operator for k."""
+    k = np.ascontiguousarray(k, np.float64)
+    dims, nx, ny, nz = _grid_args(k.shape)
+    we, wn, wt, dg = (np.zeros(k.size) for _ in range(4))
+    check("cfm_varcoef_coeffs", lib.cfm_varcoef_coeffs(dims, nx, ny, nz, _ptr(k), _ptr(we), _ptr(wn),
+                                                       _ptr(wt), _ptr(dg)))
+    return we, wn, wt, dg

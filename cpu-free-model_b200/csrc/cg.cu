@@ -1,5 +1,5 @@
-// Conjugate gradient on one GPU: the CPU-free persistent kernel, the
-// host-controlled comparator, and the cfm_csr / cfm_cg handles.
+// Conjugate gradient on one GPU: the cfm_csr / cfm_stencil operators, the
+// cfm_cg handle and its solvers (kernels in krylov.cuh).
 //
 // Algorithm (standard CG, CG/src/common.cu:399-538 and
 // CG/src/single-stream/standard.cu:158-299):
@@ -8,10 +8,8 @@
 //   x += alpha p; r -= alpha s; gamma1 = <r, r>; beta = gamma1 / gamma0
 //   p = r + beta p
 // The reference sums the dots with atomicAdd(double) in arrival order
-// (CG/src/common.cu:357-389); here every dot is a fixed tree -- tiles of 1024
-// consecutive entries, xor-butterfly within each warp, then across the 32
-// warp sums; the tile partials are summed the same way -- so the result does
-// not depend on the launch shape and the host oracle reproduces it exactly.
+// (CG/src/common.cu:357-389); here every dot is a fixed tree, so the result
+// does not depend on the launch shape and the host oracle reproduces it.
 // With tol > 0 the loop stops when the recursive residual reaches
 // tol * ||b|| and the FP64 true residual b - A x confirms it (a restart from
 // the true residual otherwise); tol <= 0 runs exactly maxiter iterations like
@@ -25,264 +23,16 @@
 #include <mutex>
 #include <vector>
 
-#include "barrier.cuh"
 #include "cfm_internal.h"
+#include "krylov.cuh"
 
 namespace cfm {
-
-constexpr int CG_TILE = 1024;  // rows per tile == threads per block
-constexpr unsigned CG_FULL = 0xffffffffu;
-
-struct CgResult {
-    long long iters;
-    int status;
-    int restarts;
-    double gamma;
-    double bnorm;
-};
-
-struct CgArgs {
-    int n;
-    int ntiles;
-    const int *rowptr;
-    const int *col;
-    const double *val;
-    const double *b;  // nullptr: ones
-    double *x, *r, *p, *s, *t;
-    double *part;  // 4 * ntiles partials: gamma | delta | true residual | b
-    CgResult *res;
-    BarrierState *bar;
-    int maxiter;
-    double tol;
-};
-
-__device__ __forceinline__ double warp_xor_sum(double v) {
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(CG_FULL, v, off));
-    return v;
+// FP32 copy of n doubles (device).
+__global__ void k_to_f32(const double *in, float *out, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __double2float_rn(in[i]);
 }
-
-// Tree sum over the 1024 threads of the block; every thread gets the result.
-__device__ __forceinline__ double block_sum(double v, double *sm /* 33 doubles */) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_xor_sum(v);
-    if (lane == 0) sm[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        double w = warp_xor_sum(sm[lane]);
-        if (lane == 0) sm[32] = w;
-    }
-    __syncthreads();
-    const double out = sm[32];
-    __syncthreads();
-    return out;
-}
-
-// Sum of tile partials in the fixed order: thread t adds part[t], part[t+1024], ...
-__device__ __forceinline__ double sum_partials(const double *part, int ntiles, double *sm) {
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < ntiles; i += CG_TILE) acc = __dadd_rn(acc, part[i]);
-    return block_sum(acc, sm);
-}
-
-__device__ __forceinline__ double row_spmv(const int *rowptr, const int *col, const double *val,
-                                           const double *x, int i) {
-    double acc = 0.0;
-    const int j1 = rowptr[i + 1];
-    for (int j = rowptr[i]; j < j1; ++j) acc = __fma_rn(val[j], x[col[j]], acc);
-    return acc;
-}
-
-__device__ __forceinline__ double row_spmv_zero(const int *rowptr, const double *val, int i) {
-    double acc = 0.0;
-    const int j1 = rowptr[i + 1];
-    for (int j = rowptr[i]; j < j1; ++j) acc = __fma_rn(val[j], 0.0, acc);
-    return acc;
-}
-
-// ---------------------------------------------------------------- phases
-// Each phase processes whole tiles (one row per thread) and writes one
-// partial per tile; tiles are dealt to blocks round-robin.
-
-__device__ void phase_init(const CgArgs &a, double *sm) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        double g = 0.0, bb = 0.0;
-        if (i < a.n) {
-            const double bi = a.b ? a.b[i] : 1.0;
-            const double s0 = row_spmv_zero(a.rowptr, a.val, i);  // A x0 with x0 = 0
-            const double ri = __fma_rn(-1.0, s0, bi);
-            a.x[i] = 0.0;
-            a.r[i] = ri;
-            a.p[i] = ri;
-            g = __dmul_rn(ri, ri);
-            bb = __dmul_rn(bi, bi);
-        }
-        g = block_sum(g, sm);
-        bb = block_sum(bb, sm);
-        if (threadIdx.x == 0) {
-            a.part[tile] = g;
-            a.part[3 * a.ntiles + tile] = bb;
-        }
-    }
-}
-
-__device__ void phase_spmv_dot(const CgArgs &a, double *sm) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        double d = 0.0;
-        if (i < a.n) {
-            const double si = row_spmv(a.rowptr, a.col, a.val, a.p, i);
-            a.s[i] = si;
-            d = __dmul_rn(a.p[i], si);
-        }
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) a.part[a.ntiles + tile] = d;
-    }
-}
-
-__device__ void phase_update(const CgArgs &a, double alpha, double *sm) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        double g = 0.0;
-        if (i < a.n) {
-            a.x[i] = __fma_rn(alpha, a.p[i], a.x[i]);
-            const double ri = __fma_rn(-alpha, a.s[i], a.r[i]);
-            a.r[i] = ri;
-            g = __dmul_rn(ri, ri);
-        }
-        g = block_sum(g, sm);
-        if (threadIdx.x == 0) a.part[tile] = g;
-    }
-}
-
-__device__ void phase_true_residual(const CgArgs &a, double *sm) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        double q = 0.0;
-        if (i < a.n) {
-            const double bi = a.b ? a.b[i] : 1.0;
-            const double ti = __dsub_rn(bi, row_spmv(a.rowptr, a.col, a.val, a.x, i));
-            a.t[i] = ti;
-            q = __dmul_rn(ti, ti);
-        }
-        q = block_sum(q, sm);
-        if (threadIdx.x == 0) a.part[2 * a.ntiles + tile] = q;
-    }
-}
-
-__device__ void phase_restart(const CgArgs &a) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        if (i < a.n) {
-            a.r[i] = a.t[i];
-            a.p[i] = a.t[i];
-        }
-    }
-}
-
-__device__ void phase_p(const CgArgs &a, double beta) {
-    for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        const int i = tile * CG_TILE + threadIdx.x;
-        if (i < a.n) a.p[i] = __fma_rn(beta, a.p[i], a.r[i]);
-    }
-}
-
-// The whole solve in one cooperative launch; 3 grid barriers per iteration.
-__global__ void __launch_bounds__(CG_TILE, 1) cg_persistent_kernel(CgArgs a) {
-    __shared__ double sm[33];
-    int site = 0;
-    phase_init(a, sm);
-    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-    double gamma0 = sum_partials(a.part, a.ntiles, sm);
-    const double bnorm = sqrt(sum_partials(a.part + 3 * a.ntiles, a.ntiles, sm));
-    const bool use_tol = a.tol > 0.0;
-    const double target = a.tol * bnorm;
-    int status = use_tol ? CFM_NOT_CONVERGED : CFM_OK;
-    int restarts = 0;
-    long long k = 0;
-    if (use_tol && sqrt(gamma0) <= target) status = CFM_OK;
-    while (k < a.maxiter && !(use_tol && status == CFM_OK)) {
-        phase_spmv_dot(a, sm);
-        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        const double delta = sum_partials(a.part + a.ntiles, a.ntiles, sm);
-        const double alpha = gamma0 / delta;
-        if (use_tol && !(delta > 0.0 && isfinite(alpha))) {
-            status = CFM_BREAKDOWN;
-            break;
-        }
-        phase_update(a, alpha, sm);
-        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        const double gamma1 = sum_partials(a.part, a.ntiles, sm);
-        ++k;
-        if (use_tol && sqrt(gamma1) <= target) {
-            phase_true_residual(a, sm);
-            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-            const double tt = sum_partials(a.part + 2 * a.ntiles, a.ntiles, sm);
-            if (sqrt(tt) <= target) {
-                status = CFM_OK;
-                gamma0 = gamma1;
-                break;
-            }
-            phase_restart(a);
-            ++restarts;
-            gamma0 = tt;
-            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-            continue;
-        }
-        const double beta = gamma1 / gamma0;
-        if (use_tol && !isfinite(beta)) {
-            status = CFM_BREAKDOWN;
-            break;
-        }
-        phase_p(a, beta);
-        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        gamma0 = gamma1;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.res->iters = k;
-        a.res->status = status;
-        a.res->restarts = restarts;
-        a.res->gamma = gamma0;
-        a.res->bnorm = bnorm;
-    }
-}
-
-// ------------------------------------------------ host-controlled comparator
-// One kernel per operation and a host read of every dot, as
-// SingleGPUDiscreteStandard::run_single_gpu does (CG/src/common.cu:458-531).
-__global__ void __launch_bounds__(CG_TILE) k_init(CgArgs a) {
-    __shared__ double sm[33];
-    phase_init(a, sm);
-}
-__global__ void __launch_bounds__(CG_TILE) k_spmv_dot(CgArgs a) {
-    __shared__ double sm[33];
-    phase_spmv_dot(a, sm);
-}
-__global__ void __launch_bounds__(CG_TILE) k_update(CgArgs a, double alpha) {
-    __shared__ double sm[33];
-    phase_update(a, alpha, sm);
-}
-__global__ void __launch_bounds__(CG_TILE) k_true_residual(CgArgs a) {
-    __shared__ double sm[33];
-    phase_true_residual(a, sm);
-}
-__global__ void __launch_bounds__(CG_TILE) k_restart(CgArgs a) { phase_restart(a); }
-__global__ void __launch_bounds__(CG_TILE) k_p(CgArgs a, double beta) { phase_p(a, beta); }
-// Single block: reduce partial slot `which` into out[which].
-__global__ void __launch_bounds__(CG_TILE) k_reduce(CgArgs a, int which, double *out) {
-    __shared__ double sm[33];
-    const double v = sum_partials(a.part + (size_t)which * a.ntiles, a.ntiles, sm);
-    if (threadIdx.x == 0) out[which] = v;
-}
-
-// y = A x, one row per thread (row order, fma accumulation).
-__global__ void k_spmv(int n, const int *rowptr, const int *col, const double *val,
-                       const double *x, double *y) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) y[i] = row_spmv(rowptr, col, val, x, i);
-}
-
 }  // namespace cfm
 
 using namespace cfm;
@@ -293,15 +43,26 @@ struct cfm_csr {
     int *rowptr = nullptr;
     int *col = nullptr;
     double *val = nullptr;
+    float *val32 = nullptr;
+};
+
+struct cfm_stencil {
+    int dims = 2, nx = 0, ny = 0, nz = 1, n = 0;
+    double *c64 = nullptr;  // we | wn | wt | dg  (4 n)
+    float *c32 = nullptr;   // FP32 copies        (4 n)
 };
 
 struct cfm_cg {
     cfm_cg_params p{};
+    int kind = 0;  // 0 CSR, 2 / 3 stencil of that dimension
     const cfm_csr *A = nullptr;
+    const cfm_stencil *S = nullptr;
+    int n = 0;
     int ntiles = 0;
-    double *vec = nullptr;  // x r p s t b (6 n)
+    double *vec = nullptr;  // x r p s t b z w0 w1 (9 n)
+    float *vec32 = nullptr; // r32 p32 s32 d32 (4 n)
     double *part = nullptr;
-    double *scal = nullptr;  // 4 reduced scalars (discrete variant)
+    double *scal = nullptr;  // NSLOTS reduced scalars (discrete variant, final residual)
     CgResult *res = nullptr;
     BarrierState *bar = nullptr;
     cudaStream_t stream = nullptr;
@@ -312,34 +73,63 @@ struct cfm_cg {
 
 namespace {
 
-CgArgs make_args(cfm_cg *h, const double *b_dev, double *x_dev) {
-    CgArgs a{};
-    const int n = h->A->n;
-    a.n = n;
+CsrOp csr_op(const cfm_csr *A) { return CsrOp{A->rowptr, A->col, A->val, A->val32}; }
+
+template <int D>
+StencilOp<D> stencil_op(const cfm_stencil *S) {
+    const size_t n = S->n;
+    StencilOp<D> o;
+    o.nx = S->nx;
+    o.ny = S->ny;
+    o.nz = S->nz;
+    o.we = S->c64;
+    o.wn = S->c64 + n;
+    o.wt = S->c64 + 2 * n;
+    o.dg = S->c64 + 3 * n;
+    o.we32 = S->c32;
+    o.wn32 = S->c32 + n;
+    o.wt32 = S->c32 + 2 * n;
+    o.dg32 = S->c32 + 3 * n;
+    return o;
+}
+
+template <class Op>
+KArgs<Op> make_args(cfm_cg *h, const Op &op, const double *b_dev, double *x_dev) {
+    KArgs<Op> a{};
+    const size_t n = h->n;
+    a.op = op;
+    a.n = h->n;
     a.ntiles = h->ntiles;
-    a.rowptr = h->A->rowptr;
-    a.col = h->A->col;
-    a.val = h->A->val;
     a.b = b_dev;
     a.x = x_dev ? x_dev : h->vec;
-    a.r = h->vec + (size_t)n;
-    a.p = h->vec + 2 * (size_t)n;
-    a.s = h->vec + 3 * (size_t)n;
-    a.t = h->vec + 4 * (size_t)n;
+    a.r = h->vec + n;
+    a.p = h->vec + 2 * n;
+    a.s = h->vec + 3 * n;
+    a.t = h->vec + 4 * n;
+    a.z = h->vec + 6 * n;
+    a.w0 = h->vec + 7 * n;
+    a.w1 = h->vec + 8 * n;
+    a.r32 = h->vec32;
+    a.p32 = h->vec32 + n;
+    a.s32 = h->vec32 + 2 * n;
+    a.d32 = h->vec32 + 3 * n;
     a.part = h->part;
     a.res = h->res;
     a.bar = h->bar;
     a.maxiter = h->p.maxiter;
     a.tol = h->p.tol;
+    a.inner_maxiter = h->p.inner_maxiter > 0 ? h->p.inner_maxiter : 1000;
+    a.inner_tol = h->p.inner_tol > 0 ? h->p.inner_tol : 1e-4;
     return a;
 }
 
-int run_discrete(cfm_cg *h, const CgArgs &a, CgResult *out, int *launches) {
+template <class Op>
+int run_discrete(cfm_cg *h, const KArgs<Op> &a, CgResult *out, int *launches) {
     const int g = a.ntiles;
     cudaStream_t st = h->stream;
-    double hs[4];
+    double hs[NSLOTS];
     auto fetch = [&](int which) -> int {
-        k_reduce<<<1, CG_TILE, 0, st>>>(a, which, h->scal);
+        k_reduce<Op><<<1, CG_TILE, 0, st>>>(a, which, h->scal);
         CFM_CUDA_TRY(cudaGetLastError());
         CFM_CUDA_TRY(cudaMemcpyAsync(&hs[which], h->scal + which, sizeof(double),
                                      cudaMemcpyDeviceToHost, st));
@@ -348,12 +138,12 @@ int run_discrete(cfm_cg *h, const CgArgs &a, CgResult *out, int *launches) {
         return CFM_OK;
     };
     int e;
-    k_init<<<g, CG_TILE, 0, st>>>(a);
+    k_init<Op><<<g, CG_TILE, 0, st>>>(a);
     CFM_CUDA_TRY(cudaGetLastError());
     *launches += 1;
-    if ((e = fetch(0)) || (e = fetch(3))) return e;
-    double gamma0 = hs[0];
-    const double bnorm = std::sqrt(hs[3]);
+    if ((e = fetch(SL_G0)) || (e = fetch(SL_B))) return e;
+    double gamma0 = hs[SL_G0];
+    const double bnorm = std::sqrt(hs[SL_B]);
     const bool use_tol = a.tol > 0.0;
     const double target = a.tol * bnorm;
     int status = use_tol ? CFM_NOT_CONVERGED : CFM_OK;
@@ -361,33 +151,33 @@ int run_discrete(cfm_cg *h, const CgArgs &a, CgResult *out, int *launches) {
     long long k = 0;
     if (use_tol && std::sqrt(gamma0) <= target) status = CFM_OK;
     while (k < a.maxiter && !(use_tol && status == CFM_OK)) {
-        k_spmv_dot<<<g, CG_TILE, 0, st>>>(a);
+        k_spmv_dot<Op><<<g, CG_TILE, 0, st>>>(a);
         *launches += 1;
-        if ((e = fetch(1))) return e;
-        const double delta = hs[1];
+        if ((e = fetch(SL_D0))) return e;
+        const double delta = hs[SL_D0];
         const double alpha = gamma0 / delta;
         if (use_tol && !(delta > 0.0 && std::isfinite(alpha))) {
             status = CFM_BREAKDOWN;
             break;
         }
-        k_update<<<g, CG_TILE, 0, st>>>(a, alpha);
+        k_update<Op><<<g, CG_TILE, 0, st>>>(a, alpha);
         *launches += 1;
-        if ((e = fetch(0))) return e;
-        const double gamma1 = hs[0];
+        if ((e = fetch(SL_G0))) return e;
+        const double gamma1 = hs[SL_G0];
         ++k;
         if (use_tol && std::sqrt(gamma1) <= target) {
-            k_true_residual<<<g, CG_TILE, 0, st>>>(a);
+            k_true_residual<Op><<<g, CG_TILE, 0, st>>>(a);
             *launches += 1;
-            if ((e = fetch(2))) return e;
-            if (std::sqrt(hs[2]) <= target) {
+            if ((e = fetch(SL_TT))) return e;
+            if (std::sqrt(hs[SL_TT]) <= target) {
                 status = CFM_OK;
                 gamma0 = gamma1;
                 break;
             }
-            k_restart<<<g, CG_TILE, 0, st>>>(a);
+            k_restart<Op><<<g, CG_TILE, 0, st>>>(a);
             *launches += 1;
             ++restarts;
-            gamma0 = hs[2];
+            gamma0 = hs[SL_TT];
             continue;
         }
         const double beta = gamma1 / gamma0;
@@ -395,7 +185,7 @@ int run_discrete(cfm_cg *h, const CgArgs &a, CgResult *out, int *launches) {
             status = CFM_BREAKDOWN;
             break;
         }
-        k_p<<<g, CG_TILE, 0, st>>>(a, beta);
+        k_p<Op><<<g, CG_TILE, 0, st>>>(a, beta);
         *launches += 1;
         gamma0 = gamma1;
     }
@@ -409,23 +199,54 @@ int run_discrete(cfm_cg *h, const CgArgs &a, CgResult *out, int *launches) {
 }
 
 // Final FP64 true relative residual (after the timed region).
-int true_relres(cfm_cg *h, const CgArgs &a, double bnorm, double *out) {
-    k_true_residual<<<a.ntiles, CG_TILE, 0, h->stream>>>(a);
+template <class Op>
+int true_relres(cfm_cg *h, const KArgs<Op> &a, double bnorm, double *out) {
+    k_true_residual<Op><<<a.ntiles, CG_TILE, 0, h->stream>>>(a);
     CFM_CUDA_TRY(cudaGetLastError());
-    k_reduce<<<1, CG_TILE, 0, h->stream>>>(a, 2, h->scal);
+    k_reduce<Op><<<1, CG_TILE, 0, h->stream>>>(a, SL_TT, h->scal);
     CFM_CUDA_TRY(cudaGetLastError());
     double tt = 0;
-    CFM_CUDA_TRY(cudaMemcpyAsync(&tt, h->scal + 2, sizeof(double), cudaMemcpyDeviceToHost,
+    CFM_CUDA_TRY(cudaMemcpyAsync(&tt, h->scal + SL_TT, sizeof(double), cudaMemcpyDeviceToHost,
                                  h->stream));
     CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     *out = bnorm > 0 ? std::sqrt(tt) / bnorm : std::sqrt(tt);
     return CFM_OK;
 }
 
-int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, double h2d,
-               double d2h, const double *b_host, double *x_host) {
-    const int n = h->A->n;
-    CgArgs a = make_args(h, b_dev, x_dev);
+template <class Op>
+const void *solver_fn(int impl) {
+    switch (impl) {
+        case CFM_CG_PERSISTENT_PIPELINED: return (const void *)cg_pipe_kernel<Op>;
+        case CFM_CG_MIXED: return (const void *)cg_mixed_kernel<Op>;
+        default: return (const void *)cg_std_kernel<Op>;
+    }
+}
+
+// Algorithmic HBM bytes of one iteration: operator data plus the vector
+// passes of the method (8 B per FP64 entry read or written, 4 per FP32).
+double bytes_per_iter(const cfm_cg *h) {
+    const double n = h->n;
+    double op64, op32;
+    if (h->kind == 0) {
+        const double nnz = (double)h->A->nnz;
+        op64 = 12.0 * nnz + 4.0 * (n + 1);
+        op32 = 8.0 * nnz + 4.0 * (n + 1);
+    } else {
+        op64 = 8.0 * h->kind * n;  // dims face arrays + diagonal
+        op32 = 4.0 * h->kind * n;
+    }
+    switch (h->p.impl) {
+        case CFM_CG_PERSISTENT_PIPELINED: return op64 + 96.0 * n;
+        case CFM_CG_MIXED: return op32 + 44.0 * n;
+        default: return op64 + 88.0 * n;
+    }
+}
+
+template <class Op>
+int solve_t(cfm_cg *h, const Op &op, const double *b_dev, double *x_dev, cfm_stats *st,
+            double h2d, double d2h, const double *b_host, double *x_host) {
+    const int n = h->n;
+    KArgs<Op> a = make_args(h, op, b_dev, x_dev);
     BarrierState bs{};
     bs.timeout_ns = barrier_timeout_ns();
     CFM_CUDA_TRY(cudaMemcpyAsync(h->bar, &bs, sizeof(bs), cudaMemcpyHostToDevice, h->stream));
@@ -442,8 +263,8 @@ int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, dou
         if (e) return e;
     } else {
         void *args[] = {&a};
-        CFM_CUDA_TRY(launch_cooperative((const void *)cg_persistent_kernel, dim3(h->blocks),
-                                        dim3(CG_TILE), args, 0, h->stream));
+        CFM_CUDA_TRY(launch_cooperative(solver_fn<Op>(h->p.impl), dim3(h->blocks), dim3(CG_TILE),
+                                        args, 0, h->stream));
         launches += 1;
     }
     if (x_host) {
@@ -454,7 +275,6 @@ int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, dou
     CFM_CUDA_TRY(cudaEventSynchronize(h->ev1));
     float ms = 0.f;
     CFM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-    int status;
     if (h->p.impl != CFM_CG_DISCRETE) {
         CFM_CUDA_TRY(cudaMemcpy(&bs, h->bar, sizeof(bs), cudaMemcpyDeviceToHost));
         if (bs.error) {
@@ -467,7 +287,7 @@ int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, dou
         }
         CFM_CUDA_TRY(cudaMemcpy(&r, h->res, sizeof(r), cudaMemcpyDeviceToHost));
     }
-    status = r.status;
+    const int status = r.status;
     double relres = 0;
     int e = true_relres(h, a, r.bnorm, &relres);
     if (e) return e;
@@ -476,10 +296,7 @@ int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, dou
         st->seconds = ms * 1e-3;
         st->iterations = r.iters;
         st->residual = relres;
-        const double nnz = (double)h->A->nnz;
-        // FP64 standard CG, fused dots: matrix (12 B/nnz + 4(n+1)) + 11 vector
-        // passes of 8 B per row per iteration.
-        st->bytes = (double)r.iters * (12.0 * nnz + 4.0 * (n + 1) + 88.0 * n);
+        st->bytes = (double)r.iters * bytes_per_iter(h);
         st->gbs = st->seconds > 0 ? st->bytes / st->seconds * 1e-9 : 0;
         st->h2d_bytes = h2d;
         st->d2h_bytes = d2h;
@@ -491,6 +308,68 @@ int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, dou
         set_error("not converged after %lld iterations (true relres %.3e)", r.iters, relres);
     if (status == CFM_BREAKDOWN) set_error("CG breakdown at iteration %lld", r.iters);
     return status;
+}
+
+int solve_impl(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st, double h2d,
+               double d2h, const double *b_host, double *x_host) {
+    switch (h->kind) {
+        case 2: return solve_t(h, stencil_op<2>(h->S), b_dev, x_dev, st, h2d, d2h, b_host, x_host);
+        case 3: return solve_t(h, stencil_op<3>(h->S), b_dev, x_dev, st, h2d, d2h, b_host, x_host);
+        default: return solve_t(h, csr_op(h->A), b_dev, x_dev, st, h2d, d2h, b_host, x_host);
+    }
+}
+
+template <class Op>
+int occupancy(int impl, int *per_sm) {
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, solver_fn<Op>(impl),
+                                                               CG_TILE, 0));
+    return CFM_OK;
+}
+
+int create_common(cfm_cg *h, const cfm_cg_params *p) {
+    h->p = *p;
+    const size_t n = h->n;
+    h->ntiles = (int)((n + CG_TILE - 1) / CG_TILE);
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->vec, sizeof(double) * 9 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->vec32, sizeof(float) * 4 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->part, sizeof(double) * NSLOTS * (size_t)h->ntiles)) != cudaSuccess ||
+        (e = cudaMalloc(&h->scal, sizeof(double) * NSLOTS)) != cudaSuccess ||
+        (e = cudaMalloc(&h->res, sizeof(CgResult))) != cudaSuccess ||
+        (e = cudaMalloc(&h->bar, sizeof(BarrierState))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev0)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+        set_error("cg handle setup failed: %s", cudaGetErrorString(e));
+        cudaGetLastError();
+        return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+    }
+    h->own_stream = true;
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    int per_sm = 0;
+    switch (h->kind) {
+        case 2: st = occupancy<StencilOp<2>>(p->impl, &per_sm); break;
+        case 3: st = occupancy<StencilOp<3>>(p->impl, &per_sm); break;
+        default: st = occupancy<CsrOp>(p->impl, &per_sm); break;
+    }
+    if (st) return st;
+    if (per_sm < 1) {
+        set_error("cg kernel cannot be resident");
+        return CFM_UNSUPPORTED;
+    }
+    h->blocks = std::min(per_sm * di.num_sms, h->ntiles);
+    return CFM_OK;
+}
+
+int check_cg_params(const cfm_cg_params *p) {
+    CFM_ARG_CHECK(p->impl >= CFM_CG_DISCRETE && p->impl <= CFM_CG_MIXED, "impl");
+    CFM_ARG_CHECK(p->maxiter >= 0, "maxiter");
+    CFM_ARG_CHECK(p->impl != CFM_CG_MIXED || p->tol > 0, "mixed precision needs tol > 0");
+    CFM_ARG_CHECK(p->inner_maxiter >= 0 && p->inner_tol >= 0 && p->inner_tol < 1,
+                  "inner_maxiter, inner_tol");
+    return CFM_OK;
 }
 
 }  // namespace
@@ -521,10 +400,12 @@ int cfm_csr_create(int n, long long nnz, const int *rowptr, const int *col, cons
     cfm_csr *A = new cfm_csr();
     A->n = n;
     A->nnz = nnz;
+    const size_t nz1 = (size_t)std::max(1LL, nnz);
     cudaError_t e;
     if ((e = cudaMalloc(&A->rowptr, sizeof(int) * (n + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&A->col, sizeof(int) * std::max(1LL, nnz))) != cudaSuccess ||
-        (e = cudaMalloc(&A->val, sizeof(double) * std::max(1LL, nnz))) != cudaSuccess ||
+        (e = cudaMalloc(&A->col, sizeof(int) * nz1)) != cudaSuccess ||
+        (e = cudaMalloc(&A->val, sizeof(double) * nz1)) != cudaSuccess ||
+        (e = cudaMalloc(&A->val32, sizeof(float) * nz1)) != cudaSuccess ||
         (e = cudaMemcpy(A->rowptr, rp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice)) !=
             cudaSuccess ||
         (nnz && (e = cudaMemcpy(A->col, cc.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice)) !=
@@ -535,6 +416,14 @@ int cfm_csr_create(int n, long long nnz, const int *rowptr, const int *col, cons
         cfm_csr_destroy(A);
         return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
     }
+    if (nnz) {
+        k_to_f32<<<1024, 256>>>(A->val, A->val32, (size_t)nnz);
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+            set_error("csr fp32 copy failed: %s", cudaGetErrorString(e));
+            cfm_csr_destroy(A);
+            return CFM_CUDA_ERROR;
+        }
+    }
     *out = A;
     return CFM_OK;
 }
@@ -544,6 +433,7 @@ void cfm_csr_destroy(cfm_csr *A) {
     cudaFree(A->rowptr);
     cudaFree(A->col);
     cudaFree(A->val);
+    cudaFree(A->val32);
     delete A;
 }
 
@@ -555,10 +445,80 @@ int cfm_csr_spmv_host(const cfm_csr *A, const double *x, double *y) {
     CFM_CUDA_TRY(cudaMalloc(&d, 2 * bytes));
     cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        k_spmv<<<(A->n + 255) / 256, 256>>>(A->n, A->rowptr, A->col, A->val, d, d + A->n);
+        k_apply<CsrOp><<<(A->n + 255) / 256, 256>>>(csr_op(A), A->n, d, d + A->n);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(y, d + A->n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    CFM_CUDA_TRY(e);
+    return CFM_OK;
+}
+
+int cfm_stencil_create(int dims, int nx, int ny, int nz, const double *k_host,
+                       cfm_stencil **out) {
+    clear_error();
+    CFM_ARG_CHECK(out && k_host, "null argument");
+    *out = nullptr;
+    CFM_ARG_CHECK(dims == 2 || dims == 3, "dims must be 2 or 3");
+    if (dims == 2) nz = 1;
+    CFM_ARG_CHECK(nx >= 1 && ny >= 1 && nz >= 1, "sizes");
+    const double cells = (double)nx * ny * nz;
+    CFM_ARG_CHECK(cells < 2.0e9, "grid too large for int32 rows");
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t i = 0; i < n; ++i)
+        CFM_ARG_CHECK(k_host[i] > 0 && std::isfinite(k_host[i]), "k must be positive and finite");
+    std::vector<double> c(4 * n, 0.0);
+    int st = cfm_varcoef_coeffs(dims, nx, ny, nz, k_host, c.data(), c.data() + n,
+                                c.data() + 2 * n, c.data() + 3 * n);
+    if (st) return st;
+    cfm_stencil *S = new cfm_stencil();
+    S->dims = dims;
+    S->nx = nx;
+    S->ny = ny;
+    S->nz = nz;
+    S->n = (int)n;
+    cudaError_t e;
+    if ((e = cudaMalloc(&S->c64, sizeof(double) * 4 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&S->c32, sizeof(float) * 4 * n)) != cudaSuccess ||
+        (e = cudaMemcpy(S->c64, c.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice)) !=
+            cudaSuccess) {
+        set_error("stencil upload failed: %s", cudaGetErrorString(e));
+        cfm_stencil_destroy(S);
+        return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+    }
+    k_to_f32<<<1024, 256>>>(S->c64, S->c32, 4 * n);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+        set_error("stencil fp32 copy failed: %s", cudaGetErrorString(e));
+        cfm_stencil_destroy(S);
+        return CFM_CUDA_ERROR;
+    }
+    *out = S;
+    return CFM_OK;
+}
+
+void cfm_stencil_destroy(cfm_stencil *S) {
+    if (!S) return;
+    cudaFree(S->c64);
+    cudaFree(S->c32);
+    delete S;
+}
+
+int cfm_stencil_apply_host(const cfm_stencil *S, const double *x, double *y) {
+    CFM_ARG_CHECK(S && x && y, "null argument");
+    clear_error();
+    const size_t bytes = sizeof(double) * S->n;
+    double *d = nullptr;
+    CFM_CUDA_TRY(cudaMalloc(&d, 2 * bytes));
+    cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const int g = (S->n + 255) / 256;
+        if (S->dims == 2)
+            k_apply<StencilOp<2>><<<g, 256>>>(stencil_op<2>(S), S->n, d, d + S->n);
+        else
+            k_apply<StencilOp<3>><<<g, 256>>>(stencil_op<3>(S), S->n, d, d + S->n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + S->n, bytes, cudaMemcpyDeviceToHost);
     cudaFree(d);
     CFM_CUDA_TRY(e);
     return CFM_OK;
@@ -568,42 +528,34 @@ int cfm_cg_create(const cfm_csr *A, const cfm_cg_params *p, cfm_cg **out) {
     clear_error();
     CFM_ARG_CHECK(A && p && out, "null argument");
     *out = nullptr;
-    CFM_ARG_CHECK(p->impl == CFM_CG_DISCRETE || p->impl == CFM_CG_PERSISTENT,
-                  "impl (pipelined and mixed are not built yet)");
-    CFM_ARG_CHECK(p->maxiter >= 0, "maxiter");
+    int st = check_cg_params(p);
+    if (st) return st;
     cfm_cg *h = new cfm_cg();
-    h->p = *p;
+    h->kind = 0;
     h->A = A;
-    const int n = A->n;
-    h->ntiles = (n + CG_TILE - 1) / CG_TILE;
-    auto fail = [&](int s) {
+    h->n = A->n;
+    if ((st = create_common(h, p))) {
         cfm_cg_destroy(h);
-        return s;
-    };
-    cudaError_t e;
-    if ((e = cudaMalloc(&h->vec, sizeof(double) * 6 * (size_t)n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->part, sizeof(double) * 4 * (size_t)h->ntiles)) != cudaSuccess ||
-        (e = cudaMalloc(&h->scal, sizeof(double) * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&h->res, sizeof(CgResult))) != cudaSuccess ||
-        (e = cudaMalloc(&h->bar, sizeof(BarrierState))) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&h->ev0)) != cudaSuccess ||
-        (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
-        set_error("cg handle setup failed: %s", cudaGetErrorString(e));
-        cudaGetLastError();
-        return fail(e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR);
+        return st;
     }
-    h->own_stream = true;
-    DeviceInfo di;
-    int st = current_device_info(&di);
-    if (st) return fail(st);
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent_kernel, CG_TILE, 0);
-    if (e != cudaSuccess || per_sm < 1) {
-        set_error("cg kernel cannot be resident");
-        return fail(CFM_UNSUPPORTED);
+    *out = h;
+    return CFM_OK;
+}
+
+int cfm_cg_create_stencil(const cfm_stencil *S, const cfm_cg_params *p, cfm_cg **out) {
+    clear_error();
+    CFM_ARG_CHECK(S && p && out, "null argument");
+    *out = nullptr;
+    int st = check_cg_params(p);
+    if (st) return st;
+    cfm_cg *h = new cfm_cg();
+    h->kind = S->dims;
+    h->S = S;
+    h->n = S->n;
+    if ((st = create_common(h, p))) {
+        cfm_cg_destroy(h);
+        return st;
     }
-    h->blocks = std::min(per_sm * di.num_sms, h->ntiles);
     *out = h;
     return CFM_OK;
 }
@@ -612,6 +564,7 @@ void cfm_cg_destroy(cfm_cg *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->vec);
+    cudaFree(h->vec32);
     cudaFree(h->part);
     cudaFree(h->scal);
     cudaFree(h->res);
@@ -641,7 +594,7 @@ int cfm_cg_set_stream(cfm_cg *h, void *cuda_stream) {
 int cfm_cg_solve(cfm_cg *h, const double *b_host, double *x_host, cfm_stats *st) {
     CFM_ARG_CHECK(h && x_host, "null argument");
     clear_error();
-    const int n = h->A->n;
+    const int n = h->n;
     double *b_dev = b_host ? h->vec + 5 * (size_t)n : nullptr;
     return solve_impl(h, b_dev, nullptr, st, b_host ? 8.0 * n : 0.0, 8.0 * n, b_host, x_host);
 }
@@ -655,7 +608,7 @@ int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats
 }  // extern "C"
 
 // ------------------------------------------- CG without device allocation
-// cfm_cg_solve_noalloc runs cg_persistent_kernel with its scratch carved out
+// cfm_cg_solve_noalloc runs cg_std_kernel<CsrOp> with its scratch carved out
 // of one fixed device array instead of cudaMalloc'd buffers, for callers
 // that cannot allocate device memory (an outside allocator owns the pool,
 // the memory is reserved up front, or an allocation would synchronise).
@@ -741,18 +694,18 @@ extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
     if ((e = current_device_info(&di))) return e;
     int per_sm = 0;
     CFM_CUDA_TRY(
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_persistent_kernel, CG_TILE, 0));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_std_kernel<CsrOp>, CG_TILE, 0));
     if (per_sm < 1) {
         set_error("cg kernel cannot be resident");
         return CFM_UNSUPPORTED;
     }
     cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
-    CgArgs a{};
+    KArgs<CsrOp> a{};
     a.n = n;
     a.ntiles = (n + CG_TILE - 1) / CG_TILE;
-    a.rowptr = rowptr_dev;
-    a.col = col_dev;
-    a.val = val_dev;
+    a.op.rowptr = rowptr_dev;
+    a.op.col = col_dev;
+    a.op.val = val_dev;
     a.b = b_dev;
     a.x = x_dev;
     a.r = scr + NA_VEC;
@@ -770,12 +723,12 @@ extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
     k_noalloc_reset<<<1, 1, 0, s>>>(a.bar, barrier_timeout_ns());
     CFM_CUDA_TRY(cudaGetLastError());
     void *args[] = {&a};
-    CFM_CUDA_TRY(launch_cooperative((const void *)cg_persistent_kernel, dim3(blocks),
+    CFM_CUDA_TRY(launch_cooperative((const void *)cg_std_kernel<CsrOp>, dim3(blocks),
                                     dim3(CG_TILE), args, 0, s));
     // final FP64 true residual b - A x into partial slot 2, reduced to scal[2]
-    k_true_residual<<<a.ntiles, CG_TILE, 0, s>>>(a);
+    k_true_residual<CsrOp><<<a.ntiles, CG_TILE, 0, s>>>(a);
     CFM_CUDA_TRY(cudaGetLastError());
-    k_reduce<<<1, CG_TILE, 0, s>>>(a, 2, scal);
+    k_reduce<CsrOp><<<1, CG_TILE, 0, s>>>(a, SL_TT, scal);
     CFM_CUDA_TRY(cudaGetLastError());
     double hdr[NA_HDR];
     CFM_CUDA_TRY(cudaMemcpyAsync(hdr, scr, sizeof(hdr), cudaMemcpyDeviceToHost, s));
@@ -794,7 +747,7 @@ extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
         }
         return CFM_BARRIER_TIMEOUT;
     }
-    const double tt = hdr[16 + 2];
+    const double tt = hdr[16 + SL_TT];
     const double relres = r.bnorm > 0 ? std::sqrt(tt) / r.bnorm : std::sqrt(tt);
     if (st) {
         std::memset(st, 0, sizeof(*st));

@@ -1,0 +1,670 @@
+// Persistent Krylov solvers on one GPU, templated on the operator.
+//
+// Operators (one row per thread, tiles of CG_TILE consecutive rows):
+//   CsrOp        CSR SpMV, row order, one fma per nonzero (CG/src/common.cu:150-168)
+//   StencilOp<D> matrix-free cell-centred -div(k grad u), 5-point (D = 2) or
+//                7-point (D = 3): t = d_i u_i, then one fma(-w, u_nb, t) per
+//                neighbour in the order x-1, x+1, y-1, y+1, z-1, z+1
+// Each operator also applies in FP32 (apply32) from FP32 copies of its
+// coefficients, for the inner solve of the mixed-precision method.
+//
+// Solvers, each one cooperative launch for the whole solve:
+//   cg_std_kernel    standard CG, 3 grid barriers per iteration
+//                    (CG/src/common.cu:399-538, CG/src/single-stream/standard.cu:158-299)
+//   cg_pipe_kernel   pipelined CG (CG/src/single-stream/pipelined.cu:176-330): the
+//                    SpMV q = A w and every vector recurrence of an iteration fused
+//                    into one pass, double-buffered w and dot partials, 1 grid
+//                    barrier per iteration
+//   cg_mixed_kernel  FP64 iterative refinement around an FP32 inner CG: the true
+//                    residual, the correction x += |r| d and the dot reductions
+//                    (FP64 sums of exact FP32 products) stay FP64
+// Every dot is a fixed tree (1024-row tiles, xor butterflies, then the tile
+// partials in lane order), so results do not depend on the launch shape and
+// the CPU oracle reproduces them bit for bit.  Scalar arithmetic is written
+// with explicit-rounding intrinsics where the compiler could otherwise fuse a
+// multiply into an add.
+#pragma once
+
+#include "barrier.cuh"
+
+namespace cfm {
+
+constexpr int CG_TILE = 1024;  // rows per tile == threads per block
+constexpr unsigned CG_FULL = 0xffffffffu;
+
+// Partial-sum slots (each ntiles doubles) in KArgs::part.
+enum : int { SL_G0 = 0, SL_D0 = 1, SL_TT = 2, SL_B = 3, SL_G1 = 4, SL_D1 = 5, NSLOTS = 6 };
+
+struct CgResult {
+    long long iters;
+    int status;
+    int restarts;  // restarts (standard, pipelined) or refinement sweeps (mixed)
+    double gamma;
+    double bnorm;
+};
+
+__device__ __forceinline__ double warp_xor_sum(double v) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(CG_FULL, v, off));
+    return v;
+}
+
+// Tree sum over the 1024 threads of the block; every thread gets the result.
+__device__ __forceinline__ double block_sum(double v, double *sm /* 33 doubles */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_xor_sum(v);
+    if (lane == 0) sm[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double w = warp_xor_sum(sm[lane]);
+        if (lane == 0) sm[32] = w;
+    }
+    __syncthreads();
+    const double out = sm[32];
+    __syncthreads();
+    return out;
+}
+
+// Sum of tile partials in the fixed order: thread t adds part[t], part[t+1024], ...
+__device__ __forceinline__ double sum_partials(const double *part, int ntiles, double *sm) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < ntiles; i += CG_TILE) acc = __dadd_rn(acc, part[i]);
+    return block_sum(acc, sm);
+}
+
+// Exact product of two FP32 values, as FP64.
+__device__ __forceinline__ double xprod(float a, float b) { return __dmul_rn((double)a, (double)b); }
+
+// ------------------------------------------------------------- operators
+struct CsrOp {
+    const int *rowptr, *col;
+    const double *val;
+    const float *val32;
+    __device__ __forceinline__ double apply(const double *x, int i) const {
+        double acc = 0.0;
+        const int j1 = rowptr[i + 1];
+        for (int j = rowptr[i]; j < j1; ++j) acc = __fma_rn(val[j], x[col[j]], acc);
+        return acc;
+    }
+    __device__ __forceinline__ float apply32(const float *x, int i) const {
+        float acc = 0.f;
+        const int j1 = rowptr[i + 1];
+        for (int j = rowptr[i]; j < j1; ++j) acc = __fmaf_rn(val32[j], x[col[j]], acc);
+        return acc;
+    }
+    // A x0 with x0 = 0, summed like apply (always +0)
+    __device__ __forceinline__ double apply_zero(int i) const {
+        double acc = 0.0;
+        const int j1 = rowptr[i + 1];
+        for (int j = rowptr[i]; j < j1; ++j) acc = __fma_rn(val[j], 0.0, acc);
+        return acc;
+    }
+};
+
+template <int D>
+struct StencilOp {
+    int nx, ny, nz;
+    const double *we, *wn, *wt, *dg;
+    const float *we32, *wn32, *wt32, *dg32;
+    __device__ __forceinline__ double apply(const double *x, int i) const {
+        const int ix = i % nx, q = i / nx, iy = q % ny;
+        double t = __dmul_rn(dg[i], x[i]);
+        if (ix > 0) t = __fma_rn(-we[i - 1], x[i - 1], t);
+        if (ix < nx - 1) t = __fma_rn(-we[i], x[i + 1], t);
+        if (iy > 0) t = __fma_rn(-wn[i - nx], x[i - nx], t);
+        if (iy < ny - 1) t = __fma_rn(-wn[i], x[i + nx], t);
+        if (D == 3) {
+            const int iz = q / ny, P = nx * ny;
+            if (iz > 0) t = __fma_rn(-wt[i - P], x[i - P], t);
+            if (iz < nz - 1) t = __fma_rn(-wt[i], x[i + P], t);
+        }
+        return t;
+    }
+    __device__ __forceinline__ float apply32(const float *x, int i) const {
+        const int ix = i % nx, q = i / nx, iy = q % ny;
+        float t = __fmul_rn(dg32[i], x[i]);
+        if (ix > 0) t = __fmaf_rn(-we32[i - 1], x[i - 1], t);
+        if (ix < nx - 1) t = __fmaf_rn(-we32[i], x[i + 1], t);
+        if (iy > 0) t = __fmaf_rn(-wn32[i - nx], x[i - nx], t);
+        if (iy < ny - 1) t = __fmaf_rn(-wn32[i], x[i + nx], t);
+        if (D == 3) {
+            const int iz = q / ny, P = nx * ny;
+            if (iz > 0) t = __fmaf_rn(-wt32[i - P], x[i - P], t);
+            if (iz < nz - 1) t = __fmaf_rn(-wt32[i], x[i + P], t);
+        }
+        return t;
+    }
+    __device__ __forceinline__ double apply_zero(int) const { return 0.0; }
+};
+
+template <class Op>
+struct KArgs {
+    Op op;
+    int n;
+    int ntiles;
+    const double *b;  // nullptr: ones
+    double *x, *r, *p, *s, *t;
+    double *z, *w0, *w1;           // pipelined
+    float *r32, *p32, *s32, *d32;  // mixed inner
+    double *part;                  // NSLOTS * ntiles
+    CgResult *res;
+    BarrierState *bar;
+    int maxiter;
+    double tol;
+    int inner_maxiter;
+    double inner_tol;
+};
+
+#define CFM_TILES(a) for (int tile = blockIdx.x; tile < (a).ntiles; tile += gridDim.x)
+#define CFM_ROW(a) const int i = tile * CG_TILE + threadIdx.x
+
+template <class Op>
+__device__ __forceinline__ double *slot(const KArgs<Op> &a, int s) {
+    return a.part + (size_t)s * a.ntiles;
+}
+
+// -------------------------------------------------------- standard phases
+template <class Op>
+__device__ void phase_init(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0, bb = 0.0;
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            const double ri = __fma_rn(-1.0, a.op.apply_zero(i), bi);  // r0 = b - A x0, x0 = 0
+            a.x[i] = 0.0;
+            a.r[i] = ri;
+            a.p[i] = ri;
+            g = __dmul_rn(ri, ri);
+            bb = __dmul_rn(bi, bi);
+        }
+        g = block_sum(g, sm);
+        bb = block_sum(bb, sm);
+        if (threadIdx.x == 0) {
+            slot(a, SL_G0)[tile] = g;
+            slot(a, SL_B)[tile] = bb;
+        }
+    }
+}
+
+template <class Op>
+__device__ void phase_spmv_dot(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double d = 0.0;
+        if (i < a.n) {
+            const double si = a.op.apply(a.p, i);
+            a.s[i] = si;
+            d = __dmul_rn(a.p[i], si);
+        }
+        d = block_sum(d, sm);
+        if (threadIdx.x == 0) slot(a, SL_D0)[tile] = d;
+    }
+}
+
+template <class Op>
+__device__ void phase_update(const KArgs<Op> &a, double alpha, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0;
+        if (i < a.n) {
+            a.x[i] = __fma_rn(alpha, a.p[i], a.x[i]);
+            const double ri = __fma_rn(-alpha, a.s[i], a.r[i]);
+            a.r[i] = ri;
+            g = __dmul_rn(ri, ri);
+        }
+        g = block_sum(g, sm);
+        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+    }
+}
+
+// t = b - A x (FP64) and its squared norm into SL_TT
+template <class Op>
+__device__ void phase_true_residual(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double q = 0.0;
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            const double ti = __dsub_rn(bi, a.op.apply(a.x, i));
+            a.t[i] = ti;
+            q = __dmul_rn(ti, ti);
+        }
+        q = block_sum(q, sm);
+        if (threadIdx.x == 0) slot(a, SL_TT)[tile] = q;
+    }
+}
+
+template <class Op>
+__device__ void phase_restart(const KArgs<Op> &a) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) {
+            a.r[i] = a.t[i];
+            a.p[i] = a.t[i];
+        }
+    }
+}
+
+template <class Op>
+__device__ void phase_p(const KArgs<Op> &a, double beta) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) a.p[i] = __fma_rn(beta, a.p[i], a.r[i]);
+    }
+}
+
+__device__ __forceinline__ void write_result(CgResult *res, long long k, int status, int restarts,
+                                             double gamma, double bnorm) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        res->iters = k;
+        res->status = status;
+        res->restarts = restarts;
+        res->gamma = gamma;
+        res->bnorm = bnorm;
+    }
+}
+
+// Standard CG; tol > 0 stops when the recursive residual reaches tol ||b||
+// and the FP64 true residual confirms it (a restart from the true residual
+// otherwise); tol <= 0 runs exactly maxiter iterations (reference -niter).
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE, 1) cg_std_kernel(KArgs<Op> a) {
+    __shared__ double sm[33];
+    int site = 0;
+    phase_init(a, sm);
+    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+    double gamma0 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+    const double bnorm = sqrt(sum_partials(slot(a, SL_B), a.ntiles, sm));
+    const bool use_tol = a.tol > 0.0;
+    const double target = a.tol * bnorm;
+    int status = use_tol ? CFM_NOT_CONVERGED : CFM_OK;
+    int restarts = 0;
+    long long k = 0;
+    if (use_tol && sqrt(gamma0) <= target) status = CFM_OK;
+    while (k < a.maxiter && !(use_tol && status == CFM_OK)) {
+        phase_spmv_dot(a, sm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        const double delta = sum_partials(slot(a, SL_D0), a.ntiles, sm);
+        const double alpha = gamma0 / delta;
+        if (use_tol && !(delta > 0.0 && isfinite(alpha))) {
+            status = CFM_BREAKDOWN;
+            break;
+        }
+        phase_update(a, alpha, sm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        const double gamma1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+        ++k;
+        if (use_tol && sqrt(gamma1) <= target) {
+            phase_true_residual(a, sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            const double tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+            if (sqrt(tt) <= target) {
+                status = CFM_OK;
+                gamma0 = gamma1;
+                break;
+            }
+            phase_restart(a);
+            ++restarts;
+            gamma0 = tt;
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            continue;
+        }
+        const double beta = gamma1 / gamma0;
+        if (use_tol && !isfinite(beta)) {
+            status = CFM_BREAKDOWN;
+            break;
+        }
+        phase_p(a, beta);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        gamma0 = gamma1;
+    }
+    write_result(a.res, k, status, restarts, gamma0, bnorm);
+}
+
+// ------------------------------------------------------- pipelined phases
+// r0 = b - A x0 with x0 = 0 (into t), and ||b||^2.
+template <class Op>
+__device__ void phase_pipe_init(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double bb = 0.0;
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            a.x[i] = 0.0;
+            a.t[i] = __fma_rn(-1.0, a.op.apply_zero(i), bi);
+            bb = __dmul_rn(bi, bi);
+        }
+        bb = block_sum(bb, sm);
+        if (threadIdx.x == 0) slot(a, SL_B)[tile] = bb;
+    }
+}
+
+// r = v, w = A v, z = s = p = 0; partials <r, r> -> G[par], <w, r> -> D[par].
+// v is the initial residual, or the true residual t at a restart.
+template <class Op>
+__device__ void phase_pipe_start(const KArgs<Op> &a, const double *v, double *w, int par,
+                                 double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0, d = 0.0;
+        if (i < a.n) {
+            const double ri = v[i];
+            const double wi = a.op.apply(v, i);
+            a.r[i] = ri;
+            w[i] = wi;
+            a.z[i] = 0.0;
+            a.s[i] = 0.0;
+            a.p[i] = 0.0;
+            g = __dmul_rn(ri, ri);
+            d = __dmul_rn(wi, ri);
+        }
+        g = block_sum(g, sm);
+        d = block_sum(d, sm);
+        if (threadIdx.x == 0) {
+            slot(a, par ? SL_G1 : SL_G0)[tile] = g;
+            slot(a, par ? SL_D1 : SL_D0)[tile] = d;
+        }
+    }
+}
+
+// One pipelined iteration, row-local once q = A w is known:
+//   z = q + beta z; s = w + beta s; p = r + beta p
+//   x += alpha p; r -= alpha s; w' = w - alpha z
+// and the next iteration's partials <r', r'>, <w', r'> into slot parity `nxt`.
+template <class Op>
+__device__ void phase_pipe_step(const KArgs<Op> &a, const double *w, double *wn, double alpha,
+                                double beta, int nxt, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0, d = 0.0;
+        if (i < a.n) {
+            const double q = a.op.apply(w, i);
+            const double wi = w[i];
+            const double zi = __fma_rn(beta, a.z[i], q);
+            const double si = __fma_rn(beta, a.s[i], wi);
+            const double pi = __fma_rn(beta, a.p[i], a.r[i]);
+            a.x[i] = __fma_rn(alpha, pi, a.x[i]);
+            const double ri = __fma_rn(-alpha, si, a.r[i]);
+            const double wni = __fma_rn(-alpha, zi, wi);
+            a.z[i] = zi;
+            a.s[i] = si;
+            a.p[i] = pi;
+            a.r[i] = ri;
+            wn[i] = wni;
+            g = __dmul_rn(ri, ri);
+            d = __dmul_rn(wni, ri);
+        }
+        g = block_sum(g, sm);
+        d = block_sum(d, sm);
+        if (threadIdx.x == 0) {
+            slot(a, nxt ? SL_G1 : SL_G0)[tile] = g;
+            slot(a, nxt ? SL_D1 : SL_D0)[tile] = d;
+        }
+    }
+}
+
+// Pipelined CG.  Scalars follow the reference's recurrence
+// (CG/src/single-stream/pipelined.cu:262-272): with rr = <r, r>, wr = <w, r>,
+//   beta = rr / rr_prev, alpha = rr / (wr - (beta / alpha_prev) rr)
+// from the third step of a run on, and beta = 0, alpha = rr / wr on the
+// first two (the reference tests `k > 1`).  Convergence as cg_std_kernel.
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
+    __shared__ double sm[33];
+    int site = 0;
+    phase_pipe_init(a, sm);
+    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+    const double bnorm = sqrt(sum_partials(slot(a, SL_B), a.ntiles, sm));
+    phase_pipe_start(a, a.t, a.w0, 0, sm);
+    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+    const bool use_tol = a.tol > 0.0;
+    const double target = a.tol * bnorm;
+    int status = use_tol ? CFM_NOT_CONVERGED : CFM_OK;
+    int restarts = 0, cur = 0;
+    long long k = 0, kk = 0;
+    double rr = 0.0, rr_prev = 0.0, alpha = 0.0;
+    while (true) {
+        double *w = cur ? a.w1 : a.w0;
+        rr = sum_partials(slot(a, cur ? SL_G1 : SL_G0), a.ntiles, sm);
+        const double wr = sum_partials(slot(a, cur ? SL_D1 : SL_D0), a.ntiles, sm);
+        if (use_tol && sqrt(rr) <= target) {
+            phase_true_residual(a, sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            const double tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+            if (sqrt(tt) <= target) {
+                status = CFM_OK;
+                break;
+            }
+            phase_pipe_start(a, a.t, w, cur, sm);  // restart from the true residual
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            ++restarts;
+            kk = 0;
+            continue;
+        }
+        if (k >= a.maxiter) break;
+        double beta;
+        if (kk > 1) {
+            beta = rr / rr_prev;
+            alpha = rr / __dsub_rn(wr, __dmul_rn(beta / alpha, rr));
+        } else {
+            beta = 0.0;
+            alpha = rr / wr;
+        }
+        if (use_tol && !(isfinite(alpha) && alpha > 0.0 && isfinite(beta))) {
+            status = CFM_BREAKDOWN;
+            break;
+        }
+        phase_pipe_step(a, w, cur ? a.w0 : a.w1, alpha, beta, cur ^ 1, sm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        rr_prev = rr;
+        cur ^= 1;
+        ++k;
+        ++kk;
+    }
+    write_result(a.res, k, status, restarts, rr, bnorm);
+}
+
+// ----------------------------------------------------------- mixed phases
+// x = 0, t = b - A x0, partials ||t||^2 (SL_TT) and ||b||^2 (SL_B).
+template <class Op>
+__device__ void phase_mixed_init(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double q = 0.0, bb = 0.0;
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            const double ti = __fma_rn(-1.0, a.op.apply_zero(i), bi);
+            a.x[i] = 0.0;
+            a.t[i] = ti;
+            q = __dmul_rn(ti, ti);
+            bb = __dmul_rn(bi, bi);
+        }
+        q = block_sum(q, sm);
+        bb = block_sum(bb, sm);
+        if (threadIdx.x == 0) {
+            slot(a, SL_TT)[tile] = q;
+            slot(a, SL_B)[tile] = bb;
+        }
+    }
+}
+
+// Inner right-hand side r32 = fl32(t / |t|), p32 = r32, d32 = 0; <r32, r32> -> G0.
+template <class Op>
+__device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0;
+        if (i < a.n) {
+            const float ri = __double2float_rn(__dmul_rn(a.t[i], scale));
+            a.r32[i] = ri;
+            a.p32[i] = ri;
+            a.d32[i] = 0.f;
+            g = xprod(ri, ri);
+        }
+        g = block_sum(g, sm);
+        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+    }
+}
+
+template <class Op>
+__device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double d = 0.0;
+        if (i < a.n) {
+            const float si = a.op.apply32(a.p32, i);
+            a.s32[i] = si;
+            d = xprod(a.p32[i], si);
+        }
+        d = block_sum(d, sm);
+        if (threadIdx.x == 0) slot(a, SL_D0)[tile] = d;
+    }
+}
+
+template <class Op>
+__device__ void phase_inner_update(const KArgs<Op> &a, float af, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0;
+        if (i < a.n) {
+            a.d32[i] = __fmaf_rn(af, a.p32[i], a.d32[i]);
+            const float ri = __fmaf_rn(-af, a.s32[i], a.r32[i]);
+            a.r32[i] = ri;
+            g = xprod(ri, ri);
+        }
+        g = block_sum(g, sm);
+        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+    }
+}
+
+template <class Op>
+__device__ void phase_inner_p(const KArgs<Op> &a, float bf) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) a.p32[i] = __fmaf_rn(bf, a.p32[i], a.r32[i]);
+    }
+}
+
+// x += |t| d32 (FP64 correction)
+template <class Op>
+__device__ void phase_correct(const KArgs<Op> &a, double norm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) a.x[i] = __fma_rn(norm, (double)a.d32[i], a.x[i]);
+    }
+}
+
+// FP64 iterative refinement around FP32 CG.  Each sweep solves A d = t / |t|
+// in FP32 (FP32 SpMV and axpys with FP32 accumulation; the dots are FP64 sums
+// of the exact FP32 products; alpha, beta in FP64, applied rounded to FP32)
+// until |r_inner| <= inner_tol |r_inner,0| or inner_maxiter steps, then
+// x += |t| d in FP64 and t = b - A x in FP64.  Stops when |t| <= tol |b|;
+// maxiter caps the inner steps over all sweeps.
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
+    __shared__ double sm[33];
+    int site = 0;
+    phase_mixed_init(a, sm);
+    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+    const double bnorm = sqrt(sum_partials(slot(a, SL_B), a.ntiles, sm));
+    const double target = a.tol * bnorm;
+    int status = CFM_NOT_CONVERGED, sweeps = 0;
+    long long k = 0;
+    double tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+    while (true) {
+        const double tnorm = sqrt(tt);
+        if (tnorm <= target) {
+            status = CFM_OK;
+            break;
+        }
+        if (k >= a.maxiter || sweeps >= 1000) break;
+        phase_inner_start(a, 1.0 / tnorm, sm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        double g0 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+        const double stop = a.inner_tol * sqrt(g0);
+        int j = 0;
+        bool broke = false;
+        while (true) {
+            phase_inner_spmv(a, sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            const double delta = sum_partials(slot(a, SL_D0), a.ntiles, sm);
+            const double alpha = g0 / delta;
+            if (!(delta > 0.0 && isfinite(alpha))) {
+                broke = true;
+                break;
+            }
+            phase_inner_update(a, __double2float_rn(alpha), sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            const double g1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+            ++j;
+            ++k;
+            if (sqrt(g1) <= stop || j >= a.inner_maxiter || k >= a.maxiter) break;
+            const double beta = g1 / g0;
+            phase_inner_p(a, __double2float_rn(beta));
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            g0 = g1;
+        }
+        if (broke && j == 0) {
+            status = CFM_BREAKDOWN;
+            break;
+        }
+        phase_correct(a, tnorm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        ++sweeps;
+        phase_true_residual(a, sm);
+        if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+        tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+    }
+    write_result(a.res, k, status, sweeps, tt, bnorm);
+}
+
+// ------------------------------------------------ host-controlled pieces
+// One kernel per operation (the comparator of CG/src/common.cu:458-531).
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_init(KArgs<Op> a) {
+    __shared__ double sm[33];
+    phase_init(a, sm);
+}
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_spmv_dot(KArgs<Op> a) {
+    __shared__ double sm[33];
+    phase_spmv_dot(a, sm);
+}
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_update(KArgs<Op> a, double alpha) {
+    __shared__ double sm[33];
+    phase_update(a, alpha, sm);
+}
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_true_residual(KArgs<Op> a) {
+    __shared__ double sm[33];
+    phase_true_residual(a, sm);
+}
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_restart(KArgs<Op> a) {
+    phase_restart(a);
+}
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_p(KArgs<Op> a, double beta) {
+    phase_p(a, beta);
+}
+// Single block: reduce partial slot `which` into out[which].
+template <class Op>
+__global__ void __launch_bounds__(CG_TILE) k_reduce(KArgs<Op> a, int which, double *out) {
+    __shared__ double sm[33];
+    const double v = sum_partials(slot(a, which), a.ntiles, sm);
+    if (threadIdx.x == 0) out[which] = v;
+}
+
+// y = A x, one row per thread.
+template <class Op>
+__global__ void k_apply(Op op, int n, const double *x, double *y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = op.apply(x, i);
+}
+
+#undef CFM_TILES
+#undef CFM_ROW
+
+}  // namespace cfm

@@ -160,9 +160,11 @@ typedef enum cfm_cg_impl {
     /* "Single Stream Standard": whole CG in one persistent kernel
      * (CG/src/single-stream/standard.cu:158-299) */
     CFM_CG_PERSISTENT = 1,
-    /* "Single Stream Pipelined" (CG/src/single-stream/pipelined.cu:176-330) */
+    /* "Single Stream Pipelined" (CG/src/single-stream/pipelined.cu:176-330):
+     * one persistent kernel, one fused pass and one grid barrier per iteration */
     CFM_CG_PERSISTENT_PIPELINED = 2,
-    /* FP32 inner persistent CG inside an FP64 iterative-refinement loop */
+    /* FP32 inner persistent CG inside an FP64 iterative-refinement loop, one
+     * persistent kernel (no reference counterpart; needs tol > 0) */
     CFM_CG_MIXED = 3
 } cfm_cg_impl;
 
@@ -176,17 +178,31 @@ void cfm_csr_destroy(cfm_csr *A);
 /* y = A x with host vectors (FP64, deterministic row order). */
 int cfm_csr_spmv_host(const cfm_csr *A, const double *x, double *y);
 
+/* Matrix-free variable-coefficient operator -div(k grad u) on a 2D (5-point)
+ * or 3D (7-point) grid of unit cells, u = 0 on the boundary; face
+ * coefficients are harmonic means 2 k_i k_j / (k_i + k_j), boundary faces
+ * 2 k_i (cfm_varcoef_coeffs).  Rows are cells, x fastest.  No reference
+ * counterpart (the reference's CG takes CSR only, CG/src/main.cu:118-135). */
+typedef struct cfm_stencil cfm_stencil;
+int cfm_stencil_create(int dims, int nx, int ny, int nz, const double *k_host, cfm_stencil **out);
+void cfm_stencil_destroy(cfm_stencil *S);
+/* y = A x with host vectors. */
+int cfm_stencil_apply_host(const cfm_stencil *S, const double *x, double *y);
+
 typedef struct cfm_cg_params {
     int impl;          /* cfm_cg_impl */
-    int maxiter;       /* iteration cap; with tol <= 0 exactly maxiter iterations run */
+    int maxiter;       /* iteration cap (CFM_CG_MIXED: inner iterations over all sweeps);
+                          with tol <= 0 exactly maxiter iterations run */
     double tol;        /* relative residual target ||r||/||b||; <= 0 = fixed count (reference -niter) */
-    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = default 200) */
+    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = default 1000) */
     double inner_tol;  /* CFM_CG_MIXED: relative reduction per sweep (0 = default 1e-4) */
 } cfm_cg_params;
 
 typedef struct cfm_cg cfm_cg;
 
 int cfm_cg_create(const cfm_csr *A, const cfm_cg_params *p, cfm_cg **out);
+/* CG handle over a matrix-free stencil operator (same solvers as CSR). */
+int cfm_cg_create_stencil(const cfm_stencil *S, const cfm_cg_params *p, cfm_cg **out);
 void cfm_cg_destroy(cfm_cg *h);
 int cfm_cg_set_stream(cfm_cg *h, void *cuda_stream);
 /* Solve A x = b from x0 = 0 with host vectors; b == NULL means b = ones, the
@@ -235,6 +251,24 @@ int cfm_poisson3d_csr(int gx, int gy, int gz, int *rowptr, int *col, double *val
 int cfm_tridiag_csr(int n, int *rowptr, int *col, double *val);
 /* n doubles uniform in [lo, hi) from a Philox-4x32-10 stream keyed by seed. */
 int cfm_uniform(unsigned long long seed, long long n, double lo, double hi, double *out);
+
+/* n doubles ~ N(0, 1): Box-Muller on Philox-4x32-10 words, counter
+ * (i / 2, stream), key seed. */
+int cfm_normal(unsigned long long seed, unsigned int stream, long long n, double *out);
+/* Gaussian random field on an nx*ny(*nz) grid: Philox white noise convolved
+ * (periodic wrap) with a separable Gaussian kernel, unit variance before the
+ * sigma scale, covariance exp(-r^2 / (2 corr_len^2)). */
+int cfm_grf(int dims, int nx, int ny, int nz, unsigned long long seed, double sigma,
+            double corr_len, double *g);
+/* Variable-coefficient diffusion problem: k = exp(grf(sigma 1, corr_len 16)),
+ * f ~ N(0, 1) per cell (stream 1). */
+int cfm_varcoef_problem(int dims, int nx, int ny, int nz, unsigned long long seed, double *k,
+                        double *f);
+/* Face coefficients of cfm_stencil from k: w_e/w_n/w_t = faces to x+1/y+1/z+1
+ * (0 on the last column/row/plane), diag = sum of the cell's face weights
+ * (boundary faces 2 k_i) in the order x-, x+, y-, y+, z-, z+.  w_t unused in 2D. */
+int cfm_varcoef_coeffs(int dims, int nx, int ny, int nz, const double *k, double *w_e,
+                       double *w_n, double *w_t, double *diag);
 
 /* One Philox-4x32-10 block (counter, key) -> 4 words; the generator behind
  * cfm_uniform, exported for its known-answer test. */

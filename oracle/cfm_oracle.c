@@ -373,3 +373,396 @@ int orc_cg(int n, const int *rowptr, const int *col, const double *val, const do
     free(bb); free(r); free(p); free(s); free(t);
     return status;
 }
+
+/* ------------------------------------------------ operator-generic Krylov */
+
+/* Operator: CSR (kind 0, index base from rowptr[0]) or the matrix-free
+ * variable-coefficient stencil (kind 2 / 3) whose row i gives
+ *   t = dg[i] x[i]; then t = fma(-w, x_nb, t) for x-1, x+1, y-1, y+1, z-1, z+1
+ * with w = we[i-1], we[i], wn[i-nx], wn[i], wt[i-P], wt[i] (neighbours that
+ * exist only).  FP32 copies (fp32 = 1) apply the same in float with fmaf. */
+typedef struct {
+    int kind, n;
+    const int *rowptr, *col;
+    const double *val;
+    int nx, ny, nz;
+    const double *we, *wn, *wt, *dg;
+    float *val32, *we32, *wn32, *wt32, *dg32;
+} orc_op;
+
+static void op_apply(const orc_op *A, const double *x, double *y, int nt) {
+    const int n = A->n;
+    if (A->kind == 0) {
+        orc_spmv(n, A->rowptr, A->col, A->val, x, y, nt);
+        return;
+    }
+    const int nx = A->nx, ny = A->ny, nz = A->nz, P = nx * ny;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const int ix = i % nx, q = i / nx, iy = q % ny, iz = q / ny;
+        double t = A->dg[i] * x[i];
+        if (ix > 0) t = fma(-A->we[i - 1], x[i - 1], t);
+        if (ix < nx - 1) t = fma(-A->we[i], x[i + 1], t);
+        if (iy > 0) t = fma(-A->wn[i - nx], x[i - nx], t);
+        if (iy < ny - 1) t = fma(-A->wn[i], x[i + nx], t);
+        if (A->kind == 3) {
+            if (iz > 0) t = fma(-A->wt[i - P], x[i - P], t);
+            if (iz < nz - 1) t = fma(-A->wt[i], x[i + P], t);
+        }
+        y[i] = t;
+    }
+}
+
+static void op_apply32(const orc_op *A, const float *x, float *y, int nt) {
+    const int n = A->n;
+    if (A->kind == 0) {
+        const int base = A->rowptr[0];
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int i = 0; i < n; ++i) {
+            float acc = 0.f;
+            for (int j = A->rowptr[i] - base; j < A->rowptr[i + 1] - base; ++j)
+                acc = fmaf(A->val32[j], x[A->col[j] - base], acc);
+            y[i] = acc;
+        }
+        return;
+    }
+    const int nx = A->nx, ny = A->ny, nz = A->nz, P = nx * ny;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const int ix = i % nx, q = i / nx, iy = q % ny, iz = q / ny;
+        float t = A->dg32[i] * x[i];
+        if (ix > 0) t = fmaf(-A->we32[i - 1], x[i - 1], t);
+        if (ix < nx - 1) t = fmaf(-A->we32[i], x[i + 1], t);
+        if (iy > 0) t = fmaf(-A->wn32[i - nx], x[i - nx], t);
+        if (iy < ny - 1) t = fmaf(-A->wn32[i], x[i + nx], t);
+        if (A->kind == 3) {
+            if (iz > 0) t = fmaf(-A->wt32[i - P], x[i - P], t);
+            if (iz < nz - 1) t = fmaf(-A->wt32[i], x[i + P], t);
+        }
+        y[i] = t;
+    }
+}
+
+/* Tree sum (tiles, then partials) of n precomputed products. */
+static double tree_sum(long long n, const double *prod, int nt) {
+    long long ntiles = (n + ORC_TILE - 1) / ORC_TILE;
+    double *part = (double *)malloc(sizeof(double) * (ntiles > 0 ? ntiles : 1));
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (long long t = 0; t < ntiles; ++t) {
+        double pr[ORC_TILE];
+        for (int l = 0; l < ORC_TILE; ++l) {
+            long long i = t * ORC_TILE + l;
+            pr[l] = i < n ? prod[i] : 0.0;
+        }
+        part[t] = tile_sum(pr);
+    }
+    double s = partials_sum(part, ntiles);
+    free(part);
+    return s;
+}
+
+/* <a, b> of FP32 vectors: FP64 sums of the exact FP32 products. */
+static double dot32(int n, const float *a, const float *b, double *scr, int nt) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int i = 0; i < n; ++i) scr[i] = (double)a[i] * (double)b[i];
+    return tree_sum(n, scr, nt);
+}
+
+/* t = b - A x; returns <t, t>. */
+static double true_res(const orc_op *A, const double *b, const double *x, double *t, double *s,
+                       int nt) {
+    op_apply(A, x, s, nt);
+    for (int i = 0; i < A->n; ++i) t[i] = b[i] - s[i];
+    return orc_dot(A->n, t, t, nt);
+}
+
+/* Standard CG: the arithmetic of cg_std_kernel (csrc/krylov.cuh). */
+static int krylov_std(const orc_op *A, const double *b, int maxiter, double tol, double *x,
+                      long long *iters, int *restarts_out, int nt) {
+    const int n = A->n;
+    double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
+    double *s = malloc(sizeof(double) * n), *t = malloc(sizeof(double) * n);
+    for (int i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        r[i] = fma(-1.0, 0.0, b[i]);
+        p[i] = r[i];
+    }
+    double gamma0 = orc_dot(n, r, r, nt);
+    const double bnorm = sqrt(orc_dot(n, b, b, nt));
+    const int use_tol = tol > 0;
+    const double target = tol * bnorm;
+    int status = use_tol ? 5 : 0, restarts = 0;
+    long long k = 0;
+    if (use_tol && sqrt(gamma0) <= target) status = 0;
+    while (k < maxiter && !(use_tol && status == 0)) {
+        op_apply(A, p, s, nt);
+        const double delta = orc_dot(n, p, s, nt);
+        const double alpha = gamma0 / delta;
+        if (use_tol && !(delta > 0.0 && isfinite(alpha))) { status = 4; break; }
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int i = 0; i < n; ++i) {
+            x[i] = fma(alpha, p[i], x[i]);
+            r[i] = fma(-alpha, s[i], r[i]);
+        }
+        const double gamma1 = orc_dot(n, r, r, nt);
+        ++k;
+        if (use_tol && sqrt(gamma1) <= target) {
+            const double tt = true_res(A, b, x, t, s, nt);
+            if (sqrt(tt) <= target) { status = 0; break; }
+            memcpy(r, t, sizeof(double) * n);
+            memcpy(p, t, sizeof(double) * n);
+            ++restarts;
+            gamma0 = tt;
+            continue;
+        }
+        const double beta = gamma1 / gamma0;
+        if (use_tol && !isfinite(beta)) { status = 4; break; }
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int i = 0; i < n; ++i) p[i] = fma(beta, p[i], r[i]);
+        gamma0 = gamma1;
+    }
+    *iters = k;
+    *restarts_out = restarts;
+    free(r); free(p); free(s); free(t);
+    return status;
+}
+
+/* Pipelined CG: the arithmetic of cg_pipe_kernel (csrc/krylov.cuh), whose
+ * scalar recurrence is the reference's (CG/src/single-stream/pipelined.cu:262-272). */
+static int krylov_pipe(const orc_op *A, const double *b, int maxiter, double tol, double *x,
+                       long long *iters, int *restarts_out, int nt) {
+    const int n = A->n;
+    double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
+    double *s = malloc(sizeof(double) * n), *t = malloc(sizeof(double) * n);
+    double *z = malloc(sizeof(double) * n), *w = malloc(sizeof(double) * n);
+    double *wn = malloc(sizeof(double) * n), *q = malloc(sizeof(double) * n);
+    double *scr = malloc(sizeof(double) * n);
+    for (int i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        t[i] = fma(-1.0, 0.0, b[i]);
+    }
+    const double bnorm = sqrt(orc_dot(n, b, b, nt));
+    double rr, wr;
+#define ORC_PIPE_START()                                                   \
+    do {                                                                   \
+        memcpy(r, t, sizeof(double) * n);                                  \
+        op_apply(A, t, w, nt);                                             \
+        memset(z, 0, sizeof(double) * n);                                  \
+        memset(s, 0, sizeof(double) * n);                                  \
+        memset(p, 0, sizeof(double) * n);                                  \
+        rr = orc_dot(n, r, r, nt);                                         \
+        for (int i_ = 0; i_ < n; ++i_) scr[i_] = w[i_] * r[i_];            \
+        wr = tree_sum(n, scr, nt);                                         \
+    } while (0)
+    ORC_PIPE_START();
+    const int use_tol = tol > 0;
+    const double target = tol * bnorm;
+    int status = use_tol ? 5 : 0, restarts = 0;
+    long long k = 0, kk = 0;
+    double rr_prev = 0.0, alpha = 0.0;
+    for (;;) {
+        if (use_tol && sqrt(rr) <= target) {
+            const double tt = true_res(A, b, x, t, q, nt);
+            if (sqrt(tt) <= target) { status = 0; break; }
+            ORC_PIPE_START();
+            ++restarts;
+            kk = 0;
+            continue;
+        }
+        if (k >= maxiter) break;
+        double beta;
+        if (kk > 1) {
+            beta = rr / rr_prev;
+            const double c = (beta / alpha) * rr;
+            alpha = rr / (wr - c);
+        } else {
+            beta = 0.0;
+            alpha = rr / wr;
+        }
+        if (use_tol && !(isfinite(alpha) && alpha > 0.0 && isfinite(beta))) { status = 4; break; }
+        op_apply(A, w, q, nt);
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int i = 0; i < n; ++i) {
+            const double zi = fma(beta, z[i], q[i]);
+            const double si = fma(beta, s[i], w[i]);
+            const double pi = fma(beta, p[i], r[i]);
+            x[i] = fma(alpha, pi, x[i]);
+            r[i] = fma(-alpha, si, r[i]);
+            wn[i] = fma(-alpha, zi, w[i]);
+            z[i] = zi;
+            s[i] = si;
+            p[i] = pi;
+        }
+        rr_prev = rr;
+        rr = orc_dot(n, r, r, nt);
+        for (int i = 0; i < n; ++i) scr[i] = wn[i] * r[i];
+        wr = tree_sum(n, scr, nt);
+        double *tmp = w; w = wn; wn = tmp;
+        ++k;
+        ++kk;
+    }
+#undef ORC_PIPE_START
+    *iters = k;
+    *restarts_out = restarts;
+    free(r); free(p); free(s); free(t); free(z); free(w); free(wn); free(q); free(scr);
+    return status;
+}
+
+/* FP64 refinement around FP32 CG: the arithmetic of cg_mixed_kernel
+ * (csrc/krylov.cuh). */
+static int krylov_mixed(const orc_op *A, const double *b, int maxiter, double tol,
+                        int inner_maxiter, double inner_tol, double *x, long long *iters,
+                        int *sweeps_out, int nt) {
+    const int n = A->n;
+    double *t = malloc(sizeof(double) * n), *s = malloc(sizeof(double) * n);
+    double *scr = malloc(sizeof(double) * n);
+    float *r32 = malloc(sizeof(float) * n), *p32 = malloc(sizeof(float) * n);
+    float *s32 = malloc(sizeof(float) * n), *d32 = malloc(sizeof(float) * n);
+    for (int i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        t[i] = fma(-1.0, 0.0, b[i]);
+    }
+    double tt = orc_dot(n, t, t, nt);
+    const double bnorm = sqrt(orc_dot(n, b, b, nt));
+    const double target = tol * bnorm;
+    int status = 5, sweeps = 0;
+    long long k = 0;
+    for (;;) {
+        const double tnorm = sqrt(tt);
+        if (tnorm <= target) { status = 0; break; }
+        if (k >= maxiter || sweeps >= 1000) break;
+        const double scale = 1.0 / tnorm;
+        for (int i = 0; i < n; ++i) {
+            r32[i] = (float)(t[i] * scale);
+            p32[i] = r32[i];
+            d32[i] = 0.f;
+        }
+        double g0 = dot32(n, r32, r32, scr, nt);
+        const double stop = inner_tol * sqrt(g0);
+        int j = 0, broke = 0;
+        for (;;) {
+            op_apply32(A, p32, s32, nt);
+            const double delta = dot32(n, p32, s32, scr, nt);
+            const double alpha = g0 / delta;
+            if (!(delta > 0.0 && isfinite(alpha))) { broke = 1; break; }
+            const float af = (float)alpha;
+#pragma omp parallel for num_threads(nt) schedule(static)
+            for (int i = 0; i < n; ++i) {
+                d32[i] = fmaf(af, p32[i], d32[i]);
+                r32[i] = fmaf(-af, s32[i], r32[i]);
+            }
+            const double g1 = dot32(n, r32, r32, scr, nt);
+            ++j;
+            ++k;
+            if (sqrt(g1) <= stop || j >= inner_maxiter || k >= maxiter) break;
+            const float bf = (float)(g1 / g0);
+#pragma omp parallel for num_threads(nt) schedule(static)
+            for (int i = 0; i < n; ++i) p32[i] = fmaf(bf, p32[i], r32[i]);
+            g0 = g1;
+        }
+        if (broke && j == 0) { status = 4; break; }
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int i = 0; i < n; ++i) x[i] = fma(tnorm, (double)d32[i], x[i]);
+        ++sweeps;
+        tt = true_res(A, b, x, t, s, nt);
+    }
+    *iters = k;
+    *sweeps_out = sweeps;
+    free(t); free(s); free(scr); free(r32); free(p32); free(s32); free(d32);
+    return status;
+}
+
+static int krylov_run(orc_op *A, int method, const double *b_in, int maxiter, double tol,
+                      int inner_maxiter, double inner_tol, double *x, long long *iters,
+                      int *restarts, double *relres, int threads) {
+    const int nt = nthreads(threads), n = A->n;
+    double *b = malloc(sizeof(double) * n), *t = malloc(sizeof(double) * n);
+    double *s = malloc(sizeof(double) * n);
+    for (int i = 0; i < n; ++i) b[i] = b_in ? b_in[i] : 1.0;
+    long long k = 0;
+    int rs = 0, status;
+    if (method == 1) {
+        status = krylov_pipe(A, b, maxiter, tol, x, &k, &rs, nt);
+    } else if (method == 2) {
+        status = krylov_mixed(A, b, maxiter, tol, inner_maxiter > 0 ? inner_maxiter : 1000,
+                              inner_tol > 0 ? inner_tol : 1e-4, x, &k, &rs, nt);
+    } else {
+        status = krylov_std(A, b, maxiter, tol, x, &k, &rs, nt);
+    }
+    const double bnorm = sqrt(orc_dot(n, b, b, nt));
+    const double tt = true_res(A, b, x, t, s, nt);
+    if (iters) *iters = k;
+    if (restarts) *restarts = rs;
+    if (relres) *relres = bnorm > 0 ? sqrt(tt) / bnorm : sqrt(tt);
+    free(b); free(t); free(s);
+    return status;
+}
+
+static float *to_f32(const double *a, size_t n) {
+    float *o = malloc(sizeof(float) * (n ? n : 1));
+    for (size_t i = 0; i < n; ++i) o[i] = (float)a[i];
+    return o;
+}
+
+int orc_krylov_csr(int n, const int *rowptr, const int *col, const double *val, int method,
+                   const double *b, int maxiter, double tol, int inner_maxiter, double inner_tol,
+                   double *x, long long *iters, int *restarts, double *relres, int threads) {
+    if (n <= 0 || !rowptr || !col || !val || !x || maxiter < 0 || method < 0 || method > 2) return 1;
+    orc_op A;
+    memset(&A, 0, sizeof(A));
+    A.kind = 0;
+    A.n = n;
+    A.rowptr = rowptr;
+    A.col = col;
+    A.val = val;
+    const long long nnz = rowptr[n] - rowptr[0];
+    A.val32 = to_f32(val, (size_t)nnz);
+    const int st = krylov_run(&A, method, b, maxiter, tol, inner_maxiter, inner_tol, x, iters,
+                              restarts, relres, threads);
+    free(A.val32);
+    return st;
+}
+
+static void stencil_op(orc_op *A, int dims, int nx, int ny, int nz, const double *we,
+                       const double *wn, const double *wt, const double *dg) {
+    memset(A, 0, sizeof(*A));
+    A->kind = dims;
+    A->nx = nx;
+    A->ny = ny;
+    A->nz = dims == 3 ? nz : 1;
+    A->n = nx * ny * A->nz;
+    A->we = we;
+    A->wn = wn;
+    A->wt = wt;
+    A->dg = dg;
+}
+
+int orc_stencil_apply(int dims, int nx, int ny, int nz, const double *we, const double *wn,
+                      const double *wt, const double *dg, const double *x, double *y,
+                      int threads) {
+    if ((dims != 2 && dims != 3) || nx < 1 || ny < 1 || !x || !y) return 1;
+    orc_op A;
+    stencil_op(&A, dims, nx, ny, nz, we, wn, wt, dg);
+    op_apply(&A, x, y, nthreads(threads));
+    return 0;
+}
+
+int orc_krylov_stencil(int dims, int nx, int ny, int nz, const double *we, const double *wn,
+                       const double *wt, const double *dg, int method, const double *b,
+                       int maxiter, double tol, int inner_maxiter, double inner_tol, double *x,
+                       long long *iters, int *restarts, double *relres, int threads) {
+    if ((dims != 2 && dims != 3) || nx < 1 || ny < 1 || !x || maxiter < 0 || method < 0 ||
+        method > 2)
+        return 1;
+    orc_op A;
+    stencil_op(&A, dims, nx, ny, nz, we, wn, wt, dg);
+    const size_t n = (size_t)A.n;
+    A.we32 = to_f32(we, n);
+    A.wn32 = to_f32(wn, n);
+    A.wt32 = dims == 3 ? to_f32(wt, n) : NULL;
+    A.dg32 = to_f32(dg, n);
+    const int st = krylov_run(&A, method, b, maxiter, tol, inner_maxiter, inner_tol, x, iters,
+                              restarts, relres, threads);
+    free(A.we32); free(A.wn32); free(A.wt32); free(A.dg32);
+    return st;
+}

@@ -62,6 +62,23 @@ int orc_cg(int n, const int *rowptr, const int *col, const double *val, const do
 int orc_spmv(int n, const int *rowptr, const int *col, const double *val, const double *x,
              double *y, int threads);
 
+/* Operator-generic persistent-solver restatements (csrc/krylov.cuh):
+ * method 0 standard CG, 1 pipelined CG, 2 FP64 refinement around FP32 CG
+ * (inner_maxiter 0 -> 1000, inner_tol 0 -> 1e-4).  b == NULL -> ones, x0 = 0.
+ * Returns 0 / 4 breakdown / 5 not converged; iters, restarts (refinement
+ * sweeps for method 2), relres (true FP64 relative residual) optional. */
+int orc_krylov_csr(int n, const int *rowptr, const int *col, const double *val, int method,
+                   const double *b, int maxiter, double tol, int inner_maxiter, double inner_tol,
+                   double *x, long long *iters, int *restarts, double *relres, int threads);
+/* Variable-coefficient stencil (coefficients as cfm_varcoef_coeffs gives them). */
+int orc_stencil_apply(int dims, int nx, int ny, int nz, const double *we, const double *wn,
+                      const double *wt, const double *dg, const double *x, double *y,
+                      int threads);
+int orc_krylov_stencil(int dims, int nx, int ny, int nz, const double *we, const double *wn,
+                       const double *wt, const double *dg, int method, const double *b,
+                       int maxiter, double tol, int inner_maxiter, double inner_tol, double *x,
+                       long long *iters, int *restarts, double *relres, int threads);
+
 int orc_max_threads(void);
 
 #ifdef __cplusplus

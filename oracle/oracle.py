@@ -37,6 +37,11 @@ def _load():
         "orc_cg": [_i, _vp, _vp, _vp, _vp, _i, ctypes.c_double, _vp, _vp, _vp, _i],
         "orc_spmv": [_i, _vp, _vp, _vp, _vp, _vp, _i],
         "orc_max_threads": [],
+        "orc_krylov_csr": [_i, _vp, _vp, _vp, _i, _vp, _i, ctypes.c_double, _i, ctypes.c_double,
+                           _vp, _vp, _vp, _vp, _i],
+        "orc_stencil_apply": [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i],
+        "orc_krylov_stencil": [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _i, ctypes.c_double, _i,
+                               ctypes.c_double, _vp, _vp, _vp, _vp, _i],
     }
     for name, args in sigs.items():
         fn = getattr(lib, name)
@@ -135,6 +140,55 @@ def cg(rowptr, col, val, b, maxiter, tol, threads=0):
     st = lib.orc_cg(n, _p(rowptr), _p(col), _p(val), None if bb is None else _p(bb), maxiter, tol,
                     _p(x), ctypes.byref(it), ctypes.byref(rr), threads)
     return x, st, it.value, rr.value
+
+
+STD, PIPELINED, MIXED = 0, 1, 2
+
+
+def krylov_csr(rowptr, col, val, b, method, maxiter, tol, inner_maxiter=0, inner_tol=0.0, threads=0):
+    """Persistent-solver restatement on a CSR matrix.
+    Returns (x, status, iterations, restarts_or_sweeps, true relative residual)."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    n = len(rowptr) - 1
+    x = np.empty(n)
+    it, rs, rr = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_double()
+    bb = None if b is None else np.ascontiguousarray(b, np.float64)
+    st = lib.orc_krylov_csr(n, _p(rowptr), _p(col), _p(val), method, None if bb is None else _p(bb),
+                            maxiter, tol, inner_maxiter, inner_tol, _p(x), ctypes.byref(it),
+                            ctypes.byref(rs), ctypes.byref(rr), threads)
+    return x, st, it.value, rs.value, rr.value
+
+
+def _coeffs(c):
+    """c = (we, wn, wt, dg) as cfm.varcoef_coeffs returns them."""
+    we, wn, wt, dg = (np.ascontiguousarray(a, np.float64) for a in c)
+    return we, wn, wt, dg
+
+
+def stencil_apply(dims, shape, c, x, threads=0):
+    we, wn, wt, dg = _coeffs(c)
+    nx, ny, nz = shape
+    x = np.ascontiguousarray(x, np.float64).reshape(-1)
+    y = np.empty_like(x)
+    assert lib.orc_stencil_apply(dims, nx, ny, nz, _p(we), _p(wn), _p(wt), _p(dg), _p(x), _p(y),
+                                 threads) == 0
+    return y
+
+
+def krylov_stencil(dims, shape, c, b, method, maxiter, tol, inner_maxiter=0, inner_tol=0.0,
+                   threads=0):
+    we, wn, wt, dg = _coeffs(c)
+    nx, ny, nz = shape
+    x = np.empty(len(dg))
+    it, rs, rr = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_double()
+    bb = None if b is None else np.ascontiguousarray(b, np.float64).reshape(-1)
+    st = lib.orc_krylov_stencil(dims, nx, ny, nz, _p(we), _p(wn), _p(wt), _p(dg), method,
+                                None if bb is None else _p(bb), maxiter, tol, inner_maxiter,
+                                inner_tol, _p(x), ctypes.byref(it), ctypes.byref(rs),
+                                ctypes.byref(rr), threads)
+    return x, st, it.value, rs.value, rr.value
 
 
 # ------------------------------------------------------ the reference itself
