@@ -118,8 +118,8 @@ KArgs<Op> make_args(cfm_cg *h, const Op &op, const double *b_dev, double *x_dev)
     a.bar = h->bar;
     a.maxiter = h->p.maxiter;
     a.tol = h->p.tol;
-    a.inner_maxiter = h->p.inner_maxiter > 0 ? h->p.inner_maxiter : 1000;
-    a.inner_tol = h->p.inner_tol > 0 ? h->p.inner_tol : 1e-4;
+    a.inner_maxiter = h->p.inner_maxiter;  // 0: no cap per sweep
+    a.inner_tol = h->p.inner_tol > 0 ? h->p.inner_tol : 1e-3;
     return a;
 }
 

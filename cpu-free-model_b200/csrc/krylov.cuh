@@ -404,11 +404,56 @@ __device__ void phase_pipe_step(const KArgs<Op> &a, const double *w, double *wn,
     }
 }
 
+// Residual replacement, first half: t = b - A x, s = A p.
+template <class Op>
+__device__ void phase_replace_a(const KArgs<Op> &a) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            a.t[i] = __dsub_rn(bi, a.op.apply(a.x, i));
+            a.s[i] = a.op.apply(a.p, i);
+        }
+    }
+}
+
+// Residual replacement, second half: r = t, w = A t, z = A s and the
+// partials <r, r> -> G[par], <w, r> -> D[par].
+template <class Op>
+__device__ void phase_replace_b(const KArgs<Op> &a, double *w, int par, double *sm) {
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double g = 0.0, d = 0.0;
+        if (i < a.n) {
+            const double ri = a.t[i];
+            const double wi = a.op.apply(a.t, i);
+            a.r[i] = ri;
+            w[i] = wi;
+            a.z[i] = a.op.apply(a.s, i);
+            g = __dmul_rn(ri, ri);
+            d = __dmul_rn(wi, ri);
+        }
+        g = block_sum(g, sm);
+        d = block_sum(d, sm);
+        if (threadIdx.x == 0) {
+            slot(a, par ? SL_G1 : SL_G0)[tile] = g;
+            slot(a, par ? SL_D1 : SL_D0)[tile] = d;
+        }
+    }
+}
+
+// Iterations between residual replacements in pipelined CG.
+constexpr long long PIPE_REPLACE = 50;
+
 // Pipelined CG.  Scalars follow the reference's recurrence
 // (CG/src/single-stream/pipelined.cu:262-272): with rr = <r, r>, wr = <w, r>,
 //   beta = rr / rr_prev, alpha = rr / (wr - (beta / alpha_prev) rr)
 // from the third step of a run on, and beta = 0, alpha = rr / wr on the
 // first two (the reference tests `k > 1`).  Convergence as cg_std_kernel.
+// The pipelined recurrences let the recursive residual drift from b - A x on
+// ill-conditioned systems, so with tol > 0 every PIPE_REPLACE iterations the
+// vectors r, w, s, z are recomputed from x and p (residual replacement: two
+// extra barriers, four operator applications); the scalar recurrence goes on.
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
     __shared__ double sm[33];
@@ -422,7 +467,7 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
     const double target = a.tol * bnorm;
     int status = use_tol ? CFM_NOT_CONVERGED : CFM_OK;
     int restarts = 0, cur = 0;
-    long long k = 0, kk = 0;
+    long long k = 0, kk = 0, replaced = -1;
     double rr = 0.0, rr_prev = 0.0, alpha = 0.0;
     while (true) {
         double *w = cur ? a.w1 : a.w0;
@@ -440,9 +485,19 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
             if (!grid_barrier(a.bar, gridDim.x, site++)) return;
             ++restarts;
             kk = 0;
+            replaced = k;  // a restart needs no replacement at this count
             continue;
         }
         if (k >= a.maxiter) break;
+        if (use_tol && k > 0 && k % PIPE_REPLACE == 0 && replaced != k) {
+            phase_replace_a(a);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            phase_replace_b(a, w, cur, sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            replaced = k;
+            ++restarts;
+            continue;
+        }
         double beta;
         if (kk > 1) {
             beta = rr / rr_prev;
@@ -599,7 +654,9 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
             const double g1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
             ++j;
             ++k;
-            if (sqrt(g1) <= stop || j >= a.inner_maxiter || k >= a.maxiter) break;
+            if (sqrt(g1) <= stop || (a.inner_maxiter > 0 && j >= a.inner_maxiter) ||
+                k >= a.maxiter)
+                break;
             const double beta = g1 / g0;
             phase_inner_p(a, __double2float_rn(beta));
             if (!grid_barrier(a.bar, gridDim.x, site++)) return;

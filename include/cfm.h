@@ -194,8 +194,8 @@ typedef struct cfm_cg_params {
     int maxiter;       /* iteration cap (CFM_CG_MIXED: inner iterations over all sweeps);
                           with tol <= 0 exactly maxiter iterations run */
     double tol;        /* relative residual target ||r||/||b||; <= 0 = fixed count (reference -niter) */
-    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = default 1000) */
-    double inner_tol;  /* CFM_CG_MIXED: relative reduction per sweep (0 = default 1e-4) */
+    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = no cap) */
+    double inner_tol;  /* CFM_CG_MIXED: relative reduction per sweep (0 = default 1e-3) */
 } cfm_cg_params;
 
 typedef struct cfm_cg cfm_cg;

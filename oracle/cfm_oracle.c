@@ -527,6 +527,9 @@ static int krylov_std(const orc_op *A, const double *b, int maxiter, double tol,
     return status;
 }
 
+/* Iterations between residual replacements (PIPE_REPLACE in csrc/krylov.cuh). */
+#define ORC_PIPE_REPLACE 50
+
 /* Pipelined CG: the arithmetic of cg_pipe_kernel (csrc/krylov.cuh), whose
  * scalar recurrence is the reference's (CG/src/single-stream/pipelined.cu:262-272). */
 static int krylov_pipe(const orc_op *A, const double *b, int maxiter, double tol, double *x,
@@ -600,6 +603,18 @@ static int krylov_pipe(const orc_op *A, const double *b, int maxiter, double tol
         double *tmp = w; w = wn; wn = tmp;
         ++k;
         ++kk;
+        if (use_tol && k < maxiter && k % ORC_PIPE_REPLACE == 0 && !(sqrt(rr) <= target)) {
+            /* residual replacement: r = b - A x, w = A r, s = A p, z = A s */
+            true_res(A, b, x, t, q, nt);
+            op_apply(A, p, s, nt);
+            memcpy(r, t, sizeof(double) * n);
+            op_apply(A, t, w, nt);
+            op_apply(A, s, z, nt);
+            rr = orc_dot(n, r, r, nt);
+            for (int i = 0; i < n; ++i) scr[i] = w[i] * r[i];
+            wr = tree_sum(n, scr, nt);
+            ++restarts;
+        }
     }
 #undef ORC_PIPE_START
     *iters = k;
@@ -654,7 +669,8 @@ static int krylov_mixed(const orc_op *A, const double *b, int maxiter, double to
             const double g1 = dot32(n, r32, r32, scr, nt);
             ++j;
             ++k;
-            if (sqrt(g1) <= stop || j >= inner_maxiter || k >= maxiter) break;
+            if (sqrt(g1) <= stop || (inner_maxiter > 0 && j >= inner_maxiter) || k >= maxiter)
+                break;
             const float bf = (float)(g1 / g0);
 #pragma omp parallel for num_threads(nt) schedule(static)
             for (int i = 0; i < n; ++i) p32[i] = fmaf(bf, p32[i], r32[i]);
@@ -684,8 +700,8 @@ static int krylov_run(orc_op *A, int method, const double *b_in, int maxiter, do
     if (method == 1) {
         status = krylov_pipe(A, b, maxiter, tol, x, &k, &rs, nt);
     } else if (method == 2) {
-        status = krylov_mixed(A, b, maxiter, tol, inner_maxiter > 0 ? inner_maxiter : 1000,
-                              inner_tol > 0 ? inner_tol : 1e-4, x, &k, &rs, nt);
+        status = krylov_mixed(A, b, maxiter, tol, inner_maxiter,
+                              inner_tol > 0 ? inner_tol : 1e-3, x, &k, &rs, nt);
     } else {
         status = krylov_std(A, b, maxiter, tol, x, &k, &rs, nt);
     }

@@ -64,7 +64,7 @@ int orc_spmv(int n, const int *rowptr, const int *col, const double *val, const 
 
 /* Operator-generic persistent-solver restatements (csrc/krylov.cuh):
  * method 0 standard CG, 1 pipelined CG, 2 FP64 refinement around FP32 CG
- * (inner_maxiter 0 -> 1000, inner_tol 0 -> 1e-4).  b == NULL -> ones, x0 = 0.
+ * (inner_maxiter 0 -> no cap per sweep, inner_tol 0 -> 1e-3).  b == NULL -> ones, x0 = 0.
  * Returns 0 / 4 breakdown / 5 not converged; iters, restarts (refinement
  * sweeps for method 2), relres (true FP64 relative residual) optional. */
 int orc_krylov_csr(int n, const int *rowptr, const int *col, const double *val, int method,
