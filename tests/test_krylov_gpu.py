@@ -107,6 +107,9 @@ def test_config3_poisson128_mixed_reaches_fp64_tolerance():
     x64, st64 = cfm.CG(A, cfm.CG_PERSISTENT, 20000, 1e-8).solve(b)
     x, st = cfm.CG(A, cfm.CG_MIXED, 20000, 1e-8).solve(b)
     assert st.status == cfm.OK and st.residual <= 1e-8
-    err = np.linalg.norm(x - x64) / np.linalg.norm(x64)
-    assert err < 1e-6, err
+    # both stop at a relative residual of 1e-8; their errors against x* are
+    # bounded by cond(A) * 1e-8 (cond ~ 6.6e3 here) and must be alike
+    err64 = np.linalg.norm(x64 - xs) / np.linalg.norm(xs)
+    err = np.linalg.norm(x - xs) / np.linalg.norm(xs)
+    assert err < 1e-5 and err < 3 * err64 + 1e-7, (err, err64)
     assert st.refinements >= 2
