@@ -60,6 +60,8 @@ _SIGS = {
                            _c.c_double, _vp]),
     "cfm_varcoef_problem": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_ulonglong, _vp, _vp]),
     "cfm_varcoef_coeffs": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "cfm_tc_conv3x3": (_c.c_int, [_c.c_int] * 5 + [_vp, _vp, _vp, _c.c_int, _vp]),
+    "cfm_tc_conv3x3_wgrad": (_c.c_int, [_c.c_int] * 5 + [_vp, _vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -393,3 +395,38 @@ def varcoef_coeffs(k):
     check("cfm_varcoef_coeffs", lib.cfm_varcoef_coeffs(dims, nx, ny, nz, _ptr(k), _ptr(we), _ptr(wn),
                                                        _ptr(wt), _ptr(dg)))
     return we, wn, wt, dg
+
+
+def to_bf16_bits(a):
+    """float array -> uint16 BF16 patterns, round to nearest even."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+def from_bf16_bits(b):
+    return (np.ascontiguousarray(b, np.uint16).astype(np.uint32) << 16).view(np.float32)
+
+
+def tc_conv3x3(x_bits, w_bits, bias=None, relu=False):
+    """x [B,H,W,Cin] and w [9,Cout,Cin] as BF16 patterns -> out [B,H,W,Cout] BF16 patterns."""
+    B, H, W, Cin = x_bits.shape
+    Cout = w_bits.shape[1]
+    x_bits = np.ascontiguousarray(x_bits, np.uint16)
+    w_bits = np.ascontiguousarray(w_bits, np.uint16)
+    out = np.empty((B, H, W, Cout), np.uint16)
+    bb = None if bias is None else np.ascontiguousarray(bias, np.float32)
+    check("cfm_tc_conv3x3", lib.cfm_tc_conv3x3(B, H, W, Cin, Cout, _ptr(x_bits), _ptr(w_bits), _ptr(bb),
+                                               int(relu), _ptr(out)))
+    return out
+
+
+def tc_conv3x3_wgrad(x_bits, dz_bits):
+    B, H, W, Cin = x_bits.shape
+    Cout = dz_bits.shape[3]
+    x_bits = np.ascontiguousarray(x_bits, np.uint16)
+    dz_bits = np.ascontiguousarray(dz_bits, np.uint16)
+    dw = np.empty((9, Cout, Cin), np.float32)
+    check("cfm_tc_conv3x3_wgrad", lib.cfm_tc_conv3x3_wgrad(B, H, W, Cin, Cout, _ptr(x_bits), _ptr(dz_bits),
+                                                           _ptr(dw)))
+    return dw

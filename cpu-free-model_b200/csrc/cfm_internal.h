@@ -1,6 +1,8 @@
 // Internal declarations shared by the libcfm translation units.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdarg>
@@ -35,6 +37,9 @@ struct BarrierState {
     int where;            // barrier index at which the first timeout happened
     unsigned long long timeout_ns;
 };
+
+// cuTensorMapEncodeTiled from the driver (nullptr when unavailable).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // Kernel launch helper: cooperative launch so that every block is resident
 // (the barrier needs co-residency).

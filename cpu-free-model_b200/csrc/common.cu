@@ -51,6 +51,23 @@ int current_device_info(DeviceInfo *out) {
     return CFM_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
 cudaError_t launch_cooperative(const void *fn, dim3 grid, dim3 block, void **args, size_t smem,
                                cudaStream_t s) {
     return cudaLaunchCooperativeKernel(fn, grid, block, args, smem, s);

@@ -461,21 +461,6 @@ const TmaVariant &tma_variant(int i) {
 
 int tma_threads(int var) { return 32 * (tma_variant(var).cw + 1); }
 
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-        else
-            cudaGetLastError();
-    }
-    return fn;
-}
-
 // Tensor maps over both grids: dims (nx, ny, nz), box (TX + 2 VN, TY + 2, 1),
 // zero fill outside.  Needs the row pitch nx * esize to be a multiple of 16.
 int setup_tma(cfm_jacobi *h, int var, int zchunk = 0) {

@@ -1,0 +1,308 @@
+// Tensor-core 3x3 convolutions (tc_conv.cuh) on the host side: tensor maps,
+// launch shapes, the channel-major transposes the weight gradient reads,
+// and C-ABI entry points that run one convolution on host buffers (the
+// parity tests drive the kernels through them).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "cfm_internal.h"
+#include "tc_conv.cuh"
+#include "unet_internal.h"
+
+namespace cfm {
+
+namespace {
+
+int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dims,
+               const cuuint64_t *strides, const cuuint32_t *box, int sw_bytes) {
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is unavailable");
+        return CFM_UNSUPPORTED;
+    }
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void *>(base), dims,
+                           strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           sw_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return CFM_BAD_ARG;
+    }
+    return CFM_OK;
+}
+
+template <int KC, int N>
+int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
+                const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
+    using G = TcGeom<KC, N>;
+    static std::once_flag once[64];
+    static cudaError_t attr_err[64];
+    int dev = 0;
+    CFM_CUDA_TRY(cudaGetDevice(&dev));
+    std::call_once(once[dev & 63], [&] {
+        attr_err[dev & 63] = cudaFuncSetAttribute(
+            tc_conv_kernel<KC, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+    });
+    CFM_CUDA_TRY(attr_err[dev & 63]);
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    const int grid = std::min(p.ntiles, di.num_sms);
+    tc_conv_kernel<KC, N><<<grid, 192, G::SMEM, s>>>(a0, a1, a2, b, p);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+template <int KC>
+int launch_kc(int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
+              const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
+    switch (n) {
+        case 32: return launch_kc_n<KC, 32>(a0, a1, a2, b, p, s);
+        case 64: return launch_kc_n<KC, 64>(a0, a1, a2, b, p, s);
+        case 128: return launch_kc_n<KC, 128>(a0, a1, a2, b, p, s);
+        case 256: return launch_kc_n<KC, 256>(a0, a1, a2, b, p, s);
+        default: set_error("unsupported channel count %d", n); return CFM_UNSUPPORTED;
+    }
+}
+
+int launch(int kc, int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
+           const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
+    return kc == 64 ? launch_kc<64>(n, a0, a1, a2, b, p, s) : launch_kc<32>(n, a0, a1, a2, b, p, s);
+}
+
+bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+}  // namespace
+
+// Channel-major copies of an NHWC tensor: out_d[img][c][y][x] =
+// in[img][y][x + d - 1][c] (zero outside) for d = 0 .. nshift - 1 when
+// nshift == 3, or the plain transpose (d = 1 only) when nshift == 1.
+// A block moves 64 pixels of one row (plus one halo pixel each side)
+// through shared memory: reads and writes are both contiguous.
+__global__ void k_nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1,
+                              __nv_bfloat16 *o2, int B, int H, int W, int C, int nshift) {
+    extern __shared__ __nv_bfloat16 tsm[];  // [66][C]
+    const int xt = blockIdx.x, y = blockIdx.y, img = blockIdx.z;
+    const int x0 = xt * 64;
+    const size_t row = ((size_t)img * H + y) * W;
+    for (int e = threadIdx.x; e < 66 * C; e += blockDim.x) {
+        const int px = e / C, c = e % C;
+        const int x = x0 - 1 + px;
+        tsm[e] = (x >= 0 && x < W) ? in[(row + x) * C + c] : __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    const size_t plane = (size_t)H * W;
+    for (int e = threadIdx.x; e < 64 * C; e += blockDim.x) {
+        const int c = e / 64, xx = e % 64, x = x0 + xx;
+        if (x >= W) continue;
+        const size_t o = ((size_t)img * C + c) * plane + (size_t)y * W + x;
+        if (nshift == 3) {
+            o0[o] = tsm[(xx + 0) * C + c];
+            o1[o] = tsm[(xx + 1) * C + c];
+            o2[o] = tsm[(xx + 2) * C + c];
+        } else {
+            o1[o] = tsm[(xx + 1) * C + c];
+        }
+    }
+}
+
+int nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1, __nv_bfloat16 *o2,
+                int B, int H, int W, int C, int nshift, cudaStream_t s) {
+    const size_t smem = 66 * (size_t)C * sizeof(__nv_bfloat16);
+    dim3 grid((W + 63) / 64, H, B);
+    k_nhwc_to_chw<<<grid, 256, smem, s>>>(in, o0, o1, o2, B, H, W, C, nshift);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
+    CFM_ARG_CHECK(a.Cin % 32 == 0 && a.Cin <= 256, "Cin must be a multiple of 32, at most 256");
+    CFM_ARG_CHECK(a.Cout == 32 || a.Cout == 64 || a.Cout == 128 || a.Cout == 256, "Cout");
+    CFM_ARG_CHECK(a.W % 128 == 0 || (pow2(a.W) && a.W <= 128), "W: a power of two or a multiple of 128");
+    CFM_ARG_CHECK(a.H >= 1 && a.B >= 1, "H, B");
+    const int kc = a.Cin % 64 == 0 ? 64 : 32;
+    TcConvParams p{};
+    p.mode = 0;
+    p.B = a.B;
+    p.H = a.H;
+    p.W = a.W;
+    p.Cin = a.Cin;
+    p.Cout = a.Cout;
+    p.bx = std::min(a.W, 128);
+    p.by = 128 / p.bx;
+    p.tiles_x = (a.W + p.bx - 1) / p.bx;
+    p.tiles_y = (a.H + p.by - 1) / p.by;
+    p.ntiles = p.tiles_x * p.tiles_y * a.B;
+    p.ksteps = 9 * (a.Cin / kc);
+    p.bias = a.bias;
+    p.relu = a.relu;
+    p.mask = a.mask;
+    p.out = a.out;
+    p.err = a.err;
+    p.budget_ns = barrier_timeout_ns();
+    CUtensorMap ma, mb;
+    const cuuint64_t da[4] = {(cuuint64_t)a.Cin, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
+    const cuuint64_t sa[3] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.W * a.Cin * 2,
+                              (cuuint64_t)a.H * a.W * a.Cin * 2};
+    const cuuint32_t ba[4] = {(cuuint32_t)kc, (cuuint32_t)p.bx, (cuuint32_t)p.by, 1};
+    int st = encode_map(&ma, a.x, 4, da, sa, ba, kc * 2);
+    if (st) return st;
+    const cuuint64_t db[3] = {(cuuint64_t)a.Cin, (cuuint64_t)a.Cout, 9};
+    const cuuint64_t sb[2] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.Cout * a.Cin * 2};
+    const cuuint32_t bb[3] = {(cuuint32_t)kc, (cuuint32_t)a.Cout, 1};
+    if ((st = encode_map(&mb, a.w, 3, db, sb, bb, kc * 2))) return st;
+    return launch(kc, a.Cout, ma, ma, ma, mb, p, s);
+}
+
+int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
+    CFM_ARG_CHECK(a.Cin % 32 == 0 && a.Cin <= 256, "Cin must be a multiple of 32, at most 256");
+    CFM_ARG_CHECK(a.Cout == 32 || a.Cout == 64 || a.Cout == 128 || a.Cout == 256, "Cout");
+    CFM_ARG_CHECK(a.W % 32 == 0, "W must be a multiple of 32");
+    const int kc = a.W % 64 == 0 ? 64 : 32;
+    TcConvParams p{};
+    p.mode = 1;
+    p.B = a.B;
+    p.H = a.H;
+    p.W = a.W;
+    p.Cin = a.Cin;
+    p.Cout = a.Cout;
+    p.ci_rows = std::min(a.Cin, 128);
+    p.ci_tiles = a.Cin / p.ci_rows;
+    p.taps_per_tile = 128 / p.ci_rows;
+    p.tap_groups = (9 + p.taps_per_tile - 1) / p.taps_per_tile;
+    p.total_k = (long long)a.B * a.H * (a.W / kc);
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    const long long base = (long long)p.tap_groups * p.ci_tiles;
+    long long ks = (2LL * di.num_sms + base - 1) / base;
+    ks = std::max(1LL, std::min(ks, p.total_k / 4 > 0 ? p.total_k / 4 : 1));
+    p.ksplit = (int)ks;
+    p.ntiles = (int)(base * ks);
+    p.dw = a.dw;
+    p.err = a.err;
+    p.budget_ns = barrier_timeout_ns();
+    CUtensorMap m0, m1, m2, mb;
+    const cuuint64_t da[4] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.Cin, (cuuint64_t)a.B};
+    const cuuint64_t sa[3] = {(cuuint64_t)a.W * 2, (cuuint64_t)a.H * a.W * 2,
+                              (cuuint64_t)a.Cin * a.H * a.W * 2};
+    const cuuint32_t ba[4] = {(cuuint32_t)kc, 1, (cuuint32_t)p.ci_rows, 1};
+    if ((st = encode_map(&m0, a.xt[0], 4, da, sa, ba, kc * 2)) ||
+        (st = encode_map(&m1, a.xt[1], 4, da, sa, ba, kc * 2)) ||
+        (st = encode_map(&m2, a.xt[2], 4, da, sa, ba, kc * 2)))
+        return st;
+    const cuuint64_t db[4] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.Cout, (cuuint64_t)a.B};
+    const cuuint64_t sb[3] = {(cuuint64_t)a.W * 2, (cuuint64_t)a.H * a.W * 2,
+                              (cuuint64_t)a.Cout * a.H * a.W * 2};
+    const cuuint32_t bb[4] = {(cuuint32_t)kc, 1, (cuuint32_t)a.Cout, 1};
+    if ((st = encode_map(&mb, a.dzt, 4, db, sb, bb, kc * 2))) return st;
+    return launch(kc, a.Cout, m0, m1, m2, mb, p, s);
+}
+
+}  // namespace cfm
+
+using namespace cfm;
+
+namespace {
+
+// Device scratch for the host-buffer entry points (freed on every path).
+struct DevBufs {
+    std::vector<void *> ptrs;
+    ~DevBufs() {
+        for (void *p : ptrs) cudaFree(p);
+    }
+    template <class T>
+    cudaError_t get(T **out, size_t count) {
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) ptrs.push_back(p);
+        *out = static_cast<T *>(p);
+        return e;
+    }
+};
+
+int finish_err(const int *err_dev) {
+    int herr = 0;
+    CFM_CUDA_TRY(cudaMemcpy(&herr, err_dev, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        set_error("tensor-core convolution: a pipeline wait timed out (site %d)", herr);
+        return CFM_BARRIER_TIMEOUT;
+    }
+    return CFM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfm_tc_conv3x3(int B, int H, int W, int Cin, int Cout, const unsigned short *x,
+                   const unsigned short *w, const float *bias, int relu, unsigned short *out) {
+    clear_error();
+    CFM_ARG_CHECK(x && w && out, "null argument");
+    CFM_ARG_CHECK(B >= 1 && H >= 1 && W >= 1, "sizes");
+    const size_t nx = (size_t)B * H * W * Cin, no = (size_t)B * H * W * Cout,
+                 nw = (size_t)9 * Cout * Cin;
+    DevBufs d;
+    __nv_bfloat16 *dx, *dw, *dout;
+    float *db = nullptr;
+    int *derr;
+    CFM_CUDA_TRY(d.get(&dx, nx));
+    CFM_CUDA_TRY(d.get(&dw, nw));
+    CFM_CUDA_TRY(d.get(&dout, no));
+    CFM_CUDA_TRY(d.get(&derr, 1));
+    if (bias) CFM_CUDA_TRY(d.get(&db, Cout));
+    CFM_CUDA_TRY(cudaMemcpy(dx, x, nx * 2, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemcpy(dw, w, nw * 2, cudaMemcpyHostToDevice));
+    if (bias) CFM_CUDA_TRY(cudaMemcpy(db, bias, Cout * 4, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
+    ConvArgs a{dx, dw, db, nullptr, dout, derr, B, H, W, Cin, Cout, relu};
+    int st = tc_conv_fwd(a, 0);
+    if (st) return st;
+    CFM_CUDA_TRY(cudaDeviceSynchronize());
+    if ((st = finish_err(derr))) return st;
+    CFM_CUDA_TRY(cudaMemcpy(out, dout, no * 2, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
+int cfm_tc_conv3x3_wgrad(int B, int H, int W, int Cin, int Cout, const unsigned short *x,
+                         const unsigned short *dz, float *dw_out) {
+    clear_error();
+    CFM_ARG_CHECK(x && dz && dw_out, "null argument");
+    CFM_ARG_CHECK(B >= 1 && H >= 1 && W >= 1, "sizes");
+    CFM_ARG_CHECK(Cin % 32 == 0 && Cin <= 256 && Cout % 32 == 0 && Cout <= 256, "channels");
+    const size_t nx = (size_t)B * H * W * Cin, nz = (size_t)B * H * W * Cout,
+                 nw = (size_t)9 * Cout * Cin;
+    DevBufs d;
+    __nv_bfloat16 *dx, *ddz, *xt0, *xt1, *xt2, *dzt;
+    float *ddw;
+    int *derr;
+    CFM_CUDA_TRY(d.get(&dx, nx));
+    CFM_CUDA_TRY(d.get(&ddz, nz));
+    CFM_CUDA_TRY(d.get(&xt0, nx));
+    CFM_CUDA_TRY(d.get(&xt1, nx));
+    CFM_CUDA_TRY(d.get(&xt2, nx));
+    CFM_CUDA_TRY(d.get(&dzt, nz));
+    CFM_CUDA_TRY(d.get(&ddw, nw));
+    CFM_CUDA_TRY(d.get(&derr, 1));
+    CFM_CUDA_TRY(cudaMemcpy(dx, x, nx * 2, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemcpy(ddz, dz, nz * 2, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemset(ddw, 0, nw * 4));
+    CFM_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
+    int st = nhwc_to_chw(dx, xt0, xt1, xt2, B, H, W, Cin, 3, 0);
+    if (st) return st;
+    if ((st = nhwc_to_chw(ddz, nullptr, dzt, nullptr, B, H, W, Cout, 1, 0))) return st;
+    WgradArgs a{{xt0, xt1, xt2}, dzt, ddw, derr, B, H, W, Cin, Cout};
+    if ((st = tc_conv_wgrad(a, 0))) return st;
+    CFM_CUDA_TRY(cudaDeviceSynchronize());
+    if ((st = finish_err(derr))) return st;
+    CFM_CUDA_TRY(cudaMemcpy(dw_out, ddw, nw * 4, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
+}  // extern "C"

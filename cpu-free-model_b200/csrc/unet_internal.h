@@ -1,0 +1,39 @@
+// Internal interface of the tensor-core convolutions used by the learned
+// preconditioner (unet.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace cfm {
+
+// out = act(conv3x3(x, w) + bias) [* (mask > 0)], NHWC BF16, padding 1.
+// w is [9][Cout][Cin] (tap = 3 dy + dx), bias FP32 [Cout] or null.
+struct ConvArgs {
+    const __nv_bfloat16 *x;
+    const __nv_bfloat16 *w;
+    const float *bias;
+    const __nv_bfloat16 *mask;  // [B][H][W][Cout] or null
+    __nv_bfloat16 *out;
+    int *err;  // device word, nonzero after a timed-out pipeline wait
+    int B, H, W, Cin, Cout;
+    int relu;
+};
+int tc_conv_fwd(const ConvArgs &a, cudaStream_t s);
+
+// dw[tap][co][ci] += sum over pixels of dz[p][co] * x[p + shift(tap)][ci],
+// from the channel-major copies xt[d] (x shifted by d - 1 in x) and dzt.
+struct WgradArgs {
+    const __nv_bfloat16 *xt[3];
+    const __nv_bfloat16 *dzt;
+    float *dw;
+    int *err;
+    int B, H, W, Cin, Cout;
+};
+int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s);
+
+// Channel-major copies of an NHWC tensor (see k_nhwc_to_chw).
+int nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1, __nv_bfloat16 *o2,
+                int B, int H, int W, int C, int nshift, cudaStream_t s);
+
+}  // namespace cfm

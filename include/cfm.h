@@ -274,6 +274,23 @@ int cfm_varcoef_coeffs(int dims, int nx, int ny, int nz, const double *k, double
  * cfm_uniform, exported for its known-answer test. */
 int cfm_philox4x32_10(const unsigned int ctr[4], const unsigned int key[2], unsigned int out[4]);
 
+/* ------------------------------------------- tensor-core convolutions */
+/* The 3x3 convolutions of the learned preconditioner on the tcgen05 tensor
+ * cores (BF16 operands, FP32 accumulation in TMEM), run once on host buffers.
+ * No reference counterpart (the reference has no tensor-core code); exposed
+ * for parity tests of the kernels.  BF16 values are passed as their 16-bit
+ * patterns.  Layouts: x [B][H][W][Cin], w [9][Cout][Cin] (tap = 3 dy + dx,
+ * padding 1), out [B][H][W][Cout]; Cin a multiple of 32 up to 256, Cout in
+ * {32, 64, 128, 256}, W a power of two up to 128 or a multiple of 128.
+ * out = relu?(conv(x, w) + bias), rounded to BF16. */
+int cfm_tc_conv3x3(int B, int H, int W, int Cin, int Cout, const unsigned short *x,
+                   const unsigned short *w, const float *bias, int relu, unsigned short *out);
+/* Weight gradient dw[tap][co][ci] = sum over pixels p of
+ * dz[p][co] * x[p + (dy - 1, dx - 1)][ci] (zero outside), FP32; W a
+ * multiple of 32. */
+int cfm_tc_conv3x3_wgrad(int B, int H, int W, int Cin, int Cout, const unsigned short *x,
+                         const unsigned short *dz, float *dw);
+
 /* -------------------------------------------------------------- testing */
 /* Launch a persistent kernel of `blocks` blocks (0 = device default) that
  * meets `rounds` grid barriers; when drop_block >= 0 that block skips its
