@@ -62,6 +62,13 @@ _SIGS = {
     "cfm_varcoef_coeffs": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp, _vp]),
     "cfm_tc_conv3x3": (_c.c_int, [_c.c_int] * 5 + [_vp, _vp, _vp, _c.c_int, _vp]),
     "cfm_tc_conv3x3_wgrad": (_c.c_int, [_c.c_int] * 5 + [_vp, _vp, _vp]),
+    "cfm_unet_num_params": (_c.c_longlong, []),
+    "cfm_unet_create": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_ulonglong, _vp]),
+    "cfm_unet_destroy": (None, [_vp]),
+    "cfm_unet_get_params": (_c.c_int, [_vp, _vp]),
+    "cfm_unet_set_params": (_c.c_int, [_vp, _vp]),
+    "cfm_unet_forward_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
+    "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -430,3 +437,45 @@ def tc_conv3x3_wgrad(x_bits, dz_bits):
     check("cfm_tc_conv3x3_wgrad", lib.cfm_tc_conv3x3_wgrad(B, H, W, Cin, Cout, _ptr(x_bits), _ptr(dz_bits),
                                                            _ptr(dw)))
     return dw
+
+
+class UNet:
+    """The learned preconditioner's network (cfm_unet)."""
+
+    def __init__(self, H, W, max_batch=1, seed=0):
+        self.H, self.W, self.max_batch = H, W, max_batch
+        self.n = lib.cfm_unet_num_params()
+        h = ctypes.c_void_p()
+        check("cfm_unet_create", lib.cfm_unet_create(H, W, max_batch, seed, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_unet_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def params(self):
+        t = np.empty(self.n, np.float32)
+        check("cfm_unet_get_params", lib.cfm_unet_get_params(self.h, _ptr(t)))
+        return t
+
+    def set_params(self, t):
+        t = np.ascontiguousarray(t, np.float32)
+        assert t.size == self.n
+        check("cfm_unet_set_params", lib.cfm_unet_set_params(self.h, _ptr(t)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        B = x.shape[0]
+        out = np.empty((B, self.H, self.W), np.float32)
+        check("cfm_unet_forward_host", lib.cfm_unet_forward_host(self.h, B, _ptr(x), _ptr(out)))
+        return out
+
+    def gradient(self, x, dout):
+        x = np.ascontiguousarray(x, np.float32)
+        dout = np.ascontiguousarray(dout, np.float32)
+        g = np.empty(self.n, np.float32)
+        check("cfm_unet_gradient_host", lib.cfm_unet_gradient_host(self.h, x.shape[0], _ptr(x), _ptr(dout), _ptr(g)))
+        return g

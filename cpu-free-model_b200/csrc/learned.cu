@@ -1,0 +1,712 @@
+// The learned preconditioner's U-Net on one B200: forward, backward and an
+// Adam step.  No reference counterpart (the reference has no learned or
+// tensor-core code).
+//
+// Architecture (levels L0..L3 at H/2^l x W/2^l, 32/64/128/256 channels):
+//   h0 = relu(cin(x))  2->32 | h1 = relu(e1(pool h0)) | h2 = relu(e2(pool h1))
+//   h3 = relu(e3(pool h2)) | g3 = relu(d3 h3) | g2 = relu(d2(up g3 + h2))
+//   g1 = relu(d1(up g2 + h1)) | g0 = relu(d0(up g1 + h0)) | out = cout(g0) 32->1
+// 3x3 convolutions with bias, zero padding; pool = 2x2 mean, up = nearest.
+// The seven wide convolutions (e1..d0) and their backward passes run on the
+// tensor cores (tc_conv.cuh): BF16 activations and weights, FP32
+// accumulation.  cin (2 input channels) and cout (1 output channel) are too
+// thin for a 128 x N MMA tile and run on the CUDA cores in FP32.
+// Parameters: one flat FP32 vector (master copy, Adam state beside it), per
+// layer weight [9][Cout][Cin] (tap = 3 dy + dx) then bias [Cout]; BF16 copies
+// of the tensor-core weights and their tap-flipped transposes (the weights
+// of the backward-data convolution) are refreshed after every update.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cfm_internal.h"
+#include "learned_internal.h"
+#include "unet_internal.h"
+
+namespace cfm {
+
+using bf16 = __nv_bfloat16;
+
+const UNetLayer UNET_LAYERS[UNET_NLAYERS] = {
+    {"cin", 2, 32, 0, false},    {"e1", 32, 64, 1, true},    {"e2", 64, 128, 2, true},
+    {"e3", 128, 256, 3, true},   {"d3", 256, 128, 3, true},  {"d2", 128, 64, 2, true},
+    {"d1", 64, 32, 1, true},     {"d0", 32, 32, 0, true},    {"cout", 32, 1, 0, false},
+};
+
+size_t unet_num_params() {
+    size_t n = 0;
+    for (const auto &l : UNET_LAYERS) n += 9 * (size_t)l.co * l.ci + l.co;
+    return n;
+}
+
+// ----------------------------------------------------------------- kernels
+namespace {
+
+__device__ __forceinline__ void load8(const bf16 *p, float *v) {
+    const uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 f = __bfloat1622float2(h[i]);
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ void store8(bf16 *p, const float *v) {
+    uint4 u;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+
+// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2], one pixel per thread.
+__global__ void k_cin_fwd(const float *x, const float *w, const float *b, bf16 *h0, int B, int H,
+                          int W) {
+    __shared__ float sw[9 * 32 * 2 + 32];
+    for (int i = threadIdx.x; i < 9 * 64 + 32; i += blockDim.x) sw[i] = i < 576 ? w[i] : b[i - 576];
+    __syncthreads();
+    const long long P = (long long)B * H * W;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const long long img0 = p - (long long)yy * W - xx;
+        float in[9][2];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
+            const bool ok = y >= 0 && y < H && xq >= 0 && xq < W;
+            const long long q = img0 + (long long)y * W + xq;
+            in[t][0] = ok ? x[2 * q] : 0.f;
+            in[t][1] = ok ? x[2 * q + 1] : 0.f;
+        }
+        float o[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            float acc = sw[576 + c];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc += sw[(t * 32 + c) * 2] * in[t][0] + sw[(t * 32 + c) * 2 + 1] * in[t][1];
+            o[c] = fmaxf(acc, 0.f);
+        }
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) store8(h0 + p * 32 + c, o + c);
+    }
+}
+
+// out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.
+__global__ void k_cout_fwd(const bf16 *g0, const float *w, const float *b, float *out, int B, int H,
+                           int W) {
+    __shared__ float sw[9 * 32 + 1];
+    for (int i = threadIdx.x; i < 289; i += blockDim.x) sw[i] = i < 288 ? w[i] : b[0];
+    __syncthreads();
+    const long long P = (long long)B * H * W;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const long long img0 = p - (long long)yy * W - xx;
+        float acc = sw[288];
+        for (int t = 0; t < 9; ++t) {
+            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
+            if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
+            const bf16 *q = g0 + (img0 + (long long)y * W + xq) * 32;
+#pragma unroll
+            for (int c = 0; c < 32; c += 8) {
+                float v[8];
+                load8(q + c, v);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc += sw[t * 32 + c + j] * v[j];
+            }
+        }
+        out[p] = acc;
+    }
+}
+
+// dz = (sum_t w[t][c] dout[q - s_t]) * (g0[q][c] > 0): the backward-data of cout
+// fused with the ReLU mask of g0.
+__global__ void k_cout_bwd(const float *dout, const float *w, const bf16 *g0, bf16 *dz, int B, int H,
+                           int W) {
+    __shared__ float sw[288];
+    for (int i = threadIdx.x; i < 288; i += blockDim.x) sw[i] = w[i];
+    __syncthreads();
+    const long long P = (long long)B * H * W;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int xx = (int)(p % W), yy = (int)((p / W) % H);
+        const long long img0 = p - (long long)yy * W - xx;
+        float d[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int y = yy - (t / 3 - 1), xq = xx - (t % 3 - 1);
+            d[t] = (y >= 0 && y < H && xq >= 0 && xq < W) ? dout[img0 + (long long)y * W + xq] : 0.f;
+        }
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+            float m[8], o[8];
+            load8(g0 + p * 32 + c, m);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float acc = 0.f;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) acc += sw[t * 32 + c + j] * d[t];
+                o[j] = m[j] > 0.f ? acc : 0.f;
+            }
+            store8(dz + p * 32 + c, o);
+        }
+    }
+}
+
+// Weight and bias gradient of a thin layer by block-local sums and one
+// atomic per block and entry:  dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci],
+// db[co] += sum_p g[p][co].  `g` is FP32 (cout: one channel) or BF16 (cin:
+// 32 channels); `in` FP32 (cin: the network input) or BF16 (cout: g0).
+template <typename GT, typename IT>
+__global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, float *dw, float *db,
+                             int B, int H, int W, long long chunk) {
+    const int nw = 9 * co_n * ci_n;
+    const long long P = (long long)B * H * W;
+    const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
+    for (int e = threadIdx.x; e < nw + co_n; e += blockDim.x) {
+        float acc = 0.f;
+        if (e < nw) {
+            const int t = e / (co_n * ci_n), co = (e / ci_n) % co_n, ci = e % ci_n;
+            const int sy = t / 3 - 1, sx = t % 3 - 1;
+            for (long long p = p0; p < p1; ++p) {
+                const int xx = (int)(p % W), yy = (int)((p / W) % H);
+                const int y = yy + sy, xq = xx + sx;
+                if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
+                const long long q = p + (long long)sy * W + sx;
+                acc += (float)g[p * co_n + co] * (float)in[q * ci_n + ci];
+            }
+            atomicAdd(dw + e, acc);
+        } else {
+            const int co = e - nw;
+            for (long long p = p0; p < p1; ++p) acc += (float)g[p * co_n + co];
+            atomicAdd(db + co, acc);
+        }
+    }
+}
+
+// 2x2 mean pool, NHWC, 8 channels per thread.
+__global__ void k_pool(const bf16 *in, bf16 *out, int B, int h, int w, int C) {
+    const long long n = (long long)B * h * w * (C / 8);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(e % (C / 8)) * 8;
+        const long long pix = e / (C / 8);
+        const int x = (int)(pix % w), y = (int)((pix / w) % h), img = (int)(pix / ((long long)w * h));
+        const long long W2 = 2LL * w;
+        const long long base = (((long long)img * 2 * h + 2 * y) * W2 + 2 * x) * C + c8;
+        float a[8], b[8], c[8], d[8], o[8];
+        load8(in + base, a);
+        load8(in + base + C, b);
+        load8(in + base + W2 * C, c);
+        load8(in + base + W2 * C + C, d);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) o[j] = 0.25f * (((a[j] + b[j]) + c[j]) + d[j]);
+        store8(out + pix * C + c8, o);
+    }
+}
+
+// u = up(g) + skip at the finer level (2h x 2w).
+__global__ void k_up_add(const bf16 *g, const bf16 *skip, bf16 *u, int B, int h, int w, int C) {
+    const long long n = (long long)B * 4 * h * w * (C / 8);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(e % (C / 8)) * 8;
+        const long long pix = e / (C / 8);
+        const int x = (int)(pix % (2 * w)), y = (int)((pix / (2 * w)) % (2 * h));
+        const int img = (int)(pix / (4LL * h * w));
+        const long long cp = ((long long)img * h + y / 2) * w + x / 2;
+        float a[8], b[8];
+        load8(g + cp * C + c8, a);
+        load8(skip + pix * C + c8, b);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] += b[j];
+        store8(u + pix * C + c8, a);
+    }
+}
+
+// dz[coarse] = (sum of the 2x2 fine gradients) * (act[coarse] > 0).
+__global__ void k_down_sum_mask(const bf16 *d, const bf16 *act, bf16 *dz, int B, int h, int w, int C) {
+    const long long n = (long long)B * h * w * (C / 8);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(e % (C / 8)) * 8;
+        const long long pix = e / (C / 8);
+        const int x = (int)(pix % w), y = (int)((pix / w) % h), img = (int)(pix / ((long long)w * h));
+        const long long W2 = 2LL * w;
+        const long long base = (((long long)img * 2 * h + 2 * y) * W2 + 2 * x) * C + c8;
+        float a[8], b[8], c[8], dd[8], m[8], o[8];
+        load8(d + base, a);
+        load8(d + base + C, b);
+        load8(d + base + W2 * C, c);
+        load8(d + base + W2 * C + C, dd);
+        load8(act + pix * C + c8, m);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) o[j] = m[j] > 0.f ? ((a[j] + b[j]) + c[j]) + dd[j] : 0.f;
+        store8(dz + pix * C + c8, o);
+    }
+}
+
+// dz[fine] = (dskip[fine] + 0.25 dpool[coarse]) * (act[fine] > 0): the skip
+// path plus the adjoint of the 2x2 mean pool, through the ReLU of act.
+__global__ void k_skip_pool_mask(const bf16 *dskip, const bf16 *dpool, const bf16 *act, bf16 *dz,
+                                 int B, int h, int w, int C) {
+    const long long n = (long long)B * 4 * h * w * (C / 8);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(e % (C / 8)) * 8;
+        const long long pix = e / (C / 8);
+        const int x = (int)(pix % (2 * w)), y = (int)((pix / (2 * w)) % (2 * h));
+        const int img = (int)(pix / (4LL * h * w));
+        const long long cp = ((long long)img * h + y / 2) * w + x / 2;
+        float a[8], b[8], m[8];
+        load8(dskip + pix * C + c8, a);
+        load8(dpool + cp * C + c8, b);
+        load8(act + pix * C + c8, m);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = m[j] > 0.f ? a[j] + 0.25f * b[j] : 0.f;
+        store8(dz + pix * C + c8, a);
+    }
+}
+
+// db[c] += sum_p dz[p][c] (NHWC BF16): block-local sums, one atomic per block and channel.
+__global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long long chunk) {
+    extern __shared__ float red[];  // [blockDim.x]
+    const int c = threadIdx.x % C, lane_p = threadIdx.x / C, np = blockDim.x / C;
+    const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
+    float acc = 0.f;
+    for (long long p = p0 + lane_p; p < p1; p += np) acc += __bfloat162float(dz[p * C + c]);
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < C) {
+        float s = 0.f;
+        for (int j = 0; j < np; ++j) s += red[j * C + threadIdx.x];
+        atomicAdd(db + threadIdx.x, s);
+    }
+}
+
+// BF16 weights [9][co][ci] and their tap-flipped transposes [9][ci][co]
+// (w'[8 - t][ci][co] = w[t][co][ci]) from the FP32 master copy.
+__global__ void k_weights_bf16(const float *w, bf16 *wb, bf16 *wt, int co, int ci) {
+    const int n = 9 * co * ci;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int t = e / (co * ci), o = (e / ci) % co, i = e % ci;
+        const bf16 v = __float2bfloat16_rn(w[e]);
+        wb[e] = v;
+        wt[((size_t)(8 - t) * ci + i) * co + o] = v;
+    }
+}
+
+// Adam (Kingma & Ba 2015) with bias correction; `scale` multiplies the raw
+// gradient first (e.g. 1 / batch).
+__global__ void k_adam(float *theta, const float *g, float *m, float *v, size_t n, float lr,
+                       float b1, float b2, float eps, float c1, float c2, float scale) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i] * scale;
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        theta[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+int grid_for(long long n, int per = 256) {
+    return (int)std::max(1LL, std::min((n + per - 1) / per, 148LL * 16));
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- the net
+struct UNetBuffers {
+    // forward
+    bf16 *h0, *p1, *h1, *p2, *h2, *p3, *h3, *g3, *u2, *g2, *u1, *g1, *u0, *g0;
+    // backward
+    bf16 *dz_g0, *du0, *dz_g1, *du1, *dz_g2, *du2, *dz_g3, *dz_h3, *dp3, *dz_h2, *dp2, *dz_h1,
+        *dp1, *dz_h0;
+    bf16 *xt[3], *dzt;
+};
+
+struct UNetImpl {
+    int H = 0, W = 0, maxB = 0;
+    size_t nparams = 0;
+    size_t woff[UNET_NLAYERS], boff[UNET_NLAYERS];
+    float *theta = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+    bf16 *wb[UNET_NLAYERS] = {}, *wt[UNET_NLAYERS] = {};
+    UNetBuffers a{};
+    int *err = nullptr;
+    long long adam_t = 0;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+template <class T>
+int dalloc(UNetImpl *u, T **p, size_t count) {
+    void *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("unet allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+    }
+    u->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return CFM_OK;
+}
+
+}  // namespace
+
+int unet_create(int H, int W, int maxB, UNetImpl **out) {
+    CFM_ARG_CHECK(out, "null argument");
+    *out = nullptr;
+    CFM_ARG_CHECK(H >= 8 && H % 8 == 0, "H must be a multiple of 8");
+    CFM_ARG_CHECK(W >= 256 && W % 256 == 0, "W must be a multiple of 256");
+    CFM_ARG_CHECK(maxB >= 1, "max batch");
+    UNetImpl *u = new UNetImpl();
+    u->H = H;
+    u->W = W;
+    u->maxB = maxB;
+    size_t o = 0;
+    for (int l = 0; l < UNET_NLAYERS; ++l) {
+        u->woff[l] = o;
+        o += 9 * (size_t)UNET_LAYERS[l].co * UNET_LAYERS[l].ci;
+        u->boff[l] = o;
+        o += UNET_LAYERS[l].co;
+    }
+    u->nparams = o;
+    const size_t L0 = (size_t)maxB * H * W, L1 = L0 / 4, L2 = L0 / 16, L3 = L0 / 64;
+    UNetBuffers &a = u->a;
+    int st = 0;
+    auto A = [&](bf16 **p, size_t n) {
+        if (!st) st = dalloc(u, p, n);
+    };
+    if (!st) st = dalloc(u, &u->theta, o);
+    if (!st) st = dalloc(u, &u->grad, o);
+    if (!st) st = dalloc(u, &u->m, o);
+    if (!st) st = dalloc(u, &u->v, o);
+    if (!st) st = dalloc(u, &u->err, 1);
+    for (int l = 0; l < UNET_NLAYERS; ++l)
+        if (UNET_LAYERS[l].tc) {
+            const size_t n = 9 * (size_t)UNET_LAYERS[l].co * UNET_LAYERS[l].ci;
+            A(&u->wb[l], n);
+            A(&u->wt[l], n);
+        }
+    A(&a.h0, L0 * 32);  A(&a.p1, L1 * 32);  A(&a.h1, L1 * 64);  A(&a.p2, L2 * 64);
+    A(&a.h2, L2 * 128); A(&a.p3, L3 * 128); A(&a.h3, L3 * 256); A(&a.g3, L3 * 128);
+    A(&a.u2, L2 * 128); A(&a.g2, L2 * 64);  A(&a.u1, L1 * 64);  A(&a.g1, L1 * 32);
+    A(&a.u0, L0 * 32);  A(&a.g0, L0 * 32);
+    A(&a.dz_g0, L0 * 32); A(&a.du0, L0 * 32); A(&a.dz_g1, L1 * 32); A(&a.du1, L1 * 64);
+    A(&a.dz_g2, L2 * 64); A(&a.du2, L2 * 128); A(&a.dz_g3, L3 * 128); A(&a.dz_h3, L3 * 256);
+    A(&a.dp3, L3 * 128); A(&a.dz_h2, L2 * 128); A(&a.dp2, L2 * 64); A(&a.dz_h1, L1 * 64);
+    A(&a.dp1, L1 * 32); A(&a.dz_h0, L0 * 32);
+    for (int d = 0; d < 3; ++d) A(&a.xt[d], L0 * 32);
+    A(&a.dzt, L0 * 32);
+    if (st) {
+        unet_destroy(u);
+        return st;
+    }
+    cudaError_t e;
+    if ((e = cudaMemset(u->theta, 0, o * 4)) != cudaSuccess ||
+        (e = cudaMemset(u->m, 0, o * 4)) != cudaSuccess ||
+        (e = cudaMemset(u->v, 0, o * 4)) != cudaSuccess ||
+        (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess) {
+        unet_destroy(u);
+        CFM_CUDA_TRY(e);
+    }
+    *out = u;
+    return CFM_OK;
+}
+
+void unet_destroy(UNetImpl *u) {
+    if (!u) return;
+    cudaDeviceSynchronize();
+    for (void *p : u->allocs) cudaFree(p);
+    delete u;
+}
+
+size_t unet_params(const UNetImpl *u) { return u->nparams; }
+float *unet_theta(UNetImpl *u) { return u->theta; }
+float *unet_grad(UNetImpl *u) { return u->grad; }
+int *unet_err(UNetImpl *u) { return u->err; }
+
+int unet_refresh_weights(UNetImpl *u, cudaStream_t s) {
+    for (int l = 0; l < UNET_NLAYERS; ++l) {
+        const UNetLayer &L = UNET_LAYERS[l];
+        if (!L.tc) continue;
+        const int n = 9 * L.co * L.ci;
+        k_weights_bf16<<<grid_for(n), 256, 0, s>>>(u->theta + u->woff[l], u->wb[l], u->wt[l], L.co,
+                                                    L.ci);
+        CFM_CUDA_TRY(cudaGetLastError());
+    }
+    return CFM_OK;
+}
+
+namespace {
+
+int conv_fwd(UNetImpl *u, int l, const bf16 *x, bf16 *out, int B, int h, int w, cudaStream_t s) {
+    const UNetLayer &L = UNET_LAYERS[l];
+    ConvArgs c{x, u->wb[l], u->theta + u->boff[l], nullptr, out, u->err, B, h, w, L.ci, L.co, 1};
+    return tc_conv_fwd(c, s);
+}
+
+// dx = conv_T(dz) (weights flipped / transposed), optionally masked.
+int conv_bwd_data(UNetImpl *u, int l, const bf16 *dz, const bf16 *mask, bf16 *dx, int B, int h,
+                  int w, cudaStream_t s) {
+    const UNetLayer &L = UNET_LAYERS[l];
+    ConvArgs c{dz, u->wt[l], nullptr, mask, dx, u->err, B, h, w, L.co, L.ci, 0};
+    return tc_conv_fwd(c, s);
+}
+
+// dW += wgrad(x, dz), db += sum dz.
+int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, int h, int w,
+                     cudaStream_t s) {
+    const UNetLayer &L = UNET_LAYERS[l];
+    UNetBuffers &a = u->a;
+    int st = nhwc_to_chw(x, a.xt[0], a.xt[1], a.xt[2], B, h, w, L.ci, 3, s);
+    if (st) return st;
+    if ((st = nhwc_to_chw(dz, nullptr, a.dzt, nullptr, B, h, w, L.co, 1, s))) return st;
+    WgradArgs g{{a.xt[0], a.xt[1], a.xt[2]}, a.dzt, u->grad + u->woff[l], u->err, B, h, w, L.ci, L.co};
+    if ((st = tc_conv_wgrad(g, s))) return st;
+    const long long P = (long long)B * h * w;
+    const int threads = 256;
+    const long long chunk = std::max(64LL, (P + 4 * 148 - 1) / (4 * 148));
+    k_bias_grad<<<(int)((P + chunk - 1) / chunk), threads, threads * sizeof(float), s>>>(
+        dz, u->grad + u->boff[l], P, L.co, chunk);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+}  // namespace
+
+int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s) {
+    CFM_ARG_CHECK(B >= 1 && B <= u->maxB, "batch");
+    UNetBuffers &a = u->a;
+    const int H = u->H, W = u->W;
+    const long long P0 = (long long)B * H * W;
+    int st;
+    k_cin_fwd<<<grid_for(P0), 256, 0, s>>>(x, u->theta + u->woff[0], u->theta + u->boff[0], a.h0, B, H, W);
+    CFM_CUDA_TRY(cudaGetLastError());
+    int h = H, w = W;
+    k_pool<<<grid_for(P0 / 4 * 4), 256, 0, s>>>(a.h0, a.p1, B, h / 2, w / 2, 32);
+    h /= 2, w /= 2;
+    if ((st = conv_fwd(u, 1, a.p1, a.h1, B, h, w, s))) return st;
+    k_pool<<<grid_for(P0 / 16 * 8), 256, 0, s>>>(a.h1, a.p2, B, h / 2, w / 2, 64);
+    h /= 2, w /= 2;
+    if ((st = conv_fwd(u, 2, a.p2, a.h2, B, h, w, s))) return st;
+    k_pool<<<grid_for(P0 / 64 * 16), 256, 0, s>>>(a.h2, a.p3, B, h / 2, w / 2, 128);
+    h /= 2, w /= 2;
+    if ((st = conv_fwd(u, 3, a.p3, a.h3, B, h, w, s))) return st;
+    if ((st = conv_fwd(u, 4, a.h3, a.g3, B, h, w, s))) return st;
+    k_up_add<<<grid_for(P0 / 16 * 16), 256, 0, s>>>(a.g3, a.h2, a.u2, B, h, w, 128);
+    h *= 2, w *= 2;
+    if ((st = conv_fwd(u, 5, a.u2, a.g2, B, h, w, s))) return st;
+    k_up_add<<<grid_for(P0 / 4 * 8), 256, 0, s>>>(a.g2, a.h1, a.u1, B, h, w, 64);
+    h *= 2, w *= 2;
+    if ((st = conv_fwd(u, 6, a.u1, a.g1, B, h, w, s))) return st;
+    k_up_add<<<grid_for(P0 * 4), 256, 0, s>>>(a.g1, a.h0, a.u0, B, h, w, 32);
+    h *= 2, w *= 2;
+    if ((st = conv_fwd(u, 7, a.u0, a.g0, B, h, w, s))) return st;
+    k_cout_fwd<<<grid_for(P0), 256, 0, s>>>(a.g0, u->theta + u->woff[8], u->theta + u->boff[8], out, B,
+                                            H, W);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+// Gradient of sum(out * dout) into u->grad (accumulated; zero it first for a
+// fresh gradient).  Needs the activations of the unet_forward just before.
+int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStream_t s) {
+    UNetBuffers &a = u->a;
+    const int H = u->H, W = u->W;
+    const long long P0 = (long long)B * H * W;
+    int st;
+    const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+    // cout
+    {
+        const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
+        k_thin_wgrad<float, bf16><<<(int)((P0 + chunk - 1) / chunk), 320, 0, s>>>(
+            dout, a.g0, 1, 32, u->grad + u->woff[8], u->grad + u->boff[8], B, H, W, chunk);
+        CFM_CUDA_TRY(cudaGetLastError());
+        k_cout_bwd<<<grid_for(P0), 256, 0, s>>>(dout, u->theta + u->woff[8], a.g0, a.dz_g0, B, H, W);
+        CFM_CUDA_TRY(cudaGetLastError());
+    }
+    // d0 @L0
+    if ((st = conv_bwd_weights(u, 7, a.u0, a.dz_g0, B, H, W, s))) return st;
+    if ((st = conv_bwd_data(u, 7, a.dz_g0, nullptr, a.du0, B, H, W, s))) return st;
+    k_down_sum_mask<<<grid_for(P0 / 4 * 4), 256, 0, s>>>(a.du0, a.g1, a.dz_g1, B, H1, W1, 32);
+    // d1 @L1
+    if ((st = conv_bwd_weights(u, 6, a.u1, a.dz_g1, B, H1, W1, s))) return st;
+    if ((st = conv_bwd_data(u, 6, a.dz_g1, nullptr, a.du1, B, H1, W1, s))) return st;
+    k_down_sum_mask<<<grid_for(P0 / 16 * 8), 256, 0, s>>>(a.du1, a.g2, a.dz_g2, B, H2, W2, 64);
+    // d2 @L2
+    if ((st = conv_bwd_weights(u, 5, a.u2, a.dz_g2, B, H2, W2, s))) return st;
+    if ((st = conv_bwd_data(u, 5, a.dz_g2, nullptr, a.du2, B, H2, W2, s))) return st;
+    k_down_sum_mask<<<grid_for(P0 / 64 * 16), 256, 0, s>>>(a.du2, a.g3, a.dz_g3, B, H3, W3, 128);
+    // d3 @L3 (its input h3 is a ReLU output: mask the data gradient)
+    if ((st = conv_bwd_weights(u, 4, a.h3, a.dz_g3, B, H3, W3, s))) return st;
+    if ((st = conv_bwd_data(u, 4, a.dz_g3, a.h3, a.dz_h3, B, H3, W3, s))) return st;
+    // e3 @L3
+    if ((st = conv_bwd_weights(u, 3, a.p3, a.dz_h3, B, H3, W3, s))) return st;
+    if ((st = conv_bwd_data(u, 3, a.dz_h3, nullptr, a.dp3, B, H3, W3, s))) return st;
+    k_skip_pool_mask<<<grid_for(P0 / 16 * 16), 256, 0, s>>>(a.du2, a.dp3, a.h2, a.dz_h2, B, H3, W3, 128);
+    // e2 @L2
+    if ((st = conv_bwd_weights(u, 2, a.p2, a.dz_h2, B, H2, W2, s))) return st;
+    if ((st = conv_bwd_data(u, 2, a.dz_h2, nullptr, a.dp2, B, H2, W2, s))) return st;
+    k_skip_pool_mask<<<grid_for(P0 / 4 * 8), 256, 0, s>>>(a.du1, a.dp2, a.h1, a.dz_h1, B, H2, W2, 64);
+    // e1 @L1
+    if ((st = conv_bwd_weights(u, 1, a.p1, a.dz_h1, B, H1, W1, s))) return st;
+    if ((st = conv_bwd_data(u, 1, a.dz_h1, nullptr, a.dp1, B, H1, W1, s))) return st;
+    k_skip_pool_mask<<<grid_for(P0 * 4), 256, 0, s>>>(a.du0, a.dp1, a.h0, a.dz_h0, B, H1, W1, 32);
+    // cin
+    {
+        const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
+        k_thin_wgrad<bf16, float><<<(int)((P0 + chunk - 1) / chunk), 608, 0, s>>>(
+            a.dz_h0, x, 32, 2, u->grad + u->woff[0], u->grad + u->boff[0], B, H, W, chunk);
+        CFM_CUDA_TRY(cudaGetLastError());
+    }
+    return CFM_OK;
+}
+
+int unet_adam(UNetImpl *u, float lr, float scale, cudaStream_t s) {
+    ++u->adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)u->adam_t), c2 = 1.f - std::pow(b2, (float)u->adam_t);
+    k_adam<<<grid_for((long long)u->nparams), 256, 0, s>>>(u->theta, u->grad, u->m, u->v, u->nparams,
+                                                            lr, b1, b2, 1e-8f, c1, c2, scale);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return unet_refresh_weights(u, s);
+}
+
+int unet_check_err(UNetImpl *u) {
+    int herr = 0;
+    CFM_CUDA_TRY(cudaMemcpy(&herr, u->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        set_error("unet: a tensor-core pipeline wait timed out (site %d)", herr);
+        return CFM_BARRIER_TIMEOUT;
+    }
+    return CFM_OK;
+}
+
+}  // namespace cfm
+
+// ------------------------------------------------------------------ C ABI
+using namespace cfm;
+
+struct cfm_unet {
+    UNetImpl *u = nullptr;
+    float *xin = nullptr, *out = nullptr, *dout = nullptr;
+    int maxB = 0;
+};
+
+extern "C" {
+
+long long cfm_unet_num_params(void) { return (long long)unet_num_params(); }
+
+int cfm_unet_create(int H, int W, int max_batch, unsigned long long seed, cfm_unet **out) {
+    clear_error();
+    CFM_ARG_CHECK(out, "null argument");
+    *out = nullptr;
+    UNetImpl *u = nullptr;
+    int st = unet_create(H, W, max_batch, &u);
+    if (st) return st;
+    cfm_unet *h = new cfm_unet();
+    h->u = u;
+    h->maxB = max_batch;
+    const size_t P = (size_t)max_batch * H * W;
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->xin, P * 2 * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&h->out, P * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&h->dout, P * 4)) != cudaSuccess) {
+        cfm_unet_destroy(h);
+        CFM_CUDA_TRY(e);
+    }
+    // He-normal weights (std sqrt(2 / (9 Cin))), zero biases; the output layer
+    // starts 10x smaller.
+    std::vector<float> theta(u->nparams, 0.f);
+    std::vector<double> z;
+    size_t o = 0;
+    for (int l = 0; l < UNET_NLAYERS; ++l) {
+        const UNetLayer &L = UNET_LAYERS[l];
+        const size_t n = 9 * (size_t)L.co * L.ci;
+        z.resize(n);
+        cfm_normal(seed, 100u + l, (long long)n, z.data());
+        const double sd = std::sqrt(2.0 / (9.0 * L.ci)) * (l == UNET_NLAYERS - 1 ? 0.1 : 1.0);
+        for (size_t i = 0; i < n; ++i) theta[o + i] = (float)(sd * z[i]);
+        o += n + L.co;
+    }
+    if ((e = cudaMemcpy(u->theta, theta.data(), theta.size() * 4, cudaMemcpyHostToDevice)) !=
+        cudaSuccess) {
+        cfm_unet_destroy(h);
+        CFM_CUDA_TRY(e);
+    }
+    if ((st = unet_refresh_weights(u, 0))) {
+        cfm_unet_destroy(h);
+        return st;
+    }
+    *out = h;
+    return CFM_OK;
+}
+
+void cfm_unet_destroy(cfm_unet *h) {
+    if (!h) return;
+    unet_destroy(h->u);
+    cudaFree(h->xin);
+    cudaFree(h->out);
+    cudaFree(h->dout);
+    delete h;
+}
+
+int cfm_unet_get_params(cfm_unet *h, float *theta) {
+    CFM_ARG_CHECK(h && theta, "null argument");
+    CFM_CUDA_TRY(cudaMemcpy(theta, h->u->theta, h->u->nparams * 4, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
+int cfm_unet_set_params(cfm_unet *h, const float *theta) {
+    CFM_ARG_CHECK(h && theta, "null argument");
+    CFM_CUDA_TRY(cudaMemcpy(h->u->theta, theta, h->u->nparams * 4, cudaMemcpyHostToDevice));
+    int st = unet_refresh_weights(h->u, 0);
+    if (st) return st;
+    CFM_CUDA_TRY(cudaDeviceSynchronize());
+    return CFM_OK;
+}
+
+int cfm_unet_forward_host(cfm_unet *h, int B, const float *in, float *out) {
+    clear_error();
+    CFM_ARG_CHECK(h && in && out, "null argument");
+    CFM_ARG_CHECK(B >= 1 && B <= h->maxB, "batch");
+    const size_t P = (size_t)B * h->u->H * h->u->W;
+    CFM_CUDA_TRY(cudaMemcpy(h->xin, in, P * 2 * 4, cudaMemcpyHostToDevice));
+    int st = unet_forward(h->u, B, h->xin, h->out, 0);
+    if (st) return st;
+    CFM_CUDA_TRY(cudaDeviceSynchronize());
+    if ((st = unet_check_err(h->u))) return st;
+    CFM_CUDA_TRY(cudaMemcpy(out, h->out, P * 4, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
+int cfm_unet_gradient_host(cfm_unet *h, int B, const float *in, const float *dout, float *grad) {
+    clear_error();
+    CFM_ARG_CHECK(h && in && dout && grad, "null argument");
+    CFM_ARG_CHECK(B >= 1 && B <= h->maxB, "batch");
+    const size_t P = (size_t)B * h->u->H * h->u->W;
+    CFM_CUDA_TRY(cudaMemcpy(h->xin, in, P * 2 * 4, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemcpy(h->dout, dout, P * 4, cudaMemcpyHostToDevice));
+    CFM_CUDA_TRY(cudaMemset(h->u->grad, 0, h->u->nparams * 4));
+    int st = unet_forward(h->u, B, h->xin, h->out, 0);
+    if (st) return st;
+    if ((st = unet_backward(h->u, B, h->xin, h->dout, 0))) return st;
+    CFM_CUDA_TRY(cudaDeviceSynchronize());
+    if ((st = unet_check_err(h->u))) return st;
+    CFM_CUDA_TRY(cudaMemcpy(grad, h->u->grad, h->u->nparams * 4, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
+}  // extern "C"

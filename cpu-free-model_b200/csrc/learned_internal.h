@@ -1,0 +1,36 @@
+// Internal interface of the learned preconditioner (learned.cu, fpcg.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace cfm {
+
+constexpr int UNET_NLAYERS = 9;
+
+struct UNetLayer {
+    const char *name;
+    int ci, co;
+    int level;  // 0..3 (resolution H / 2^level)
+    bool tc;    // tensor-core convolution (else CUDA cores)
+};
+extern const UNetLayer UNET_LAYERS[UNET_NLAYERS];
+size_t unet_num_params();
+
+struct UNetImpl;
+int unet_create(int H, int W, int max_batch, UNetImpl **out);
+void unet_destroy(UNetImpl *u);
+size_t unet_params(const UNetImpl *u);
+float *unet_theta(UNetImpl *u);
+float *unet_grad(UNetImpl *u);
+int *unet_err(UNetImpl *u);
+int unet_refresh_weights(UNetImpl *u, cudaStream_t s);
+// x FP32 [B][H][W][2] -> out FP32 [B][H][W] (device pointers).
+int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s);
+// Accumulates the gradient of sum(out * dout) into unet_grad (after unet_forward).
+int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStream_t s);
+int unet_adam(UNetImpl *u, float lr, float grad_scale, cudaStream_t s);
+int unet_check_err(UNetImpl *u);
+
+}  // namespace cfm

@@ -291,6 +291,28 @@ int cfm_tc_conv3x3(int B, int H, int W, int Cin, int Cout, const unsigned short 
 int cfm_tc_conv3x3_wgrad(int B, int H, int W, int Cin, int Cout, const unsigned short *x,
                          const unsigned short *dz, float *dw);
 
+/* ------------------------------------------------ learned preconditioner */
+/* The U-Net of the learned preconditioner (no reference counterpart):
+ * 4 levels (H, H/2, H/4, H/8) with 32/64/128/256 channels, 3x3 convolutions
+ * with bias and ReLU, 2x2 mean pooling, nearest upsampling with additive
+ * skips; input [B][H][W][2] FP32 (normalised residual, log k), output
+ * [B][H][W] FP32.  Wide convolutions on the tcgen05 tensor cores (BF16,
+ * FP32 accumulate).  Parameters: one flat FP32 vector, per layer
+ * (cin 2->32, e1 32->64, e2 64->128, e3 128->256, d3 256->128, d2 128->64,
+ * d1 64->32, d0 32->32, cout 32->1) weight [9][Cout][Cin] then bias [Cout].
+ * H a multiple of 8, W a multiple of 256. */
+typedef struct cfm_unet cfm_unet;
+long long cfm_unet_num_params(void);
+int cfm_unet_create(int H, int W, int max_batch, unsigned long long seed, cfm_unet **out);
+void cfm_unet_destroy(cfm_unet *net);
+int cfm_unet_get_params(cfm_unet *net, float *theta);
+int cfm_unet_set_params(cfm_unet *net, const float *theta);
+/* One forward pass on host buffers. */
+int cfm_unet_forward_host(cfm_unet *net, int B, const float *in, float *out);
+/* Forward, then the gradient of sum(out * dout) with respect to the
+ * parameters into grad (cfm_unet_num_params floats). */
+int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *dout, float *grad);
+
 /* -------------------------------------------------------------- testing */
 /* Launch a persistent kernel of `blocks` blocks (0 = device default) that
  * meets `rounds` grid barriers; when drop_block >= 0 that block skips its
