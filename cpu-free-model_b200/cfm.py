@@ -69,6 +69,7 @@ _SIGS = {
     "cfm_unet_set_params": (_c.c_int, [_vp, _vp]),
     "cfm_unet_forward_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
+    "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -471,6 +472,19 @@ class UNet:
         B = x.shape[0]
         out = np.empty((B, self.H, self.W), np.float32)
         check("cfm_unet_forward_host", lib.cfm_unet_forward_host(self.h, B, _ptr(x), _ptr(out)))
+        return out
+
+    ACTIVATIONS = [("h0", 0, 32), ("p1", 1, 32), ("h1", 1, 64), ("p2", 2, 64), ("h2", 2, 128),
+                   ("p3", 3, 128), ("h3", 3, 256), ("g3", 3, 128), ("u2", 2, 128), ("g2", 2, 64),
+                   ("u1", 1, 64), ("g1", 1, 32), ("u0", 0, 32), ("g0", 0, 32)]
+
+    def activations(self, B):
+        """The last forward pass's activations as float32 arrays, by name."""
+        out = {}
+        for i, (name, lev, ch) in enumerate(self.ACTIVATIONS):
+            a = np.empty((B, self.H >> lev, self.W >> lev, ch), np.uint16)
+            check("cfm_unet_activation_host", lib.cfm_unet_activation_host(self.h, i, B, _ptr(a)))
+            out[name] = from_bf16_bits(a)
         return out
 
     def gradient(self, x, dout):

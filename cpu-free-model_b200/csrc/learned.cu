@@ -709,4 +709,20 @@ int cfm_unet_gradient_host(cfm_unet *h, int B, const float *in, const float *dou
     return CFM_OK;
 }
 
+// BF16 patterns of one activation of the last forward pass, in the order
+// h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0 (index 0..13), B images.
+int cfm_unet_activation_host(cfm_unet *h, int which, int B, unsigned short *out) {
+    clear_error();
+    CFM_ARG_CHECK(h && out, "null argument");
+    CFM_ARG_CHECK(B >= 1 && B <= h->maxB, "batch");
+    const UNetBuffers &a = h->u->a;
+    const bf16 *bufs[14] = {a.h0, a.p1, a.h1, a.p2, a.h2, a.p3, a.h3, a.g3, a.u2, a.g2, a.u1, a.g1, a.u0, a.g0};
+    const int lev[14] = {0, 1, 1, 2, 2, 3, 3, 3, 2, 2, 1, 1, 0, 0};
+    const int ch[14] = {32, 32, 64, 64, 128, 128, 256, 128, 128, 64, 64, 32, 32, 32};
+    CFM_ARG_CHECK(which >= 0 && which < 14, "activation index");
+    const size_t n = (size_t)B * (h->u->H >> lev[which]) * (h->u->W >> lev[which]) * ch[which];
+    CFM_CUDA_TRY(cudaMemcpy(out, bufs[which], n * 2, cudaMemcpyDeviceToHost));
+    return CFM_OK;
+}
+
 }  // extern "C"

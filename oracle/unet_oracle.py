@@ -119,29 +119,32 @@ def forward(theta, x, round_bf16=True):
     return out, c
 
 
-def backward(c, dout):
-    """Gradient of sum(out * dout) with respect to the flat parameters."""
+def backward(c, dout, round_bf16=False):
+    """Gradient of sum(out * dout) with respect to the flat parameters.
+    round_bf16: round every gradient tensor the GPU stores in BF16 (the
+    convolution operands of the backward pass) at the same place."""
     W = c["W"]
+    r = bf16 if round_bf16 else (lambda a: a)
     g = {}
     d = dout[..., None].astype(np.float64)
     g["cout"] = (conv_w(c["g0"], d), d.sum(axis=(0, 1, 2)))
-    dz = conv_t(d, W["cout"][0]) * (c["g0"] > 0)
+    dz = r(conv_t(d, W["cout"][0]) * (c["g0"] > 0))
     g["d0"] = (conv_w(c["u0"], dz), dz.sum(axis=(0, 1, 2)))
-    du0 = conv_t(dz, W["d0"][0])
-    dz = down_sum(du0) * (c["g1"] > 0)
+    du0 = r(conv_t(dz, W["d0"][0]))
+    dz = r(down_sum(du0) * (c["g1"] > 0))
     g["d1"] = (conv_w(c["u1"], dz), dz.sum(axis=(0, 1, 2)))
-    du1 = conv_t(dz, W["d1"][0])
-    dz = down_sum(du1) * (c["g2"] > 0)
+    du1 = r(conv_t(dz, W["d1"][0]))
+    dz = r(down_sum(du1) * (c["g2"] > 0))
     g["d2"] = (conv_w(c["u2"], dz), dz.sum(axis=(0, 1, 2)))
-    du2 = conv_t(dz, W["d2"][0])
-    dz = down_sum(du2) * (c["g3"] > 0)
+    du2 = r(conv_t(dz, W["d2"][0]))
+    dz = r(down_sum(du2) * (c["g3"] > 0))
     g["d3"] = (conv_w(c["h3"], dz), dz.sum(axis=(0, 1, 2)))
-    dz = conv_t(dz, W["d3"][0]) * (c["h3"] > 0)
+    dz = r(conv_t(dz, W["d3"][0]) * (c["h3"] > 0))
     g["e3"] = (conv_w(c["p3"], dz), dz.sum(axis=(0, 1, 2)))
-    dz = (du2 + 0.25 * up(conv_t(dz, W["e3"][0]))) * (c["h2"] > 0)
+    dz = r((du2 + 0.25 * up(r(conv_t(dz, W["e3"][0])))) * (c["h2"] > 0))
     g["e2"] = (conv_w(c["p2"], dz), dz.sum(axis=(0, 1, 2)))
-    dz = (du1 + 0.25 * up(conv_t(dz, W["e2"][0]))) * (c["h1"] > 0)
+    dz = r((du1 + 0.25 * up(r(conv_t(dz, W["e2"][0])))) * (c["h1"] > 0))
     g["e1"] = (conv_w(c["p1"], dz), dz.sum(axis=(0, 1, 2)))
-    dz = (du0 + 0.25 * up(conv_t(dz, W["e1"][0]))) * (c["h0"] > 0)
+    dz = r((du0 + 0.25 * up(r(conv_t(dz, W["e1"][0])))) * (c["h0"] > 0))
     g["cin"] = (conv_w(c["x"], dz), dz.sum(axis=(0, 1, 2)))
     return np.concatenate([np.concatenate([g[k][0].ravel(), g[k][1].ravel()]) for k, _, _ in LAYERS])

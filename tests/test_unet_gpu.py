@@ -34,18 +34,42 @@ def test_unet_forward_matches_oracle(case):
     assert rel(got, want) < 2e-2, rel(got, want)
 
 
-def test_unet_gradient_matches_oracle_per_layer(case):
+def test_unet_backward_matches_oracle_on_gpu_activations(case):
+    """The backward kernels alone: the oracle's backward runs on the GPU's
+    own forward activations (same ReLU masks), rounding the gradient tensors
+    to BF16 where the GPU stores them.  Per-layer relative error < 2e-2."""
+    net, theta, x, dout = case
+    got = net.gradient(x, dout).astype(np.float64)
+    acts = net.activations(x.shape[0])
+    _, cache = U.forward(theta.astype(np.float64), x.astype(np.float64))
+    cache.update({k: v.astype(np.float64) for k, v in acts.items()})
+    want = U.backward(cache, dout.astype(np.float64), round_bf16=True)
+    o, errs = 0, {}
+    for name, ci, co in U.LAYERS:
+        nw = 9 * ci * co
+        errs[name + ".w"] = rel(got[o:o + nw], want[o:o + nw])
+        errs[name + ".b"] = rel(got[o + nw:o + nw + co], want[o + nw:o + nw + co])
+        o += nw + co
+    print("relative gradient errors:", errs)
+    assert all(e < 2e-2 for e in errs.values()), errs
+
+
+def test_unet_gradient_end_to_end_close_to_float64(case):
+    """End to end against the float64 oracle: the GPU's BF16 activations and
+    tensor-core accumulation differ from float64 by ~0.2% (the forward
+    test), which flips a few ReLU masks near zero; each flip changes the
+    backpropagated gradient by a full term, so the bar here is direction
+    (cosine > 0.99) and 15% relative error per layer."""
     net, theta, x, dout = case
     got = net.gradient(x, dout).astype(np.float64)
     _, cache = U.forward(theta.astype(np.float64), x.astype(np.float64))
     want = U.backward(cache, dout.astype(np.float64))
     o = 0
     for name, ci, co in U.LAYERS:
-        nw = 9 * ci * co
-        for part, sl in (("w", slice(o, o + nw)), ("b", slice(o + nw, o + nw + co))):
-            e = rel(got[sl], want[sl])
-            assert e < 5e-2, (name, part, e)
-        o += nw + co
+        sl = slice(o, o + 9 * ci * co + co)
+        a, b = got[sl], want[sl]
+        assert rel(a, b) < 0.15 and a @ b / (np.linalg.norm(a) * np.linalg.norm(b)) > 0.99, name
+        o += 9 * ci * co + co
 
 
 def test_unet_params_roundtrip(case):
