@@ -70,6 +70,11 @@ _SIGS = {
     "cfm_unet_forward_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
+    "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
+                                          _c.c_float, _vp, _vp, _vp, _vp]),
+    "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_double, _vp]),
+    "cfm_fpcg_destroy": (None, [_vp]),
+    "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -487,9 +492,42 @@ class UNet:
             out[name] = from_bf16_bits(a)
         return out
 
+    def train_varcoef(self, nsys, snaps, seed0, epochs, batch, lr=1e-3):
+        """Plain-CG training pairs + Adam; returns dict(loss_first, loss_last, data_s, train_s)."""
+        v = [ctypes.c_double() for _ in range(4)]
+        check("cfm_unet_train_varcoef",
+              lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr,
+                                         *[ctypes.byref(x) for x in v]))
+        return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
+
     def gradient(self, x, dout):
         x = np.ascontiguousarray(x, np.float32)
         dout = np.ascontiguousarray(dout, np.float32)
         g = np.empty(self.n, np.float32)
         check("cfm_unet_gradient_host", lib.cfm_unet_gradient_host(self.h, x.shape[0], _ptr(x), _ptr(dout), _ptr(g)))
         return g
+
+
+class FPCG:
+    """Flexible PCG with the network as preconditioner (cfm_fpcg)."""
+
+    def __init__(self, S, k, net, maxiter=5000, tol=1e-8):
+        self.S, self.net = S, net
+        self.k = np.ascontiguousarray(k, np.float64)
+        h = ctypes.c_void_p()
+        check("cfm_fpcg_create", lib.cfm_fpcg_create(S.h, _ptr(self.k), net.h, maxiter, tol, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_fpcg_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def solve(self, b, allowed=(OK, NOT_CONVERGED)):
+        b = np.ascontiguousarray(b, np.float64).reshape(-1)
+        x = np.empty_like(b)
+        st = Stats()
+        check("cfm_fpcg_solve", lib.cfm_fpcg_solve(self.h, _ptr(b), _ptr(x), ctypes.byref(st)), allowed)
+        return x, st

@@ -374,6 +374,64 @@ int check_cg_params(const cfm_cg_params *p) {
 
 }  // namespace
 
+namespace cfm {
+
+// Standard persistent CG on a stencil operator with iterate snapshots (the
+// training data of the learned preconditioner): solves A x = b (device
+// vectors, x0 = 0) to tol, storing x after every `every`-th iteration into
+// snap (up to `max_snaps` n-vectors).  Returns the status; *iters and
+// *taken (snapshots written) optional.
+int cg_stencil_snapshots(const cfm_stencil *S, const double *b_dev, double *x_dev, double tol,
+                         int maxiter, double *snap, int every, int max_snaps, long long *iters,
+                         int *taken, cudaStream_t stream) {
+    CFM_ARG_CHECK(S && b_dev && x_dev && every > 0 && max_snaps >= 0, "snapshot solve arguments");
+    cfm_cg_params p{};
+    p.impl = CFM_CG_PERSISTENT;
+    p.maxiter = maxiter;
+    p.tol = tol;
+    cfm_cg *h = nullptr;
+    int st = cfm_cg_create_stencil(S, &p, &h);
+    if (st) return st;
+    if (stream) cfm_cg_set_stream(h, stream);
+    auto run = [&](auto op) -> int {
+        KArgs<decltype(op)> a = make_args(h, op, b_dev, x_dev);
+        a.snap = snap;
+        a.snap_every = every;
+        a.snap_max = max_snaps;
+        BarrierState bs{};
+        bs.timeout_ns = barrier_timeout_ns();
+        CFM_CUDA_TRY(cudaMemcpyAsync(h->bar, &bs, sizeof(bs), cudaMemcpyHostToDevice, h->stream));
+        void *args[] = {&a};
+        CFM_CUDA_TRY(launch_cooperative((const void *)cg_std_kernel<decltype(op)>, dim3(h->blocks),
+                                        dim3(CG_TILE), args, 0, h->stream));
+        CgResult r{};
+        CFM_CUDA_TRY(cudaMemcpyAsync(&bs, h->bar, sizeof(bs), cudaMemcpyDeviceToHost, h->stream));
+        CFM_CUDA_TRY(cudaMemcpyAsync(&r, h->res, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+        CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        if (bs.error) {
+            set_error("grid barrier %d timed out", bs.where);
+            return CFM_BARRIER_TIMEOUT;
+        }
+        if (iters) *iters = r.iters;
+        if (taken) *taken = (int)std::min<long long>(r.iters / every, max_snaps);
+        return r.status;
+    };
+    st = S->dims == 2 ? run(stencil_op<2>(S)) : run(stencil_op<3>(S));
+    cfm_cg_destroy(h);
+    return st;
+}
+
+// Device coefficient arrays of a stencil (we | wn | wt | dg, 4 n doubles).
+const double *stencil_coeffs(const cfm_stencil *S) { return S->c64; }
+void stencil_shape(const cfm_stencil *S, int *dims, int *nx, int *ny, int *nz) {
+    *dims = S->dims;
+    *nx = S->nx;
+    *ny = S->ny;
+    *nz = S->nz;
+}
+
+}  // namespace cfm
+
 extern "C" {
 
 int cfm_csr_create(int n, long long nnz, const int *rowptr, const int *col, const double *val,

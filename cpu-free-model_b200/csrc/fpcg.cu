@@ -1,0 +1,736 @@
+// Learned preconditioning on one GPU (no reference counterpart):
+//  - training pairs from plain CG: for fresh seeds, the 2D variable-
+//    coefficient problem is solved by the persistent FP64 CG kernel to
+//    1e-10 (x*), then again with iterate snapshots x_j; each pair is the
+//    residual r_j = b - A x_j (input, with log k) and the error
+//    e_j = x* - x_j (target), both scaled to unit RMS;
+//  - training of the U-Net (learned.cu) with a per-sample scale-invariant
+//    loss 1 - cos^2(net(r), e) (a preconditioner's output scale does not
+//    matter to flexible CG) and Adam;
+//  - flexible PCG (Notay 2000; Polak-Ribiere beta, clipped at 0) with
+//    z = M(r) = |r|_rms * net(r / |r|_rms, log k): FP64 vectors and dots,
+//    the network in BF16 on the tensor cores.  One iteration is a fixed
+//    kernel sequence; it is captured once into a CUDA graph whose
+//    conditional WHILE node repeats it on the device until the residual
+//    reaches the tolerance, so the host launches the whole solve once.
+//    If the loop stalls or hits its cap, plain FP64 persistent CG finishes
+//    from the current iterate (the fallback) and judges the result by the
+//    FP64 true residual.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <type_traits>
+#include <vector>
+
+#include "cfm_internal.h"
+#include "krylov.cuh"
+#include "learned_internal.h"
+
+namespace cfm {
+int cg_stencil_snapshots(const cfm_stencil *S, const double *b_dev, double *x_dev, double tol,
+                         int maxiter, double *snap, int every, int max_snaps, long long *iters,
+                         int *taken, cudaStream_t stream);
+const double *stencil_coeffs(const cfm_stencil *S);
+void stencil_shape(const cfm_stencil *S, int *dims, int *nx, int *ny, int *nz);
+}  // namespace cfm
+
+namespace cfm {
+
+namespace {
+
+StencilOp<2> op2(const cfm_stencil *S) {
+    int dims, nx, ny, nz;
+    stencil_shape(S, &dims, &nx, &ny, &nz);
+    const double *c = stencil_coeffs(S);
+    const size_t n = (size_t)nx * ny;
+    StencilOp<2> o{};
+    o.nx = nx;
+    o.ny = ny;
+    o.nz = 1;
+    o.we = c;
+    o.wn = c + n;
+    o.wt = c + 2 * n;
+    o.dg = c + 3 * n;
+    return o;
+}
+
+// ------------------------------------------------------- training data
+// r = b - A xj, e = xs - xj; accumulates |r|^2, |e|^2 into acc[0], acc[1].
+__global__ void k_pair(StencilOp<2> op, int n, const double *b, const double *xs, const double *xj,
+                       double *r, double *e, double *acc) {
+    __shared__ double red[2][32];
+    double rr = 0, ee = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double ri = b[i] - (xj ? op.apply(xj, i) : 0.0);
+        const double ei = xs[i] - (xj ? xj[i] : 0.0);
+        r[i] = ri;
+        e[i] = ei;
+        rr += ri * ri;
+        ee += ei * ei;
+    }
+    for (int o = 16; o; o >>= 1) {
+        rr += __shfl_xor_sync(CG_FULL, rr, o);
+        ee += __shfl_xor_sync(CG_FULL, ee, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = rr;
+        red[1][threadIdx.x >> 5] = ee;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, c = 0;
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) {
+            a += red[0][w];
+            c += red[1][w];
+        }
+        atomicAdd(acc, a);
+        atomicAdd(acc + 1, c);
+    }
+}
+
+// Network input [r / rms(r), g] and target e / rms(e) (FP32).
+__global__ void k_pair_store(int n, const double *r, const double *e, const float *g,
+                             const double *acc, float *xin, float *tgt) {
+    const double sr = acc[0] > 0 ? sqrt((double)n / acc[0]) : 0.0;
+    const double se = acc[1] > 0 ? sqrt((double)n / acc[1]) : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        xin[2 * i] = (float)(r[i] * sr);
+        xin[2 * i + 1] = g[i];
+        tgt[i] = (float)(e[i] * se);
+    }
+}
+
+// ------------------------------------------------------------- the loss
+// Per sample: s[0] = <u,t>, s[1] = <u,u>, s[2] = <t,t> (FP64 atomics).
+__global__ void k_loss_dots(const float *u, const float *t, int n, double *s) {
+    const int b = blockIdx.y;
+    u += (size_t)b * n;
+    t += (size_t)b * n;
+    __shared__ double red[3][32];
+    double ut = 0, uu = 0, tt = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double a = u[i], c = t[i];
+        ut += a * c;
+        uu += a * a;
+        tt += c * c;
+    }
+    for (int o = 16; o; o >>= 1) {
+        ut += __shfl_xor_sync(CG_FULL, ut, o);
+        uu += __shfl_xor_sync(CG_FULL, uu, o);
+        tt += __shfl_xor_sync(CG_FULL, tt, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = ut;
+        red[1][threadIdx.x >> 5] = uu;
+        red[2][threadIdx.x >> 5] = tt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, c = 0, d = 0;
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) {
+            a += red[0][w];
+            c += red[1][w];
+            d += red[2][w];
+        }
+        atomicAdd(s + 3 * b, a);
+        atomicAdd(s + 3 * b + 1, c);
+        atomicAdd(s + 3 * b + 2, d);
+    }
+}
+
+// L_b = 1 - <u,t>^2 / (|u|^2 |t|^2);  dL/du = 2 c (c_u u - t) / (|u|^2 |t|^2)
+// with c = <u,t>, c_u = <u,t> / |u|^2; the batch mean's gradient.
+__global__ void k_loss_grad(const float *u, const float *t, int n, int B, const double *s,
+                            float *dout, double *loss) {
+    const int b = blockIdx.y;
+    const double ut = s[3 * b], uu = s[3 * b + 1], tt = s[3 * b + 2];
+    const double den = uu * tt > 0 ? uu * tt : 1.0;
+    const double f = 2.0 * ut / den / B, cu = uu > 0 ? ut / uu : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const size_t j = (size_t)b * n + i;
+        dout[j] = (float)(f * (cu * u[j] - t[j]));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(loss, (1.0 - ut * ut / den) / B);
+}
+
+// ------------------------------------------------------------------ FPCG
+enum : int { FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_NSLOT = 5 };
+
+struct FpState {
+    double rz[2];        // <z, r> of the current direction (double-buffered by k parity)
+    double target;       // tol * |b|
+    double best_rr;      // smallest |r|^2 seen
+    long long k;         // iterations
+    long long best_k;    // iteration of best_rr
+    int done;            // 1 converged, 2 stalled / capped
+    int pad;
+};
+
+struct FpArgs {
+    StencilOp<2> op;
+    int n, ntiles;
+    const double *b;
+    double *x, *r, *rold, *p, *s, *z;
+    float *xin, *out;
+    double *part;
+    FpState *st;
+    long long maxiter;
+    int stall;
+};
+
+__device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.ntiles; }
+
+#define FP_ROW const int i = blockIdx.x * CG_TILE + threadIdx.x
+
+// x = 0, r = b; partials |b|^2, |r|^2.
+__global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
+    __shared__ double sm[33];
+    FP_ROW;
+    double bb = 0;
+    if (i < a.n) {
+        const double bi = a.b[i];
+        a.x[i] = 0.0;
+        a.r[i] = bi;
+        a.rold[i] = 0.0;
+        a.p[i] = 0.0;
+        bb = bi * bi;
+    }
+    bb = block_sum(bb, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_BB)[blockIdx.x] = bb;
+        fslot(a, FP_RR)[blockIdx.x] = bb;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->k = 0;
+        a.st->done = 0;
+        a.st->best_rr = 1e300;
+        a.st->best_k = 0;
+        a.st->rz[0] = a.st->rz[1] = 0;
+        a.st->target = -tol;  // resolved by k_fp_prep from |b|
+    }
+}
+
+// rr = |r|^2; convergence / stall test; network input channel 0 = r / rms(r).
+__global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
+    __shared__ double sm[33];
+    const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
+    const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);  // block-wide: every thread
+    const double scale = rr > 0 ? sqrt((double)a.n / rr) : 0.0;
+    FP_ROW;
+    if (i < a.n) a.xin[2 * i] = (float)(a.r[i] * scale);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        FpState *st = a.st;
+        double target = st->target;
+        if (target < 0) {  // first call: target = tol * |b|
+            target = -target * sqrt(bb);
+            st->target = target;
+        }
+        if (sqrt(rr) <= target) st->done = 1;
+        if (rr < st->best_rr) {
+            st->best_rr = rr;
+            st->best_k = st->k;
+        } else if (st->k - st->best_k > a.stall) {
+            st->done = 2;
+        }
+        if (st->k >= a.maxiter && !st->done) st->done = 2;
+    }
+}
+
+// z = out / scale (FP64); partials <z, r>, <z, r_old>.
+__global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a) {
+    __shared__ double sm[33];
+    const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
+    const double inv = rr > 0 ? sqrt(rr / (double)a.n) : 0.0;
+    FP_ROW;
+    double zr = 0, zro = 0;
+    if (i < a.n) {
+        const double zi = (double)a.out[i] * inv;
+        a.z[i] = zi;
+        zr = zi * a.r[i];
+        zro = zi * a.rold[i];
+    }
+    zr = block_sum(zr, sm);
+    zro = block_sum(zro, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_ZR)[blockIdx.x] = zr;
+        fslot(a, FP_ZRO)[blockIdx.x] = zro;
+    }
+}
+
+// beta = max(0, (<z,r> - <z,r_old>) / <z_old, r_old>) (0 on the first
+// step); p = z + beta p; and the loop condition.  <z, r> of direction k
+// lives in rz[(k + 1) & 1] (k = iterations done when it was formed), so the
+// value being read and the value being written never share a slot.
+__global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond,
+                                                    int set_cond) {
+    __shared__ double sm[33];
+    const double zr = sum_partials(fslot(a, FP_ZR), a.ntiles, sm);
+    const double zro = sum_partials(fslot(a, FP_ZRO), a.ntiles, sm);
+    const long long k = a.st->k;
+    const double rz_old = a.st->rz[k & 1];
+    double beta = 0.0;
+    if (k > 0 && rz_old != 0.0) beta = fmax(0.0, (zr - zro) / rz_old);
+    FP_ROW;
+    if (i < a.n) a.p[i] = a.z[i] + beta * a.p[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->rz[(k + 1) & 1] = zr;
+        if (set_cond) cudaGraphSetConditional(cond, a.st->done ? 0u : 1u);
+    }
+}
+
+// s = A p; partial <p, s>.
+__global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
+    __shared__ double sm[33];
+    FP_ROW;
+    double ps = 0;
+    if (i < a.n) {
+        const double si = a.op.apply(a.p, i);
+        a.s[i] = si;
+        ps = a.p[i] * si;
+    }
+    ps = block_sum(ps, sm);
+    if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
+}
+
+// alpha = <z, r> / <p, s>; x += alpha p; r_old = r; r -= alpha s; |r|^2.
+__global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
+    __shared__ double sm[33];
+    const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
+    const long long k = a.st->k;
+    const double rz = a.st->rz[(k + 1) & 1];
+    const double alpha = ps != 0.0 ? rz / ps : 0.0;
+    FP_ROW;
+    double rr = 0;
+    if (i < a.n) {
+        a.x[i] += alpha * a.p[i];
+        const double ri = a.r[i];
+        a.rold[i] = ri;
+        const double rn = ri - alpha * a.s[i];
+        a.r[i] = rn;
+        rr = rn * rn;
+    }
+    rr = block_sum(rr, sm);
+    if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
+}
+
+// k += 1 (its own launch: every block of the kernels around it reads k).
+__global__ void k_fp_tick(FpState *st) { st->k += 1; }
+
+// t = b - A x, |t|^2 (atomics; the reported true residual).
+__global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const double *x, double *t,
+                              double *acc) {
+    double q = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double ti = b[i] - op.apply(x, i);
+        t[i] = ti;
+        q += ti * ti;
+    }
+    for (int o = 16; o; o >>= 1) q += __shfl_xor_sync(CG_FULL, q, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(acc, q);
+}
+
+__global__ void k_log_f32(const double *k, float *xin, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        xin[2 * i + 1] = (float)log(k[i]);
+}
+
+__global__ void k_axpy_inplace(double *x, const double *d, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += d[i];
+}
+
+}  // namespace
+
+}  // namespace cfm
+
+using namespace cfm;
+
+struct cfm_fpcg {
+    const cfm_stencil *S = nullptr;
+    cfm_unet *net = nullptr;
+    int n = 0, ntiles = 0, nx = 0, ny = 0;
+    long long maxiter = 0;
+    double tol = 0;
+    double *vec = nullptr;  // x r rold p s z b t d (9 n)
+    float *xin = nullptr, *out = nullptr;
+    double *part = nullptr, *acc = nullptr;
+    FpState *st = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool conditional = false;
+};
+
+namespace {
+
+FpArgs fp_args(cfm_fpcg *h) {
+    FpArgs a{};
+    const size_t n = h->n;
+    a.op = op2(h->S);
+    a.n = h->n;
+    a.ntiles = h->ntiles;
+    a.x = h->vec;
+    a.r = h->vec + n;
+    a.rold = h->vec + 2 * n;
+    a.p = h->vec + 3 * n;
+    a.s = h->vec + 4 * n;
+    a.z = h->vec + 5 * n;
+    a.b = h->vec + 6 * n;
+    a.xin = h->xin;
+    a.out = h->out;
+    a.part = h->part;
+    a.st = h->st;
+    a.maxiter = h->maxiter;
+    a.stall = 200;
+    return a;
+}
+
+// One FPCG iteration's tail (from the preconditioner on): prep, network, z, dir.
+int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    cudaStream_t s = h->stream;
+    k_fp_prep<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    CFM_CUDA_TRY(cudaGetLastError());
+    int st = unet_forward(h->net->u, 1, h->xin, h->out, s);
+    if (st) return st;
+    k_fp_z<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    k_fp_dir<<<h->ntiles, CG_TILE, 0, s>>>(a, cond, set_cond);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    k_fp_spmv<<<h->ntiles, CG_TILE, 0, h->stream>>>(a);
+    k_fp_update<<<h->ntiles, CG_TILE, 0, h->stream>>>(a);
+    k_fp_tick<<<1, 1, 0, h->stream>>>(a.st);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return fp_precond_dir(h, a, cond, set_cond);
+}
+
+// Graph: a conditional WHILE node whose body is one FPCG iteration.
+int build_graph(cfm_fpcg *h) {
+    const FpArgs a = fp_args(h);
+    CFM_CUDA_TRY(cudaGraphCreate(&h->graph, 0));
+    cudaGraphConditionalHandle cond;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, h->graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        e = cudaGraphAddNode(&node, h->graph, nullptr, 0, &cp);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            CFM_CUDA_TRY(cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal));
+            int st = fp_body(h, a, cond, 1);
+            cudaGraph_t captured = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(h->stream, &captured);
+            if (st) return st;
+            CFM_CUDA_TRY(ce);
+            h->conditional = true;
+        }
+    }
+    if (!h->conditional) {
+        // no conditional nodes: a graph of 16 iterations the host relaunches
+        cudaGetLastError();
+        cudaGraphDestroy(h->graph);
+        h->graph = nullptr;
+        CFM_CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int st = 0;
+        for (int i = 0; i < 16 && !st; ++i) st = fp_body(h, a, 0, 0);
+        const cudaError_t ce = cudaStreamEndCapture(h->stream, &h->graph);
+        if (st) return st;
+        CFM_CUDA_TRY(ce);
+    }
+    CFM_CUDA_TRY(cudaGraphInstantiate(&h->exec, h->graph, 0));
+    return CFM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int maxiter,
+                    double tol, cfm_fpcg **out) {
+    clear_error();
+    CFM_ARG_CHECK(S && k_host && net && out, "null argument");
+    *out = nullptr;
+    int dims, nx, ny, nz;
+    stencil_shape(S, &dims, &nx, &ny, &nz);
+    CFM_ARG_CHECK(dims == 2, "the learned preconditioner is 2D");
+    CFM_ARG_CHECK(tol > 0 && maxiter > 0, "tol, maxiter");
+    int H = 0, W = 0;
+    unet_shape(net->u, &H, &W);
+    CFM_ARG_CHECK(H == ny && W == nx, "the network's grid must equal the stencil's");
+    cfm_fpcg *h = new cfm_fpcg();
+    h->S = S;
+    h->net = net;
+    h->nx = nx;
+    h->ny = ny;
+    h->n = nx * ny;
+    h->ntiles = (h->n + CG_TILE - 1) / CG_TILE;
+    h->maxiter = maxiter;
+    h->tol = tol;
+    const size_t n = h->n;
+    cudaError_t e;
+    std::vector<double> kk(k_host, k_host + n);
+    double *kd = nullptr;
+    if ((e = cudaMalloc(&h->vec, sizeof(double) * 9 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->xin, sizeof(float) * 2 * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->out, sizeof(float) * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->ntiles)) != cudaSuccess ||
+        (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess ||
+        (e = cudaMalloc(&kd, sizeof(double) * n)) != cudaSuccess ||
+        (e = cudaMemcpy(kd, kk.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaFree(kd);
+        cfm_fpcg_destroy(h);
+        CFM_CUDA_TRY(e);
+    }
+    k_log_f32<<<256, 256>>>(kd, h->xin, h->n);
+    e = cudaDeviceSynchronize();
+    cudaFree(kd);
+    if (e != cudaSuccess) {
+        cfm_fpcg_destroy(h);
+        CFM_CUDA_TRY(e);
+    }
+    *out = h;
+    return CFM_OK;
+}
+
+void cfm_fpcg_destroy(cfm_fpcg *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    cudaFree(h->vec);
+    cudaFree(h->xin);
+    cudaFree(h->out);
+    cudaFree(h->part);
+    cudaFree(h->acc);
+    cudaFree(h->st);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *stats) {
+    clear_error();
+    CFM_ARG_CHECK(h && b_host && x_host, "null argument");
+    const size_t n = h->n;
+    FpArgs a = fp_args(h);
+    cudaStream_t s = h->stream;
+    double *b = h->vec + 6 * n, *t = h->vec + 7 * n, *d = h->vec + 8 * n;
+    CFM_CUDA_TRY(cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    CFM_CUDA_TRY(cudaMemsetAsync(unet_err(h->net->u), 0, sizeof(int), s));
+    int st = 0;
+    if (!h->exec) {
+        // eager warm-up of the network (kernel attributes) before capture
+        if ((st = unet_forward(h->net->u, 1, h->xin, h->out, s))) return st;
+        CFM_CUDA_TRY(cudaStreamSynchronize(s));
+        if ((st = build_graph(h))) return st;
+    }
+    int launches = 0;
+    CFM_CUDA_TRY(cudaEventRecord(h->ev0, s));
+    k_fp_init<<<h->ntiles, CG_TILE, 0, s>>>(a, h->tol);
+    CFM_CUDA_TRY(cudaGetLastError());
+    if ((st = fp_precond_dir(h, a, 0, 0))) return st;
+    launches += 2;
+    FpState hs{};
+    if (h->conditional) {
+        CFM_CUDA_TRY(cudaGraphLaunch(h->exec, s));
+        ++launches;
+    } else {
+        for (;;) {
+            CFM_CUDA_TRY(cudaGraphLaunch(h->exec, s));
+            ++launches;
+            CFM_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+            CFM_CUDA_TRY(cudaStreamSynchronize(s));
+            if (hs.done) break;
+        }
+    }
+    CFM_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    // FP64 true residual; plain persistent CG finishes if FPCG fell short
+    CFM_CUDA_TRY(cudaMemsetAsync(h->acc, 0, sizeof(double) * 2, s));
+    k_fp_true_res<<<256, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc);
+    double acc[2] = {0, 0};
+    CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CFM_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((st = unet_check_err(h->net->u))) return st;
+    const double bnorm = hs.target / h->tol;
+    double tnorm = std::sqrt(acc[0]);
+    int fallback = 0;
+    long long fb_iters = 0;
+    int status = CFM_OK;
+    if (!(tnorm <= h->tol * bnorm)) {
+        fallback = 1;
+        const double tol2 = h->tol * bnorm / tnorm;
+        status = cg_stencil_snapshots(h->S, t, d, tol2, 50000, nullptr, 1, 0, &fb_iters, nullptr, s);
+        if (status != CFM_OK && status != CFM_NOT_CONVERGED) return status;
+        k_axpy_inplace<<<256, 256, 0, s>>>(a.x, d, h->n);
+        CFM_CUDA_TRY(cudaMemsetAsync(h->acc, 0, sizeof(double), s));
+        k_fp_true_res<<<256, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc);
+        CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+        launches += 3;
+    }
+    CFM_CUDA_TRY(cudaMemcpyAsync(x_host, a.x, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    CFM_CUDA_TRY(cudaEventRecord(h->ev1, s));
+    CFM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    CFM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    tnorm = std::sqrt(acc[0]);
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->seconds = ms * 1e-3;
+        stats->iterations = hs.k + fb_iters;
+        stats->residual = tnorm / bnorm;
+        stats->h2d_bytes = 8.0 * n;
+        stats->d2h_bytes = 8.0 * n;
+        stats->launches = launches;
+        stats->refinements = fallback;
+        stats->status = status;
+        stats->lups = (double)hs.k;  // FPCG iterations alone (before any fallback)
+    }
+    return status;
+}
+
+// Training data from plain CG runs (fresh seeds seed0 .. seed0 + nsys - 1)
+// and `epochs` passes of Adam over it; loss values of the first and last
+// epoch (mean per-sample 1 - cos^2) are returned.
+int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
+                           int batch, float lr, double *loss_first, double *loss_last,
+                           double *data_seconds, double *train_seconds) {
+    clear_error();
+    CFM_ARG_CHECK(net && nsys >= 1 && snaps >= 1 && epochs >= 1, "arguments");
+    CFM_ARG_CHECK(batch >= 1 && batch <= net->maxB, "batch must be in [1, max_batch]");
+    UNetImpl *u = net->u;
+    int H = 0, W = 0;
+    unet_shape(u, &H, &W);
+    const int n = H * W;
+    const int per = snaps + 1;  // + the initial residual b
+    const long long N = (long long)nsys * per;
+    cudaStream_t s = nullptr;
+    CFM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct Guard {
+        std::vector<void *> p;
+        cudaStream_t s;
+        ~Guard() {
+            if (s) cudaStreamSynchronize(s);
+            for (void *q : p) cudaFree(q);
+            if (s) cudaStreamDestroy(s);
+        }
+    } g{{}, s};
+    auto alloc = [&](auto **ptr, size_t bytes) -> cudaError_t {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(bytes, 1));
+        if (e == cudaSuccess) g.p.push_back(q);
+        *ptr = static_cast<std::remove_reference_t<decltype(**ptr)> *>(q);
+        return e;
+    };
+    float *xin_all, *tgt_all, *gf, *tgt_b, *out_b, *dout_b;
+    double *bd, *xs, *snap, *r, *e, *acc, *sums, *lossd;
+    CFM_CUDA_TRY(alloc(&xin_all, sizeof(float) * 2 * (size_t)n * N));
+    CFM_CUDA_TRY(alloc(&tgt_all, sizeof(float) * (size_t)n * N));
+    CFM_CUDA_TRY(alloc(&gf, sizeof(float) * n));
+    CFM_CUDA_TRY(alloc(&bd, sizeof(double) * n));
+    CFM_CUDA_TRY(alloc(&xs, sizeof(double) * n));
+    CFM_CUDA_TRY(alloc(&snap, sizeof(double) * (size_t)n * snaps));
+    CFM_CUDA_TRY(alloc(&r, sizeof(double) * n));
+    CFM_CUDA_TRY(alloc(&e, sizeof(double) * n));
+    CFM_CUDA_TRY(alloc(&acc, sizeof(double) * 2));
+    CFM_CUDA_TRY(alloc(&tgt_b, sizeof(float) * (size_t)n * batch));
+    CFM_CUDA_TRY(alloc(&out_b, sizeof(float) * (size_t)n * batch));
+    CFM_CUDA_TRY(alloc(&dout_b, sizeof(float) * (size_t)n * batch));
+    CFM_CUDA_TRY(alloc(&sums, sizeof(double) * 3 * batch));
+    CFM_CUDA_TRY(alloc(&lossd, sizeof(double)));
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<double> kh(n), fh(n);
+    std::vector<float> gh(n);
+    int st = 0;
+    for (int sy = 0; sy < nsys; ++sy) {
+        if ((st = cfm_varcoef_problem(2, W, H, 1, seed0 + sy, kh.data(), fh.data()))) return st;
+        for (int i = 0; i < n; ++i) gh[i] = (float)std::log(kh[i]);
+        cfm_stencil *S = nullptr;
+        if ((st = cfm_stencil_create(2, W, H, 1, kh.data(), &S))) return st;
+        CFM_CUDA_TRY(cudaMemcpyAsync(bd, fh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        CFM_CUDA_TRY(cudaMemcpyAsync(gf, gh.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        long long K = 0;
+        st = cg_stencil_snapshots(S, bd, xs, 1e-10, 200000, nullptr, 1, 0, &K, nullptr, s);
+        int taken = 0;
+        if (st == CFM_OK) {
+            // snapshots spread over the iterations that reach ~1e-7
+            const int every = (int)std::max(1LL, (long long)(0.8 * K) / (snaps + 1));
+            st = cg_stencil_snapshots(S, bd, r, 1e-10, (int)(every * (long long)snaps), snap, every,
+                                      snaps, nullptr, &taken, s);
+            if (st == CFM_NOT_CONVERGED) st = CFM_OK;
+        }
+        cfm_stencil_destroy(S);
+        if (st) return st;
+        cfm_stencil *S2 = nullptr;
+        if ((st = cfm_stencil_create(2, W, H, 1, kh.data(), &S2))) return st;
+        const StencilOp<2> o2 = op2(S2);
+        for (int j = 0; j < per; ++j) {
+            const double *xj = j == 0 ? nullptr : snap + (size_t)(std::min(j, std::max(taken, 1)) - 1) * n;
+            const size_t idx = (size_t)sy * per + j;
+            CFM_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
+            k_pair<<<256, 256, 0, s>>>(o2, n, bd, xs, xj, r, e, acc);
+            k_pair_store<<<256, 256, 0, s>>>(n, r, e, gf, acc, xin_all + idx * 2 * n, tgt_all + idx * n);
+        }
+        CFM_CUDA_TRY(cudaStreamSynchronize(s));
+        cfm_stencil_destroy(S2);
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    // training
+    std::mt19937_64 rng(seed0 ^ 0x5eedULL);
+    std::vector<long long> order(N);
+    for (long long i = 0; i < N; ++i) order[i] = i;
+    double first = 0, last = 0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(order.begin(), order.end(), rng);
+        double ep_loss = 0;
+        int nb = 0;
+        CFM_CUDA_TRY(cudaMemsetAsync(lossd, 0, sizeof(double), s));
+        for (long long i0 = 0; i0 + batch <= N; i0 += batch) {
+            for (int bi = 0; bi < batch; ++bi) {
+                const long long id = order[i0 + bi];
+                CFM_CUDA_TRY(cudaMemcpyAsync(net->xin + (size_t)bi * 2 * n, xin_all + (size_t)id * 2 * n,
+                                             sizeof(float) * 2 * n, cudaMemcpyDeviceToDevice, s));
+                CFM_CUDA_TRY(cudaMemcpyAsync(tgt_b + (size_t)bi * n, tgt_all + (size_t)id * n,
+                                             sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+            }
+            if ((st = unet_forward(u, batch, net->xin, out_b, s))) return st;
+            CFM_CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(double) * 3 * batch, s));
+            k_loss_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, tgt_b, n, sums);
+            k_loss_grad<<<dim3(64, batch), 256, 0, s>>>(out_b, tgt_b, n, batch, sums, dout_b, lossd);
+            CFM_CUDA_TRY(cudaMemsetAsync(unet_grad(u), 0, unet_params(u) * sizeof(float), s));
+            if ((st = unet_backward(u, batch, net->xin, dout_b, s))) return st;
+            if ((st = unet_adam(u, lr, 1.0f, s))) return st;
+            ++nb;
+        }
+        double l = 0;
+        CFM_CUDA_TRY(cudaMemcpyAsync(&l, lossd, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CFM_CUDA_TRY(cudaStreamSynchronize(s));
+        if ((st = unet_check_err(u))) return st;
+        ep_loss = nb ? l / nb : 0;
+        if (ep == 0) first = ep_loss;
+        last = ep_loss;
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    if (loss_first) *loss_first = first;
+    if (loss_last) *loss_last = last;
+    if (data_seconds) *data_seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (train_seconds) *train_seconds = std::chrono::duration<double>(t2 - t1).count();
+    return CFM_OK;
+}
+
+}  // extern "C"

@@ -153,6 +153,10 @@ struct KArgs {
     double tol;
     int inner_maxiter;
     double inner_tol;
+    // standard CG only: copy x after every snap_every-th iteration into
+    // snap[(k / snap_every - 1) * n ...] while fewer than snap_max are taken
+    double *snap;
+    int snap_every, snap_max;
 };
 
 #define CFM_TILES(a) for (int tile = blockIdx.x; tile < (a).ntiles; tile += gridDim.x)
@@ -236,6 +240,15 @@ __device__ void phase_true_residual(const KArgs<Op> &a, double *sm) {
 }
 
 template <class Op>
+__device__ void phase_snap(const KArgs<Op> &a, int slot_i) {
+    double *dst = a.snap + (size_t)slot_i * a.n;
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        if (i < a.n) dst[i] = a.x[i];
+    }
+}
+
+template <class Op>
 __device__ void phase_restart(const KArgs<Op> &a) {
     CFM_TILES(a) {
         CFM_ROW(a);
@@ -295,6 +308,8 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_std_kernel(KArgs<Op> a) {
         if (!grid_barrier(a.bar, gridDim.x, site++)) return;
         const double gamma1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
         ++k;
+        if (a.snap && k % a.snap_every == 0 && k / a.snap_every <= a.snap_max)
+            phase_snap(a, (int)(k / a.snap_every) - 1);  // x is stable until the next update
         if (use_tol && sqrt(gamma1) <= target) {
             phase_true_residual(a, sm);
             if (!grid_barrier(a.bar, gridDim.x, site++)) return;

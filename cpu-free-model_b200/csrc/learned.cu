@@ -433,6 +433,10 @@ void unet_destroy(UNetImpl *u) {
 }
 
 size_t unet_params(const UNetImpl *u) { return u->nparams; }
+void unet_shape(const UNetImpl *u, int *H, int *W) {
+    *H = u->H;
+    *W = u->W;
+}
 float *unet_theta(UNetImpl *u) { return u->theta; }
 float *unet_grad(UNetImpl *u) { return u->grad; }
 int *unet_err(UNetImpl *u) { return u->err; }
@@ -599,11 +603,6 @@ int unet_check_err(UNetImpl *u) {
 // ------------------------------------------------------------------ C ABI
 using namespace cfm;
 
-struct cfm_unet {
-    UNetImpl *u = nullptr;
-    float *xin = nullptr, *out = nullptr, *dout = nullptr;
-    int maxB = 0;
-};
 
 extern "C" {
 

@@ -22,6 +22,7 @@ struct UNetImpl;
 int unet_create(int H, int W, int max_batch, UNetImpl **out);
 void unet_destroy(UNetImpl *u);
 size_t unet_params(const UNetImpl *u);
+void unet_shape(const UNetImpl *u, int *H, int *W);
 float *unet_theta(UNetImpl *u);
 float *unet_grad(UNetImpl *u);
 int *unet_err(UNetImpl *u);
@@ -34,3 +35,10 @@ int unet_adam(UNetImpl *u, float lr, float grad_scale, cudaStream_t s);
 int unet_check_err(UNetImpl *u);
 
 }  // namespace cfm
+
+// The C-ABI handle of a network: the net and its host-call staging buffers.
+struct cfm_unet {
+    cfm::UNetImpl *u = nullptr;
+    float *xin = nullptr, *out = nullptr, *dout = nullptr;
+    int maxB = 0;
+};

@@ -316,6 +316,33 @@ int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *d
  * 0..13 = h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0, NHWC at its level. */
 int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *out);
 
+/* Training of the network for the 2D variable-coefficient problem on its
+ * H x W grid: nsys systems from fresh seeds seed0, seed0+1, ... (k = exp(GRF),
+ * f ~ N(0,1), cfm_varcoef_problem) are solved by plain persistent FP64 CG to
+ * 1e-10; from a second run, `snaps` iterates x_j spread over the solve plus
+ * x_0 = 0 give (snaps + 1) * nsys residual/error pairs (r_j = f - A x_j,
+ * e_j = x* - x_j); then `epochs` shuffled passes of Adam (lr, batch <=
+ * the net's max_batch) on the per-sample loss 1 - cos^2(net(r_j), e_j).
+ * Mean loss of the first and last epoch and the seconds spent on data and on
+ * training are returned (each pointer optional). */
+int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
+                           int batch, float lr, double *loss_first, double *loss_last,
+                           double *data_seconds, double *train_seconds);
+
+/* Flexible PCG (Polak-Ribiere beta) on a 2D stencil operator with the
+ * network as preconditioner z = |r| net(r / |r|, log k) (k_host: the cell
+ * coefficients the stencil was built from).  FP64 vectors and dots; one
+ * CUDA graph whose conditional while-node runs the iterations on the device.
+ * If the loop stalls or reaches maxiter, plain persistent FP64 CG finishes
+ * from the current iterate; stats->refinements = 1 then.  stats->iterations
+ * = FPCG iterations + fallback iterations; stats->lups = FPCG iterations.
+ * The network's grid must equal the stencil's. */
+typedef struct cfm_fpcg cfm_fpcg;
+int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int maxiter,
+                    double tol, cfm_fpcg **out);
+void cfm_fpcg_destroy(cfm_fpcg *h);
+int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
+
 /* -------------------------------------------------------------- testing */
 /* Launch a persistent kernel of `blocks` blocks (0 = device default) that
  * meets `rounds` grid barriers; when drop_block >= 0 that block skips its
