@@ -71,10 +71,11 @@ _SIGS = {
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
-                                          _c.c_float, _vp, _vp, _vp, _vp]),
-    "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_double, _vp]),
+                                          _c.c_float, _c.c_int, _vp, _vp, _vp, _vp]),
+    "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_destroy": (None, [_vp]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
+    "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -450,6 +451,7 @@ class UNet:
 
     def __init__(self, H, W, max_batch=1, seed=0):
         self.H, self.W, self.max_batch = H, W, max_batch
+        self.smooth = 0
         self.n = lib.cfm_unet_num_params()
         h = ctypes.c_void_p()
         check("cfm_unet_create", lib.cfm_unet_create(H, W, max_batch, seed, ctypes.byref(h)))
@@ -492,11 +494,12 @@ class UNet:
             out[name] = from_bf16_bits(a)
         return out
 
-    def train_varcoef(self, nsys, snaps, seed0, epochs, batch, lr=1e-3):
+    def train_varcoef(self, nsys, snaps, seed0, epochs, batch, lr=1e-3, smooth=0):
         """Plain-CG training pairs + Adam; returns dict(loss_first, loss_last, data_s, train_s)."""
         v = [ctypes.c_double() for _ in range(4)]
+        self.smooth = smooth
         check("cfm_unet_train_varcoef",
-              lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr,
+              lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth,
                                          *[ctypes.byref(x) for x in v]))
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
 
@@ -511,11 +514,15 @@ class UNet:
 class FPCG:
     """Flexible PCG with the network as preconditioner (cfm_fpcg)."""
 
-    def __init__(self, S, k, net, maxiter=5000, tol=1e-8):
+    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None):
         self.S, self.net = S, net
         self.k = np.ascontiguousarray(k, np.float64)
         h = ctypes.c_void_p()
-        check("cfm_fpcg_create", lib.cfm_fpcg_create(S.h, _ptr(self.k), net.h, maxiter, tol, ctypes.byref(h)))
+        self.maxiter = maxiter
+        if smooth is None:
+            smooth = getattr(net, "smooth", 0) if net is not None else 0
+        check("cfm_fpcg_create", lib.cfm_fpcg_create(S.h, _ptr(self.k), None if net is None else net.h,
+                                                     smooth, maxiter, tol, ctypes.byref(h)))
         self.h = h
 
     def close(self):
@@ -524,6 +531,12 @@ class FPCG:
             self.h = None
 
     __del__ = close
+
+    def history(self):
+        out = np.empty(self.maxiter + 1)
+        n = ctypes.c_longlong()
+        check("cfm_fpcg_history", lib.cfm_fpcg_history(self.h, _ptr(out), len(out), ctypes.byref(n)))
+        return out[:n.value]
 
     def solve(self, b, allowed=(OK, NOT_CONVERGED)):
         b = np.ascontiguousarray(b, np.float64).reshape(-1)

@@ -421,8 +421,10 @@ int cg_stencil_snapshots(const cfm_stencil *S, const double *b_dev, double *x_de
     return st;
 }
 
-// Device coefficient arrays of a stencil (we | wn | wt | dg, 4 n doubles).
+// Device coefficient arrays of a stencil (we | wn | wt | dg, 4 n doubles,
+// and their FP32 copies).
 const double *stencil_coeffs(const cfm_stencil *S) { return S->c64; }
+const float *stencil_coeffs32(const cfm_stencil *S) { return S->c32; }
 void stencil_shape(const cfm_stencil *S, int *dims, int *nx, int *ny, int *nz) {
     *dims = S->dims;
     *nx = S->nx;

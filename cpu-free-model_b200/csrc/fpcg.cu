@@ -4,9 +4,11 @@
 //    1e-10 (x*), then again with iterate snapshots x_j; each pair is the
 //    residual r_j = b - A x_j (input, with log k) and the error
 //    e_j = x* - x_j (target), both scaled to unit RMS;
-//  - training of the U-Net (learned.cu) with a per-sample scale-invariant
-//    loss 1 - cos^2(net(r), e) (a preconditioner's output scale does not
-//    matter to flexible CG) and Adam;
+//  - training of the U-Net (learned.cu) with Adam on the per-sample
+//    energy-norm loss 1 - <z, r>^2 / (<z, A z> <e, r>), z = net(r): one minus
+//    the fraction of the A-norm error ||e||_A^2 a CG step along z removes.
+//    It is blind to the output's scale (which flexible CG ignores) and,
+//    unlike an L2 loss, punishes output noise that A amplifies;
 //  - flexible PCG (Notay 2000; Polak-Ribiere beta, clipped at 0) with
 //    z = M(r) = |r|_rms * net(r / |r|_rms, log k): FP64 vectors and dots,
 //    the network in BF16 on the tensor cores.  One iteration is a fixed
@@ -36,12 +38,19 @@ int cg_stencil_snapshots(const cfm_stencil *S, const double *b_dev, double *x_de
                          int maxiter, double *snap, int every, int max_snaps, long long *iters,
                          int *taken, cudaStream_t stream);
 const double *stencil_coeffs(const cfm_stencil *S);
+const float *stencil_coeffs32(const cfm_stencil *S);
 void stencil_shape(const cfm_stencil *S, int *dims, int *nx, int *ny, int *nz);
 }  // namespace cfm
 
 namespace cfm {
 
 namespace {
+
+// n-vectors in cfm_fpcg::vec: x r rold p s z b t d za zb r1.
+constexpr int FP_NVEC = 12;
+
+// Damping of the Jacobi smoothing sweeps around the network.
+constexpr double JACOBI_OMEGA = 0.8;
 
 StencilOp<2> op2(const cfm_stencil *S) {
     int dims, nx, ny, nz;
@@ -61,25 +70,26 @@ StencilOp<2> op2(const cfm_stencil *S) {
 
 // ------------------------------------------------------- training data
 // r = b - A xj, e = xs - xj; accumulates |r|^2, |e|^2 into acc[0], acc[1].
+// r = b - A xj, e = xs - xj; accumulates |r|^2, <e, r> into acc[0], acc[1].
 __global__ void k_pair(StencilOp<2> op, int n, const double *b, const double *xs, const double *xj,
                        double *r, double *e, double *acc) {
     __shared__ double red[2][32];
-    double rr = 0, ee = 0;
+    double rr = 0, er = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double ri = b[i] - (xj ? op.apply(xj, i) : 0.0);
         const double ei = xs[i] - (xj ? xj[i] : 0.0);
         r[i] = ri;
         e[i] = ei;
         rr += ri * ri;
-        ee += ei * ei;
+        er += ei * ri;
     }
     for (int o = 16; o; o >>= 1) {
         rr += __shfl_xor_sync(CG_FULL, rr, o);
-        ee += __shfl_xor_sync(CG_FULL, ee, o);
+        er += __shfl_xor_sync(CG_FULL, er, o);
     }
     if ((threadIdx.x & 31) == 0) {
         red[0][threadIdx.x >> 5] = rr;
-        red[1][threadIdx.x >> 5] = ee;
+        red[1][threadIdx.x >> 5] = er;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -93,73 +103,126 @@ __global__ void k_pair(StencilOp<2> op, int n, const double *b, const double *xs
     }
 }
 
-// Network input [r / rms(r), g] and target e / rms(e) (FP32).
-__global__ void k_pair_store(int n, const double *r, const double *e, const float *g,
-                             const double *acc, float *xin, float *tgt) {
-    const double sr = acc[0] > 0 ? sqrt((double)n / acc[0]) : 0.0;
-    const double se = acc[1] > 0 ? sqrt((double)n / acc[1]) : 0.0;
+// Damped Jacobi sweep for the training pairs: zout = zin + omega (r - A zin) / diag.
+__global__ void k_data_jacobi(StencilOp<2> op, int n, const double *r, const double *zin,
+                              double *zout) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        xin[2 * i] = (float)(r[i] * sr);
-        xin[2 * i + 1] = g[i];
-        tgt[i] = (float)(e[i] * se);
+        const double res = zin ? r[i] - op.apply(zin, i) : r[i];
+        zout[i] = (zin ? zin[i] : 0.0) + JACOBI_OMEGA * res / op.dg[i];
     }
 }
 
-// ------------------------------------------------------------- the loss
-// Per sample: s[0] = <u,t>, s[1] = <u,u>, s[2] = <t,t> (FP64 atomics).
-__global__ void k_loss_dots(const float *u, const float *t, int n, double *s) {
-    const int b = blockIdx.y;
-    u += (size_t)b * n;
-    t += (size_t)b * n;
-    __shared__ double red[3][32];
-    double ut = 0, uu = 0, tt = 0;
+// After pre-smoothing z: r <- r - A z, e <- e - z (the pair the network sees
+// inside the preconditioner); |r|^2, <e, r> into acc (fresh).
+__global__ void k_data_smoothed(StencilOp<2> op, int n, const double *z, double *r, double *e,
+                                double *r1, double *acc) {
+    __shared__ double red[2][32];
+    double rr = 0, er = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double a = u[i], c = t[i];
-        ut += a * c;
-        uu += a * a;
-        tt += c * c;
+        const double ri = r[i] - op.apply(z, i);
+        const double ei = e[i] - z[i];
+        r1[i] = ri;
+        e[i] = ei;
+        rr += ri * ri;
+        er += ei * ri;
     }
     for (int o = 16; o; o >>= 1) {
-        ut += __shfl_xor_sync(CG_FULL, ut, o);
-        uu += __shfl_xor_sync(CG_FULL, uu, o);
-        tt += __shfl_xor_sync(CG_FULL, tt, o);
+        rr += __shfl_xor_sync(CG_FULL, rr, o);
+        er += __shfl_xor_sync(CG_FULL, er, o);
     }
     if ((threadIdx.x & 31) == 0) {
-        red[0][threadIdx.x >> 5] = ut;
-        red[1][threadIdx.x >> 5] = uu;
-        red[2][threadIdx.x >> 5] = tt;
+        red[0][threadIdx.x >> 5] = rr;
+        red[1][threadIdx.x >> 5] = er;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double a = 0, c = 0, d = 0;
+        double a = 0, c = 0;
         for (int w = 0; w < (int)blockDim.x / 32; ++w) {
             a += red[0][w];
             c += red[1][w];
-            d += red[2][w];
         }
-        atomicAdd(s + 3 * b, a);
-        atomicAdd(s + 3 * b + 1, c);
-        atomicAdd(s + 3 * b + 2, d);
+        atomicAdd(acc, a);
+        atomicAdd(acc + 1, c);
     }
 }
 
-// L_b = 1 - <u,t>^2 / (|u|^2 |t|^2);  dL/du = 2 c (c_u u - t) / (|u|^2 |t|^2)
-// with c = <u,t>, c_u = <u,t> / |u|^2; the batch mean's gradient.
-__global__ void k_loss_grad(const float *u, const float *t, int n, int B, const double *s,
-                            float *dout, double *loss) {
+// Network input [r / rms(r), g] (FP32) and the sample's <e, r> at that
+// scale: <e / rms(r), r / rms(r)> = <e, r> n / |r|^2.
+__global__ void k_pair_store(int n, const double *r, const float *g, const double *acc, float *xin,
+                             double *er_out) {
+    const double sr = acc[0] > 0 ? sqrt((double)n / acc[0]) : 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        xin[2 * i] = (float)(r[i] * sr);
+        xin[2 * i + 1] = g[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *er_out = acc[1] * sr * sr;
+}
+
+// ------------------------------------------------------------- the loss
+// Per batch element b (sample ids[b] of system ids[b] / per, whose FP32
+// stencil coefficients we | wn | dg sit at coef + sys * 3 n):
+//   Az = A z (FP32 apply), s[0] = <z, r>, s[1] = <z, A z>  (FP64 atomics),
+// with r = channel 0 of the network input.
+__global__ void k_loss_anorm_dots(const float *z, const float *xin, const float *coef,
+                                  const long long *ids, int per, int nx, int ny, float *Az,
+                                  double *s) {
+    const int b = blockIdx.y, n = nx * ny;
+    const float *c = coef + (size_t)(ids[b] / per) * 3 * n;
+    const float *we = c, *wn = c + n, *dg = c + 2 * n;
+    z += (size_t)b * n;
+    xin += (size_t)b * 2 * n;
+    Az += (size_t)b * n;
+    __shared__ double red[2][32];
+    double zr = 0, zaz = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ix = i % nx, iy = i / nx;
+        float t = dg[i] * z[i];
+        if (ix > 0) t -= we[i - 1] * z[i - 1];
+        if (ix < nx - 1) t -= we[i] * z[i + 1];
+        if (iy > 0) t -= wn[i - nx] * z[i - nx];
+        if (iy < ny - 1) t -= wn[i] * z[i + nx];
+        Az[i] = t;
+        zr += (double)z[i] * xin[2 * i];
+        zaz += (double)z[i] * t;
+    }
+    for (int o = 16; o; o >>= 1) {
+        zr += __shfl_xor_sync(CG_FULL, zr, o);
+        zaz += __shfl_xor_sync(CG_FULL, zaz, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = zr;
+        red[1][threadIdx.x >> 5] = zaz;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, q = 0;
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) {
+            a += red[0][w];
+            q += red[1][w];
+        }
+        atomicAdd(s + 2 * b, a);
+        atomicAdd(s + 2 * b + 1, q);
+    }
+}
+
+// L_b = 1 - a^2 / (q c), a = <z, r>, q = <z, A z>, c = <e, r>;
+// dL_b/dz = (2 a / (q c)) ((a / q) A z - r); the batch mean and its gradient.
+__global__ void k_loss_anorm_grad(const float *Az, const float *xin, const double *s,
+                                  const double *er, const long long *ids, int n, int B,
+                                  float *dout, double *loss) {
     const int b = blockIdx.y;
-    const double ut = s[3 * b], uu = s[3 * b + 1], tt = s[3 * b + 2];
-    const double den = uu * tt > 0 ? uu * tt : 1.0;
-    const double f = 2.0 * ut / den / B, cu = uu > 0 ? ut / uu : 0.0;
+    const double a = s[2 * b], q = s[2 * b + 1], c = er[ids[b]];
+    const bool ok = q > 0 && c > 0;
+    const double f = ok ? 2.0 * a / (q * c) / B : 0.0, aq = ok ? a / q : 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const size_t j = (size_t)b * n + i;
-        dout[j] = (float)(f * (cu * u[j] - t[j]));
+        dout[j] = (float)(f * (aq * Az[j] - (double)xin[2 * j]));
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(loss, (1.0 - ut * ut / den) / B);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ok) atomicAdd(loss, (1.0 - a * a / (q * c)) / B);
 }
 
 // ------------------------------------------------------------------ FPCG
-enum : int { FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_NSLOT = 5 };
+enum : int { FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_R1 = 5, FP_NSLOT = 6 };
 
 struct FpState {
     double rz[2];        // <z, r> of the current direction (double-buffered by k parity)
@@ -176,9 +239,11 @@ struct FpArgs {
     int n, ntiles;
     const double *b;
     double *x, *r, *rold, *p, *s, *z;
+    double *za, *zb, *r1;  // smoothing iterates, smoothed residual
     float *xin, *out;
     double *part;
     FpState *st;
+    double *hist;  // |r| before each preconditioner application (maxiter + 1 entries)
     long long maxiter;
     int stall;
 };
@@ -215,14 +280,11 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
     }
 }
 
-// rr = |r|^2; convergence / stall test; network input channel 0 = r / rms(r).
+// rr = |r|^2; convergence / stall test (block 0).
 __global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
     __shared__ double sm[33];
     const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
     const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);  // block-wide: every thread
-    const double scale = rr > 0 ? sqrt((double)a.n / rr) : 0.0;
-    FP_ROW;
-    if (i < a.n) a.xin[2 * i] = (float)(a.r[i] * scale);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         FpState *st = a.st;
         double target = st->target;
@@ -230,6 +292,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
             target = -target * sqrt(bb);
             st->target = target;
         }
+        if (st->k <= a.maxiter) a.hist[st->k] = sqrt(rr);
         if (sqrt(rr) <= target) st->done = 1;
         if (rr < st->best_rr) {
             st->best_rr = rr;
@@ -241,15 +304,60 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
     }
 }
 
-// z = out / scale (FP64); partials <z, r>, <z, r_old>.
-__global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a) {
+// Damped Jacobi sweep on A z = r: zout = zin + omega (r - A zin) / diag
+// (zin == nullptr: zout = omega r / diag).
+__global__ void k_fp_jacobi(FpArgs a, const double *zin, double *zout) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double res = zin ? a.r[i] - a.op.apply(zin, i) : a.r[i];
+        zout[i] = (zin ? zin[i] : 0.0) + JACOBI_OMEGA * res / a.op.dg[i];
+    }
+}
+
+// r1 = r - A zc (zc == nullptr: r1 = r) and partial |r1|^2.
+__global__ void __launch_bounds__(CG_TILE) k_fp_r1(FpArgs a, const double *zc) {
     __shared__ double sm[33];
-    const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
-    const double inv = rr > 0 ? sqrt(rr / (double)a.n) : 0.0;
+    FP_ROW;
+    double q = 0;
+    if (i < a.n) {
+        const double v = zc ? a.r[i] - a.op.apply(zc, i) : a.r[i];
+        a.r1[i] = v;
+        q = v * v;
+    }
+    q = block_sum(q, sm);
+    if (threadIdx.x == 0) fslot(a, FP_R1)[blockIdx.x] = q;
+}
+
+// Network input channel 0 = r1 / rms(r1).
+__global__ void __launch_bounds__(CG_TILE) k_fp_in(FpArgs a) {
+    __shared__ double sm[33];
+    const double q = sum_partials(fslot(a, FP_R1), a.ntiles, sm);
+    const double scale = q > 0 ? sqrt((double)a.n / q) : 0.0;
+    FP_ROW;
+    if (i < a.n) a.xin[2 * i] = (float)(a.r1[i] * scale);
+}
+
+// Identity in place of the network: out = the normalised r1.
+__global__ void k_fp_identity(FpArgs a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        a.out[i] = a.xin[2 * i];
+}
+
+// zout = zc + rms(r1) out (zc == nullptr: 0).
+__global__ void __launch_bounds__(CG_TILE) k_fp_corr(FpArgs a, const double *zc, double *zout) {
+    __shared__ double sm[33];
+    const double q = sum_partials(fslot(a, FP_R1), a.ntiles, sm);
+    const double inv = q > 0 ? sqrt(q / (double)a.n) : 0.0;
+    FP_ROW;
+    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + (double)a.out[i] * inv;
+}
+
+// z = zf; partials <z, r>, <z, r_old>.
+__global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a, const double *zf) {
+    __shared__ double sm[33];
     FP_ROW;
     double zr = 0, zro = 0;
     if (i < a.n) {
-        const double zi = (double)a.out[i] * inv;
+        const double zi = zf[i];
         a.z[i] = zi;
         zr = zi * a.r[i];
         zro = zi * a.rold[i];
@@ -355,15 +463,17 @@ struct cfm_fpcg {
     int n = 0, ntiles = 0, nx = 0, ny = 0;
     long long maxiter = 0;
     double tol = 0;
-    double *vec = nullptr;  // x r rold p s z b t d (9 n)
+    double *vec = nullptr;  // x r rold p s z b t d za zb r1 (12 n)
+    int smooth = 0;
     float *xin = nullptr, *out = nullptr;
-    double *part = nullptr, *acc = nullptr;
+    double *part = nullptr, *acc = nullptr, *hist = nullptr;
     FpState *st = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool conditional = false;
+    long long last_k = 0;
 };
 
 namespace {
@@ -381,23 +491,51 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.s = h->vec + 4 * n;
     a.z = h->vec + 5 * n;
     a.b = h->vec + 6 * n;
+    a.za = h->vec + 9 * n;
+    a.zb = h->vec + 10 * n;
+    a.r1 = h->vec + 11 * n;
+    static_assert(FP_NVEC == 12, "x r rold p s z b t d za zb r1");
     a.xin = h->xin;
     a.out = h->out;
     a.part = h->part;
     a.st = h->st;
+    a.hist = h->hist;
     a.maxiter = h->maxiter;
     a.stall = 200;
     return a;
 }
 
-// One FPCG iteration's tail (from the preconditioner on): prep, network, z, dir.
+// One FPCG iteration's tail (from the preconditioner on): convergence test,
+// z = M(r) = post-smooth(pre-smooth(r) + rms(r1) net(r1 / rms(r1), log k))
+// with r1 = r - A pre-smooth(r) and `smooth` damped Jacobi sweeps on each
+// side, then the new direction.
 int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
     cudaStream_t s = h->stream;
     k_fp_prep<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    double *buf[2] = {a.za, a.zb};
+    const double *cur = nullptr;
+    int nb = 0;
+    for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
+        k_fp_jacobi<<<256, 256, 0, s>>>(a, cur, buf[nb]);
+        cur = buf[nb];
+    }
+    k_fp_r1<<<h->ntiles, CG_TILE, 0, s>>>(a, cur);
+    k_fp_in<<<h->ntiles, CG_TILE, 0, s>>>(a);
     CFM_CUDA_TRY(cudaGetLastError());
-    int st = unet_forward(h->net->u, 1, h->xin, h->out, s);
-    if (st) return st;
-    k_fp_z<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    if (h->net) {
+        int st = unet_forward(h->net->u, 1, h->xin, h->out, s);
+        if (st) return st;
+    } else {
+        k_fp_identity<<<256, 256, 0, s>>>(a);
+    }
+    k_fp_corr<<<h->ntiles, CG_TILE, 0, s>>>(a, cur, buf[nb]);
+    cur = buf[nb];
+    nb ^= 1;
+    for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
+        k_fp_jacobi<<<256, 256, 0, s>>>(a, cur, buf[nb]);
+        cur = buf[nb];
+    }
+    k_fp_z<<<h->ntiles, CG_TILE, 0, s>>>(a, cur);
     k_fp_dir<<<h->ntiles, CG_TILE, 0, s>>>(a, cond, set_cond);
     CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
@@ -457,19 +595,24 @@ int build_graph(cfm_fpcg *h) {
 
 extern "C" {
 
-int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int maxiter,
-                    double tol, cfm_fpcg **out) {
+int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int smooth,
+                    int maxiter, double tol, cfm_fpcg **out) {
     clear_error();
-    CFM_ARG_CHECK(S && k_host && net && out, "null argument");
+    CFM_ARG_CHECK(S && k_host && out, "null argument");
     *out = nullptr;
     int dims, nx, ny, nz;
     stencil_shape(S, &dims, &nx, &ny, &nz);
     CFM_ARG_CHECK(dims == 2, "the learned preconditioner is 2D");
     CFM_ARG_CHECK(tol > 0 && maxiter > 0, "tol, maxiter");
-    int H = 0, W = 0;
-    unet_shape(net->u, &H, &W);
-    CFM_ARG_CHECK(H == ny && W == nx, "the network's grid must equal the stencil's");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
+    if (net) {
+        int H = 0, W = 0;
+        unet_shape(net->u, &H, &W);
+        CFM_ARG_CHECK(H == ny && W == nx, "the network's grid must equal the stencil's");
+        CFM_ARG_CHECK(smooth == net->smooth, "smooth must equal the sweeps the network was trained with");
+    }
     cfm_fpcg *h = new cfm_fpcg();
+    h->smooth = smooth;
     h->S = S;
     h->net = net;
     h->nx = nx;
@@ -482,12 +625,13 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     cudaError_t e;
     std::vector<double> kk(k_host, k_host + n);
     double *kd = nullptr;
-    if ((e = cudaMalloc(&h->vec, sizeof(double) * 9 * n)) != cudaSuccess ||
+    if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->xin, sizeof(float) * 2 * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->out, sizeof(float) * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->ntiles)) != cudaSuccess ||
         (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
+        (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess ||
         (e = cudaMalloc(&kd, sizeof(double) * n)) != cudaSuccess ||
@@ -518,6 +662,7 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     cudaFree(h->part);
     cudaFree(h->acc);
     cudaFree(h->st);
+    cudaFree(h->hist);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -532,11 +677,11 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     cudaStream_t s = h->stream;
     double *b = h->vec + 6 * n, *t = h->vec + 7 * n, *d = h->vec + 8 * n;
     CFM_CUDA_TRY(cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    CFM_CUDA_TRY(cudaMemsetAsync(unet_err(h->net->u), 0, sizeof(int), s));
+    if (h->net) CFM_CUDA_TRY(cudaMemsetAsync(unet_err(h->net->u), 0, sizeof(int), s));
     int st = 0;
     if (!h->exec) {
         // eager warm-up of the network (kernel attributes) before capture
-        if ((st = unet_forward(h->net->u, 1, h->xin, h->out, s))) return st;
+        if (h->net && (st = unet_forward(h->net->u, 1, h->xin, h->out, s))) return st;
         CFM_CUDA_TRY(cudaStreamSynchronize(s));
         if ((st = build_graph(h))) return st;
     }
@@ -566,7 +711,8 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     double acc[2] = {0, 0};
     CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
     CFM_CUDA_TRY(cudaStreamSynchronize(s));
-    if ((st = unet_check_err(h->net->u))) return st;
+    if (h->net && (st = unet_check_err(h->net->u))) return st;
+    h->last_k = hs.k;
     const double bnorm = hs.target / h->tol;
     double tnorm = std::sqrt(acc[0]);
     int fallback = 0;
@@ -604,14 +750,25 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     return status;
 }
 
+// |r| before each preconditioner application of the last solve (k + 1 values).
+int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out) {
+    CFM_ARG_CHECK(h && out && n_out, "null argument");
+    const long long n = std::min(max_n, std::min(h->last_k + 1, h->maxiter + 1));
+    CFM_CUDA_TRY(cudaMemcpy(out, h->hist, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    *n_out = n;
+    return CFM_OK;
+}
+
 // Training data from plain CG runs (fresh seeds seed0 .. seed0 + nsys - 1)
 // and `epochs` passes of Adam over it; loss values of the first and last
 // epoch (mean per-sample 1 - cos^2) are returned.
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
-                           int batch, float lr, double *loss_first, double *loss_last,
+                           int batch, float lr, int smooth, double *loss_first, double *loss_last,
                            double *data_seconds, double *train_seconds) {
     clear_error();
     CFM_ARG_CHECK(net && nsys >= 1 && snaps >= 1 && epochs >= 1, "arguments");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
+    net->smooth = smooth;
     CFM_ARG_CHECK(batch >= 1 && batch <= net->maxB, "batch must be in [1, max_batch]");
     UNetImpl *u = net->u;
     int H = 0, W = 0;
@@ -637,10 +794,13 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         *ptr = static_cast<std::remove_reference_t<decltype(**ptr)> *>(q);
         return e;
     };
-    float *xin_all, *tgt_all, *gf, *tgt_b, *out_b, *dout_b;
-    double *bd, *xs, *snap, *r, *e, *acc, *sums, *lossd;
+    float *xin_all, *coef_all, *gf, *az_b, *out_b, *dout_b;
+    double *bd, *xs, *snap, *r, *e, *acc, *sums, *lossd, *er_all;
+    long long *ids_d;
     CFM_CUDA_TRY(alloc(&xin_all, sizeof(float) * 2 * (size_t)n * N));
-    CFM_CUDA_TRY(alloc(&tgt_all, sizeof(float) * (size_t)n * N));
+    CFM_CUDA_TRY(alloc(&coef_all, sizeof(float) * 3 * (size_t)n * nsys));
+    CFM_CUDA_TRY(alloc(&er_all, sizeof(double) * N));
+    CFM_CUDA_TRY(alloc(&ids_d, sizeof(long long) * batch));
     CFM_CUDA_TRY(alloc(&gf, sizeof(float) * n));
     CFM_CUDA_TRY(alloc(&bd, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&xs, sizeof(double) * n));
@@ -648,10 +808,13 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
     CFM_CUDA_TRY(alloc(&r, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&e, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&acc, sizeof(double) * 2));
-    CFM_CUDA_TRY(alloc(&tgt_b, sizeof(float) * (size_t)n * batch));
+    double *zs, *r1s;
+    CFM_CUDA_TRY(alloc(&zs, sizeof(double) * 2 * n));
+    CFM_CUDA_TRY(alloc(&r1s, sizeof(double) * n));
+    CFM_CUDA_TRY(alloc(&az_b, sizeof(float) * (size_t)n * batch));
     CFM_CUDA_TRY(alloc(&out_b, sizeof(float) * (size_t)n * batch));
     CFM_CUDA_TRY(alloc(&dout_b, sizeof(float) * (size_t)n * batch));
-    CFM_CUDA_TRY(alloc(&sums, sizeof(double) * 3 * batch));
+    CFM_CUDA_TRY(alloc(&sums, sizeof(double) * 2 * batch));
     CFM_CUDA_TRY(alloc(&lossd, sizeof(double)));
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<double> kh(n), fh(n);
@@ -679,12 +842,29 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         cfm_stencil *S2 = nullptr;
         if ((st = cfm_stencil_create(2, W, H, 1, kh.data(), &S2))) return st;
         const StencilOp<2> o2 = op2(S2);
+        const float *c32 = stencil_coeffs32(S2);  // we | wn | wt | dg
+        float *cdst = coef_all + (size_t)sy * 3 * n;
+        CFM_CUDA_TRY(cudaMemcpyAsync(cdst, c32, sizeof(float) * 2 * n, cudaMemcpyDeviceToDevice, s));
+        CFM_CUDA_TRY(cudaMemcpyAsync(cdst + 2 * (size_t)n, c32 + 3 * (size_t)n, sizeof(float) * n,
+                                     cudaMemcpyDeviceToDevice, s));
         for (int j = 0; j < per; ++j) {
             const double *xj = j == 0 ? nullptr : snap + (size_t)(std::min(j, std::max(taken, 1)) - 1) * n;
             const size_t idx = (size_t)sy * per + j;
             CFM_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
             k_pair<<<256, 256, 0, s>>>(o2, n, bd, xs, xj, r, e, acc);
-            k_pair_store<<<256, 256, 0, s>>>(n, r, e, gf, acc, xin_all + idx * 2 * n, tgt_all + idx * n);
+            const double *rin = r;
+            if (smooth > 0) {
+                double *zz[2] = {zs, zs + n};
+                const double *cur = nullptr;
+                for (int q = 0; q < smooth; ++q) {
+                    k_data_jacobi<<<256, 256, 0, s>>>(o2, n, r, cur, zz[q & 1]);
+                    cur = zz[q & 1];
+                }
+                CFM_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
+                k_data_smoothed<<<256, 256, 0, s>>>(o2, n, cur, r, e, r1s, acc);
+                rin = r1s;
+            }
+            k_pair_store<<<256, 256, 0, s>>>(n, rin, gf, acc, xin_all + idx * 2 * n, er_all + idx);
         }
         CFM_CUDA_TRY(cudaStreamSynchronize(s));
         cfm_stencil_destroy(S2);
@@ -705,13 +885,16 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                 const long long id = order[i0 + bi];
                 CFM_CUDA_TRY(cudaMemcpyAsync(net->xin + (size_t)bi * 2 * n, xin_all + (size_t)id * 2 * n,
                                              sizeof(float) * 2 * n, cudaMemcpyDeviceToDevice, s));
-                CFM_CUDA_TRY(cudaMemcpyAsync(tgt_b + (size_t)bi * n, tgt_all + (size_t)id * n,
-                                             sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
             }
+            // the ids are read by the loss kernels queued below: copy synchronously
+            CFM_CUDA_TRY(cudaStreamSynchronize(s));
+            CFM_CUDA_TRY(cudaMemcpy(ids_d, &order[i0], sizeof(long long) * batch, cudaMemcpyHostToDevice));
             if ((st = unet_forward(u, batch, net->xin, out_b, s))) return st;
-            CFM_CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(double) * 3 * batch, s));
-            k_loss_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, tgt_b, n, sums);
-            k_loss_grad<<<dim3(64, batch), 256, 0, s>>>(out_b, tgt_b, n, batch, sums, dout_b, lossd);
+            CFM_CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(double) * 2 * batch, s));
+            k_loss_anorm_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, net->xin, coef_all, ids_d, per, W,
+                                                             H, az_b, sums);
+            k_loss_anorm_grad<<<dim3(64, batch), 256, 0, s>>>(az_b, net->xin, sums, er_all, ids_d, n,
+                                                             batch, dout_b, lossd);
             CFM_CUDA_TRY(cudaMemsetAsync(unet_grad(u), 0, unet_params(u) * sizeof(float), s));
             if ((st = unet_backward(u, batch, net->xin, dout_b, s))) return st;
             if ((st = unet_adam(u, lr, 1.0f, s))) return st;

@@ -41,4 +41,5 @@ struct cfm_unet {
     cfm::UNetImpl *u = nullptr;
     float *xin = nullptr, *out = nullptr, *dout = nullptr;
     int maxB = 0;
+    int smooth = 0;  // Jacobi sweeps around the network it was trained for
 };

@@ -322,26 +322,37 @@ int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *ou
  * 1e-10; from a second run, `snaps` iterates x_j spread over the solve plus
  * x_0 = 0 give (snaps + 1) * nsys residual/error pairs (r_j = f - A x_j,
  * e_j = x* - x_j); then `epochs` shuffled passes of Adam (lr, batch <=
- * the net's max_batch) on the per-sample loss 1 - cos^2(net(r_j), e_j).
+ * the net's max_batch) on the per-sample energy-norm loss
+ * 1 - <z, r_j>^2 / (<z, A z> <e_j, r_j>), z = net(r_j): one minus the share
+ * of ||e_j||_A^2 that one CG step along z removes.
  * Mean loss of the first and last epoch and the seconds spent on data and on
- * training are returned (each pointer optional). */
+ * training are returned (each pointer optional).  smooth > 0: every pair is
+ * first passed through `smooth` damped Jacobi sweeps z on A z = r_j, giving
+ * (r_j - A z, e_j - z), the pair the network sees inside the preconditioner. */
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
-                           int batch, float lr, double *loss_first, double *loss_last,
+                           int batch, float lr, int smooth, double *loss_first, double *loss_last,
                            double *data_seconds, double *train_seconds);
 
 /* Flexible PCG (Polak-Ribiere beta) on a 2D stencil operator with the
- * network as preconditioner z = |r| net(r / |r|, log k) (k_host: the cell
- * coefficients the stencil was built from).  FP64 vectors and dots; one
+ * preconditioner z = J(z0 + |r1| net(r1 / |r1|, log k)), z0 = J(0),
+ * r1 = r - A z0, where J is `smooth` damped Jacobi sweeps (omega 0.8) on
+ * A z = r, and k_host the cell coefficients the stencil was built from;
+ * smooth must equal the value the network was trained with.  FP64 vectors and dots; one
  * CUDA graph whose conditional while-node runs the iterations on the device.
  * If the loop stalls or reaches maxiter, plain persistent FP64 CG finishes
  * from the current iterate; stats->refinements = 1 then.  stats->iterations
  * = FPCG iterations + fallback iterations; stats->lups = FPCG iterations.
  * The network's grid must equal the stencil's. */
 typedef struct cfm_fpcg cfm_fpcg;
-int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int maxiter,
-                    double tol, cfm_fpcg **out);
+int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int smooth,
+                    int maxiter, double tol, cfm_fpcg **out);
 void cfm_fpcg_destroy(cfm_fpcg *h);
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
+/* Recursive residual norms |r_k| of the last solve, one per iteration from
+ * k = 0 (at most max_n; *n_out = the count).  net == NULL in
+ * cfm_fpcg_create gives the identity preconditioner (plain CG in the same
+ * device loop). */
+int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out);
 
 /* -------------------------------------------------------------- testing */
 /* Launch a persistent kernel of `blocks` blocks (0 = device default) that
