@@ -9,9 +9,11 @@
 //    the fraction of the A-norm error ||e||_A^2 a CG step along z removes.
 //    It is blind to the output's scale (which flexible CG ignores) and,
 //    unlike an L2 loss, punishes output noise that A amplifies;
-//  - flexible PCG (Notay 2000; Polak-Ribiere beta, clipped at 0) with
-//    z = M(r) = |r|_rms * net(r / |r|_rms, log k): FP64 vectors and dots,
-//    the network in BF16 on the tensor cores.  One iteration is a fixed
+//  - flexible PCG (Notay 2000; Polak-Ribiere beta, clipped at 0) with the
+//    hybrid preconditioner z = J(z0 + c y): z0 = J(0) damped Jacobi sweeps,
+//    y = net(r1) on the smoothed residual r1 = r - A z0, c the optimal step
+//    <y, r1> / <y, A y>; FP64 vectors and dots, the network in BF16 on the
+//    tensor cores.  One iteration is a fixed
 //    kernel sequence; it is captured once into a CUDA graph whose
 //    conditional WHILE node repeats it on the device until the residual
 //    reaches the tolerance, so the host launches the whole solve once.
@@ -222,7 +224,10 @@ __global__ void k_loss_anorm_grad(const float *Az, const float *xin, const doubl
 }
 
 // ------------------------------------------------------------------ FPCG
-enum : int { FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_R1 = 5, FP_NSLOT = 6 };
+enum : int {
+    FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_R1 = 5, FP_YR = 6, FP_YAY = 7,
+    FP_NSLOT = 8
+};
 
 struct FpState {
     double rz[2];        // <z, r> of the current direction (double-buffered by k parity)
@@ -342,13 +347,41 @@ __global__ void k_fp_identity(FpArgs a) {
         a.out[i] = a.xin[2 * i];
 }
 
-// zout = zc + rms(r1) out (zc == nullptr: 0).
+// Partials <y, r1> and <y, A y> of the network output y (FP32, applied in FP64).
+__global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
+    __shared__ double sm[33];
+    FP_ROW;
+    double yr = 0, yay = 0;
+    if (i < a.n) {
+        const StencilOp<2> &o = a.op;
+        const int nx = o.nx, ix = i % nx, iy = i / nx;
+        const float *y = a.out;
+        double t = o.dg[i] * (double)y[i];
+        if (ix > 0) t -= o.we[i - 1] * (double)y[i - 1];
+        if (ix < nx - 1) t -= o.we[i] * (double)y[i + 1];
+        if (iy > 0) t -= o.wn[i - nx] * (double)y[i - nx];
+        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[i + nx];
+        yr = (double)y[i] * a.r1[i];
+        yay = (double)y[i] * t;
+    }
+    yr = block_sum(yr, sm);
+    yay = block_sum(yay, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_YR)[blockIdx.x] = yr;
+        fslot(a, FP_YAY)[blockIdx.x] = yay;
+    }
+}
+
+// zout = zc + c y with the optimal step c = <y, r1> / <y, A y>: of all
+// multiples of y, c y removes the most A-norm error from A d = r1, so the
+// network's correction can only help the smoothed iterate (zc == nullptr: 0).
 __global__ void __launch_bounds__(CG_TILE) k_fp_corr(FpArgs a, const double *zc, double *zout) {
     __shared__ double sm[33];
-    const double q = sum_partials(fslot(a, FP_R1), a.ntiles, sm);
-    const double inv = q > 0 ? sqrt(q / (double)a.n) : 0.0;
+    const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
+    const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
+    const double c = yay > 0 ? yr / yay : 0.0;
     FP_ROW;
-    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + (double)a.out[i] * inv;
+    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + c * (double)a.out[i];
 }
 
 // z = zf; partials <z, r>, <z, r_old>.
@@ -506,9 +539,9 @@ FpArgs fp_args(cfm_fpcg *h) {
 }
 
 // One FPCG iteration's tail (from the preconditioner on): convergence test,
-// z = M(r) = post-smooth(pre-smooth(r) + rms(r1) net(r1 / rms(r1), log k))
-// with r1 = r - A pre-smooth(r) and `smooth` damped Jacobi sweeps on each
-// side, then the new direction.
+// z = M(r) = post-smooth(z0 + c y), z0 = pre-smooth(r), r1 = r - A z0,
+// y = net(r1 / rms(r1), log k), c = <y, r1> / <y, A y>, with `smooth` damped
+// Jacobi sweeps on each side; then the new direction.
 int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
     cudaStream_t s = h->stream;
     k_fp_prep<<<h->ntiles, CG_TILE, 0, s>>>(a);
@@ -528,6 +561,7 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
     } else {
         k_fp_identity<<<256, 256, 0, s>>>(a);
     }
+    k_fp_ydots<<<h->ntiles, CG_TILE, 0, s>>>(a);
     k_fp_corr<<<h->ntiles, CG_TILE, 0, s>>>(a, cur, buf[nb]);
     cur = buf[nb];
     nb ^= 1;

@@ -334,10 +334,11 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                            double *data_seconds, double *train_seconds);
 
 /* Flexible PCG (Polak-Ribiere beta) on a 2D stencil operator with the
- * preconditioner z = J(z0 + |r1| net(r1 / |r1|, log k)), z0 = J(0),
- * r1 = r - A z0, where J is `smooth` damped Jacobi sweeps (omega 0.8) on
- * A z = r, and k_host the cell coefficients the stencil was built from;
- * smooth must equal the value the network was trained with.  FP64 vectors and dots; one
+ * preconditioner z = J(z0 + c y): z0 = J(0), r1 = r - A z0,
+ * y = net(r1 / |r1|_rms, log k), c = <y, r1> / <y, A y> (the optimal step
+ * along y), J = `smooth` damped Jacobi sweeps (omega 0.8) on A z = r;
+ * k_host the cell coefficients the stencil was built from; smooth must
+ * equal the value the network was trained with.  FP64 vectors and dots; one
  * CUDA graph whose conditional while-node runs the iterations on the device.
  * If the loop stalls or reaches maxiter, plain persistent FP64 CG finishes
  * from the current iterate; stats->refinements = 1 then.  stats->iterations
