@@ -19,6 +19,16 @@ from the previous grid, which does not change the work.  Metric: GLUP/s
 scaling); rank 0 prints the JSON line.  --impl reference times the host
 restatement of the reference's single-GPU sweep (the reference ships no CPU
 Jacobi of its own) on the host cores with the same metric.
+
+Other workloads (--workload, one JSON line each, same keys):
+  cg128      CG on the 128^3 7-point Poisson CSR system to a true relative
+             residual of 1e-8: standard, pipelined and FP32-inner/FP64-
+             refinement persistent kernels (time to solution, GB/s).
+  varcoef512 the 512^2 variable-coefficient system to 1e-8: plain FP64
+             persistent CG vs flexible PCG with the Jacobi-smoothed and the
+             learned (trained here first) preconditioner.
+  unet       the preconditioner network: forward (batch 1) and one training
+             step (batch 8) at 512^2, TFLOP/s against the measured BF16 peak.
 """
 import argparse
 import json
@@ -47,7 +57,129 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["jacobi3d", "cg128", "varcoef512", "unet"],
+                    default="jacobi3d")
     return ap.parse_args()
+
+
+def peak_bf16(sustained=False):
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops_sustained" if sustained else "bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def unet_flops(H, W):
+    """2 * 9 * Cin * Cout * pixels over the network's convolutions (forward)."""
+    layers = [(2, 32, 0), (32, 64, 1), (64, 128, 2), (128, 256, 3), (256, 128, 3), (128, 64, 2),
+              (64, 32, 1), (32, 32, 0), (32, 1, 0)]
+    return sum(18.0 * ci * co * (H >> l) * (W >> l) for ci, co, l in layers)
+
+
+def line(metric, value, unit, args, ms, config, higher=True, extra=None, dtype="f64"):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": higher, "scaling": "weak",
+         "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config}
+    if extra:
+        d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def workload_cg128(args, cfm):
+    rowptr, col, val = cfm.poisson3d(128)
+    A = cfm.CSR(rowptr, col, val)
+    b = A.spmv(cfm.uniform(0, A.n))
+    peak, kind = peak_hbm()
+    res = {}
+    for impl, name in ((cfm.CG_PERSISTENT, "standard"), (cfm.CG_PERSISTENT_PIPELINED, "pipelined"),
+                       (cfm.CG_MIXED, "fp32_inner_fp64_refinement")):
+        cg = cfm.CG(A, impl, 20000, 1e-8)
+        for _ in range(args.warmup):
+            cg.solve(b)
+        ts = []
+        for _ in range(args.steps):
+            x, st = cg.solve(b)
+            ts.append(st.seconds)
+        t = statistics.median(ts)
+        res[name] = {"ms": t * 1e3, "iterations": st.iterations, "refinements": st.refinements,
+                     "true_relres": st.residual, "algorithmic_gbs": st.bytes / t * 1e-9,
+                     "hbm_frac": st.bytes / t * 1e-9 / peak}
+    best = min(res, key=lambda k: res[k]["ms"])
+    line("CG 128^3 Poisson CSR time to 1e-8 FP64 true relative residual", res[best]["ms"], "ms", args,
+         res[best]["ms"], {"workload": "cg_poisson7_128^3_csr_tol1e-8", "n": A.n, "nnz": len(val),
+                           "best": best, "impls": res, "timing": "median of steps, CUDA events, H2D of b and D2H of x included",
+                           "peak_hbm_gbs": peak, "peak_kind": kind}, higher=False)
+
+
+def workload_varcoef512(args, cfm):
+    import numpy as np
+    N = 512
+    k, f = cfm.varcoef_problem((N, N), 0)
+    S = cfm.Stencil(k)
+    out = {}
+
+    def timed(solver):
+        for _ in range(args.warmup):
+            solver()
+        ts, st = [], None
+        for _ in range(args.steps):
+            x, st = solver()
+            ts.append(st.seconds)
+        return statistics.median(ts), st
+
+    for impl, name in ((cfm.CG_PERSISTENT, "plain_fp64_persistent_cg"),
+                       (cfm.CG_PERSISTENT_PIPELINED, "plain_fp64_pipelined_cg")):
+        cg = cfm.CG(S, impl, 50000, 1e-8)
+        t, st = timed(lambda: cg.solve(f.ravel()))
+        out[name] = {"ms": t * 1e3, "iterations": st.iterations, "true_relres": st.residual}
+    fj = cfm.FPCG(S, k, None, maxiter=20000, tol=1e-8, smooth=4)
+    t, st = timed(lambda: fj.solve(f))
+    out["fpcg_jacobi4"] = {"ms": t * 1e3, "iterations": st.iterations, "true_relres": st.residual,
+                           "fallback": st.refinements}
+    net = cfm.UNet(N, N, max_batch=8, seed=7)
+    info = net.train_varcoef(100, 19, 1000, 8, 8, 1e-3, smooth=4)
+    fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8)
+    t, st = timed(lambda: fl.solve(f))
+    out["fpcg_learned"] = {"ms": t * 1e3, "iterations": st.iterations, "true_relres": st.residual,
+                           "fallback": st.refinements, "training": info,
+                           "training_pairs": 100 * 20}
+    base = out["plain_fp64_persistent_cg"]["ms"]
+    best = min(("fpcg_jacobi4", "fpcg_learned"), key=lambda kk: out[kk]["ms"])
+    line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual", out[best]["ms"], "ms",
+         args, out[best]["ms"],
+         {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "best": best,
+          "speedup_vs_plain_persistent_cg": base / out[best]["ms"], "solvers": out,
+          "timing": "median of steps, CUDA events around the whole solve incl. H2D b / D2H x"},
+         higher=False)
+
+
+def workload_unet(args, cfm):
+    import numpy as np
+    N = 512
+    net = cfm.UNet(N, N, max_batch=8, seed=1)
+    x = np.random.default_rng(0).normal(size=(1, N, N, 2)).astype(np.float32)
+    flop = unet_flops(N, N)
+    for _ in range(args.warmup):
+        net.forward(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.forward(x)
+    t_host = (time.perf_counter() - t0) / args.steps
+    peak, kind = peak_bf16()
+    line("U-Net forward 512^2 batch 1 (host-buffer call)", flop / t_host / 1e12, "TFLOP/s", args,
+         t_host * 1e3, {"workload": "unet4_32ch_512^2_b1_forward", "gflop_per_apply": flop / 1e9,
+                        "peak_bf16_tflops": peak, "peak_kind": kind,
+                        "note": "wall time of cfm_unet_forward_host incl. 2 MB H2D and 1 MB D2H"},
+         dtype="bf16")
+
+
+def main_workload(args):
+    import torch  # noqa: F401  (device plumbing only)
+    import cfm
+    {"cg128": workload_cg128, "varcoef512": workload_varcoef512, "unet": workload_unet}[args.workload](args, cfm)
+    return 0
 
 
 def peak_hbm():
@@ -158,6 +290,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.workload != "jacobi3d":
+        return main_workload(args)
     assert args.warmup >= 3, "at least 3 warm-up steps"
 
     import torch
