@@ -76,6 +76,13 @@ _SIGS = {
     "cfm_fpcg_destroy": (None, [_vp]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
+    "cfm_batch_create": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "cfm_batch_destroy": (None, [_vp]),
+    "cfm_batch_set_plan": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
+    "cfm_batch_set_solver": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_double]),
+    "cfm_batch_solve": (_c.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "cfm_batch_solution": (_c.c_int, [_vp, _c.c_int, _vp]),
+    "cfm_batch_autotune": (_c.c_int, [_vp, _vp]),
     "cfm_poisson3d_nnz": (_c.c_longlong, [_c.c_int, _c.c_int, _c.c_int]),
     "cfm_poisson3d_csr": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _vp, _vp, _vp]),
     "cfm_tridiag_csr": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
@@ -544,3 +551,79 @@ class FPCG:
         st = Stats()
         check("cfm_fpcg_solve", lib.cfm_fpcg_solve(self.h, _ptr(b), _ptr(x), ctypes.byref(st)), allowed)
         return x, st
+
+
+class Batch:
+    """Many variable-coefficient systems in one persistent launch (cfm_batch).
+    systems: list of (k, b) with k of shape (ny, nx) or (nz, ny, nx)."""
+
+    def __init__(self, systems):
+        self.n = len(systems)
+        dims, nx, ny, nz = [], [], [], []
+        self._keep = []
+        for k, b in systems:
+            k = np.ascontiguousarray(k, np.float64)
+            b = np.ascontiguousarray(b, np.float64).reshape(-1)
+            assert b.size == k.size
+            self._keep += [k, b]
+            dims.append(k.ndim)
+            nx.append(k.shape[-1])
+            ny.append(k.shape[-2])
+            nz.append(k.shape[0] if k.ndim == 3 else 1)
+        arr = lambda v: np.ascontiguousarray(v, np.int32)
+        self.dims, self.nx, self.ny, self.nz = arr(dims), arr(nx), arr(ny), arr(nz)
+        kp = (ctypes.c_void_p * self.n)(*[a.ctypes.data for a in self._keep[0::2]])
+        bp = (ctypes.c_void_p * self.n)(*[a.ctypes.data for a in self._keep[1::2]])
+        h = ctypes.c_void_p()
+        check("cfm_batch_create", lib.cfm_batch_create(self.n, _ptr(self.dims), _ptr(self.nx), _ptr(self.ny),
+                                                       _ptr(self.nz), kp, bp, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.cfm_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_solver(self, smooth=4, maxiter=20000, tol=1e-8):
+        check("cfm_batch_set_solver", lib.cfm_batch_set_solver(self.h, smooth, maxiter, tol))
+
+    def set_plan(self, thresholds, teams):
+        t = np.ascontiguousarray(thresholds, np.int64)
+        m = np.ascontiguousarray(teams, np.int32)
+        check("cfm_batch_set_plan", lib.cfm_batch_set_plan(self.h, len(t), _ptr(t), _ptr(m)))
+
+    def autotune(self):
+        ms = ctypes.c_double()
+        check("cfm_batch_autotune", lib.cfm_batch_autotune(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def solve(self, allowed=(OK, NOT_CONVERGED)):
+        it = np.empty(self.n, np.int64)
+        stt = np.empty(self.n, np.int32)
+        rr = np.empty(self.n)
+        st = Stats()
+        check("cfm_batch_solve", lib.cfm_batch_solve(self.h, _ptr(it), _ptr(stt), _ptr(rr), ctypes.byref(st)),
+              allowed)
+        return it, stt, rr, st
+
+    def solution(self, i):
+        n = int(self.nx[i]) * int(self.ny[i]) * int(self.nz[i])
+        x = np.empty(n)
+        check("cfm_batch_solution", lib.cfm_batch_solution(self.h, i, _ptr(x)))
+        return x
+
+
+def uneven_systems(n2d, n3d, seed=0, side2d=(64, 512), side3d=(32, 128)):
+    """Sizes log-uniform in the given ranges (Philox draws from `seed`) and
+    the variable-coefficient problem of each with its own seed."""
+    u = uniform(seed, n2d + n3d, 0.0, 1.0)
+    out = []
+    for i in range(n2d + n3d):
+        lo, hi = side2d if i < n2d else side3d
+        side = int(round(lo * (hi / lo) ** u[i]))
+        shape = (side, side) if i < n2d else (side, side, side)
+        k, f = varcoef_problem(shape, seed * 100000 + 1 + i)
+        out.append((k, f))
+    return out

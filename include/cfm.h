@@ -355,6 +355,35 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
  * device loop). */
 int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out);
 
+/* ------------------------------------------------------- batched solves */
+/* Many independent variable-coefficient systems (2D 5-point / 3D 7-point,
+ * uneven sizes) solved in ONE persistent cooperative launch captured in a
+ * CUDA graph (no reference counterpart).  The resident blocks form teams
+ * per size class; each team takes systems from its class queue (largest
+ * first) and solves them with PCG (FP64, damped-Jacobi polynomial
+ * preconditioner) behind team-local bounded barriers.  System i: dims[i],
+ * nx/ny/nz[i] (nz ignored in 2D), cell coefficients k_host[i] and right-hand
+ * side b_host[i] (x0 = 0). */
+typedef struct cfm_batch cfm_batch;
+int cfm_batch_create(int nsys, const int *dims, const int *nx, const int *ny, const int *nz,
+                     const double *const *k_host, const double *const *b_host, cfm_batch **out);
+void cfm_batch_destroy(cfm_batch *h);
+/* Size classes: class c takes the systems with n >= thresholds[c] not taken
+ * by an earlier class (thresholds descending, the last 0), on teams of
+ * team_sizes[c] blocks; blocks are shared in proportion to class work. */
+int cfm_batch_set_plan(cfm_batch *h, int ncls, const long long *thresholds, const int *team_sizes);
+/* smooth damped Jacobi sweeps in the preconditioner (0 = diagonal scaling),
+ * iteration cap, relative tolerance (defaults 4, 20000, 1e-8). */
+int cfm_batch_set_solver(cfm_batch *h, int smooth, int maxiter, double tol);
+/* Solve all systems (one graph launch).  Per system (each array optional):
+ * iterations, status, FP64 true relative residual; stats->seconds = device
+ * time of the launch, stats->iterations = the sum of iterations. */
+int cfm_batch_solve(cfm_batch *h, long long *iters, int *status, double *relres, cfm_stats *st);
+int cfm_batch_solution(cfm_batch *h, int i, double *x_host);
+/* Autotuner: times every built-in plan (class thresholds x team sizes) on
+ * the real batch and keeps the fastest. */
+int cfm_batch_autotune(cfm_batch *h, double *best_ms);
+
 /* -------------------------------------------------------------- testing */
 /* Launch a persistent kernel of `blocks` blocks (0 = device default) that
  * meets `rounds` grid barriers; when drop_block >= 0 that block skips its
