@@ -27,8 +27,13 @@ Other workloads (--workload, one JSON line each, same keys):
   varcoef512 the 512^2 variable-coefficient system to 1e-8: plain FP64
              persistent CG vs flexible PCG with the Jacobi-smoothed and the
              learned (trained here first) preconditioner.
-  unet       the preconditioner network: forward (batch 1) and one training
-             step (batch 8) at 512^2, TFLOP/s against the measured BF16 peak.
+  unet       the preconditioner network: forward (batch 1) at 512^2,
+             TFLOP/s against the measured BF16 peak.
+  batch256   256 uneven variable-coefficient systems (192 2D, sides
+             log-uniform in [64, 512]; 64 3D, sides in [32, 128]) solved to
+             1e-8 in one persistent launch (CUDA graph, autotuned plan,
+             Jacobi-polynomial PCG) vs one plain persistent CG solve per
+             launch; solves/s.
 """
 import argparse
 import json
@@ -57,7 +62,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["jacobi3d", "cg128", "varcoef512", "unet"],
+    ap.add_argument("--workload", choices=["jacobi3d", "cg128", "varcoef512", "unet", "batch256"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -175,10 +180,49 @@ def workload_unet(args, cfm):
          dtype="bf16")
 
 
+def workload_batch256(args, cfm):
+    import numpy as np
+    t0 = time.perf_counter()
+    systems = cfm.uneven_systems(192, 64, seed=5)
+    gen_s = time.perf_counter() - t0
+    B = cfm.Batch(systems)
+    B.set_solver(smooth=4, maxiter=20000, tol=1e-8)
+    tune_ms = B.autotune()
+    for _ in range(args.warmup):
+        B.solve()
+    ts = []
+    for _ in range(args.steps):
+        it, stt, rr, st = B.solve()
+        ts.append(st.seconds)
+    t = statistics.median(ts)
+    # one plain persistent FP64 CG solve per launch, same tolerance
+    t_plain, it_plain = 0.0, []
+    for k, f in systems:
+        S = cfm.Stencil(k)
+        x, sp = cfm.CG(S, cfm.CG_PERSISTENT, 50000, 1e-8).solve(f.ravel())
+        t_plain += sp.seconds
+        it_plain.append(sp.iterations)
+    n = len(systems)
+    line("256 uneven variable-coefficient systems to 1e-8: aggregate solves/s", n / t, "solves/s", args,
+         t * 1e3, {"workload": "batch_192x2d_64..512_64x3d_32..128_varcoef_tol1e-8",
+                   "systems": n, "cells": int(sum(k.size for k, _ in systems)),
+                   "batched_ms": t * 1e3, "all_converged": bool((stt == cfm.OK).all()),
+                   "max_true_relres": float(rr.max()),
+                   "iterations_batched": {"min": int(it.min()), "median": float(np.median(it)), "max": int(it.max())},
+                   "iterations_plain": {"min": int(min(it_plain)), "median": float(np.median(it_plain)),
+                                        "max": int(max(it_plain))},
+                   "per_system_iterations": [int(v) for v in it],
+                   "plain_one_solve_per_launch_ms": t_plain * 1e3,
+                   "speedup_vs_one_plain_solve_per_launch": t_plain / t,
+                   "autotune_best_ms": tune_ms, "generation_s": gen_s,
+                   "method": "PCG FP64, 4 damped-Jacobi sweeps, one cooperative launch in a CUDA graph"})
+
+
 def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
-    {"cg128": workload_cg128, "varcoef512": workload_varcoef512, "unet": workload_unet}[args.workload](args, cfm)
+    {"cg128": workload_cg128, "varcoef512": workload_varcoef512, "unet": workload_unet,
+     "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
 
 
