@@ -447,7 +447,8 @@ const TmaVariant *tma_variants(int *count) {
     static const TmaVariant v[] = {
         make_tma_variant<8, 2, 6>(), make_tma_variant<4, 2, 8>(),  make_tma_variant<4, 4, 6>(),
         make_tma_variant<8, 1, 8>(), make_tma_variant<4, 2, 12>(), make_tma_variant<2, 4, 8>(),
-        make_tma_variant<8, 4, 4>(), make_tma_variant<16, 2, 4>(),
+        make_tma_variant<8, 4, 4>(), make_tma_variant<16, 2, 4>(),  make_tma_variant<16, 2, 6>(),
+        make_tma_variant<16, 2, 8>(), make_tma_variant<8, 4, 8>(),  make_tma_variant<16, 4, 4>(),
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;

@@ -112,8 +112,9 @@ def test_autotune_restores_grid_and_stays_bitexact():
         assert j.autotune(2)[0] == -1  # nothing to tune outside the 3D TMA pipeline
 
 
-@pytest.mark.parametrize("variant", range(8))
+@pytest.mark.parametrize("variant", range(12))
 def test_every_pipeline_variant_bitexact(variant, monkeypatch):
+    assert cfm.variant_info(variant) is not None and cfm.variant_info(12) is None
     monkeypatch.setenv("CFM_J3D_TMA_VARIANT", str(variant))
     for prec, py, shape in ((cfm.FP64, 1, (21, 19, 128)), (cfm.FP32, 0, (13, 40, 136))):
         a = rand_grid(shape, cfm.np_dtype(prec), 16)
