@@ -172,11 +172,15 @@ def workload_unet(args, cfm):
     for _ in range(args.steps):
         net.forward(x)
     t_host = (time.perf_counter() - t0) / args.steps
+    dev = {b: net.time_forward(b, max(args.steps, 5)) * 1e-3 for b in (1, 8)}
     peak, kind = peak_bf16()
-    line("U-Net forward 512^2 batch 1 (host-buffer call)", flop / t_host / 1e12, "TFLOP/s", args,
-         t_host * 1e3, {"workload": "unet4_32ch_512^2_b1_forward", "gflop_per_apply": flop / 1e9,
+    line("U-Net forward 512^2 batch 1, device-resident", flop / dev[1] / 1e12, "TFLOP/s", args,
+         dev[1] * 1e3, {"workload": "unet4_32ch_512^2_b1_forward", "gflop_per_apply": flop / 1e9,
+                        "batch8_ms": dev[8] * 1e3, "batch8_tflops": 8 * flop / dev[8] / 1e12,
+                        "host_call_ms_incl_copies": t_host * 1e3,
                         "peak_bf16_tflops": peak, "peak_kind": kind,
-                        "note": "wall time of cfm_unet_forward_host incl. 2 MB H2D and 1 MB D2H"},
+                        "roofline_frac_batch1": flop / dev[1] / 1e12 / peak,
+                        "timing": "CUDA events around unet forward passes on device buffers"},
          dtype="bf16")
 
 

@@ -70,6 +70,7 @@ _SIGS = {
     "cfm_unet_forward_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
+    "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
                                           _c.c_float, _c.c_int, _vp, _vp, _vp, _vp]),
     "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
@@ -509,6 +510,11 @@ class UNet:
               lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth,
                                          *[ctypes.byref(x) for x in v]))
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
+
+    def time_forward(self, B=1, iters=20):
+        ms = ctypes.c_double()
+        check("cfm_unet_time_forward", lib.cfm_unet_time_forward(self.h, B, iters, ctypes.byref(ms)))
+        return ms.value
 
     def gradient(self, x, dout):
         x = np.ascontiguousarray(x, np.float32)

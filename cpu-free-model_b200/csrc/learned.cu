@@ -708,6 +708,36 @@ int cfm_unet_gradient_host(cfm_unet *h, int B, const float *in, const float *dou
     return CFM_OK;
 }
 
+// Device time of one forward pass on the net's own input buffer (whatever it
+// holds), averaged over `iters` passes after one warm-up: CUDA events.
+int cfm_unet_time_forward(cfm_unet *h, int B, int iters, double *ms_per_forward) {
+    clear_error();
+    CFM_ARG_CHECK(h && ms_per_forward && iters >= 1, "arguments");
+    CFM_ARG_CHECK(B >= 1 && B <= h->maxB, "batch");
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CFM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = unet_forward(h->u, B, h->xin, h->out, s);
+    if (!st) {
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < iters && !st; ++i) st = unet_forward(h->u, B, h->xin, h->out, s);
+        cudaEventRecord(e1, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    float ms = 0;
+    if (!st && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (st) return st;
+    CFM_CUDA_TRY(e);
+    if ((st = unet_check_err(h->u))) return st;
+    *ms_per_forward = ms / iters;
+    return CFM_OK;
+}
+
 // BF16 patterns of one activation of the last forward pass, in the order
 // h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0 (index 0..13), B images.
 int cfm_unet_activation_host(cfm_unet *h, int which, int B, unsigned short *out) {

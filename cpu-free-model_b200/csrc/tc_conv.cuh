@@ -151,8 +151,10 @@ struct TcGeom {
     static constexpr int A_BYTES = 128 * SW;
     static constexpr int B_BYTES = N * SW;
     static constexpr int STAGE = (A_BYTES + B_BYTES + 1023) / 1024 * 1024;
-    static constexpr int STAGES = (200 * 1024) / STAGE > 8 ? 8 : (200 * 1024) / STAGE;
-    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 /* align */ + 256 /* barriers */;
+    // deep enough to keep more than one tile's loads in flight (<= 16 stages, <= 200 KB)
+    static constexpr int STAGES = (200 * 1024) / STAGE > 16 ? 16 : (200 * 1024) / STAGE;
+    // + 1024 alignment slack + full/empty/acc/drain mbarriers and the TMEM base slot
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 + (2 * STAGES + 8) * 8;
     static constexpr uint32_t TMEM_COLS = 2 * N < 32 ? 32 : 2 * N;
 };
 
@@ -173,6 +175,7 @@ __global__ void __launch_bounds__(192, 1)
     uint64_t *drain = acc_empty + 2;       // [1]
     uint32_t *tmem_base_slot = reinterpret_cast<uint32_t *>(drain + 1);
     __shared__ int s_abort;
+    __shared__ float s_bias[N];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -188,6 +191,7 @@ __global__ void __launch_bounds__(192, 1)
         s_abort = 0;
         mbar_fence_init();
     }
+    for (int c = threadIdx.x; c < N; c += blockDim.x) s_bias[c] = p.bias ? p.bias[c] : 0.f;
     if (warp == 1) {
         tmem_alloc(tmem_base_slot, G::TMEM_COLS);
         tmem_relinquish();
@@ -332,22 +336,37 @@ __global__ void __launch_bounds__(192, 1)
                 const size_t pix = ((size_t)img * p.H + (in ? y : 0)) * p.W + (in ? x : 0);
                 __nv_bfloat16 *o = p.out + pix * N;
                 const __nv_bfloat16 *mk = p.mask ? p.mask + pix * N : nullptr;
-#pragma unroll 1
-                for (int c = 0; c < N; c += 16) {
-                    float acc[16];
-                    tmem_ld16(tbase + c, acc);
-                    if (in) {
-                        __align__(16) __nv_bfloat16 v16[16];
+                auto emit16 = [&](int c, const float *acc) {
+                    if (!in) return;
+                    __align__(16) __nv_bfloat16 v16[16];
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float v = acc[j];
-                            if (p.bias) v += p.bias[c + j];
-                            if (p.relu) v = fmaxf(v, 0.f);
-                            if (mk && !(__bfloat162float(mk[c + j]) > 0.f)) v = 0.f;
-                            v16[j] = __float2bfloat16_rn(v);
-                        }
-                        reinterpret_cast<uint4 *>(o + c)[0] = reinterpret_cast<const uint4 *>(v16)[0];
-                        reinterpret_cast<uint4 *>(o + c)[1] = reinterpret_cast<const uint4 *>(v16)[1];
+                    for (int j = 0; j < 16; ++j) {
+                        float v = acc[j] + s_bias[c + j];
+                        if (p.relu) v = fmaxf(v, 0.f);
+                        if (mk && !(__bfloat162float(mk[c + j]) > 0.f)) v = 0.f;
+                        v16[j] = __float2bfloat16_rn(v);
+                    }
+                    reinterpret_cast<uint4 *>(o + c)[0] = reinterpret_cast<const uint4 *>(v16)[0];
+                    reinterpret_cast<uint4 *>(o + c)[1] = reinterpret_cast<const uint4 *>(v16)[1];
+                };
+                if constexpr (N <= 64) {
+                    // narrow tile: drain TMEM first and hand the accumulator back
+                    // to the MMA warp before the global stores
+                    float accall[N];
+#pragma unroll
+                    for (int c = 0; c < N; c += 16) tmem_ld16(tbase + c, accall + c);
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acc_empty[ab]);
+#pragma unroll
+                    for (int c = 0; c < N; c += 16) emit16(c, accall + c);
+                    continue;
+                } else {
+#pragma unroll 1
+                    for (int c = 0; c < N; c += 16) {
+                        float acc[16];
+                        tmem_ld16(tbase + c, acc);
+                        emit16(c, acc);
                     }
                 }
             } else {

@@ -312,6 +312,9 @@ int cfm_unet_forward_host(cfm_unet *net, int B, const float *in, float *out);
 /* Forward, then the gradient of sum(out * dout) with respect to the
  * parameters into grad (cfm_unet_num_params floats). */
 int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *dout, float *grad);
+/* Device time of one forward pass of batch B on device-resident buffers
+ * (mean over `iters` after a warm-up; CUDA events). */
+int cfm_unet_time_forward(cfm_unet *net, int B, int iters, double *ms_per_forward);
 /* BF16 patterns of one activation of the last forward pass (testing): index
  * 0..13 = h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0, NHWC at its level. */
 int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *out);
