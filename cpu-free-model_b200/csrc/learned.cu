@@ -65,64 +65,69 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
     *reinterpret_cast<uint4 *>(p) = u;
 }
 
-// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2], one pixel per thread.
+// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Four threads per
+// pixel, each producing 8 of the 32 output channels (one 16-byte store).
 __global__ void k_cin_fwd(const float *x, const float *w, const float *b, bf16 *h0, int B, int H,
                           int W) {
     __shared__ float sw[9 * 32 * 2 + 32];
     for (int i = threadIdx.x; i < 9 * 64 + 32; i += blockDim.x) sw[i] = i < 576 ? w[i] : b[i - 576];
     __syncthreads();
     const long long P = (long long)B * H * W;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
-         p += (long long)gridDim.x * blockDim.x) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 4 * P;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e >> 2;
+        const int c0 = (int)(e & 3) * 8;
         const int xx = (int)(p % W), yy = (int)((p / W) % H);
         const long long img0 = p - (long long)yy * W - xx;
-        float in[9][2];
+        float o[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) o[c] = sw[576 + c0 + c];
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
             const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-            const bool ok = y >= 0 && y < H && xq >= 0 && xq < W;
-            const long long q = img0 + (long long)y * W + xq;
-            in[t][0] = ok ? x[2 * q] : 0.f;
-            in[t][1] = ok ? x[2 * q + 1] : 0.f;
-        }
-        float o[32];
+            if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
+            const float2 v = *reinterpret_cast<const float2 *>(x + 2 * (img0 + (long long)y * W + xq));
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-            float acc = sw[576 + c];
-#pragma unroll
-            for (int t = 0; t < 9; ++t) acc += sw[(t * 32 + c) * 2] * in[t][0] + sw[(t * 32 + c) * 2 + 1] * in[t][1];
-            o[c] = fmaxf(acc, 0.f);
+            for (int c = 0; c < 8; ++c)
+                o[c] += sw[(t * 32 + c0 + c) * 2] * v.x + sw[(t * 32 + c0 + c) * 2 + 1] * v.y;
         }
 #pragma unroll
-        for (int c = 0; c < 32; c += 8) store8(h0 + p * 32 + c, o + c);
+        for (int c = 0; c < 8; ++c) o[c] = fmaxf(o[c], 0.f);
+        store8(h0 + p * 32 + c0, o);
     }
 }
 
-// out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.
+// out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.  Four threads
+// per pixel, each summing 8 channels over the 9 taps (one 16-byte load per
+// tap), combined by two xor shuffles.
 __global__ void k_cout_fwd(const bf16 *g0, const float *w, const float *b, float *out, int B, int H,
                            int W) {
     __shared__ float sw[9 * 32 + 1];
     for (int i = threadIdx.x; i < 289; i += blockDim.x) sw[i] = i < 288 ? w[i] : b[0];
     __syncthreads();
     const long long P = (long long)B * H * W;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
-         p += (long long)gridDim.x * blockDim.x) {
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
-        const long long img0 = p - (long long)yy * W - xx;
-        float acc = sw[288];
-        for (int t = 0; t < 9; ++t) {
-            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-            if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
-            const bf16 *q = g0 + (img0 + (long long)y * W + xq) * 32;
+    // the loop bound is a multiple of 4 per pixel, so the 4 lanes of a pixel stay together
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ((4 * P + 31) & ~31LL);
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e >> 2;
+        const int c0 = (int)(e & 3) * 8;
+        float acc = 0.f;
+        if (p < P) {
+            const int xx = (int)(p % W), yy = (int)((p / W) % H);
+            const long long img0 = p - (long long)yy * W - xx;
 #pragma unroll
-            for (int c = 0; c < 32; c += 8) {
+            for (int t = 0; t < 9; ++t) {
+                const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
+                if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
                 float v[8];
-                load8(q + c, v);
+                load8(g0 + (img0 + (long long)y * W + xq) * 32 + c0, v);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc += sw[t * 32 + c + j] * v[j];
+                for (int j = 0; j < 8; ++j) acc += sw[t * 32 + c0 + j] * v[j];
             }
         }
-        out[p] = acc;
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        if (p < P && (e & 3) == 0) out[p] = acc + sw[288];
     }
 }
 
@@ -496,7 +501,7 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s)
     const int H = u->H, W = u->W;
     const long long P0 = (long long)B * H * W;
     int st;
-    k_cin_fwd<<<grid_for(P0), 256, 0, s>>>(x, u->theta + u->woff[0], u->theta + u->boff[0], a.h0, B, H, W);
+    k_cin_fwd<<<grid_for(4 * P0), 256, 0, s>>>(x, u->theta + u->woff[0], u->theta + u->boff[0], a.h0, B, H, W);
     CFM_CUDA_TRY(cudaGetLastError());
     int h = H, w = W;
     k_pool<<<grid_for(P0 / 4 * 4), 256, 0, s>>>(a.h0, a.p1, B, h / 2, w / 2, 32);
@@ -518,8 +523,8 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s)
     k_up_add<<<grid_for(P0 * 4), 256, 0, s>>>(a.g1, a.h0, a.u0, B, h, w, 32);
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 7, a.u0, a.g0, B, h, w, s))) return st;
-    k_cout_fwd<<<grid_for(P0), 256, 0, s>>>(a.g0, u->theta + u->woff[8], u->theta + u->boff[8], out, B,
-                                            H, W);
+    k_cout_fwd<<<grid_for(4 * P0), 256, 0, s>>>(a.g0, u->theta + u->woff[8], u->theta + u->boff[8], out,
+                                                B, H, W);
     CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
 }

@@ -151,15 +151,18 @@ struct TcGeom {
     static constexpr int A_BYTES = 128 * SW;
     static constexpr int B_BYTES = N * SW;
     static constexpr int STAGE = (A_BYTES + B_BYTES + 1023) / 1024 * 1024;
-    // deep enough to keep more than one tile's loads in flight (<= 16 stages, <= 200 KB)
-    static constexpr int STAGES = (200 * 1024) / STAGE > 16 ? 16 : (200 * 1024) / STAGE;
+    // Narrow tiles (N <= 64) keep the ring near 100 KB so two CTAs share an
+    // SM (two independent load / MMA / epilogue pipelines, 2 x 2N TMEM
+    // columns); wide ones take up to 200 KB alone.  At most 16 stages.
+    static constexpr int BUDGET = (N <= 64 ? 100 : 200) * 1024;
+    static constexpr int STAGES = BUDGET / STAGE > 16 ? 16 : BUDGET / STAGE;
     // + 1024 alignment slack + full/empty/acc/drain mbarriers and the TMEM base slot
     static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 + (2 * STAGES + 8) * 8;
     static constexpr uint32_t TMEM_COLS = 2 * N < 32 ? 32 : 2 * N;
 };
 
 template <int KC, int N>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
     tc_conv_kernel(const __grid_constant__ CUtensorMap mapA0, const __grid_constant__ CUtensorMap mapA1,
                    const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB,
                    TcConvParams p) {

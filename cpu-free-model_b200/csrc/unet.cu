@@ -53,7 +53,15 @@ int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap 
     DeviceInfo di;
     int st = current_device_info(&di);
     if (st) return st;
-    const int grid = std::min(p.ntiles, di.num_sms);
+    static int per_sm_cache[64];
+    int &per_sm = per_sm_cache[dev & 63];
+    if (per_sm <= 0) {
+        CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_conv_kernel<KC, N>, 192,
+                                                                   G::SMEM));
+        // TMEM: every resident CTA holds TMEM_COLS of the SM's 512 columns
+        per_sm = std::max(1, std::min(per_sm, (int)(512 / G::TMEM_COLS)));
+    }
+    const int grid = std::min(p.ntiles, di.num_sms * per_sm);
     tc_conv_kernel<KC, N><<<grid, 192, G::SMEM, s>>>(a0, a1, a2, b, p);
     CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
