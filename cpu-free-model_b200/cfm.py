@@ -72,7 +72,7 @@ _SIGS = {
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
-                                          _c.c_float, _c.c_int, _vp, _vp, _vp, _vp]),
+                                          _c.c_float, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp]),
     "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_destroy": (None, [_vp]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
@@ -460,6 +460,7 @@ class UNet:
     def __init__(self, H, W, max_batch=1, seed=0):
         self.H, self.W, self.max_batch = H, W, max_batch
         self.smooth = 0
+        self.coarsen = 1
         self.n = lib.cfm_unet_num_params()
         h = ctypes.c_void_p()
         check("cfm_unet_create", lib.cfm_unet_create(H, W, max_batch, seed, ctypes.byref(h)))
@@ -502,12 +503,13 @@ class UNet:
             out[name] = from_bf16_bits(a)
         return out
 
-    def train_varcoef(self, nsys, snaps, seed0, epochs, batch, lr=1e-3, smooth=0):
-        """Plain-CG training pairs + Adam; returns dict(loss_first, loss_last, data_s, train_s)."""
+    def train_varcoef(self, nsys, snaps, seed0, epochs, batch, lr=1e-3, smooth=0, coarsen=1):
+        """Plain-CG training pairs + Adam on systems of (coarsen H) x (coarsen W);
+        returns dict(loss_first, loss_last, data_s, train_s)."""
         v = [ctypes.c_double() for _ in range(4)]
-        self.smooth = smooth
+        self.smooth, self.coarsen = smooth, coarsen
         check("cfm_unet_train_varcoef",
-              lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth,
+              lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth, coarsen,
                                          *[ctypes.byref(x) for x in v]))
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
 

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <string>
+#include <utility>
 
 #include "cfm.h"
 
@@ -45,6 +46,40 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 // (the barrier needs co-residency).
 cudaError_t launch_cooperative(const void *fn, dim3 grid, dim3 block, void **args, size_t smem,
                                cudaStream_t s);
+
+// Programmatic dependent launch: the kernel may be scheduled while its
+// predecessor in the stream is still running, which hides the launch gap
+// between the short kernels of a solver iteration.  Every kernel launched
+// this way starts with pdl_enter() (griddepcontrol.wait: the predecessor has
+// completed and its writes are visible) before it touches global memory.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+#ifdef __CUDACC__
+// Waits for the stream predecessor (no-op without a programmatic launch),
+// then lets the successor be scheduled.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_enter() {
+    pdl_wait();
+    pdl_trigger();
+}
+#endif
 
 }  // namespace cfm
 

@@ -148,44 +148,61 @@ __global__ void k_data_smoothed(StencilOp<2> op, int n, const double *z, double 
     }
 }
 
-// Network input [r / rms(r), g] (FP32) and the sample's <e, r> at that
-// scale: <e / rms(r), r / rms(r)> = <e, r> n / |r|^2.
-__global__ void k_pair_store(int n, const double *r, const float *g, const double *acc, float *xin,
-                             double *er_out) {
+// One training sample at residual scale sr = 1 / rms(r) (r on the nx x ny
+// grid): the fine residual r1 = r sr (FP32, for the loss), the network
+// input on the (nx / f) x (ny / f) grid [R(r) sr, gc] with R the mean over
+// f x f blocks and gc the block-mean log k, and <e, r> sr^2.
+__global__ void k_pair_store(int nx, int ny, int f, const double *r, const float *gc, const double *acc,
+                             float *xin, float *r1, double *er_out) {
+    const int n = nx * ny, ncx = nx / f, nc = n / (f * f);
     const double sr = acc[0] > 0 ? sqrt((double)n / acc[0]) : 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        xin[2 * i] = (float)(r[i] * sr);
-        xin[2 * i + 1] = g[i];
+    const double inv = 1.0 / (f * f);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        r1[i] = (float)(r[i] * sr);
+    for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+        const int cx = ic % ncx, cy = ic / ncx;
+        double sum = 0;
+        for (int dy = 0; dy < f; ++dy)
+            for (int dx = 0; dx < f; ++dx) sum += r[(size_t)(cy * f + dy) * nx + cx * f + dx] * sr;
+        xin[2 * ic] = (float)(sum * inv);
+        xin[2 * ic + 1] = gc[ic];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *er_out = acc[1] * sr * sr;
 }
 
 // ------------------------------------------------------------- the loss
-// Per batch element b (sample ids[b] of system ids[b] / per, whose FP32
-// stencil coefficients we | wn | dg sit at coef + sys * 3 n):
-//   Az = A z (FP32 apply), s[0] = <z, r>, s[1] = <z, A z>  (FP64 atomics),
-// with r = channel 0 of the network input.
-__global__ void k_loss_anorm_dots(const float *z, const float *xin, const float *coef,
-                                  const long long *ids, int per, int nx, int ny, float *Az,
+// The network output y lives on the (nx / f) x (ny / f) grid; the correction
+// is its piecewise-constant prolongation z = P y on the nx x ny grid,
+// z[i] = y[cell(i)].  Per batch element b (sample ids[b] of system
+// ids[b] / per, whose FP32 stencil coefficients we | wn | dg sit at
+// coef + sys * 3 n and whose fine residual r is r1 + ids[b] n):
+//   Az = A z (FP32 apply), s[0] = <z, r>, s[1] = <z, A z>  (FP64 atomics).
+__device__ __forceinline__ int coarse_cell(int ix, int iy, int f, int ncx) {
+    return (iy / f) * ncx + ix / f;
+}
+
+__global__ void k_loss_anorm_dots(const float *y, const float *r1, const float *coef,
+                                  const long long *ids, int per, int nx, int ny, int f, float *Az,
                                   double *s) {
-    const int b = blockIdx.y, n = nx * ny;
+    const int b = blockIdx.y, n = nx * ny, ncx = nx / f, nc = n / (f * f);
     const float *c = coef + (size_t)(ids[b] / per) * 3 * n;
     const float *we = c, *wn = c + n, *dg = c + 2 * n;
-    z += (size_t)b * n;
-    xin += (size_t)b * 2 * n;
+    const float *r = r1 + (size_t)ids[b] * n;
+    y += (size_t)b * nc;
     Az += (size_t)b * n;
     __shared__ double red[2][32];
     double zr = 0, zaz = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int ix = i % nx, iy = i / nx;
-        float t = dg[i] * z[i];
-        if (ix > 0) t -= we[i - 1] * z[i - 1];
-        if (ix < nx - 1) t -= we[i] * z[i + 1];
-        if (iy > 0) t -= wn[i - nx] * z[i - nx];
-        if (iy < ny - 1) t -= wn[i] * z[i + nx];
+        const float zi = y[coarse_cell(ix, iy, f, ncx)];
+        float t = dg[i] * zi;
+        if (ix > 0) t -= we[i - 1] * y[coarse_cell(ix - 1, iy, f, ncx)];
+        if (ix < nx - 1) t -= we[i] * y[coarse_cell(ix + 1, iy, f, ncx)];
+        if (iy > 0) t -= wn[i - nx] * y[coarse_cell(ix, iy - 1, f, ncx)];
+        if (iy < ny - 1) t -= wn[i] * y[coarse_cell(ix, iy + 1, f, ncx)];
         Az[i] = t;
-        zr += (double)z[i] * xin[2 * i];
-        zaz += (double)z[i] * t;
+        zr += (double)zi * r[i];
+        zaz += (double)zi * t;
     }
     for (int o = 16; o; o >>= 1) {
         zr += __shfl_xor_sync(CG_FULL, zr, o);
@@ -208,17 +225,26 @@ __global__ void k_loss_anorm_dots(const float *z, const float *xin, const float 
 }
 
 // L_b = 1 - a^2 / (q c), a = <z, r>, q = <z, A z>, c = <e, r>;
-// dL_b/dz = (2 a / (q c)) ((a / q) A z - r); the batch mean and its gradient.
-__global__ void k_loss_anorm_grad(const float *Az, const float *xin, const double *s,
-                                  const double *er, const long long *ids, int n, int B,
+// dL_b/dz = (2 a / (q c)) ((a / q) A z - r) and dL_b/dy = P^T dL_b/dz (the
+// sum over each f x f block); the batch mean and its gradient.
+__global__ void k_loss_anorm_grad(const float *Az, const float *r1, const double *s,
+                                  const double *er, const long long *ids, int nx, int ny, int f, int B,
                                   float *dout, double *loss) {
-    const int b = blockIdx.y;
+    const int b = blockIdx.y, n = nx * ny, ncx = nx / f, nc = n / (f * f);
     const double a = s[2 * b], q = s[2 * b + 1], c = er[ids[b]];
     const bool ok = q > 0 && c > 0;
-    const double f = ok ? 2.0 * a / (q * c) / B : 0.0, aq = ok ? a / q : 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const size_t j = (size_t)b * n + i;
-        dout[j] = (float)(f * (aq * Az[j] - (double)xin[2 * j]));
+    const double fb = ok ? 2.0 * a / (q * c) / B : 0.0, aq = ok ? a / q : 0.0;
+    const float *r = r1 + (size_t)ids[b] * n;
+    const float *az = Az + (size_t)b * n;
+    for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+        const int cx = ic % ncx, cy = ic / ncx;
+        double g = 0;
+        for (int dy = 0; dy < f; ++dy)
+            for (int dx = 0; dx < f; ++dx) {
+                const size_t j = (size_t)(cy * f + dy) * nx + cx * f + dx;
+                g += fb * (aq * az[j] - (double)r[j]);
+            }
+        dout[(size_t)b * nc + ic] = (float)g;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && ok) atomicAdd(loss, (1.0 - a * a / (q * c)) / B);
 }
@@ -251,7 +277,14 @@ struct FpArgs {
     double *hist;  // |r| before each preconditioner application (maxiter + 1 entries)
     long long maxiter;
     int stall;
+    int f, ncx, nc;  // network grid: (nx / f) x (ny / f) = nc cells, ncx per row
 };
+
+// The network cell of fine cell i (piecewise-constant prolongation).
+__device__ __forceinline__ int fp_cell(const FpArgs &a, int i) {
+    const int ix = i % a.op.nx, iy = i / a.op.nx;
+    return (iy / a.f) * a.ncx + ix / a.f;
+}
 
 __device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.ntiles; }
 
@@ -287,6 +320,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
 
 // rr = |r|^2; convergence / stall test (block 0).
 __global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
+    pdl_enter();
     __shared__ double sm[33];
     const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
     const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);  // block-wide: every thread
@@ -312,6 +346,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
 // Damped Jacobi sweep on A z = r: zout = zin + omega (r - A zin) / diag
 // (zin == nullptr: zout = omega r / diag).
 __global__ void k_fp_jacobi(FpArgs a, const double *zin, double *zout) {
+    pdl_enter();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         const double res = zin ? a.r[i] - a.op.apply(zin, i) : a.r[i];
         zout[i] = (zin ? zin[i] : 0.0) + JACOBI_OMEGA * res / a.op.dg[i];
@@ -320,6 +355,7 @@ __global__ void k_fp_jacobi(FpArgs a, const double *zin, double *zout) {
 
 // r1 = r - A zc (zc == nullptr: r1 = r) and partial |r1|^2.
 __global__ void __launch_bounds__(CG_TILE) k_fp_r1(FpArgs a, const double *zc) {
+    pdl_enter();
     __shared__ double sm[33];
     FP_ROW;
     double q = 0;
@@ -332,37 +368,49 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_r1(FpArgs a, const double *zc) {
     if (threadIdx.x == 0) fslot(a, FP_R1)[blockIdx.x] = q;
 }
 
-// Network input channel 0 = r1 / rms(r1).
+// Network input channel 0 = R(r1) / rms(r1), R the mean over f x f blocks.
 __global__ void __launch_bounds__(CG_TILE) k_fp_in(FpArgs a) {
+    pdl_enter();
     __shared__ double sm[33];
     const double q = sum_partials(fslot(a, FP_R1), a.ntiles, sm);
     const double scale = q > 0 ? sqrt((double)a.n / q) : 0.0;
-    FP_ROW;
-    if (i < a.n) a.xin[2 * i] = (float)(a.r1[i] * scale);
+    const double inv = 1.0 / (a.f * a.f);
+    const int nx = a.op.nx;
+    for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < a.nc; ic += gridDim.x * blockDim.x) {
+        const int cx = ic % a.ncx, cy = ic / a.ncx;
+        double sum = 0;
+        for (int dy = 0; dy < a.f; ++dy)
+            for (int dx = 0; dx < a.f; ++dx) sum += a.r1[(size_t)(cy * a.f + dy) * nx + cx * a.f + dx] * scale;
+        a.xin[2 * ic] = (float)(sum * inv);
+    }
 }
 
 // Identity in place of the network: out = the normalised r1.
 __global__ void k_fp_identity(FpArgs a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+    pdl_enter();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x)
         a.out[i] = a.xin[2 * i];
 }
 
-// Partials <y, r1> and <y, A y> of the network output y (FP32, applied in FP64).
+// Partials <z, r1> and <z, A z> of the prolongated network output z = P y
+// (FP32 values, applied in FP64).
 __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
+    pdl_enter();
     __shared__ double sm[33];
     FP_ROW;
     double yr = 0, yay = 0;
     if (i < a.n) {
         const StencilOp<2> &o = a.op;
         const int nx = o.nx, ix = i % nx, iy = i / nx;
-        const float *y = a.out;
-        double t = o.dg[i] * (double)y[i];
-        if (ix > 0) t -= o.we[i - 1] * (double)y[i - 1];
-        if (ix < nx - 1) t -= o.we[i] * (double)y[i + 1];
-        if (iy > 0) t -= o.wn[i - nx] * (double)y[i - nx];
-        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[i + nx];
-        yr = (double)y[i] * a.r1[i];
-        yay = (double)y[i] * t;
+        const float *y = a.out;  // z = P y on this grid: z[j] = y[fp_cell(j)]
+        const double zi = (double)y[fp_cell(a, i)];
+        double t = o.dg[i] * zi;
+        if (ix > 0) t -= o.we[i - 1] * (double)y[fp_cell(a, i - 1)];
+        if (ix < nx - 1) t -= o.we[i] * (double)y[fp_cell(a, i + 1)];
+        if (iy > 0) t -= o.wn[i - nx] * (double)y[fp_cell(a, i - nx)];
+        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[fp_cell(a, i + nx)];
+        yr = zi * a.r1[i];
+        yay = zi * t;
     }
     yr = block_sum(yr, sm);
     yay = block_sum(yay, sm);
@@ -372,20 +420,23 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     }
 }
 
-// zout = zc + c y with the optimal step c = <y, r1> / <y, A y>: of all
-// multiples of y, c y removes the most A-norm error from A d = r1, so the
-// network's correction can only help the smoothed iterate (zc == nullptr: 0).
+// zout = zc + c z with z = P y and the optimal step c = <z, r1> / <z, A z>:
+// of all multiples of z, c z removes the most A-norm error from A d = r1, so
+// the network's correction can only help the smoothed iterate (zc ==
+// nullptr: 0).
 __global__ void __launch_bounds__(CG_TILE) k_fp_corr(FpArgs a, const double *zc, double *zout) {
+    pdl_enter();
     __shared__ double sm[33];
     const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
     const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
     const double c = yay > 0 ? yr / yay : 0.0;
     FP_ROW;
-    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + c * (double)a.out[i];
+    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + c * (double)a.out[fp_cell(a, i)];
 }
 
 // z = zf; partials <z, r>, <z, r_old>.
 __global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a, const double *zf) {
+    pdl_enter();
     __shared__ double sm[33];
     FP_ROW;
     double zr = 0, zro = 0;
@@ -409,6 +460,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a, const double *zf) {
 // value being read and the value being written never share a slot.
 __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond,
                                                     int set_cond) {
+    pdl_enter();
     __shared__ double sm[33];
     const double zr = sum_partials(fslot(a, FP_ZR), a.ntiles, sm);
     const double zro = sum_partials(fslot(a, FP_ZRO), a.ntiles, sm);
@@ -426,6 +478,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
 
 // s = A p; partial <p, s>.
 __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
+    pdl_enter();
     __shared__ double sm[33];
     FP_ROW;
     double ps = 0;
@@ -440,6 +493,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
 
 // alpha = <z, r> / <p, s>; x += alpha p; r_old = r; r -= alpha s; |r|^2.
 __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
+    pdl_enter();
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const long long k = a.st->k;
@@ -460,7 +514,10 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
 }
 
 // k += 1 (its own launch: every block of the kernels around it reads k).
-__global__ void k_fp_tick(FpState *st) { st->k += 1; }
+__global__ void k_fp_tick(FpState *st) {
+    pdl_enter();
+    st->k += 1;
+}
 
 // t = b - A x, |t|^2 (atomics; the reported true residual).
 __global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const double *x, double *t,
@@ -475,9 +532,16 @@ __global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const dou
     if ((threadIdx.x & 31) == 0) atomicAdd(acc, q);
 }
 
-__global__ void k_log_f32(const double *k, float *xin, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        xin[2 * i + 1] = (float)log(k[i]);
+// Network input channel 1: the mean of log k over each f x f block.
+__global__ void k_log_coarse(const double *k, float *xin, int nx, int ny, int f) {
+    const int ncx = nx / f, nc = (nx / f) * (ny / f);
+    for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+        const int cx = ic % ncx, cy = ic / ncx;
+        double sum = 0;
+        for (int dy = 0; dy < f; ++dy)
+            for (int dx = 0; dx < f; ++dx) sum += log(k[(size_t)(cy * f + dy) * nx + cx * f + dx]);
+        xin[2 * ic + 1] = (float)(sum / (f * f));
+    }
 }
 
 __global__ void k_axpy_inplace(double *x, const double *d, int n) {
@@ -494,6 +558,7 @@ struct cfm_fpcg {
     const cfm_stencil *S = nullptr;
     cfm_unet *net = nullptr;
     int n = 0, ntiles = 0, nx = 0, ny = 0;
+    int coarsen = 1, nc = 0;  // the network runs on (nx / coarsen) x (ny / coarsen) = nc cells
     long long maxiter = 0;
     double tol = 0;
     double *vec = nullptr;  // x r rold p s z b t d za zb r1 (12 n)
@@ -535,6 +600,9 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.hist = h->hist;
     a.maxiter = h->maxiter;
     a.stall = 200;
+    a.f = h->coarsen;
+    a.ncx = h->nx / h->coarsen;
+    a.nc = h->nc;
     return a;
 }
 
@@ -544,41 +612,41 @@ FpArgs fp_args(cfm_fpcg *h) {
 // Jacobi sweeps on each side; then the new direction.
 int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
     cudaStream_t s = h->stream;
-    k_fp_prep<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    CFM_CUDA_TRY(launch_pdl(k_fp_prep, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
     double *buf[2] = {a.za, a.zb};
     const double *cur = nullptr;
     int nb = 0;
     for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
-        k_fp_jacobi<<<256, 256, 0, s>>>(a, cur, buf[nb]);
+        CFM_CUDA_TRY(launch_pdl(k_fp_jacobi, dim3(256), dim3(256), 0, s, a, cur, buf[nb]));
         cur = buf[nb];
     }
-    k_fp_r1<<<h->ntiles, CG_TILE, 0, s>>>(a, cur);
-    k_fp_in<<<h->ntiles, CG_TILE, 0, s>>>(a);
+    CFM_CUDA_TRY(launch_pdl(k_fp_r1, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur));
+    CFM_CUDA_TRY(launch_pdl(k_fp_in, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
     CFM_CUDA_TRY(cudaGetLastError());
     if (h->net) {
         int st = unet_forward(h->net->u, 1, h->xin, h->out, s);
         if (st) return st;
     } else {
-        k_fp_identity<<<256, 256, 0, s>>>(a);
+        CFM_CUDA_TRY(launch_pdl(k_fp_identity, dim3(256), dim3(256), 0, s, a));
     }
-    k_fp_ydots<<<h->ntiles, CG_TILE, 0, s>>>(a);
-    k_fp_corr<<<h->ntiles, CG_TILE, 0, s>>>(a, cur, buf[nb]);
+    CFM_CUDA_TRY(launch_pdl(k_fp_ydots, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
+    CFM_CUDA_TRY(launch_pdl(k_fp_corr, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur, buf[nb]));
     cur = buf[nb];
     nb ^= 1;
     for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
-        k_fp_jacobi<<<256, 256, 0, s>>>(a, cur, buf[nb]);
+        CFM_CUDA_TRY(launch_pdl(k_fp_jacobi, dim3(256), dim3(256), 0, s, a, cur, buf[nb]));
         cur = buf[nb];
     }
-    k_fp_z<<<h->ntiles, CG_TILE, 0, s>>>(a, cur);
-    k_fp_dir<<<h->ntiles, CG_TILE, 0, s>>>(a, cond, set_cond);
+    CFM_CUDA_TRY(launch_pdl(k_fp_z, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur));
+    CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
     CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
 }
 
 int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
-    k_fp_spmv<<<h->ntiles, CG_TILE, 0, h->stream>>>(a);
-    k_fp_update<<<h->ntiles, CG_TILE, 0, h->stream>>>(a);
-    k_fp_tick<<<1, 1, 0, h->stream>>>(a.st);
+    CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+    CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+    CFM_CUDA_TRY(launch_pdl(k_fp_tick, dim3(1), dim3(1), 0, h->stream, a.st));
     CFM_CUDA_TRY(cudaGetLastError());
     return fp_precond_dir(h, a, cond, set_cond);
 }
@@ -639,13 +707,17 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     CFM_ARG_CHECK(dims == 2, "the learned preconditioner is 2D");
     CFM_ARG_CHECK(tol > 0 && maxiter > 0, "tol, maxiter");
     CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
+    const int f = net ? net->coarsen : 1;
     if (net) {
         int H = 0, W = 0;
         unet_shape(net->u, &H, &W);
-        CFM_ARG_CHECK(H == ny && W == nx, "the network's grid must equal the stencil's");
+        CFM_ARG_CHECK((long long)H * f == ny && (long long)W * f == nx,
+                      "the network's grid must be the stencil's divided by the factor it was trained with");
         CFM_ARG_CHECK(smooth == net->smooth, "smooth must equal the sweeps the network was trained with");
     }
     cfm_fpcg *h = new cfm_fpcg();
+    h->coarsen = f;
+    h->nc = (nx / f) * (ny / f);
     h->smooth = smooth;
     h->S = S;
     h->net = net;
@@ -660,8 +732,8 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     std::vector<double> kk(k_host, k_host + n);
     double *kd = nullptr;
     if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->xin, sizeof(float) * 2 * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->out, sizeof(float) * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->xin, sizeof(float) * 2 * h->nc)) != cudaSuccess ||
+        (e = cudaMalloc(&h->out, sizeof(float) * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->ntiles)) != cudaSuccess ||
         (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
@@ -674,7 +746,7 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
         cfm_fpcg_destroy(h);
         CFM_CUDA_TRY(e);
     }
-    k_log_f32<<<256, 256>>>(kd, h->xin, h->n);
+    k_log_coarse<<<256, 256>>>(kd, h->xin, nx, ny, f);
     e = cudaDeviceSynchronize();
     cudaFree(kd);
     if (e != cudaSuccess) {
@@ -797,17 +869,20 @@ int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out
 // and `epochs` passes of Adam over it; loss values of the first and last
 // epoch (mean per-sample 1 - cos^2) are returned.
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
-                           int batch, float lr, int smooth, double *loss_first, double *loss_last,
-                           double *data_seconds, double *train_seconds) {
+                           int batch, float lr, int smooth, int coarsen, double *loss_first,
+                           double *loss_last, double *data_seconds, double *train_seconds) {
     clear_error();
     CFM_ARG_CHECK(net && nsys >= 1 && snaps >= 1 && epochs >= 1, "arguments");
     CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
-    net->smooth = smooth;
+    CFM_ARG_CHECK(coarsen == 1 || coarsen == 2, "coarsen must be 1 or 2");
     CFM_ARG_CHECK(batch >= 1 && batch <= net->maxB, "batch must be in [1, max_batch]");
+    net->smooth = smooth;
+    net->coarsen = coarsen;
     UNetImpl *u = net->u;
-    int H = 0, W = 0;
-    unet_shape(u, &H, &W);
-    const int n = H * W;
+    int Hc = 0, Wc = 0;
+    unet_shape(u, &Hc, &Wc);
+    const int f = coarsen, H = Hc * f, W = Wc * f;  // the systems' grid
+    const int n = H * W, nc = Hc * Wc;
     const int per = snaps + 1;  // + the initial residual b
     const long long N = (long long)nsys * per;
     cudaStream_t s = nullptr;
@@ -828,14 +903,15 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         *ptr = static_cast<std::remove_reference_t<decltype(**ptr)> *>(q);
         return e;
     };
-    float *xin_all, *coef_all, *gf, *az_b, *out_b, *dout_b;
+    float *xin_all, *r1_all, *coef_all, *gf, *az_b, *out_b, *dout_b;
     double *bd, *xs, *snap, *r, *e, *acc, *sums, *lossd, *er_all;
     long long *ids_d;
-    CFM_CUDA_TRY(alloc(&xin_all, sizeof(float) * 2 * (size_t)n * N));
+    CFM_CUDA_TRY(alloc(&xin_all, sizeof(float) * 2 * (size_t)nc * N));
+    CFM_CUDA_TRY(alloc(&r1_all, sizeof(float) * (size_t)n * N));
     CFM_CUDA_TRY(alloc(&coef_all, sizeof(float) * 3 * (size_t)n * nsys));
     CFM_CUDA_TRY(alloc(&er_all, sizeof(double) * N));
     CFM_CUDA_TRY(alloc(&ids_d, sizeof(long long) * batch));
-    CFM_CUDA_TRY(alloc(&gf, sizeof(float) * n));
+    CFM_CUDA_TRY(alloc(&gf, sizeof(float) * nc));
     CFM_CUDA_TRY(alloc(&bd, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&xs, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&snap, sizeof(double) * (size_t)n * snaps));
@@ -846,21 +922,27 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
     CFM_CUDA_TRY(alloc(&zs, sizeof(double) * 2 * n));
     CFM_CUDA_TRY(alloc(&r1s, sizeof(double) * n));
     CFM_CUDA_TRY(alloc(&az_b, sizeof(float) * (size_t)n * batch));
-    CFM_CUDA_TRY(alloc(&out_b, sizeof(float) * (size_t)n * batch));
-    CFM_CUDA_TRY(alloc(&dout_b, sizeof(float) * (size_t)n * batch));
+    CFM_CUDA_TRY(alloc(&out_b, sizeof(float) * (size_t)nc * batch));
+    CFM_CUDA_TRY(alloc(&dout_b, sizeof(float) * (size_t)nc * batch));
     CFM_CUDA_TRY(alloc(&sums, sizeof(double) * 2 * batch));
     CFM_CUDA_TRY(alloc(&lossd, sizeof(double)));
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<double> kh(n), fh(n);
-    std::vector<float> gh(n);
+    std::vector<float> gh(nc);
     int st = 0;
     for (int sy = 0; sy < nsys; ++sy) {
         if ((st = cfm_varcoef_problem(2, W, H, 1, seed0 + sy, kh.data(), fh.data()))) return st;
-        for (int i = 0; i < n; ++i) gh[i] = (float)std::log(kh[i]);
+        for (int ic = 0; ic < nc; ++ic) {  // block-mean log k on the network's grid
+            const int cx = ic % Wc, cy = ic / Wc;
+            double sum = 0;
+            for (int dy = 0; dy < f; ++dy)
+                for (int dx = 0; dx < f; ++dx) sum += std::log(kh[(size_t)(cy * f + dy) * W + cx * f + dx]);
+            gh[ic] = (float)(sum / (f * f));
+        }
         cfm_stencil *S = nullptr;
         if ((st = cfm_stencil_create(2, W, H, 1, kh.data(), &S))) return st;
         CFM_CUDA_TRY(cudaMemcpyAsync(bd, fh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
-        CFM_CUDA_TRY(cudaMemcpyAsync(gf, gh.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        CFM_CUDA_TRY(cudaMemcpyAsync(gf, gh.data(), sizeof(float) * nc, cudaMemcpyHostToDevice, s));
         long long K = 0;
         st = cg_stencil_snapshots(S, bd, xs, 1e-10, 200000, nullptr, 1, 0, &K, nullptr, s);
         int taken = 0;
@@ -898,7 +980,8 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                 k_data_smoothed<<<256, 256, 0, s>>>(o2, n, cur, r, e, r1s, acc);
                 rin = r1s;
             }
-            k_pair_store<<<256, 256, 0, s>>>(n, rin, gf, acc, xin_all + idx * 2 * n, er_all + idx);
+            k_pair_store<<<256, 256, 0, s>>>(W, H, f, rin, gf, acc, xin_all + idx * 2 * nc,
+                                             r1_all + idx * n, er_all + idx);
         }
         CFM_CUDA_TRY(cudaStreamSynchronize(s));
         cfm_stencil_destroy(S2);
@@ -917,17 +1000,17 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         for (long long i0 = 0; i0 + batch <= N; i0 += batch) {
             for (int bi = 0; bi < batch; ++bi) {
                 const long long id = order[i0 + bi];
-                CFM_CUDA_TRY(cudaMemcpyAsync(net->xin + (size_t)bi * 2 * n, xin_all + (size_t)id * 2 * n,
-                                             sizeof(float) * 2 * n, cudaMemcpyDeviceToDevice, s));
+                CFM_CUDA_TRY(cudaMemcpyAsync(net->xin + (size_t)bi * 2 * nc, xin_all + (size_t)id * 2 * nc,
+                                             sizeof(float) * 2 * nc, cudaMemcpyDeviceToDevice, s));
             }
             // the ids are read by the loss kernels queued below: copy synchronously
             CFM_CUDA_TRY(cudaStreamSynchronize(s));
             CFM_CUDA_TRY(cudaMemcpy(ids_d, &order[i0], sizeof(long long) * batch, cudaMemcpyHostToDevice));
             if ((st = unet_forward(u, batch, net->xin, out_b, s))) return st;
             CFM_CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(double) * 2 * batch, s));
-            k_loss_anorm_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, net->xin, coef_all, ids_d, per, W,
-                                                             H, az_b, sums);
-            k_loss_anorm_grad<<<dim3(64, batch), 256, 0, s>>>(az_b, net->xin, sums, er_all, ids_d, n,
+            k_loss_anorm_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, r1_all, coef_all, ids_d, per, W,
+                                                             H, f, az_b, sums);
+            k_loss_anorm_grad<<<dim3(64, batch), 256, 0, s>>>(az_b, r1_all, sums, er_all, ids_d, W, H, f,
                                                              batch, dout_b, lossd);
             CFM_CUDA_TRY(cudaMemsetAsync(unet_grad(u), 0, unet_params(u) * sizeof(float), s));
             if ((st = unet_backward(u, batch, net->xin, dout_b, s))) return st;

@@ -65,69 +65,109 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
     *reinterpret_cast<uint4 *>(p) = u;
 }
 
-// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Four threads per
-// pixel, each producing 8 of the 32 output channels (one 16-byte store).
-__global__ void k_cin_fwd(const float *x, const float *w, const float *b, bf16 *h0, int B, int H,
-                          int W) {
-    __shared__ float sw[9 * 32 * 2 + 32];
-    for (int i = threadIdx.x; i < 9 * 64 + 32; i += blockDim.x) sw[i] = i < 576 ? w[i] : b[i - 576];
-    __syncthreads();
-    const long long P = (long long)B * H * W;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 4 * P;
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long p = e >> 2;
-        const int c0 = (int)(e & 3) * 8;
-        const int xx = (int)(p % W), yy = (int)((p / W) % H);
-        const long long img0 = p - (long long)yy * W - xx;
-        float o[8];
+// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Eight threads per
+// pixel, each producing 4 channels (one 8-byte store; a warp writes 4 whole
+// pixels) with its 72 weights and 4 biases held in registers across
+// CIN_PASSES pixels.  The 9 input loads of a pixel are issued together from
+// clamped coordinates and zeroed outside the image.
+// grid: (ceil(W / (32 CIN_PASSES)), H, B), 256 threads.
+constexpr int CIN_PASSES = 8;
+__global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w, const float *b,
+                                                 bf16 *h0, int H, int W) {
+    pdl_enter();
+    const int q = threadIdx.x & 7, c0 = q * 4;
+    float wr[9][8];  // [t][(c - c0) * 2 + in]
 #pragma unroll
-        for (int c = 0; c < 8; ++c) o[c] = sw[576 + c0 + c];
+    for (int t = 0; t < 9; ++t) {
+        const float4 w0 = *reinterpret_cast<const float4 *>(w + t * 64 + c0 * 2);
+        const float4 w1 = *reinterpret_cast<const float4 *>(w + t * 64 + c0 * 2 + 4);
+        wr[t][0] = w0.x, wr[t][1] = w0.y, wr[t][2] = w0.z, wr[t][3] = w0.w;
+        wr[t][4] = w1.x, wr[t][5] = w1.y, wr[t][6] = w1.z, wr[t][7] = w1.w;
+    }
+    const float4 bq = *reinterpret_cast<const float4 *>(b + c0);
+    const int yy = blockIdx.y, img = blockIdx.z;
+    const float *xi = x + (size_t)img * H * W * 2;
+    bf16 *hrow = h0 + ((size_t)img * H + yy) * W * 32;
+#pragma unroll 1
+    for (int pass = 0; pass < CIN_PASSES; ++pass) {
+        const int xx = (blockIdx.x * CIN_PASSES + pass) * 32 + (threadIdx.x >> 3);
+        if (xx >= W) break;
+        float2 v[9];
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
             const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-            if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
-            const float2 v = *reinterpret_cast<const float2 *>(x + 2 * (img0 + (long long)y * W + xq));
-#pragma unroll
-            for (int c = 0; c < 8; ++c)
-                o[c] += sw[(t * 32 + c0 + c) * 2] * v.x + sw[(t * 32 + c0 + c) * 2 + 1] * v.y;
+            const bool in = y >= 0 && y < H && xq >= 0 && xq < W;
+            const int yc = min(max(y, 0), H - 1), xc = min(max(xq, 0), W - 1);
+            v[t] = *reinterpret_cast<const float2 *>(xi + 2 * (yc * W + xc));
+            if (!in) v[t] = make_float2(0.f, 0.f);
         }
+        float o[4] = {bq.x, bq.y, bq.z, bq.w};
 #pragma unroll
-        for (int c = 0; c < 8; ++c) o[c] = fmaxf(o[c], 0.f);
-        store8(h0 + p * 32 + c0, o);
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) o[c] += wr[t][2 * c] * v[t].x + wr[t][2 * c + 1] * v[t].y;
+        __nv_bfloat162 r[2];
+        r[0] = __floats2bfloat162_rn(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f));
+        r[1] = __floats2bfloat162_rn(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f));
+        *reinterpret_cast<uint2 *>(hrow + (size_t)xx * 32 + c0) = *reinterpret_cast<const uint2 *>(r);
     }
 }
 
 // out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.  Four threads
-// per pixel, each summing 8 channels over the 9 taps (one 16-byte load per
-// tap), combined by two xor shuffles.
-__global__ void k_cout_fwd(const bf16 *g0, const float *w, const float *b, float *out, int B, int H,
-                           int W) {
-    __shared__ float sw[9 * 32 + 1];
-    for (int i = threadIdx.x; i < 289; i += blockDim.x) sw[i] = i < 288 ? w[i] : b[0];
-    __syncthreads();
-    const long long P = (long long)B * H * W;
-    // the loop bound is a multiple of 4 per pixel, so the 4 lanes of a pixel stay together
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ((4 * P + 31) & ~31LL);
-         e += (long long)gridDim.x * blockDim.x) {
-        const long long p = e >> 2;
-        const int c0 = (int)(e & 3) * 8;
+// per pixel (a warp reads 8 whole pixels, 512 contiguous bytes, per tap),
+// each summing one 8-channel group over the 9 taps with its 72 weights held
+// in registers across COUT_PASSES pixels; the 9 loads of a pixel are issued
+// together from clamped coordinates and zeroed outside the image; two xor
+// shuffles add the groups, (g0 + g1) + (g2 + g3).
+// grid: (ceil(W / (64 COUT_PASSES)), H, B), 256 threads.
+constexpr int COUT_PASSES = 4;
+__global__ void __launch_bounds__(256, 2) k_cout_fwd(const bf16 *g0, const float *w, const float *b,
+                                                     float *out, int H, int W) {
+    pdl_enter();
+    const int q = threadIdx.x & 3, c0 = q * 8;
+    float wr[9][8];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+        const float4 w0 = *reinterpret_cast<const float4 *>(w + t * 32 + c0);
+        const float4 w1 = *reinterpret_cast<const float4 *>(w + t * 32 + c0 + 4);
+        wr[t][0] = w0.x, wr[t][1] = w0.y, wr[t][2] = w0.z, wr[t][3] = w0.w;
+        wr[t][4] = w1.x, wr[t][5] = w1.y, wr[t][6] = w1.z, wr[t][7] = w1.w;
+    }
+    const float bias = b[0];
+    const int yy = blockIdx.y, img = blockIdx.z;
+    const bf16 *gi = g0 + (size_t)img * H * W * 32;
+    float *oi = out + ((size_t)img * H + yy) * W;
+#pragma unroll 1
+    for (int pass = 0; pass < COUT_PASSES; ++pass) {
+        // every lane stays to the shuffles; those past the row end sum zero
+        const int xx = (blockIdx.x * COUT_PASSES + pass) * 64 + (threadIdx.x >> 2);
+        const bool valid = xx < W;
+        uint4 raw[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
+            const bool in = valid && y >= 0 && y < H && xq >= 0 && xq < W;
+            const int yc = min(max(y, 0), H - 1), xc = min(max(xq, 0), W - 1);
+            raw[t] = *reinterpret_cast<const uint4 *>(gi + (size_t)(yc * W + xc) * 32 + c0);
+            if (!in) raw[t] = make_uint4(0u, 0u, 0u, 0u);
+        }
         float acc = 0.f;
-        if (p < P) {
-            const int xx = (int)(p % W), yy = (int)((p / W) % H);
-            const long long img0 = p - (long long)yy * W - xx;
 #pragma unroll
-            for (int t = 0; t < 9; ++t) {
-                const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-                if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
-                float v[8];
-                load8(g0 + (img0 + (long long)y * W + xq) * 32 + c0, v);
+        for (int t = 0; t < 9; ++t) {
+            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw[t]);
+            float v[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc += sw[t * 32 + c0 + j] * v[j];
+            for (int i = 0; i < 4; ++i) {
+                const float2 f = __bfloat1622float2(h[i]);
+                v[2 * i] = f.x;
+                v[2 * i + 1] = f.y;
             }
+            acc += wr[t][0] * v[0] + wr[t][1] * v[1] + wr[t][2] * v[2] + wr[t][3] * v[3] +
+                   wr[t][4] * v[4] + wr[t][5] * v[5] + wr[t][6] * v[6] + wr[t][7] * v[7];
         }
         acc += __shfl_xor_sync(0xffffffffu, acc, 1);
         acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (p < P && (e & 3) == 0) out[p] = acc + sw[288];
+        if (valid && q == 0) oi[xx] = acc + bias;
     }
 }
 
@@ -196,44 +236,46 @@ __global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, floa
     }
 }
 
-// 2x2 mean pool, NHWC, 8 channels per thread.
-__global__ void k_pool(const bf16 *in, bf16 *out, int B, int h, int w, int C) {
-    const long long n = (long long)B * h * w * (C / 8);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int c8 = (int)(e % (C / 8)) * 8;
-        const long long pix = e / (C / 8);
-        const int x = (int)(pix % w), y = (int)((pix / w) % h), img = (int)(pix / ((long long)w * h));
-        const long long W2 = 2LL * w;
-        const long long base = (((long long)img * 2 * h + 2 * y) * W2 + 2 * x) * C + c8;
-        float a[8], b[8], c[8], d[8], o[8];
-        load8(in + base, a);
-        load8(in + base + C, b);
-        load8(in + base + W2 * C, c);
-        load8(in + base + W2 * C + C, d);
+// 2x2 mean pool, NHWC, 8 channels per thread; (h, w) is the pooled size.
+// grid: (items of a pooled row / blockDim, h, B).
+template <int C>
+__global__ void k_pool(const bf16 *in, bf16 *out, int h, int w) {
+    pdl_enter();
+    constexpr int G = C / 8;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= w * G) return;
+    const int y = blockIdx.y, img = blockIdx.z;
+    const int c8 = (e % G) * 8, x = e / G;
+    const size_t W2 = 2 * (size_t)w;
+    const size_t base = (((size_t)img * 2 * h + 2 * y) * W2 + 2 * x) * C + c8;
+    float a[8], b[8], c[8], d[8], o[8];
+    load8(in + base, a);
+    load8(in + base + C, b);
+    load8(in + base + W2 * C, c);
+    load8(in + base + W2 * C + C, d);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) o[j] = 0.25f * (((a[j] + b[j]) + c[j]) + d[j]);
-        store8(out + pix * C + c8, o);
-    }
+    for (int j = 0; j < 8; ++j) o[j] = 0.25f * (((a[j] + b[j]) + c[j]) + d[j]);
+    store8(out + (((size_t)img * h + y) * w + x) * C + c8, o);
 }
 
-// u = up(g) + skip at the finer level (2h x 2w).
-__global__ void k_up_add(const bf16 *g, const bf16 *skip, bf16 *u, int B, int h, int w, int C) {
-    const long long n = (long long)B * 4 * h * w * (C / 8);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int c8 = (int)(e % (C / 8)) * 8;
-        const long long pix = e / (C / 8);
-        const int x = (int)(pix % (2 * w)), y = (int)((pix / (2 * w)) % (2 * h));
-        const int img = (int)(pix / (4LL * h * w));
-        const long long cp = ((long long)img * h + y / 2) * w + x / 2;
-        float a[8], b[8];
-        load8(g + cp * C + c8, a);
-        load8(skip + pix * C + c8, b);
+// u = up(g) + skip at the finer level (2h x 2w; (h, w) is the coarse size).
+// grid: (items of a fine row / blockDim, 2h, B).
+template <int C>
+__global__ void k_up_add(const bf16 *g, const bf16 *skip, bf16 *u, int h, int w) {
+    pdl_enter();
+    constexpr int G = C / 8;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 2 * w * G) return;
+    const int y = blockIdx.y, img = blockIdx.z;
+    const int c8 = (e % G) * 8, x = e / G;
+    const size_t cp = ((size_t)img * h + y / 2) * w + x / 2;
+    const size_t pix = ((size_t)img * 2 * h + y) * 2 * w + x;
+    float a[8], b[8];
+    load8(g + cp * C + c8, a);
+    load8(skip + pix * C + c8, b);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) a[j] += b[j];
-        store8(u + pix * C + c8, a);
-    }
+    for (int j = 0; j < 8; ++j) a[j] += b[j];
+    store8(u + pix * C + c8, a);
 }
 
 // dz[coarse] = (sum of the 2x2 fine gradients) * (act[coarse] > 0).
@@ -327,6 +369,9 @@ int grid_for(long long n, int per = 256) {
     return (int)std::max(1LL, std::min((n + per - 1) / per, 148LL * 16));
 }
 
+// One block row per image row: (ceil(items / 256), rows, images).
+dim3 row_grid(int items, int rows, int images) { return dim3((items + 255) / 256, rows, images); }
+
 }  // namespace
 
 // --------------------------------------------------------------- the net
@@ -347,6 +392,7 @@ struct UNetImpl {
     bf16 *wb[UNET_NLAYERS] = {}, *wt[UNET_NLAYERS] = {};
     UNetBuffers a{};
     int *err = nullptr;
+    float *ws = nullptr;  // split-K workspace of the convolutions (TC_WS_FLOATS)
     long long adam_t = 0;
     std::vector<void *> allocs;
 };
@@ -398,6 +444,7 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     if (!st) st = dalloc(u, &u->m, o);
     if (!st) st = dalloc(u, &u->v, o);
     if (!st) st = dalloc(u, &u->err, 1);
+    if (!st) st = dalloc(u, &u->ws, (size_t)TC_WS_FLOATS);
     for (int l = 0; l < UNET_NLAYERS; ++l)
         if (UNET_LAYERS[l].tc) {
             const size_t n = 9 * (size_t)UNET_LAYERS[l].co * UNET_LAYERS[l].ci;
@@ -463,6 +510,8 @@ namespace {
 int conv_fwd(UNetImpl *u, int l, const bf16 *x, bf16 *out, int B, int h, int w, cudaStream_t s) {
     const UNetLayer &L = UNET_LAYERS[l];
     ConvArgs c{x, u->wb[l], u->theta + u->boff[l], nullptr, out, u->err, B, h, w, L.ci, L.co, 1};
+    c.ws = u->ws;
+    c.ws_floats = TC_WS_FLOATS;
     return tc_conv_fwd(c, s);
 }
 
@@ -471,6 +520,8 @@ int conv_bwd_data(UNetImpl *u, int l, const bf16 *dz, const bf16 *mask, bf16 *dx
                   int w, cudaStream_t s) {
     const UNetLayer &L = UNET_LAYERS[l];
     ConvArgs c{dz, u->wt[l], nullptr, mask, dx, u->err, B, h, w, L.co, L.ci, 0};
+    c.ws = u->ws;
+    c.ws_floats = TC_WS_FLOATS;
     return tc_conv_fwd(c, s);
 }
 
@@ -499,33 +550,39 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s)
     CFM_ARG_CHECK(B >= 1 && B <= u->maxB, "batch");
     UNetBuffers &a = u->a;
     const int H = u->H, W = u->W;
-    const long long P0 = (long long)B * H * W;
     int st;
-    k_cin_fwd<<<grid_for(4 * P0), 256, 0, s>>>(x, u->theta + u->woff[0], u->theta + u->boff[0], a.h0, B, H, W);
-    CFM_CUDA_TRY(cudaGetLastError());
+    CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + 32 * CIN_PASSES - 1) / (32 * CIN_PASSES), H, B), dim3(256),
+                            0, s, x, (const float *)(u->theta + u->woff[0]),
+                            (const float *)(u->theta + u->boff[0]), a.h0, H, W));
     int h = H, w = W;
-    k_pool<<<grid_for(P0 / 4 * 4), 256, 0, s>>>(a.h0, a.p1, B, h / 2, w / 2, 32);
+    CFM_CUDA_TRY(launch_pdl(k_pool<32>, row_grid(w / 2 * 4, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h0,
+                            a.p1, h / 2, w / 2));
     h /= 2, w /= 2;
     if ((st = conv_fwd(u, 1, a.p1, a.h1, B, h, w, s))) return st;
-    k_pool<<<grid_for(P0 / 16 * 8), 256, 0, s>>>(a.h1, a.p2, B, h / 2, w / 2, 64);
+    CFM_CUDA_TRY(launch_pdl(k_pool<64>, row_grid(w / 2 * 8, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h1,
+                            a.p2, h / 2, w / 2));
     h /= 2, w /= 2;
     if ((st = conv_fwd(u, 2, a.p2, a.h2, B, h, w, s))) return st;
-    k_pool<<<grid_for(P0 / 64 * 16), 256, 0, s>>>(a.h2, a.p3, B, h / 2, w / 2, 128);
+    CFM_CUDA_TRY(launch_pdl(k_pool<128>, row_grid(w / 2 * 16, h / 2, B), dim3(256), 0, s,
+                            (const bf16 *)a.h2, a.p3, h / 2, w / 2));
     h /= 2, w /= 2;
     if ((st = conv_fwd(u, 3, a.p3, a.h3, B, h, w, s))) return st;
     if ((st = conv_fwd(u, 4, a.h3, a.g3, B, h, w, s))) return st;
-    k_up_add<<<grid_for(P0 / 16 * 16), 256, 0, s>>>(a.g3, a.h2, a.u2, B, h, w, 128);
+    CFM_CUDA_TRY(launch_pdl(k_up_add<128>, row_grid(2 * w * 16, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g3, (const bf16 *)a.h2, a.u2, h, w));
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 5, a.u2, a.g2, B, h, w, s))) return st;
-    k_up_add<<<grid_for(P0 / 4 * 8), 256, 0, s>>>(a.g2, a.h1, a.u1, B, h, w, 64);
+    CFM_CUDA_TRY(launch_pdl(k_up_add<64>, row_grid(2 * w * 8, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g2, (const bf16 *)a.h1, a.u1, h, w));
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 6, a.u1, a.g1, B, h, w, s))) return st;
-    k_up_add<<<grid_for(P0 * 4), 256, 0, s>>>(a.g1, a.h0, a.u0, B, h, w, 32);
+    CFM_CUDA_TRY(launch_pdl(k_up_add<32>, row_grid(2 * w * 4, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g1, (const bf16 *)a.h0, a.u0, h, w));
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 7, a.u0, a.g0, B, h, w, s))) return st;
-    k_cout_fwd<<<grid_for(4 * P0), 256, 0, s>>>(a.g0, u->theta + u->woff[8], u->theta + u->boff[8], out,
-                                                B, H, W);
-    CFM_CUDA_TRY(cudaGetLastError());
+    CFM_CUDA_TRY(launch_pdl(k_cout_fwd, dim3((W + 64 * COUT_PASSES - 1) / (64 * COUT_PASSES), H, B),
+                            dim3(256), 0, s, (const bf16 *)a.g0, (const float *)(u->theta + u->woff[8]),
+                            (const float *)(u->theta + u->boff[8]), out, H, W));
     return CFM_OK;
 }
 

@@ -41,5 +41,6 @@ struct cfm_unet {
     cfm::UNetImpl *u = nullptr;
     float *xin = nullptr, *out = nullptr, *dout = nullptr;
     int maxB = 0;
-    int smooth = 0;  // Jacobi sweeps around the network it was trained for
+    int smooth = 0;   // Jacobi sweeps around the network it was trained for
+    int coarsen = 1;  // the systems' grid is the network's times this factor
 };

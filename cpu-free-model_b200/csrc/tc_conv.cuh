@@ -8,11 +8,18 @@
 //
 //  conv (forward, and backward-data with flipped/transposed weights):
 //    m = 128 output pixels (a bx x by block of one image), n = output
-//    channel, k = (tap, input channel chunk).  A tile for tap (dy, dx) is the
-//    activation box at (c0, x0 + dx - 1, y0 + dy - 1, img) of the NHWC tensor;
-//    coordinates outside the image read as zero, which is the padding.
+//    channel, k = (tap, input channel chunk).  Coordinates outside the image
+//    read as zero, which is the padding.  Two ways to stage A:
+//      halo (bx = 128): per (chunk, dy) one box of the 130 pixels
+//        x0 - 1 .. x0 + 128 of row y0 + dy - 1; the three dx taps are the
+//        descriptors starting 0, 1 and 2 rows into it (the swizzle follows
+//        the absolute shared-memory address, so a row-shifted start reads
+//        the shifted rows).  A third of the TMA requests of 9 tap boxes.
+//      per tap (bx < 128): the box at (c0, x0 + dx - 1, y0 + dy - 1, img).
+//    B (weights) either streams with A or, when a CTA runs several tiles
+//    and they fit, stays resident: all 9 x nch tiles loaded once per CTA.
 //    Epilogue: + bias, optional ReLU, optional mask (zero where mask <= 0),
-//    BF16 store NHWC.
+//    BF16 store NHWC (lane pairs write whole 32-byte sectors).
 //  weight gradient:
 //    m = (tap of a tap group, input channel), n = output channel, k = pixels
 //    (KC consecutive x of one row per step).  A rows come from x-shifted
@@ -21,18 +28,20 @@
 //    the channel-major output gradient.  Tiles split K; the epilogue adds
 //    its partial tile to dW[tap][co][ci] (FP32 atomics).
 //
-// One persistent CTA per SM, 6 warps: warp 0 issues TMA (one elected lane),
-// warp 1 owns TMEM and issues tcgen05.mma (one lane), warps 2-5 drain the
-// accumulator (tcgen05.ld, 32 TMEM lanes each).  A ring of STAGES operand
-// buffers (full/empty mbarriers) and two TMEM accumulators (acc_full /
-// acc_empty) overlap loads, MMAs and the epilogue of the previous tile.
-// Every wait is bounded; on a timeout the CTA records an error, lets its
-// in-flight copies and MMAs land (bounded), frees TMEM and returns.
+// Persistent CTAs (one or two per SM, as the host plan says), 6 warps: warp
+// 0 issues TMA (one elected lane), warp 1 owns TMEM and issues tcgen05.mma
+// (one lane), warps 2-5 drain the accumulator (tcgen05.ld, 32 TMEM lanes
+// each).  A ring of operand slots (full/empty mbarriers) and two TMEM
+// accumulators (acc_full / acc_empty) overlap loads, MMAs and the epilogue
+// of the previous tile.  Every wait is bounded; on a timeout the CTA
+// records an error, lets its in-flight copies and MMAs land (bounded),
+// frees TMEM and returns.
 #pragma once
 
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include "cfm_internal.h"
 #include "tma.cuh"
 
 namespace cfm {
@@ -129,12 +138,23 @@ struct TcConvParams {
     int B, H, W;
     int Cin, Cout;  // of the convolution this pass belongs to (conv mode: Cin -> Cout = N)
     int ntiles;
-    int ksteps;  // conv: 9 * Cin / KC; wgrad: steps per split
+    int ksteps;  // conv: 3 * nch (halo) or 9 * nch; wgrad: steps per split
     // conv mode tiling
     int bx, by, tiles_x, tiles_y;
+    int nch;   // Cin / KC
+    int halo;  // one (bx + 2)-pixel box per (chunk, dy); the dx taps are row offsets into it
+    int wres;  // every weight tile resident in shared memory, loaded once per CTA
+    int csplit;  // split-K: work item t = (pixel tile t / csplit, k range t % csplit)
+    float *ws;   // csplit > 1: FP32 partials [csplit][B H W][N], reduced by tc_splitk_epilogue
+    long long ws_floats;  // capacity of ws (0: no split)
     // wgrad mode tiling
     int ci_rows, ci_tiles, taps_per_tile, tap_groups, ksplit;
     long long total_k;  // B * H * (W / KC)
+    // shared-memory plan
+    int stages;       // operand ring depth
+    int stage_bytes;  // one ring slot (a multiple of 1024)
+    int a_region;     // bytes of the A part of a slot; B (if streamed) follows it
+    int wres_bytes;   // resident weight region in front of the ring (a multiple of 1024)
     // epilogue
     const float *bias;
     int relu;
@@ -145,38 +165,60 @@ struct TcConvParams {
     unsigned long long budget_ns;
 };
 
-template <int KC, int N>
-struct TcGeom {
-    static constexpr int SW = KC * 2;
-    static constexpr int A_BYTES = 128 * SW;
-    static constexpr int B_BYTES = N * SW;
-    static constexpr int STAGE = (A_BYTES + B_BYTES + 1023) / 1024 * 1024;
-    // Narrow tiles (N <= 64) keep the ring near 100 KB so two CTAs share an
-    // SM (two independent load / MMA / epilogue pipelines, 2 x 2N TMEM
-    // columns); wide ones take up to 200 KB alone.  At most 16 stages.
-    static constexpr int BUDGET = (N <= 64 ? 100 : 200) * 1024;
-    static constexpr int STAGES = BUDGET / STAGE > 16 ? 16 : BUDGET / STAGE;
-    // + 1024 alignment slack + full/empty/acc/drain mbarriers and the TMEM base slot
-    static constexpr size_t SMEM = (size_t)STAGES * STAGE + 1024 + (2 * STAGES + 8) * 8;
-    static constexpr uint32_t TMEM_COLS = 2 * N < 32 ? 32 : 2 * N;
-};
+// Rows of a halo box: the 128 output pixels of a tile plus one on each side.
+constexpr int TC_HALO_ROWS = 130;
+// Shared-memory bytes of a conv pass with this plan: 1024 alignment slack,
+// the resident weights, the ring, the full/empty/acc/drain/weight mbarriers
+// and the TMEM base slot.
+__host__ __device__ constexpr size_t tc_conv_smem(int wres_bytes, int stages, int stage_bytes) {
+    return 1024 + (size_t)wres_bytes + (size_t)stages * stage_bytes + (2 * (size_t)stages + 8) * 8 + 16;
+}
+
+template <int N>
+__host__ __device__ constexpr uint32_t tc_tmem_cols() {
+    return 2 * N < 32 ? 32 : 2 * N;
+}
+
+// Stores 16 BF16 channels of pixel pairs (lanes 2i, 2i + 1) so that each
+// store instruction writes whole 32-byte sectors: the even lane writes the
+// first 16 bytes and the odd lane the second 16 bytes of one pixel, first
+// for the even lane's pixel, then for the odd lane's.
+__device__ __forceinline__ void store16_pairs(__nv_bfloat16 *pix_even, __nv_bfloat16 *pix_odd,
+                                              bool in_even, bool in_odd, int lane, const uint4 &lo,
+                                              const uint4 &hi) {
+    const bool odd = lane & 1;
+    const uint4 give = odd ? lo : hi;  // the half the partner lane needs
+    uint4 got;
+    got.x = __shfl_xor_sync(0xffffffffu, give.x, 1);
+    got.y = __shfl_xor_sync(0xffffffffu, give.y, 1);
+    got.z = __shfl_xor_sync(0xffffffffu, give.z, 1);
+    got.w = __shfl_xor_sync(0xffffffffu, give.w, 1);
+    const int half = odd ? 8 : 0;
+    if (in_even) *reinterpret_cast<uint4 *>(pix_even + half) = odd ? got : lo;
+    if (in_odd) *reinterpret_cast<uint4 *>(pix_odd + half) = odd ? hi : got;
+}
 
 template <int KC, int N>
-__global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
+__global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
     tc_conv_kernel(const __grid_constant__ CUtensorMap mapA0, const __grid_constant__ CUtensorMap mapA1,
                    const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB,
                    TcConvParams p) {
-    using G = TcGeom<KC, N>;
-    constexpr int STAGES = G::STAGES;
+    constexpr int SW = KC * 2;              // bytes of one operand row (the swizzle span)
+    constexpr int BTAP = N * SW;            // one weight tile (N rows)
+    constexpr uint32_t TMEM_COLS = tc_tmem_cols<N>();
+    const int STAGES = p.stages;
     extern __shared__ unsigned char tc_smem_raw[];
     unsigned char *smem =
         (unsigned char *)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * G::STAGE);
+    unsigned char *wres = smem;                  // [9][nch] weight tiles (when p.wres)
+    unsigned char *ring = smem + p.wres_bytes;   // STAGES slots of p.stage_bytes
+    uint64_t *full = reinterpret_cast<uint64_t *>(ring + (size_t)STAGES * p.stage_bytes);
     uint64_t *empty = full + STAGES;
     uint64_t *acc_full = empty + STAGES;   // [2]
     uint64_t *acc_empty = acc_full + 2;    // [2]
     uint64_t *drain = acc_empty + 2;       // [1]
-    uint32_t *tmem_base_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint64_t *wbar = drain + 1;            // [1]
+    uint32_t *tmem_base_slot = reinterpret_cast<uint32_t *>(wbar + 1);
     __shared__ int s_abort;
     __shared__ float s_bias[N];
 
@@ -191,14 +233,18 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
             mbar_init(&acc_empty[b], 4);
         }
         mbar_init(drain, 1);
+        mbar_init(wbar, 1);
         s_abort = 0;
         mbar_fence_init();
     }
-    for (int c = threadIdx.x; c < N; c += blockDim.x) s_bias[c] = p.bias ? p.bias[c] : 0.f;
     if (warp == 1) {
-        tmem_alloc(tmem_base_slot, G::TMEM_COLS);
+        tmem_alloc(tmem_base_slot, TMEM_COLS);
         tmem_relinquish();
     }
+    // everything above is on-chip set-up; global memory only after the
+    // predecessor kernel has completed (programmatic dependent launch)
+    pdl_enter();
+    for (int c = threadIdx.x; c < N; c += blockDim.x) s_bias[c] = p.bias ? p.bias[c] : 0.f;
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -209,42 +255,62 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
         atomicCAS(p.err, 0, code);
         *abort_flag = 1;
     };
+    const bool conv = p.mode == 0;
+    const bool use_wres = conv && p.wres;
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA
         if (lane == 0) {
+            bool wres_loaded = false;
+            if (use_wres) {
+                // all 9 * nch weight tiles, once, on their own barrier
+                mbar_arrive_expect_tx(wbar, (unsigned)(9 * p.nch * BTAP));
+                for (int tap = 0; tap < 9; ++tap)
+                    for (int ch = 0; ch < p.nch; ++ch)
+                        tma_load_3d(wres + (size_t)(tap * p.nch + ch) * BTAP, &mapB, ch * KC, 0, tap, wbar);
+                wres_loaded = true;
+            }
             unsigned it = 0;
             for (int t = blockIdx.x; t < p.ntiles && !*abort_flag; t += gridDim.x) {
                 int img = 0, y0 = 0, x0 = 0, g = 0, ct = 0;
                 long long k0 = 0;
-                if (p.mode == 0) {
-                    const int tx = t % p.tiles_x, rest = t / p.tiles_x;
+                int q0 = 0, q1 = 0;
+                if (conv) {
+                    const int pt = t / p.csplit, sp = t % p.csplit;
+                    const int tx = pt % p.tiles_x, rest = pt / p.tiles_x;
                     x0 = tx * p.bx;
                     y0 = (rest % p.tiles_y) * p.by;
                     img = rest / p.tiles_y;
+                    q0 = p.ksteps * sp / p.csplit;
+                    q1 = p.ksteps * (sp + 1) / p.csplit;
                 } else {
                     const int s = t % p.ksplit, rest = t / p.ksplit;
                     ct = rest % p.ci_tiles;
                     g = rest / p.ci_tiles;
                     k0 = p.total_k * s / p.ksplit;
+                    q1 = (int)(p.total_k * ((t % p.ksplit) + 1) / p.ksplit - k0);
                 }
-                const int nsteps = p.mode == 0 ? p.ksteps
-                                               : (int)(p.total_k * ((t % p.ksplit) + 1) / p.ksplit - k0);
-                for (int q = 0; q < nsteps; ++q, ++it) {
+                for (int q = q0; q < q1; ++q, ++it) {
                     const int st = it % STAGES;
                     if (!mbar_wait_bounded(&empty[st], ((it / STAGES) & 1) ^ 1, budget)) {
                         fail(1);
                         break;
                     }
-                    unsigned char *a_dst = smem + st * G::STAGE;
-                    unsigned char *b_dst = a_dst + G::A_BYTES;
-                    if (p.mode == 0) {
-                        const int nch = p.Cin / KC;
-                        const int tap = q / nch, c0 = (q % nch) * KC;
+                    unsigned char *a_dst = ring + (size_t)st * p.stage_bytes;
+                    unsigned char *b_dst = a_dst + p.a_region;
+                    if (conv && p.halo) {
+                        const int ch = q / 3, dy = q % 3;
+                        mbar_arrive_expect_tx(&full[st], TC_HALO_ROWS * SW + (use_wres ? 0 : 3 * BTAP));
+                        tma_load_4d(a_dst, &mapA1, ch * KC, x0 - 1, y0 + dy - 1, img, &full[st]);
+                        if (!use_wres)
+                            for (int dx = 0; dx < 3; ++dx)
+                                tma_load_3d(b_dst + dx * BTAP, &mapB, ch * KC, 0, dy * 3 + dx, &full[st]);
+                    } else if (conv) {
+                        const int tap = q / p.nch, ch = q % p.nch;
                         const int dy = tap / 3, dx = tap % 3;
-                        mbar_arrive_expect_tx(&full[st], G::A_BYTES + G::B_BYTES);
-                        tma_load_4d(a_dst, &mapA0, c0, x0 + dx - 1, y0 + dy - 1, img, &full[st]);
-                        tma_load_3d(b_dst, &mapB, c0, 0, tap, &full[st]);
+                        mbar_arrive_expect_tx(&full[st], 128 * SW + (use_wres ? 0 : BTAP));
+                        tma_load_4d(a_dst, &mapA0, ch * KC, x0 + dx - 1, y0 + dy - 1, img, &full[st]);
+                        if (!use_wres) tma_load_3d(b_dst, &mapB, ch * KC, 0, tap, &full[st]);
                     } else {
                         const long long kq = k0 + q;
                         const int xchunks = p.W / KC;
@@ -253,8 +319,7 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
                         const int y = (int)(r2 % p.H), im = (int)(r2 / p.H);
                         int ntap = 9 - g * p.taps_per_tile;
                         if (ntap > p.taps_per_tile) ntap = p.taps_per_tile;
-                        const unsigned bytes =
-                            (unsigned)ntap * p.ci_rows * KC * 2 + (unsigned)G::B_BYTES;
+                        const unsigned bytes = (unsigned)ntap * p.ci_rows * KC * 2 + (unsigned)BTAP;
                         mbar_arrive_expect_tx(&full[st], bytes);
                         for (int j = 0; j < ntap; ++j) {
                             const int tap = g * p.taps_per_tile + j;
@@ -271,14 +336,21 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
             const unsigned lo = it > (unsigned)STAGES ? it - STAGES : 0u;
             for (unsigned j = lo; j < it; ++j)
                 mbar_wait_bounded(&full[j % STAGES], (j / STAGES) & 1, budget);
+            if (wres_loaded) mbar_wait_bounded(wbar, 0, budget);
         }
         __syncwarp();
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16_m128<N>();
+            const uint32_t wres_addr = smem_u32(wres);
+            bool ok = true;
+            if (use_wres && !mbar_wait_bounded(wbar, 0, budget)) {
+                fail(5);
+                ok = false;
+            }
             unsigned it = 0, lt = 0;
-            for (int t = blockIdx.x; t < p.ntiles && !*abort_flag; t += gridDim.x, ++lt) {
+            for (int t = blockIdx.x; ok && t < p.ntiles && !*abort_flag; t += gridDim.x, ++lt) {
                 const int ab = lt & 1;
                 if (!mbar_wait_bounded(&acc_empty[ab], ((lt >> 1) & 1) ^ 1, budget)) {
                     fail(2);
@@ -286,12 +358,16 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
                 }
                 tc_fence_after();
                 const uint32_t d_tmem = tmem + ab * N;
-                const int nsteps =
-                    p.mode == 0 ? p.ksteps
-                                : (int)(p.total_k * ((t % p.ksplit) + 1) / p.ksplit -
-                                        p.total_k * (t % p.ksplit) / p.ksplit);
-                bool ok = true;
-                for (int q = 0; q < nsteps; ++q, ++it) {
+                int q0 = 0, q1;
+                if (conv) {
+                    const int sp = t % p.csplit;
+                    q0 = p.ksteps * sp / p.csplit;
+                    q1 = p.ksteps * (sp + 1) / p.csplit;
+                } else {
+                    q1 = (int)(p.total_k * ((t % p.ksplit) + 1) / p.ksplit -
+                               p.total_k * (t % p.ksplit) / p.ksplit);
+                }
+                for (int q = q0; q < q1; ++q, ++it) {
                     const int st = it % STAGES;
                     if (!mbar_wait_bounded(&full[st], (it / STAGES) & 1, budget)) {
                         fail(3);
@@ -299,15 +375,34 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t a_addr = smem_u32(smem + st * G::STAGE);
-                    const uint32_t b_addr = a_addr + G::A_BYTES;
+                    const uint32_t a_addr = smem_u32(ring + (size_t)st * p.stage_bytes);
+                    const uint32_t b_addr = a_addr + p.a_region;
+                    if (conv && p.halo) {
+                        // tap (dy, dx): A = rows dx .. dx + 127 of the halo box
+                        const int ch = q / 3, dy = q % 3;
 #pragma unroll
-                    for (int kk = 0; kk < KC / 16; ++kk) {
-                        umma_bf16(d_tmem, kmajor_desc<G::SW>(a_addr + kk * 32),
-                                  kmajor_desc<G::SW>(b_addr + kk * 32), idesc,
-                                  (q > 0 || kk > 0) ? 1u : 0u);
+                        for (int dx = 0; dx < 3; ++dx) {
+                            const uint32_t a0 = a_addr + dx * SW;
+                            const uint32_t b0 =
+                                use_wres ? wres_addr + (uint32_t)((dy * 3 + dx) * p.nch + ch) * BTAP
+                                         : b_addr + dx * BTAP;
+#pragma unroll
+                            for (int kk = 0; kk < KC / 16; ++kk)
+                                umma_bf16(d_tmem, kmajor_desc<SW>(a0 + kk * 32), kmajor_desc<SW>(b0 + kk * 32),
+                                          idesc, (q > q0 || dx > 0 || kk > 0) ? 1u : 0u);
+                        }
+                    } else {
+                        uint32_t b0 = b_addr;
+                        if (use_wres) {
+                            const int tap = q / p.nch, ch = q % p.nch;
+                            b0 = wres_addr + (uint32_t)(tap * p.nch + ch) * BTAP;
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < KC / 16; ++kk)
+                            umma_bf16(d_tmem, kmajor_desc<SW>(a_addr + kk * 32), kmajor_desc<SW>(b0 + kk * 32),
+                                      idesc, (q > q0 || kk > 0) ? 1u : 0u);
                     }
-                    umma_commit(&empty[st]);  // frees the stage once these MMAs are done
+                    umma_commit(&empty[st]);  // frees the slot once these MMAs are done
                 }
                 if (!ok) break;
                 umma_commit(&acc_full[ab]);
@@ -330,27 +425,61 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
             }
             tc_fence_after();
             const uint32_t tbase = tmem + ((uint32_t)(q4 * 32) << 16) + ab * N;
-            if (p.mode == 0) {
-                const int tx = t % p.tiles_x, rest = t / p.tiles_x;
-                const int x = tx * p.bx + row % p.bx;
-                const int y = (rest % p.tiles_y) * p.by + row / p.bx;
+            if (conv) {
+                const int pt = t / p.csplit, sp = t % p.csplit;
+                const int tx = pt % p.tiles_x, rest = pt / p.tiles_x;
                 const int img = rest / p.tiles_y;
-                const bool in = x < p.W && y < p.H;
-                const size_t pix = ((size_t)img * p.H + (in ? y : 0)) * p.W + (in ? x : 0);
-                __nv_bfloat16 *o = p.out + pix * N;
+                // this lane's pixel and those of the even/odd lanes of its pair
+                auto pixel = [&](int r, bool &in) {
+                    const int x = tx * p.bx + r % p.bx;
+                    const int y = (rest % p.tiles_y) * p.by + r / p.bx;
+                    in = x < p.W && y < p.H;
+                    return ((size_t)img * p.H + (in ? y : 0)) * p.W + (in ? x : 0);
+                };
+                bool in_me, in_e, in_o;
+                const size_t pix = pixel(row, in_me);
+                __nv_bfloat16 *oe = p.out + pixel(row & ~1, in_e) * N;
+                __nv_bfloat16 *oo = p.out + pixel(row | 1, in_o) * N;
                 const __nv_bfloat16 *mk = p.mask ? p.mask + pix * N : nullptr;
+                float *wsrow = p.csplit > 1
+                                   ? p.ws + ((size_t)sp * p.B * p.H * p.W + pix) * N
+                                   : nullptr;
                 auto emit16 = [&](int c, const float *acc) {
-                    if (!in) return;
-                    __align__(16) __nv_bfloat16 v16[16];
+                    if (wsrow) {  // split-K partial: FP32, the reduction applies the epilogue
+                        if (in_me) {
+                            float4 *d = reinterpret_cast<float4 *>(wsrow + c);
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                d[j] = make_float4(acc[4 * j], acc[4 * j + 1], acc[4 * j + 2], acc[4 * j + 3]);
+                        }
+                        return;
+                    }
+                    float v[16];
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        float v = acc[j] + s_bias[c + j];
-                        if (p.relu) v = fmaxf(v, 0.f);
-                        if (mk && !(__bfloat162float(mk[c + j]) > 0.f)) v = 0.f;
-                        v16[j] = __float2bfloat16_rn(v);
+                        v[j] = acc[j] + s_bias[c + j];
+                        if (p.relu) v[j] = fmaxf(v[j], 0.f);
                     }
-                    reinterpret_cast<uint4 *>(o + c)[0] = reinterpret_cast<const uint4 *>(v16)[0];
-                    reinterpret_cast<uint4 *>(o + c)[1] = reinterpret_cast<const uint4 *>(v16)[1];
+                    if (mk && in_me) {
+                        const uint4 m0 = reinterpret_cast<const uint4 *>(mk + c)[0];
+                        const uint4 m1 = reinterpret_cast<const uint4 *>(mk + c)[1];
+                        const __nv_bfloat16 *mb0 = reinterpret_cast<const __nv_bfloat16 *>(&m0);
+                        const __nv_bfloat16 *mb1 = reinterpret_cast<const __nv_bfloat16 *>(&m1);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            if (!(__bfloat162float(mb0[j]) > 0.f)) v[j] = 0.f;
+                            if (!(__bfloat162float(mb1[j]) > 0.f)) v[8 + j] = 0.f;
+                        }
+                    }
+                    uint4 lo, hi;
+                    __nv_bfloat162 *l2 = reinterpret_cast<__nv_bfloat162 *>(&lo);
+                    __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&hi);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        l2[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                        h2[j] = __floats2bfloat162_rn(v[8 + 2 * j], v[8 + 2 * j + 1]);
+                    }
+                    store16_pairs(oe + c, oo + c, in_e, in_o, lane, lo, hi);
                 };
                 if constexpr (N <= 64) {
                     // narrow tile: drain TMEM first and hand the accumulator back
@@ -401,7 +530,51 @@ __global__ void __launch_bounds__(192, N <= 64 ? 2 : 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem, G::TMEM_COLS);
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+}  // namespace cfm
+
+namespace cfm {
+
+// Split-K reduction and epilogue of tc_conv_kernel: out[p][c] =
+// act(sum_j ws[j][p][c] + bias[c]) [* (mask > 0)], the partials summed in
+// split order (deterministic).  One thread per (pixel, 8 channels).
+template <int N>
+__global__ void tc_splitk_epilogue(const float *ws, int csplit, long long npix, const float *bias, int relu,
+                                   const __nv_bfloat16 *mask, __nv_bfloat16 *out) {
+    pdl_enter();
+    constexpr int G = N / 8;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < npix * G;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long pix = e / G;
+        const int c = (int)(e % G) * 8;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = 0.f;
+        for (int sp = 0; sp < csplit; ++sp) {
+            const float4 *src = reinterpret_cast<const float4 *>(ws + ((size_t)sp * npix + pix) * N + c);
+            const float4 a = src[0], b = src[1];
+            v[0] += a.x, v[1] += a.y, v[2] += a.z, v[3] += a.w;
+            v[4] += b.x, v[5] += b.y, v[6] += b.z, v[7] += b.w;
+        }
+        uint4 m = make_uint4(0u, 0u, 0u, 0u);
+        if (mask) m = *reinterpret_cast<const uint4 *>(mask + pix * N + c);
+        const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&m);
+        uint4 o;
+        __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+            float a = v[j] + (bias ? bias[c + j] : 0.f), b = v[j + 1] + (bias ? bias[c + j + 1] : 0.f);
+            if (relu) a = fmaxf(a, 0.f), b = fmaxf(b, 0.f);
+            if (mask) {
+                if (!(__bfloat162float(mb[j]) > 0.f)) a = 0.f;
+                if (!(__bfloat162float(mb[j + 1]) > 0.f)) b = 0.f;
+            }
+            o2[j / 2] = __floats2bfloat162_rn(a, b);
+        }
+        *reinterpret_cast<uint4 *>(out + pix * N + c) = o;
     }
 }
 

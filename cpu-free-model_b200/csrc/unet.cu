@@ -37,33 +37,93 @@ int encode_map(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dim
     return CFM_OK;
 }
 
+constexpr int round1k(int v) { return (v + 1023) / 1024 * 1024; }
+// Dynamic shared memory of one CTA alone on an SM (the 227 KB a block may
+// opt into, less its static part and some slack); two CTAs take half each.
+constexpr int TC_SMEM_MAX = 220 * 1024;
+
+// Shared-memory plan of one pass: ring depth and slot size, resident
+// weights, CTAs per SM.  Two CTAs share an SM when the grid has at least two
+// tiles per SM and both fit (shared memory, 512 TMEM columns); the weights
+// stay resident when a CTA runs at least two tiles and they leave room for
+// three slots.
+template <int KC, int N>
+int plan_kc_n(TcConvParams &p, int num_sms, int *cps_out) {
+    constexpr int SW = KC * 2, BTAP = N * SW;
+    const bool conv = p.mode == 0;
+    if (conv) {
+        // split-K when the pixel tiles leave SMs idle: at least one halo step
+        // (three taps) or two per-tap steps per split, within the workspace
+        const int ptiles = p.tiles_x * p.tiles_y * p.B;
+        const long long npix = (long long)p.B * p.H * p.W;
+        int S = ptiles < num_sms ? num_sms / ptiles : 1;
+        S = std::min(S, p.ksteps / (p.halo ? 1 : 2));
+        if (p.ws_floats > 0) S = (int)std::min<long long>(S, p.ws_floats / (npix * N));
+        else S = 1;
+        p.csplit = std::max(S, 1);
+        p.ntiles = ptiles * p.csplit;
+    }
+    p.a_region = conv && p.halo ? round1k(136 * SW) : 128 * SW;
+    const int b_stage = conv && p.halo ? 3 * BTAP : BTAP;
+    const int wbytes = conv ? round1k(9 * p.nch * BTAP) : 0;
+    const int cps = (2 * tc_tmem_cols<N>() <= 512 && p.ntiles >= 2 * num_sms) ? 2 : 1;
+    // per-CTA dynamic shared memory (the SM has 228 KB; 1 KB per CTA is reserved)
+    const int budget = cps == 2 ? TC_SMEM_MAX / 2 : TC_SMEM_MAX;
+    const int overhead = 1024 + 8 * 8 + 16;
+    const long long tiles_per_cta = (p.ntiles + (long long)num_sms * cps - 1) / ((long long)num_sms * cps);
+    p.wres = conv && tiles_per_cta >= 2 && wbytes + 3 * (p.a_region + 16) + overhead <= budget;
+    p.wres_bytes = p.wres ? wbytes : 0;
+    p.stage_bytes = p.wres ? p.a_region : round1k(p.a_region + b_stage);
+    int stages = (budget - overhead - p.wres_bytes) / (p.stage_bytes + 16);
+    if (stages < 2 && conv && p.halo) {
+        // wide streamed weights: three taps per slot do not fit twice, go per tap
+        p.halo = 0;
+        p.ksteps = 9 * p.nch;
+        return plan_kc_n<KC, N>(p, num_sms, cps_out);  // (re-plans the split too)
+    }
+    stages = std::min(stages, 16);
+    if (stages < 2) {
+        set_error("tensor-core convolution: no shared-memory plan for KC %d, N %d", KC, N);
+        return CFM_UNSUPPORTED;
+    }
+    p.stages = stages;
+    *cps_out = cps;
+    return CFM_OK;
+}
+
 template <int KC, int N>
 int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
-                const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
-    using G = TcGeom<KC, N>;
+                const CUtensorMap &b, TcConvParams p, cudaStream_t s) {
     static std::once_flag once[64];
     static cudaError_t attr_err[64];
     int dev = 0;
     CFM_CUDA_TRY(cudaGetDevice(&dev));
     std::call_once(once[dev & 63], [&] {
-        attr_err[dev & 63] = cudaFuncSetAttribute(
-            tc_conv_kernel<KC, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+        attr_err[dev & 63] = cudaFuncSetAttribute(tc_conv_kernel<KC, N>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_MAX);
+        if (attr_err[dev & 63] == cudaSuccess)
+            attr_err[dev & 63] = cudaFuncSetAttribute(
+                tc_conv_kernel<KC, N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                (int)cudaSharedmemCarveoutMaxShared);
     });
     CFM_CUDA_TRY(attr_err[dev & 63]);
     DeviceInfo di;
     int st = current_device_info(&di);
     if (st) return st;
-    static int per_sm_cache[64];
-    int &per_sm = per_sm_cache[dev & 63];
-    if (per_sm <= 0) {
-        CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tc_conv_kernel<KC, N>, 192,
-                                                                   G::SMEM));
-        // TMEM: every resident CTA holds TMEM_COLS of the SM's 512 columns
-        per_sm = std::max(1, std::min(per_sm, (int)(512 / G::TMEM_COLS)));
+    int cps = 1;
+    if ((st = plan_kc_n<KC, N>(p, di.num_sms, &cps))) return st;
+    const size_t smem = tc_conv_smem(p.wres_bytes, p.stages, p.stage_bytes);
+    // (the occupancy query under-reports two CTAs of ~110 KB; the plan keeps
+    // 2 x (dynamic + static + 1 KB reserved) inside the SM's 228 KB)
+    const int grid = std::min(p.ntiles, di.num_sms * cps);
+    CFM_CUDA_TRY(launch_pdl(tc_conv_kernel<KC, N>, dim3(grid), dim3(192), smem, s, a0, a1, a2, b, p));
+    if (p.mode == 0 && p.csplit > 1) {
+        const long long npix = (long long)p.B * p.H * p.W;
+        const long long items = npix * (N / 8);
+        const int blocks = (int)std::min<long long>((items + 255) / 256, (long long)di.num_sms * 8);
+        CFM_CUDA_TRY(launch_pdl(tc_splitk_epilogue<N>, dim3(blocks), dim3(256), 0, s, (const float *)p.ws,
+                                p.csplit, npix, p.bias, p.relu, p.mask, p.out));
     }
-    const int grid = std::min(p.ntiles, di.num_sms * per_sm);
-    tc_conv_kernel<KC, N><<<grid, 192, G::SMEM, s>>>(a0, a1, a2, b, p);
-    CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
 }
 
@@ -147,12 +207,17 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     p.tiles_x = (a.W + p.bx - 1) / p.bx;
     p.tiles_y = (a.H + p.by - 1) / p.by;
     p.ntiles = p.tiles_x * p.tiles_y * a.B;
-    p.ksteps = 9 * (a.Cin / kc);
+    p.nch = a.Cin / kc;
+    p.halo = p.bx == 128;
+    p.ksteps = (p.halo ? 3 : 9) * p.nch;
     p.bias = a.bias;
     p.relu = a.relu;
     p.mask = a.mask;
     p.out = a.out;
     p.err = a.err;
+    p.ws = a.ws;
+    p.ws_floats = a.ws ? a.ws_floats : 0;
+    p.csplit = 1;
     p.budget_ns = barrier_timeout_ns();
     CUtensorMap ma, mb;
     const cuuint64_t da[4] = {(cuuint64_t)a.Cin, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
@@ -161,11 +226,16 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     const cuuint32_t ba[4] = {(cuuint32_t)kc, (cuuint32_t)p.bx, (cuuint32_t)p.by, 1};
     int st = encode_map(&ma, a.x, 4, da, sa, ba, kc * 2);
     if (st) return st;
+    CUtensorMap mh = ma;  // halo boxes: 130 pixels of one row
+    if (p.halo) {
+        const cuuint32_t bh[4] = {(cuuint32_t)kc, (cuuint32_t)TC_HALO_ROWS, 1, 1};
+        if ((st = encode_map(&mh, a.x, 4, da, sa, bh, kc * 2))) return st;
+    }
     const cuuint64_t db[3] = {(cuuint64_t)a.Cin, (cuuint64_t)a.Cout, 9};
     const cuuint64_t sb[2] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.Cout * a.Cin * 2};
     const cuuint32_t bb[3] = {(cuuint32_t)kc, (cuuint32_t)a.Cout, 1};
     if ((st = encode_map(&mb, a.w, 3, db, sb, bb, kc * 2))) return st;
-    return launch(kc, a.Cout, ma, ma, ma, mb, p, s);
+    return launch(kc, a.Cout, ma, mh, ma, mb, p, s);
 }
 
 int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
@@ -175,6 +245,7 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     const int kc = a.W % 64 == 0 ? 64 : 32;
     TcConvParams p{};
     p.mode = 1;
+    p.csplit = 1;
     p.B = a.B;
     p.H = a.H;
     p.W = a.W;
@@ -269,7 +340,11 @@ int cfm_tc_conv3x3(int B, int H, int W, int Cin, int Cout, const unsigned short 
     CFM_CUDA_TRY(cudaMemcpy(dw, w, nw * 2, cudaMemcpyHostToDevice));
     if (bias) CFM_CUDA_TRY(cudaMemcpy(db, bias, Cout * 4, cudaMemcpyHostToDevice));
     CFM_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
+    float *dws;
+    CFM_CUDA_TRY(d.get(&dws, (size_t)TC_WS_FLOATS));
     ConvArgs a{dx, dw, db, nullptr, dout, derr, B, H, W, Cin, Cout, relu};
+    a.ws = dws;
+    a.ws_floats = TC_WS_FLOATS;
     int st = tc_conv_fwd(a, 0);
     if (st) return st;
     CFM_CUDA_TRY(cudaDeviceSynchronize());

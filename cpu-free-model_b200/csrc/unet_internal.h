@@ -18,8 +18,14 @@ struct ConvArgs {
     int *err;  // device word, nonzero after a timed-out pipeline wait
     int B, H, W, Cin, Cout;
     int relu;
+    // optional split-K workspace (FP32); layers with fewer pixel tiles than
+    // SMs then split their K steps over several CTAs
+    float *ws = nullptr;
+    long long ws_floats = 0;
 };
 int tc_conv_fwd(const ConvArgs &a, cudaStream_t s);
+// Split-K workspace a net keeps for its convolutions (floats).
+constexpr long long TC_WS_FLOATS = 4LL << 20;
 
 // dw[tap][co][ci] += sum over pixels of dz[p][co] * x[p + shift(tap)][ci],
 // from the channel-major copies xt[d] (x shifted by d - 1 in x) and dzt.

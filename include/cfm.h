@@ -319,8 +319,9 @@ int cfm_unet_time_forward(cfm_unet *net, int B, int iters, double *ms_per_forwar
  * 0..13 = h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0, NHWC at its level. */
 int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *out);
 
-/* Training of the network for the 2D variable-coefficient problem on its
- * H x W grid: nsys systems from fresh seeds seed0, seed0+1, ... (k = exp(GRF),
+/* Training of the network for the 2D variable-coefficient problem on the
+ * (coarsen H) x (coarsen W) grid of an H x W network (coarsen 1 or 2):
+ * nsys systems from fresh seeds seed0, seed0+1, ... (k = exp(GRF),
  * f ~ N(0,1), cfm_varcoef_problem) are solved by plain persistent FP64 CG to
  * 1e-10; from a second run, `snaps` iterates x_j spread over the solve plus
  * x_0 = 0 give (snaps + 1) * nsys residual/error pairs (r_j = f - A x_j,
@@ -331,10 +332,13 @@ int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *ou
  * Mean loss of the first and last epoch and the seconds spent on data and on
  * training are returned (each pointer optional).  smooth > 0: every pair is
  * first passed through `smooth` damped Jacobi sweeps z on A z = r_j, giving
- * (r_j - A z, e_j - z), the pair the network sees inside the preconditioner. */
+ * (r_j - A z, e_j - z), the pair the network sees inside the preconditioner.
+ * With coarsen = 2 the network sees the residual restricted to its grid
+ * (2 x 2 means of r_j / rms(r_j), block-mean log k) and z = P net(.) is its
+ * piecewise-constant prolongation; the loss is taken on the systems' grid. */
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
-                           int batch, float lr, int smooth, double *loss_first, double *loss_last,
-                           double *data_seconds, double *train_seconds);
+                           int batch, float lr, int smooth, int coarsen, double *loss_first,
+                           double *loss_last, double *data_seconds, double *train_seconds);
 
 /* Flexible PCG (Polak-Ribiere beta) on a 2D stencil operator with the
  * preconditioner z = J(z0 + c y): z0 = J(0), r1 = r - A z0,
@@ -346,7 +350,10 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
  * If the loop stalls or reaches maxiter, plain persistent FP64 CG finishes
  * from the current iterate; stats->refinements = 1 then.  stats->iterations
  * = FPCG iterations + fallback iterations; stats->lups = FPCG iterations.
- * The network's grid must equal the stencil's. */
+ * The stencil's grid must be the network's times the factor it was trained
+ * with (cfm_unet_train_varcoef coarsen); with factor 2 the network sees
+ * R(r1) (2 x 2 means) and y above is P net(.), its piecewise-constant
+ * prolongation (a learned coarse-grid correction). */
 typedef struct cfm_fpcg cfm_fpcg;
 int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int smooth,
                     int maxiter, double tol, cfm_fpcg **out);
