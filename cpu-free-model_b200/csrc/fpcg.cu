@@ -110,7 +110,7 @@ __global__ void k_data_jacobi(StencilOp<2> op, int n, const double *r, const dou
                               double *zout) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double res = zin ? r[i] - op.apply(zin, i) : r[i];
-        zout[i] = (zin ? zin[i] : 0.0) + JACOBI_OMEGA * res / op.dg[i];
+        zout[i] = __fma_rn(JACOBI_OMEGA / op.dg[i], res, zin ? zin[i] : 0.0);  // as the solver's sweeps
     }
 }
 
@@ -278,15 +278,14 @@ struct FpArgs {
     long long maxiter;
     int stall;
     int f, ncx, nc;  // network grid: (nx / f) x (ny / f) = nc cells, ncx per row
+    int fsh;         // log2 f
+    int ntiles2, tx2;  // FP_TILE x FP_TILE tiles of the smoothing kernels (tx2 per row)
+    int pstride;       // partial-sum slot stride: max(ntiles, ntiles2)
+    int smooth;
 };
 
-// The network cell of fine cell i (piecewise-constant prolongation).
-__device__ __forceinline__ int fp_cell(const FpArgs &a, int i) {
-    const int ix = i % a.op.nx, iy = i / a.op.nx;
-    return (iy / a.f) * a.ncx + ix / a.f;
-}
 
-__device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.ntiles; }
+__device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.pstride; }
 
 #define FP_ROW const int i = blockIdx.x * CG_TILE + threadIdx.x
 
@@ -314,78 +313,210 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
         a.st->best_rr = 1e300;
         a.st->best_k = 0;
         a.st->rz[0] = a.st->rz[1] = 0;
-        a.st->target = -tol;  // resolved by k_fp_prep from |b|
+        a.st->target = -tol;  // resolved by k_fp_pre from |b|
     }
 }
 
-// rr = |r|^2; convergence / stall test (block 0).
-__global__ void __launch_bounds__(CG_TILE) k_fp_prep(FpArgs a) {
-    pdl_enter();
-    __shared__ double sm[33];
-    const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
-    const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);  // block-wide: every thread
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        FpState *st = a.st;
-        double target = st->target;
-        if (target < 0) {  // first call: target = tol * |b|
-            target = -target * sqrt(bb);
-            st->target = target;
+// ------------------------------------------------ smoothing, temporally blocked
+// The preconditioner's Jacobi sweeps run on FP_TILE x FP_TILE tiles held in
+// shared memory with a halo as wide as the sweeps need, so that all sweeps of
+// one application (and what surrounds them) take one launch: each sweep
+// shrinks the valid region by one cell, cells outside the grid are never read
+// (the Dirichlet apply skips them), and the arithmetic is the global
+// operator's (A u)_i = dg u_i - we_{i-1} u_{i-1} - we_i u_{i+1} - wn_{i-nx}
+// u_{i-nx} - wn_i u_{i+nx}, in that order.
+constexpr int FP_TILE = 32;  // one thread per tile cell: FP_TILE^2 = CG_TILE threads
+static_assert(FP_TILE * FP_TILE == CG_TILE, "one thread per tile cell");
+constexpr int FP_MAX_SMOOTH = 8;
+
+struct FpTile {
+    int x0, y0, H, R;  // tile origin, halo, region side (FP_TILE + 2 H)
+    double *r, *z0, *z1, *we, *wn, *dg, *wd;  // [R * R] each, region-local; wd = omega / dg
+};
+
+// Region cells are visited as (row, column) by warps over rows and lanes
+// over columns: no integer division in the loops.
+#define FP_FOR_SQUARE(m, side, row, col)                                                   \
+    for (int row = (m) + (int)(threadIdx.x >> 5); row < (m) + (side); row += (int)(blockDim.x >> 5)) \
+        for (int col = (m) + (int)(threadIdx.x & 31); col < (m) + (side); col += 32)
+
+__device__ __forceinline__ bool fp_inside(const FpTile &t, const FpArgs &a, int row, int col, int *gi) {
+    const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
+    *gi = gy * a.op.nx + gx;
+    return gx >= 0 && gx < a.op.nx && gy >= 0 && gy < a.op.ny;
+}
+
+__device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
+    FpTile t;
+    t.x0 = (blockIdx.x % a.tx2) * FP_TILE;
+    t.y0 = (blockIdx.x / a.tx2) * FP_TILE;
+    t.H = H;
+    t.R = FP_TILE + 2 * H;
+    double *d = reinterpret_cast<double *>(smem);
+    const int RR = t.R * t.R;
+    t.r = d, t.z0 = d + RR, t.z1 = d + 2 * RR, t.we = d + 3 * RR, t.wn = d + 4 * RR, t.dg = d + 5 * RR;
+    t.wd = d + 6 * RR;
+    FP_FOR_SQUARE(0, t.R, row, col) {
+        int i;
+        const bool in = fp_inside(t, a, row, col, &i);
+        const int l = row * t.R + col;
+        t.r[l] = in ? a.r[i] : 0.0;
+        t.we[l] = in ? a.op.we[i] : 0.0;
+        t.wn[l] = in ? a.op.wn[i] : 0.0;
+        const double dg = in ? a.op.dg[i] : 1.0;
+        t.dg[l] = dg;
+        t.wd[l] = JACOBI_OMEGA / dg;
+    }
+    return t;
+}
+
+// (A u) at region cell (row, col) of a global cell (gx, gy) inside the grid,
+// its neighbours in the region.
+__device__ __forceinline__ double fp_apply(const FpTile &t, const FpArgs &a, const double *u, int row,
+                                           int col) {
+    const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row, l = row * t.R + col;
+    double v = __dmul_rn(t.dg[l], u[l]);
+    if (gx > 0) v = __fma_rn(-t.we[l - 1], u[l - 1], v);
+    if (gx < a.op.nx - 1) v = __fma_rn(-t.we[l], u[l + 1], v);
+    if (gy > 0) v = __fma_rn(-t.wn[l - t.R], u[l - t.R], v);
+    if (gy < a.op.ny - 1) v = __fma_rn(-t.wn[l], u[l + t.R], v);
+    return v;
+}
+
+// `sweeps` damped Jacobi sweeps on A z = r, z += (omega / dg) (r - A z),
+// starting from *cur (valid at margin m0 of the region); returns the buffer
+// holding the result, valid at margin m0 + sweeps.
+__device__ double *fp_sweeps(const FpTile &t, const FpArgs &a, double *cur, double *nxt, int m0, int sweeps) {
+    for (int s = 0; s < sweeps; ++s) {
+        const int m = m0 + s + 1, side = t.R - 2 * m;
+        FP_FOR_SQUARE(m, side, row, col) {
+            int i;
+            if (!fp_inside(t, a, row, col, &i)) continue;
+            const int l = row * t.R + col;
+            const double res = t.r[l] - fp_apply(t, a, cur, row, col);
+            nxt[l] = __fma_rn(t.wd[l], res, cur[l]);
         }
-        if (st->k <= a.maxiter) a.hist[st->k] = sqrt(rr);
-        if (sqrt(rr) <= target) st->done = 1;
-        if (rr < st->best_rr) {
-            st->best_rr = rr;
-            st->best_k = st->k;
-        } else if (st->k - st->best_k > a.stall) {
-            st->done = 2;
-        }
-        if (st->k >= a.maxiter && !st->done) st->done = 2;
+        __syncthreads();
+        double *sw = cur;
+        cur = nxt;
+        nxt = sw;
     }
+    return cur;
 }
 
-// Damped Jacobi sweep on A z = r: zout = zin + omega (r - A zin) / diag
-// (zin == nullptr: zout = omega r / diag).
-__global__ void k_fp_jacobi(FpArgs a, const double *zin, double *zout) {
+// Start of the preconditioner (one launch): [k += 1 when `tick`; block 0:
+// |r|^2 history, convergence / stall test]; z0 = `smooth` sweeps from zero,
+// r1 = r - A z0, partial |r1|^2, and the network input channel 0 = R(r1)
+// (f x f means; the network scales it by 1 / rms(r1) itself).
+__global__ void __launch_bounds__(CG_TILE) k_fp_pre(FpArgs a, int tick) {
     pdl_enter();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const double res = zin ? a.r[i] - a.op.apply(zin, i) : a.r[i];
-        zout[i] = (zin ? zin[i] : 0.0) + JACOBI_OMEGA * res / a.op.dg[i];
-    }
-}
-
-// r1 = r - A zc (zc == nullptr: r1 = r) and partial |r1|^2.
-__global__ void __launch_bounds__(CG_TILE) k_fp_r1(FpArgs a, const double *zc) {
-    pdl_enter();
+    extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
-    FP_ROW;
+    if (blockIdx.x == 0) {
+        const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
+        const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);
+        if (threadIdx.x == 0) {
+            FpState *st = a.st;
+            if (tick) st->k += 1;
+            double target = st->target;
+            if (target < 0) {  // first call: target = tol * |b|
+                target = -target * sqrt(bb);
+                st->target = target;
+            }
+            if (st->k <= a.maxiter) a.hist[st->k] = sqrt(rr);
+            if (sqrt(rr) <= target) st->done = 1;
+            if (rr < st->best_rr) {
+                st->best_rr = rr;
+                st->best_k = st->k;
+            } else if (st->k - st->best_k > a.stall) {
+                st->done = 2;
+            }
+            if (st->k >= a.maxiter && !st->done) st->done = 2;
+        }
+    }
+    const int H = a.smooth > 0 ? a.smooth : 1;
+    FpTile t = fp_tile(a, H, fp_smem);
+    __syncthreads();
+    // sweep 1 from zero is pointwise: z = (omega / dg) r on the whole region
+    FP_FOR_SQUARE(0, t.R, row, col) {
+        const int l = row * t.R + col;
+        t.z0[l] = a.smooth > 0 ? t.wd[l] * t.r[l] : 0.0;
+    }
+    __syncthreads();
+    const double *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0, t.z1, 0, a.smooth - 1) : t.z0;
+    // this thread's tile cell
+    const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
+    const int row = H + ly, col = H + lx, l = row * t.R + col;
+    int i;
+    const bool in = fp_inside(t, a, row, col, &i);
     double q = 0;
-    if (i < a.n) {
-        const double v = zc ? a.r[i] - a.op.apply(zc, i) : a.r[i];
+    if (in) {
+        const double v = t.r[l] - fp_apply(t, a, z, row, col);
         a.r1[i] = v;
+        a.za[i] = z[l];
         q = v * v;
     }
-    q = block_sum(q, sm);
+    q = block_sum(q, sm);  // (its barriers also order the r1 stores before the restriction)
     if (threadIdx.x == 0) fslot(a, FP_R1)[blockIdx.x] = q;
-}
-
-// Network input channel 0 = R(r1) / rms(r1), R the mean over f x f blocks.
-__global__ void __launch_bounds__(CG_TILE) k_fp_in(FpArgs a) {
-    pdl_enter();
-    __shared__ double sm[33];
-    const double q = sum_partials(fslot(a, FP_R1), a.ntiles, sm);
-    const double scale = q > 0 ? sqrt((double)a.n / q) : 0.0;
-    const double inv = 1.0 / (a.f * a.f);
-    const int nx = a.op.nx;
-    for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < a.nc; ic += gridDim.x * blockDim.x) {
-        const int cx = ic % a.ncx, cy = ic / a.ncx;
-        double sum = 0;
-        for (int dy = 0; dy < a.f; ++dy)
-            for (int dx = 0; dx < a.f; ++dx) sum += a.r1[(size_t)(cy * a.f + dy) * nx + cx * a.f + dx] * scale;
-        a.xin[2 * ic] = (float)(sum * inv);
+    // restriction of this tile's cells (f divides FP_TILE and the tile origin)
+    const int f = a.f, cs = FP_TILE / f;
+    if (threadIdx.x < cs * cs) {
+        const int cx = threadIdx.x % cs, cy = threadIdx.x / cs;
+        const int gx = t.x0 + cx * f, gy = t.y0 + cy * f;
+        if (gx < a.op.nx && gy < a.op.ny) {
+            double sum = 0;
+            for (int dy = 0; dy < f; ++dy)
+                for (int dx = 0; dx < f; ++dx)
+                    sum += a.r1[(size_t)(gy + dy) * a.op.nx + gx + dx];
+            a.xin[2 * ((gy / f) * a.ncx + gx / f)] = (float)(sum / (f * f));
+        }
     }
 }
 
-// Identity in place of the network: out = the normalised r1.
+// End of the preconditioner (one launch): z = `smooth` sweeps starting from
+// z0 + c P y, c = <P y, r1> / <P y, A P y> from the ydots partials (of all
+// multiples of P y, c P y removes the most A-norm error from A d = r1, so the
+// network's correction can only help the smoothed iterate), written to a.z
+// with the partials <z, r> and <z, r_old>.
+__global__ void __launch_bounds__(CG_TILE) k_fp_post(FpArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char fp_smem[];
+    __shared__ double sm[33];
+    const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
+    const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
+    const double c = yay > 0 ? yr / yay : 0.0;
+    const int H = a.smooth;
+    FpTile t = fp_tile(a, H, fp_smem);
+    FP_FOR_SQUARE(0, t.R, row, col) {
+        int i;
+        const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
+        t.z0[row * t.R + col] = fp_inside(t, a, row, col, &i)
+                                    ? a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)]
+                                    : 0.0;
+    }
+    __syncthreads();
+    const double *z = fp_sweeps(t, a, t.z0, t.z1, 0, a.smooth);
+    const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
+    const int row = H + ly, col = H + lx, l = row * t.R + col;
+    int i;
+    double zr = 0, zro = 0;
+    if (fp_inside(t, a, row, col, &i)) {
+        const double zi = z[l];
+        a.z[i] = zi;
+        zr = zi * a.r[i];
+        zro = zi * a.rold[i];
+    }
+    zr = block_sum(zr, sm);
+    zro = block_sum(zro, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_ZR)[blockIdx.x] = zr;
+        fslot(a, FP_ZRO)[blockIdx.x] = zro;
+    }
+}
+
+size_t fp_smem_bytes(int H) { return 7 * sizeof(double) * (size_t)(FP_TILE + 2 * H) * (FP_TILE + 2 * H); }
+
+// Identity in place of the network: out = R(r1) (unscaled; c absorbs the scale).
 __global__ void k_fp_identity(FpArgs a) {
     pdl_enter();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x)
@@ -401,14 +532,16 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     double yr = 0, yay = 0;
     if (i < a.n) {
         const StencilOp<2> &o = a.op;
-        const int nx = o.nx, ix = i % nx, iy = i / nx;
-        const float *y = a.out;  // z = P y on this grid: z[j] = y[fp_cell(j)]
-        const double zi = (double)y[fp_cell(a, i)];
+        const int nx = o.nx, iy = i / nx, ix = i - iy * nx;
+        const int sh = a.fsh, cx = ix >> sh, cy = iy >> sh;
+        const float *y = a.out;  // z = P y on this grid: z[j] = y[cell(j)]
+        const float *yrow = y + cy * a.ncx;
+        const double zi = (double)yrow[cx];
         double t = o.dg[i] * zi;
-        if (ix > 0) t -= o.we[i - 1] * (double)y[fp_cell(a, i - 1)];
-        if (ix < nx - 1) t -= o.we[i] * (double)y[fp_cell(a, i + 1)];
-        if (iy > 0) t -= o.wn[i - nx] * (double)y[fp_cell(a, i - nx)];
-        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[fp_cell(a, i + nx)];
+        if (ix > 0) t -= o.we[i - 1] * (double)yrow[(ix - 1) >> sh];
+        if (ix < nx - 1) t -= o.we[i] * (double)yrow[(ix + 1) >> sh];
+        if (iy > 0) t -= o.wn[i - nx] * (double)y[((iy - 1) >> sh) * a.ncx + cx];
+        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[((iy + 1) >> sh) * a.ncx + cx];
         yr = zi * a.r1[i];
         yay = zi * t;
     }
@@ -420,40 +553,6 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     }
 }
 
-// zout = zc + c z with z = P y and the optimal step c = <z, r1> / <z, A z>:
-// of all multiples of z, c z removes the most A-norm error from A d = r1, so
-// the network's correction can only help the smoothed iterate (zc ==
-// nullptr: 0).
-__global__ void __launch_bounds__(CG_TILE) k_fp_corr(FpArgs a, const double *zc, double *zout) {
-    pdl_enter();
-    __shared__ double sm[33];
-    const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
-    const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
-    const double c = yay > 0 ? yr / yay : 0.0;
-    FP_ROW;
-    if (i < a.n) zout[i] = (zc ? zc[i] : 0.0) + c * (double)a.out[fp_cell(a, i)];
-}
-
-// z = zf; partials <z, r>, <z, r_old>.
-__global__ void __launch_bounds__(CG_TILE) k_fp_z(FpArgs a, const double *zf) {
-    pdl_enter();
-    __shared__ double sm[33];
-    FP_ROW;
-    double zr = 0, zro = 0;
-    if (i < a.n) {
-        const double zi = zf[i];
-        a.z[i] = zi;
-        zr = zi * a.r[i];
-        zro = zi * a.rold[i];
-    }
-    zr = block_sum(zr, sm);
-    zro = block_sum(zro, sm);
-    if (threadIdx.x == 0) {
-        fslot(a, FP_ZR)[blockIdx.x] = zr;
-        fslot(a, FP_ZRO)[blockIdx.x] = zro;
-    }
-}
-
 // beta = max(0, (<z,r> - <z,r_old>) / <z_old, r_old>) (0 on the first
 // step); p = z + beta p; and the loop condition.  <z, r> of direction k
 // lives in rz[(k + 1) & 1] (k = iterations done when it was formed), so the
@@ -462,8 +561,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
                                                     int set_cond) {
     pdl_enter();
     __shared__ double sm[33];
-    const double zr = sum_partials(fslot(a, FP_ZR), a.ntiles, sm);
-    const double zro = sum_partials(fslot(a, FP_ZRO), a.ntiles, sm);
+    const double zr = sum_partials(fslot(a, FP_ZR), a.ntiles2, sm);
+    const double zro = sum_partials(fslot(a, FP_ZRO), a.ntiles2, sm);
     const long long k = a.st->k;
     const double rz_old = a.st->rz[k & 1];
     double beta = 0.0;
@@ -513,12 +612,6 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
 }
 
-// k += 1 (its own launch: every block of the kernels around it reads k).
-__global__ void k_fp_tick(FpState *st) {
-    pdl_enter();
-    st->k += 1;
-}
-
 // t = b - A x, |t|^2 (atomics; the reported true residual).
 __global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const double *x, double *t,
                               double *acc) {
@@ -558,6 +651,7 @@ struct cfm_fpcg {
     const cfm_stencil *S = nullptr;
     cfm_unet *net = nullptr;
     int n = 0, ntiles = 0, nx = 0, ny = 0;
+    int ntiles2 = 0, tx2 = 0, pstride = 0;  // smoothing tiles (FP_TILE^2) and partial-slot stride
     int coarsen = 1, nc = 0;  // the network runs on (nx / coarsen) x (ny / coarsen) = nc cells
     long long maxiter = 0;
     double tol = 0;
@@ -601,54 +695,43 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.maxiter = h->maxiter;
     a.stall = 200;
     a.f = h->coarsen;
+    a.fsh = h->coarsen == 2 ? 1 : 0;
     a.ncx = h->nx / h->coarsen;
     a.nc = h->nc;
+    a.ntiles2 = h->ntiles2;
+    a.tx2 = h->tx2;
+    a.pstride = h->pstride;
+    a.smooth = h->smooth;
     return a;
 }
 
-// One FPCG iteration's tail (from the preconditioner on): convergence test,
-// z = M(r) = post-smooth(z0 + c y), z0 = pre-smooth(r), r1 = r - A z0,
-// y = net(r1 / rms(r1), log k), c = <y, r1> / <y, A y>, with `smooth` damped
-// Jacobi sweeps on each side; then the new direction.
-int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+// One FPCG iteration's tail (from the preconditioner on), five launches:
+// k_fp_pre (k += 1 when `tick`, convergence test, z0 = `smooth` Jacobi
+// sweeps from zero, r1 = r - A z0, R(r1)), the network y = net(R(r1) /
+// rms(r1), log k) (or the identity), k_fp_ydots (<P y, r1>, <P y, A P y>),
+// k_fp_post (z = `smooth` sweeps from z0 + c P y, <z, r>, <z, r_old>) and
+// k_fp_dir (beta, p, the loop condition).
+int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, int tick) {
     cudaStream_t s = h->stream;
-    CFM_CUDA_TRY(launch_pdl(k_fp_prep, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
-    double *buf[2] = {a.za, a.zb};
-    const double *cur = nullptr;
-    int nb = 0;
-    for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
-        CFM_CUDA_TRY(launch_pdl(k_fp_jacobi, dim3(256), dim3(256), 0, s, a, cur, buf[nb]));
-        cur = buf[nb];
-    }
-    CFM_CUDA_TRY(launch_pdl(k_fp_r1, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur));
-    CFM_CUDA_TRY(launch_pdl(k_fp_in, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
-    CFM_CUDA_TRY(cudaGetLastError());
+    CFM_CUDA_TRY(launch_pdl(k_fp_pre, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(std::max(h->smooth, 1)), s,
+                            a, tick));
     if (h->net) {
-        int st = unet_forward(h->net->u, 1, h->xin, h->out, s);
+        const UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride, h->ntiles2, (double)h->n};
+        int st = unet_forward(h->net->u, 1, h->xin, h->out, s, &sc);
         if (st) return st;
     } else {
         CFM_CUDA_TRY(launch_pdl(k_fp_identity, dim3(256), dim3(256), 0, s, a));
     }
     CFM_CUDA_TRY(launch_pdl(k_fp_ydots, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
-    CFM_CUDA_TRY(launch_pdl(k_fp_corr, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur, buf[nb]));
-    cur = buf[nb];
-    nb ^= 1;
-    for (int k = 0; k < h->smooth; ++k, nb ^= 1) {
-        CFM_CUDA_TRY(launch_pdl(k_fp_jacobi, dim3(256), dim3(256), 0, s, a, cur, buf[nb]));
-        cur = buf[nb];
-    }
-    CFM_CUDA_TRY(launch_pdl(k_fp_z, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cur));
+    CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a));
     CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
-    CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
 }
 
 int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
     CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
     CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-    CFM_CUDA_TRY(launch_pdl(k_fp_tick, dim3(1), dim3(1), 0, h->stream, a.st));
-    CFM_CUDA_TRY(cudaGetLastError());
-    return fp_precond_dir(h, a, cond, set_cond);
+    return fp_precond_dir(h, a, cond, set_cond, 1);
 }
 
 // Graph: a conditional WHILE node whose body is one FPCG iteration.
@@ -706,7 +789,7 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     stencil_shape(S, &dims, &nx, &ny, &nz);
     CFM_ARG_CHECK(dims == 2, "the learned preconditioner is 2D");
     CFM_ARG_CHECK(tol > 0 && maxiter > 0, "tol, maxiter");
-    CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= FP_MAX_SMOOTH, "smooth must be in [0, 8]");
     const int f = net ? net->coarsen : 1;
     if (net) {
         int H = 0, W = 0;
@@ -725,6 +808,9 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     h->ny = ny;
     h->n = nx * ny;
     h->ntiles = (h->n + CG_TILE - 1) / CG_TILE;
+    h->tx2 = (nx + FP_TILE - 1) / FP_TILE;
+    h->ntiles2 = h->tx2 * ((ny + FP_TILE - 1) / FP_TILE);
+    h->pstride = std::max(h->ntiles, h->ntiles2);
     h->maxiter = maxiter;
     h->tol = tol;
     const size_t n = h->n;
@@ -734,7 +820,11 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->xin, sizeof(float) * 2 * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->out, sizeof(float) * h->nc)) != cudaSuccess ||
-        (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->ntiles)) != cudaSuccess ||
+        (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->pstride)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
         (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
         (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1))) != cudaSuccess ||
@@ -795,7 +885,7 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     CFM_CUDA_TRY(cudaEventRecord(h->ev0, s));
     k_fp_init<<<h->ntiles, CG_TILE, 0, s>>>(a, h->tol);
     CFM_CUDA_TRY(cudaGetLastError());
-    if ((st = fp_precond_dir(h, a, 0, 0))) return st;
+    if ((st = fp_precond_dir(h, a, 0, 0, 0))) return st;
     launches += 2;
     FpState hs{};
     if (h->conditional) {
@@ -873,7 +963,7 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                            double *loss_last, double *data_seconds, double *train_seconds) {
     clear_error();
     CFM_ARG_CHECK(net && nsys >= 1 && snaps >= 1 && epochs >= 1, "arguments");
-    CFM_ARG_CHECK(smooth >= 0 && smooth <= 16, "smooth");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= FP_MAX_SMOOTH, "smooth must be in [0, 8]");
     CFM_ARG_CHECK(coarsen == 1 || coarsen == 2, "coarsen must be 1 or 2");
     CFM_ARG_CHECK(batch >= 1 && batch <= net->maxB, "batch must be in [1, max_batch]");
     net->smooth = smooth;

@@ -73,8 +73,21 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
 // grid: (ceil(W / (32 CIN_PASSES)), H, B), 256 threads.
 constexpr int CIN_PASSES = 8;
 __global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w, const float *b,
-                                                 bf16 *h0, int H, int W) {
+                                                 bf16 *h0, int H, int W, UNetInputScale in_scale) {
     pdl_enter();
+    // input channel 0 scale: 1 / rms from a solver's partial sums (fixed order)
+    float sc = 1.f;
+    if (in_scale.part) {
+        __shared__ double red[8];
+        double acc = 0;
+        for (int j = threadIdx.x; j < in_scale.nparts; j += blockDim.x) acc += in_scale.part[j];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        double tot = 0;
+        for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) tot += red[wi];
+        sc = tot > 0 ? (float)sqrt(in_scale.cells / tot) : 0.f;
+    }
     const int q = threadIdx.x & 7, c0 = q * 4;
     float wr[9][8];  // [t][(c - c0) * 2 + in]
 #pragma unroll
@@ -99,6 +112,7 @@ __global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w,
             const bool in = y >= 0 && y < H && xq >= 0 && xq < W;
             const int yc = min(max(y, 0), H - 1), xc = min(max(xq, 0), W - 1);
             v[t] = *reinterpret_cast<const float2 *>(xi + 2 * (yc * W + xc));
+            if (in_scale.part) v[t].x *= sc;
             if (!in) v[t] = make_float2(0.f, 0.f);
         }
         float o[4] = {bq.x, bq.y, bq.z, bq.w};
@@ -546,14 +560,16 @@ int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, i
 
 }  // namespace
 
-int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s) {
+int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
+                 const UNetInputScale *in_scale) {
     CFM_ARG_CHECK(B >= 1 && B <= u->maxB, "batch");
     UNetBuffers &a = u->a;
     const int H = u->H, W = u->W;
     int st;
     CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + 32 * CIN_PASSES - 1) / (32 * CIN_PASSES), H, B), dim3(256),
                             0, s, x, (const float *)(u->theta + u->woff[0]),
-                            (const float *)(u->theta + u->boff[0]), a.h0, H, W));
+                            (const float *)(u->theta + u->boff[0]), a.h0, H, W,
+                            in_scale ? *in_scale : UNetInputScale{nullptr, 0, 0.0}));
     int h = H, w = W;
     CFM_CUDA_TRY(launch_pdl(k_pool<32>, row_grid(w / 2 * 4, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h0,
                             a.p1, h / 2, w / 2));

@@ -27,8 +27,16 @@ float *unet_theta(UNetImpl *u);
 float *unet_grad(UNetImpl *u);
 int *unet_err(UNetImpl *u);
 int unet_refresh_weights(UNetImpl *u, cudaStream_t s);
+// Optional scaling of input channel 0 by sqrt(cells / sum(part[0 .. nparts))),
+// the partial sums of |r|^2 a solver left on the device (1 / rms(r)).
+struct UNetInputScale {
+    const double *part;
+    int nparts;
+    double cells;
+};
 // x FP32 [B][H][W][2] -> out FP32 [B][H][W] (device pointers).
-int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s);
+int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
+                 const UNetInputScale *in_scale = nullptr);
 // Accumulates the gradient of sum(out * dout) into unet_grad (after unet_forward).
 int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStream_t s);
 int unet_adam(UNetImpl *u, float lr, float grad_scale, cudaStream_t s);
