@@ -75,6 +75,7 @@ _SIGS = {
                                           _c.c_float, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp]),
     "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_destroy": (None, [_vp]),
+    "cfm_fpcg_set_truncation": (_c.c_int, [_vp, _c.c_int]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
     "cfm_batch_create": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -529,7 +530,7 @@ class UNet:
 class FPCG:
     """Flexible PCG with the network as preconditioner (cfm_fpcg)."""
 
-    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None):
+    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None):
         self.S, self.net = S, net
         self.k = np.ascontiguousarray(k, np.float64)
         h = ctypes.c_void_p()
@@ -539,6 +540,8 @@ class FPCG:
         check("cfm_fpcg_create", lib.cfm_fpcg_create(S.h, _ptr(self.k), None if net is None else net.h,
                                                      smooth, maxiter, tol, ctypes.byref(h)))
         self.h = h
+        if truncation is not None:
+            check("cfm_fpcg_set_truncation", lib.cfm_fpcg_set_truncation(self.h, truncation))
 
     def close(self):
         if self.h:

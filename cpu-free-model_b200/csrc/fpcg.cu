@@ -49,7 +49,7 @@ namespace cfm {
 namespace {
 
 // n-vectors in cfm_fpcg::vec: x r rold p s z b t d za zb r1.
-constexpr int FP_NVEC = 12;
+constexpr int FP_NVEC = 8;  // x r z b t d za r1
 
 // Damping of the Jacobi smoothing sweeps around the network.
 constexpr double JACOBI_OMEGA = 0.8;
@@ -251,12 +251,17 @@ __global__ void k_loss_anorm_grad(const float *Az, const float *r1, const double
 
 // ------------------------------------------------------------------ FPCG
 enum : int {
-    FP_PS = 0, FP_RR = 1, FP_ZR = 2, FP_ZRO = 3, FP_BB = 4, FP_R1 = 5, FP_YR = 6, FP_YAY = 7,
-    FP_NSLOT = 8
+    FP_PS = 0, FP_RR = 1, FP_PR = 2, FP_BB = 3, FP_R1 = 4, FP_YR = 5, FP_YAY = 6,
+    FP_ZS = 7,  // FP_ZS + j: <z_k, s_{k-1-j}>, j < m
 };
+// Truncated flexible CG (Notay's FCG(m)): each direction is A-orthogonalised
+// against the last m; directions p_j and s_j = A p_j live in a ring of m + 1
+// slots (slot j mod (m + 1)).
+constexpr int FP_MAX_TRUNC = 8;
+constexpr int FP_NSLOT = FP_ZS + FP_MAX_TRUNC;
 
 struct FpState {
-    double rz[2];        // <z, r> of the current direction (double-buffered by k parity)
+    double ps[FP_MAX_TRUNC + 1];  // <p_j, s_j> by ring slot
     double target;       // tol * |b|
     double best_rr;      // smallest |r|^2 seen
     long long k;         // iterations
@@ -269,8 +274,10 @@ struct FpArgs {
     StencilOp<2> op;
     int n, ntiles;
     const double *b;
-    double *x, *r, *rold, *p, *s, *z;
-    double *za, *zb, *r1;  // smoothing iterates, smoothed residual
+    double *x, *r, *z;
+    double *za, *r1;       // pre-smoothed z0, r1 = r - A z0
+    double *pring, *sring;  // FCG directions p_j and A p_j: ring slots of n
+    int m, ring;            // truncation m and ring size m + 1
     float *xin, *out;
     double *part;
     FpState *st;
@@ -287,6 +294,28 @@ struct FpArgs {
 
 __device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.pstride; }
 
+// Block sums of nv <= FP_MAX_TRUNC values at once (one barrier round instead
+// of nv): warp xor trees, then warp 0 adds the 32 warp sums in a fixed order.
+// Every thread gets the sums in v.  sm: 32 * FP_MAX_TRUNC + FP_MAX_TRUNC doubles.
+__device__ void block_sum_multi(double *v, int nv, double *sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = 0; j < nv; ++j) {
+        double x = v[j];
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sm[warp * FP_MAX_TRUNC + j] = x;
+    }
+    __syncthreads();
+    if (warp == 0)
+        for (int j = 0; j < nv; ++j) {
+            double x = lane < nw ? sm[lane * FP_MAX_TRUNC + j] : 0.0;
+            for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) sm[32 * FP_MAX_TRUNC + j] = x;
+        }
+    __syncthreads();
+    for (int j = 0; j < nv; ++j) v[j] = sm[32 * FP_MAX_TRUNC + j];
+    __syncthreads();
+}
+
 #define FP_ROW const int i = blockIdx.x * CG_TILE + threadIdx.x
 
 // x = 0, r = b; partials |b|^2, |r|^2.
@@ -298,8 +327,6 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
         const double bi = a.b[i];
         a.x[i] = 0.0;
         a.r[i] = bi;
-        a.rold[i] = 0.0;
-        a.p[i] = 0.0;
         bb = bi * bi;
     }
     bb = block_sum(bb, sm);
@@ -312,7 +339,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
         a.st->done = 0;
         a.st->best_rr = 1e300;
         a.st->best_k = 0;
-        a.st->rz[0] = a.st->rz[1] = 0;
+        for (int j = 0; j <= FP_MAX_TRUNC; ++j) a.st->ps[j] = 0;
         a.st->target = -tol;  // resolved by k_fp_pre from |b|
     }
 }
@@ -329,9 +356,19 @@ constexpr int FP_TILE = 32;  // one thread per tile cell: FP_TILE^2 = CG_TILE th
 static_assert(FP_TILE * FP_TILE == CG_TILE, "one thread per tile cell");
 constexpr int FP_MAX_SMOOTH = 8;
 
+// Region arrays [R * R] each, region-local, one after the other in shared
+// memory: r, z0, z1, we, wn, dg, wd = omega / dg (addressed from one base
+// to keep registers free).
 struct FpTile {
-    int x0, y0, H, R;  // tile origin, halo, region side (FP_TILE + 2 H)
-    double *r, *z0, *z1, *we, *wn, *dg, *wd;  // [R * R] each, region-local; wd = omega / dg
+    int x0, y0, H, R, RR;  // tile origin, halo, region side (FP_TILE + 2 H), R * R
+    double *d;
+    __device__ __forceinline__ double *r() const { return d; }
+    __device__ __forceinline__ double *z0() const { return d + RR; }
+    __device__ __forceinline__ double *z1() const { return d + 2 * RR; }
+    __device__ __forceinline__ double *we() const { return d + 3 * RR; }
+    __device__ __forceinline__ double *wn() const { return d + 4 * RR; }
+    __device__ __forceinline__ double *dg() const { return d + 5 * RR; }
+    __device__ __forceinline__ double *wd() const { return d + 6 * RR; }
 };
 
 // Region cells are visited as (row, column) by warps over rows and lanes
@@ -352,20 +389,18 @@ __device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
     t.y0 = (blockIdx.x / a.tx2) * FP_TILE;
     t.H = H;
     t.R = FP_TILE + 2 * H;
-    double *d = reinterpret_cast<double *>(smem);
-    const int RR = t.R * t.R;
-    t.r = d, t.z0 = d + RR, t.z1 = d + 2 * RR, t.we = d + 3 * RR, t.wn = d + 4 * RR, t.dg = d + 5 * RR;
-    t.wd = d + 6 * RR;
+    t.d = reinterpret_cast<double *>(smem);
+    t.RR = t.R * t.R;
     FP_FOR_SQUARE(0, t.R, row, col) {
         int i;
         const bool in = fp_inside(t, a, row, col, &i);
         const int l = row * t.R + col;
-        t.r[l] = in ? a.r[i] : 0.0;
-        t.we[l] = in ? a.op.we[i] : 0.0;
-        t.wn[l] = in ? a.op.wn[i] : 0.0;
+        t.r()[l] = in ? a.r[i] : 0.0;
+        t.we()[l] = in ? a.op.we[i] : 0.0;
+        t.wn()[l] = in ? a.op.wn[i] : 0.0;
         const double dg = in ? a.op.dg[i] : 1.0;
-        t.dg[l] = dg;
-        t.wd[l] = JACOBI_OMEGA / dg;
+        t.dg()[l] = dg;
+        t.wd()[l] = JACOBI_OMEGA / dg;
     }
     return t;
 }
@@ -375,11 +410,12 @@ __device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
 __device__ __forceinline__ double fp_apply(const FpTile &t, const FpArgs &a, const double *u, int row,
                                            int col) {
     const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row, l = row * t.R + col;
-    double v = __dmul_rn(t.dg[l], u[l]);
-    if (gx > 0) v = __fma_rn(-t.we[l - 1], u[l - 1], v);
-    if (gx < a.op.nx - 1) v = __fma_rn(-t.we[l], u[l + 1], v);
-    if (gy > 0) v = __fma_rn(-t.wn[l - t.R], u[l - t.R], v);
-    if (gy < a.op.ny - 1) v = __fma_rn(-t.wn[l], u[l + t.R], v);
+    const double *we = t.we(), *wn = t.wn();
+    double v = __dmul_rn(t.dg()[l], u[l]);
+    if (gx > 0) v = __fma_rn(-we[l - 1], u[l - 1], v);
+    if (gx < a.op.nx - 1) v = __fma_rn(-we[l], u[l + 1], v);
+    if (gy > 0) v = __fma_rn(-wn[l - t.R], u[l - t.R], v);
+    if (gy < a.op.ny - 1) v = __fma_rn(-wn[l], u[l + t.R], v);
     return v;
 }
 
@@ -393,8 +429,8 @@ __device__ double *fp_sweeps(const FpTile &t, const FpArgs &a, double *cur, doub
             int i;
             if (!fp_inside(t, a, row, col, &i)) continue;
             const int l = row * t.R + col;
-            const double res = t.r[l] - fp_apply(t, a, cur, row, col);
-            nxt[l] = __fma_rn(t.wd[l], res, cur[l]);
+            const double res = t.r()[l] - fp_apply(t, a, cur, row, col);
+            nxt[l] = __fma_rn(t.wd()[l], res, cur[l]);
         }
         __syncthreads();
         double *sw = cur;
@@ -408,7 +444,7 @@ __device__ double *fp_sweeps(const FpTile &t, const FpArgs &a, double *cur, doub
 // |r|^2 history, convergence / stall test]; z0 = `smooth` sweeps from zero,
 // r1 = r - A z0, partial |r1|^2, and the network input channel 0 = R(r1)
 // (f x f means; the network scales it by 1 / rms(r1) itself).
-__global__ void __launch_bounds__(CG_TILE) k_fp_pre(FpArgs a, int tick) {
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
@@ -440,10 +476,10 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_pre(FpArgs a, int tick) {
     // sweep 1 from zero is pointwise: z = (omega / dg) r on the whole region
     FP_FOR_SQUARE(0, t.R, row, col) {
         const int l = row * t.R + col;
-        t.z0[l] = a.smooth > 0 ? t.wd[l] * t.r[l] : 0.0;
+        t.z0()[l] = a.smooth > 0 ? t.wd()[l] * t.r()[l] : 0.0;
     }
     __syncthreads();
-    const double *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0, t.z1, 0, a.smooth - 1) : t.z0;
+    const double *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth - 1) : t.z0();
     // this thread's tile cell
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
@@ -451,7 +487,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_pre(FpArgs a, int tick) {
     const bool in = fp_inside(t, a, row, col, &i);
     double q = 0;
     if (in) {
-        const double v = t.r[l] - fp_apply(t, a, z, row, col);
+        const double v = t.r()[l] - fp_apply(t, a, z, row, col);
         a.r1[i] = v;
         a.za[i] = z[l];
         q = v * v;
@@ -477,8 +513,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_pre(FpArgs a, int tick) {
 // z0 + c P y, c = <P y, r1> / <P y, A P y> from the ydots partials (of all
 // multiples of P y, c P y removes the most A-norm error from A d = r1, so the
 // network's correction can only help the smoothed iterate), written to a.z
-// with the partials <z, r> and <z, r_old>.
-__global__ void __launch_bounds__(CG_TILE) k_fp_post(FpArgs a) {
+// with the partials <z_k, s_{k-1-j}> (j < min(k, m)) of the orthogonalisation.
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
@@ -490,27 +526,31 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_post(FpArgs a) {
     FP_FOR_SQUARE(0, t.R, row, col) {
         int i;
         const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
-        t.z0[row * t.R + col] = fp_inside(t, a, row, col, &i)
+        t.z0()[row * t.R + col] = fp_inside(t, a, row, col, &i)
                                     ? a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)]
                                     : 0.0;
     }
     __syncthreads();
-    const double *z = fp_sweeps(t, a, t.z0, t.z1, 0, a.smooth);
+    const double *z = fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth);
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
     int i;
-    double zr = 0, zro = 0;
-    if (fp_inside(t, a, row, col, &i)) {
-        const double zi = z[l];
+    const bool in = fp_inside(t, a, row, col, &i);
+    double zi = 0;
+    if (in) {
+        zi = z[l];
         a.z[i] = zi;
-        zr = zi * a.r[i];
-        zro = zi * a.rold[i];
     }
-    zr = block_sum(zr, sm);
-    zro = block_sum(zro, sm);
-    if (threadIdx.x == 0) {
-        fslot(a, FP_ZR)[blockIdx.x] = zr;
-        fslot(a, FP_ZRO)[blockIdx.x] = zro;
+    const long long k = a.st->k;
+    const int nj = (int)min((long long)a.m, k);
+    if (nj > 0) {
+        __shared__ double smm[33 * FP_MAX_TRUNC];
+        double v[FP_MAX_TRUNC];
+#pragma unroll
+        for (int j = 0; j < FP_MAX_TRUNC; ++j)
+            v[j] = (j < nj && in) ? zi * a.sring[(size_t)((k - 1 - j) % a.ring) * a.n + i] : 0.0;
+        block_sum_multi(v, nj, smm);
+        if (threadIdx.x < nj) fslot(a, FP_ZS + threadIdx.x)[blockIdx.x] = v[threadIdx.x];
     }
 }
 
@@ -553,63 +593,82 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     }
 }
 
-// beta = max(0, (<z,r> - <z,r_old>) / <z_old, r_old>) (0 on the first
-// step); p = z + beta p; and the loop condition.  <z, r> of direction k
-// lives in rz[(k + 1) & 1] (k = iterations done when it was formed), so the
-// value being read and the value being written never share a slot.
+// p_k = z_k - sum_j (<z_k, s_j> / <p_j, s_j>) p_j over the last min(k, m)
+// directions (into ring slot k mod (m + 1)), partial <p_k, r_k>, and the
+// loop condition.
 __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond,
                                                     int set_cond) {
     pdl_enter();
     __shared__ double sm[33];
-    const double zr = sum_partials(fslot(a, FP_ZR), a.ntiles2, sm);
-    const double zro = sum_partials(fslot(a, FP_ZRO), a.ntiles2, sm);
     const long long k = a.st->k;
-    const double rz_old = a.st->rz[k & 1];
-    double beta = 0.0;
-    if (k > 0 && rz_old != 0.0) beta = fmax(0.0, (zr - zro) / rz_old);
-    FP_ROW;
-    if (i < a.n) a.p[i] = a.z[i] + beta * a.p[i];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        a.st->rz[(k + 1) & 1] = zr;
-        if (set_cond) cudaGraphSetConditional(cond, a.st->done ? 0u : 1u);
+    const int nj = (int)min((long long)a.m, k);
+    double beta[FP_MAX_TRUNC];
+    if (nj > 0) {
+        __shared__ double smm[33 * FP_MAX_TRUNC];
+#pragma unroll
+        for (int j = 0; j < FP_MAX_TRUNC; ++j) {
+            double acc = 0.0;
+            if (j < nj)
+                for (int t = threadIdx.x; t < a.ntiles2; t += blockDim.x) acc += fslot(a, FP_ZS + j)[t];
+            beta[j] = acc;
+        }
+        block_sum_multi(beta, nj, smm);
+        for (int j = 0; j < nj; ++j) {
+            const double ps = a.st->ps[(k - 1 - j) % a.ring];
+            beta[j] = ps != 0.0 ? beta[j] / ps : 0.0;
+        }
     }
+    FP_ROW;
+    double pr = 0;
+    if (i < a.n) {
+        double pi = a.z[i];
+        for (int j = 0; j < nj; ++j) pi -= beta[j] * a.pring[(size_t)((k - 1 - j) % a.ring) * a.n + i];
+        a.pring[(size_t)(k % a.ring) * a.n + i] = pi;
+        pr = pi * a.r[i];
+    }
+    pr = block_sum(pr, sm);
+    if (threadIdx.x == 0) fslot(a, FP_PR)[blockIdx.x] = pr;
+    if (set_cond && blockIdx.x == 0 && threadIdx.x == 0)
+        cudaGraphSetConditional(cond, a.st->done ? 0u : 1u);
 }
 
-// s = A p; partial <p, s>.
+// s_k = A p_k; partial <p_k, s_k>.
 __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
     pdl_enter();
     __shared__ double sm[33];
+    const long long slot = a.st->k % a.ring;
+    const double *p = a.pring + (size_t)slot * a.n;
     FP_ROW;
     double ps = 0;
     if (i < a.n) {
-        const double si = a.op.apply(a.p, i);
-        a.s[i] = si;
-        ps = a.p[i] * si;
+        const double si = a.op.apply(p, i);
+        a.sring[(size_t)slot * a.n + i] = si;
+        ps = p[i] * si;
     }
     ps = block_sum(ps, sm);
     if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
 }
 
-// alpha = <z, r> / <p, s>; x += alpha p; r_old = r; r -= alpha s; |r|^2.
+// alpha = <p_k, r_k> / <p_k, s_k>; x += alpha p_k; r -= alpha s_k; |r|^2;
+// <p_k, s_k> kept in the ring for the orthogonalisations to come.
 __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     pdl_enter();
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
-    const long long k = a.st->k;
-    const double rz = a.st->rz[(k + 1) & 1];
-    const double alpha = ps != 0.0 ? rz / ps : 0.0;
+    const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
+    const long long slot = a.st->k % a.ring;
+    const double alpha = ps != 0.0 ? pr / ps : 0.0;
     FP_ROW;
     double rr = 0;
     if (i < a.n) {
-        a.x[i] += alpha * a.p[i];
-        const double ri = a.r[i];
-        a.rold[i] = ri;
-        const double rn = ri - alpha * a.s[i];
+        a.x[i] += alpha * a.pring[(size_t)slot * a.n + i];
+        const double rn = a.r[i] - alpha * a.sring[(size_t)slot * a.n + i];
         a.r[i] = rn;
         rr = rn * rn;
     }
     rr = block_sum(rr, sm);
     if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
 }
 
 // t = b - A x, |t|^2 (atomics; the reported true residual).
@@ -655,7 +714,9 @@ struct cfm_fpcg {
     int coarsen = 1, nc = 0;  // the network runs on (nx / coarsen) x (ny / coarsen) = nc cells
     long long maxiter = 0;
     double tol = 0;
-    double *vec = nullptr;  // x r rold p s z b t d za zb r1 (12 n)
+    double *vec = nullptr;   // x r z b t d za r1 (FP_NVEC n)
+    int m = 0;               // FCG truncation
+    double *ring = nullptr;  // p and A p ring slots: 2 (m + 1) n
     int smooth = 0;
     float *xin = nullptr, *out = nullptr;
     double *part = nullptr, *acc = nullptr, *hist = nullptr;
@@ -678,15 +739,15 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.ntiles = h->ntiles;
     a.x = h->vec;
     a.r = h->vec + n;
-    a.rold = h->vec + 2 * n;
-    a.p = h->vec + 3 * n;
-    a.s = h->vec + 4 * n;
-    a.z = h->vec + 5 * n;
-    a.b = h->vec + 6 * n;
-    a.za = h->vec + 9 * n;
-    a.zb = h->vec + 10 * n;
-    a.r1 = h->vec + 11 * n;
-    static_assert(FP_NVEC == 12, "x r rold p s z b t d za zb r1");
+    a.z = h->vec + 2 * n;
+    a.b = h->vec + 3 * n;
+    a.za = h->vec + 6 * n;
+    a.r1 = h->vec + 7 * n;
+    static_assert(FP_NVEC == 8, "x r z b t d za r1");
+    a.m = h->m;
+    a.ring = h->m + 1;
+    a.pring = h->ring;
+    a.sring = h->ring + (size_t)(h->m + 1) * n;
     a.xin = h->xin;
     a.out = h->out;
     a.part = h->part;
@@ -817,7 +878,11 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     cudaError_t e;
     std::vector<double> kk(k_host, k_host + n);
     double *kd = nullptr;
+    // a linear SPD preconditioner (Jacobi alone) needs no more than the
+    // one-term recurrence; the network's nonlinear one gains from a deeper one
+    h->m = net ? FP_MAX_TRUNC : 1;
     if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->ring, sizeof(double) * 2 * (h->m + 1) * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->xin, sizeof(float) * 2 * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->out, sizeof(float) * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->pstride)) != cudaSuccess ||
@@ -825,6 +890,10 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
                                   (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
         (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
         (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
         (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1))) != cudaSuccess ||
@@ -853,6 +922,7 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     cudaFree(h->vec);
+    cudaFree(h->ring);
     cudaFree(h->xin);
     cudaFree(h->out);
     cudaFree(h->part);
@@ -865,13 +935,33 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     delete h;
 }
 
+int cfm_fpcg_set_truncation(cfm_fpcg *h, int m) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(m >= 1 && m <= FP_MAX_TRUNC, "truncation must be in [1, 8]");
+    if (m == h->m) return CFM_OK;
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    double *ring = nullptr;
+    CFM_CUDA_TRY(cudaMalloc(&ring, sizeof(double) * 2 * (m + 1) * (size_t)h->n));
+    cudaFree(h->ring);
+    h->ring = ring;
+    h->m = m;
+    // the captured iteration graph holds the old ring: build it again
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->exec = nullptr;
+    h->graph = nullptr;
+    h->conditional = false;
+    return CFM_OK;
+}
+
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *stats) {
     clear_error();
     CFM_ARG_CHECK(h && b_host && x_host, "null argument");
     const size_t n = h->n;
     FpArgs a = fp_args(h);
     cudaStream_t s = h->stream;
-    double *b = h->vec + 6 * n, *t = h->vec + 7 * n, *d = h->vec + 8 * n;
+    double *b = h->vec + 3 * n, *t = h->vec + 4 * n, *d = h->vec + 5 * n;
     CFM_CUDA_TRY(cudaMemcpyAsync(b, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     if (h->net) CFM_CUDA_TRY(cudaMemsetAsync(unet_err(h->net->u), 0, sizeof(int), s));
     int st = 0;

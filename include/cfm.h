@@ -340,10 +340,11 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                            int batch, float lr, int smooth, int coarsen, double *loss_first,
                            double *loss_last, double *data_seconds, double *train_seconds);
 
-/* Flexible PCG (Polak-Ribiere beta) on a 2D stencil operator with the
+/* Flexible PCG (truncated FCG(m): each direction A-orthogonalised against
+ * the last m, alpha = <p, r> / <p, A p>) on a 2D stencil operator with the
  * preconditioner z = J(z0 + c y): z0 = J(0), r1 = r - A z0,
  * y = net(r1 / |r1|_rms, log k), c = <y, r1> / <y, A y> (the optimal step
- * along y), J = `smooth` damped Jacobi sweeps (omega 0.8) on A z = r;
+ * along y), J = `smooth` damped Jacobi sweeps (omega 0.8, smooth <= 8) on A z = r;
  * k_host the cell coefficients the stencil was built from; smooth must
  * equal the value the network was trained with.  FP64 vectors and dots; one
  * CUDA graph whose conditional while-node runs the iterations on the device.
@@ -358,6 +359,9 @@ typedef struct cfm_fpcg cfm_fpcg;
 int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int smooth,
                     int maxiter, double tol, cfm_fpcg **out);
 void cfm_fpcg_destroy(cfm_fpcg *h);
+/* Truncation m in [1, 8] of the orthogonalisation (default 8 with a
+ * network, 1 without); m = 1 is the Polak-Ribiere-like one-term recurrence. */
+int cfm_fpcg_set_truncation(cfm_fpcg *h, int m);
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
 /* Recursive residual norms |r_k| of the last solve, one per iteration from
  * k = 0 (at most max_n; *n_out = the count).  net == NULL in
