@@ -287,6 +287,7 @@ struct FpArgs {
     int f, ncx, nc;  // network grid: (nx / f) x (ny / f) = nc cells, ncx per row
     int fsh;         // log2 f
     int ntiles2, tx2;  // FP_TILE x FP_TILE tiles of the smoothing kernels (tx2 per row)
+    const float *we32, *wn32, *dg32, *wd32;  // FP32 operator and omega / dg for the smoothing
     int pstride;       // partial-sum slot stride: max(ntiles, ntiles2)
     int smooth;
 };
@@ -345,13 +346,14 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
 }
 
 // ------------------------------------------------ smoothing, temporally blocked
-// The preconditioner's Jacobi sweeps run on FP_TILE x FP_TILE tiles held in
-// shared memory with a halo as wide as the sweeps need, so that all sweeps of
-// one application (and what surrounds them) take one launch: each sweep
-// shrinks the valid region by one cell, cells outside the grid are never read
-// (the Dirichlet apply skips them), and the arithmetic is the global
-// operator's (A u)_i = dg u_i - we_{i-1} u_{i-1} - we_i u_{i+1} - wn_{i-nx}
-// u_{i-nx} - wn_i u_{i+nx}, in that order.
+// The preconditioner's Jacobi sweeps run in FP32 (the Krylov recurrences
+// around them stay FP64; a preconditioner may be inexact in flexible CG) on
+// FP_TILE x FP_TILE tiles held in shared memory with a halo as wide as the
+// sweeps need, so that all sweeps of one application (and what surrounds
+// them) take one launch: each sweep shrinks the valid region by one cell,
+// cells outside the grid are never read (the Dirichlet apply skips them),
+// and the arithmetic is the operator's (A u)_i = dg u_i - we_{i-1} u_{i-1} -
+// we_i u_{i+1} - wn_{i-nx} u_{i-nx} - wn_i u_{i+nx}, in that order.
 constexpr int FP_TILE = 32;  // one thread per tile cell: FP_TILE^2 = CG_TILE threads
 static_assert(FP_TILE * FP_TILE == CG_TILE, "one thread per tile cell");
 constexpr int FP_MAX_SMOOTH = 8;
@@ -361,14 +363,14 @@ constexpr int FP_MAX_SMOOTH = 8;
 // to keep registers free).
 struct FpTile {
     int x0, y0, H, R, RR;  // tile origin, halo, region side (FP_TILE + 2 H), R * R
-    double *d;
-    __device__ __forceinline__ double *r() const { return d; }
-    __device__ __forceinline__ double *z0() const { return d + RR; }
-    __device__ __forceinline__ double *z1() const { return d + 2 * RR; }
-    __device__ __forceinline__ double *we() const { return d + 3 * RR; }
-    __device__ __forceinline__ double *wn() const { return d + 4 * RR; }
-    __device__ __forceinline__ double *dg() const { return d + 5 * RR; }
-    __device__ __forceinline__ double *wd() const { return d + 6 * RR; }
+    float *d;
+    __device__ __forceinline__ float *r() const { return d; }
+    __device__ __forceinline__ float *z0() const { return d + RR; }
+    __device__ __forceinline__ float *z1() const { return d + 2 * RR; }
+    __device__ __forceinline__ float *we() const { return d + 3 * RR; }
+    __device__ __forceinline__ float *wn() const { return d + 4 * RR; }
+    __device__ __forceinline__ float *dg() const { return d + 5 * RR; }
+    __device__ __forceinline__ float *wd() const { return d + 6 * RR; }
 };
 
 // Region cells are visited as (row, column) by warps over rows and lanes
@@ -389,51 +391,49 @@ __device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
     t.y0 = (blockIdx.x / a.tx2) * FP_TILE;
     t.H = H;
     t.R = FP_TILE + 2 * H;
-    t.d = reinterpret_cast<double *>(smem);
+    t.d = reinterpret_cast<float *>(smem);
     t.RR = t.R * t.R;
     FP_FOR_SQUARE(0, t.R, row, col) {
         int i;
         const bool in = fp_inside(t, a, row, col, &i);
         const int l = row * t.R + col;
-        t.r()[l] = in ? a.r[i] : 0.0;
-        t.we()[l] = in ? a.op.we[i] : 0.0;
-        t.wn()[l] = in ? a.op.wn[i] : 0.0;
-        const double dg = in ? a.op.dg[i] : 1.0;
-        t.dg()[l] = dg;
-        t.wd()[l] = JACOBI_OMEGA / dg;
+        t.r()[l] = in ? (float)a.r[i] : 0.f;
+        t.we()[l] = in ? a.we32[i] : 0.f;
+        t.wn()[l] = in ? a.wn32[i] : 0.f;
+        t.dg()[l] = in ? a.dg32[i] : 1.f;
+        t.wd()[l] = in ? a.wd32[i] : 0.f;
     }
     return t;
 }
 
 // (A u) at region cell (row, col) of a global cell (gx, gy) inside the grid,
 // its neighbours in the region.
-__device__ __forceinline__ double fp_apply(const FpTile &t, const FpArgs &a, const double *u, int row,
-                                           int col) {
+__device__ __forceinline__ float fp_apply(const FpTile &t, const FpArgs &a, const float *u, int row, int col) {
     const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row, l = row * t.R + col;
-    const double *we = t.we(), *wn = t.wn();
-    double v = __dmul_rn(t.dg()[l], u[l]);
-    if (gx > 0) v = __fma_rn(-we[l - 1], u[l - 1], v);
-    if (gx < a.op.nx - 1) v = __fma_rn(-we[l], u[l + 1], v);
-    if (gy > 0) v = __fma_rn(-wn[l - t.R], u[l - t.R], v);
-    if (gy < a.op.ny - 1) v = __fma_rn(-wn[l], u[l + t.R], v);
+    const float *we = t.we(), *wn = t.wn();
+    float v = __fmul_rn(t.dg()[l], u[l]);
+    if (gx > 0) v = __fmaf_rn(-we[l - 1], u[l - 1], v);
+    if (gx < a.op.nx - 1) v = __fmaf_rn(-we[l], u[l + 1], v);
+    if (gy > 0) v = __fmaf_rn(-wn[l - t.R], u[l - t.R], v);
+    if (gy < a.op.ny - 1) v = __fmaf_rn(-wn[l], u[l + t.R], v);
     return v;
 }
 
 // `sweeps` damped Jacobi sweeps on A z = r, z += (omega / dg) (r - A z),
 // starting from *cur (valid at margin m0 of the region); returns the buffer
 // holding the result, valid at margin m0 + sweeps.
-__device__ double *fp_sweeps(const FpTile &t, const FpArgs &a, double *cur, double *nxt, int m0, int sweeps) {
+__device__ float *fp_sweeps(const FpTile &t, const FpArgs &a, float *cur, float *nxt, int m0, int sweeps) {
     for (int s = 0; s < sweeps; ++s) {
         const int m = m0 + s + 1, side = t.R - 2 * m;
         FP_FOR_SQUARE(m, side, row, col) {
             int i;
             if (!fp_inside(t, a, row, col, &i)) continue;
             const int l = row * t.R + col;
-            const double res = t.r()[l] - fp_apply(t, a, cur, row, col);
-            nxt[l] = __fma_rn(t.wd()[l], res, cur[l]);
+            const float res = t.r()[l] - fp_apply(t, a, cur, row, col);
+            nxt[l] = __fmaf_rn(t.wd()[l], res, cur[l]);
         }
         __syncthreads();
-        double *sw = cur;
+        float *sw = cur;
         cur = nxt;
         nxt = sw;
     }
@@ -476,10 +476,10 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
     // sweep 1 from zero is pointwise: z = (omega / dg) r on the whole region
     FP_FOR_SQUARE(0, t.R, row, col) {
         const int l = row * t.R + col;
-        t.z0()[l] = a.smooth > 0 ? t.wd()[l] * t.r()[l] : 0.0;
+        t.z0()[l] = a.smooth > 0 ? t.wd()[l] * t.r()[l] : 0.f;
     }
     __syncthreads();
-    const double *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth - 1) : t.z0();
+    const float *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth - 1) : t.z0();
     // this thread's tile cell
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
@@ -487,9 +487,9 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
     const bool in = fp_inside(t, a, row, col, &i);
     double q = 0;
     if (in) {
-        const double v = t.r()[l] - fp_apply(t, a, z, row, col);
+        const double v = (double)(t.r()[l] - fp_apply(t, a, z, row, col));
         a.r1[i] = v;
-        a.za[i] = z[l];
+        a.za[i] = (double)z[l];
         q = v * v;
     }
     q = block_sum(q, sm);  // (its barriers also order the r1 stores before the restriction)
@@ -526,35 +526,44 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a) {
     FP_FOR_SQUARE(0, t.R, row, col) {
         int i;
         const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
-        t.z0()[row * t.R + col] = fp_inside(t, a, row, col, &i)
-                                    ? a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)]
-                                    : 0.0;
+        t.z0()[row * t.R + col] =
+            fp_inside(t, a, row, col, &i)
+                ? (float)(a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)])
+                : 0.f;
     }
     __syncthreads();
-    const double *z = fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth);
+    const float *z = fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth);
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
     int i;
     const bool in = fp_inside(t, a, row, col, &i);
     double zi = 0;
     if (in) {
-        zi = z[l];
+        zi = (double)z[l];
         a.z[i] = zi;
     }
-    const long long k = a.st->k;
-    const int nj = (int)min((long long)a.m, k);
+    const int k = (int)a.st->k;
+    const int nj = min(a.m, k);
     if (nj > 0) {
         __shared__ double smm[33 * FP_MAX_TRUNC];
+        __shared__ const double *sj[FP_MAX_TRUNC];
+        if (threadIdx.x < nj) sj[threadIdx.x] = a.sring + (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
+        __syncthreads();
         double v[FP_MAX_TRUNC];
 #pragma unroll
-        for (int j = 0; j < FP_MAX_TRUNC; ++j)
-            v[j] = (j < nj && in) ? zi * a.sring[(size_t)((k - 1 - j) % a.ring) * a.n + i] : 0.0;
+        for (int j = 0; j < FP_MAX_TRUNC; ++j) v[j] = (j < nj && in) ? zi * sj[j][i] : 0.0;
         block_sum_multi(v, nj, smm);
         if (threadIdx.x < nj) fslot(a, FP_ZS + threadIdx.x)[blockIdx.x] = v[threadIdx.x];
     }
 }
 
-size_t fp_smem_bytes(int H) { return 7 * sizeof(double) * (size_t)(FP_TILE + 2 * H) * (FP_TILE + 2 * H); }
+size_t fp_smem_bytes(int H) { return 7 * sizeof(float) * (size_t)(FP_TILE + 2 * H) * (FP_TILE + 2 * H); }
+
+// omega / dg in FP32 for the smoothing (once per solver).
+__global__ void k_fp_wd(const float *dg32, float *wd32, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        wd32[i] = (float)(JACOBI_OMEGA / (double)dg32[i]);
+}
 
 // Identity in place of the network: out = R(r1) (unscaled; c absorbs the scale).
 __global__ void k_fp_identity(FpArgs a) {
@@ -600,8 +609,10 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
                                                     int set_cond) {
     pdl_enter();
     __shared__ double sm[33];
-    const long long k = a.st->k;
-    const int nj = (int)min((long long)a.m, k);
+    const int k = (int)a.st->k;
+    const int nj = min(a.m, k);
+    __shared__ const double *pj[FP_MAX_TRUNC];
+    if (threadIdx.x < nj) pj[threadIdx.x] = a.pring + (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
     double beta[FP_MAX_TRUNC];
     if (nj > 0) {
         __shared__ double smm[33 * FP_MAX_TRUNC];
@@ -618,11 +629,12 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
             beta[j] = ps != 0.0 ? beta[j] / ps : 0.0;
         }
     }
+    __syncthreads();  // pj
     FP_ROW;
     double pr = 0;
     if (i < a.n) {
         double pi = a.z[i];
-        for (int j = 0; j < nj; ++j) pi -= beta[j] * a.pring[(size_t)((k - 1 - j) % a.ring) * a.n + i];
+        for (int j = 0; j < nj; ++j) pi -= beta[j] * pj[j][i];
         a.pring[(size_t)(k % a.ring) * a.n + i] = pi;
         pr = pi * a.r[i];
     }
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
 __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
     pdl_enter();
     __shared__ double sm[33];
-    const long long slot = a.st->k % a.ring;
+    const int slot = (int)a.st->k % a.ring;
     const double *p = a.pring + (size_t)slot * a.n;
     FP_ROW;
     double ps = 0;
@@ -656,7 +668,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
-    const long long slot = a.st->k % a.ring;
+    const int slot = (int)a.st->k % a.ring;
     const double alpha = ps != 0.0 ? pr / ps : 0.0;
     FP_ROW;
     double rr = 0;
@@ -716,6 +728,7 @@ struct cfm_fpcg {
     double tol = 0;
     double *vec = nullptr;   // x r z b t d za r1 (FP_NVEC n)
     int m = 0;               // FCG truncation
+    float *wd32 = nullptr;   // omega / dg (FP32)
     double *ring = nullptr;  // p and A p ring slots: 2 (m + 1) n
     int smooth = 0;
     float *xin = nullptr, *out = nullptr;
@@ -760,6 +773,13 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.ncx = h->nx / h->coarsen;
     a.nc = h->nc;
     a.ntiles2 = h->ntiles2;
+    {
+        const float *c32 = stencil_coeffs32(h->S);  // we | wn | wt | dg
+        a.we32 = c32;
+        a.wn32 = c32 + n;
+        a.dg32 = c32 + 3 * n;
+        a.wd32 = h->wd32;
+    }
     a.tx2 = h->tx2;
     a.pstride = h->pstride;
     a.smooth = h->smooth;
@@ -883,6 +903,7 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     h->m = net ? FP_MAX_TRUNC : 1;
     if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->ring, sizeof(double) * 2 * (h->m + 1) * n)) != cudaSuccess ||
+        (e = cudaMalloc(&h->wd32, sizeof(float) * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->xin, sizeof(float) * 2 * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->out, sizeof(float) * h->nc)) != cudaSuccess ||
         (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->pstride)) != cudaSuccess ||
@@ -906,6 +927,7 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
         CFM_CUDA_TRY(e);
     }
     k_log_coarse<<<256, 256>>>(kd, h->xin, nx, ny, f);
+    k_fp_wd<<<256, 256>>>(stencil_coeffs32(S) + 3 * n, h->wd32, h->n);
     e = cudaDeviceSynchronize();
     cudaFree(kd);
     if (e != cudaSuccess) {
@@ -923,6 +945,7 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     cudaFree(h->vec);
     cudaFree(h->ring);
+    cudaFree(h->wd32);
     cudaFree(h->xin);
     cudaFree(h->out);
     cudaFree(h->part);
