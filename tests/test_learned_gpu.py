@@ -67,3 +67,53 @@ def test_fpcg_rejects_mismatched_smoothing(trained, system):
     k, f, S = system
     with pytest.raises(cfm.CfmError):
         cfm.FPCG(S, k, net, smooth=SMOOTH + 1)
+
+
+# ------------------------------------------- the two-level (coarse) network
+NC = 512
+
+
+@pytest.fixture(scope="module")
+def coarse_trained():
+    """A (NC/2)^2 network trained on plain-CG pairs of NC^2 systems: it sees
+    the 2x-restricted residual and its output is prolongated."""
+    net = cfm.UNet(NC // 2, NC // 2, max_batch=8, seed=5)
+    info = net.train_varcoef(24, 9, 7000, 8, 8, 1e-3, smooth=SMOOTH, coarsen=2)
+    return net, info
+
+
+def test_coarse_network_preconditioner(coarse_trained):
+    net, info = coarse_trained
+    assert info["loss_last"] < info["loss_first"], info
+    k, f = cfm.varcoef_problem((NC, NC), 78)
+    S = cfm.Stencil(k)
+    xs, st_cg = cfm.CG(S, cfm.CG_PERSISTENT, 50000, 1e-8).solve(f.ravel())
+    _, st_j = cfm.FPCG(S, k, None, maxiter=20000, tol=1e-8, smooth=SMOOTH).solve(f)
+    x_n, st_n = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8).solve(f)  # FCG(8) by default
+    print(f"plain CG {st_cg.iterations} it; Jacobi FPCG {st_j.iterations} it; "
+          f"coarse learned FCG(8) {st_n.iterations} it ({st_n.seconds * 1e3:.1f} ms)")
+    assert st_n.status == cfm.OK and st_n.refinements == 0 and st_n.residual <= 1e-8
+    assert st_n.iterations < 0.85 * st_j.iterations
+    assert np.linalg.norm(x_n - xs) / np.linalg.norm(xs) < 1e-5
+
+
+def test_truncation_choices_converge(coarse_trained):
+    """Every truncation of the orthogonalisation reaches the tolerance (the
+    fallback stays unused), and m can be changed between solves."""
+    net, _ = coarse_trained
+    k, f = cfm.varcoef_problem((NC, NC), 79)
+    S = cfm.Stencil(k)
+    fp = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8)
+    for m in (1, 2, 8):
+        cfm.check("cfm_fpcg_set_truncation", cfm.lib.cfm_fpcg_set_truncation(fp.h, m))
+        _, st = fp.solve(f)
+        assert st.status == cfm.OK and st.refinements == 0 and st.residual <= 1e-8, m
+    with pytest.raises(cfm.CfmError):
+        cfm.check("cfm_fpcg_set_truncation", cfm.lib.cfm_fpcg_set_truncation(fp.h, 9))
+
+
+def test_coarse_network_grid_must_match(coarse_trained):
+    net, _ = coarse_trained
+    k, _ = cfm.varcoef_problem((NC // 2, NC // 2), 1)
+    with pytest.raises(cfm.CfmError):
+        cfm.FPCG(cfm.Stencil(k), k, net)  # a factor-2 net needs the 2x grid
