@@ -148,18 +148,19 @@ def workload_varcoef512(args, cfm):
     # (256^2), trained here on plain-CG pairs of 100 fresh 512^2 systems
     net = cfm.UNet(N // 2, N // 2, max_batch=8, seed=7)
     info = net.train_varcoef(100, 19, 1000, 16, 8, 1e-3, smooth=4, coarsen=2)
-    for m in (8, 4):
-        fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, truncation=m)
+    for m, per in ((8, 2), (8, 1), (4, 1)):
+        fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, truncation=m, net_period=per)
         t, st = timed(lambda: fl.solve(f))
-        out[f"fpcg_learned_m{m}"] = {"ms": t * 1e3, "iterations": st.iterations, "true_relres": st.residual,
-                                     "fallback": st.refinements, "truncation": m}
-    out["fpcg_learned_m8"].update({"training": info, "training_pairs": 100 * 20,
-                                   "network_grid": [N // 2, N // 2], "forward_ms_b1": net.time_forward(1, 20)})
+        out[f"fpcg_learned_m{m}_p{per}"] = {"ms": t * 1e3, "iterations": st.iterations,
+                                            "true_relres": st.residual, "fallback": st.refinements,
+                                            "truncation": m, "network_every": per}
+    head = out["fpcg_learned_m8_p2"]  # the defaults with a network
+    head.update({"training": info, "training_pairs": 100 * 20, "network_grid": [N // 2, N // 2],
+                 "forward_ms_b1": net.time_forward(1, 20)})
     base = out["plain_fp64_persistent_cg"]["ms"]
-    head = out["fpcg_learned_m8"]
     line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual, learned FPCG", head["ms"],
          "ms", args, head["ms"],
-         {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_m8",
+         {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_m8_p2",
           "speedup_vs_plain_persistent_cg": base / head["ms"],
           "speedup_jacobi_only_vs_plain": base / out["fpcg_jacobi4"]["ms"], "solvers": out,
           "precision": "FP64 Krylov recurrences and dots, FP32 smoothing, BF16 network (FP32 accumulate)",

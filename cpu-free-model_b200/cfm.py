@@ -76,6 +76,7 @@ _SIGS = {
     "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_destroy": (None, [_vp]),
     "cfm_fpcg_set_truncation": (_c.c_int, [_vp, _c.c_int]),
+    "cfm_fpcg_set_network_period": (_c.c_int, [_vp, _c.c_int]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
     "cfm_batch_create": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -530,7 +531,7 @@ class UNet:
 class FPCG:
     """Flexible PCG with the network as preconditioner (cfm_fpcg)."""
 
-    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None):
+    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None, net_period=None):
         self.S, self.net = S, net
         self.k = np.ascontiguousarray(k, np.float64)
         h = ctypes.c_void_p()
@@ -542,6 +543,8 @@ class FPCG:
         self.h = h
         if truncation is not None:
             check("cfm_fpcg_set_truncation", lib.cfm_fpcg_set_truncation(self.h, truncation))
+        if net_period is not None:
+            check("cfm_fpcg_set_network_period", lib.cfm_fpcg_set_network_period(self.h, net_period))
 
     def close(self):
         if self.h:

@@ -528,7 +528,8 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a) {
         const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
         t.z0()[row * t.R + col] =
             fp_inside(t, a, row, col, &i)
-                ? (float)(a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)])
+                ? (float)(c != 0.0 ? a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)]
+                                   : a.za[i])
                 : 0.f;
     }
     __syncthreads();
@@ -728,6 +729,7 @@ struct cfm_fpcg {
     double tol = 0;
     double *vec = nullptr;   // x r z b t d za r1 (FP_NVEC n)
     int m = 0;               // FCG truncation
+    int net_every = 1;       // the network in one of every net_every iterations
     float *wd32 = nullptr;   // omega / dg (FP32)
     double *ring = nullptr;  // p and A p ring slots: 2 (m + 1) n
     int smooth = 0;
@@ -792,10 +794,19 @@ FpArgs fp_args(cfm_fpcg *h) {
 // rms(r1), log k) (or the identity), k_fp_ydots (<P y, r1>, <P y, A P y>),
 // k_fp_post (z = `smooth` sweeps from z0 + c P y, <z, r>, <z, r_old>) and
 // k_fp_dir (beta, p, the loop condition).
-int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, int tick) {
+int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, int tick,
+                   bool use_net = true) {
     cudaStream_t s = h->stream;
     CFM_CUDA_TRY(launch_pdl(k_fp_pre, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(std::max(h->smooth, 1)), s,
                             a, tick));
+    if (h->net && !use_net) {
+        // smoothing alone this iteration: no <y, .> partials, so c = 0
+        CFM_CUDA_TRY(cudaMemsetAsync(a.part + (size_t)FP_YR * a.pstride, 0, sizeof(double) * a.ntiles, s));
+        CFM_CUDA_TRY(cudaMemsetAsync(a.part + (size_t)FP_YAY * a.pstride, 0, sizeof(double) * a.ntiles, s));
+        CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a));
+        CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
+        return CFM_OK;
+    }
     if (h->net) {
         const UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride, h->ntiles2, (double)h->n};
         int st = unet_forward(h->net->u, 1, h->xin, h->out, s, &sc);
@@ -809,10 +820,21 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
     return CFM_OK;
 }
 
-int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+int fp_iteration(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, bool use_net) {
     CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
     CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-    return fp_precond_dir(h, a, cond, set_cond, 1);
+    return fp_precond_dir(h, a, cond, set_cond, 1, use_net);
+}
+
+// One pass of the device loop: h->net_every iterations, the network in the
+// first (a converged system may take up to net_every - 1 extra iterations,
+// which only lower its residual further).
+int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    for (int j = 0; j < h->net_every; ++j) {
+        const int st = fp_iteration(h, a, cond, set_cond && j == h->net_every - 1, j == 0);
+        if (st) return st;
+    }
+    return CFM_OK;
 }
 
 // Graph: a conditional WHILE node whose body is one FPCG iteration.
@@ -901,6 +923,7 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     // a linear SPD preconditioner (Jacobi alone) needs no more than the
     // one-term recurrence; the network's nonlinear one gains from a deeper one
     h->m = net ? FP_MAX_TRUNC : 1;
+    h->net_every = net ? 2 : 1;  // network every other iteration (smoothing alone in between)
     if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->ring, sizeof(double) * 2 * (h->m + 1) * n)) != cudaSuccess ||
         (e = cudaMalloc(&h->wd32, sizeof(float) * n)) != cudaSuccess ||
@@ -970,6 +993,21 @@ int cfm_fpcg_set_truncation(cfm_fpcg *h, int m) {
     h->ring = ring;
     h->m = m;
     // the captured iteration graph holds the old ring: build it again
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->exec = nullptr;
+    h->graph = nullptr;
+    h->conditional = false;
+    return CFM_OK;
+}
+
+int cfm_fpcg_set_network_period(cfm_fpcg *h, int every) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(every >= 1 && every <= 8, "period must be in [1, 8]");
+    if (every == h->net_every) return CFM_OK;
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->net_every = every;
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     h->exec = nullptr;

@@ -362,6 +362,9 @@ void cfm_fpcg_destroy(cfm_fpcg *h);
 /* Truncation m in [1, 8] of the orthogonalisation (default 8 with a
  * network, 1 without); m = 1 is the Polak-Ribiere-like one-term recurrence. */
 int cfm_fpcg_set_truncation(cfm_fpcg *h, int m);
+/* Apply the network in one of every `every` iterations (1..8; default 2
+ * with a network); the others use the smoothing alone (c = 0). */
+int cfm_fpcg_set_network_period(cfm_fpcg *h, int every);
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
 /* Recursive residual norms |r_k| of the last solve, one per iteration from
  * k = 0 (at most max_n; *n_out = the count).  net == NULL in
