@@ -68,6 +68,7 @@ _SIGS = {
     "cfm_unet_get_params": (_c.c_int, [_vp, _vp]),
     "cfm_unet_set_params": (_c.c_int, [_vp, _vp]),
     "cfm_unet_forward_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
+    "cfm_unet_set_training_info": (_c.c_int, [_vp, _c.c_int, _c.c_int]),
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
@@ -514,6 +515,11 @@ class UNet:
               lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth, coarsen,
                                          *[ctypes.byref(x) for x in v]))
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
+
+    def set_training_info(self, smooth, coarsen=1):
+        """What a network restored with set_params was trained for."""
+        check("cfm_unet_set_training_info", lib.cfm_unet_set_training_info(self.h, smooth, coarsen))
+        self.smooth, self.coarsen = smooth, coarsen
 
     def time_forward(self, B=1, iters=20):
         ms = ctypes.c_double()

@@ -755,6 +755,16 @@ int cfm_unet_set_params(cfm_unet *h, const float *theta) {
     return CFM_OK;
 }
 
+int cfm_unet_set_training_info(cfm_unet *h, int smooth, int coarsen) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= 8, "smooth must be in [0, 8]");
+    CFM_ARG_CHECK(coarsen == 1 || coarsen == 2, "coarsen must be 1 or 2");
+    h->smooth = smooth;
+    h->coarsen = coarsen;
+    return CFM_OK;
+}
+
 int cfm_unet_forward_host(cfm_unet *h, int B, const float *in, float *out) {
     clear_error();
     CFM_ARG_CHECK(h && in && out, "null argument");

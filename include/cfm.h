@@ -307,6 +307,10 @@ int cfm_unet_create(int H, int W, int max_batch, unsigned long long seed, cfm_un
 void cfm_unet_destroy(cfm_unet *net);
 int cfm_unet_get_params(cfm_unet *net, float *theta);
 int cfm_unet_set_params(cfm_unet *net, const float *theta);
+/* Records what a network restored with cfm_unet_set_params was trained for
+ * (smoothing sweeps 0..8, coarsening 1 or 2), as cfm_unet_train_varcoef
+ * does, so that cfm_fpcg_create accepts it. */
+int cfm_unet_set_training_info(cfm_unet *net, int smooth, int coarsen);
 /* One forward pass on host buffers. */
 int cfm_unet_forward_host(cfm_unet *net, int B, const float *in, float *out);
 /* Forward, then the gradient of sum(out * dout) with respect to the

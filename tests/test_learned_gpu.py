@@ -117,3 +117,19 @@ def test_coarse_network_grid_must_match(coarse_trained):
     k, _ = cfm.varcoef_problem((NC // 2, NC // 2), 1)
     with pytest.raises(cfm.CfmError):
         cfm.FPCG(cfm.Stencil(k), k, net)  # a factor-2 net needs the 2x grid
+
+
+def test_restored_network_needs_training_info(coarse_trained):
+    """Parameters saved from one net and restored into another give the same
+    solve once the restored net is told what it was trained for."""
+    net, _ = coarse_trained
+    k, f = cfm.varcoef_problem((NC, NC), 80)
+    S = cfm.Stencil(k)
+    twin = cfm.UNet(NC // 2, NC // 2, max_batch=1, seed=99)
+    twin.set_params(net.params())
+    with pytest.raises(cfm.CfmError):
+        cfm.FPCG(S, k, twin)  # not yet told its smoothing and coarsening
+    twin.set_training_info(SMOOTH, 2)
+    _, st_a = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8).solve(f)
+    _, st_b = cfm.FPCG(S, k, twin, maxiter=20000, tol=1e-8).solve(f)
+    assert st_b.status == cfm.OK and st_b.iterations == st_a.iterations
