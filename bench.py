@@ -375,7 +375,7 @@ def main():
     stream = torch.cuda.Stream()
     j.set_stream(stream.cuda_stream)
     j.load_problem(cfm.PROBLEM_CONFIG)
-    best, _ = j.autotune(20)  # pipeline shape and z-chunk; restores the grid
+    best, _ = j.autotune(40)  # pipeline shape and z-chunk; restores the grid
     tuned = cfm.variant_info(best) if best >= 0 else None
     blocks, threads = j.launch_shape()
     for _ in range(args.warmup):

@@ -41,6 +41,7 @@ _SIGS = {
     "cfm_jacobi_launch_shape": (_c.c_int, [_vp, _vp, _vp]),
     "cfm_jacobi_autotune": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_jacobi_variant_info": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
+    "cfm_jacobi_variant_sweeps": (_c.c_int, [_c.c_int]),
     "cfm_csr_create": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp]),
     "cfm_csr_destroy": (None, [_vp]),
     "cfm_csr_spmv_host": (_c.c_int, [_vp, _vp, _vp]),
@@ -179,7 +180,7 @@ class Jacobi:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_jacobi_destroy(self.h)
             self.h = None
 
@@ -241,9 +242,10 @@ class Jacobi:
 
 
 def variant_info(i):
+    """(consumer warps, rows per warp, stages, sweeps per pass) of pipeline shape i, or None."""
     cw, rpw, st = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     s = lib.cfm_jacobi_variant_info(i, ctypes.byref(cw), ctypes.byref(rpw), ctypes.byref(st))
-    return None if s != OK else (cw.value, rpw.value, st.value)
+    return None if s != OK else (cw.value, rpw.value, st.value, lib.cfm_jacobi_variant_sweeps(i))
 
 
 class CSR:
@@ -258,7 +260,7 @@ class CSR:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_csr_destroy(self.h)
             self.h = None
 
@@ -287,7 +289,7 @@ class Stencil:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_stencil_destroy(self.h)
             self.h = None
 
@@ -312,7 +314,7 @@ class CG:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_cg_destroy(self.h)
             self.h = None
 
@@ -470,7 +472,7 @@ class UNet:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_unet_destroy(self.h)
             self.h = None
 
@@ -553,7 +555,7 @@ class FPCG:
             check("cfm_fpcg_set_network_period", lib.cfm_fpcg_set_network_period(self.h, net_period))
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_fpcg_destroy(self.h)
             self.h = None
 
@@ -600,7 +602,7 @@ class Batch:
         self.h = h
 
     def close(self):
-        if self.h:
+        if getattr(self, "h", None):
             lib.cfm_batch_destroy(self.h)
             self.h = None
 

@@ -27,6 +27,7 @@
 #include "barrier.cuh"
 #include "cfm_internal.h"
 #include "j3d_tma.cuh"
+#include "j3d_tma2.cuh"
 #include "tma.cuh"
 
 namespace cfm {
@@ -362,6 +363,19 @@ __global__ void load_problem_kernel(T *a, int dims, int nx, int ny, int nz, int 
 
 using namespace cfm;
 
+namespace cfm {
+// One configuration of the 3D TMA pipeline: tensor maps over both grids
+// (main boxes and, for two sweeps per pass, the 3-row far-row boxes), the
+// kernel and its launch shape.
+struct TmaConfig {
+    bool ok = false;
+    CUtensorMap map[2], xmap[2];
+    const void *fn = nullptr;
+    int var = 0, sweeps = 1, blocks = 0, zchunk = 0, threads = 0;
+    size_t smem = 0;
+};
+}  // namespace cfm
+
 struct cfm_jacobi {
     cfm_jacobi_params p;
     size_t elems = 0, esize = 0;
@@ -379,12 +393,10 @@ struct cfm_jacobi {
     int res_blocks = 0;
     size_t res_smem = 0;
     bool resident = false;
-    // 3D TMA pipeline: tensor maps of the two grids, shape
+    // 3D TMA pipeline: the chosen shape, and (for a two-sweep shape) the
+    // one-sweep shape that does the last sweep of an odd count
     bool tma = false;
-    CUtensorMap tmap[2];
-    int tma_blocks = 0, tma_zchunk = 0, tma_var = 0;
-    const void *tma_fn = nullptr;
-    size_t tma_smem = 0;
+    cfm::TmaConfig tc, tail;
     size_t smem_optin = 0;
 };
 
@@ -424,6 +436,7 @@ constexpr int J3_TY = 8;
 // CFM_J3D_TMA_VARIANT (an index into this table) overrides the choice.
 struct TmaVariant {
     int cw, rpw, stages;
+    int sweeps;            // sweeps per pass over the grid (2: j3d_tma2_kernel)
     const void *fn[2][2];  // [precision][periodic_y]
     size_t smem[2];        // [precision]
     int tx[2];             // [precision]
@@ -431,7 +444,7 @@ struct TmaVariant {
 
 template <int CW, int RPW, int S>
 TmaVariant make_tma_variant() {
-    TmaVariant v{CW, RPW, S, {}, {}, {}};
+    TmaVariant v{CW, RPW, S, 1, {}, {}, {}};
     v.fn[CFM_FP64][0] = (const void *)j3d_tma_kernel<double, CW, RPW, S, false>;
     v.fn[CFM_FP64][1] = (const void *)j3d_tma_kernel<double, CW, RPW, S, true>;
     v.fn[CFM_FP32][0] = (const void *)j3d_tma_kernel<float, CW, RPW, S, false>;
@@ -443,12 +456,29 @@ TmaVariant make_tma_variant() {
     return v;
 }
 
+template <int CW, int RPW, int S>
+TmaVariant make_tma2_variant() {
+    TmaVariant v{CW, RPW, S, 2, {}, {}, {}};
+    v.fn[CFM_FP64][0] = (const void *)j3d_tma2_kernel<double, CW, RPW, S, false>;
+    v.fn[CFM_FP64][1] = (const void *)j3d_tma2_kernel<double, CW, RPW, S, true>;
+    v.fn[CFM_FP32][0] = (const void *)j3d_tma2_kernel<float, CW, RPW, S, false>;
+    v.fn[CFM_FP32][1] = (const void *)j3d_tma2_kernel<float, CW, RPW, S, true>;
+    v.smem[CFM_FP64] = Tma2Geom<double, CW, RPW, S>::SMEM;
+    v.smem[CFM_FP32] = Tma2Geom<float, CW, RPW, S>::SMEM;
+    v.tx[CFM_FP64] = Tma2Geom<double, CW, RPW, S>::TX;
+    v.tx[CFM_FP32] = Tma2Geom<float, CW, RPW, S>::TX;
+    return v;
+}
+
+// Variants 0-11 take one sweep per pass, 12-15 two (temporal blocking).
 const TmaVariant *tma_variants(int *count) {
     static const TmaVariant v[] = {
         make_tma_variant<8, 2, 6>(), make_tma_variant<4, 2, 8>(),  make_tma_variant<4, 4, 6>(),
         make_tma_variant<8, 1, 8>(), make_tma_variant<4, 2, 12>(), make_tma_variant<2, 4, 8>(),
         make_tma_variant<8, 4, 4>(), make_tma_variant<16, 2, 4>(),  make_tma_variant<16, 2, 6>(),
         make_tma_variant<16, 2, 8>(), make_tma_variant<8, 4, 8>(),  make_tma_variant<16, 4, 4>(),
+        make_tma2_variant<16, 2, 4>(), make_tma2_variant<16, 2, 6>(), make_tma2_variant<8, 4, 5>(),
+        make_tma2_variant<8, 2, 4>(),
     };
     *count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -460,13 +490,14 @@ const TmaVariant &tma_variant(int i) {
     return v[(i >= 0 && i < n) ? i : 0];
 }
 
-int tma_threads(int var) { return 32 * (tma_variant(var).cw + 1); }
 
-// Tensor maps over both grids: dims (nx, ny, nz), box (TX + 2 VN, TY + 2, 1),
-// zero fill outside.  Needs the row pitch nx * esize to be a multiple of 16.
-int setup_tma(cfm_jacobi *h, int var, int zchunk = 0) {
+// Tensor maps over both grids: dims (nx, ny, nz), box (TX + 2 VN, TY + 2, 1)
+// for one sweep per pass, (TX + 2 VN, TY + 4, 1) plus the 3-row far-row box
+// for two; zero fill outside.  Needs the row pitch nx * esize to be a
+// multiple of 16.  Leaves c->ok false when the pipeline does not apply.
+int build_tma(cfm_jacobi *h, int var, int zchunk, TmaConfig *c) {
     const cfm_jacobi_params &p = h->p;
-    h->tma = false;
+    c->ok = false;
     if (p.dims != 3 || ((size_t)p.nx * h->esize) % 16 != 0) return CFM_OK;
     auto enc = tensor_map_encoder();
     if (!enc) return CFM_OK;
@@ -475,38 +506,66 @@ int setup_tma(cfm_jacobi *h, int var, int zchunk = 0) {
     const int vn = (int)(16 / h->esize);
     const cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
     const cuuint64_t strides[2] = {(cuuint64_t)p.nx * h->esize, (cuuint64_t)p.nx * p.ny * h->esize};
-    const cuuint32_t box[3] = {(cuuint32_t)(tx + 2 * vn), (cuuint32_t)(ty + 2), 1u};
+    const cuuint32_t box[3] = {(cuuint32_t)(tx + 2 * vn), (cuuint32_t)(ty + (V.sweeps == 2 ? 4 : 2)), 1u};
+    const cuuint32_t xbox[3] = {(cuuint32_t)(tx + 2 * vn), 3u, 1u};
     const cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapDataType dt =
+        p.precision == CFM_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     for (int i = 0; i < 2; ++i) {
-        CUresult r = enc(&h->tmap[i],
-                         p.precision == CFM_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
-                                                 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                         3, h->buf[i], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CUresult r = enc(&c->map[i], dt, 3, h->buf[i], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r == CUDA_SUCCESS && V.sweeps == 2)
+            r = enc(&c->xmap[i], dt, 3, h->buf[i], dims, strides, xbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return CFM_OK;  // stay on the register kernel
     }
     const void *fn = V.fn[p.precision][p.periodic_y ? 1 : 0];
     const size_t smem = V.smem[p.precision];
     if (smem > h->smem_optin) return CFM_OK;
+    const int threads = 32 * (V.cw + 1);
     CFM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // all of the SM's shared memory for the ring (two rings per SM when they fit)
+    CFM_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
     int per_sm = 0;
-    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, tma_threads(var), smem));
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
     if (per_sm < 1) return CFM_OK;
-    h->tma_blocks = per_sm * h->num_sms;
+    c->blocks = per_sm * h->num_sms;
     const long long ntiles = (long long)((p.nx + tx - 1) / tx) * ((p.ny - 2 + ty - 1) / ty);
     if (zchunk <= 0)
         if (const char *zc = std::getenv("CFM_J3D_ZCHUNK")) zchunk = std::atoi(zc);
     if (zchunk >= 1) {
-        h->tma_zchunk = std::min(zchunk, p.nz - 2);
-        const long long U = units_of(ntiles, p.nz - 2, h->tma_zchunk);
-        if (U < h->tma_blocks) h->tma_blocks = (int)std::max(1LL, U);
+        c->zchunk = std::min(zchunk, p.nz - 2);
+        const long long U = units_of(ntiles, p.nz - 2, c->zchunk);
+        if (U < c->blocks) c->blocks = (int)std::max(1LL, U);
     } else {
-        h->tma_zchunk = pick_zchunk(ntiles, p.nz - 2, &h->tma_blocks);
+        c->zchunk = pick_zchunk(ntiles, p.nz - 2, &c->blocks);
     }
-    h->tma_var = var;
-    h->tma_fn = fn;
-    h->tma_smem = smem;
+    c->var = var;
+    c->sweeps = V.sweeps;
+    c->threads = threads;
+    c->fn = fn;
+    c->smem = smem;
+    c->ok = true;
+    return CFM_OK;
+}
+
+int default_tma_variant();
+
+// The pipeline shape `var` (and, for two sweeps per pass, the default
+// one-sweep shape for the last sweep of an odd count).
+int setup_tma(cfm_jacobi *h, int var, int zchunk = 0) {
+    h->tma = false;
+    int st = build_tma(h, var, zchunk, &h->tc);
+    if (st || !h->tc.ok) return st;
+    if (h->tc.sweeps == 2) {
+        int dv = default_tma_variant();
+        if (tma_variant(dv).sweeps != 1) dv = 0;
+        if ((st = build_tma(h, dv, 0, &h->tail))) return st;
+        if (!h->tail.ok) return CFM_OK;
+    }
     h->tma = true;
     return CFM_OK;
 }
@@ -735,20 +794,34 @@ int resident2d(cfm_jacobi *h, int niter, int *launches) {
     return CFM_OK;
 }
 
-int persistent_tma(cfm_jacobi *h, int niter, int *launches) {
+int launch_tma(cfm_jacobi *h, const TmaConfig &c, int count, int *launches) {
     const cfm_jacobi_params &p = h->p;
-    // tm0 / g0 is the grid read by the first sweep
-    const int c = h->cur;
-    const CUtensorMap *m0 = &h->tmap[c], *m1 = &h->tmap[c ^ 1];
-    void *g0 = h->buf[c], *g1 = h->buf[c ^ 1];
-    int n = niter;
-    void *args[] = {(void *)m0, (void *)m1, &g0, &g1, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz,
-                    &n, &h->tma_zchunk, &h->bar};
-    CFM_CUDA_TRY(launch_cooperative(h->tma_fn, dim3(h->tma_blocks), dim3(tma_threads(h->tma_var)),
-                                    args, h->tma_smem, h->stream));
-    h->cur ^= (niter & 1);
+    // map[cur] / g0 is the grid read by the first pass
+    const int cu = h->cur;
+    void *g0 = h->buf[cu], *g1 = h->buf[cu ^ 1];
+    int n = count, zc = c.zchunk;
+    if (c.sweeps == 2) {
+        void *args[] = {(void *)&c.map[cu], (void *)&c.map[cu ^ 1], (void *)&c.xmap[cu], (void *)&c.xmap[cu ^ 1],
+                        &g0, &g1, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &n, &zc, &h->bar};
+        CFM_CUDA_TRY(launch_cooperative(c.fn, dim3(c.blocks), dim3(c.threads), args, c.smem, h->stream));
+    } else {
+        void *args[] = {(void *)&c.map[cu], (void *)&c.map[cu ^ 1], &g0, &g1, (void *)&p.nx, (void *)&p.ny,
+                        (void *)&p.nz, &n, &zc, &h->bar};
+        CFM_CUDA_TRY(launch_cooperative(c.fn, dim3(c.blocks), dim3(c.threads), args, c.smem, h->stream));
+    }
+    h->cur ^= (count & 1);
     ++*launches;
     return CFM_OK;
+}
+
+// niter sweeps: one launch, or for two sweeps per pass niter / 2 passes and,
+// for an odd count, one more launch of the one-sweep shape.
+int persistent_tma(cfm_jacobi *h, int niter, int *launches) {
+    if (h->tc.sweeps == 1) return launch_tma(h, h->tc, niter, launches);
+    int st = CFM_OK;
+    if (niter / 2 > 0 && (st = launch_tma(h, h->tc, niter / 2, launches))) return st;
+    if (niter & 1) st = launch_tma(h, h->tail, 1, launches);
+    return st;
 }
 
 int persistent(cfm_jacobi *h, int niter, int *launches) {
@@ -1038,6 +1111,13 @@ int cfm_jacobi_variant_info(int index, int *consumer_warps, int *rows_per_warp, 
     return CFM_OK;
 }
 
+int cfm_jacobi_variant_sweeps(int index) {
+    int n = 0;
+    const TmaVariant *v = tma_variants(&n);
+    if (index < 0 || index >= n) return CFM_BAD_ARG;
+    return v[index].sweeps;
+}
+
 int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *best_glups) {
     CFM_ARG_CHECK(h, "handle is null");
     CFM_ARG_CHECK(sweeps >= 1, "sweeps must be >= 1");
@@ -1060,20 +1140,27 @@ int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *be
     int n = 0, best = -1, best_zc = 0;
     double best_rate = 0.0;
     tma_variants(&n);
-    const int zcands[] = {0, 16, 32, 64, 128};  // 0: the cost-model choice
+    const int zcands[] = {0, 16, 24, 32, 48, 64, 128};  // 0: the cost-model choice
     for (int v = 0; v < n && e == cudaSuccess && st == CFM_OK; ++v) {
         for (int zc : zcands) {
             if ((st = setup_tma(h, v, zc)) || !h->tma) {
                 st = CFM_OK;
                 break;
             }
-            if ((st = restore())) break;
-            cfm_stats s{};
-            if ((st = cfm_jacobi_run(h, sweeps, &s))) break;
-            if (s.glups > best_rate) {
-                best_rate = s.glups;
+            // a warm-up run, then the better of two timed runs (single short
+            // runs were noisy enough to miss the best z-chunk)
+            double rate = 0.0;
+            for (int rep = 0; rep < 3 && st == CFM_OK; ++rep) {
+                if ((st = restore())) break;
+                cfm_stats s{};
+                if ((st = cfm_jacobi_run(h, sweeps, &s))) break;
+                if (rep > 0) rate = std::max(rate, s.glups);
+            }
+            if (st) break;
+            if (rate > best_rate) {
+                best_rate = rate;
                 best = v;
-                best_zc = h->tma_zchunk;
+                best_zc = h->tc.zchunk;
             }
         }
     }
@@ -1097,8 +1184,8 @@ int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads) {
         b = h->res_blocks;
         t = 1024;
     } else if (h->tma) {
-        b = h->tma_blocks;
-        t = tma_threads(h->tma_var);
+        b = h->tc.blocks;
+        t = h->tc.threads;
     }
     if (blocks) *blocks = b;
     if (threads) *threads = t;

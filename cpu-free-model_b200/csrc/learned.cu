@@ -65,20 +65,17 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
     *reinterpret_cast<uint4 *>(p) = u;
 }
 
-// h0 = relu(cin(x)) and p1 = pool(h0): x FP32 [B][H][W][2], w [9][32][2].
-// A warp computes one 2 x 2 pixel quad: lane = 8 * quad pixel + channel
-// group, quad pixels in the order (0,0) (1,0) (0,1) (1,1), each lane 4
-// channels with its 72 weights and 4 biases held in registers across the
-// quads it visits.  The 9 input loads of a pixel are issued together from
-// clamped coordinates and zeroed outside the image.  The pool averages the
-// BF16-rounded h0 values as ((a + b) + c) + d, gathered by shuffles.
-// Input channel 0 is optionally scaled by 1 / rms from a solver's partials.
-// grid: (ceil((W / 2) / (8 CIN_PASSES)), H / 2, B), 256 threads.
-constexpr int CIN_PASSES = 4;
-__global__ void __launch_bounds__(256) k_cin_pool_fwd(const float *x, const float *w, const float *b,
-                                                      bf16 *h0, bf16 *p1, int H, int W,
-                                                      UNetInputScale in_scale) {
+// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Eight threads per
+// pixel, each producing 4 channels (one 8-byte store; a warp writes 4 whole
+// pixels) with its 72 weights and 4 biases held in registers across
+// CIN_PASSES pixels.  The 9 input loads of a pixel are issued together from
+// clamped coordinates and zeroed outside the image.
+// grid: (ceil(W / (32 CIN_PASSES)), H, B), 256 threads.
+constexpr int CIN_PASSES = 8;
+__global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w, const float *b,
+                                                 bf16 *h0, int H, int W, UNetInputScale in_scale) {
     pdl_enter();
+    // input channel 0 scale: 1 / rms from a solver's partial sums (fixed order)
     float sc = 1.f;
     if (in_scale.part) {
         __shared__ double red[8];
@@ -91,8 +88,7 @@ __global__ void __launch_bounds__(256) k_cin_pool_fwd(const float *x, const floa
         for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) tot += red[wi];
         sc = tot > 0 ? (float)sqrt(in_scale.cells / tot) : 0.f;
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int q = lane & 7, c0 = q * 4, qp = lane >> 3;
+    const int q = threadIdx.x & 7, c0 = q * 4;
     float wr[9][8];  // [t][(c - c0) * 2 + in]
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
@@ -102,14 +98,13 @@ __global__ void __launch_bounds__(256) k_cin_pool_fwd(const float *x, const floa
         wr[t][4] = w1.x, wr[t][5] = w1.y, wr[t][6] = w1.z, wr[t][7] = w1.w;
     }
     const float4 bq = *reinterpret_cast<const float4 *>(b + c0);
-    const int yp = blockIdx.y, img = blockIdx.z, Wp = W / 2, Hp = H / 2;
-    const int yy = 2 * yp + (qp >> 1);
+    const int yy = blockIdx.y, img = blockIdx.z;
     const float *xi = x + (size_t)img * H * W * 2;
+    bf16 *hrow = h0 + ((size_t)img * H + yy) * W * 32;
 #pragma unroll 1
     for (int pass = 0; pass < CIN_PASSES; ++pass) {
-        const int xp = (blockIdx.x * CIN_PASSES + pass) * 8 + warp;
-        if (xp >= Wp) break;  // warp-uniform
-        const int xx = 2 * xp + (qp & 1);
+        const int xx = (blockIdx.x * CIN_PASSES + pass) * 32 + (threadIdx.x >> 3);
+        if (xx >= W) break;
         float2 v[9];
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
@@ -128,27 +123,7 @@ __global__ void __launch_bounds__(256) k_cin_pool_fwd(const float *x, const floa
         __nv_bfloat162 r[2];
         r[0] = __floats2bfloat162_rn(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f));
         r[1] = __floats2bfloat162_rn(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f));
-        *reinterpret_cast<uint2 *>(h0 + (((size_t)img * H + yy) * W + xx) * 32 + c0) =
-            *reinterpret_cast<const uint2 *>(r);
-        // pool: the four quad pixels' rounded values of these channels
-        float hv[4], pa[4];
-        hv[0] = __low2float(r[0]), hv[1] = __high2float(r[0]);
-        hv[2] = __low2float(r[1]), hv[3] = __high2float(r[1]);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const float a0 = __shfl_sync(0xffffffffu, hv[c], q);
-            const float a1 = __shfl_sync(0xffffffffu, hv[c], q + 8);
-            const float a2 = __shfl_sync(0xffffffffu, hv[c], q + 16);
-            const float a3 = __shfl_sync(0xffffffffu, hv[c], q + 24);
-            pa[c] = 0.25f * (((a0 + a1) + a2) + a3);
-        }
-        if (qp == 0) {
-            __nv_bfloat162 pr[2];
-            pr[0] = __floats2bfloat162_rn(pa[0], pa[1]);
-            pr[1] = __floats2bfloat162_rn(pa[2], pa[3]);
-            *reinterpret_cast<uint2 *>(p1 + (((size_t)img * Hp + yp) * Wp + xp) * 32 + c0) =
-                *reinterpret_cast<const uint2 *>(pr);
-        }
+        *reinterpret_cast<uint2 *>(hrow + (size_t)xx * 32 + c0) = *reinterpret_cast<const uint2 *>(r);
     }
 }
 
@@ -295,6 +270,26 @@ __global__ void k_pool(const bf16 *in, bf16 *out, int h, int w) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) o[j] = 0.25f * (((a[j] + b[j]) + c[j]) + d[j]);
     store8(out + (((size_t)img * h + y) * w + x) * C + c8, o);
+}
+
+// u = up(g) + skip at the finer level (2h x 2w; (h, w) is the coarse size).
+// grid: (items of a fine row / blockDim, 2h, B).
+template <int C>
+__global__ void k_up_add(const bf16 *g, const bf16 *skip, bf16 *u, int h, int w) {
+    pdl_enter();
+    constexpr int G = C / 8;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 2 * w * G) return;
+    const int y = blockIdx.y, img = blockIdx.z;
+    const int c8 = (e % G) * 8, x = e / G;
+    const size_t cp = ((size_t)img * h + y / 2) * w + x / 2;
+    const size_t pix = ((size_t)img * 2 * h + y) * 2 * w + x;
+    float a[8], b[8];
+    load8(g + cp * C + c8, a);
+    load8(skip + pix * C + c8, b);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] += b[j];
+    store8(u + pix * C + c8, a);
 }
 
 // dz[coarse] = (sum of the 2x2 fine gradients) * (act[coarse] > 0).
@@ -526,14 +521,11 @@ int unet_refresh_weights(UNetImpl *u, cudaStream_t s) {
 
 namespace {
 
-int conv_fwd(UNetImpl *u, int l, const bf16 *x, bf16 *out, int B, int h, int w, cudaStream_t s,
-             const bf16 *up_skip = nullptr, bf16 *up_out = nullptr) {
+int conv_fwd(UNetImpl *u, int l, const bf16 *x, bf16 *out, int B, int h, int w, cudaStream_t s) {
     const UNetLayer &L = UNET_LAYERS[l];
     ConvArgs c{x, u->wb[l], u->theta + u->boff[l], nullptr, out, u->err, B, h, w, L.ci, L.co, 1};
     c.ws = u->ws;
     c.ws_floats = TC_WS_FLOATS;
-    c.up_skip = up_skip;
-    c.up_out = up_out;
     return tc_conv_fwd(c, s);
 }
 
@@ -574,11 +566,14 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
     UNetBuffers &a = u->a;
     const int H = u->H, W = u->W;
     int st;
-    CFM_CUDA_TRY(launch_pdl(k_cin_pool_fwd, dim3((W / 2 + 8 * CIN_PASSES - 1) / (8 * CIN_PASSES), H / 2, B),
-                            dim3(256), 0, s, x, (const float *)(u->theta + u->woff[0]),
-                            (const float *)(u->theta + u->boff[0]), a.h0, a.p1, H, W,
+    CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + 32 * CIN_PASSES - 1) / (32 * CIN_PASSES), H, B), dim3(256),
+                            0, s, x, (const float *)(u->theta + u->woff[0]),
+                            (const float *)(u->theta + u->boff[0]), a.h0, H, W,
                             in_scale ? *in_scale : UNetInputScale{nullptr, 0, 0.0}));
-    int h = H / 2, w = W / 2;
+    int h = H, w = W;
+    CFM_CUDA_TRY(launch_pdl(k_pool<32>, row_grid(w / 2 * 4, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h0,
+                            a.p1, h / 2, w / 2));
+    h /= 2, w /= 2;
     if ((st = conv_fwd(u, 1, a.p1, a.h1, B, h, w, s))) return st;
     CFM_CUDA_TRY(launch_pdl(k_pool<64>, row_grid(w / 2 * 8, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h1,
                             a.p2, h / 2, w / 2));
@@ -588,12 +583,17 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
                             (const bf16 *)a.h2, a.p3, h / 2, w / 2));
     h /= 2, w /= 2;
     if ((st = conv_fwd(u, 3, a.p3, a.h3, B, h, w, s))) return st;
-    // decoder convolutions write g and, fused, u = up(g) + skip one level up
-    if ((st = conv_fwd(u, 4, a.h3, a.g3, B, h, w, s, a.h2, a.u2))) return st;
+    if ((st = conv_fwd(u, 4, a.h3, a.g3, B, h, w, s))) return st;
+    CFM_CUDA_TRY(launch_pdl(k_up_add<128>, row_grid(2 * w * 16, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g3, (const bf16 *)a.h2, a.u2, h, w));
     h *= 2, w *= 2;
-    if ((st = conv_fwd(u, 5, a.u2, a.g2, B, h, w, s, a.h1, a.u1))) return st;
+    if ((st = conv_fwd(u, 5, a.u2, a.g2, B, h, w, s))) return st;
+    CFM_CUDA_TRY(launch_pdl(k_up_add<64>, row_grid(2 * w * 8, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g2, (const bf16 *)a.h1, a.u1, h, w));
     h *= 2, w *= 2;
-    if ((st = conv_fwd(u, 6, a.u1, a.g1, B, h, w, s, a.h0, a.u0))) return st;
+    if ((st = conv_fwd(u, 6, a.u1, a.g1, B, h, w, s))) return st;
+    CFM_CUDA_TRY(launch_pdl(k_up_add<32>, row_grid(2 * w * 4, 2 * h, B), dim3(256), 0, s,
+                            (const bf16 *)a.g1, (const bf16 *)a.h0, a.u0, h, w));
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 7, a.u0, a.g0, B, h, w, s))) return st;
     CFM_CUDA_TRY(launch_pdl(k_cout_fwd, dim3((W + 64 * COUT_PASSES - 1) / (64 * COUT_PASSES), H, B),

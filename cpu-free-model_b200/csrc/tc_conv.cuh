@@ -160,10 +160,6 @@ struct TcConvParams {
     int relu;
     const __nv_bfloat16 *mask;  // [B][H][W][N]; zero the output where mask <= 0
     __nv_bfloat16 *out;         // [B][H][W][N]
-    // optional fused upsample + skip: up_out[2y + dy][2x + dx] = out[y][x] +
-    // up_skip[2y + dy][2x + dx] ([B][2H][2W][N], the BF16 out value as stored)
-    const __nv_bfloat16 *up_skip;
-    __nv_bfloat16 *up_out;
     float *dw;                  // [9][Cout][Cin]
     int *err;
     unsigned long long budget_ns;
@@ -200,33 +196,6 @@ __device__ __forceinline__ void store16_pairs(__nv_bfloat16 *pix_even, __nv_bflo
     const int half = odd ? 8 : 0;
     if (in_even) *reinterpret_cast<uint4 *>(pix_even + half) = odd ? got : lo;
     if (in_odd) *reinterpret_cast<uint4 *>(pix_odd + half) = odd ? hi : got;
-}
-
-// up_out[f] = bf16(float(v) + float(up_skip[f])) for the 2 x 2 fine pixels f
-// under coarse pixel (x, y, img), channels c .. c + 8 * NV - 1 (v: NV uint4
-// of 8 BF16 each).
-template <int N, int NV>
-__device__ __forceinline__ void tc_up_add(const TcConvParams &p, int img, int y, int x, int c,
-                                          const uint4 *v) {
-    const size_t W2 = 2 * (size_t)p.W;
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        const size_t fp = (((size_t)img * 2 * p.H + 2 * y + (f >> 1)) * W2 + 2 * x + (f & 1)) * N + c;
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            const uint4 sk = *reinterpret_cast<const uint4 *>(p.up_skip + fp + 8 * k);
-            const __nv_bfloat162 *a2 = reinterpret_cast<const __nv_bfloat162 *>(&v[k]);
-            const __nv_bfloat162 *b2 = reinterpret_cast<const __nv_bfloat162 *>(&sk);
-            uint4 o;
-            __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(&o);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float2 fa = __bfloat1622float2(a2[j]), fb = __bfloat1622float2(b2[j]);
-                o2[j] = __floats2bfloat162_rn(fa.x + fb.x, fa.y + fb.y);
-            }
-            *reinterpret_cast<uint4 *>(p.up_out + fp + 8 * k) = o;
-        }
-    }
 }
 
 template <int KC, int N>
@@ -469,7 +438,6 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                 };
                 bool in_me, in_e, in_o;
                 const size_t pix = pixel(row, in_me);
-                const int my_x = tx * p.bx + row % p.bx, my_y = (rest % p.tiles_y) * p.by + row / p.bx;
                 __nv_bfloat16 *oe = p.out + pixel(row & ~1, in_e) * N;
                 __nv_bfloat16 *oo = p.out + pixel(row | 1, in_o) * N;
                 const __nv_bfloat16 *mk = p.mask ? p.mask + pix * N : nullptr;
@@ -512,10 +480,6 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                         h2[j] = __floats2bfloat162_rn(v[8 + 2 * j], v[8 + 2 * j + 1]);
                     }
                     store16_pairs(oe + c, oo + c, in_e, in_o, lane, lo, hi);
-                    if (p.up_out && in_me) {
-                        const uint4 v2[2] = {lo, hi};
-                        tc_up_add<N, 2>(p, img, my_y, my_x, c, v2);
-                    }
                 };
                 if constexpr (N <= 64) {
                     // narrow tile: drain TMEM first and hand the accumulator back
@@ -579,7 +543,7 @@ namespace cfm {
 // split order (deterministic).  One thread per (pixel, 8 channels).
 template <int N>
 __global__ void tc_splitk_epilogue(const float *ws, int csplit, long long npix, const float *bias, int relu,
-                                   const __nv_bfloat16 *mask, __nv_bfloat16 *out, TcConvParams up) {
+                                   const __nv_bfloat16 *mask, __nv_bfloat16 *out) {
     pdl_enter();
     constexpr int G = N / 8;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < npix * G;
@@ -611,10 +575,6 @@ __global__ void tc_splitk_epilogue(const float *ws, int csplit, long long npix, 
             o2[j / 2] = __floats2bfloat162_rn(a, b);
         }
         *reinterpret_cast<uint4 *>(out + pix * N + c) = o;
-        if (up.up_out) {
-            const int x = (int)(pix % up.W), y = (int)((pix / up.W) % up.H), img = (int)(pix / ((long long)up.W * up.H));
-            tc_up_add<N, 1>(up, img, y, x, c, &o);
-        }
     }
 }
 

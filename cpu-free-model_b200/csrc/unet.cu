@@ -122,7 +122,7 @@ int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap 
         const long long items = npix * (N / 8);
         const int blocks = (int)std::min<long long>((items + 255) / 256, (long long)di.num_sms * 8);
         CFM_CUDA_TRY(launch_pdl(tc_splitk_epilogue<N>, dim3(blocks), dim3(256), 0, s, (const float *)p.ws,
-                                p.csplit, npix, p.bias, p.relu, p.mask, p.out, p));
+                                p.csplit, npix, p.bias, p.relu, p.mask, p.out));
     }
     return CFM_OK;
 }
@@ -217,8 +217,6 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     p.err = a.err;
     p.ws = a.ws;
     p.ws_floats = a.ws ? a.ws_floats : 0;
-    p.up_skip = a.up_skip;
-    p.up_out = a.up_out;
     p.csplit = 1;
     p.budget_ns = barrier_timeout_ns();
     CUtensorMap ma, mb;

@@ -22,10 +22,6 @@ struct ConvArgs {
     // SMs then split their K steps over several CTAs
     float *ws = nullptr;
     long long ws_floats = 0;
-    // optional fused 2x upsample + skip add: up_out = up(out) + up_skip on
-    // the (2H) x (2W) grid (both [B][2H][2W][Cout])
-    const __nv_bfloat16 *up_skip = nullptr;
-    __nv_bfloat16 *up_out = nullptr;
 };
 int tc_conv_fwd(const ConvArgs &a, cudaStream_t s);
 // Split-K workspace a net keeps for its convolutions (floats).

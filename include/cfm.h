@@ -151,6 +151,10 @@ int cfm_jacobi_launch_shape(cfm_jacobi *h, int *blocks, int *threads);
 int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *best_glups);
 /* Shape of compiled pipeline variant `index` (CFM_BAD_ARG past the last). */
 int cfm_jacobi_variant_info(int index, int *consumer_warps, int *rows_per_warp, int *stages);
+/* Sweeps per pass over the grid of pipeline shape `index`: 1, or 2 for the
+ * temporally blocked shapes (an odd sweep count ends with one one-sweep
+ * launch); a negative status for an unknown index. */
+int cfm_jacobi_variant_sweeps(int index);
 
 /* ------------------------------------------------------------------- CG */
 typedef enum cfm_cg_impl {

@@ -112,14 +112,42 @@ def test_autotune_restores_grid_and_stays_bitexact():
         assert j.autotune(2)[0] == -1  # nothing to tune outside the 3D TMA pipeline
 
 
-@pytest.mark.parametrize("variant", range(12))
+NVARIANTS = 16  # pipeline shapes: 0-11 one sweep per pass, 12-15 two
+
+
+@pytest.mark.parametrize("variant", range(NVARIANTS))
 def test_every_pipeline_variant_bitexact(variant, monkeypatch):
-    assert cfm.variant_info(variant) is not None and cfm.variant_info(12) is None
+    assert cfm.variant_info(variant) is not None and cfm.variant_info(NVARIANTS) is None
+    assert cfm.variant_info(variant)[3] == (2 if variant >= 12 else 1)
     monkeypatch.setenv("CFM_J3D_TMA_VARIANT", str(variant))
     for prec, py, shape in ((cfm.FP64, 1, (21, 19, 128)), (cfm.FP32, 0, (13, 40, 136))):
         a = rand_grid(shape, cfm.np_dtype(prec), 16)
         got, _ = run_gpu(a, 5, cfm.JACOBI_PERSISTENT, py)
         np.testing.assert_array_equal(got, oracle.jacobi3d(a, 5, py))
+
+
+@pytest.mark.parametrize("variant", range(12, NVARIANTS))
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("py", [0, 1])
+@pytest.mark.parametrize("shape", [(3, 3, 64), (4, 5, 64), (5, 3, 130), (7, 36, 64), (40, 35, 192),
+                                   (70, 9, 128)])
+@pytest.mark.parametrize("niter", [1, 2, 3, 6])
+def test_two_sweep_pipeline_bitexact(variant, prec, py, shape, niter, monkeypatch):
+    """Two sweeps per pass: the periodic images (far rows and planes), tiny
+    grids where one tile or one z-chunk touches both ends, odd counts."""
+    monkeypatch.setenv("CFM_J3D_TMA_VARIANT", str(variant))
+    a = rand_grid(shape, cfm.np_dtype(prec), 17)
+    got, st = run_gpu(a, niter, cfm.JACOBI_PERSISTENT, py)
+    np.testing.assert_array_equal(got, oracle.jacobi3d(a, niter, py))
+
+
+@pytest.mark.parametrize("zc", [1, 2, 5, 64])
+def test_two_sweep_pipeline_zchunks(zc, monkeypatch):
+    monkeypatch.setenv("CFM_J3D_TMA_VARIANT", "13")
+    monkeypatch.setenv("CFM_J3D_ZCHUNK", str(zc))
+    a = rand_grid((23, 21, 128), np.float64, 18)
+    got, _ = run_gpu(a, 4, cfm.JACOBI_PERSISTENT, 1)
+    np.testing.assert_array_equal(got, oracle.jacobi3d(a, 4, 1))
 
 
 def test_jacobi_run_twice_equals_one_long_run():
