@@ -59,7 +59,7 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "jacobi3d_persistent_512_fp64.md")
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -375,9 +375,11 @@ def main():
     stream = torch.cuda.Stream()
     j.set_stream(stream.cuda_stream)
     j.load_problem(cfm.PROBLEM_CONFIG)
-    best, _ = j.autotune(40)  # pipeline shape and z-chunk; restores the grid
+    best, _ = j.autotune(NITER // 2)  # pipeline shape and z-chunk; restores the grid
     tuned = cfm.variant_info(best) if best >= 0 else None
+    zchunk = cfm.lib.cfm_jacobi_zchunk(j.h)
     blocks, threads = j.launch_shape()
+    time.sleep(1.5)  # let the power state settle after tuning's seconds at full load
     for _ in range(args.warmup):
         j.run(NITER)
 
@@ -435,7 +437,8 @@ def main():
                    "impl": "persistent cooperative kernel, grid barrier per sweep",
                    "launch": f"{blocks}x{threads}", "parallelism": f"replicas x{world}",
                    "tuned": None if tuned is None else
-                   {"variant": best, "consumer_warps": tuned[0], "rows_per_warp": tuned[1], "stages": tuned[2]},
+                   {"variant": best, "consumer_warps": tuned[0], "rows_per_warp": tuned[1], "stages": tuned[2],
+                    "sweeps_per_pass": tuned[3], "zchunk": zchunk},
                    "l2": "inputs larger than L2 (two 1.07 GB grids)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,

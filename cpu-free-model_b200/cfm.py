@@ -42,6 +42,7 @@ _SIGS = {
     "cfm_jacobi_autotune": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_jacobi_variant_info": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
     "cfm_jacobi_variant_sweeps": (_c.c_int, [_c.c_int]),
+    "cfm_jacobi_zchunk": (_c.c_int, [_vp]),
     "cfm_csr_create": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp]),
     "cfm_csr_destroy": (None, [_vp]),
     "cfm_csr_spmv_host": (_c.c_int, [_vp, _vp, _vp]),

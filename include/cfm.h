@@ -155,6 +155,9 @@ int cfm_jacobi_variant_info(int index, int *consumer_warps, int *rows_per_warp, 
  * temporally blocked shapes (an odd sweep count ends with one one-sweep
  * launch); a negative status for an unknown index. */
 int cfm_jacobi_variant_sweeps(int index);
+/* z-chunk (planes per work unit) the 3D persistent kernel of this handle
+ * uses (after cfm_jacobi_autotune: the chosen one). */
+int cfm_jacobi_zchunk(cfm_jacobi *h);
 
 /* ------------------------------------------------------------------- CG */
 typedef enum cfm_cg_impl {
