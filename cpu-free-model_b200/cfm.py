@@ -42,6 +42,7 @@ _SIGS = {
     "cfm_jacobi_autotune": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_jacobi_variant_info": (_c.c_int, [_c.c_int, _vp, _vp, _vp]),
     "cfm_jacobi_variant_sweeps": (_c.c_int, [_c.c_int]),
+    "cfm_mm_read": (_c.c_int, [_c.c_char_p, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cfm_jacobi_zchunk": (_c.c_int, [_vp]),
     "cfm_csr_create": (_c.c_int, [_c.c_int, _c.c_longlong, _vp, _vp, _vp, _vp]),
     "cfm_csr_destroy": (None, [_vp]),
@@ -240,6 +241,20 @@ class Jacobi:
         v, r = ctypes.c_int(), ctypes.c_double()
         check("cfm_jacobi_autotune", lib.cfm_jacobi_autotune(self.h, sweeps, ctypes.byref(v), ctypes.byref(r)))
         return v.value, r.value
+
+
+def mm_read(path):
+    """MatrixMarket coordinate file -> (rowptr, col, val, m, n) with the file's
+    index base kept in rowptr[0] (cfm_mm_read)."""
+    m, n, nnz = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+    p = os.fsencode(path)
+    check("cfm_mm_read", lib.cfm_mm_read(p, ctypes.byref(m), ctypes.byref(n), ctypes.byref(nnz), None, None, None))
+    rowptr = np.empty(m.value + 1, np.int32)
+    col = np.empty(nnz.value, np.int32)
+    val = np.empty(nnz.value, np.float64)
+    check("cfm_mm_read", lib.cfm_mm_read(p, ctypes.byref(m), ctypes.byref(n), ctypes.byref(nnz), _ptr(rowptr),
+                                         _ptr(col), _ptr(val)))
+    return rowptr, col, val, m.value, n.value
 
 
 def variant_info(i):

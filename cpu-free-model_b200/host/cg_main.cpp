@@ -64,10 +64,6 @@ int main(int argc, char **argv) {
             std::fprintf(stderr, "ERROR: -v %d out of range [0, %zu)\n", v, versions.size());
             return 1;
         }
-    if (!matrix_path.empty()) {
-        std::fprintf(stderr, "ERROR: -matrix_path: MatrixMarket input is not built yet\n");
-        return 1;
-    }
     if (cmp_cpu)
         std::fprintf(stderr,
                      "NOTE: -compare-cpu ignored: the reference's CPU CG never writes its SpMV "
@@ -77,7 +73,23 @@ int main(int argc, char **argv) {
     int n = 0;
     std::vector<int> rowptr, col;
     std::vector<double> val, b;
-    if (problem == "tridiag") {
+    if (!matrix_path.empty()) {
+        // MatrixMarket file, as the reference's -matrix_path (b = ones)
+        int m = 0, nn = 0;
+        long long nnz = 0;
+        int st = cfm_mm_read(matrix_path.c_str(), &m, &nn, &nnz, nullptr, nullptr, nullptr);
+        if (st) return cli::fail("cfm_mm_read", st);
+        if (m != nn) {
+            std::fprintf(stderr, "ERROR: -matrix_path: the matrix is %d x %d, not square\n", m, nn);
+            return 1;
+        }
+        n = m;
+        rowptr.resize(n + 1);
+        col.resize(nnz);
+        val.resize(nnz);
+        if ((st = cfm_mm_read(matrix_path.c_str(), &m, &nn, &nnz, rowptr.data(), col.data(), val.data())))
+            return cli::fail("cfm_mm_read", st);
+    } else if (problem == "tridiag") {
         n = 10485760 * 2;
         const long long nnz = (long long)(n - 2) * 3 + 4;
         rowptr.resize(n + 1);

@@ -182,6 +182,15 @@ typedef struct cfm_csr cfm_csr;
 int cfm_csr_create(int n, long long nnz, const int *rowptr, const int *col, const double *val,
                    cfm_csr **out);
 void cfm_csr_destroy(cfm_csr *A);
+/* MatrixMarket coordinate file -> CSR on the host, with the behaviour of the
+ * reference's loadMMSparseMatrix (CG/src/mmio_wrapper.cpp:170-378): real or
+ * integer field; general, symmetric, hermitian or skew-symmetric (expanded
+ * to the full pattern); entries sorted by (row, column); the index base of
+ * the file (1 when an index equals the dimension, 0 when one is 0) kept in
+ * rowptr[0], as cfm_csr_create expects.  Call first with rowptr = NULL for
+ * *m, *n and *nnz, then with rowptr (m + 1), col and val (nnz) allocated.
+ * Dense (array), pattern and complex files are CFM_UNSUPPORTED. */
+int cfm_mm_read(const char *path, int *m, int *n, long long *nnz, int *rowptr, int *col, double *val);
 /* y = A x with host vectors (FP64, deterministic row order). */
 int cfm_csr_spmv_host(const cfm_csr *A, const double *x, double *y);
 

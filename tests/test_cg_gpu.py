@@ -78,3 +78,32 @@ def test_cg_config3_poisson128_persistent_vs_oracle():
     assert rel <= 1e-12, rel
     assert st.residual <= 1e-8
     assert st.launches == 1
+
+
+def test_cg_on_matrixmarket_file(tmp_path):
+    """-matrix_path input: a symmetric MatrixMarket file (lower triangle
+    stored) read back, uploaded with its 1-based indices and solved with
+    b = ones, equals the same system built in memory, bit for bit."""
+    import os
+    import subprocess
+
+    import scipy.io
+    import scipy.sparse as sp
+
+    rowptr, col, val = cfm.poisson3d(9)
+    n = len(rowptr) - 1
+    A = sp.csr_matrix((val, col, rowptr), shape=(n, n))
+    p = tmp_path / "poisson9.mtx"
+    scipy.io.mmwrite(str(p), A.tocoo(), symmetry="symmetric")
+    r2, c2, v2, m, n2 = cfm.mm_read(str(p))
+    assert m == n2 == n and r2[0] == 1
+    x_file, st = cfm.CG(cfm.CSR(r2, c2, v2), cfm.CG_PERSISTENT, 2000, 1e-10).solve(None)
+    x_mem, st_mem = cfm.CG(cfm.CSR(rowptr, col, val), cfm.CG_PERSISTENT, 2000, 1e-10).solve(None)
+    assert st.status == cfm.OK and st.iterations == st_mem.iterations
+    np.testing.assert_array_equal(x_file, x_mem)
+    binary = os.path.join(os.path.dirname(cfm.__file__), "bin", "cg")
+    out = subprocess.run([binary, "-v", "1", "-s", "-matrix_path", str(p), "-niter", "50"],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    first = next(t for t in out.stdout.split() if t.replace(".", "", 1).isdigit())
+    assert float(first) > 0  # the first float is the time, as the reference prints it
