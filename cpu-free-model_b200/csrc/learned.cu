@@ -65,17 +65,20 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
     *reinterpret_cast<uint4 *>(p) = u;
 }
 
-// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Eight threads per
-// pixel, each producing 4 channels (one 8-byte store; a warp writes 4 whole
-// pixels) with its 72 weights and 4 biases held in registers across
-// CIN_PASSES pixels.  The 9 input loads of a pixel are issued together from
-// clamped coordinates and zeroed outside the image.
-// grid: (ceil(W / (32 CIN_PASSES)), H, B), 256 threads.
-constexpr int CIN_PASSES = 8;
-__global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w, const float *b,
-                                                 bf16 *h0, int H, int W, UNetInputScale in_scale) {
+// Pixels a thread of the first / last layer computes side by side in x: the
+// 3 x (PXB + 2) input neighbourhood is loaded once for all of them.
+constexpr int PXB = 4;
+
+// h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Lane = 8 * group +
+// q: a group of 8 lanes covers PXB consecutive pixels, lane q their channels
+// 4q .. 4q + 3, with its 72 weights and 4 biases in registers; per tap and
+// channel o += w0 x0 + w1 x1, taps in order.  Input channel 0 is optionally
+// scaled by 1 / rms from a solver's partial sums.  A block walks CIN_SPAN
+// pixel groups of one row.  grid: (ceil(W / (PXB CIN_SPAN 32)), H, B), 256 threads.
+constexpr int CIN_SPAN = 2;
+__global__ void __launch_bounds__(256, 2) k_cin_fwd(const float *x, const float *w, const float *b,
+                                                    bf16 *h0, int H, int W, UNetInputScale in_scale) {
     pdl_enter();
-    // input channel 0 scale: 1 / rms from a solver's partial sums (fixed order)
     float sc = 1.f;
     if (in_scale.part) {
         __shared__ double red[8];
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w,
         for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) tot += red[wi];
         sc = tot > 0 ? (float)sqrt(in_scale.cells / tot) : 0.f;
     }
-    const int q = threadIdx.x & 7, c0 = q * 4;
+    const int q = threadIdx.x & 7, c0 = q * 4, grp = threadIdx.x >> 3;  // 32 groups per block
     float wr[9][8];  // [t][(c - c0) * 2 + in]
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
@@ -102,43 +105,58 @@ __global__ void __launch_bounds__(256) k_cin_fwd(const float *x, const float *w,
     const float *xi = x + (size_t)img * H * W * 2;
     bf16 *hrow = h0 + ((size_t)img * H + yy) * W * 32;
 #pragma unroll 1
-    for (int pass = 0; pass < CIN_PASSES; ++pass) {
-        const int xx = (blockIdx.x * CIN_PASSES + pass) * 32 + (threadIdx.x >> 3);
-        if (xx >= W) break;
-        float2 v[9];
+    for (int span = 0; span < CIN_SPAN; ++span) {
+        const int xs = ((blockIdx.x * CIN_SPAN + span) * 32 + grp) * PXB;  // first pixel of the group
+        if (xs >= W) break;
+        float o[PXB][4];
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-            const bool in = y >= 0 && y < H && xq >= 0 && xq < W;
-            const int yc = min(max(y, 0), H - 1), xc = min(max(xq, 0), W - 1);
-            v[t] = *reinterpret_cast<const float2 *>(xi + 2 * (yc * W + xc));
-            if (in_scale.part) v[t].x *= sc;
-            if (!in) v[t] = make_float2(0.f, 0.f);
+        for (int p = 0; p < PXB; ++p) o[p][0] = bq.x, o[p][1] = bq.y, o[p][2] = bq.z, o[p][3] = bq.w;
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy) {
+            const int y = yy + dy - 1;
+            const bool yin = y >= 0 && y < H;
+            const int yc = min(max(y, 0), H - 1);
+            float2 v[PXB + 2];
+#pragma unroll
+            for (int k = 0; k < PXB + 2; ++k) {
+                const int xq = xs + k - 1;
+                const int xc = min(max(xq, 0), W - 1);
+                v[k] = *reinterpret_cast<const float2 *>(xi + 2 * (yc * W + xc));
+                if (in_scale.part) v[k].x *= sc;
+                if (!(yin && xq >= 0 && xq < W)) v[k] = make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int t = dy * 3 + dx;
+#pragma unroll
+                for (int p = 0; p < PXB; ++p)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        o[p][c] += wr[t][2 * c] * v[p + dx].x + wr[t][2 * c + 1] * v[p + dx].y;
+            }
         }
-        float o[4] = {bq.x, bq.y, bq.z, bq.w};
 #pragma unroll
-        for (int t = 0; t < 9; ++t)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) o[c] += wr[t][2 * c] * v[t].x + wr[t][2 * c + 1] * v[t].y;
-        __nv_bfloat162 r[2];
-        r[0] = __floats2bfloat162_rn(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f));
-        r[1] = __floats2bfloat162_rn(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f));
-        *reinterpret_cast<uint2 *>(hrow + (size_t)xx * 32 + c0) = *reinterpret_cast<const uint2 *>(r);
+        for (int p = 0; p < PXB; ++p) {
+            if (xs + p >= W) break;
+            __nv_bfloat162 r[2];
+            r[0] = __floats2bfloat162_rn(fmaxf(o[p][0], 0.f), fmaxf(o[p][1], 0.f));
+            r[1] = __floats2bfloat162_rn(fmaxf(o[p][2], 0.f), fmaxf(o[p][3], 0.f));
+            *reinterpret_cast<uint2 *>(hrow + (size_t)(xs + p) * 32 + c0) = *reinterpret_cast<const uint2 *>(r);
+        }
     }
 }
 
-// out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.  Four threads
-// per pixel (a warp reads 8 whole pixels, 512 contiguous bytes, per tap),
-// each summing one 8-channel group over the 9 taps with its 72 weights held
-// in registers across COUT_PASSES pixels; the 9 loads of a pixel are issued
-// together from clamped coordinates and zeroed outside the image; two xor
-// shuffles add the groups, (g0 + g1) + (g2 + g3).
-// grid: (ceil(W / (64 COUT_PASSES)), H, B), 256 threads.
-constexpr int COUT_PASSES = 4;
+// out = cout(g0): g0 [B][H][W][32], w [9][1][32], out FP32.  Lane = 4 *
+// group + q: a group of 4 lanes covers PXB consecutive pixels, lane q the
+// 8-channel group q with its 72 weights in registers, summing over the 9
+// taps in order (one 8-term expression per tap); two xor shuffles add the
+// groups, (g0 + g1) + (g2 + g3).  A block walks COUT_SPAN pixel groups of
+// one row.  grid: (ceil(W / (PXB COUT_SPAN 64)), H, B), 256 threads.
+constexpr int COUT_SPAN = 2;
 __global__ void __launch_bounds__(256, 2) k_cout_fwd(const bf16 *g0, const float *w, const float *b,
                                                      float *out, int H, int W) {
     pdl_enter();
-    const int q = threadIdx.x & 3, c0 = q * 8;
+    const int q = threadIdx.x & 3, c0 = q * 8, grp = threadIdx.x >> 2;  // 64 groups per block
     float wr[9][8];
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
@@ -152,36 +170,50 @@ __global__ void __launch_bounds__(256, 2) k_cout_fwd(const bf16 *g0, const float
     const bf16 *gi = g0 + (size_t)img * H * W * 32;
     float *oi = out + ((size_t)img * H + yy) * W;
 #pragma unroll 1
-    for (int pass = 0; pass < COUT_PASSES; ++pass) {
-        // every lane stays to the shuffles; those past the row end sum zero
-        const int xx = (blockIdx.x * COUT_PASSES + pass) * 64 + (threadIdx.x >> 2);
-        const bool valid = xx < W;
-        uint4 raw[9];
+    for (int span = 0; span < COUT_SPAN; ++span) {
+        // every lane stays to the shuffles; pixels past the row end sum zero
+        const int xs = ((blockIdx.x * COUT_SPAN + span) * 64 + grp) * PXB;
+        float acc[PXB];
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            const int y = yy + t / 3 - 1, xq = xx + t % 3 - 1;
-            const bool in = valid && y >= 0 && y < H && xq >= 0 && xq < W;
-            const int yc = min(max(y, 0), H - 1), xc = min(max(xq, 0), W - 1);
-            raw[t] = *reinterpret_cast<const uint4 *>(gi + (size_t)(yc * W + xc) * 32 + c0);
-            if (!in) raw[t] = make_uint4(0u, 0u, 0u, 0u);
-        }
-        float acc = 0.f;
+        for (int p = 0; p < PXB; ++p) acc[p] = 0.f;
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw[t]);
-            float v[8];
+        for (int dy = 0; dy < 3; ++dy) {
+            const int y = yy + dy - 1;
+            const bool yin = y >= 0 && y < H;
+            const int yc = min(max(y, 0), H - 1);
+            float v[PXB + 2][8];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const float2 f = __bfloat1622float2(h[i]);
-                v[2 * i] = f.x;
-                v[2 * i + 1] = f.y;
+            for (int k = 0; k < PXB + 2; ++k) {
+                const int xq = xs + k - 1;
+                const int xc = min(max(xq, 0), W - 1);
+                uint4 raw = *reinterpret_cast<const uint4 *>(gi + (size_t)(yc * W + xc) * 32 + c0);
+                if (!(yin && xq >= 0 && xq < W)) raw = make_uint4(0u, 0u, 0u, 0u);
+                const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&raw);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float2 f = __bfloat1622float2(h[i]);
+                    v[k][2 * i] = f.x;
+                    v[k][2 * i + 1] = f.y;
+                }
             }
-            acc += wr[t][0] * v[0] + wr[t][1] * v[1] + wr[t][2] * v[2] + wr[t][3] * v[3] +
-                   wr[t][4] * v[4] + wr[t][5] * v[5] + wr[t][6] * v[6] + wr[t][7] * v[7];
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) {
+                const int t = dy * 3 + dx;
+#pragma unroll
+                for (int p = 0; p < PXB; ++p) {
+                    const float *vv = v[p + dx];
+                    acc[p] += wr[t][0] * vv[0] + wr[t][1] * vv[1] + wr[t][2] * vv[2] + wr[t][3] * vv[3] +
+                              wr[t][4] * vv[4] + wr[t][5] * vv[5] + wr[t][6] * vv[6] + wr[t][7] * vv[7];
+                }
+            }
         }
-        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-        if (valid && q == 0) oi[xx] = acc + bias;
+#pragma unroll
+        for (int p = 0; p < PXB; ++p) {
+            float a = acc[p];
+            a += __shfl_xor_sync(0xffffffffu, a, 1);
+            a += __shfl_xor_sync(0xffffffffu, a, 2);
+            if (q == 0 && xs + p < W) oi[xs + p] = a + bias;
+        }
     }
 }
 
@@ -566,7 +598,7 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
     UNetBuffers &a = u->a;
     const int H = u->H, W = u->W;
     int st;
-    CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + 32 * CIN_PASSES - 1) / (32 * CIN_PASSES), H, B), dim3(256),
+    CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + PXB * CIN_SPAN * 32 - 1) / (PXB * CIN_SPAN * 32), H, B), dim3(256),
                             0, s, x, (const float *)(u->theta + u->woff[0]),
                             (const float *)(u->theta + u->boff[0]), a.h0, H, W,
                             in_scale ? *in_scale : UNetInputScale{nullptr, 0, 0.0}));
@@ -596,7 +628,7 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
                             (const bf16 *)a.g1, (const bf16 *)a.h0, a.u0, h, w));
     h *= 2, w *= 2;
     if ((st = conv_fwd(u, 7, a.u0, a.g0, B, h, w, s))) return st;
-    CFM_CUDA_TRY(launch_pdl(k_cout_fwd, dim3((W + 64 * COUT_PASSES - 1) / (64 * COUT_PASSES), H, B),
+    CFM_CUDA_TRY(launch_pdl(k_cout_fwd, dim3((W + PXB * COUT_SPAN * 64 - 1) / (PXB * COUT_SPAN * 64), H, B),
                             dim3(256), 0, s, (const bf16 *)a.g0, (const float *)(u->theta + u->woff[8]),
                             (const float *)(u->theta + u->boff[8]), out, H, W));
     return CFM_OK;
