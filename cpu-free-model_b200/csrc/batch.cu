@@ -652,6 +652,7 @@ int cfm_batch_set_solver(cfm_batch *h, int smooth, int maxiter, double tol) {
 // Solve every system (one graph launch = one persistent kernel).  iters /
 // status / relres (true FP64 relative residual) per system, optional.
 int cfm_batch_solve(cfm_batch *h, long long *iters, int *status, double *relres, cfm_stats *st) {
+    const cfm::NvtxRange nvtx_range("cfm_batch_solve");
     clear_error();
     CFM_ARG_CHECK(h, "null argument");
     float ms = 0;
@@ -700,6 +701,7 @@ int cfm_batch_solution(cfm_batch *h, int i, double *x_host) {
 // Autotuner: times each candidate (classes, thresholds, team sizes) on the
 // real batch and keeps the fastest; `best_ms` gets its time.
 int cfm_batch_autotune(cfm_batch *h, double *best_ms) {
+    const cfm::NvtxRange nvtx_range("cfm_batch_autotune");
     clear_error();
     CFM_ARG_CHECK(h, "null argument");
     struct Cand {

@@ -11,6 +11,7 @@
 #include <utility>
 
 #include "cfm.h"
+#include "nvtx3/nvToolsExt.h"
 
 namespace cfm {
 
@@ -80,6 +81,16 @@ __device__ __forceinline__ void pdl_enter() {
     pdl_trigger();
 }
 #endif
+
+// NVTX range over a host phase (the reference's PUSH_RANGE / POP_RANGE
+// tracing, Stencil/jacobi2D/include/common.h:81-105): visible in a profiler
+// timeline, free when none is attached (NVTX v3 loads its back end lazily).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 }  // namespace cfm
 

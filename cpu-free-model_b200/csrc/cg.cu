@@ -652,6 +652,7 @@ int cfm_cg_set_stream(cfm_cg *h, void *cuda_stream) {
 }
 
 int cfm_cg_solve(cfm_cg *h, const double *b_host, double *x_host, cfm_stats *st) {
+    const cfm::NvtxRange nvtx_range("cfm_cg_solve");
     CFM_ARG_CHECK(h && x_host, "null argument");
     clear_error();
     const int n = h->n;
@@ -660,6 +661,7 @@ int cfm_cg_solve(cfm_cg *h, const double *b_host, double *x_host, cfm_stats *st)
 }
 
 int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats *st) {
+    const cfm::NvtxRange nvtx_range("cfm_cg_solve_device");
     CFM_ARG_CHECK(h && x_dev, "null argument");
     clear_error();
     return solve_impl(h, b_dev, x_dev, st, 0, 0, nullptr, nullptr);
@@ -737,6 +739,7 @@ extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
                                     const int *col_dev, const double *val_dev,
                                     const double *b_dev, double *x_dev, int maxiter, double tol,
                                     void *cuda_stream, cfm_stats *st) {
+    const NvtxRange nvtx_range("cfm_cg_solve_noalloc");
     clear_error();
     CFM_ARG_CHECK(n > 0, "n must be positive");
     if ((size_t)n > NA_MAX_N) {

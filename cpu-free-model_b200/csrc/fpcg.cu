@@ -1017,6 +1017,7 @@ int cfm_fpcg_set_network_period(cfm_fpcg *h, int every) {
 }
 
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *stats) {
+    const cfm::NvtxRange nvtx_range("cfm_fpcg_solve");
     clear_error();
     CFM_ARG_CHECK(h && b_host && x_host, "null argument");
     const size_t n = h->n;
@@ -1112,6 +1113,7 @@ int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
                            int batch, float lr, int smooth, int coarsen, double *loss_first,
                            double *loss_last, double *data_seconds, double *train_seconds) {
+    const NvtxRange nvtx_range("cfm_unet_train_varcoef");
     clear_error();
     CFM_ARG_CHECK(net && nsys >= 1 && snaps >= 1 && epochs >= 1, "arguments");
     CFM_ARG_CHECK(smooth >= 0 && smooth <= FP_MAX_SMOOTH, "smooth must be in [0, 8]");
@@ -1171,6 +1173,15 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
     std::vector<double> kh(n), fh(n);
     std::vector<float> gh(nc);
     int st = 0;
+    nvtxRangePushA("training data: plain-CG pairs");
+    struct PopAtExit {
+        bool on = true;
+        void pop() {
+            if (on) nvtxRangePop();
+            on = false;
+        }
+        ~PopAtExit() { pop(); }
+    } data_range;
     for (int sy = 0; sy < nsys; ++sy) {
         if ((st = cfm_varcoef_problem(2, W, H, 1, seed0 + sy, kh.data(), fh.data()))) return st;
         for (int ic = 0; ic < nc; ++ic) {  // block-mean log k on the network's grid
@@ -1228,7 +1239,9 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         cfm_stencil_destroy(S2);
     }
     const auto t1 = std::chrono::steady_clock::now();
+    data_range.pop();
     // training
+    const NvtxRange train_range("training: Adam epochs");
     std::mt19937_64 rng(seed0 ^ 0x5eedULL);
     std::vector<long long> order(N);
     for (long long i = 0; i < N; ++i) order[i] = i;

@@ -1067,6 +1067,7 @@ int cfm_jacobi_download(cfm_jacobi *h, void *host_grid) {
 }
 
 int cfm_jacobi_run(cfm_jacobi *h, int niter, cfm_stats *st) {
+    const cfm::NvtxRange nvtx_range("cfm_jacobi_run");
     CFM_ARG_CHECK(h, "handle is null");
     CFM_ARG_CHECK(niter >= 0, "niter must be >= 0");
     clear_error();
@@ -1081,6 +1082,7 @@ int cfm_jacobi_run(cfm_jacobi *h, int niter, cfm_stats *st) {
 
 int cfm_jacobi_run_host(cfm_jacobi *h, int niter, const void *host_in, void *host_out,
                         cfm_stats *st) {
+    const cfm::NvtxRange nvtx_range("cfm_jacobi_run_host");
     CFM_ARG_CHECK(h && host_in && host_out, "null argument");
     CFM_ARG_CHECK(niter >= 0, "niter must be >= 0");
     clear_error();
@@ -1124,6 +1126,7 @@ int cfm_jacobi_variant_sweeps(int index) {
 }
 
 int cfm_jacobi_autotune(cfm_jacobi *h, int sweeps, int *best_variant, double *best_glups) {
+    const cfm::NvtxRange nvtx_range("cfm_jacobi_autotune");
     CFM_ARG_CHECK(h, "handle is null");
     CFM_ARG_CHECK(sweeps >= 1, "sweeps must be >= 1");
     if (best_variant) *best_variant = -1;
