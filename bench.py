@@ -21,6 +21,8 @@ restatement of the reference's single-GPU sweep (the reference ships no CPU
 Jacobi of its own) on the host cores with the same metric.
 
 Other workloads (--workload, one JSON line each, same keys):
+  jacobi3d_fp32  the same 512^3 problem in FP32 (8 B/LUP) and its error after
+             100 sweeps against the FP64 (bit-exact) result.
   cg128      CG on the 128^3 7-point Poisson CSR system to a true relative
              residual of 1e-8: standard, pipelined and FP32-inner/FP64-
              refinement persistent kernels (time to solution, GB/s).
@@ -63,7 +65,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["jacobi3d", "cg128", "varcoef512", "unet", "batch256"],
+    ap.add_argument("--workload", choices=["jacobi3d", "jacobi3d_fp32", "cg128", "varcoef512", "unet", "batch256"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -117,6 +119,50 @@ def workload_cg128(args, cfm):
          res[best]["ms"], {"workload": "cg_poisson7_128^3_csr_tol1e-8", "n": A.n, "nnz": len(val),
                            "best": best, "impls": res, "timing": "median of steps, CUDA events, H2D of b and D2H of x included",
                            "peak_hbm_gbs": peak, "peak_kind": kind}, higher=False)
+
+
+def workload_jacobi3d_fp32(args, cfm):
+    """The 512^3 periodic problem in FP32 (8 B/LUP), with its max-abs and
+    relative L2 error after 100 sweeps against the FP64 sweep (which is bit
+    for bit the reference's)."""
+    import numpy as np
+    peak, kind = peak_hbm()
+    j64 = cfm.Jacobi(3, N, N, N, cfm.FP64, 1, cfm.JACOBI_PERSISTENT)
+    j64.load_problem(cfm.PROBLEM_CONFIG)
+    j64.run(NITER)
+    ref = j64.download()
+    j64.close()
+    j = cfm.Jacobi(3, N, N, N, cfm.FP32, 1, cfm.JACOBI_PERSISTENT)
+    j.load_problem(cfm.PROBLEM_CONFIG)
+    best, _ = j.autotune(NITER // 2)
+    tuned = cfm.variant_info(best) if best >= 0 else None
+    j.load_problem(cfm.PROBLEM_CONFIG)
+    j.run(NITER)
+    got = j.download().astype(np.float64)
+    err = got - ref
+    inner = (slice(1, -1),) * 3
+    max_abs = float(np.abs(err[inner]).max())
+    rel_l2 = float(np.linalg.norm(err[inner]) / np.linalg.norm(ref[inner]))
+    del got, err, ref
+    for _ in range(args.warmup):
+        j.run(NITER)
+    secs = []
+    for _ in range(args.steps):
+        secs.append(j.run(NITER).seconds)
+    j.close()
+    t = statistics.median(secs)
+    glups = NITER * LUP_PER_SWEEP / t / 1e9
+    achieved = 8.0 * NITER * LUP_PER_SWEEP / t / 1e9
+    line("Jacobi 3d7p 512^3 FP32 GLUP/s", glups, "GLUP/s", args, t * 1e3,
+         {"workload": "jacobi3d7p_512^3_fp32_periodic", "niter_per_step": NITER,
+          "tuned": None if tuned is None else {"variant": best, "consumer_warps": tuned[0],
+                                               "rows_per_warp": tuned[1], "stages": tuned[2],
+                                               "sweeps_per_pass": tuned[3]},
+          "error_vs_fp64_after_100_sweeps": {"max_abs": max_abs, "rel_l2": rel_l2},
+          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "peak_kind": kind, "bytes_per_lup": 8},
+          "timing": "median of steps, CUDA events around one 100-sweep launch"},
+         dtype="f32")
 
 
 def workload_varcoef512(args, cfm):
@@ -233,7 +279,8 @@ def workload_batch256(args, cfm):
 def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
-    {"cg128": workload_cg128, "varcoef512": workload_varcoef512, "unet": workload_unet,
+    {"cg128": workload_cg128, "jacobi3d_fp32": workload_jacobi3d_fp32, "varcoef512": workload_varcoef512,
+     "unet": workload_unet,
      "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
 
