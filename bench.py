@@ -358,6 +358,35 @@ def cpu_baseline():
             "sample": f"{k} FP64 sweeps of the 512^3 periodic problem, sweep loop only (OpenMP)"}
 
 
+class Ranks:
+    """What the replicas share: a barrier and the max over ranks of a time
+    (CUDA tensors over NCCL on the GPUs; CPU tensors over gloo in the tests).
+    With one rank both are no-ops."""
+
+    def __init__(self, world, device):
+        self.world, self.device = world, device
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def whole_job_rate(world, steps, units_per_step, seconds):
+    """Units per second over all replicas: every rank did `steps` steps of
+    `units_per_step` units, timed by the slowest rank (`seconds`)."""
+    return world * steps * units_per_step / seconds
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -407,16 +436,8 @@ def main():
                                 device_id=torch.device("cuda", local))
     import cfm
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world, "cuda")
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     j = cfm.Jacobi(3, N, N, N, cfm.FP64, 1, cfm.JACOBI_PERSISTENT)
     stream = torch.cuda.Stream()
@@ -468,8 +489,8 @@ def main():
     j.close()
 
     lup_step = NITER * LUP_PER_SWEEP
-    value = world * args.steps * lup_step / t_dev / 1e9
-    e2e_value = world * e2e_steps * lup_step / e2e_s / 1e9
+    value = whole_job_rate(world, args.steps, lup_step, t_dev) / 1e9
+    e2e_value = whole_job_rate(world, e2e_steps, lup_step, e2e_s) / 1e9
     peak, peak_kind = peak_hbm()
     per_launch_s = kern_s / args.steps
     achieved = BYTES_PER_LUP * lup_step / per_launch_s / 1e9
