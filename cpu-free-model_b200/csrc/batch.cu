@@ -146,31 +146,37 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
     int site = 0;
     double *part = a.part + S.poff;
     // x = 0, r = b; |b|^2
-    for (int tile = rank; tile < S.ntiles; tile += T) {
-        const long long i = (long long)tile * CG_TILE + threadIdx.x;
-        double bb = 0.0;
-        if (i < S.n) {
-            const long long g = S.off + i;
-            const double bi = a.b[g];
-            a.x[g] = 0.0;
-            a.r[g] = bi;
-            bb = bi * bi;
+    {
+        TileSums<1> ts(sm, T, part + 3 * S.ntiles);
+        for (int tile = rank; tile < S.ntiles; tile += T) {
+            const long long i = (long long)tile * CG_TILE + threadIdx.x;
+            double bb = 0.0;
+            if (i < S.n) {
+                const long long g = S.off + i;
+                const double bi = a.b[g];
+                a.x[g] = 0.0;
+                a.r[g] = bi;
+                bb = bi * bi;
+            }
+            ts.add(tile, bb);
         }
-        bb = block_sum(bb, sm);
-        if (threadIdx.x == 0) part[3 * S.ntiles + tile] = bb;
+        ts.flush();
     }
     if (!bt_precond(a, S, rank, T, bar, site)) return false;
     // p = z; <r, z>
-    for (int tile = rank; tile < S.ntiles; tile += T) {
-        const long long i = (long long)tile * CG_TILE + threadIdx.x;
-        double rz = 0.0;
-        if (i < S.n) {
-            const long long g = S.off + i;
-            a.p[g] = a.z[g];
-            rz = a.r[g] * a.z[g];
+    {
+        TileSums<1> ts(sm, T, part);
+        for (int tile = rank; tile < S.ntiles; tile += T) {
+            const long long i = (long long)tile * CG_TILE + threadIdx.x;
+            double rz = 0.0;
+            if (i < S.n) {
+                const long long g = S.off + i;
+                a.p[g] = a.z[g];
+                rz = a.r[g] * a.z[g];
+            }
+            ts.add(tile, rz);
         }
-        rz = block_sum(rz, sm);
-        if (threadIdx.x == 0) part[tile] = rz;
+        ts.flush();
     }
     if (!grid_barrier(bar, T, site++)) return false;
     const double bb = bt_sum(a, S, 3, sm);
@@ -182,17 +188,20 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
     if (rr <= target2) status = CFM_OK;
     while (status != CFM_OK && k < a.maxiter) {
         // s = A p; <p, s>
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            double ps = 0.0;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                const double si = bt_apply(a, S, a.p, i);
-                a.s[g] = si;
-                ps = a.p[g] * si;
+        {
+            TileSums<1> ts(sm, T, part + S.ntiles);
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                double ps = 0.0;
+                if (i < S.n) {
+                    const long long g = S.off + i;
+                    const double si = bt_apply(a, S, a.p, i);
+                    a.s[g] = si;
+                    ps = a.p[g] * si;
+                }
+                ts.add(tile, ps);
             }
-            ps = block_sum(ps, sm);
-            if (threadIdx.x == 0) part[S.ntiles + tile] = ps;
+            ts.flush();
         }
         if (!grid_barrier(bar, T, site++)) return false;
         const double ps = bt_sum(a, S, 1, sm);
@@ -202,18 +211,21 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
             break;
         }
         // x += alpha p; r -= alpha s; |r|^2
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            double q = 0.0;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                a.x[g] = fma(alpha, a.p[g], a.x[g]);
-                const double ri = fma(-alpha, a.s[g], a.r[g]);
-                a.r[g] = ri;
-                q = ri * ri;
+        {
+            TileSums<1> ts(sm, T, part + 2 * S.ntiles);
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                double q = 0.0;
+                if (i < S.n) {
+                    const long long g = S.off + i;
+                    a.x[g] = fma(alpha, a.p[g], a.x[g]);
+                    const double ri = fma(-alpha, a.s[g], a.r[g]);
+                    a.r[g] = ri;
+                    q = ri * ri;
+                }
+                ts.add(tile, q);
             }
-            q = block_sum(q, sm);
-            if (threadIdx.x == 0) part[2 * S.ntiles + tile] = q;
+            ts.flush();
         }
         ++k;
         if (!grid_barrier(bar, T, site++)) return false;
@@ -225,12 +237,15 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
         if (!bt_precond(a, S, rank, T, bar, site)) return false;
         if (a.smooth > 0 && !grid_barrier(bar, T, site++)) return false;
         // <r, z>
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            double q = 0.0;
-            if (i < S.n) q = a.r[S.off + i] * a.z[S.off + i];
-            q = block_sum(q, sm);
-            if (threadIdx.x == 0) part[tile] = q;
+        {
+            TileSums<1> ts(sm, T, part);
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                double q = 0.0;
+                if (i < S.n) q = a.r[S.off + i] * a.z[S.off + i];
+                ts.add(tile, q);
+            }
+            ts.flush();
         }
         if (!grid_barrier(bar, T, site++)) return false;
         const double rz1 = bt_sum(a, S, 0, sm);
@@ -256,7 +271,7 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
 }
 
 __global__ void __launch_bounds__(CG_TILE, 1) batch_kernel(BtArgs a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     __shared__ int s_sys;
     int c = 0;
     while (c + 1 < a.ncls && (int)blockIdx.x >= a.cls_block0[c + 1]) ++c;

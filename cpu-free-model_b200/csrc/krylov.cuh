@@ -72,6 +72,52 @@ __device__ __forceinline__ double sum_partials(const double *part, int ntiles, d
     return block_sum(acc, sm);
 }
 
+// Per-tile sums of a tile loop without a block barrier per tile.  Each
+// warp reduces its 32 rows at once (the xor butterfly of block_sum) and
+// parks the warp sum in shared memory; every TS_TILES tiles, and at the end,
+// one barrier, then warp w reduces parked entry w (the 32 warp sums of one
+// tile, in warp order: again block_sum's tree) into dst[k][tile].  The
+// partials are bit for bit block_sum's, while the warps of a block run ahead
+// of each other from tile to tile.  The block's tiles are t0, t0 + stride,
+// ...; every thread of the block calls add() for every tile, and flush()
+// after the loop.
+constexpr int TS_TILES = 16;
+constexpr int TS_SMEM = TS_TILES * 2 * 32;  // doubles (also >= 33 for block_sum)
+
+template <int K>
+struct TileSums {
+    double *sm;
+    double *dst[K];
+    int stride, t0 = 0, g = 0;
+    __device__ __forceinline__ TileSums(double *s, int step, double *d0, double *d1 = nullptr)
+        : sm(s), stride(step) {
+        dst[0] = d0;
+        if (K > 1) dst[K - 1] = d1;
+    }
+    __device__ __forceinline__ void add(int tile, double v0, double v1 = 0.0) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (g == 0) t0 = tile;
+        v0 = warp_xor_sum(v0);
+        if (lane == 0) sm[(g * K) * 32 + warp] = v0;
+        if (K > 1) {
+            v1 = warp_xor_sum(v1);
+            if (lane == 0) sm[(g * K + K - 1) * 32 + warp] = v1;
+        }
+        if (++g == TS_TILES) flush();
+    }
+    __device__ __forceinline__ void flush() {
+        if (g == 0) return;
+        __syncthreads();
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (warp < g * K) {
+            const double v = warp_xor_sum(sm[warp * 32 + lane]);
+            if (lane == 0) dst[warp % K][t0 + (warp / K) * stride] = v;
+        }
+        __syncthreads();
+        g = 0;
+    }
+};
+
 // Exact product of two FP32 values, as FP64.
 __device__ __forceinline__ double xprod(float a, float b) { return __dmul_rn((double)a, (double)b); }
 
@@ -170,6 +216,7 @@ __device__ __forceinline__ double *slot(const KArgs<Op> &a, int s) {
 // -------------------------------------------------------- standard phases
 template <class Op>
 __device__ void phase_init(const KArgs<Op> &a, double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, SL_G0), slot(a, SL_B));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0, bb = 0.0;
@@ -182,17 +229,14 @@ __device__ void phase_init(const KArgs<Op> &a, double *sm) {
             g = __dmul_rn(ri, ri);
             bb = __dmul_rn(bi, bi);
         }
-        g = block_sum(g, sm);
-        bb = block_sum(bb, sm);
-        if (threadIdx.x == 0) {
-            slot(a, SL_G0)[tile] = g;
-            slot(a, SL_B)[tile] = bb;
-        }
+        ts.add(tile, g, bb);
     }
+    ts.flush();
 }
 
 template <class Op>
 __device__ void phase_spmv_dot(const KArgs<Op> &a, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_D0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double d = 0.0;
@@ -201,13 +245,14 @@ __device__ void phase_spmv_dot(const KArgs<Op> &a, double *sm) {
             a.s[i] = si;
             d = __dmul_rn(a.p[i], si);
         }
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) slot(a, SL_D0)[tile] = d;
+        ts.add(tile, d);
     }
+    ts.flush();
 }
 
 template <class Op>
 __device__ void phase_update(const KArgs<Op> &a, double alpha, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0;
@@ -217,14 +262,15 @@ __device__ void phase_update(const KArgs<Op> &a, double alpha, double *sm) {
             a.r[i] = ri;
             g = __dmul_rn(ri, ri);
         }
-        g = block_sum(g, sm);
-        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+        ts.add(tile, g);
     }
+    ts.flush();
 }
 
 // t = b - A x (FP64) and its squared norm into SL_TT
 template <class Op>
 __device__ void phase_true_residual(const KArgs<Op> &a, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_TT));
     CFM_TILES(a) {
         CFM_ROW(a);
         double q = 0.0;
@@ -234,9 +280,9 @@ __device__ void phase_true_residual(const KArgs<Op> &a, double *sm) {
             a.t[i] = ti;
             q = __dmul_rn(ti, ti);
         }
-        q = block_sum(q, sm);
-        if (threadIdx.x == 0) slot(a, SL_TT)[tile] = q;
+        ts.add(tile, q);
     }
+    ts.flush();
 }
 
 template <class Op>
@@ -283,7 +329,7 @@ __device__ __forceinline__ void write_result(CgResult *res, long long k, int sta
 // otherwise); tol <= 0 runs exactly maxiter iterations (reference -niter).
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE, 1) cg_std_kernel(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     int site = 0;
     phase_init(a, sm);
     if (!grid_barrier(a.bar, gridDim.x, site++)) return;
@@ -341,6 +387,7 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_std_kernel(KArgs<Op> a) {
 // r0 = b - A x0 with x0 = 0 (into t), and ||b||^2.
 template <class Op>
 __device__ void phase_pipe_init(const KArgs<Op> &a, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_B));
     CFM_TILES(a) {
         CFM_ROW(a);
         double bb = 0.0;
@@ -350,9 +397,9 @@ __device__ void phase_pipe_init(const KArgs<Op> &a, double *sm) {
             a.t[i] = __fma_rn(-1.0, a.op.apply_zero(i), bi);
             bb = __dmul_rn(bi, bi);
         }
-        bb = block_sum(bb, sm);
-        if (threadIdx.x == 0) slot(a, SL_B)[tile] = bb;
+        ts.add(tile, bb);
     }
+    ts.flush();
 }
 
 // r = v, w = A v, z = s = p = 0; partials <r, r> -> G[par], <w, r> -> D[par].
@@ -360,6 +407,7 @@ __device__ void phase_pipe_init(const KArgs<Op> &a, double *sm) {
 template <class Op>
 __device__ void phase_pipe_start(const KArgs<Op> &a, const double *v, double *w, int par,
                                  double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, par ? SL_G1 : SL_G0), slot(a, par ? SL_D1 : SL_D0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0, d = 0.0;
@@ -374,13 +422,9 @@ __device__ void phase_pipe_start(const KArgs<Op> &a, const double *v, double *w,
             g = __dmul_rn(ri, ri);
             d = __dmul_rn(wi, ri);
         }
-        g = block_sum(g, sm);
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) {
-            slot(a, par ? SL_G1 : SL_G0)[tile] = g;
-            slot(a, par ? SL_D1 : SL_D0)[tile] = d;
-        }
+        ts.add(tile, g, d);
     }
+    ts.flush();
 }
 
 // One pipelined iteration, row-local once q = A w is known:
@@ -390,6 +434,7 @@ __device__ void phase_pipe_start(const KArgs<Op> &a, const double *v, double *w,
 template <class Op>
 __device__ void phase_pipe_step(const KArgs<Op> &a, const double *w, double *wn, double alpha,
                                 double beta, int nxt, double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, nxt ? SL_G1 : SL_G0), slot(a, nxt ? SL_D1 : SL_D0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0, d = 0.0;
@@ -410,13 +455,9 @@ __device__ void phase_pipe_step(const KArgs<Op> &a, const double *w, double *wn,
             g = __dmul_rn(ri, ri);
             d = __dmul_rn(wni, ri);
         }
-        g = block_sum(g, sm);
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) {
-            slot(a, nxt ? SL_G1 : SL_G0)[tile] = g;
-            slot(a, nxt ? SL_D1 : SL_D0)[tile] = d;
-        }
+        ts.add(tile, g, d);
     }
+    ts.flush();
 }
 
 // Residual replacement, first half: t = b - A x, s = A p.
@@ -436,6 +477,7 @@ __device__ void phase_replace_a(const KArgs<Op> &a) {
 // partials <r, r> -> G[par], <w, r> -> D[par].
 template <class Op>
 __device__ void phase_replace_b(const KArgs<Op> &a, double *w, int par, double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, par ? SL_G1 : SL_G0), slot(a, par ? SL_D1 : SL_D0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0, d = 0.0;
@@ -448,13 +490,9 @@ __device__ void phase_replace_b(const KArgs<Op> &a, double *w, int par, double *
             g = __dmul_rn(ri, ri);
             d = __dmul_rn(wi, ri);
         }
-        g = block_sum(g, sm);
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) {
-            slot(a, par ? SL_G1 : SL_G0)[tile] = g;
-            slot(a, par ? SL_D1 : SL_D0)[tile] = d;
-        }
+        ts.add(tile, g, d);
     }
+    ts.flush();
 }
 
 // Iterations between residual replacements in pipelined CG.
@@ -471,7 +509,7 @@ constexpr long long PIPE_REPLACE = 50;
 // extra barriers, four operator applications); the scalar recurrence goes on.
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     int site = 0;
     phase_pipe_init(a, sm);
     if (!grid_barrier(a.bar, gridDim.x, site++)) return;
@@ -539,6 +577,7 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_pipe_kernel(KArgs<Op> a) {
 // x = 0, t = b - A x0, partials ||t||^2 (SL_TT) and ||b||^2 (SL_B).
 template <class Op>
 __device__ void phase_mixed_init(const KArgs<Op> &a, double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, SL_TT), slot(a, SL_B));
     CFM_TILES(a) {
         CFM_ROW(a);
         double q = 0.0, bb = 0.0;
@@ -550,18 +589,15 @@ __device__ void phase_mixed_init(const KArgs<Op> &a, double *sm) {
             q = __dmul_rn(ti, ti);
             bb = __dmul_rn(bi, bi);
         }
-        q = block_sum(q, sm);
-        bb = block_sum(bb, sm);
-        if (threadIdx.x == 0) {
-            slot(a, SL_TT)[tile] = q;
-            slot(a, SL_B)[tile] = bb;
-        }
+        ts.add(tile, q, bb);
     }
+    ts.flush();
 }
 
 // Inner right-hand side r32 = fl32(t / |t|), p32 = r32, d32 = 0; <r32, r32> -> G0.
 template <class Op>
 __device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0;
@@ -572,13 +608,14 @@ __device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) 
             a.d32[i] = 0.f;
             g = xprod(ri, ri);
         }
-        g = block_sum(g, sm);
-        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+        ts.add(tile, g);
     }
+    ts.flush();
 }
 
 template <class Op>
 __device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_D0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double d = 0.0;
@@ -587,13 +624,14 @@ __device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
             a.s32[i] = si;
             d = xprod(a.p32[i], si);
         }
-        d = block_sum(d, sm);
-        if (threadIdx.x == 0) slot(a, SL_D0)[tile] = d;
+        ts.add(tile, d);
     }
+    ts.flush();
 }
 
 template <class Op>
 __device__ void phase_inner_update(const KArgs<Op> &a, float af, double *sm) {
+    TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
     CFM_TILES(a) {
         CFM_ROW(a);
         double g = 0.0;
@@ -603,9 +641,9 @@ __device__ void phase_inner_update(const KArgs<Op> &a, float af, double *sm) {
             a.r32[i] = ri;
             g = xprod(ri, ri);
         }
-        g = block_sum(g, sm);
-        if (threadIdx.x == 0) slot(a, SL_G0)[tile] = g;
+        ts.add(tile, g);
     }
+    ts.flush();
 }
 
 template <class Op>
@@ -633,7 +671,7 @@ __device__ void phase_correct(const KArgs<Op> &a, double norm) {
 // maxiter caps the inner steps over all sweeps.
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     int site = 0;
     phase_mixed_init(a, sm);
     if (!grid_barrier(a.bar, gridDim.x, site++)) return;
@@ -695,22 +733,22 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
 // One kernel per operation (the comparator of CG/src/common.cu:458-531).
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE) k_init(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     phase_init(a, sm);
 }
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE) k_spmv_dot(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     phase_spmv_dot(a, sm);
 }
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE) k_update(KArgs<Op> a, double alpha) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     phase_update(a, alpha, sm);
 }
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE) k_true_residual(KArgs<Op> a) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     phase_true_residual(a, sm);
 }
 template <class Op>
@@ -724,7 +762,7 @@ __global__ void __launch_bounds__(CG_TILE) k_p(KArgs<Op> a, double beta) {
 // Single block: reduce partial slot `which` into out[which].
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE) k_reduce(KArgs<Op> a, int which, double *out) {
-    __shared__ double sm[33];
+    __shared__ double sm[TS_SMEM];
     const double v = sum_partials(slot(a, which), a.ntiles, sm);
     if (threadIdx.x == 0) out[which] = v;
 }

@@ -59,6 +59,63 @@ def test_csr_new_solvers_bitexact(impl, g):
     np.testing.assert_array_equal(x, xo)
 
 
+def banded_spd(n, seed):
+    """Symmetric, diagonally dominant band matrix whose half-bandwidth steps
+    through 1..5 every 40 rows: row lengths 2..11, similar within a slice."""
+    rng = np.random.default_rng(seed)
+    h = 1 + (np.arange(n) // 40) % 5
+    rows = [[] for _ in range(n)]
+    for i in range(n):
+        for j in range(i + 1, min(n, i + h[i] + 1)):
+            v = -rng.uniform(0.1, 1.0)
+            rows[i].append((j, v))
+            rows[j].append((i, v))
+    rowptr, col, val = [0], [], []
+    for i in range(n):
+        ent = sorted(rows[i] + [(i, 1.0 - sum(v for _, v in rows[i]))])
+        col += [c for c, _ in ent]
+        val += [v for _, v in ent]
+        rowptr.append(len(col))
+    return np.array(rowptr, np.int32), np.array(col, np.int32), np.array(val)
+
+
+def arrow_spd(n):
+    """Row and column 0 full (-1), tridiagonal -1 elsewhere: one row n
+    entries long among rows of 2 and 3."""
+    rowptr, col, val = [0], [], []
+    for i in range(n):
+        ent = {0: -1.0} if i else {j: -1.0 for j in range(n)}
+        if i > 1:
+            ent[i - 1] = -1.0
+        if 0 < i < n - 1:
+            ent[i + 1] = -1.0
+        ent[i] = 2.0 * n if i == 0 else 4.0
+        for c in sorted(ent):
+            col.append(c)
+            val.append(ent[c])
+        rowptr.append(len(col))
+    return np.array(rowptr, np.int32), np.array(col, np.int32), np.array(val)
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("kind", ["banded", "arrow", "poisson"])
+def test_csr_uneven_rows_bitexact(impl, kind):
+    """Uneven rows (2..11 entries, or one full row), n not a multiple of 32:
+    every solver gives the oracle's SpMV, x, iteration count and
+    refinements bit for bit."""
+    rowptr, col, val = {"banded": lambda: banded_spd(1007, 5), "arrow": lambda: arrow_spd(301),
+                        "poisson": lambda: cfm.poisson3d(11)}[kind]()
+    A = cfm.CSR(rowptr, col, val)
+    xs = cfm.uniform(6, A.n)
+    np.testing.assert_array_equal(A.spmv(xs), oracle.spmv(rowptr, col, val, xs))
+    b = oracle.spmv(rowptr, col, val, xs)
+    xo, st_o, it_o, rs_o, _ = oracle.krylov_csr(rowptr, col, val, b, METHOD[impl], 20000, 1e-8)
+    x, st = cfm.CG(A, impl, 20000, 1e-8).solve(b)
+    assert st_o == 0 and st.status == cfm.OK
+    assert st.iterations == it_o and st.refinements == rs_o
+    np.testing.assert_array_equal(x, xo)
+
+
 def test_pipelined_fixed_count_reference_mode():
     """-niter semantics: exactly maxiter pipelined iterations, b = ones."""
     rowptr, col, val = cfm.tridiag(3000)
