@@ -238,21 +238,50 @@ def workload_unet(args, cfm):
          dtype="bf16")
 
 
+def batch_bytes_per_iteration(dims, n, smooth, word):
+    """Algorithmic bytes of one PCG iteration of one batched system: the
+    operator pass (c coefficient arrays + p read + s write), the x / r update
+    (4 reads, 2 writes), the damped-Jacobi sweeps (first: r, d read, z write;
+    each further one: z, r and the c arrays read, z written; <r, z> fused into
+    the last) and p = z + beta p (2 reads, 1 write); c = dims + 1."""
+    c = dims + 1
+    sweeps = 3 + max(0, smooth - 1) * (c + 3)
+    return word * n * ((c + 2) + 6 + sweeps + 3)
+
+
 def workload_batch256(args, cfm):
     import numpy as np
     t0 = time.perf_counter()
     systems = cfm.uneven_systems(192, 64, seed=5)
     gen_s = time.perf_counter() - t0
+    peak, kind = peak_hbm()
     B = cfm.Batch(systems)
-    B.set_solver(smooth=4, maxiter=20000, tol=1e-8)
-    tune_ms = B.autotune()
-    for _ in range(args.warmup):
-        B.solve()
-    ts = []
-    for _ in range(args.steps):
-        it, stt, rr, st = B.solve()
-        ts.append(st.seconds)
-    t = statistics.median(ts)
+    smooth = 4
+    B.set_solver(smooth=smooth, maxiter=20000, tol=1e-8)
+    methods = {}
+    for name, prec, delta, word in (("pcg_fp64", cfm.FP64, 0.1, 8),
+                                    ("pcg_fp32_fp64_reliable_updates_delta0.1", cfm.FP32, 0.1, 4),
+                                    ("pcg_fp32_fp64_reliable_updates_delta0.01", cfm.FP32, 0.01, 4)):
+        B.set_precision(prec, 0, delta)
+        tune_ms = B.autotune()
+        for _ in range(args.warmup):
+            B.solve()
+        ts = []
+        for _ in range(args.steps):
+            it, stt, rr, st = B.solve()
+            ts.append(st.seconds)
+        t = statistics.median(ts)
+        nbytes = sum(batch_bytes_per_iteration(k.ndim, k.size, smooth, word) * int(v)
+                     for (k, _), v in zip(systems, it))
+        methods[name] = {"ms": t * 1e3, "solves_per_s": len(systems) / t,
+                         "all_converged": bool((stt == cfm.OK).all()), "max_true_relres": float(rr.max()),
+                         "iterations": {"min": int(it.min()), "median": float(np.median(it)),
+                                        "max": int(it.max()), "sum": int(it.sum())},
+                         "fp64_updates": int(st.refinements),
+                         "algorithmic_gbs": nbytes / t * 1e-9, "hbm_frac": nbytes / t * 1e-9 / peak,
+                         "autotune_best_ms": tune_ms, "per_system_iterations": [int(v) for v in it]}
+    best = min(methods, key=lambda m: methods[m]["ms"])
+    t = methods[best]["ms"] * 1e-3
     # one plain persistent FP64 CG solve per launch, same tolerance
     t_plain, it_plain = 0.0, []
     for k, f in systems:
@@ -264,16 +293,13 @@ def workload_batch256(args, cfm):
     line("256 uneven variable-coefficient systems to 1e-8: aggregate solves/s", n / t, "solves/s", args,
          t * 1e3, {"workload": "batch_192x2d_64..512_64x3d_32..128_varcoef_tol1e-8",
                    "systems": n, "cells": int(sum(k.size for k, _ in systems)),
-                   "batched_ms": t * 1e3, "all_converged": bool((stt == cfm.OK).all()),
-                   "max_true_relres": float(rr.max()),
-                   "iterations_batched": {"min": int(it.min()), "median": float(np.median(it)), "max": int(it.max())},
+                   "method": best, "methods": methods,
                    "iterations_plain": {"min": int(min(it_plain)), "median": float(np.median(it_plain)),
                                         "max": int(max(it_plain))},
-                   "per_system_iterations": [int(v) for v in it],
                    "plain_one_solve_per_launch_ms": t_plain * 1e3,
                    "speedup_vs_one_plain_solve_per_launch": t_plain / t,
-                   "autotune_best_ms": tune_ms, "generation_s": gen_s,
-                   "method": "PCG FP64, 4 damped-Jacobi sweeps, one cooperative launch in a CUDA graph"})
+                   "generation_s": gen_s, "peak_hbm_gbs": peak, "peak_kind": kind,
+                   "launch": "one cooperative launch in a CUDA graph per step; 4 damped-Jacobi sweeps"})
 
 
 def main_workload(args):

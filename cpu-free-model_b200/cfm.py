@@ -87,6 +87,7 @@ _SIGS = {
     "cfm_batch_destroy": (None, [_vp]),
     "cfm_batch_set_plan": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
     "cfm_batch_set_solver": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_double]),
+    "cfm_batch_set_precision": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_double]),
     "cfm_batch_solve": (_c.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "cfm_batch_solution": (_c.c_int, [_vp, _c.c_int, _vp]),
     "cfm_batch_autotune": (_c.c_int, [_vp, _vp]),
@@ -626,6 +627,13 @@ class Batch:
 
     def set_solver(self, smooth=4, maxiter=20000, tol=1e-8):
         check("cfm_batch_set_solver", lib.cfm_batch_set_solver(self.h, smooth, maxiter, tol))
+
+    def set_precision(self, precision, inner_maxiter=0, inner_tol=0.1):
+        """FP64, or FP32 (FP32 PCG with FP64 reliable updates: inner_tol is
+        the residual drop that triggers one, inner_maxiter caps the steps
+        between two)."""
+        check("cfm_batch_set_precision", lib.cfm_batch_set_precision(self.h, precision, inner_maxiter,
+                                                                     inner_tol))
 
     def set_plan(self, thresholds, teams):
         t = np.ascontiguousarray(thresholds, np.int64)

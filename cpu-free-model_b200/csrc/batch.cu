@@ -46,7 +46,7 @@ struct BtSys {
 struct BtOut {
     long long iters;
     int status;
-    int pad;
+    int sweeps;     // FP64 reliable updates (mixed precision); 0 in FP64
     double rr, bb;  // final recursive |r|^2, |b|^2
 };
 
@@ -69,6 +69,11 @@ struct BtArgs {
     int smooth;
     int maxiter;
     double tol;
+    // FP32 iteration with FP64 reliable updates (batch_kernel<true>)
+    const float *we32, *wn32, *wt32, *dg32;  // FP32 copies of the coefficients
+    float *r32, *p32, *s32, *z32, *y32, *d32; // FP32 inner vectors
+    int inner_maxiter;                        // 0: no cap per sweep
+    double inner_tol;
 };
 
 __device__ __forceinline__ double bt_apply(const BtArgs &a, const BtSys &S, const double *x,
@@ -90,6 +95,26 @@ __device__ __forceinline__ double bt_apply(const BtArgs &a, const BtSys &S, cons
     return t;
 }
 
+// A x in FP32 from the FP32 coefficient copies (same neighbour order).
+__device__ __forceinline__ float bt_apply32(const BtArgs &a, const BtSys &S, const float *x,
+                                            long long i) {
+    const long long g = S.off + i;
+    const int nx = S.nx, ny = S.ny;
+    const int ix = (int)(i % nx), q = (int)(i / nx), iy = q % ny;
+    float t = a.dg32[g] * x[g];
+    if (ix > 0) t = fmaf(-a.we32[g - 1], x[g - 1], t);
+    if (ix < nx - 1) t = fmaf(-a.we32[g], x[g + 1], t);
+    if (iy > 0) t = fmaf(-a.wn32[g - nx], x[g - nx], t);
+    if (iy < ny - 1) t = fmaf(-a.wn32[g], x[g + nx], t);
+    if (S.dims == 3) {
+        const int iz = q / ny;
+        const long long P = (long long)nx * ny;
+        if (iz > 0) t = fmaf(-a.wt32[g - P], x[g - P], t);
+        if (iz < S.nz - 1) t = fmaf(-a.wt32[g], x[g + P], t);
+    }
+    return t;
+}
+
 // Sum of one partial slot over the system's tiles (fixed order).
 __device__ __forceinline__ double bt_sum(const BtArgs &a, const BtSys &S, int slot, double *sm) {
     const double *pp = a.part + S.poff + (long long)slot * S.ntiles;
@@ -98,43 +123,238 @@ __device__ __forceinline__ double bt_sum(const BtArgs &a, const BtSys &S, int sl
     return block_sum(acc, sm);
 }
 
-// Preconditioner z = J_m(r) over the team's tiles; m sweeps need a team
-// barrier between them (z is read at neighbours).  Returns false on timeout.
-// On exit the result is in a.z.
+// r_i z_i for the <r, z> partials: the FP64 product, or the exact product
+// of two FP32 values as FP64.
+__device__ __forceinline__ double bt_prod(double u, double v) { return u * v; }
+__device__ __forceinline__ double bt_prod(float u, float v) { return (double)u * (double)v; }
+
+struct BtApply64 {
+    __device__ __forceinline__ double operator()(const BtArgs &a, const BtSys &S, const double *x,
+                                                 long long i) const {
+        return bt_apply(a, S, x, i);
+    }
+};
+struct BtApply32 {
+    __device__ __forceinline__ float operator()(const BtArgs &a, const BtSys &S, const float *x,
+                                                long long i) const {
+        return bt_apply32(a, S, x, i);
+    }
+};
+
+// Preconditioner z = J_m(r) over the team's tiles (damped Jacobi from
+// z = 0: the first sweep is w r / d, or r / d for smooth = 0), with the
+// <r, z> partials of the result into slot 0 and, when pcopy is set, p = z,
+// both in the last sweep.  Sweeps read z at neighbours, so a team barrier
+// separates them; the sweeps alternate between z and z2, starting in the
+// one that leaves the result in z.  Returns false on a barrier timeout.
+template <class V, class Apply>
 __device__ bool bt_precond(const BtArgs &a, const BtSys &S, int rank, int T, BarrierState *bar,
-                           int &site) {
-    if (a.smooth <= 0) {
+                           int &site, double *sm, const V *r, V *z, V *z2, const V *dg,
+                           V *pcopy) {
+    const V w = (V)BT_OMEGA;
+    const int extra = a.smooth > 1 ? a.smooth - 1 : 0;
+    V *src = nullptr, *dst = (extra & 1) ? z2 : z;
+    for (int m = 0; m <= extra; ++m) {
+        if (m > 0 && !grid_barrier(bar, T, site++)) return false;
+        const bool last = m == extra;
+        TileSums<1> ts(sm, T, a.part + S.poff);
         for (int tile = rank; tile < S.ntiles; tile += T) {
             const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            if (i < S.n) a.z[S.off + i] = a.r[S.off + i] / a.dg[S.off + i];
+            double q = 0.0;
+            if (i < S.n) {
+                const long long g = S.off + i;
+                V zi;
+                if (m == 0)
+                    zi = a.smooth <= 0 ? r[g] / dg[g] : w * r[g] / dg[g];
+                else
+                    zi = src[g] + w * (r[g] - Apply()(a, S, src, i)) / dg[g];
+                dst[g] = zi;
+                if (last) {
+                    if (pcopy) pcopy[g] = zi;
+                    q = bt_prod(r[g], zi);
+                }
+            }
+            if (last) ts.add(tile, q);
         }
-        return true;
+        if (last) ts.flush();
+        src = dst;
+        dst = dst == z ? z2 : z;
     }
-    double *src = a.z, *dst = a.z2;
-    // sweep 1 from z = 0 writes z directly
-    for (int tile = rank; tile < S.ntiles; tile += T) {
-        const long long i = (long long)tile * CG_TILE + threadIdx.x;
-        if (i < S.n) a.z[S.off + i] = BT_OMEGA * a.r[S.off + i] / a.dg[S.off + i];
+    return true;
+}
+
+// Mixed-precision PCG with reliable updates for one system.  The iteration
+// runs in FP32 (FP32 operator, preconditioner and vectors r, z, p, s; dots
+// as FP64 sums of exact FP32 products; alpha, beta in FP64, applied rounded
+// to FP32) and gathers its steps in an FP32 correction d.  When the
+// recursive residual falls below the tolerance, below delta times its
+// largest norm since the last update (a.inner_tol = delta), or after
+// a.inner_maxiter steps (0: no cap), the update folds d into x in FP64 and
+// replaces r by the FP64 true residual t = b - A x (rounded to FP32); the
+// search direction p is kept, so the Krylov recurrence goes on instead of
+// restarting (residual replacement as in Sleijpen and van der Vorst's
+// reliable updates).  It stops when |t| <= tol |b| in FP64.  The FP64 r
+// array holds t.  Slots: 0 <r, z>, 1 <p, s>, 2 <r, r>, 3 <b, b> then <t, t>.
+__device__ bool bt_solve_mixed(const BtArgs &a, int sid, int rank, int T, BarrierState *bar,
+                               double *sm) {
+    const BtSys S = a.sys[sid];
+    int site = 0;
+    double *part = a.part + S.poff;
+    double *t64 = a.r;
+    // x = 0, d = 0, r = fl32(b); |b|^2, |r|^2
+    {
+        TileSums<2> ts(sm, T, part + 3 * S.ntiles, part + 2 * S.ntiles);
+        for (int tile = rank; tile < S.ntiles; tile += T) {
+            const long long i = (long long)tile * CG_TILE + threadIdx.x;
+            double bb = 0.0, q = 0.0;
+            if (i < S.n) {
+                const long long g = S.off + i;
+                const double bi = a.b[g];
+                const float ri = (float)bi;
+                a.x[g] = 0.0;
+                a.d32[g] = 0.f;
+                a.r32[g] = ri;
+                bb = bi * bi;
+                q = bt_prod(ri, ri);
+            }
+            ts.add(tile, bb, q);
+        }
+        ts.flush();
     }
-    for (int m = 1; m < a.smooth; ++m) {
+    // z = M r, p = z, <r, z>
+    if (!bt_precond<float, BtApply32>(a, S, rank, T, bar, site, sm, a.r32, a.z32, a.y32, a.dg32,
+                                      a.p32))
+        return false;
+    if (!grid_barrier(bar, T, site++)) return false;
+    const double bb = bt_sum(a, S, 3, sm);
+    const double target2 = a.tol * a.tol * bb;
+    const double delta2 = a.inner_tol * a.inner_tol;
+    double rr = bt_sum(a, S, 2, sm), rz = bt_sum(a, S, 0, sm);
+    double tt = bb, rmax2 = rr;
+    long long k = 0;
+    int updates = 0, since = 0, status = CFM_NOT_CONVERGED;
+    if (tt <= target2) status = CFM_OK;
+    while (status != CFM_OK && k < a.maxiter) {
+        // s = A p; <p, s>
+        {
+            TileSums<1> ts(sm, T, part + S.ntiles);
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                double q = 0.0;
+                if (i < S.n) {
+                    const long long g = S.off + i;
+                    const float si = bt_apply32(a, S, a.p32, i);
+                    a.s32[g] = si;
+                    q = bt_prod(a.p32[g], si);
+                }
+                ts.add(tile, q);
+            }
+            ts.flush();
+        }
         if (!grid_barrier(bar, T, site++)) return false;
+        const double ps = bt_sum(a, S, 1, sm);
+        const double alpha = rz / ps;
+        if (!(ps > 0.0 && isfinite(alpha))) {
+            status = CFM_BREAKDOWN;
+            break;
+        }
+        const float af = (float)alpha;
+        // d += alpha p; r -= alpha s; |r|^2
+        {
+            TileSums<1> ts(sm, T, part + 2 * S.ntiles);
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                double q = 0.0;
+                if (i < S.n) {
+                    const long long g = S.off + i;
+                    a.d32[g] = fmaf(af, a.p32[g], a.d32[g]);
+                    const float ri = fmaf(-af, a.s32[g], a.r32[g]);
+                    a.r32[g] = ri;
+                    q = bt_prod(ri, ri);
+                }
+                ts.add(tile, q);
+            }
+            ts.flush();
+        }
+        ++k;
+        ++since;
+        if (!grid_barrier(bar, T, site++)) return false;
+        rr = bt_sum(a, S, 2, sm);
+        if (rr <= target2 || rr < delta2 * rmax2 || k >= a.maxiter ||
+            (a.inner_maxiter > 0 && since >= a.inner_maxiter)) {
+            // reliable update: x += d (FP64), d = 0
+            for (int tile = rank; tile < S.ntiles; tile += T) {
+                const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                if (i < S.n) {
+                    const long long g = S.off + i;
+                    a.x[g] += (double)a.d32[g];
+                    a.d32[g] = 0.f;
+                }
+            }
+            if (!grid_barrier(bar, T, site++)) return false;
+            // t = b - A x (FP64), r = fl32(t); |t|^2, |r|^2
+            {
+                TileSums<2> ts(sm, T, part + 3 * S.ntiles, part + 2 * S.ntiles);
+                for (int tile = rank; tile < S.ntiles; tile += T) {
+                    const long long i = (long long)tile * CG_TILE + threadIdx.x;
+                    double q = 0.0, q32 = 0.0;
+                    if (i < S.n) {
+                        const long long g = S.off + i;
+                        const double ti = a.b[g] - bt_apply(a, S, a.x, i);
+                        const float ri = (float)ti;
+                        t64[g] = ti;
+                        a.r32[g] = ri;
+                        q = ti * ti;
+                        q32 = bt_prod(ri, ri);
+                    }
+                    ts.add(tile, q, q32);
+                }
+                ts.flush();
+            }
+            if (!grid_barrier(bar, T, site++)) return false;
+            tt = bt_sum(a, S, 3, sm);
+            rr = bt_sum(a, S, 2, sm);
+            ++updates;
+            since = 0;
+            rmax2 = rr;
+            if (tt <= target2) {
+                status = CFM_OK;
+                break;
+            }
+            if (k >= a.maxiter) break;
+        } else if (rr > rmax2) {
+            rmax2 = rr;
+        }
+        // z = M r, <r, z>
+        if (!bt_precond<float, BtApply32>(a, S, rank, T, bar, site, sm, a.r32, a.z32, a.y32,
+                                          a.dg32, nullptr))
+            return false;
+        if (!grid_barrier(bar, T, site++)) return false;
+        const double rz1 = bt_sum(a, S, 0, sm);
+        const float bf = (float)(rz1 / rz);
+        rz = rz1;
+        // p = z + beta p
         for (int tile = rank; tile < S.ntiles; tile += T) {
             const long long i = (long long)tile * CG_TILE + threadIdx.x;
             if (i < S.n) {
                 const long long g = S.off + i;
-                dst[g] = src[g] + BT_OMEGA * (a.r[g] - bt_apply(a, S, src, i)) / a.dg[g];
+                a.p32[g] = fmaf(bf, a.p32[g], a.z32[g]);
             }
         }
-        double *t = src;
-        src = dst;
-        dst = t;
-    }
-    if (src != a.z) {  // odd number of extra sweeps: copy back into z
         if (!grid_barrier(bar, T, site++)) return false;
+    }
+    if (since > 0) {  // a breakdown left steps in d
         for (int tile = rank; tile < S.ntiles; tile += T) {
             const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            if (i < S.n) a.z[S.off + i] = src[S.off + i];
+            if (i < S.n) a.x[S.off + i] += (double)a.d32[S.off + i];
         }
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        a.out[sid].iters = k;
+        a.out[sid].status = status;
+        a.out[sid].sweeps = updates;
+        a.out[sid].rr = tt;
+        a.out[sid].bb = bb;
     }
     return true;
 }
@@ -162,22 +382,9 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
         }
         ts.flush();
     }
-    if (!bt_precond(a, S, rank, T, bar, site)) return false;
-    // p = z; <r, z>
-    {
-        TileSums<1> ts(sm, T, part);
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            double rz = 0.0;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                a.p[g] = a.z[g];
-                rz = a.r[g] * a.z[g];
-            }
-            ts.add(tile, rz);
-        }
-        ts.flush();
-    }
+    // z = M r, p = z, <r, z>
+    if (!bt_precond<double, BtApply64>(a, S, rank, T, bar, site, sm, a.r, a.z, a.z2, a.dg, a.p))
+        return false;
     if (!grid_barrier(bar, T, site++)) return false;
     const double bb = bt_sum(a, S, 3, sm);
     double rz = bt_sum(a, S, 0, sm);
@@ -234,19 +441,10 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
             status = CFM_OK;
             break;
         }
-        if (!bt_precond(a, S, rank, T, bar, site)) return false;
-        if (a.smooth > 0 && !grid_barrier(bar, T, site++)) return false;
-        // <r, z>
-        {
-            TileSums<1> ts(sm, T, part);
-            for (int tile = rank; tile < S.ntiles; tile += T) {
-                const long long i = (long long)tile * CG_TILE + threadIdx.x;
-                double q = 0.0;
-                if (i < S.n) q = a.r[S.off + i] * a.z[S.off + i];
-                ts.add(tile, q);
-            }
-            ts.flush();
-        }
+        // z = M r, <r, z>
+        if (!bt_precond<double, BtApply64>(a, S, rank, T, bar, site, sm, a.r, a.z, a.z2, a.dg,
+                                           nullptr))
+            return false;
         if (!grid_barrier(bar, T, site++)) return false;
         const double rz1 = bt_sum(a, S, 0, sm);
         const double beta = rz1 / rz;
@@ -264,12 +462,14 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
     if (rank == 0 && threadIdx.x == 0) {
         a.out[sid].iters = k;
         a.out[sid].status = status;
+        a.out[sid].sweeps = 0;
         a.out[sid].rr = rr;
         a.out[sid].bb = bb;
     }
     return true;
 }
 
+template <bool MIXED>
 __global__ void __launch_bounds__(CG_TILE, 1) batch_kernel(BtArgs a) {
     __shared__ double sm[TS_SMEM];
     __shared__ int s_sys;
@@ -289,7 +489,8 @@ __global__ void __launch_bounds__(CG_TILE, 1) batch_kernel(BtArgs a) {
         __syncthreads();
         const int sid = s_sys;
         if (sid < 0) return;
-        if (!bt_solve(a, sid, rank, T, bar, sm)) return;
+        if (!(MIXED ? bt_solve_mixed(a, sid, rank, T, bar, sm) : bt_solve(a, sid, rank, T, bar, sm)))
+            return;
         // everyone has read team_sys before the leader overwrites it
         if (!grid_barrier(bar, T, -2)) return;
     }
@@ -305,6 +506,12 @@ __global__ void batch_reset(BarrierState *bars, int nteams, int *qnext, int ncls
         bars[t].timeout_ns = timeout_ns;
     }
     if (blockIdx.x == 0 && threadIdx.x < ncls) qnext[threadIdx.x] = 0;
+}
+
+__global__ void batch_to_f32(const double *in, float *out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
 }
 
 // True residual of every system: rr_true[s] += |b - A x|^2 (atomics).
@@ -350,9 +557,27 @@ struct cfm_batch {
     long long thr[BT_MAXCLS] = {};
     int smooth = 4, maxiter = 20000;
     double tol = 1e-8;
+    // FP32 iteration with FP64 reliable updates
+    bool mixed = false;
+    int inner_maxiter = 0;
+    double inner_tol = 0.1;
+    float *coef32 = nullptr;  // we | wn | wt | dg in FP32 (4 ntot)
+    float *vec32 = nullptr;   // r p s z y d in FP32   (6 ntot)
 };
 
 namespace {
+
+// Drop the captured graph (the launch it holds no longer matches).
+void drop_graph(cfm_batch *h) {
+    if (h->exec) {
+        cudaGraphExecDestroy(h->exec);
+        h->exec = nullptr;
+    }
+    if (h->graph) {
+        cudaGraphDestroy(h->graph);
+        h->graph = nullptr;
+    }
+}
 
 // Classes by size: class c holds systems with n >= thr[c] (thr descending,
 // thr[ncls-1] = 0); blocks are shared out in proportion to each class's
@@ -407,14 +632,7 @@ int plan(cfm_batch *h, int ncls, const long long *thr, const int *team, int bloc
     h->ncls = ncls;
     h->blocks = b0;
     h->nteams = t0;
-    if (h->exec) {
-        cudaGraphExecDestroy(h->exec);
-        h->exec = nullptr;
-    }
-    if (h->graph) {
-        cudaGraphDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    drop_graph(h);
     if (h->order) cudaFree(h->order);
     if (h->bars) cudaFree(h->bars);
     if (h->team_sys) cudaFree(h->team_sys);
@@ -460,8 +678,23 @@ BtArgs bt_args(cfm_batch *h) {
     a.smooth = h->smooth;
     a.maxiter = h->maxiter;
     a.tol = h->tol;
+    if (h->coef32 && h->vec32) {
+        a.we32 = h->coef32;
+        a.wn32 = h->coef32 + N;
+        a.wt32 = h->coef32 + 2 * N;
+        a.dg32 = h->coef32 + 3 * N;
+        a.r32 = h->vec32;
+        a.p32 = h->vec32 + N;
+        a.s32 = h->vec32 + 2 * N;
+        a.z32 = h->vec32 + 3 * N;
+        a.y32 = h->vec32 + 4 * N;
+        a.d32 = h->vec32 + 5 * N;
+    }
+    a.inner_maxiter = h->inner_maxiter;
+    a.inner_tol = h->inner_tol;
     return a;
 }
+
 
 // Reset + the persistent launch, on h->stream (capturable).
 int enqueue(cfm_batch *h) {
@@ -478,7 +711,10 @@ int enqueue(cfm_batch *h) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CFM_CUDA_TRY(cudaLaunchKernelEx(&cfg, batch_kernel, a));
+    if (h->mixed)
+        CFM_CUDA_TRY(cudaLaunchKernelEx(&cfg, batch_kernel<true>, a));
+    else
+        CFM_CUDA_TRY(cudaLaunchKernelEx(&cfg, batch_kernel<false>, a));
     return CFM_OK;
 }
 
@@ -519,9 +755,12 @@ int resident_blocks(int *out) {
     DeviceInfo di;
     int st = current_device_info(&di);
     if (st) return st;
-    int per_sm = 0;
-    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, CG_TILE, 0));
-    *out = per_sm * di.num_sms;
+    int per_sm64 = 0, per_sm32 = 0;
+    CFM_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm64, batch_kernel<false>, CG_TILE, 0));
+    CFM_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, batch_kernel<true>, CG_TILE, 0));
+    *out = std::min(per_sm64, per_sm32) * di.num_sms;
     return CFM_OK;
 }
 
@@ -630,6 +869,8 @@ void cfm_batch_destroy(cfm_batch *h) {
     cudaFree(h->bars);
     cudaFree(h->team_sys);
     cudaFree(h->rr_true);
+    cudaFree(h->coef32);
+    cudaFree(h->vec32);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -653,14 +894,36 @@ int cfm_batch_set_solver(cfm_batch *h, int smooth, int maxiter, double tol) {
     h->smooth = smooth;
     h->maxiter = maxiter;
     h->tol = tol;
-    if (h->exec) {
-        cudaGraphExecDestroy(h->exec);
-        h->exec = nullptr;
+    drop_graph(h);
+    return CFM_OK;
+}
+
+int cfm_batch_set_precision(cfm_batch *h, int precision, int inner_maxiter, double inner_tol) {
+    clear_error();
+    CFM_ARG_CHECK(h && (precision == CFM_FP64 || precision == CFM_FP32), "precision");
+    CFM_ARG_CHECK(inner_maxiter >= 0 && inner_tol >= 0 && inner_tol < 1,
+                  "inner_maxiter >= 0, 0 <= inner_tol < 1");
+    if (precision == CFM_FP32 && !h->coef32) {
+        const long long N = h->ntot;
+        cudaError_t e;
+        if ((e = cudaMalloc(&h->coef32, sizeof(float) * 4 * N)) != cudaSuccess ||
+            (e = cudaMalloc(&h->vec32, sizeof(float) * 6 * N)) != cudaSuccess) {
+            cudaFree(h->coef32);
+            cudaFree(h->vec32);
+            h->coef32 = nullptr;
+            h->vec32 = nullptr;
+            set_error("batch FP32 arrays: %s", cudaGetErrorString(e));
+            cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+        }
+        batch_to_f32<<<1024, 256, 0, h->stream>>>(h->coef, h->coef32, 4 * N);
+        CFM_CUDA_TRY(cudaGetLastError());
+        CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     }
-    if (h->graph) {
-        cudaGraphDestroy(h->graph);
-        h->graph = nullptr;
-    }
+    h->mixed = precision == CFM_FP32;
+    h->inner_maxiter = inner_maxiter;
+    h->inner_tol = inner_tol > 0 ? inner_tol : 0.1;
+    drop_graph(h);
     return CFM_OK;
 }
 
@@ -686,13 +949,14 @@ int cfm_batch_solve(cfm_batch *h, long long *iters, int *status, double *relres,
         CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     }
     int worst = CFM_OK;
-    long long total = 0;
+    long long total = 0, sweeps = 0;
     for (int i = 0; i < h->nsys; ++i) {
         if (iters) iters[i] = o[i].iters;
         if (status) status[i] = o[i].status;
         if (relres) relres[i] = o[i].bb > 0 ? std::sqrt(rt[i] / o[i].bb) : std::sqrt(rt[i]);
         if (o[i].status != CFM_OK) worst = o[i].status;
         total += o[i].iters;
+        sweeps += o[i].sweeps;
     }
     if (st) {
         std::memset(st, 0, sizeof(*st));
@@ -700,6 +964,7 @@ int cfm_batch_solve(cfm_batch *h, long long *iters, int *status, double *relres,
         st->iterations = total;
         st->launches = 2;
         st->status = worst;
+        st->refinements = sweeps;
     }
     return worst;
 }

@@ -397,8 +397,9 @@ int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out
  * uneven sizes) solved in ONE persistent cooperative launch captured in a
  * CUDA graph (no reference counterpart).  The resident blocks form teams
  * per size class; each team takes systems from its class queue (largest
- * first) and solves them with PCG (FP64, damped-Jacobi polynomial
- * preconditioner) behind team-local bounded barriers.  System i: dims[i],
+ * first) and solves them with PCG (FP64, or FP32 inside FP64 refinement:
+ * cfm_batch_set_precision; damped-Jacobi polynomial preconditioner) behind
+ * team-local bounded barriers.  System i: dims[i],
  * nx/ny/nz[i] (nz ignored in 2D), cell coefficients k_host[i] and right-hand
  * side b_host[i] (x0 = 0). */
 typedef struct cfm_batch cfm_batch;
@@ -412,6 +413,18 @@ int cfm_batch_set_plan(cfm_batch *h, int ncls, const long long *thresholds, cons
 /* smooth damped Jacobi sweeps in the preconditioner (0 = diagonal scaling),
  * iteration cap, relative tolerance (defaults 4, 20000, 1e-8). */
 int cfm_batch_set_solver(cfm_batch *h, int smooth, int maxiter, double tol);
+/* CFM_FP64 (default): PCG in FP64.  CFM_FP32: mixed-precision PCG with
+ * reliable updates, per system in the same persistent launch: the iteration
+ * runs in FP32 (FP32 copies of the coefficients, FP32 preconditioner and
+ * vectors; dots as FP64 sums of exact FP32 products; alpha, beta in FP64)
+ * and gathers its steps in an FP32 correction; when the recursive residual
+ * falls below the tolerance, below inner_tol (0: 0.1) times its largest
+ * norm since the last update, or after inner_maxiter steps (0: no cap), the
+ * correction is added to x in FP64 and r is replaced by the FP64 true
+ * residual b - A x, keeping the search direction.  It stops on the FP64
+ * true residual |b - A x| <= tol |b|; stats->refinements = the sum of
+ * updates. */
+int cfm_batch_set_precision(cfm_batch *h, int precision, int inner_maxiter, double inner_tol);
 /* Solve all systems (one graph launch).  Per system (each array optional):
  * iterations, status, FP64 true relative residual; stats->seconds = device
  * time of the launch, stats->iterations = the sum of iterations. */

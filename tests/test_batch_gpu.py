@@ -57,3 +57,52 @@ def test_plans_and_autotune_do_not_change_results(batch):
     itC, _, _, st = B.solve()
     np.testing.assert_array_equal(itA, itC)
     assert ms > 0
+
+
+def test_mixed_precision_batch_reaches_fp64_tolerance(batch):
+    """FP32 PCG with FP64 reliable updates, in the same persistent launch:
+    every system reaches the FP64 true relative residual target, each needs
+    at least one update, the iteration counts stay within 25% of FP64 PCG
+    (the search direction survives the updates) and the solutions agree with
+    the FP64 batch to the tolerance's order."""
+    systems, B = batch
+    B.set_solver(smooth=4, maxiter=20000, tol=1e-8)
+    B.set_precision(cfm.FP64)
+    it64, stt64, rr64, _ = B.solve()
+    x64 = [B.solution(i) for i in range(len(systems))]
+    B.set_precision(cfm.FP32, 0, 0.1)
+    it, stt, rr, st = B.solve()
+    assert (stt == cfm.OK).all() and (rr <= 1e-8).all(), rr.max()
+    assert st.refinements >= len(systems) and st.iterations == it.sum()
+    assert it.sum() <= 1.25 * it64.sum(), (it.sum(), it64.sum())
+    for i in range(len(systems)):
+        x = B.solution(i)
+        assert np.linalg.norm(x - x64[i]) / np.linalg.norm(x64[i]) < 1e-6
+    # back to FP64: the same iterations and solutions as before, bit for bit
+    B.set_precision(cfm.FP64)
+    itB, _, _, stB = B.solve()
+    np.testing.assert_array_equal(itB, it64)
+    np.testing.assert_array_equal(B.solution(2), x64[2])
+    assert stB.refinements == 0
+
+
+def test_mixed_precision_plan_independent_and_inner_cap(batch):
+    systems, B = batch
+    B.set_solver(smooth=2, maxiter=20000, tol=1e-8)
+    B.set_precision(cfm.FP32, 0, 0.1)
+    B.set_plan([1 << 12, 0], [4, 1])
+    itA, sttA, _, stA = B.solve()
+    xA = B.solution(5)
+    B.set_plan([1 << 14, 1 << 10, 0], [8, 2, 1])
+    itB, _, _, stB = B.solve()
+    np.testing.assert_array_equal(itA, itB)
+    np.testing.assert_array_equal(xA, B.solution(5))
+    assert stA.refinements == stB.refinements
+    # an update at least every 5 steps still converges, with more updates
+    B.set_precision(cfm.FP32, 5, 0.1)
+    itC, sttC, rrC, stC = B.solve()
+    assert (sttC == cfm.OK).all() and (rrC <= 1e-8).all()
+    assert stC.refinements >= itC.sum() // 5 and stC.refinements > stA.refinements
+    B.set_precision(cfm.FP64)
+    with pytest.raises(cfm.CfmError):
+        B.set_precision(7)
