@@ -138,6 +138,48 @@ struct CsrOp {
         for (int j = rowptr[i]; j < j1; ++j) acc = __fmaf_rn(val32[j], x[col[j]], acc);
         return acc;
     }
+    // apply for rows i (if v1) and i2 (if v2), their entries interleaved so
+    // that both rows' loads are in flight together; 0 for an absent row.
+    template <class T>
+    __device__ __forceinline__ void apply2_t(const T *v, const T *x, int i, bool v1, int i2,
+                                             bool v2, T &y1, T &y2) const {
+        int j1 = 0, e1 = 0, j2 = 0, e2 = 0;
+        if (v1) {
+            j1 = rowptr[i];
+            e1 = rowptr[i + 1];
+        }
+        if (v2) {
+            j2 = rowptr[i2];
+            e2 = rowptr[i2 + 1];
+        }
+        T a1 = T(0), a2 = T(0);
+        while (j1 < e1 || j2 < e2) {
+            if (j1 < e1) {
+                a1 = fma_rn(v[j1], x[col[j1]], a1);
+                ++j1;
+            }
+            if (j2 < e2) {
+                a2 = fma_rn(v[j2], x[col[j2]], a2);
+                ++j2;
+            }
+        }
+        y1 = a1;
+        y2 = a2;
+    }
+    __device__ __forceinline__ static double fma_rn(double u, double w, double c) {
+        return __fma_rn(u, w, c);
+    }
+    __device__ __forceinline__ static float fma_rn(float u, float w, float c) {
+        return __fmaf_rn(u, w, c);
+    }
+    __device__ __forceinline__ void apply2(const double *x, int i, bool v1, int i2, bool v2,
+                                           double &y1, double &y2) const {
+        apply2_t(val, x, i, v1, i2, v2, y1, y2);
+    }
+    __device__ __forceinline__ void apply2_32(const float *x, int i, bool v1, int i2, bool v2,
+                                              float &y1, float &y2) const {
+        apply2_t(val32, x, i, v1, i2, v2, y1, y2);
+    }
     // A x0 with x0 = 0, summed like apply (always +0)
     __device__ __forceinline__ double apply_zero(int i) const {
         double acc = 0.0;
@@ -181,6 +223,16 @@ struct StencilOp {
         return t;
     }
     __device__ __forceinline__ double apply_zero(int) const { return 0.0; }
+    __device__ __forceinline__ void apply2(const double *x, int i, bool v1, int i2, bool v2,
+                                           double &y1, double &y2) const {
+        y1 = v1 ? apply(x, i) : 0.0;
+        y2 = v2 ? apply(x, i2) : 0.0;
+    }
+    __device__ __forceinline__ void apply2_32(const float *x, int i, bool v1, int i2, bool v2,
+                                              float &y1, float &y2) const {
+        y1 = v1 ? apply32(x, i) : 0.f;
+        y2 = v2 ? apply32(x, i2) : 0.f;
+    }
 };
 
 template <class Op>
@@ -207,6 +259,15 @@ struct KArgs {
 
 #define CFM_TILES(a) for (int tile = blockIdx.x; tile < (a).ntiles; tile += gridDim.x)
 #define CFM_ROW(a) const int i = tile * CG_TILE + threadIdx.x
+// Two of the block's tiles per step (tile, tile2 = tile + gridDim.x): the
+// loads of both rows go out before either row's arithmetic, halving the
+// chains of dependent memory round trips a warp waits on.
+#define CFM_TILE_PAIRS(a) for (int tile = blockIdx.x; tile < (a).ntiles; tile += 2 * (int)gridDim.x)
+#define CFM_ROW_PAIR(a)                                                      \
+    const int tile2 = tile + (int)gridDim.x;                                 \
+    const bool has2 = tile2 < (a).ntiles;                                    \
+    const int i = tile * CG_TILE + threadIdx.x, i2 = tile2 * CG_TILE + threadIdx.x; \
+    const bool v1 = i < (a).n, v2 = has2 && i2 < (a).n
 
 template <class Op>
 __device__ __forceinline__ double *slot(const KArgs<Op> &a, int s) {
@@ -237,15 +298,16 @@ __device__ void phase_init(const KArgs<Op> &a, double *sm) {
 template <class Op>
 __device__ void phase_spmv_dot(const KArgs<Op> &a, double *sm) {
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_D0));
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        double d = 0.0;
-        if (i < a.n) {
-            const double si = a.op.apply(a.p, i);
-            a.s[i] = si;
-            d = __dmul_rn(a.p[i], si);
-        }
-        ts.add(tile, d);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        double p1 = 0.0, p2 = 0.0, s1, s2;
+        if (v1) p1 = a.p[i];
+        if (v2) p2 = a.p[i2];
+        a.op.apply2(a.p, i, v1, i2, v2, s1, s2);
+        if (v1) a.s[i] = s1;
+        if (v2) a.s[i2] = s2;
+        ts.add(tile, v1 ? __dmul_rn(p1, s1) : 0.0);
+        if (has2) ts.add(tile2, v2 ? __dmul_rn(p2, s2) : 0.0);
     }
     ts.flush();
 }
@@ -253,16 +315,36 @@ __device__ void phase_spmv_dot(const KArgs<Op> &a, double *sm) {
 template <class Op>
 __device__ void phase_update(const KArgs<Op> &a, double alpha, double *sm) {
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        double g = 0.0;
-        if (i < a.n) {
-            a.x[i] = __fma_rn(alpha, a.p[i], a.x[i]);
-            const double ri = __fma_rn(-alpha, a.s[i], a.r[i]);
-            a.r[i] = ri;
-            g = __dmul_rn(ri, ri);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        double x1 = 0.0, p1 = 0.0, r1 = 0.0, s1 = 0.0, x2 = 0.0, p2 = 0.0, r2 = 0.0, s2 = 0.0;
+        if (v1) {
+            x1 = a.x[i];
+            p1 = a.p[i];
+            r1 = a.r[i];
+            s1 = a.s[i];
         }
-        ts.add(tile, g);
+        if (v2) {
+            x2 = a.x[i2];
+            p2 = a.p[i2];
+            r2 = a.r[i2];
+            s2 = a.s[i2];
+        }
+        double g1 = 0.0, g2 = 0.0;
+        if (v1) {
+            a.x[i] = __fma_rn(alpha, p1, x1);
+            const double ri = __fma_rn(-alpha, s1, r1);
+            a.r[i] = ri;
+            g1 = __dmul_rn(ri, ri);
+        }
+        if (v2) {
+            a.x[i2] = __fma_rn(alpha, p2, x2);
+            const double ri = __fma_rn(-alpha, s2, r2);
+            a.r[i2] = ri;
+            g2 = __dmul_rn(ri, ri);
+        }
+        ts.add(tile, g1);
+        if (has2) ts.add(tile2, g2);
     }
     ts.flush();
 }
@@ -307,9 +389,19 @@ __device__ void phase_restart(const KArgs<Op> &a) {
 
 template <class Op>
 __device__ void phase_p(const KArgs<Op> &a, double beta) {
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        if (i < a.n) a.p[i] = __fma_rn(beta, a.p[i], a.r[i]);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        double p1 = 0.0, r1 = 0.0, p2 = 0.0, r2 = 0.0;
+        if (v1) {
+            p1 = a.p[i];
+            r1 = a.r[i];
+        }
+        if (v2) {
+            p2 = a.p[i2];
+            r2 = a.r[i2];
+        }
+        if (v1) a.p[i] = __fma_rn(beta, p1, r1);
+        if (v2) a.p[i2] = __fma_rn(beta, p2, r2);
     }
 }
 
@@ -616,15 +708,16 @@ __device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) 
 template <class Op>
 __device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_D0));
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        double d = 0.0;
-        if (i < a.n) {
-            const float si = a.op.apply32(a.p32, i);
-            a.s32[i] = si;
-            d = xprod(a.p32[i], si);
-        }
-        ts.add(tile, d);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        float p1 = 0.f, p2 = 0.f, s1, s2;
+        if (v1) p1 = a.p32[i];
+        if (v2) p2 = a.p32[i2];
+        a.op.apply2_32(a.p32, i, v1, i2, v2, s1, s2);
+        if (v1) a.s32[i] = s1;
+        if (v2) a.s32[i2] = s2;
+        ts.add(tile, v1 ? xprod(p1, s1) : 0.0);
+        if (has2) ts.add(tile2, v2 ? xprod(p2, s2) : 0.0);
     }
     ts.flush();
 }
@@ -632,25 +725,55 @@ __device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
 template <class Op>
 __device__ void phase_inner_update(const KArgs<Op> &a, float af, double *sm) {
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        double g = 0.0;
-        if (i < a.n) {
-            a.d32[i] = __fmaf_rn(af, a.p32[i], a.d32[i]);
-            const float ri = __fmaf_rn(-af, a.s32[i], a.r32[i]);
-            a.r32[i] = ri;
-            g = xprod(ri, ri);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        float d1 = 0.f, p1 = 0.f, r1 = 0.f, s1 = 0.f, d2 = 0.f, p2 = 0.f, r2 = 0.f, s2 = 0.f;
+        if (v1) {
+            d1 = a.d32[i];
+            p1 = a.p32[i];
+            r1 = a.r32[i];
+            s1 = a.s32[i];
         }
-        ts.add(tile, g);
+        if (v2) {
+            d2 = a.d32[i2];
+            p2 = a.p32[i2];
+            r2 = a.r32[i2];
+            s2 = a.s32[i2];
+        }
+        double g1 = 0.0, g2 = 0.0;
+        if (v1) {
+            a.d32[i] = __fmaf_rn(af, p1, d1);
+            const float ri = __fmaf_rn(-af, s1, r1);
+            a.r32[i] = ri;
+            g1 = xprod(ri, ri);
+        }
+        if (v2) {
+            a.d32[i2] = __fmaf_rn(af, p2, d2);
+            const float ri = __fmaf_rn(-af, s2, r2);
+            a.r32[i2] = ri;
+            g2 = xprod(ri, ri);
+        }
+        ts.add(tile, g1);
+        if (has2) ts.add(tile2, g2);
     }
     ts.flush();
 }
 
 template <class Op>
 __device__ void phase_inner_p(const KArgs<Op> &a, float bf) {
-    CFM_TILES(a) {
-        CFM_ROW(a);
-        if (i < a.n) a.p32[i] = __fmaf_rn(bf, a.p32[i], a.r32[i]);
+    CFM_TILE_PAIRS(a) {
+        CFM_ROW_PAIR(a);
+        float p1 = 0.f, r1 = 0.f, p2 = 0.f, r2 = 0.f;
+        if (v1) {
+            p1 = a.p32[i];
+            r1 = a.r32[i];
+        }
+        if (v2) {
+            p2 = a.p32[i2];
+            r2 = a.r32[i2];
+        }
+        if (v1) a.p32[i] = __fmaf_rn(bf, p1, r1);
+        if (v2) a.p32[i2] = __fmaf_rn(bf, p2, r2);
     }
 }
 
