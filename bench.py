@@ -102,7 +102,7 @@ def workload_cg128(args, cfm):
     peak, kind = peak_hbm()
     res = {}
     for impl, name in ((cfm.CG_PERSISTENT, "standard"), (cfm.CG_PERSISTENT_PIPELINED, "pipelined"),
-                       (cfm.CG_MIXED, "fp32_inner_fp64_refinement")):
+                       (cfm.CG_MIXED, "fp32_cg_fp64_reliable_updates")):
         cg = cfm.CG(A, impl, 20000, 1e-8)
         for _ in range(args.warmup):
             cg.solve(b)

@@ -119,7 +119,7 @@ KArgs<Op> make_args(cfm_cg *h, const Op &op, const double *b_dev, double *x_dev)
     a.maxiter = h->p.maxiter;
     a.tol = h->p.tol;
     a.inner_maxiter = h->p.inner_maxiter;  // 0: no cap per sweep
-    a.inner_tol = h->p.inner_tol > 0 ? h->p.inner_tol : 1e-3;
+    a.inner_tol = h->p.inner_tol > 0 ? h->p.inner_tol : 0.1;
     return a;
 }
 

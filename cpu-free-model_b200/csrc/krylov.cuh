@@ -15,9 +15,9 @@
 //                    SpMV q = A w and every vector recurrence of an iteration fused
 //                    into one pass, double-buffered w and dot partials, 1 grid
 //                    barrier per iteration
-//   cg_mixed_kernel  FP64 iterative refinement around an FP32 inner CG: the true
-//                    residual, the correction x += |r| d and the dot reductions
-//                    (FP64 sums of exact FP32 products) stay FP64
+//   cg_mixed_kernel  FP32 CG with FP64 reliable updates: the true residual, the
+//                    correction x += |b| d and the dot reductions (FP64 sums of
+//                    exact FP32 products) stay FP64
 // Every dot is a fixed tree (1024-row tiles, xor butterflies, then the tile
 // partials in lane order), so results do not depend on the launch shape and
 // the CPU oracle reproduces them bit for bit.  Scalar arithmetic is written
@@ -686,7 +686,8 @@ __device__ void phase_mixed_init(const KArgs<Op> &a, double *sm) {
     ts.flush();
 }
 
-// Inner right-hand side r32 = fl32(t / |t|), p32 = r32, d32 = 0; <r32, r32> -> G0.
+// Start of the FP32 iteration: r32 = fl32(t * scale), p32 = r32, d32 = 0;
+// <r32, r32> -> G0.
 template <class Op>
 __device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) {
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
@@ -777,21 +778,51 @@ __device__ void phase_inner_p(const KArgs<Op> &a, float bf) {
     }
 }
 
-// x += |t| d32 (FP64 correction)
+// Reliable update, first half: x += |b| d32 in FP64, d32 = 0.
 template <class Op>
 __device__ void phase_correct(const KArgs<Op> &a, double norm) {
     CFM_TILES(a) {
         CFM_ROW(a);
-        if (i < a.n) a.x[i] = __fma_rn(norm, (double)a.d32[i], a.x[i]);
+        if (i < a.n) {
+            a.x[i] = __fma_rn(norm, (double)a.d32[i], a.x[i]);
+            a.d32[i] = 0.f;
+        }
     }
 }
 
-// FP64 iterative refinement around FP32 CG.  Each sweep solves A d = t / |t|
-// in FP32 (FP32 SpMV and axpys with FP32 accumulation; the dots are FP64 sums
-// of the exact FP32 products; alpha, beta in FP64, applied rounded to FP32)
-// until |r_inner| <= inner_tol |r_inner,0| or inner_maxiter steps, then
-// x += |t| d in FP64 and t = b - A x in FP64.  Stops when |t| <= tol |b|;
-// maxiter caps the inner steps over all sweeps.
+// Reliable update, second half: t = b - A x (FP64) with |t|^2 -> TT, and
+// r32 = fl32(t / |b|) with <r32, r32> -> G0.
+template <class Op>
+__device__ void phase_replace32(const KArgs<Op> &a, double scale, double *sm) {
+    TileSums<2> ts(sm, gridDim.x, slot(a, SL_TT), slot(a, SL_G0));
+    CFM_TILES(a) {
+        CFM_ROW(a);
+        double q = 0.0, g = 0.0;
+        if (i < a.n) {
+            const double bi = a.b ? a.b[i] : 1.0;
+            const double ti = __dsub_rn(bi, a.op.apply(a.x, i));
+            const float ri = __double2float_rn(__dmul_rn(ti, scale));
+            a.t[i] = ti;
+            a.r32[i] = ri;
+            q = __dmul_rn(ti, ti);
+            g = xprod(ri, ri);
+        }
+        ts.add(tile, q, g);
+    }
+    ts.flush();
+}
+
+// Mixed-precision CG with reliable updates.  The iteration runs in FP32
+// (FP32 SpMV and axpys; the dots are FP64 sums of the exact FP32 products;
+// alpha, beta in FP64, applied rounded to FP32) on r32 = fl32(r / |b|) and
+// gathers its steps in an FP32 correction d32.  When <r32, r32> falls to
+// tol^2, below inner_tol^2 times its largest value since the last update,
+// or after inner_maxiter steps (0: no cap), a reliable update adds |b| d32
+// to x in FP64 and replaces r32 by fl32((b - A x) / |b|) from the FP64 true
+// residual; the search direction p32 is kept, so the recurrence goes on
+// (beta from the replaced residual) instead of restarting (Sleijpen and van
+// der Vorst's reliable updated residuals).  Stops when the FP64 true
+// residual |b - A x| <= tol |b|; maxiter caps the FP32 steps.
 template <class Op>
 __global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
     __shared__ double sm[TS_SMEM];
@@ -800,56 +831,59 @@ __global__ void __launch_bounds__(CG_TILE, 1) cg_mixed_kernel(KArgs<Op> a) {
     if (!grid_barrier(a.bar, gridDim.x, site++)) return;
     const double bnorm = sqrt(sum_partials(slot(a, SL_B), a.ntiles, sm));
     const double target = a.tol * bnorm;
-    int status = CFM_NOT_CONVERGED, sweeps = 0;
-    long long k = 0;
     double tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
-    while (true) {
-        const double tnorm = sqrt(tt);
-        if (tnorm <= target) {
-            status = CFM_OK;
-            break;
-        }
-        if (k >= a.maxiter || sweeps >= 1000) break;
-        phase_inner_start(a, 1.0 / tnorm, sm);
+    int status = CFM_NOT_CONVERGED, updates = 0;
+    long long k = 0;
+    if (sqrt(tt) <= target || bnorm == 0.0) {
+        write_result(a.res, 0, sqrt(tt) <= target ? CFM_OK : CFM_NOT_CONVERGED, 0, tt, bnorm);
+        return;
+    }
+    const double scale = 1.0 / bnorm, tol2 = a.tol * a.tol;
+    const double delta2 = a.inner_tol * a.inner_tol;
+    phase_inner_start(a, scale, sm);
+    if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+    double g0 = sum_partials(slot(a, SL_G0), a.ntiles, sm), gmax = g0;
+    int since = 0;
+    while (k < a.maxiter) {
+        phase_inner_spmv(a, sm);
         if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        double g0 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
-        const double stop = a.inner_tol * sqrt(g0);
-        int j = 0;
-        bool broke = false;
-        while (true) {
-            phase_inner_spmv(a, sm);
-            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-            const double delta = sum_partials(slot(a, SL_D0), a.ntiles, sm);
-            const double alpha = g0 / delta;
-            if (!(delta > 0.0 && isfinite(alpha))) {
-                broke = true;
-                break;
-            }
-            phase_inner_update(a, __double2float_rn(alpha), sm);
-            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-            const double g1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
-            ++j;
-            ++k;
-            if (sqrt(g1) <= stop || (a.inner_maxiter > 0 && j >= a.inner_maxiter) ||
-                k >= a.maxiter)
-                break;
-            const double beta = g1 / g0;
-            phase_inner_p(a, __double2float_rn(beta));
-            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-            g0 = g1;
-        }
-        if (broke && j == 0) {
+        const double delta = sum_partials(slot(a, SL_D0), a.ntiles, sm);
+        const double alpha = g0 / delta;
+        if (!(delta > 0.0 && isfinite(alpha))) {
             status = CFM_BREAKDOWN;
             break;
         }
-        phase_correct(a, tnorm);
+        phase_inner_update(a, __double2float_rn(alpha), sm);
         if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        ++sweeps;
-        phase_true_residual(a, sm);
+        double g1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+        ++k;
+        ++since;
+        if (g1 <= tol2 || g1 < delta2 * gmax || k >= a.maxiter ||
+            (a.inner_maxiter > 0 && since >= a.inner_maxiter)) {
+            phase_correct(a, bnorm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            phase_replace32(a, scale, sm);
+            if (!grid_barrier(a.bar, gridDim.x, site++)) return;
+            tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+            g1 = sum_partials(slot(a, SL_G0), a.ntiles, sm);
+            ++updates;
+            since = 0;
+            gmax = g1;
+            if (sqrt(tt) <= target) {
+                status = CFM_OK;
+                break;
+            }
+            if (k >= a.maxiter) break;
+        } else if (g1 > gmax) {
+            gmax = g1;
+        }
+        const double beta = g1 / g0;
+        phase_inner_p(a, __double2float_rn(beta));
         if (!grid_barrier(a.bar, gridDim.x, site++)) return;
-        tt = sum_partials(slot(a, SL_TT), a.ntiles, sm);
+        g0 = g1;
     }
-    write_result(a.res, k, status, sweeps, tt, bnorm);
+    if (since > 0) phase_correct(a, bnorm);  // a breakdown left steps in d32
+    write_result(a.res, k, status, updates, tt, bnorm);
 }
 
 // ------------------------------------------------ host-controlled pieces

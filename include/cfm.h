@@ -91,7 +91,7 @@ typedef struct cfm_stats {
     double d2h_bytes;     /* device->host bytes copied inside the call */
     int launches;         /* kernel launches issued inside the timed region */
     int status;           /* cfm_status of the run */
-    int refinements;      /* CG mixed precision: outer refinement sweeps */
+    int refinements;      /* mixed precision: FP64 reliable updates; standard / pipelined CG: restarts */
     int pad;
 } cfm_stats;
 
@@ -170,8 +170,10 @@ typedef enum cfm_cg_impl {
     /* "Single Stream Pipelined" (CG/src/single-stream/pipelined.cu:176-330):
      * one persistent kernel, one fused pass and one grid barrier per iteration */
     CFM_CG_PERSISTENT_PIPELINED = 2,
-    /* FP32 inner persistent CG inside an FP64 iterative-refinement loop, one
-     * persistent kernel (no reference counterpart; needs tol > 0) */
+    /* FP32 persistent CG with FP64 reliable updates (the correction is added
+     * to x and the residual replaced by b - A x in FP64, keeping the search
+     * direction), one persistent kernel (no reference counterpart; needs
+     * tol > 0) */
     CFM_CG_MIXED = 3
 } cfm_cg_impl;
 
@@ -207,11 +209,12 @@ int cfm_stencil_apply_host(const cfm_stencil *S, const double *x, double *y);
 
 typedef struct cfm_cg_params {
     int impl;          /* cfm_cg_impl */
-    int maxiter;       /* iteration cap (CFM_CG_MIXED: inner iterations over all sweeps);
+    int maxiter;       /* iteration cap (CFM_CG_MIXED: FP32 iterations);
                           with tol <= 0 exactly maxiter iterations run */
     double tol;        /* relative residual target ||r||/||b||; <= 0 = fixed count (reference -niter) */
-    int inner_maxiter; /* CFM_CG_MIXED: FP32 iterations per refinement sweep (0 = no cap) */
-    double inner_tol;  /* CFM_CG_MIXED: relative reduction per sweep (0 = default 1e-3) */
+    int inner_maxiter; /* CFM_CG_MIXED: most FP32 iterations between two FP64 updates (0 = no cap) */
+    double inner_tol;  /* CFM_CG_MIXED: an FP64 update when |r| falls below inner_tol times its
+                          largest norm since the last one (0 = default 0.1) */
 } cfm_cg_params;
 
 typedef struct cfm_cg cfm_cg;

@@ -623,11 +623,15 @@ static int krylov_pipe(const orc_op *A, const double *b, int maxiter, double tol
     return status;
 }
 
-/* FP64 refinement around FP32 CG: the arithmetic of cg_mixed_kernel
- * (csrc/krylov.cuh). */
+/* FP32 CG with FP64 reliable updates: the arithmetic of cg_mixed_kernel
+ * (csrc/krylov.cuh).  r32 = fl32(r / |b|); the FP32 steps gather in d32;
+ * an update (when <r32, r32> <= tol^2, < inner_tol^2 times its largest value
+ * since the last update, after inner_maxiter steps, or at maxiter) adds
+ * |b| d32 to x in FP64 and replaces r32 by fl32((b - A x) / |b|), keeping
+ * p32; beta comes from the replaced residual. */
 static int krylov_mixed(const orc_op *A, const double *b, int maxiter, double tol,
                         int inner_maxiter, double inner_tol, double *x, long long *iters,
-                        int *sweeps_out, int nt) {
+                        int *updates_out, int nt) {
     const int n = A->n;
     double *t = malloc(sizeof(double) * n), *s = malloc(sizeof(double) * n);
     double *scr = malloc(sizeof(double) * n);
@@ -640,50 +644,60 @@ static int krylov_mixed(const orc_op *A, const double *b, int maxiter, double to
     double tt = orc_dot(n, t, t, nt);
     const double bnorm = sqrt(orc_dot(n, b, b, nt));
     const double target = tol * bnorm;
-    int status = 5, sweeps = 0;
+    int status = 5, updates = 0, since = 0;
     long long k = 0;
-    for (;;) {
-        const double tnorm = sqrt(tt);
-        if (tnorm <= target) { status = 0; break; }
-        if (k >= maxiter || sweeps >= 1000) break;
-        const double scale = 1.0 / tnorm;
+    if (sqrt(tt) <= target || bnorm == 0.0) {
+        status = sqrt(tt) <= target ? 0 : 5;
+    } else {
+        const double scale = 1.0 / bnorm, tol2 = tol * tol, delta2 = inner_tol * inner_tol;
         for (int i = 0; i < n; ++i) {
             r32[i] = (float)(t[i] * scale);
             p32[i] = r32[i];
             d32[i] = 0.f;
         }
-        double g0 = dot32(n, r32, r32, scr, nt);
-        const double stop = inner_tol * sqrt(g0);
-        int j = 0, broke = 0;
-        for (;;) {
+        double g0 = dot32(n, r32, r32, scr, nt), gmax = g0;
+        while (k < maxiter) {
             op_apply32(A, p32, s32, nt);
             const double delta = dot32(n, p32, s32, scr, nt);
             const double alpha = g0 / delta;
-            if (!(delta > 0.0 && isfinite(alpha))) { broke = 1; break; }
+            if (!(delta > 0.0 && isfinite(alpha))) { status = 4; break; }
             const float af = (float)alpha;
 #pragma omp parallel for num_threads(nt) schedule(static)
             for (int i = 0; i < n; ++i) {
                 d32[i] = fmaf(af, p32[i], d32[i]);
                 r32[i] = fmaf(-af, s32[i], r32[i]);
             }
-            const double g1 = dot32(n, r32, r32, scr, nt);
-            ++j;
+            double g1 = dot32(n, r32, r32, scr, nt);
             ++k;
-            if (sqrt(g1) <= stop || (inner_maxiter > 0 && j >= inner_maxiter) || k >= maxiter)
-                break;
+            ++since;
+            if (g1 <= tol2 || g1 < delta2 * gmax || k >= maxiter ||
+                (inner_maxiter > 0 && since >= inner_maxiter)) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+                for (int i = 0; i < n; ++i) {
+                    x[i] = fma(bnorm, (double)d32[i], x[i]);
+                    d32[i] = 0.f;
+                }
+                tt = true_res(A, b, x, t, s, nt);
+                for (int i = 0; i < n; ++i) r32[i] = (float)(t[i] * scale);
+                g1 = dot32(n, r32, r32, scr, nt);
+                ++updates;
+                since = 0;
+                gmax = g1;
+                if (sqrt(tt) <= target) { status = 0; break; }
+                if (k >= maxiter) break;
+            } else if (g1 > gmax) {
+                gmax = g1;
+            }
             const float bf = (float)(g1 / g0);
 #pragma omp parallel for num_threads(nt) schedule(static)
             for (int i = 0; i < n; ++i) p32[i] = fmaf(bf, p32[i], r32[i]);
             g0 = g1;
         }
-        if (broke && j == 0) { status = 4; break; }
-#pragma omp parallel for num_threads(nt) schedule(static)
-        for (int i = 0; i < n; ++i) x[i] = fma(tnorm, (double)d32[i], x[i]);
-        ++sweeps;
-        tt = true_res(A, b, x, t, s, nt);
+        if (since > 0)
+            for (int i = 0; i < n; ++i) x[i] = fma(bnorm, (double)d32[i], x[i]);
     }
     *iters = k;
-    *sweeps_out = sweeps;
+    *updates_out = updates;
     free(t); free(s); free(scr); free(r32); free(p32); free(s32); free(d32);
     return status;
 }
@@ -701,7 +715,7 @@ static int krylov_run(orc_op *A, int method, const double *b_in, int maxiter, do
         status = krylov_pipe(A, b, maxiter, tol, x, &k, &rs, nt);
     } else if (method == 2) {
         status = krylov_mixed(A, b, maxiter, tol, inner_maxiter,
-                              inner_tol > 0 ? inner_tol : 1e-3, x, &k, &rs, nt);
+                              inner_tol > 0 ? inner_tol : 0.1, x, &k, &rs, nt);
     } else {
         status = krylov_std(A, b, maxiter, tol, x, &k, &rs, nt);
     }
