@@ -35,10 +35,12 @@ __device__ __forceinline__ int ld_relaxed_i32(const int *p) {
 // Generation-counting barrier over all `nblocks` blocks of the grid.
 // Returns true when every block arrived; false once any wait timed out (the
 // caller must then leave its loop).  `site` labels the barrier for the
-// error report.
+// error report.  A single block needs only the block barrier, which orders
+// the block's global-memory accesses for its own threads.
 __device__ __forceinline__ bool grid_barrier(BarrierState *b, unsigned int nblocks, int site) {
     __shared__ int s_ok;
     __syncthreads();
+    if (nblocks == 1) return true;
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
         int ok = 1;
         const unsigned int g = ld_acquire_u32(&b->gen);
