@@ -232,24 +232,49 @@ __global__ void __launch_bounds__(1024, 1)
     __syncthreads();
     __shared__ int s_ok;
     const int inner = nx - 2;
-    for (int t = 0; t < niter; ++t) {
-        for (int p = tid; p < h * inner; p += nth) {
-            const int r = 1 + p / inner;
-            const int x = 1 + p % inner;
+    // rows [ra, rb) of the band as a flat run of cells, row r / column x of
+    // the first cell of each thread stepped without a division per cell
+    const int dr = nth / inner, dx = nth % inner;
+    auto sweep_rows = [&](int ra, int rb, T *pub) {
+        int r = ra + tid / inner, x = 1 + tid % inner;
+        for (; r < rb; r += dr, x += dx) {
+            if (x > inner) {
+                x -= inner;
+                ++r;
+                if (r >= rb) break;
+            }
             const T *c = cur + (size_t)r * nx + x;
-            nxt[(size_t)r * nx + x] = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
+            const T v = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
+            nxt[(size_t)r * nx + x] = v;
+            if (pub) {  // the rows the neighbours read: first to slot 0, last to slot 1
+                if (r == 1) __stcg(pub + x, v);
+                if (r == h) __stcg(pub + nx + x, v);
+            }
         }
-        __syncthreads();
+    };
+    for (int t = 0; t < niter; ++t) {
         T *xb = xbuf + ((size_t)(t & 1) * B + b) * 2 * nx;
-        for (int x = tid; x < nx; x += nth) {
-            __stcg(xb + x, nxt[(size_t)nx + x]);
-            __stcg(xb + nx + x, nxt[(size_t)h * nx + x]);
+        // 1. the first and last rows, published as they are computed (a
+        //    one-row band publishes its row in both slots)
+        sweep_rows(1, 2, xb);
+        if (h > 1) sweep_rows(h, h + 1, xb);
+        // the slot columns 0 and nx-1 carry the band's boundary cells
+        if (tid == 0) {
+            __stcg(xb, nxt[nx]);
+            __stcg(xb + nx - 1, nxt[2 * (size_t)nx - 1]);
+            __stcg(xb + nx, nxt[(size_t)h * nx]);
+            __stcg(xb + 2 * nx - 1, nxt[(size_t)(h + 1) * nx - 1]);
         }
         __syncthreads();
         if (tid == 0) {
-            int ok = 1;
             __threadfence();
             st_release_u32(flags + b, (unsigned)(t + 1));
+        }
+        // 2. the inner rows while the neighbours' counters move
+        if (h > 2) sweep_rows(2, h, nullptr);
+        // 3. wait for the two ring neighbours' rows of this sweep
+        if (tid == 0) {
+            int ok = 1;
             const unsigned long long t0 = global_ns();
             const unsigned long long budget = bar->timeout_ns;
             while (ld_acquire_u32(flags + up_blk) < (unsigned)(t + 1) ||
