@@ -32,6 +32,24 @@ __device__ __forceinline__ int ld_relaxed_i32(const int *p) {
     return v;
 }
 
+// Arrival: fetch-add with acquire-release order at GPU scope, so the block's
+// writes (ordered before it by the block barrier) are released with the
+// arrival and the last arriver acquires every earlier block's.
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(p), "r"(v)
+                 : "memory");
+    return old;
+}
+
+// Generation bump by the last arriver: a release, cumulative over the
+// arrivals it acquired.
+__device__ __forceinline__ void red_add_release_u32(unsigned int *p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Generation-counting barrier over all `nblocks` blocks of the grid.
 // Returns true when every block arrived; false once any wait timed out (the
 // caller must then leave its loop).  `site` labels the barrier for the
@@ -43,14 +61,15 @@ __device__ __forceinline__ bool grid_barrier(BarrierState *b, unsigned int nbloc
     if (nblocks == 1) return true;
     if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
         int ok = 1;
+        // the generation cannot move before this block arrives
         const unsigned int g = ld_acquire_u32(&b->gen);
-        __threadfence();  // release this block's writes before arriving
-        const unsigned int arrived = atomicAdd(&b->count, 1u);
+        const unsigned int arrived = atom_add_acq_rel_u32(&b->count, 1u);
         if (arrived == nblocks - 1) {
             atomicExch(&b->count, 0u);
-            __threadfence();
-            atomicAdd(&b->gen, 1u);
+            red_add_release_u32(&b->gen, 1u);
         } else {
+            // the acquire load that sees the new generation synchronises
+            // with the last arriver's release
             const unsigned long long t0 = global_ns();
             const unsigned long long budget = b->timeout_ns;
             while (ld_acquire_u32(&b->gen) == g) {
@@ -63,10 +82,8 @@ __device__ __forceinline__ bool grid_barrier(BarrierState *b, unsigned int nbloc
                     ok = 0;
                     break;
                 }
-                __nanosleep(20);
             }
         }
-        __threadfence();  // acquire the other blocks' writes
         if (ld_relaxed_i32(&b->error)) ok = 0;
         s_ok = ok;
     }
