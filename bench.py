@@ -194,7 +194,7 @@ def workload_varcoef512(args, cfm):
     # (256^2), trained here on plain-CG pairs of 100 fresh 512^2 systems
     net = cfm.UNet(N // 2, N // 2, max_batch=8, seed=7)
     info = net.train_varcoef(100, 19, 1000, 16, 8, 1e-3, smooth=4, coarsen=2)
-    for m, per in ((8, 2), (8, 1), (4, 1)):
+    for m, per in ((8, 2), (8, 3), (8, 4), (8, 1), (4, 1)):
         fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, truncation=m, net_period=per)
         t, st = timed(lambda: fl.solve(f))
         out[f"fpcg_learned_m{m}_p{per}"] = {"ms": t * 1e3, "iterations": st.iterations,

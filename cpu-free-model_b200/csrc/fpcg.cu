@@ -441,10 +441,11 @@ __device__ float *fp_sweeps(const FpTile &t, const FpArgs &a, float *cur, float 
 }
 
 // Start of the preconditioner (one launch): [k += 1 when `tick`; block 0:
-// |r|^2 history, convergence / stall test]; z0 = `smooth` sweeps from zero,
-// r1 = r - A z0, partial |r1|^2, and the network input channel 0 = R(r1)
-// (f x f means; the network scales it by 1 / rms(r1) itself).
-__global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
+// |r|^2 history, convergence / stall test]; z0 = `smooth` sweeps from zero
+// and, when the network follows (`net_next`), r1 = r - A z0, partial
+// |r1|^2, and the network input channel 0 = R(r1) (f x f means; the network
+// scales it by 1 / rms(r1) itself).
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int net_next) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
@@ -485,6 +486,10 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
     const int row = H + ly, col = H + lx, l = row * t.R + col;
     int i;
     const bool in = fp_inside(t, a, row, col, &i);
+    if (!net_next) {
+        if (in) a.za[i] = (double)z[l];
+        return;
+    }
     double q = 0;
     if (in) {
         const double v = (double)(t.r()[l] - fp_apply(t, a, z, row, col));
@@ -514,13 +519,16 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick) {
 // multiples of P y, c P y removes the most A-norm error from A d = r1, so the
 // network's correction can only help the smoothed iterate), written to a.z
 // with the partials <z_k, s_{k-1-j}> (j < min(k, m)) of the orthogonalisation.
-__global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a) {
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
-    const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
-    const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
-    const double c = yay > 0 ? yr / yay : 0.0;
+    double c = 0.0;  // without the network's y this iteration: smoothing alone
+    if (use_y) {
+        const double yr = sum_partials(fslot(a, FP_YR), a.ntiles, sm);
+        const double yay = sum_partials(fslot(a, FP_YAY), a.ntiles, sm);
+        c = yay > 0 ? yr / yay : 0.0;
+    }
     const int H = a.smooth;
     FpTile t = fp_tile(a, H, fp_smem);
     FP_FOR_SQUARE(0, t.R, row, col) {
@@ -797,13 +805,12 @@ FpArgs fp_args(cfm_fpcg *h) {
 int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, int tick,
                    bool use_net = true) {
     cudaStream_t s = h->stream;
+    const int net_next = !(h->net && !use_net);
     CFM_CUDA_TRY(launch_pdl(k_fp_pre, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(std::max(h->smooth, 1)), s,
-                            a, tick));
-    if (h->net && !use_net) {
-        // smoothing alone this iteration: no <y, .> partials, so c = 0
-        CFM_CUDA_TRY(cudaMemsetAsync(a.part + (size_t)FP_YR * a.pstride, 0, sizeof(double) * a.ntiles, s));
-        CFM_CUDA_TRY(cudaMemsetAsync(a.part + (size_t)FP_YAY * a.pstride, 0, sizeof(double) * a.ntiles, s));
-        CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a));
+                            a, tick, net_next));
+    if (!net_next) {
+        // smoothing alone this iteration: no r1, no network, c = 0
+        CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 0));
         CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
         return CFM_OK;
     }
@@ -815,7 +822,7 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
         CFM_CUDA_TRY(launch_pdl(k_fp_identity, dim3(256), dim3(256), 0, s, a));
     }
     CFM_CUDA_TRY(launch_pdl(k_fp_ydots, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
-    CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a));
+    CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 1));
     CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
     return CFM_OK;
 }
