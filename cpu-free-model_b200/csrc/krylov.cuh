@@ -111,7 +111,9 @@ struct TileSums {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         if (warp < g * K) {
             const double v = warp_xor_sum(sm[warp * 32 + lane]);
-            if (lane == 0) dst[warp % K][t0 + (warp / K) * stride] = v;
+            double *d = dst[0];
+            if (K > 1 && (warp & 1)) d = dst[K - 1];  // a select: no indexed local array
+            if (lane == 0) d[t0 + (warp / K) * stride] = v;
         }
         __syncthreads();
         g = 0;
@@ -120,6 +122,29 @@ struct TileSums {
 
 // Exact product of two FP32 values, as FP64.
 __device__ __forceinline__ double xprod(float a, float b) { return __dmul_rn((double)a, (double)b); }
+
+// U of the block's tiles per step (t0 + u gridDim.x, u < U), the FP32
+// passes' form of the tile pairs.  U = 2 measured best on 128^3 Poisson
+// (4: 22.3 ms mixed against 19.6 ms).
+constexpr int INNER_U = 2;
+template <int U>
+struct TileGroup {
+    int tile[U], row[U];
+    bool has[U], ok[U];
+    __device__ __forceinline__ TileGroup(int ntiles, int n, int t0) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            tile[u] = t0 + u * (int)gridDim.x;
+            has[u] = tile[u] < ntiles;
+            row[u] = tile[u] * CG_TILE + (int)threadIdx.x;
+            ok[u] = has[u] && row[u] < n;
+        }
+    }
+};
+template <int U>
+struct Vals32 {
+    float v[U];
+};
 
 // ------------------------------------------------------------- operators
 struct CsrOp {
@@ -180,6 +205,31 @@ struct CsrOp {
                                               float &y1, float &y2) const {
         apply2_t(val32, x, i, v1, i2, v2, y1, y2);
     }
+    // FP32 apply for the rows of a tile group (0 for an absent row), their
+    // entries interleaved.
+    template <int U>
+    __device__ __forceinline__ Vals32<U> applyN32(const float *x, const TileGroup<U> &g) const {
+        int j[U], e[U];
+        Vals32<U> y;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            j[u] = g.ok[u] ? rowptr[g.row[u]] : 0;
+            e[u] = g.ok[u] ? rowptr[g.row[u] + 1] : 0;
+            y.v[u] = 0.f;
+        }
+        bool more = true;
+        while (more) {
+            more = false;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j[u] < e[u]) {
+                    y.v[u] = __fmaf_rn(val32[j[u]], x[col[j[u]]], y.v[u]);
+                    ++j[u];
+                    more = true;
+                }
+        }
+        return y;
+    }
     // A x0 with x0 = 0, summed like apply (always +0)
     __device__ __forceinline__ double apply_zero(int i) const {
         double acc = 0.0;
@@ -233,6 +283,13 @@ struct StencilOp {
         y1 = v1 ? apply32(x, i) : 0.f;
         y2 = v2 ? apply32(x, i2) : 0.f;
     }
+    template <int U>
+    __device__ __forceinline__ Vals32<U> applyN32(const float *x, const TileGroup<U> &g) const {
+        Vals32<U> y;
+#pragma unroll
+        for (int u = 0; u < U; ++u) y.v[u] = g.ok[u] ? apply32(x, g.row[u]) : 0.f;
+        return y;
+    }
 };
 
 template <class Op>
@@ -262,6 +319,7 @@ struct KArgs {
 // Two of the block's tiles per step (tile, tile2 = tile + gridDim.x): the
 // loads of both rows go out before either row's arithmetic, halving the
 // chains of dependent memory round trips a warp waits on.
+#define CFM_TILE_GROUPS(a, U) for (int tile = blockIdx.x; tile < (a).ntiles; tile += (U) * (int)gridDim.x)
 #define CFM_TILE_PAIRS(a) for (int tile = blockIdx.x; tile < (a).ntiles; tile += 2 * (int)gridDim.x)
 #define CFM_ROW_PAIR(a)                                                      \
     const int tile2 = tile + (int)gridDim.x;                                 \
@@ -708,73 +766,73 @@ __device__ void phase_inner_start(const KArgs<Op> &a, double scale, double *sm) 
 
 template <class Op>
 __device__ void phase_inner_spmv(const KArgs<Op> &a, double *sm) {
+    constexpr int U = INNER_U;
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_D0));
-    CFM_TILE_PAIRS(a) {
-        CFM_ROW_PAIR(a);
-        float p1 = 0.f, p2 = 0.f, s1, s2;
-        if (v1) p1 = a.p32[i];
-        if (v2) p2 = a.p32[i2];
-        a.op.apply2_32(a.p32, i, v1, i2, v2, s1, s2);
-        if (v1) a.s32[i] = s1;
-        if (v2) a.s32[i2] = s2;
-        ts.add(tile, v1 ? xprod(p1, s1) : 0.0);
-        if (has2) ts.add(tile2, v2 ? xprod(p2, s2) : 0.0);
+    CFM_TILE_GROUPS(a, U) {
+        const TileGroup<U> g(a.ntiles, a.n, tile);
+        float p[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) p[u] = g.ok[u] ? a.p32[g.row[u]] : 0.f;
+        const Vals32<U> y = a.op.template applyN32<U>(a.p32, g);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (g.ok[u]) a.s32[g.row[u]] = y.v[u];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (g.has[u]) ts.add(g.tile[u], g.ok[u] ? xprod(p[u], y.v[u]) : 0.0);
     }
     ts.flush();
 }
 
 template <class Op>
 __device__ void phase_inner_update(const KArgs<Op> &a, float af, double *sm) {
+    constexpr int U = INNER_U;
     TileSums<1> ts(sm, gridDim.x, slot(a, SL_G0));
-    CFM_TILE_PAIRS(a) {
-        CFM_ROW_PAIR(a);
-        float d1 = 0.f, p1 = 0.f, r1 = 0.f, s1 = 0.f, d2 = 0.f, p2 = 0.f, r2 = 0.f, s2 = 0.f;
-        if (v1) {
-            d1 = a.d32[i];
-            p1 = a.p32[i];
-            r1 = a.r32[i];
-            s1 = a.s32[i];
+    CFM_TILE_GROUPS(a, U) {
+        const TileGroup<U> g(a.ntiles, a.n, tile);
+        float d[U], p[U], r[U], sv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            d[u] = p[u] = r[u] = sv[u] = 0.f;
+            if (g.ok[u]) {
+                d[u] = a.d32[g.row[u]];
+                p[u] = a.p32[g.row[u]];
+                r[u] = a.r32[g.row[u]];
+                sv[u] = a.s32[g.row[u]];
+            }
         }
-        if (v2) {
-            d2 = a.d32[i2];
-            p2 = a.p32[i2];
-            r2 = a.r32[i2];
-            s2 = a.s32[i2];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            double q = 0.0;
+            if (g.ok[u]) {
+                a.d32[g.row[u]] = __fmaf_rn(af, p[u], d[u]);
+                const float ri = __fmaf_rn(-af, sv[u], r[u]);
+                a.r32[g.row[u]] = ri;
+                q = xprod(ri, ri);
+            }
+            if (g.has[u]) ts.add(g.tile[u], q);
         }
-        double g1 = 0.0, g2 = 0.0;
-        if (v1) {
-            a.d32[i] = __fmaf_rn(af, p1, d1);
-            const float ri = __fmaf_rn(-af, s1, r1);
-            a.r32[i] = ri;
-            g1 = xprod(ri, ri);
-        }
-        if (v2) {
-            a.d32[i2] = __fmaf_rn(af, p2, d2);
-            const float ri = __fmaf_rn(-af, s2, r2);
-            a.r32[i2] = ri;
-            g2 = xprod(ri, ri);
-        }
-        ts.add(tile, g1);
-        if (has2) ts.add(tile2, g2);
     }
     ts.flush();
 }
 
 template <class Op>
 __device__ void phase_inner_p(const KArgs<Op> &a, float bf) {
-    CFM_TILE_PAIRS(a) {
-        CFM_ROW_PAIR(a);
-        float p1 = 0.f, r1 = 0.f, p2 = 0.f, r2 = 0.f;
-        if (v1) {
-            p1 = a.p32[i];
-            r1 = a.r32[i];
+    constexpr int U = INNER_U;
+    CFM_TILE_GROUPS(a, U) {
+        const TileGroup<U> g(a.ntiles, a.n, tile);
+        float p[U], r[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            p[u] = r[u] = 0.f;
+            if (g.ok[u]) {
+                p[u] = a.p32[g.row[u]];
+                r[u] = a.r32[g.row[u]];
+            }
         }
-        if (v2) {
-            p2 = a.p32[i2];
-            r2 = a.r32[i2];
-        }
-        if (v1) a.p32[i] = __fmaf_rn(bf, p1, r1);
-        if (v2) a.p32[i2] = __fmaf_rn(bf, p2, r2);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (g.ok[u]) a.p32[g.row[u]] = __fmaf_rn(bf, p[u], r[u]);
     }
 }
 

@@ -106,3 +106,21 @@ def test_mixed_precision_plan_independent_and_inner_cap(batch):
     B.set_precision(cfm.FP64)
     with pytest.raises(cfm.CfmError):
         B.set_precision(7)
+
+
+def test_mixed_precision_iteration_cap(batch):
+    """maxiter below convergence: every unconverged system stops at the cap
+    with NOT_CONVERGED, its FP32 steps folded into x by a last FP64 update
+    (the true residual is below |b|), in both precisions."""
+    systems, B = batch
+    for prec in (cfm.FP32, cfm.FP64):
+        B.set_precision(prec, 0, 0.1)
+        B.set_solver(smooth=4, maxiter=12, tol=1e-12)
+        it, stt, rr, st = B.solve(allowed=(cfm.OK, cfm.NOT_CONVERGED))
+        assert (stt == cfm.NOT_CONVERGED).all() and (it == 12).all()
+        assert np.isfinite(rr).all() and (rr < 1.0).all()
+        assert all(np.abs(B.solution(i)).max() > 0 for i in (0, 9, len(systems) - 1))
+        if prec == cfm.FP32:
+            assert st.refinements >= len(systems)
+    B.set_precision(cfm.FP64)
+    B.set_solver(smooth=4, maxiter=20000, tol=1e-8)

@@ -138,6 +138,37 @@ def test_mixed_inner_parameters_and_launch_count():
     np.testing.assert_array_equal(x, xo)
 
 
+@pytest.mark.parametrize("maxiter", [1, 7, 30])
+def test_mixed_iteration_cap_folds_the_correction(maxiter):
+    """A cap below convergence: the FP32 steps taken so far are folded into
+    x by a last FP64 update; x, the count and the updates equal the
+    oracle's, and the status is NOT_CONVERGED."""
+    rowptr, col, val = cfm.poisson3d(12)
+    A = cfm.CSR(rowptr, col, val)
+    b = A.spmv(cfm.uniform(9, A.n))
+    xo, st_o, it_o, rs_o, _ = oracle.krylov_csr(rowptr, col, val, b, oracle.MIXED, maxiter, 1e-10)
+    x, st = cfm.CG(A, cfm.CG_MIXED, maxiter, 1e-10).solve(b, allowed=(cfm.NOT_CONVERGED,))
+    assert st_o == cfm.NOT_CONVERGED and st.status == cfm.NOT_CONVERGED
+    assert st.iterations == it_o == maxiter and st.refinements == rs_o
+    np.testing.assert_array_equal(x, xo)
+    assert np.abs(x).max() > 0
+
+
+@pytest.mark.parametrize("delta", [0.5, 0.1, 1e-3])
+def test_mixed_update_threshold_bitexact(delta):
+    """The reliable-update threshold changes when the FP64 updates happen
+    (more of them for a larger delta); every setting equals the oracle and
+    reaches the FP64 tolerance."""
+    k, f = cfm.varcoef_problem((40, 56), 4)
+    S = cfm.Stencil(k)
+    xo, st_o, it_o, rs_o, _ = oracle.krylov_stencil(2, (56, 40, 1), cfm.varcoef_coeffs(k), f, oracle.MIXED,
+                                                    20000, 1e-9, inner_tol=delta)
+    x, st = cfm.CG(S, cfm.CG_MIXED, 20000, 1e-9, inner_tol=delta).solve(f.ravel())
+    assert st_o == 0 and st.status == cfm.OK and st.residual <= 1e-9
+    assert (st.iterations, st.refinements) == (it_o, rs_o)
+    np.testing.assert_array_equal(x, xo)
+
+
 def test_config4_varcoef_512_plain_and_pipelined_persistent():
     """The 512^2 variable-coefficient system (k = exp(GRF), f ~ N(0,1)) to
     1e-8: standard and pipelined persistent CG match the oracle exactly."""
