@@ -193,7 +193,9 @@ def workload_varcoef512(args, cfm):
     # the learned preconditioner: the U-Net on the 2x-restricted residual
     # (256^2), trained here on plain-CG pairs of 100 fresh 512^2 systems
     net = cfm.UNet(N // 2, N // 2, max_batch=8, seed=7)
+    net.set_validation(1000, 1)  # keep the checkpoint fastest on a held-out system (not this one)
     info = net.train_varcoef(100, 19, 1000, 16, 8, 1e-3, smooth=4, coarsen=2)
+    info["kept_epoch"], info["validation_ms"] = net.validation()
     for m, per in ((8, 2), (8, 3), (8, 4), (8, 1), (4, 1)):
         fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, truncation=m, net_period=per)
         t, st = timed(lambda: fl.solve(f))

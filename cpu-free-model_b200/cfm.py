@@ -77,6 +77,8 @@ _SIGS = {
     "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
                                           _c.c_float, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp]),
+    "cfm_unet_set_validation": (_c.c_int, [_vp, _c.c_ulonglong, _c.c_int]),
+    "cfm_unet_validation": (_c.c_int, [_vp, _vp, _vp]),
     "cfm_fpcg_create": (_c.c_int, [_vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_destroy": (None, [_vp]),
     "cfm_fpcg_set_truncation": (_c.c_int, [_vp, _c.c_int]),
@@ -534,6 +536,16 @@ class UNet:
               lib.cfm_unet_train_varcoef(self.h, nsys, snaps, seed0, epochs, batch, lr, smooth, coarsen,
                                          *[ctypes.byref(x) for x in v]))
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
+
+    def set_validation(self, seed, every):
+        """Keep the checkpoint whose FPCG solve of a held-out system is fastest."""
+        check("cfm_unet_set_validation", lib.cfm_unet_set_validation(self.h, seed, every))
+
+    def validation(self):
+        """(epochs of the kept checkpoint or -1, its validation solve in ms)."""
+        ep, ms = ctypes.c_int(), ctypes.c_double()
+        check("cfm_unet_validation", lib.cfm_unet_validation(self.h, ctypes.byref(ep), ctypes.byref(ms)))
+        return ep.value, ms.value
 
     def set_training_info(self, smooth, coarsen=1):
         """What a network restored with set_params was trained for."""

@@ -1247,6 +1247,48 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
     }
     const auto t1 = std::chrono::steady_clock::now();
     data_range.pop();
+    // validation: one held-out system solved by FPCG with the network as it
+    // trains; the parameters of the fastest solve are kept
+    struct Val {
+        cfm_stencil *S = nullptr;
+        cfm_fpcg *fp = nullptr;
+        std::vector<double> k, b, x;
+        std::vector<float> best;
+        double best_s = 1e300;
+        int best_ep = -1;
+        ~Val() {
+            cfm_fpcg_destroy(fp);
+            cfm_stencil_destroy(S);
+        }
+    } val;
+    net->val_best_epoch = -1;
+    net->val_best_ms = 0.0;
+    if (net->val_every > 0) {
+        val.k.resize(n);
+        val.b.resize(n);
+        val.x.resize(n);
+        if ((st = cfm_varcoef_problem(2, W, H, 1, net->val_seed, val.k.data(), val.b.data()))) return st;
+        if ((st = cfm_stencil_create(2, W, H, 1, val.k.data(), &val.S))) return st;
+        if ((st = cfm_fpcg_create(val.S, val.k.data(), net, smooth, 20000, 1e-8, &val.fp))) return st;
+    }
+    auto validate = [&](int ep) -> int {
+        CFM_CUDA_TRY(cudaStreamSynchronize(s));
+        double secs = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {  // the first solve also instantiates the graph
+            cfm_stats vs{};
+            const int e2 = cfm_fpcg_solve(val.fp, val.b.data(), val.x.data(), &vs);
+            if (e2 == CFM_OK) secs = std::min(secs, vs.seconds);
+            else if (e2 != CFM_NOT_CONVERGED && e2 != CFM_BREAKDOWN) return e2;
+        }
+        if (secs < val.best_s) {
+            val.best_s = secs;
+            val.best_ep = ep;
+            val.best.resize(unet_params(u));
+            const int e3 = cfm_unet_get_params(net, val.best.data());
+            if (e3) return e3;
+        }
+        return CFM_OK;
+    };
     // training
     const NvtxRange train_range("training: Adam epochs");
     std::mt19937_64 rng(seed0 ^ 0x5eedULL);
@@ -1285,12 +1327,34 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         ep_loss = nb ? l / nb : 0;
         if (ep == 0) first = ep_loss;
         last = ep_loss;
+        if (net->val_every > 0 && ((ep + 1) % net->val_every == 0 || ep + 1 == epochs))
+            if ((st = validate(ep + 1))) return st;
+    }
+    if (val.best_ep >= 0) {
+        if ((st = cfm_unet_set_params(net, val.best.data()))) return st;
+        net->val_best_epoch = val.best_ep;
+        net->val_best_ms = val.best_s * 1e3;
     }
     const auto t2 = std::chrono::steady_clock::now();
     if (loss_first) *loss_first = first;
     if (loss_last) *loss_last = last;
     if (data_seconds) *data_seconds = std::chrono::duration<double>(t1 - t0).count();
     if (train_seconds) *train_seconds = std::chrono::duration<double>(t2 - t1).count();
+    return CFM_OK;
+}
+
+int cfm_unet_set_validation(cfm_unet *net, unsigned long long seed, int every) {
+    clear_error();
+    CFM_ARG_CHECK(net && every >= 0, "arguments");
+    net->val_seed = seed;
+    net->val_every = every;
+    return CFM_OK;
+}
+
+int cfm_unet_validation(const cfm_unet *net, int *best_epoch, double *best_ms) {
+    CFM_ARG_CHECK(net, "null argument");
+    if (best_epoch) *best_epoch = net->val_best_epoch;
+    if (best_ms) *best_ms = net->val_best_ms;
     return CFM_OK;
 }
 

@@ -51,4 +51,9 @@ struct cfm_unet {
     int maxB = 0;
     int smooth = 0;   // Jacobi sweeps around the network it was trained for
     int coarsen = 1;  // the systems' grid is the network's times this factor
+    // checkpoint selection during training (cfm_unet_set_validation)
+    unsigned long long val_seed = 0;
+    int val_every = 0;           // 0: off
+    int val_best_epoch = -1;     // epochs of the kept parameters
+    double val_best_ms = 0.0;    // their FPCG time on the validation system
 };

@@ -362,6 +362,16 @@ int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *ou
 int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long long seed0, int epochs,
                            int batch, float lr, int smooth, int coarsen, double *loss_first,
                            double *loss_last, double *data_seconds, double *train_seconds);
+/* Checkpoint selection for cfm_unet_train_varcoef: with every > 0, one
+ * held-out variable-coefficient system (cfm_varcoef_problem with `seed`, the
+ * training systems' size) is solved to 1e-8 by FPCG (the defaults with a
+ * network) with the network as it trains, after every `every` epochs and
+ * after the last; training ends with the parameters of the fastest solve.
+ * every = 0 (default) keeps the last epoch's. */
+int cfm_unet_set_validation(cfm_unet *net, unsigned long long seed, int every);
+/* The kept checkpoint of the last training: epochs trained (-1: no
+ * validation) and its FPCG time on the validation system (ms). */
+int cfm_unet_validation(const cfm_unet *net, int *best_epoch, double *best_ms);
 
 /* Flexible PCG (truncated FCG(m): each direction A-orthogonalised against
  * the last m, alpha = <p, r> / <p, A p>) on a 2D stencil operator with the

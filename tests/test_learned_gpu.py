@@ -136,3 +136,21 @@ def test_restored_network_needs_training_info(coarse_trained):
     _, st_a = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8).solve(f)
     _, st_b = cfm.FPCG(S, k, twin, maxiter=20000, tol=1e-8).solve(f)
     assert st_b.status == cfm.OK and st_b.iterations == st_a.iterations
+
+
+def test_validation_keeps_a_checkpoint():
+    """Checkpoint selection: with a held-out system every 2 epochs, training
+    keeps the parameters of an evaluated checkpoint (epoch 2 or 4) and
+    reports its FPCG time; the kept network still solves that system."""
+    net = cfm.UNet(64, 256, max_batch=4, seed=3)
+    assert net.validation() == (-1, 0.0)
+    net.set_validation(1000, 2)
+    net.train_varcoef(6, 3, 40, 4, 4, 1e-3, smooth=4, coarsen=2)
+    ep, ms = net.validation()
+    assert ep in (2, 4) and ms > 0
+    k, f = cfm.varcoef_problem((128, 512), 1000)
+    x, st = cfm.FPCG(cfm.Stencil(k), k, net, maxiter=20000, tol=1e-8).solve(f)
+    assert st.status == cfm.OK and st.residual <= 1e-8
+    net.set_validation(0, 0)
+    net.train_varcoef(6, 3, 40, 2, 4, 1e-3, smooth=4, coarsen=2)
+    assert net.validation()[0] == -1
