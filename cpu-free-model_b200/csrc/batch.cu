@@ -72,7 +72,7 @@ struct BtArgs {
     // FP32 iteration with FP64 reliable updates (batch_kernel<true>)
     const float *we32, *wn32, *wt32, *dg32;  // FP32 copies of the coefficients
     float *r32, *p32, *s32, *z32, *y32, *d32; // FP32 inner vectors
-    int inner_maxiter;                        // 0: no cap per sweep
+    int inner_maxiter;                        // most FP32 steps between updates (0: no cap)
     double inner_tol;
 };
 

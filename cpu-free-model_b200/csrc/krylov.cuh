@@ -38,7 +38,7 @@ enum : int { SL_G0 = 0, SL_D0 = 1, SL_TT = 2, SL_B = 3, SL_G1 = 4, SL_D1 = 5, NS
 struct CgResult {
     long long iters;
     int status;
-    int restarts;  // restarts (standard, pipelined) or refinement sweeps (mixed)
+    int restarts;  // restarts (standard, pipelined) or FP64 reliable updates (mixed)
     double gamma;
     double bnorm;
 };

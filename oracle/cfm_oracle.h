@@ -63,10 +63,11 @@ int orc_spmv(int n, const int *rowptr, const int *col, const double *val, const 
              double *y, int threads);
 
 /* Operator-generic persistent-solver restatements (csrc/krylov.cuh):
- * method 0 standard CG, 1 pipelined CG, 2 FP64 refinement around FP32 CG
- * (inner_maxiter 0 -> no cap per sweep, inner_tol 0 -> 1e-3).  b == NULL -> ones, x0 = 0.
- * Returns 0 / 4 breakdown / 5 not converged; iters, restarts (refinement
- * sweeps for method 2), relres (true FP64 relative residual) optional. */
+ * method 0 standard CG, 1 pipelined CG, 2 FP32 CG with FP64 reliable
+ * updates (inner_maxiter 0 -> no cap between updates, inner_tol 0 -> 0.1,
+ * the residual drop that triggers one).  b == NULL -> ones, x0 = 0.
+ * Returns 0 / 4 breakdown / 5 not converged; iters, restarts (FP64 updates
+ * for method 2), relres (true FP64 relative residual) optional. */
 int orc_krylov_csr(int n, const int *rowptr, const int *col, const double *val, int method,
                    const double *b, int maxiter, double tol, int inner_maxiter, double inner_tol,
                    double *x, long long *iters, int *restarts, double *relres, int threads);

@@ -1,7 +1,7 @@
 """Persistent Krylov solvers on the GPU through the C ABI, against the oracle:
 the matrix-free variable-coefficient stencil operator and every solver
-(host-controlled, standard persistent, pipelined persistent, FP64-refined
-FP32 persistent) on CSR and stencil operators give the oracle's x, iteration
+(host-controlled, standard persistent, pipelined persistent, FP32 with
+FP64 reliable updates) on CSR and stencil operators give the oracle's x, iteration
 count and status bit for bit (same reduction trees, same rounding)."""
 import numpy as np
 import pytest

@@ -104,7 +104,7 @@ def test_oracle_methods_solve_varcoef(method, shape):
     xs = spla.spsolve(fv_matrix(k).tocsc(), f.ravel())
     assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-6
     if method == oracle.MIXED:
-        assert rs >= 2  # refinement sweeps
+        assert rs >= 2  # FP64 reliable updates
 
 
 def test_oracle_std_csr_equals_reference_restatement():
