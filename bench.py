@@ -65,7 +65,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["jacobi3d", "jacobi3d_fp32", "cg128", "varcoef512", "unet", "batch256"],
+    ap.add_argument("--workload", choices=["jacobi3d", "jacobi3d_fp32", "cg128", "varcoef512", "unet", "unet_train",
+                                           "batch256"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -240,6 +241,24 @@ def workload_unet(args, cfm):
          dtype="bf16")
 
 
+def workload_unet_train(args, cfm):
+    """One training step of the learned preconditioner's network at its
+    training shape (256^2, batch 8): forward, backward (data and weight
+    gradients on the tensor cores) and Adam, on a scratch network."""
+    N, B = 256, 8
+    net = cfm.UNet(N, N, max_batch=B, seed=11)
+    net.time_train_step(B, max(args.warmup, 1))
+    ms = net.time_train_step(B, max(args.steps, 5))
+    flop = 3 * B * unet_flops(N, N)  # forward + backward-data + weight gradient
+    peak, kind = peak_bf16()
+    line("U-Net training step 256^2 batch 8, device-resident", flop / (ms * 1e-3) / 1e12, "TFLOP/s", args,
+         ms, {"workload": "unet4_32ch_256^2_b8_train_step", "gflop_per_step": flop / 1e9,
+              "peak_bf16_tflops": peak, "peak_kind": kind,
+              "roofline_frac": flop / (ms * 1e-3) / 1e12 / peak,
+              "timing": "CUDA events around forward + backward + Adam on device buffers"},
+         dtype="bf16")
+
+
 def batch_bytes_per_iteration(dims, n, smooth, word):
     """Algorithmic bytes of one PCG iteration of one batched system: the
     operator pass (c coefficient arrays + p read + s write), the x / r update
@@ -308,7 +327,7 @@ def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
     {"cg128": workload_cg128, "jacobi3d_fp32": workload_jacobi3d_fp32, "varcoef512": workload_varcoef512,
-     "unet": workload_unet,
+     "unet": workload_unet, "unet_train": workload_unet_train,
      "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
 

@@ -75,6 +75,7 @@ _SIGS = {
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
+    "cfm_unet_time_train_step": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
                                           _c.c_float, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp]),
     "cfm_unet_set_validation": (_c.c_int, [_vp, _c.c_ulonglong, _c.c_int]),
@@ -555,6 +556,13 @@ class UNet:
     def time_forward(self, B=1, iters=20):
         ms = ctypes.c_double()
         check("cfm_unet_time_forward", lib.cfm_unet_time_forward(self.h, B, iters, ctypes.byref(ms)))
+        return ms.value
+
+    def time_train_step(self, B=8, iters=10):
+        """ms per training step (forward, backward, Adam) on synthetic inputs;
+        it changes the weights: use a scratch network."""
+        ms = ctypes.c_double()
+        check("cfm_unet_time_train_step", lib.cfm_unet_time_train_step(self.h, B, iters, ctypes.byref(ms)))
         return ms.value
 
     def gradient(self, x, dout):

@@ -858,6 +858,57 @@ int cfm_unet_time_forward(cfm_unet *h, int B, int iters, double *ms_per_forward)
     return CFM_OK;
 }
 
+// Deterministic bounded input and output-gradient patterns for the
+// training-step timing.
+__global__ void k_train_pattern(float *x, long long nx, float *d, long long nd) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nx;
+         i += (long long)gridDim.x * blockDim.x)
+        x[i] = (float)((i * 2654435761LL) % 2001 - 1000) * 5e-4f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nd;
+         i += (long long)gridDim.x * blockDim.x)
+        d[i] = (float)((i * 40503LL) % 2001 - 1000) * 1e-4f;
+}
+
+int cfm_unet_time_train_step(cfm_unet *h, int B, int iters, double *ms_per_step) {
+    clear_error();
+    CFM_ARG_CHECK(h && ms_per_step && iters >= 1, "arguments");
+    CFM_ARG_CHECK(B >= 1 && B <= h->maxB, "batch");
+    int H = 0, W = 0;
+    unet_shape(h->u, &H, &W);
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CFM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const long long px = (long long)B * H * W;
+    k_train_pattern<<<1024, 256, 0, s>>>(h->xin, 2 * px, h->dout, px);
+    auto step = [&]() -> int {
+        int st = unet_forward(h->u, B, h->xin, h->out, s);
+        if (st) return st;
+        if (cudaMemsetAsync(unet_grad(h->u), 0, unet_params(h->u) * sizeof(float), s) != cudaSuccess)
+            return CFM_CUDA_ERROR;
+        if ((st = unet_backward(h->u, B, h->xin, h->dout, s))) return st;
+        return unet_adam(h->u, 1e-4f, 1.0f, s);
+    };
+    int st = step();
+    if (!st) {
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < iters && !st; ++i) st = step();
+        cudaEventRecord(e1, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    float ms = 0;
+    if (!st && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (st) return st;
+    CFM_CUDA_TRY(e);
+    if ((st = unet_check_err(h->u))) return st;
+    *ms_per_step = ms / iters;
+    return CFM_OK;
+}
+
 // BF16 patterns of one activation of the last forward pass, in the order
 // h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0 (index 0..13), B images.
 int cfm_unet_activation_host(cfm_unet *h, int which, int B, unsigned short *out) {

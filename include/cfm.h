@@ -338,6 +338,11 @@ int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *d
 /* Device time of one forward pass of batch B on device-resident buffers
  * (mean over `iters` after a warm-up; CUDA events). */
 int cfm_unet_time_forward(cfm_unet *net, int B, int iters, double *ms_per_forward);
+/* Device time of one training step at batch B (forward, the backward pass
+ * of sum(out * dout) with its weight gradients, one Adam step at lr 1e-4)
+ * on fixed synthetic inputs, averaged over `iters` steps after one warm-up
+ * step.  It trains the network on those inputs: time a scratch network. */
+int cfm_unet_time_train_step(cfm_unet *net, int B, int iters, double *ms_per_step);
 /* BF16 patterns of one activation of the last forward pass (testing): index
  * 0..13 = h0 p1 h1 p2 h2 p3 h3 g3 u2 g2 u1 g1 u0 g0, NHWC at its level. */
 int cfm_unet_activation_host(cfm_unet *net, int which, int B, unsigned short *out);
