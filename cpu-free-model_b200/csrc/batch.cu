@@ -141,6 +141,22 @@ struct BtApply32 {
     }
 };
 
+// Two of a block's tiles per step (tile, tile + T): each pass computes both
+// rows' values before storing either, so their loads are in flight together.
+struct BtPair {
+    int t2;
+    bool has2, ok1, ok2;
+    long long i1, i2;
+    __device__ __forceinline__ BtPair(const BtSys &S, int tile, int T) {
+        t2 = tile + T;
+        has2 = t2 < S.ntiles;
+        i1 = (long long)tile * CG_TILE + threadIdx.x;
+        i2 = (long long)t2 * CG_TILE + threadIdx.x;
+        ok1 = i1 < S.n;
+        ok2 = has2 && i2 < S.n;
+    }
+};
+
 // Preconditioner z = J_m(r) over the team's tiles (damped Jacobi from
 // z = 0: the first sweep is w r / d, or r / d for smooth = 0), with the
 // <r, z> partials of the result into slot 0 and, when pcopy is set, p = z,
@@ -158,23 +174,32 @@ __device__ bool bt_precond(const BtArgs &a, const BtSys &S, int rank, int T, Bar
         if (m > 0 && !grid_barrier(bar, T, site++)) return false;
         const bool last = m == extra;
         TileSums<1> ts(sm, T, a.part + S.poff);
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            double q = 0.0;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                V zi;
-                if (m == 0)
-                    zi = a.smooth <= 0 ? r[g] / dg[g] : w * r[g] / dg[g];
-                else
-                    zi = src[g] + w * (r[g] - Apply()(a, S, src, i)) / dg[g];
-                dst[g] = zi;
-                if (last) {
-                    if (pcopy) pcopy[g] = zi;
-                    q = bt_prod(r[g], zi);
+        auto sweep_at = [&](long long i) -> V {
+            const long long g = S.off + i;
+            if (m == 0) return a.smooth <= 0 ? r[g] / dg[g] : w * r[g] / dg[g];
+            return src[g] + w * (r[g] - Apply()(a, S, src, i)) / dg[g];
+        };
+        for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+            const BtPair q(S, tile, T);
+            const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+            V z1 = V(0), z2 = V(0);
+            if (q.ok1) z1 = sweep_at(q.i1);
+            if (q.ok2) z2 = sweep_at(q.i2);
+            if (q.ok1) dst[g1] = z1;
+            if (q.ok2) dst[g2] = z2;
+            if (last) {
+                double p1 = 0.0, p2 = 0.0;
+                if (q.ok1) {
+                    if (pcopy) pcopy[g1] = z1;
+                    p1 = bt_prod(r[g1], z1);
                 }
+                if (q.ok2) {
+                    if (pcopy) pcopy[g2] = z2;
+                    p2 = bt_prod(r[g2], z2);
+                }
+                ts.add(tile, p1);
+                if (q.has2) ts.add(q.t2, p2);
             }
-            if (last) ts.add(tile, q);
         }
         if (last) ts.flush();
         src = dst;
@@ -238,16 +263,22 @@ __device__ bool bt_solve_mixed(const BtArgs &a, int sid, int rank, int T, Barrie
         // s = A p; <p, s>
         {
             TileSums<1> ts(sm, T, part + S.ntiles);
-            for (int tile = rank; tile < S.ntiles; tile += T) {
-                const long long i = (long long)tile * CG_TILE + threadIdx.x;
-                double q = 0.0;
-                if (i < S.n) {
-                    const long long g = S.off + i;
-                    const float si = bt_apply32(a, S, a.p32, i);
-                    a.s32[g] = si;
-                    q = bt_prod(a.p32[g], si);
+            for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+                const BtPair q(S, tile, T);
+                const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+                float s1 = 0.f, s2 = 0.f, p1 = 0.f, p2 = 0.f;
+                if (q.ok1) {
+                    s1 = bt_apply32(a, S, a.p32, q.i1);
+                    p1 = a.p32[g1];
                 }
-                ts.add(tile, q);
+                if (q.ok2) {
+                    s2 = bt_apply32(a, S, a.p32, q.i2);
+                    p2 = a.p32[g2];
+                }
+                if (q.ok1) a.s32[g1] = s1;
+                if (q.ok2) a.s32[g2] = s2;
+                ts.add(tile, q.ok1 ? bt_prod(p1, s1) : 0.0);
+                if (q.has2) ts.add(q.t2, q.ok2 ? bt_prod(p2, s2) : 0.0);
             }
             ts.flush();
         }
@@ -262,17 +293,37 @@ __device__ bool bt_solve_mixed(const BtArgs &a, int sid, int rank, int T, Barrie
         // d += alpha p; r -= alpha s; |r|^2
         {
             TileSums<1> ts(sm, T, part + 2 * S.ntiles);
-            for (int tile = rank; tile < S.ntiles; tile += T) {
-                const long long i = (long long)tile * CG_TILE + threadIdx.x;
-                double q = 0.0;
-                if (i < S.n) {
-                    const long long g = S.off + i;
-                    a.d32[g] = fmaf(af, a.p32[g], a.d32[g]);
-                    const float ri = fmaf(-af, a.s32[g], a.r32[g]);
-                    a.r32[g] = ri;
-                    q = bt_prod(ri, ri);
+            for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+                const BtPair q(S, tile, T);
+                const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+                float d1 = 0.f, p1 = 0.f, s1 = 0.f, r1 = 0.f, d2 = 0.f, p2 = 0.f, s2 = 0.f, r2 = 0.f;
+                if (q.ok1) {
+                    d1 = a.d32[g1];
+                    p1 = a.p32[g1];
+                    s1 = a.s32[g1];
+                    r1 = a.r32[g1];
                 }
-                ts.add(tile, q);
+                if (q.ok2) {
+                    d2 = a.d32[g2];
+                    p2 = a.p32[g2];
+                    s2 = a.s32[g2];
+                    r2 = a.r32[g2];
+                }
+                double q1 = 0.0, q2 = 0.0;
+                if (q.ok1) {
+                    a.d32[g1] = fmaf(af, p1, d1);
+                    const float ri = fmaf(-af, s1, r1);
+                    a.r32[g1] = ri;
+                    q1 = bt_prod(ri, ri);
+                }
+                if (q.ok2) {
+                    a.d32[g2] = fmaf(af, p2, d2);
+                    const float ri = fmaf(-af, s2, r2);
+                    a.r32[g2] = ri;
+                    q2 = bt_prod(ri, ri);
+                }
+                ts.add(tile, q1);
+                if (q.has2) ts.add(q.t2, q2);
             }
             ts.flush();
         }
@@ -334,12 +385,20 @@ __device__ bool bt_solve_mixed(const BtArgs &a, int sid, int rank, int T, Barrie
         const float bf = (float)(rz1 / rz);
         rz = rz1;
         // p = z + beta p
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                a.p32[g] = fmaf(bf, a.p32[g], a.z32[g]);
+        for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+            const BtPair q(S, tile, T);
+            const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+            float p1 = 0.f, z1 = 0.f, p2 = 0.f, z2 = 0.f;
+            if (q.ok1) {
+                p1 = a.p32[g1];
+                z1 = a.z32[g1];
             }
+            if (q.ok2) {
+                p2 = a.p32[g2];
+                z2 = a.z32[g2];
+            }
+            if (q.ok1) a.p32[g1] = fmaf(bf, p1, z1);
+            if (q.ok2) a.p32[g2] = fmaf(bf, p2, z2);
         }
         if (!grid_barrier(bar, T, site++)) return false;
     }
@@ -397,16 +456,22 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
         // s = A p; <p, s>
         {
             TileSums<1> ts(sm, T, part + S.ntiles);
-            for (int tile = rank; tile < S.ntiles; tile += T) {
-                const long long i = (long long)tile * CG_TILE + threadIdx.x;
-                double ps = 0.0;
-                if (i < S.n) {
-                    const long long g = S.off + i;
-                    const double si = bt_apply(a, S, a.p, i);
-                    a.s[g] = si;
-                    ps = a.p[g] * si;
+            for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+                const BtPair q(S, tile, T);
+                const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+                double s1 = 0.0, s2 = 0.0, p1 = 0.0, p2 = 0.0;
+                if (q.ok1) {
+                    s1 = bt_apply(a, S, a.p, q.i1);
+                    p1 = a.p[g1];
                 }
-                ts.add(tile, ps);
+                if (q.ok2) {
+                    s2 = bt_apply(a, S, a.p, q.i2);
+                    p2 = a.p[g2];
+                }
+                if (q.ok1) a.s[g1] = s1;
+                if (q.ok2) a.s[g2] = s2;
+                ts.add(tile, q.ok1 ? p1 * s1 : 0.0);
+                if (q.has2) ts.add(q.t2, q.ok2 ? p2 * s2 : 0.0);
             }
             ts.flush();
         }
@@ -420,17 +485,37 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
         // x += alpha p; r -= alpha s; |r|^2
         {
             TileSums<1> ts(sm, T, part + 2 * S.ntiles);
-            for (int tile = rank; tile < S.ntiles; tile += T) {
-                const long long i = (long long)tile * CG_TILE + threadIdx.x;
-                double q = 0.0;
-                if (i < S.n) {
-                    const long long g = S.off + i;
-                    a.x[g] = fma(alpha, a.p[g], a.x[g]);
-                    const double ri = fma(-alpha, a.s[g], a.r[g]);
-                    a.r[g] = ri;
-                    q = ri * ri;
+            for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+                const BtPair q(S, tile, T);
+                const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+                double x1 = 0.0, p1 = 0.0, s1 = 0.0, r1 = 0.0, x2 = 0.0, p2 = 0.0, s2 = 0.0, r2 = 0.0;
+                if (q.ok1) {
+                    x1 = a.x[g1];
+                    p1 = a.p[g1];
+                    s1 = a.s[g1];
+                    r1 = a.r[g1];
                 }
-                ts.add(tile, q);
+                if (q.ok2) {
+                    x2 = a.x[g2];
+                    p2 = a.p[g2];
+                    s2 = a.s[g2];
+                    r2 = a.r[g2];
+                }
+                double q1 = 0.0, q2 = 0.0;
+                if (q.ok1) {
+                    a.x[g1] = fma(alpha, p1, x1);
+                    const double ri = fma(-alpha, s1, r1);
+                    a.r[g1] = ri;
+                    q1 = ri * ri;
+                }
+                if (q.ok2) {
+                    a.x[g2] = fma(alpha, p2, x2);
+                    const double ri = fma(-alpha, s2, r2);
+                    a.r[g2] = ri;
+                    q2 = ri * ri;
+                }
+                ts.add(tile, q1);
+                if (q.has2) ts.add(q.t2, q2);
             }
             ts.flush();
         }
@@ -450,12 +535,20 @@ __device__ bool bt_solve(const BtArgs &a, int sid, int rank, int T, BarrierState
         const double beta = rz1 / rz;
         rz = rz1;
         // p = z + beta p
-        for (int tile = rank; tile < S.ntiles; tile += T) {
-            const long long i = (long long)tile * CG_TILE + threadIdx.x;
-            if (i < S.n) {
-                const long long g = S.off + i;
-                a.p[g] = fma(beta, a.p[g], a.z[g]);
+        for (int tile = rank; tile < S.ntiles; tile += 2 * T) {
+            const BtPair q(S, tile, T);
+            const long long g1 = S.off + q.i1, g2 = S.off + q.i2;
+            double p1 = 0.0, z1 = 0.0, p2 = 0.0, z2 = 0.0;
+            if (q.ok1) {
+                p1 = a.p[g1];
+                z1 = a.z[g1];
             }
+            if (q.ok2) {
+                p2 = a.p[g2];
+                z2 = a.z[g2];
+            }
+            if (q.ok1) a.p[g1] = fma(beta, p1, z1);
+            if (q.ok2) a.p[g2] = fma(beta, p2, z2);
         }
         if (!grid_barrier(bar, T, site++)) return false;
     }
