@@ -148,7 +148,6 @@ int main(int argc, char **argv) {
         }
         cfm_cg_params pp = base;
         pp.impl = ver.impl;
-        if (pp.impl == CFM_CG_PERSISTENT_PIPELINED) pp.impl = CFM_CG_PERSISTENT;
         cfm_cg *h = nullptr;
         if ((st = cfm_cg_create(A, &pp, &h))) return cli::fail("cfm_cg_create", st);
         for (int run = 1; run <= num_runs; ++run) {
@@ -177,8 +176,9 @@ int main(int argc, char **argv) {
                         "%8.2f, efficiency: %8.2f \n",
                         t_ref, s.seconds, t_ref / s.seconds, t_ref / s.seconds * 100);
             }
-            std::printf("Iterations: %lld, true relative residual: %.3e, %.1f GB/s, %d launches%s\n",
-                        s.iterations, s.residual, s.gbs, s.launches,
+            std::printf("Iterations: %lld, restarts: %d, true relative residual: %.3e, %.1f GB/s, "
+                        "%d launches%s\n",
+                        s.iterations, s.refinements, s.residual, s.gbs, s.launches,
                         st == CFM_NOT_CONVERGED ? " (not converged)" : "");
         }
         cfm_cg_destroy(h);

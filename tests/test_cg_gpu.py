@@ -107,3 +107,28 @@ def test_cg_on_matrixmarket_file(tmp_path):
     assert out.returncode == 0, out.stderr
     first = next(t for t in out.stdout.split() if t.replace(".", "", 1).isdigit())
     assert float(first) > 0  # the first float is the time, as the reference prints it
+
+
+@pytest.mark.parametrize("version,method", [(2, "std"), (3, "pipelined"), (5, "std"), (9, "pipelined")])
+def test_cg_binary_versions_run_their_kernel(version, method):
+    """The binary's "Single Stream Standard / Pipelined" versions run the
+    standard and the pipelined persistent kernels: the iteration count and
+    the restarts (the pipelined kernel's residual replacement every 50
+    iterations) are that method's (the oracle's), in one launch."""
+    import os
+    import re
+    import subprocess
+
+    g = 16
+    rowptr, col, val = cfm.poisson3d(g)
+    b = cfm.CSR(rowptr, col, val).spmv(cfm.uniform(0, len(rowptr) - 1))
+    m = oracle.STD if method == "std" else oracle.PIPELINED
+    _, st_o, it_o, rs_o, _ = oracle.krylov_csr(rowptr, col, val, b, m, 20000, 1e-8)
+    binary = os.path.join(os.path.dirname(cfm.__file__), "bin", "cg")
+    out = subprocess.run([binary, "-v", str(version), "-s", "-problem", "poisson", "-grid", str(g), "-tol", "1e-8"],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    its, rs = map(int, re.search(r"Iterations: (\d+), restarts: (\d+)", out.stdout).groups())
+    assert st_o == 0 and (its, rs) == (it_o, rs_o)
+    assert rs == (1 if method == "pipelined" else 0)
+    assert "1 launches" in out.stdout
