@@ -147,7 +147,7 @@ STD, PIPELINED, MIXED = 0, 1, 2
 
 def krylov_csr(rowptr, col, val, b, method, maxiter, tol, inner_maxiter=0, inner_tol=0.0, threads=0):
     """Persistent-solver restatement on a CSR matrix.
-    Returns (x, status, iterations, restarts_or_sweeps, true relative residual)."""
+    Returns (x, status, iterations, restarts or FP64 updates, true relative residual)."""
     rowptr = np.ascontiguousarray(rowptr, np.int32)
     col = np.ascontiguousarray(col, np.int32)
     val = np.ascontiguousarray(val, np.float64)

@@ -201,3 +201,28 @@ def test_oracle_cg_breakdown_on_indefinite():
     A = sp.diags([1.0, -1.0, 2.0]).tocsr()
     _, st, _, _ = oracle.cg(A.indptr, A.indices, A.data, np.array([1.0, 1.0, 0.0]), 10, 1e-12)
     assert st == 4
+
+
+@pytest.mark.parametrize("g", [6, 14])
+def test_oracle_mixed_reliable_updates_keep_the_fp64_count(g):
+    """The mixed-precision restatement (FP32 CG with FP64 reliable updates)
+    keeps the search direction across its updates: on Poisson it needs the
+    FP64 iteration count, with several FP64 updates, and its answer meets
+    the FP64 true-residual tolerance and SciPy's solution."""
+    A = poisson_scipy(g)
+    xs = np.random.default_rng(g).uniform(-1, 1, A.shape[0])
+    b = A @ xs
+    _, st64, it64, _, _ = oracle.krylov_csr(A.indptr, A.indices, A.data, b, oracle.STD, 20000, 1e-9)
+    x, st, it, ups, rr = oracle.krylov_csr(A.indptr, A.indices, A.data, b, oracle.MIXED, 20000, 1e-9)
+    assert st64 == 0 and st == 0 and rr <= 1e-9
+    assert abs(it - it64) <= 1 and ups >= 2
+    np.testing.assert_allclose(x, spla.spsolve(A.tocsc(), b), rtol=0, atol=1e-7)
+
+
+def test_oracle_mixed_independent_of_threads():
+    A = poisson_scipy(11)
+    b = A @ np.random.default_rng(3).uniform(-1, 1, A.shape[0])
+    runs = [oracle.krylov_csr(A.indptr, A.indices, A.data, b, oracle.MIXED, 20000, 1e-9, threads=t)
+            for t in (1, 3)]
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1:4] == runs[1][1:4]
