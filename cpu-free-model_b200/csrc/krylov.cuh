@@ -201,10 +201,6 @@ struct CsrOp {
                                            double &y1, double &y2) const {
         apply2_t(val, x, i, v1, i2, v2, y1, y2);
     }
-    __device__ __forceinline__ void apply2_32(const float *x, int i, bool v1, int i2, bool v2,
-                                              float &y1, float &y2) const {
-        apply2_t(val32, x, i, v1, i2, v2, y1, y2);
-    }
     // FP32 apply for the rows of a tile group (0 for an absent row), their
     // entries interleaved.
     template <int U>
@@ -277,11 +273,6 @@ struct StencilOp {
                                            double &y1, double &y2) const {
         y1 = v1 ? apply(x, i) : 0.0;
         y2 = v2 ? apply(x, i2) : 0.0;
-    }
-    __device__ __forceinline__ void apply2_32(const float *x, int i, bool v1, int i2, bool v2,
-                                              float &y1, float &y2) const {
-        y1 = v1 ? apply32(x, i) : 0.f;
-        y2 = v2 ? apply32(x, i2) : 0.f;
     }
     template <int U>
     __device__ __forceinline__ Vals32<U> applyN32(const float *x, const TileGroup<U> &g) const {
