@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["jacobi3d", "jacobi3d_fp32", "cg128", "varcoef512", "unet", "unet_train",
-                                           "batch256"],
+                                           "batch256", "cpufree"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -259,6 +259,54 @@ def workload_unet_train(args, cfm):
          dtype="bf16")
 
 
+def workload_cpufree(args, cfm):
+    """The reference's own 1-GPU comparison: CPU-controlled (a host launch
+    per sweep / per CG phase) against CPU-free (one persistent launch), on
+    the reference's cases: 2D Jacobi 256^2 FP32 (its launch-bound weak-scaling
+    point) and 16384^2 FP32, and CG on its default random tridiagonal matrix
+    (n = 20,971,520, b = ones, 1000 iterations, no tolerance exit)."""
+    import statistics as stt
+    out = {}
+    for n2, niter in ((256, 20000), (16384, 200)):
+        row = {}
+        for impl, name in ((cfm.JACOBI_HOST_LOOP, "host_loop"), (cfm.JACOBI_PERSISTENT, "persistent"),
+                           (cfm.JACOBI_RESIDENT, "resident")):
+            j = cfm.Jacobi(2, n2, n2, 1, cfm.FP32, 1, impl)
+            if impl == cfm.JACOBI_RESIDENT and j.launch_shape()[1] != 1024:
+                j.close()
+                continue  # does not fit on chip: no resident form at this size
+            j.load_problem(cfm.PROBLEM_REF)
+            for _ in range(max(args.warmup, 1)):
+                j.run(niter)
+            ts = [j.run(niter).seconds for _ in range(max(args.steps, 3))]
+            t = stt.median(ts)
+            row[name] = {"us_per_sweep": t / niter * 1e6, "glups": (n2 - 2) ** 2 * niter / t / 1e9}
+            j.close()
+        out[f"jacobi2d_{n2}_fp32"] = row
+    n = 20971520
+    rowptr, col, val = cfm.tridiag(n)
+    A = cfm.CSR(rowptr, col, val)
+    cgr = {}
+    for impl, name in ((cfm.CG_DISCRETE, "cpu_controlled_standard"), (cfm.CG_PERSISTENT, "cpu_free_standard"),
+                       (cfm.CG_PERSISTENT_PIPELINED, "cpu_free_pipelined")):
+        cg = cfm.CG(A, impl, 1000, 0.0)
+        cg.solve(None)
+        ts = [cg.solve(None)[1].seconds for _ in range(max(args.steps, 3))]
+        cgr[name] = {"s_per_1000_iterations": stt.median(ts)}
+        cg.close()
+    out["cg_tridiag_20971520"] = cgr
+    speed = cgr["cpu_controlled_standard"]["s_per_1000_iterations"] / cgr["cpu_free_standard"]["s_per_1000_iterations"]
+    j256 = out["jacobi2d_256_fp32"]
+    line("CPU-free over CPU-controlled speedup, CG standard on the reference's tridiagonal matrix", speed, "x",
+         args, cgr["cpu_free_standard"]["s_per_1000_iterations"] * 1e3,
+         {"workload": "cpufree_vs_cpu_controlled_1gpu", "cases": out,
+          "jacobi2d_256_host_loop_over_persistent": j256["host_loop"]["us_per_sweep"] / j256["persistent"]["us_per_sweep"],
+          "jacobi2d_256_host_loop_over_resident": j256["host_loop"]["us_per_sweep"] / j256["resident"]["us_per_sweep"],
+          "reference_a100": {"jacobi2d_256_us_per_iter_copy_vs_design2": [8.9, 2.4],
+                             "cg_tridiag_1000_iter_s_discrete_vs_persistent": [19.99, 10.66]},
+          "timing": "CUDA events per call (b and x copies included for CG), median of steps"})
+
+
 def batch_bytes_per_iteration(dims, n, smooth, word):
     """Algorithmic bytes of one PCG iteration of one batched system: the
     operator pass (c coefficient arrays + p read + s write), the x / r update
@@ -327,7 +375,7 @@ def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
     {"cg128": workload_cg128, "jacobi3d_fp32": workload_jacobi3d_fp32, "varcoef512": workload_varcoef512,
-     "unet": workload_unet, "unet_train": workload_unet_train,
+     "unet": workload_unet, "unet_train": workload_unet_train, "cpufree": workload_cpufree,
      "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
 

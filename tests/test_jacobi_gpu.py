@@ -37,9 +37,12 @@ def run_gpu(a, niter, impl, periodic_y=0):
 
 @pytest.mark.parametrize("impl", IMPLS)
 @pytest.mark.parametrize("prec", PRECS)
-@pytest.mark.parametrize("shape", [(3, 3), (9, 7), (17, 33), (70, 130), (1026, 100)])
+@pytest.mark.parametrize("shape", [(3, 3), (9, 7), (17, 33), (70, 130), (1026, 100), (6, 4), (5, 64),
+                                   (37, 128), (260, 256), (300, 1032)])
 @pytest.mark.parametrize("niter", [0, 1, 2, 7])
 def test_jacobi2d_random_bitexact(impl, prec, shape, niter):
+    """Rows of a multiple of 16 bytes take the row-marching vector kernel,
+    the others the warp-per-segment one; both equal the oracle."""
     a = rand_grid(shape, cfm.np_dtype(prec), 11)
     got, _ = run_gpu(a, niter, impl)
     np.testing.assert_array_equal(got, oracle.jacobi2d(a, niter))
