@@ -812,8 +812,15 @@ int choose_launch(cfm_jacobi *h) {
         const long long ntiles = (long long)((p.nx + 31) / 32) * ((p.ny - 2 + J3_TY - 1) / J3_TY);
         h->zchunk = pick_zchunk(ntiles, p.nz - 2, &h->blocks);
     } else {
-        const long long nseg = (long long)((p.nx + 31) / 32) * (p.ny - 2);
-        const long long need = (nseg * 32 + threads - 1) / threads;
+        // no more blocks than there are warp work units (more only lengthen
+        // the grid barrier): row segments of 32 columns, or for the
+        // row-marching kernel tiles of 16-byte lanes over row chunks of at
+        // least 8 rows
+        const int vec = 16 / (int)h->esize;
+        const bool march = p.nx % vec == 0;
+        const long long units = march ? (long long)((p.nx + 32 * vec - 1) / (32 * vec)) * ((p.ny - 2 + 7) / 8)
+                                      : (long long)((p.nx + 31) / 32) * (p.ny - 2);
+        const long long need = (units * 32 + threads - 1) / threads;
         if (need < h->blocks) h->blocks = (int)std::max(1LL, need);
     }
     if (p.dims == 2 && p.impl == CFM_JACOBI_RESIDENT) {
