@@ -18,7 +18,7 @@
 //    conditional WHILE node repeats it on the device until the residual
 //    reaches the tolerance, so the host launches the whole solve once.
 //    If the loop stalls or hits its cap, plain FP64 persistent CG finishes
-//    from the current iterate (the fallback) and judges the result by the
+//    from the current iterate (the fallback) and checks the result by the
 //    FP64 true residual.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
