@@ -205,36 +205,40 @@ double orc_jacobi3d_bench_f64(int nx, int ny, int nz, int niter, int threads) {
 
 /* Stencil/jacobi2D/src/common.cu:44-66: rows 1..ny-2, every column, east and
  * west clamped at the x edges, 0.25f * (N + S + E + W), then the same halo
- * rows copies as single_gpu(). */
-int orc_jacobi2d_mirror_f32(int nx, int ny, int niter, const float *in, float *out, int threads) {
-    if (nx < 2 || ny < 3 || niter < 0 || !in || !out) return 1;
-    size_t N = (size_t)nx * ny;
-    float *a = (float *)malloc(sizeof(float) * N), *b = (float *)malloc(sizeof(float) * N);
-    if (!a || !b) { free(a); free(b); return 1; }
-    memcpy(a, in, sizeof(float) * N);
-    memcpy(b, in, sizeof(float) * N);
-    for (int it = 0; it < niter; ++it) {
-#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
-        for (int iy = 1; iy < ny - 1; ++iy) {
-            const float *r = a + (size_t)iy * nx;
-            float *w = b + (size_t)iy * nx;
-            for (int ix = 0; ix < nx; ++ix) {
-                float e = r[ix + (ix < nx - 1)];
-                float wv = r[ix - (ix > 0)];
-                float s = r[ix + nx] + r[ix - nx];
-                s = s + e;
-                s = s + wv;
-                w[ix] = 0.25f * s;
-            }
-        }
-        memcpy(b, b + (size_t)(ny - 2) * nx, sizeof(float) * nx);
-        memcpy(b + (size_t)(ny - 1) * nx, b + (size_t)nx, sizeof(float) * nx);
-        float *t = a; a = b; b = t;
+ * rows copies as single_gpu().  The reference is FP32; the FP64 twin runs the
+ * same steps in double. */
+#define ORC_MIRROR2D(NAME, T)                                                         \
+    int NAME(int nx, int ny, int niter, const T *in, T *out, int threads) {           \
+        if (nx < 2 || ny < 3 || niter < 0 || !in || !out) return 1;                   \
+        size_t N = (size_t)nx * ny;                                                   \
+        T *a = (T *)malloc(sizeof(T) * N), *b = (T *)malloc(sizeof(T) * N);           \
+        if (!a || !b) { free(a); free(b); return 1; }                                 \
+        memcpy(a, in, sizeof(T) * N);                                                 \
+        memcpy(b, in, sizeof(T) * N);                                                 \
+        for (int it = 0; it < niter; ++it) {                                          \
+            _Pragma("omp parallel for num_threads(nthreads(threads)) schedule(static)") \
+            for (int iy = 1; iy < ny - 1; ++iy) {                                     \
+                const T *r = a + (size_t)iy * nx;                                     \
+                T *w = b + (size_t)iy * nx;                                           \
+                for (int ix = 0; ix < nx; ++ix) {                                     \
+                    T e = r[ix + (ix < nx - 1)];                                      \
+                    T wv = r[ix - (ix > 0)];                                          \
+                    T s = r[ix + nx] + r[ix - nx];                                    \
+                    s = s + e;                                                        \
+                    s = s + wv;                                                       \
+                    w[ix] = (T)0.25 * s;                                              \
+                }                                                                     \
+            }                                                                         \
+            memcpy(b, b + (size_t)(ny - 2) * nx, sizeof(T) * nx);                     \
+            memcpy(b + (size_t)(ny - 1) * nx, b + (size_t)nx, sizeof(T) * nx);        \
+            T *t = a; a = b; b = t;                                                   \
+        }                                                                             \
+        memcpy(out, a, sizeof(T) * N);                                                \
+        free(a); free(b);                                                             \
+        return 0;                                                                     \
     }
-    memcpy(out, a, sizeof(float) * N);
-    free(a); free(b);
-    return 0;
-}
+ORC_MIRROR2D(orc_jacobi2d_mirror_f32, float)
+ORC_MIRROR2D(orc_jacobi2d_mirror_f64, double)
 
 /* -------------------------------------------------------------------- CG */
 

@@ -16,9 +16,13 @@
  *
  * Parity pin: the Jacobi FP32 restatement is checked bit-for-bit against
  * grids written by the reference's own single_gpu() (oracle/ref/, fixtures
- * in tests/golden/).  The CG reference needs NVSHMEM and MPI to build, so the
- * CG restatement is unpinned against reference outputs; tests cross-check it
- * against SciPy and manufactured solutions.
+ * in tests/golden/ref_jacobi*.npz).  The CG restatement is checked against x
+ * written by the reference's own SingleGPUDiscreteStandard::run_single_gpu()
+ * (CG/src/common.cu compiled unmodified with oracle/ref/shim standing in for
+ * the NVSHMEM calls of its multi-GPU kernels; fixtures
+ * tests/golden/ref_cg_*.npz) to 1e-12 relative -- not bit for bit, since the
+ * reference sums its dots with atomicAdd in arrival order -- and cross-
+ * checked against SciPy and manufactured solutions.
  */
 #ifndef CFM_ORACLE_H
 #define CFM_ORACLE_H
@@ -45,8 +49,9 @@ int orc_jacobi3d_f32(int nx, int ny, int nz, int niter, int periodic_y, const fl
  * the seconds of the sweep loop alone (-1 on bad arguments). */
 double orc_jacobi3d_bench_f64(int nx, int ny, int nz, int niter, int threads);
 /* The reference's PERKS mirror-boundary sweep (Stencil/jacobi2D/src/common.cu:44-66),
- * FP32, all x columns updated with clamped east/west neighbours. */
+ * FP32 (and its FP64 twin), all x columns updated with clamped east/west neighbours. */
 int orc_jacobi2d_mirror_f32(int nx, int ny, int niter, const float *in, float *out, int threads);
+int orc_jacobi2d_mirror_f64(int nx, int ny, int niter, const double *in, double *out, int threads);
 
 /* Deterministic dot product (the tile tree the GPU uses). */
 double orc_dot(long long n, const double *a, const double *b, int threads);

@@ -3,8 +3,8 @@
 Imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline and
 --impl reference legs, always as the checker or the timed host baseline,
 never as the thing measured.  See cfm_oracle.h for the reference lines each
-function restates.  Also exposes the reference's own single-GPU Jacobi runs
-(oracle/_ref, built from the reference sources) when they were built.
+function restates.  Also exposes the reference's own single-GPU Jacobi and CG
+runs (oracle/_ref, built from the reference sources) when they were built.
 """
 import ctypes
 import os
@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF2D_PATH = os.path.join(HERE, "_ref", "libref_jacobi2d.so")
 REF3D_PATH = os.path.join(HERE, "_ref", "libref_jacobi3d.so")
+REFCG_PATH = os.path.join(HERE, "_ref", "libref_cg.so")
 
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -34,6 +35,7 @@ def _load():
         "orc_jacobi3d_f64": [_i, _i, _i, _i, _i, _vp, _vp, _i],
         "orc_jacobi3d_f32": [_i, _i, _i, _i, _i, _vp, _vp, _i],
         "orc_jacobi2d_mirror_f32": [_i, _i, _i, _vp, _vp, _i],
+        "orc_jacobi2d_mirror_f64": [_i, _i, _i, _vp, _vp, _i],
         "orc_cg": [_i, _vp, _vp, _vp, _vp, _i, ctypes.c_double, _vp, _vp, _vp, _i],
         "orc_spmv": [_i, _vp, _vp, _vp, _vp, _vp, _i],
         "orc_max_threads": [],
@@ -90,10 +92,13 @@ def jacobi2d(a, niter, threads=0):
 
 
 def jacobi2d_mirror(a, niter, threads=0):
-    a = np.ascontiguousarray(a, np.float32)
+    a = np.ascontiguousarray(a)
+    if a.dtype != np.float64:
+        a = np.ascontiguousarray(a, np.float32)
     ny, nx = a.shape
     out = np.empty_like(a)
-    assert lib.orc_jacobi2d_mirror_f32(nx, ny, niter, _p(a), _p(out), threads) == 0
+    assert getattr(lib, f"orc_jacobi2d_mirror_{_suffix(a.dtype)}")(nx, ny, niter, _p(a), _p(out),
+                                                                  threads) == 0
     return out
 
 
@@ -220,3 +225,41 @@ def ref_jacobi3d(nx, ny, nz, niter):
     out = np.empty((nz, ny, nx), np.float32)
     lib.ref_jacobi3d_single_gpu(nx, ny, nz, niter, _p(out))
     return out
+
+
+def ref_cg_available():
+    return os.path.exists(REFCG_PATH)
+
+
+def _ref_cg_lib():
+    lib = ctypes.CDLL(REFCG_PATH)
+    lib.ref_cg_standard.argtypes = [_i, _i, _vp, _vp, _vp, _i, _i, _vp]
+    lib.ref_cg_standard.restype = ctypes.c_double
+    lib.ref_gen_tridiag.argtypes = [_i, _vp, _vp, _vp]
+    lib.ref_gen_tridiag.restype = _i
+    return lib
+
+
+def ref_cg(rowptr, col, val, niter):
+    """The reference's SingleGPUDiscreteStandard::run_single_gpu() on the
+    current GPU: b = ones, x0 = 0, exactly `niter` iterations.  The index base
+    is taken from rowptr[0], as the reference's main() does.  Returns x."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    col = np.ascontiguousarray(col, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    n = len(rowptr) - 1
+    x = np.empty(n)
+    t = _ref_cg_lib().ref_cg_standard(n, len(val), _p(rowptr), _p(col), _p(val),
+                                       int(rowptr[0] == 0), niter, _p(x))
+    assert t >= 0, "reference CG run failed"
+    return x
+
+
+def ref_tridiag(n):
+    """The reference's genTridiag() from libc rand()'s unseeded start state."""
+    nnz = 3 * (n - 2) + 4
+    rowptr = np.empty(n + 1, np.int32)
+    col = np.empty(nnz, np.int32)
+    val = np.empty(nnz)
+    assert _ref_cg_lib().ref_gen_tridiag(n, _p(rowptr), _p(col), _p(val)) == 0
+    return rowptr, col, val

@@ -12,6 +12,29 @@ for p in (ROOT, PKG, ORACLE):
         sys.path.insert(0, p)
 
 
+def ref_cg_fixtures():
+    """tests/golden/ref_cg_*.npz: x written by the reference's own single-GPU
+    CG (made by tests/golden/make_ref_fixtures.py)."""
+    import glob
+    return sorted(glob.glob(os.path.join(GOLDEN, "ref_cg_*.npz")))
+
+
+def ref_cg_system(path):
+    """(rowptr, col, val, niter, x_ref) of a reference CG fixture, the matrix
+    in the index base the reference was given."""
+    import numpy as np
+
+    import cfm
+    f = np.load(path)
+    if str(f["matrix"]) == "tridiag":
+        rowptr, col, val = f["rowptr"], f["col"], f["val"]
+    else:
+        rowptr, col, val = cfm.poisson3d(int(f["size"]))
+    if bool(f["one_based"]):
+        rowptr, col = rowptr + 1, col + 1
+    return rowptr, col, val, int(f["niter"]), f["x"]
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA library")
 

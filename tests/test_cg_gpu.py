@@ -6,6 +6,7 @@ import pytest
 
 import cfm
 import oracle
+from conftest import ref_cg_fixtures, ref_cg_system
 
 pytestmark = pytest.mark.gpu
 
@@ -43,6 +44,20 @@ def test_cg_reference_mode_fixed_count_tridiag(impl):
     x, st = cfm.CG(A, impl, 25, 0.0).solve(None)
     assert st.iterations == 25 == it_o
     np.testing.assert_array_equal(x, x_o)
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("path", ref_cg_fixtures(), ids=lambda p: p.rsplit("/", 1)[-1])
+def test_cg_matches_reference_run(impl, path):
+    """Parity with the reference's own single-GPU CG (x written by
+    SingleGPUDiscreteStandard::run_single_gpu(), CG/src/common.cu:399-538, on a
+    B200): b = ones, x0 = 0, the same fixed count; x within 1e-12 relative
+    (the reference's dots are atomicAdd sums in arrival order)."""
+    rowptr, col, val, niter, x_ref = ref_cg_system(path)
+    x, st = cfm.CG(cfm.CSR(rowptr, col, val), impl, niter, 0.0).solve(None)
+    assert st.iterations == niter
+    rel = np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref)
+    assert rel <= 1e-12, rel
 
 
 def test_cg_one_based_csr_same_result():

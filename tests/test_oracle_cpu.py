@@ -9,7 +9,7 @@ import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 import oracle
-from conftest import GOLDEN
+from conftest import GOLDEN, ref_cg_fixtures, ref_cg_system
 
 
 # ---------------------------------------------------------------- numpy restatements
@@ -195,6 +195,42 @@ def test_oracle_cg_fixed_count_reference_mode():
     x, st, it, rr = oracle.cg(A.indptr, A.indices, A.data, None, 30, 0.0)
     assert st == 0 and it == 30
     np.testing.assert_allclose(A @ x, np.ones(A.shape[0]), atol=1e-9)
+
+
+def test_reference_cg_fixtures_present():
+    assert len(ref_cg_fixtures()) >= 5, "tests/golden/ref_cg_*.npz missing"
+
+
+@pytest.mark.parametrize("path", ref_cg_fixtures(), ids=os.path.basename)
+def test_oracle_cg_matches_reference_run(path):
+    """Pin: the CG restatement agrees with x written by the reference's own
+    SingleGPUDiscreteStandard::run_single_gpu() (CG/src/common.cu:399-538;
+    b = ones, x0 = 0, a fixed count) to 1e-12 relative.  Not bit for bit: the
+    reference sums its dots with atomicAdd(double) in arrival order, the
+    oracle in a fixed tree."""
+    rowptr, col, val, niter, x_ref = ref_cg_system(path)
+    x, st, it, _ = oracle.cg(rowptr, col, val, None, niter, 0.0)
+    assert st == 0 and it == niter
+    rel = np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref)
+    assert rel <= 1e-12, rel
+
+
+def test_tridiag_generator_matches_reference():
+    """cfm_tridiag_csr from libc rand()'s unseeded state is the reference's
+    genTridiag (CG/src/common.cu:46-76) bit for bit: the fixtures store the
+    matrix the reference generated."""
+    import ctypes
+
+    import cfm
+    paths = [p for p in ref_cg_fixtures() if "tridiag" in os.path.basename(p)]
+    assert paths
+    for p in paths:
+        f = np.load(p)
+        ctypes.CDLL(None).srand(1)
+        rowptr, col, val = cfm.tridiag(int(f["size"]))
+        np.testing.assert_array_equal(rowptr, f["rowptr"])
+        np.testing.assert_array_equal(col, f["col"])
+        np.testing.assert_array_equal(val, f["val"])
 
 
 def test_oracle_cg_breakdown_on_indefinite():
