@@ -17,6 +17,7 @@ OK, BAD_ARG, CUDA_ERROR, BARRIER_TIMEOUT, BREAKDOWN, NOT_CONVERGED, NO_DEVICE, U
 FP64, FP32 = 0, 1
 PROBLEM_REF, PROBLEM_CONFIG = 0, 1
 JACOBI_HOST_LOOP, JACOBI_HOST_LOOP_INKERNEL_HALO, JACOBI_PERSISTENT, JACOBI_RESIDENT = range(4)
+BOUNDARY_DIRICHLET, BOUNDARY_MIRROR = 0, 1
 CG_DISCRETE, CG_PERSISTENT, CG_PERSISTENT_PIPELINED, CG_MIXED = range(4)
 
 # Every function include/cfm.h declares, with (restype, argtypes).
@@ -32,6 +33,7 @@ _SIGS = {
     "cfm_jacobi_create": (_c.c_int, [_vp, _vp]),
     "cfm_jacobi_destroy": (None, [_vp]),
     "cfm_jacobi_set_stream": (_c.c_int, [_vp, _vp]),
+    "cfm_jacobi_set_boundary": (_c.c_int, [_vp, _c.c_int]),
     "cfm_jacobi_load_problem": (_c.c_int, [_vp, _c.c_int]),
     "cfm_jacobi_upload": (_c.c_int, [_vp, _vp]),
     "cfm_jacobi_download": (_c.c_int, [_vp, _vp]),
@@ -232,6 +234,11 @@ class Jacobi:
 
     def set_stream(self, stream_handle):
         check("cfm_jacobi_set_stream", lib.cfm_jacobi_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def set_boundary(self, boundary):
+        """BOUNDARY_DIRICHLET (fixed x columns) or, 2D only, BOUNDARY_MIRROR
+        (the reference's PERKS comparator sweep)."""
+        check("cfm_jacobi_set_boundary", lib.cfm_jacobi_set_boundary(self.h, boundary))
 
     def device_grid(self):
         return lib.cfm_jacobi_device_grid(self.h)

@@ -114,6 +114,55 @@ __global__ void __launch_bounds__(256) j2d_sweeps_kernel(T *g0, T *g1, int nx, i
     }
 }
 
+// 2D sweep with the mirror x boundary of the reference's PERKS comparator
+// (jacobi_kernel_single_gpu_mirror, Stencil/jacobi2D/src/common.cu:44-66):
+// every column of the interior rows is updated, the east and west neighbours
+// clamped to the cell itself at x = nx-1 and x = 0, summed as
+// 0.25 * (((N + S) + E) + W) with N the row below in memory (iy + 1).  One
+// warp per 32-column segment as in j2d_sweeps_kernel; with IMAGES the
+// periodic halo rows are written in-kernel (whole rows, corners included).
+template <typename T, bool IMAGES>
+__global__ void __launch_bounds__(256) j2d_mirror_kernel(T *g0, T *g1, int nx, int ny, int niter,
+                                                         BarrierState *bar) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int ntx = (nx + 31) >> 5;
+    const long long nseg = (long long)ntx * (ny - 2);
+    T *in = g0, *out = g1;
+    for (int it = 0; it < niter; ++it) {
+        for (long long s = warp; s < nseg; s += nwarps) {
+            const int y = 1 + (int)(s / ntx);
+            const int x = (int)(s % ntx) * 32 + lane;
+            const bool ld = x < nx;
+            const size_t idx = (size_t)y * nx + x;
+            const T cur = ld ? in[idx] : T(0);
+            T e = __shfl_down_sync(FULL, cur, 1);
+            T w = __shfl_up_sync(FULL, cur, 1);
+            if (lane == 31 && x + 1 < nx) e = in[idx + 1];
+            if (lane == 0 && x >= 1 && ld) w = in[idx - 1];
+            if (x == nx - 1) e = cur;
+            if (x == 0) w = cur;
+            if (ld) {
+                const T n = in[idx + nx];
+                const T so = in[idx - nx];
+                const T v = quarter<T>(add_rn(add_rn(add_rn(n, so), e), w));
+                out[idx] = v;
+                if (IMAGES) {
+                    if (y == 1) out[idx + (size_t)(ny - 2) * nx] = v;
+                    if (y == ny - 2) out[idx - (size_t)(ny - 2) * nx] = v;
+                }
+            }
+        }
+        if (it + 1 < niter) {
+            if (!grid_barrier(bar, gridDim.x, it)) return;
+        }
+        T *t = in;
+        in = out;
+        out = t;
+    }
+}
+
 // 2D sweep for rows whose byte length is a multiple of 16 (nx a multiple of
 // V = 16 / sizeof(T)).  Work unit = (row chunk, column tile of 32 V columns),
 // one warp per unit, units chunk-major and dealt to warps round-robin (the
@@ -334,7 +383,7 @@ __device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) 
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-template <typename T>
+template <typename T, bool MIRROR>
 __global__ void __launch_bounds__(1024, 1)
     j2d_resident_kernel(const T *in, T *final_out, int nx, int ny, int niter, T *xbuf,
                         unsigned int *flags, BarrierState *bar) {
@@ -355,20 +404,27 @@ __global__ void __launch_bounds__(1024, 1)
     }
     __syncthreads();
     __shared__ int s_ok;
-    const int inner = nx - 2;
+    // updated columns: 1 .. nx-2, or with the mirror boundary 0 .. nx-1
+    const int x0 = MIRROR ? 0 : 1;
+    const int inner = MIRROR ? nx : nx - 2;
     // rows [ra, rb) of the band as a flat run of cells, row r / column x of
     // the first cell of each thread stepped without a division per cell
     const int dr = nth / inner, dx = nth % inner;
     auto sweep_rows = [&](int ra, int rb, T *pub) {
-        int r = ra + tid / inner, x = 1 + tid % inner;
+        int r = ra + tid / inner, x = x0 + tid % inner;
         for (; r < rb; r += dr, x += dx) {
-            if (x > inner) {
+            if (x >= x0 + inner) {
                 x -= inner;
                 ++r;
                 if (r >= rb) break;
             }
             const T *c = cur + (size_t)r * nx + x;
-            const T v = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
+            T v;
+            if (MIRROR)  // Stencil/jacobi2D/src/common.cu:57-63
+                v = quarter<T>(add_rn(add_rn(add_rn(c[nx], c[-nx]), c[x < nx - 1 ? 1 : 0]),
+                                      c[x > 0 ? -1 : 0]));
+            else
+                v = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
             nxt[(size_t)r * nx + x] = v;
             if (pub) {  // the rows the neighbours read: first to slot 0, last to slot 1
                 if (r == 1) __stcg(pub + x, v);
@@ -383,7 +439,7 @@ __global__ void __launch_bounds__(1024, 1)
         sweep_rows(1, 2, xb);
         if (h > 1) sweep_rows(h, h + 1, xb);
         // the slot columns 0 and nx-1 carry the band's boundary cells
-        if (tid == 0) {
+        if (!MIRROR && tid == 0) {  // (mirror: sweep_rows published them)
             __stcg(xb, nxt[nx]);
             __stcg(xb + nx - 1, nxt[2 * (size_t)nx - 1]);
             __stcg(xb + nx, nxt[(size_t)h * nx]);
@@ -547,6 +603,8 @@ struct cfm_jacobi {
     bool tma = false;
     cfm::TmaConfig tc, tail;
     size_t smem_optin = 0;
+    // 2D: the mirror x boundary of the reference's PERKS comparator
+    bool mirror = false;
 };
 
 namespace {
@@ -747,7 +805,10 @@ size_t grid_elems(const cfm_jacobi_params *p) {
 }
 
 template <typename T>
-const void *sweep_fn(const cfm_jacobi_params &p, bool images) {
+const void *sweep_fn(const cfm_jacobi_params &p, bool images, bool mirror) {
+    if (p.dims == 2 && mirror)
+        return images ? (const void *)j2d_mirror_kernel<T, true>
+                      : (const void *)j2d_mirror_kernel<T, false>;
     if (p.dims == 2 && p.nx % (16 / (int)sizeof(T)) == 0)
         return images ? (const void *)j2d_march_kernel<T, true>
                       : (const void *)j2d_march_kernel<T, false>;
@@ -761,8 +822,17 @@ const void *sweep_fn(const cfm_jacobi_params &p, bool images) {
                   : (const void *)j3d_sweeps_kernel<T, J3_TY, false, false>;
 }
 
-const void *sweep_fn_any(const cfm_jacobi_params &p, bool images) {
-    return p.precision == CFM_FP64 ? sweep_fn<double>(p, images) : sweep_fn<float>(p, images);
+const void *sweep_fn_any(const cfm_jacobi_params &p, bool images, bool mirror) {
+    return p.precision == CFM_FP64 ? sweep_fn<double>(p, images, mirror)
+                                   : sweep_fn<float>(p, images, mirror);
+}
+
+const void *resident_fn(const cfm_jacobi_params &p, bool mirror) {
+    if (p.precision == CFM_FP64)
+        return mirror ? (const void *)j2d_resident_kernel<double, true>
+                      : (const void *)j2d_resident_kernel<double, false>;
+    return mirror ? (const void *)j2d_resident_kernel<float, true>
+                  : (const void *)j2d_resident_kernel<float, false>;
 }
 
 dim3 block_of(const cfm_jacobi_params &p) { return p.dims == 2 ? dim3(256) : dim3(32, J3_TY); }
@@ -812,7 +882,7 @@ int choose_launch(cfm_jacobi *h) {
     h->num_sms = di.num_sms;
     h->smem_optin = di.smem_optin;
     const cfm_jacobi_params &p = h->p;
-    const void *fn = sweep_fn_any(p, true);
+    const void *fn = sweep_fn_any(p, true, h->mirror);
     dim3 b = block_of(p);
     const int threads = (int)(b.x * b.y);
     int per_sm = 0;
@@ -832,7 +902,7 @@ int choose_launch(cfm_jacobi *h) {
         // row-marching kernel tiles of 16-byte lanes over row chunks of at
         // least 8 rows
         const int vec = 16 / (int)h->esize;
-        const bool march = p.nx % vec == 0;
+        const bool march = p.nx % vec == 0 && !h->mirror;
         const long long units = march ? (long long)((p.nx + 32 * vec - 1) / (32 * vec)) * ((p.ny - 2 + 7) / 8)
                                       : (long long)((p.nx + 31) / 32) * (p.ny - 2);
         const long long need = (units * 32 + threads - 1) / threads;
@@ -844,8 +914,7 @@ int choose_launch(cfm_jacobi *h) {
         const int B = std::min(di.num_sms, p.ny - 2);
         const int hmax = (p.ny - 2 + B - 1) / B;
         const size_t smem = 2 * (size_t)(hmax + 2) * p.nx * h->esize;
-        const void *rfn = p.precision == CFM_FP64 ? (const void *)j2d_resident_kernel<double>
-                                                  : (const void *)j2d_resident_kernel<float>;
+        const void *rfn = resident_fn(p, h->mirror);
         if (smem <= di.smem_optin) {
             CFM_CUDA_TRY(cudaFuncSetAttribute(rfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem));
@@ -878,7 +947,7 @@ int launch_edge_preset(cfm_jacobi *h) {
 // copies with cudaMemcpyAsync (Stencil/jacobi3D/src/common.cu:174-215).
 int host_loop_copy(cfm_jacobi *h, int niter, int *launches) {
     const cfm_jacobi_params &p = h->p;
-    const void *fn = sweep_fn_any(p, false);
+    const void *fn = sweep_fn_any(p, false, h->mirror);
     const size_t es = h->esize;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     int one = 1;
@@ -920,7 +989,7 @@ int host_loop_copy(cfm_jacobi *h, int niter, int *launches) {
 
 int host_loop_images(cfm_jacobi *h, int niter, int *launches) {
     const cfm_jacobi_params &p = h->p;
-    const void *fn = sweep_fn_any(p, true);
+    const void *fn = sweep_fn_any(p, true, h->mirror);
     int one = 1;
     const dim3 block = block_of(p);
     for (int it = 0; it < niter; ++it) {
@@ -944,8 +1013,7 @@ int resident2d(cfm_jacobi *h, int niter, int *launches) {
     int n = niter;
     void *args[] = {(void *)&in, &fin, (void *)&p.nx, (void *)&p.ny, &n, &h->xbuf, &h->flags,
                     &h->bar};
-    const void *fn = p.precision == CFM_FP64 ? (const void *)j2d_resident_kernel<double>
-                                             : (const void *)j2d_resident_kernel<float>;
+    const void *fn = resident_fn(p, h->mirror);
     CFM_CUDA_TRY(launch_cooperative(fn, dim3(h->res_blocks), dim3(1024), args, h->res_smem,
                                     h->stream));
     h->cur ^= (niter & 1);
@@ -987,7 +1055,7 @@ int persistent(cfm_jacobi *h, int niter, int *launches) {
     const cfm_jacobi_params &p = h->p;
     if (h->resident) return resident2d(h, niter, launches);
     if (h->tma) return persistent_tma(h, niter, launches);
-    const void *fn = sweep_fn_any(p, true);
+    const void *fn = sweep_fn_any(p, true, h->mirror);
     void *in = h->buf[h->cur], *out = h->buf[h->cur ^ 1];
     int n = niter;
     void *args3[] = {&in, &out, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &n, &h->zchunk,
@@ -1011,7 +1079,8 @@ int reset_barrier(cfm_jacobi *h) {
 int enqueue_sweeps(cfm_jacobi *h, int niter, int *launches) {
     if (niter == 0) return CFM_OK;
     int st;
-    if (h->p.impl != CFM_JACOBI_HOST_LOOP) {
+    // (the mirror sweep reads the edge cells and writes whole rows: no preset)
+    if (h->p.impl != CFM_JACOBI_HOST_LOOP && !h->mirror) {
         st = h->p.precision == CFM_FP64 ? launch_edge_preset<double>(h)
                                         : launch_edge_preset<float>(h);
         if (st) return st;
@@ -1166,6 +1235,20 @@ int cfm_jacobi_set_stream(cfm_jacobi *h, void *cuda_stream) {
     h->own_stream = false;
     h->stream = (cudaStream_t)cuda_stream;
     return CFM_OK;
+}
+
+int cfm_jacobi_set_boundary(cfm_jacobi *h, int boundary) {
+    CFM_ARG_CHECK(h, "handle is null");
+    CFM_ARG_CHECK(boundary == CFM_BOUNDARY_DIRICHLET || boundary == CFM_BOUNDARY_MIRROR,
+                  "boundary must be CFM_BOUNDARY_DIRICHLET or CFM_BOUNDARY_MIRROR");
+    CFM_ARG_CHECK(boundary == CFM_BOUNDARY_DIRICHLET || h->p.dims == 2,
+                  "the mirror boundary is a 2D sweep");
+    const bool m = boundary == CFM_BOUNDARY_MIRROR;
+    if (m == h->mirror) return CFM_OK;
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->mirror = m;
+    // the sweep kernel changes: its occupancy and work units set the grid
+    return choose_launch(h);
 }
 
 int cfm_jacobi_load_problem(cfm_jacobi *h, int problem) {

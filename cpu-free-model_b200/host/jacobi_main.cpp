@@ -9,6 +9,12 @@
 //   -precision fp32|fp64   grid type (reference: fp32, `typedef float real`)
 //   -problem ref|config    initial state, see cfm.h (3D config is y-periodic)
 //   -out FILE              write the final grid (raw, row-major) to FILE
+//   -boundary dirichlet|mirror
+//                          2D x boundary, see cfm_boundary in cfm.h.  Default:
+//                          mirror for PERKS, whose reference run is checked
+//                          against the mirror sweep (Stencil/jacobi2D/src/
+//                          PERKS/multi-stream-perks.cu:225-226), dirichlet for
+//                          every other version and for 3D
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -63,6 +69,14 @@ int main(int argc, char **argv) {
     const std::string prec = cli::argval<std::string>(argc, argv, "-precision", "fp32");
     const std::string prob = cli::argval<std::string>(argc, argv, "-problem", "ref");
     const std::string out = cli::argval<std::string>(argc, argv, "-out", "");
+    const std::string bnd = cli::argval<std::string>(
+        argc, argv, "-boundary",
+        (CFM_DIMS == 2 && v.impl == CFM_JACOBI_RESIDENT) ? "mirror" : "dirichlet");
+    if (bnd != "dirichlet" && (bnd != "mirror" || CFM_DIMS != 2)) {
+        std::fprintf(stderr, "ERROR: -boundary must be dirichlet%s\n", CFM_DIMS == 2 ? " or mirror" : "");
+        return 1;
+    }
+    const int boundary = bnd == "mirror" ? CFM_BOUNDARY_MIRROR : CFM_BOUNDARY_DIRICHLET;
     if (prec != "fp32" && prec != "fp64") {
         std::fprintf(stderr, "ERROR: -precision must be fp32 or fp64\n");
         return 1;
@@ -79,6 +93,7 @@ int main(int argc, char **argv) {
     cfm_jacobi *h = nullptr;
     int st = cfm_jacobi_create(&p, &h);
     if (st) return cli::fail("cfm_jacobi_create", st);
+    if ((st = cfm_jacobi_set_boundary(h, boundary))) return cli::fail("boundary", st);
     if ((st = cfm_jacobi_load_problem(h, problem))) return cli::fail("load problem", st);
     cfm_stats s{};
     st = cfm_jacobi_run(h, niter, &s);
@@ -99,6 +114,7 @@ int main(int argc, char **argv) {
         pr.impl = CFM_JACOBI_HOST_LOOP;
         cfm_jacobi *hr = nullptr;
         if ((st = cfm_jacobi_create(&pr, &hr))) return cli::fail("compare create", st);
+        if ((st = cfm_jacobi_set_boundary(hr, boundary))) return cli::fail("compare boundary", st);
         if ((st = cfm_jacobi_load_problem(hr, problem))) return cli::fail("compare load", st);
         if ((st = cfm_jacobi_run(hr, niter, &sref))) return cli::fail("compare run", st);
         std::vector<unsigned char> ref(n * es);

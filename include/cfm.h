@@ -125,6 +125,24 @@ int cfm_jacobi_problem_host(const cfm_jacobi_params *p, int problem, void *host_
 int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out);
 void cfm_jacobi_destroy(cfm_jacobi *h);
 int cfm_jacobi_set_stream(cfm_jacobi *h, void *cuda_stream);
+/* x boundary of the 2D sweep. */
+typedef enum cfm_boundary {
+    /* x = 0 and x = nx-1 are fixed columns, rows 1..ny-2 x 1..nx-2 updated as
+     * 0.25 * (((E + W) + N) + S) (jacobi_kernel_single_gpu,
+     * Stencil/jacobi2D/src/common.cu:28-42).  The default. */
+    CFM_BOUNDARY_DIRICHLET = 0,
+    /* every column of rows 1..ny-2 updated, east / west clamped to the cell
+     * itself at the x edges, 0.25 * (((N + S) + E) + W): the reference's PERKS
+     * comparator jacobi_kernel_single_gpu_mirror (Stencil/jacobi2D/src/
+     * common.cu:44-66), which its PERKS run is checked against
+     * (Stencil/jacobi2D/src/PERKS/multi-stream-perks.cu:225-226).  Same
+     * periodic halo rows.  Every implementation supports it. */
+    CFM_BOUNDARY_MIRROR = 1
+} cfm_boundary;
+/* Select the 2D x boundary for later runs (3D: only CFM_BOUNDARY_DIRICHLET).
+ * Replaces the kernel argument of the reference's single_gpu()
+ * (Stencil/jacobi2D/src/common.cu:154-156). */
+int cfm_jacobi_set_boundary(cfm_jacobi *h, int boundary);
 /* Device-side equivalent of cfm_jacobi_problem_host into the handle's grid. */
 int cfm_jacobi_load_problem(cfm_jacobi *h, int problem);
 /* Copy a caller-owned host grid in / the current grid out (blocking). */

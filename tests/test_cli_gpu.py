@@ -38,8 +38,43 @@ def test_jacobi2d_versions_compare_and_match_oracle(version, prec, tmp_path):
     assert out.lstrip().startswith("Execution time:") and first_float(out) >= 0
     dt = np.float32 if prec == "fp32" else np.float64
     got = np.fromfile(path, dt).reshape(ny, nx)
-    want = oracle.jacobi2d(oracle.jacobi2d_init(nx, ny, dt), niter)
+    a = oracle.jacobi2d_init(nx, ny, dt)
+    # PERKS (-v 5) runs the mirror x boundary, as the reference's PERKS version
+    # is checked against jacobi_kernel_single_gpu_mirror
+    want = oracle.jacobi2d_mirror(a, niter) if version == 5 else oracle.jacobi2d(a, niter)
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("version,boundary", [(3, "mirror"), (5, "dirichlet"), (0, "mirror")])
+def test_jacobi2d_boundary_flag(version, boundary, tmp_path):
+    nx, ny, niter = 64, 30, 11
+    path = tmp_path / "grid.bin"
+    rc, out, err = run("jacobi2D", "-v", version, "-s", "-nx", nx, "-ny", ny, "-niter", niter,
+                       "-boundary", boundary, "-compare", "-out", path)
+    assert rc == 0 and "ERROR" not in err, err
+    got = np.fromfile(path, np.float32).reshape(ny, nx)
+    a = oracle.jacobi2d_init(nx, ny, np.float32)
+    want = oracle.jacobi2d_mirror(a, niter) if boundary == "mirror" else oracle.jacobi2d(a, niter)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("version", [3, 5])
+def test_jacobi2d_config1_full_length_and_norm(version, tmp_path):
+    """Config 1 at its stated size and length: 1024^2 FP64, 1000 sweeps
+    (Dirichlet columns), Design 1 and PERKS; the -out grid equals the oracle
+    bit for bit and the printed final L2 norm is the oracle grid's."""
+    nx = ny = 1024
+    niter = 1000
+    path = tmp_path / "grid.bin"
+    rc, out, err = run("jacobi2D", "-v", version, "-s", "-nx", nx, "-ny", ny, "-niter", niter,
+                       "-precision", "fp64", "-boundary", "dirichlet", "-out", path)
+    assert rc == 0 and "ERROR" not in err, err
+    got = np.fromfile(path, np.float64).reshape(ny, nx)
+    want = oracle.jacobi2d(oracle.jacobi2d_init(nx, ny, np.float64), niter)
+    np.testing.assert_array_equal(got, want)
+    norm = float(re.search(r"Final grid L2 norm: (\S+)", out).group(1))
+    want_norm = float(np.sqrt(np.sum(want.astype(np.longdouble) ** 2)))
+    assert abs(norm - want_norm) <= 1e-14 * want_norm
 
 
 @pytest.mark.parametrize("version", range(6))

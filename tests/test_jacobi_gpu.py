@@ -20,7 +20,7 @@ def rand_grid(shape, dtype, seed):
     return np.random.default_rng(seed).uniform(-1, 1, shape).astype(dtype)
 
 
-def run_gpu(a, niter, impl, periodic_y=0):
+def run_gpu(a, niter, impl, periodic_y=0, mirror=False):
     prec = cfm.FP64 if a.dtype == np.float64 else cfm.FP32
     if a.ndim == 2:
         ny, nx = a.shape
@@ -29,6 +29,8 @@ def run_gpu(a, niter, impl, periodic_y=0):
         nz, ny, nx = a.shape
         j = cfm.Jacobi(3, nx, ny, nz, prec, periodic_y, impl)
     with j:
+        if mirror:
+            j.set_boundary(cfm.BOUNDARY_MIRROR)
         j.upload(a)
         st = j.run(niter)
         assert st.iterations == niter
@@ -46,6 +48,36 @@ def test_jacobi2d_random_bitexact(impl, prec, shape, niter):
     a = rand_grid(shape, cfm.np_dtype(prec), 11)
     got, _ = run_gpu(a, niter, impl)
     np.testing.assert_array_equal(got, oracle.jacobi2d(a, niter))
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("shape", [(3, 3), (9, 7), (17, 33), (70, 130), (1026, 100), (5, 64),
+                                   (260, 256), (40, 2050)])
+@pytest.mark.parametrize("niter", [0, 1, 2, 7])
+def test_jacobi2d_mirror_random_bitexact(impl, prec, shape, niter):
+    """The mirror x boundary (the reference's PERKS comparator,
+    Stencil/jacobi2D/src/common.cu:44-66) on every implementation, edge
+    columns and corner cells included."""
+    a = rand_grid(shape, cfm.np_dtype(prec), 21)
+    got, _ = run_gpu(a, niter, impl, mirror=True)
+    np.testing.assert_array_equal(got, oracle.jacobi2d_mirror(a, niter))
+
+
+def test_mirror_boundary_is_2d_only_and_switchable():
+    a = rand_grid((34, 64), np.float64, 5)
+    with cfm.Jacobi(2, 64, 34, 1, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
+        j.set_boundary(cfm.BOUNDARY_MIRROR)
+        j.upload(a)
+        j.run(3)
+        np.testing.assert_array_equal(j.download(), oracle.jacobi2d_mirror(a, 3))
+        j.set_boundary(cfm.BOUNDARY_DIRICHLET)
+        j.upload(a)
+        j.run(3)
+        np.testing.assert_array_equal(j.download(), oracle.jacobi2d(a, 3))
+    with cfm.Jacobi(3, 8, 8, 8, cfm.FP64, 0, cfm.JACOBI_PERSISTENT) as j:
+        with pytest.raises(cfm.CfmError):
+            j.set_boundary(cfm.BOUNDARY_MIRROR)
 
 
 @pytest.mark.parametrize("impl", IMPLS)
@@ -73,15 +105,46 @@ def test_device_problem_matches_host_problem(prec, dims, problem):
 
 
 def test_jacobi2d_config1_problem_1024():
-    """1024^2 FP64 problem, 50 sweeps, persistent and resident against the oracle."""
+    """Config 1 at its stated length: 1024^2 FP64, 1000 sweeps, persistent and
+    resident against the oracle bit for bit."""
     a = oracle.jacobi2d_init(1024, 1024, np.float64)
-    want = oracle.jacobi2d(a, 50)
+    want = oracle.jacobi2d(a, 1000)
     with cfm.Jacobi(2, 1024, 1024, 1, cfm.FP64, 1, cfm.JACOBI_RESIDENT) as j:
         assert j.launch_shape()[1] == 1024  # the on-chip resident kernel
     for impl in (cfm.JACOBI_PERSISTENT, cfm.JACOBI_RESIDENT):
-        got, st = run_gpu(a, 50, impl)
+        got, st = run_gpu(a, 1000, impl)
         np.testing.assert_array_equal(got, want)
         assert st.launches <= 2
+
+
+@pytest.fixture(scope="module")
+def config2_fp64():
+    """The 512^3 periodic config problem and the oracle's grid after config
+    2's 100 sweeps (about 1.07 GB each)."""
+    with cfm.Jacobi(3, 512, 512, 512, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) as j:
+        a = j.problem_host(cfm.PROBLEM_CONFIG)
+    return a, oracle.jacobi3d(a, 100, 1)
+
+
+def test_jacobi3d_config2_fp64_100_sweeps_bitexact(config2_fp64):
+    """Config 2 at its stated size and length: 512^3 FP64, 100 sweeps, the
+    persistent TMA pipeline equals the oracle bit for bit."""
+    a, want = config2_fp64
+    got, st = run_gpu(a, 100, cfm.JACOBI_PERSISTENT, 1)
+    assert st.launches == 2
+    np.testing.assert_array_equal(got, want)
+
+
+def test_jacobi3d_config2_fp32_100_sweeps(config2_fp64):
+    """Config 2's FP32 variant: 512^3, 100 sweeps, bit for bit against the FP32
+    oracle, and within 1.5e-6 (max-abs and relative L2) of the FP64 grid."""
+    a64, want64 = config2_fp64
+    a32 = a64.astype(np.float32)
+    got, _ = run_gpu(a32, 100, cfm.JACOBI_PERSISTENT, 1)
+    np.testing.assert_array_equal(got, oracle.jacobi3d(a32, 100, 1))
+    err = got.astype(np.float64) - want64
+    assert np.abs(err).max() <= 1.5e-6
+    assert np.linalg.norm(err) / np.linalg.norm(want64) <= 1.5e-6
 
 
 def test_jacobi3d_512_fp64_bitexact_and_e2e():
@@ -186,10 +249,16 @@ def test_gpu_matches_reference_fixture(path, impl):
     """Our kernels reproduce grids written by the reference's own single_gpu()."""
     f = np.load(path)
     kind = str(f["kind"])
-    if kind == "2d_mirror":
-        pytest.skip("mirror-boundary (PERKS comparator) sweep is an oracle-only variant")
     out = f["out"]
     niter = int(f["niter"])
+    if kind == "2d_mirror":
+        # the mirror sweep updates the x edge columns, so it starts from the
+        # initial state (the oracle's, pinned to these fixtures on the CPU)
+        ny, nx = out.shape
+        a = oracle.jacobi2d_init(nx, ny, np.float32)
+        got, _ = run_gpu(a, niter, impl, mirror=True)
+        np.testing.assert_array_equal(got, out)
+        return
     if kind == "2d":
         ny, nx = out.shape
         # the reference computed its boundary columns with device sin; a sweep
