@@ -707,7 +707,12 @@ namespace {
 
 // Device address of g_cg_noalloc_scratch on the current device.  In host
 // code the symbol names a host-side stand-in, so the address is looked up
-// once per device with that device current and cached.
+// once per device with that device current and cached.  With lazy module
+// loading (the CUDA default) that first lookup is also what loads this
+// file's kernels and the array onto the device, so it can allocate device
+// memory: an allocation failure there is CFM_OUT_OF_MEMORY.  The cache
+// assumes the device's primary context lives as long as the process; after
+// a cudaDeviceReset the array may sit at another address.
 int noalloc_scratch(double **out) {
     static std::mutex mu;
     static double *addr[64] = {};
@@ -724,7 +729,7 @@ int noalloc_scratch(double **out) {
         if (e != cudaSuccess || !p) {
             set_error("cudaGetSymbolAddress(g_cg_noalloc_scratch) failed: %s",
                       cudaGetErrorString(e));
-            return CFM_CUDA_ERROR;
+            return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
         }
         addr[dev] = static_cast<double *>(p);
     }
@@ -750,6 +755,9 @@ extern "C" int cfm_cg_solve_noalloc(int n, long long nnz, const int *rowptr_dev,
     CFM_ARG_CHECK(nnz >= 0 && nnz < 2147483647LL, "nnz");
     CFM_ARG_CHECK(rowptr_dev && x_dev && (nnz == 0 || (col_dev && val_dev)), "null argument");
     CFM_ARG_CHECK(maxiter >= 0, "maxiter");
+    // The kernel zeroes x first and reads b again for the true residual.
+    CFM_ARG_CHECK(b_dev == nullptr || (const void *)b_dev != (const void *)x_dev,
+                  "b and x must not be the same array");
     double *scr = nullptr;
     int e = noalloc_scratch(&scr);
     if (e) return e;

@@ -263,10 +263,18 @@ int cfm_cg_solve_device(cfm_cg *h, const double *b_dev, double *x_dev, cfm_stats
  *  - Inputs and outputs are the caller's device memory: a 0-based CSR
  *    matrix (rowptr n+1, col nnz, val nnz) with n <= CFM_CG_NOALLOC_MAX_N
  *    (larger n: CFM_BAD_ARG), b (NULL = ones) and x (length n, written).
+ *    b and x must be different arrays (CFM_BAD_ARG otherwise).
  *  - Work goes on `cuda_stream` (NULL = the legacy default stream); the
- *    call returns when the solve is done.  stats->seconds is host time.
- *  - The first call on a device looks up the array's device address (with
- *    that device current); make that first call before any stream capture.
+ *    call waits for that stream and reads the result back before it
+ *    returns.  stats->seconds is host time.
+ *  - Set-up: the first call on a device looks up the array's device address
+ *    with that device current; make that first call before any stream
+ *    capture.  With lazy module loading (the CUDA default) this first call is
+ *    also what loads the array onto the device, so it may allocate device
+ *    memory itself: make it (a 1-row system is enough) before the caller
+ *    reserves or hands out its memory.  Out of memory there is
+ *    CFM_OUT_OF_MEMORY.  The address is kept for the process: calls after a
+ *    cudaDeviceReset of that device are not supported.
  *  - All calls share the one array and the call resets what must start at
  *    zero, so calls whose kernels overlap on the GPU (other threads, other
  *    streams) race; serialise them.

@@ -41,6 +41,14 @@ def test_noalloc_rejects_sizes_beyond_the_fixed_array():
     assert s == cfm.BAD_ARG
 
 
+def test_noalloc_rejects_b_aliasing_x():
+    # the solve zeroes x before it reads b again, so b == x is refused up
+    # front (before any CUDA call: no GPU needed)
+    s, _ = _call(1000, 7000, 16, 16, 16, 32, 32, 10, 1e-8)
+    assert s == cfm.BAD_ARG
+    assert b"b and x" in cfm.lib.cfm_last_error()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("g", [24, 64])
 def test_noalloc_matches_allocating_cg_two_calls(g):
