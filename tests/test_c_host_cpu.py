@@ -1,5 +1,5 @@
 """A foreign C host: a C99 program that includes include/cfm.h and links
-libcfm.so the way INTEGRATION.md shows compiles, runs, and gets status codes
+libcfm.so (-I include -L lib -lcfm, as a foreign build would) compiles, runs, and gets status codes
 back (never an exit) for bad arguments.  No GPU needed: device-side calls on a
 machine without a GPU must return a status too."""
 import os
