@@ -546,7 +546,8 @@ class UNet:
         return dict(zip(("loss_first", "loss_last", "data_s", "train_s"), (x.value for x in v)))
 
     def set_validation(self, seed, every):
-        """Keep the checkpoint whose FPCG solve of a held-out system is fastest."""
+        """Keep the checkpoint whose FPCG solve of a held-out system takes the
+        fewest iterations (ties: the earlier epoch)."""
         check("cfm_unet_set_validation", lib.cfm_unet_set_validation(self.h, seed, every))
 
     def validation(self):

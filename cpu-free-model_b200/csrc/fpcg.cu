@@ -70,11 +70,43 @@ StencilOp<2> op2(const cfm_stencil *S) {
     return o;
 }
 
+// Cross-block sums of K doubles that come out the same on every run.  The
+// participating block `idx` of `n` stores its K values (v, read on thread 0)
+// at slots[idx * K + j]; the last participant to arrive (counted on *count)
+// adds the slots in participant order -- lane l of its first warp takes
+// participants l, l + 32, ..., then a fixed xor butterfly -- writes out[j]
+// (adds to it when `add`) and re-arms *count for the next launch.  Every
+// thread of a participating block calls it.
+template <int K>
+__device__ void ordered_grid_sum(const double *v, double *slots, int idx, int n, unsigned int *count,
+                                 double *out, bool add) {
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < K; ++j) slots[(size_t)idx * K + j] = v[j];
+        __threadfence();
+        s_last = atomicAdd(count, 1u) == (unsigned int)(n - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x < 32) {
+        __threadfence();
+        double t[K];
+        for (int j = 0; j < K; ++j) t[j] = 0.0;
+        for (int i = threadIdx.x; i < n; i += 32)
+            for (int j = 0; j < K; ++j) t[j] += __ldcg(slots + (size_t)i * K + j);
+        for (int o = 16; o; o >>= 1)
+            for (int j = 0; j < K; ++j) t[j] += __shfl_xor_sync(CG_FULL, t[j], o);
+        if (threadIdx.x == 0) {
+            for (int j = 0; j < K; ++j) out[j] = add ? out[j] + t[j] : t[j];
+            *count = 0;
+        }
+    }
+}
+
 // ------------------------------------------------------- training data
-// r = b - A xj, e = xs - xj; accumulates |r|^2, |e|^2 into acc[0], acc[1].
-// r = b - A xj, e = xs - xj; accumulates |r|^2, <e, r> into acc[0], acc[1].
+// r = b - A xj, e = xs - xj; |r|^2, <e, r> into acc[0], acc[1] (grid sums in
+// block order: slots of 2 x gridDim.x doubles, one counter).
 __global__ void k_pair(StencilOp<2> op, int n, const double *b, const double *xs, const double *xj,
-                       double *r, double *e, double *acc) {
+                       double *r, double *e, double *acc, double *slots, unsigned int *count) {
     __shared__ double red[2][32];
     double rr = 0, er = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -94,15 +126,13 @@ __global__ void k_pair(StencilOp<2> op, int n, const double *b, const double *xs
         red[1][threadIdx.x >> 5] = er;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, c = 0;
+    double v[2] = {0.0, 0.0};
+    if (threadIdx.x == 0)
         for (int w = 0; w < (int)blockDim.x / 32; ++w) {
-            a += red[0][w];
-            c += red[1][w];
+            v[0] += red[0][w];
+            v[1] += red[1][w];
         }
-        atomicAdd(acc, a);
-        atomicAdd(acc + 1, c);
-    }
+    ordered_grid_sum<2>(v, slots, blockIdx.x, gridDim.x, count, acc, false);
 }
 
 // Damped Jacobi sweep for the training pairs: zout = zin + omega (r - A zin) / diag.
@@ -115,9 +145,9 @@ __global__ void k_data_jacobi(StencilOp<2> op, int n, const double *r, const dou
 }
 
 // After pre-smoothing z: r <- r - A z, e <- e - z (the pair the network sees
-// inside the preconditioner); |r|^2, <e, r> into acc (fresh).
+// inside the preconditioner); |r|^2, <e, r> into acc (as k_pair).
 __global__ void k_data_smoothed(StencilOp<2> op, int n, const double *z, double *r, double *e,
-                                double *r1, double *acc) {
+                                double *r1, double *acc, double *slots, unsigned int *count) {
     __shared__ double red[2][32];
     double rr = 0, er = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -137,15 +167,13 @@ __global__ void k_data_smoothed(StencilOp<2> op, int n, const double *z, double 
         red[1][threadIdx.x >> 5] = er;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, c = 0;
+    double v[2] = {0.0, 0.0};
+    if (threadIdx.x == 0)
         for (int w = 0; w < (int)blockDim.x / 32; ++w) {
-            a += red[0][w];
-            c += red[1][w];
+            v[0] += red[0][w];
+            v[1] += red[1][w];
         }
-        atomicAdd(acc, a);
-        atomicAdd(acc + 1, c);
-    }
+    ordered_grid_sum<2>(v, slots, blockIdx.x, gridDim.x, count, acc, false);
 }
 
 // One training sample at residual scale sr = 1 / rms(r) (r on the nx x ny
@@ -176,14 +204,16 @@ __global__ void k_pair_store(int nx, int ny, int f, const double *r, const float
 // z[i] = y[cell(i)].  Per batch element b (sample ids[b] of system
 // ids[b] / per, whose FP32 stencil coefficients we | wn | dg sit at
 // coef + sys * 3 n and whose fine residual r is r1 + ids[b] n):
-//   Az = A z (FP32 apply), s[0] = <z, r>, s[1] = <z, A z>  (FP64 atomics).
+//   Az = A z (FP32 apply), s[0] = <z, r>, s[1] = <z, A z> (FP64, the blocks
+//   of batch element b summed in block order: slots 2 x gridDim.x from
+//   slots + 2 b gridDim.x, counter count[b]).
 __device__ __forceinline__ int coarse_cell(int ix, int iy, int f, int ncx) {
     return (iy / f) * ncx + ix / f;
 }
 
 __global__ void k_loss_anorm_dots(const float *y, const float *r1, const float *coef,
                                   const long long *ids, int per, int nx, int ny, int f, float *Az,
-                                  double *s) {
+                                  double *s, double *slots, unsigned int *count) {
     const int b = blockIdx.y, n = nx * ny, ncx = nx / f, nc = n / (f * f);
     const float *c = coef + (size_t)(ids[b] / per) * 3 * n;
     const float *we = c, *wn = c + n, *dg = c + 2 * n;
@@ -213,23 +243,23 @@ __global__ void k_loss_anorm_dots(const float *y, const float *r1, const float *
         red[1][threadIdx.x >> 5] = zaz;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, q = 0;
+    double v[2] = {0.0, 0.0};
+    if (threadIdx.x == 0)
         for (int w = 0; w < (int)blockDim.x / 32; ++w) {
-            a += red[0][w];
-            q += red[1][w];
+            v[0] += red[0][w];
+            v[1] += red[1][w];
         }
-        atomicAdd(s + 2 * b, a);
-        atomicAdd(s + 2 * b + 1, q);
-    }
+    ordered_grid_sum<2>(v, slots + (size_t)2 * b * gridDim.x, blockIdx.x, gridDim.x, count + b, s + 2 * b,
+                        false);
 }
 
 // L_b = 1 - a^2 / (q c), a = <z, r>, q = <z, A z>, c = <e, r>;
 // dL_b/dz = (2 a / (q c)) ((a / q) A z - r) and dL_b/dy = P^T dL_b/dz (the
-// sum over each f x f block); the batch mean and its gradient.
+// sum over each f x f block); the batch mean (added to *loss, the batch
+// elements in order: slots of gridDim.y doubles, one counter) and its gradient.
 __global__ void k_loss_anorm_grad(const float *Az, const float *r1, const double *s,
                                   const double *er, const long long *ids, int nx, int ny, int f, int B,
-                                  float *dout, double *loss) {
+                                  float *dout, double *loss, double *slots, unsigned int *count) {
     const int b = blockIdx.y, n = nx * ny, ncx = nx / f, nc = n / (f * f);
     const double a = s[2 * b], q = s[2 * b + 1], c = er[ids[b]];
     const bool ok = q > 0 && c > 0;
@@ -246,7 +276,10 @@ __global__ void k_loss_anorm_grad(const float *Az, const float *r1, const double
             }
         dout[(size_t)b * nc + ic] = (float)g;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && ok) atomicAdd(loss, (1.0 - a * a / (q * c)) / B);
+    if (blockIdx.x == 0) {
+        const double v = ok ? (1.0 - a * a / (q * c)) / B : 0.0;
+        ordered_grid_sum<1>(&v, slots, b, gridDim.y, count, loss, true);
+    }
 }
 
 // ------------------------------------------------------------------ FPCG
@@ -258,6 +291,7 @@ enum : int {
 // against the last m; directions p_j and s_j = A p_j live in a ring of m + 1
 // slots (slot j mod (m + 1)).
 constexpr int FP_MAX_TRUNC = 8;
+constexpr int FP_RES_BLOCKS = 256;  // grid of the true-residual pass
 constexpr int FP_NSLOT = FP_ZS + FP_MAX_TRUNC;
 
 struct FpState {
@@ -692,9 +726,11 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
 }
 
-// t = b - A x, |t|^2 (atomics; the reported true residual).
+// t = b - A x, |t|^2 into acc[0] (the judged true residual; grid sum in
+// block order: slots of gridDim.x doubles, one counter).
 __global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const double *x, double *t,
-                              double *acc) {
+                              double *acc, double *slots, unsigned int *count) {
+    __shared__ double red[32];
     double q = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const double ti = b[i] - op.apply(x, i);
@@ -702,7 +738,12 @@ __global__ void k_fp_true_res(StencilOp<2> op, int n, const double *b, const dou
         q += ti * ti;
     }
     for (int o = 16; o; o >>= 1) q += __shfl_xor_sync(CG_FULL, q, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(acc, q);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = q;
+    __syncthreads();
+    double v = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) v += red[w];
+    ordered_grid_sum<1>(&v, slots, blockIdx.x, gridDim.x, count, acc, false);
 }
 
 // Network input channel 1: the mean of log k over each f x f block.
@@ -743,6 +784,8 @@ struct cfm_fpcg {
     int smooth = 0;
     float *xin = nullptr, *out = nullptr;
     double *part = nullptr, *acc = nullptr, *hist = nullptr;
+    double *rslots = nullptr;       // block sums of the true residual (FP_RES_BLOCKS)
+    unsigned int *rcount = nullptr;  // their arrival counter
     FpState *st = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -946,6 +989,9 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
         (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
         (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&h->rslots, sizeof(double) * FP_RES_BLOCKS)) != cudaSuccess ||
+        (e = cudaMalloc(&h->rcount, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMemset(h->rcount, 0, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
         (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -980,6 +1026,8 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     cudaFree(h->out);
     cudaFree(h->part);
     cudaFree(h->acc);
+    cudaFree(h->rslots);
+    cudaFree(h->rcount);
     cudaFree(h->st);
     cudaFree(h->hist);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1062,7 +1110,7 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     CFM_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
     // FP64 true residual; plain persistent CG finishes if FPCG fell short
     CFM_CUDA_TRY(cudaMemsetAsync(h->acc, 0, sizeof(double) * 2, s));
-    k_fp_true_res<<<256, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc);
+    k_fp_true_res<<<FP_RES_BLOCKS, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc, h->rslots, h->rcount);
     double acc[2] = {0, 0};
     CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
     CFM_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1080,7 +1128,7 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
         if (status != CFM_OK && status != CFM_NOT_CONVERGED) return status;
         k_axpy_inplace<<<256, 256, 0, s>>>(a.x, d, h->n);
         CFM_CUDA_TRY(cudaMemsetAsync(h->acc, 0, sizeof(double), s));
-        k_fp_true_res<<<256, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc);
+        k_fp_true_res<<<FP_RES_BLOCKS, 256, 0, s>>>(a.op, h->n, b, a.x, t, h->acc, h->rslots, h->rcount);
         CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
         launches += 3;
     }
@@ -1176,6 +1224,17 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
     CFM_CUDA_TRY(alloc(&dout_b, sizeof(float) * (size_t)nc * batch));
     CFM_CUDA_TRY(alloc(&sums, sizeof(double) * 2 * batch));
     CFM_CUDA_TRY(alloc(&lossd, sizeof(double)));
+    // block sums of the data pairs (256 blocks x 2), the loss dots (64 blocks
+    // x 2 per batch element) and the batch loss, added in a fixed order; and
+    // their counters: [0] pairs, [1] loss, [2 + b] dots of element b
+    constexpr int DATA_BLOCKS = 256, LOSS_BLOCKS = 64;
+    double *dslots;
+    unsigned int *dcount;
+    CFM_CUDA_TRY(alloc(&dslots, sizeof(double) * std::max<size_t>(2 * DATA_BLOCKS, 2 * (size_t)LOSS_BLOCKS * batch)));
+    CFM_CUDA_TRY(alloc(&dcount, sizeof(unsigned int) * (2 + (size_t)batch)));
+    CFM_CUDA_TRY(cudaMemsetAsync(dcount, 0, sizeof(unsigned int) * (2 + (size_t)batch), s));
+    double *lslots;
+    CFM_CUDA_TRY(alloc(&lslots, sizeof(double) * batch));
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<double> kh(n), fh(n);
     std::vector<float> gh(nc);
@@ -1226,7 +1285,7 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
             const double *xj = j == 0 ? nullptr : snap + (size_t)(std::min(j, std::max(taken, 1)) - 1) * n;
             const size_t idx = (size_t)sy * per + j;
             CFM_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
-            k_pair<<<256, 256, 0, s>>>(o2, n, bd, xs, xj, r, e, acc);
+            k_pair<<<DATA_BLOCKS, 256, 0, s>>>(o2, n, bd, xs, xj, r, e, acc, dslots, dcount);
             const double *rin = r;
             if (smooth > 0) {
                 double *zz[2] = {zs, zs + n};
@@ -1236,7 +1295,7 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
                     cur = zz[q & 1];
                 }
                 CFM_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 2, s));
-                k_data_smoothed<<<256, 256, 0, s>>>(o2, n, cur, r, e, r1s, acc);
+                k_data_smoothed<<<DATA_BLOCKS, 256, 0, s>>>(o2, n, cur, r, e, r1s, acc, dslots, dcount);
                 rin = r1s;
             }
             k_pair_store<<<256, 256, 0, s>>>(W, H, f, rin, gf, acc, xin_all + idx * 2 * nc,
@@ -1255,6 +1314,7 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         std::vector<double> k, b, x;
         std::vector<float> best;
         double best_s = 1e300;
+        long long best_it = -1;
         int best_ep = -1;
         ~Val() {
             cfm_fpcg_destroy(fp);
@@ -1271,16 +1331,25 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
         if ((st = cfm_stencil_create(2, W, H, 1, val.k.data(), &val.S))) return st;
         if ((st = cfm_fpcg_create(val.S, val.k.data(), net, smooth, 20000, 1e-8, &val.fp))) return st;
     }
+    // The kept checkpoint is the one whose validation solve took the fewest
+    // iterations (ties: the earlier epoch): a count, not a time, so the
+    // choice, like the training, is the same on every run.
     auto validate = [&](int ep) -> int {
         CFM_CUDA_TRY(cudaStreamSynchronize(s));
         double secs = 1e300;
+        long long iters = -1;
         for (int rep = 0; rep < 2; ++rep) {  // the first solve also instantiates the graph
             cfm_stats vs{};
             const int e2 = cfm_fpcg_solve(val.fp, val.b.data(), val.x.data(), &vs);
-            if (e2 == CFM_OK) secs = std::min(secs, vs.seconds);
-            else if (e2 != CFM_NOT_CONVERGED && e2 != CFM_BREAKDOWN) return e2;
+            if (e2 == CFM_OK) {
+                secs = std::min(secs, vs.seconds);
+                iters = vs.iterations;
+            } else if (e2 != CFM_NOT_CONVERGED && e2 != CFM_BREAKDOWN) {
+                return e2;
+            }
         }
-        if (secs < val.best_s) {
+        if (iters >= 0 && (val.best_ep < 0 || iters < val.best_it)) {
+            val.best_it = iters;
             val.best_s = secs;
             val.best_ep = ep;
             val.best.resize(unet_params(u));
@@ -1311,10 +1380,12 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
             CFM_CUDA_TRY(cudaMemcpy(ids_d, &order[i0], sizeof(long long) * batch, cudaMemcpyHostToDevice));
             if ((st = unet_forward(u, batch, net->xin, out_b, s))) return st;
             CFM_CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(double) * 2 * batch, s));
-            k_loss_anorm_dots<<<dim3(64, batch), 256, 0, s>>>(out_b, r1_all, coef_all, ids_d, per, W,
-                                                             H, f, az_b, sums);
-            k_loss_anorm_grad<<<dim3(64, batch), 256, 0, s>>>(az_b, r1_all, sums, er_all, ids_d, W, H, f,
-                                                             batch, dout_b, lossd);
+            k_loss_anorm_dots<<<dim3(LOSS_BLOCKS, batch), 256, 0, s>>>(out_b, r1_all, coef_all, ids_d, per,
+                                                                      W, H, f, az_b, sums, dslots,
+                                                                      dcount + 2);
+            k_loss_anorm_grad<<<dim3(LOSS_BLOCKS, batch), 256, 0, s>>>(az_b, r1_all, sums, er_all, ids_d, W,
+                                                                      H, f, batch, dout_b, lossd, lslots,
+                                                                      dcount + 1);
             CFM_CUDA_TRY(cudaMemsetAsync(unet_grad(u), 0, unet_params(u) * sizeof(float), s));
             if ((st = unet_backward(u, batch, net->xin, dout_b, s))) return st;
             if ((st = unet_adam(u, lr, 1.0f, s))) return st;

@@ -68,6 +68,9 @@ __device__ __forceinline__ void store8(bf16 *p, const float *v) {
 // Pixels a thread of the first / last layer computes side by side in x: the
 // 3 x (PXB + 2) input neighbourhood is loaded once for all of them.
 constexpr int PXB = 4;
+// Capacity (floats) of a net's block-partials buffer for the thin layers'
+// and the biases' gradients: blocks x entries of the largest such launch.
+constexpr long long GPART_FLOATS = 1LL << 18;
 
 // h0 = relu(cin(x)): x FP32 [B][H][W][2], w [9][32][2].  Lane = 8 * group +
 // q: a group of 8 lanes covers PXB consecutive pixels, lane q their channels
@@ -251,17 +254,40 @@ __global__ void k_cout_bwd(const float *dout, const float *w, const bf16 *g0, bf
     }
 }
 
-// Weight and bias gradient of a thin layer by block-local sums and one
-// atomic per block and entry:  dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci],
-// db[co] += sum_p g[p][co].  `g` is FP32 (cout: one channel) or BF16 (cin:
-// 32 channels); `in` FP32 (cin: the network input) or BF16 (cout: g0).
+// Cross-block sums that come out the same on every run.  Every block has
+// stored its `ne` partial sums at part[blockIdx.x * ne + e]; the last block
+// to arrive (counted on *count) adds them in block order, b = 0, 1, ...,
+// hands each total to dst(e, total) and re-arms *count for the next launch.
+// Called by every thread of the block.
+template <class Dst>
+__device__ void add_partials_in_block_order(const float *part, int ne, unsigned int *count, Dst dst) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(count, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        float v = 0.f;
+        for (unsigned int b = 0; b < gridDim.x; ++b) v += __ldcg(part + (size_t)b * ne + e);
+        dst(e, v);
+    }
+    if (threadIdx.x == 0) *count = 0;
+}
+
+// Weight and bias gradient of a thin layer: per block, the sums over its
+// chunk of pixels, dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci] and
+// db[co] += sum_p g[p][co], then the blocks' sums added in block order.
+// `g` is FP32 (cout: one channel) or BF16 (cin: 32 channels); `in` FP32
+// (cin: the network input) or BF16 (cout: g0).
 template <typename GT, typename IT>
 __global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, float *dw, float *db,
-                             int B, int H, int W, long long chunk) {
-    const int nw = 9 * co_n * ci_n;
+                             int B, int H, int W, long long chunk, float *part, unsigned int *count) {
+    const int nw = 9 * co_n * ci_n, ne = nw + co_n;
     const long long P = (long long)B * H * W;
     const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
-    for (int e = threadIdx.x; e < nw + co_n; e += blockDim.x) {
+    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
         float acc = 0.f;
         if (e < nw) {
             const int t = e / (co_n * ci_n), co = (e / ci_n) % co_n, ci = e % ci_n;
@@ -273,13 +299,16 @@ __global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, floa
                 const long long q = p + (long long)sy * W + sx;
                 acc += (float)g[p * co_n + co] * (float)in[q * ci_n + ci];
             }
-            atomicAdd(dw + e, acc);
         } else {
             const int co = e - nw;
             for (long long p = p0; p < p1; ++p) acc += (float)g[p * co_n + co];
-            atomicAdd(db + co, acc);
         }
+        part[(size_t)blockIdx.x * ne + e] = acc;
     }
+    add_partials_in_block_order(part, ne, count, [&](int e, float v) {
+        if (e < nw) dw[e] += v;
+        else db[e - nw] += v;
+    });
 }
 
 // 2x2 mean pool, NHWC, 8 channels per thread; (h, w) is the pooled size.
@@ -368,8 +397,10 @@ __global__ void k_skip_pool_mask(const bf16 *dskip, const bf16 *dpool, const bf1
     }
 }
 
-// db[c] += sum_p dz[p][c] (NHWC BF16): block-local sums, one atomic per block and channel.
-__global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long long chunk) {
+// db[c] += sum_p dz[p][c] (NHWC BF16): block-local sums over a chunk of
+// pixels, then the blocks' sums added in block order.
+__global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long long chunk, float *part,
+                            unsigned int *count) {
     extern __shared__ float red[];  // [blockDim.x]
     const int c = threadIdx.x % C, lane_p = threadIdx.x / C, np = blockDim.x / C;
     const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
@@ -380,8 +411,9 @@ __global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long 
     if (threadIdx.x < C) {
         float s = 0.f;
         for (int j = 0; j < np; ++j) s += red[j * C + threadIdx.x];
-        atomicAdd(db + threadIdx.x, s);
+        part[(size_t)blockIdx.x * C + threadIdx.x] = s;
     }
+    add_partials_in_block_order(part, C, count, [&](int c, float v) { db[c] += v; });
 }
 
 // BF16 weights [9][co][ci] and their tap-flipped transposes [9][ci][co]
@@ -438,7 +470,13 @@ struct UNetImpl {
     bf16 *wb[UNET_NLAYERS] = {}, *wt[UNET_NLAYERS] = {};
     UNetBuffers a{};
     int *err = nullptr;
-    float *ws = nullptr;  // split-K workspace of the convolutions (TC_WS_FLOATS)
+    float *ws = nullptr;  // split-K workspace of the convolutions and weight gradients
+    long long ws_floats = 0;
+    // per-block partial sums of the thin layers' and the biases' gradients,
+    // added in block order by the last block (deterministic), and the
+    // arrival counters of those reductions
+    float *gpart = nullptr;
+    unsigned int *gcount = nullptr;
     long long adam_t = 0;
     std::vector<void *> allocs;
 };
@@ -490,7 +528,23 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     if (!st) st = dalloc(u, &u->m, o);
     if (!st) st = dalloc(u, &u->v, o);
     if (!st) st = dalloc(u, &u->err, 1);
-    if (!st) st = dalloc(u, &u->ws, (size_t)TC_WS_FLOATS);
+    // the split-K workspace: the forward split's TC_WS_FLOATS or the widest
+    // weight-gradient split of any tensor-core layer at the largest batch
+    u->ws_floats = TC_WS_FLOATS;
+    {
+        DeviceInfo di;
+        if (!st) st = current_device_info(&di);
+        for (int l = 0; !st && l < UNET_NLAYERS; ++l)
+            if (UNET_LAYERS[l].tc) {
+                const int lv = UNET_LAYERS[l].level;
+                u->ws_floats = std::max(u->ws_floats,
+                                        tc_wgrad_ws_floats(maxB, H >> lv, W >> lv, UNET_LAYERS[l].ci,
+                                                           UNET_LAYERS[l].co, di.num_sms));
+            }
+    }
+    if (!st) st = dalloc(u, &u->ws, (size_t)u->ws_floats);
+    if (!st) st = dalloc(u, &u->gpart, (size_t)GPART_FLOATS);
+    if (!st) st = dalloc(u, &u->gcount, 4);
     for (int l = 0; l < UNET_NLAYERS; ++l)
         if (UNET_LAYERS[l].tc) {
             const size_t n = 9 * (size_t)UNET_LAYERS[l].co * UNET_LAYERS[l].ci;
@@ -515,7 +569,8 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     if ((e = cudaMemset(u->theta, 0, o * 4)) != cudaSuccess ||
         (e = cudaMemset(u->m, 0, o * 4)) != cudaSuccess ||
         (e = cudaMemset(u->v, 0, o * 4)) != cudaSuccess ||
-        (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess) {
+        (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(u->gcount, 0, 4 * sizeof(unsigned int))) != cudaSuccess) {
         unet_destroy(u);
         CFM_CUDA_TRY(e);
     }
@@ -579,13 +634,16 @@ int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, i
     int st = nhwc_to_chw(x, a.xt[0], a.xt[1], a.xt[2], B, h, w, L.ci, 3, s);
     if (st) return st;
     if ((st = nhwc_to_chw(dz, nullptr, a.dzt, nullptr, B, h, w, L.co, 1, s))) return st;
-    WgradArgs g{{a.xt[0], a.xt[1], a.xt[2]}, a.dzt, u->grad + u->woff[l], u->err, B, h, w, L.ci, L.co};
+    WgradArgs g{{a.xt[0], a.xt[1], a.xt[2]}, a.dzt, u->grad + u->woff[l], u->err, B, h, w, L.ci, L.co,
+                u->ws, u->ws_floats};
     if ((st = tc_conv_wgrad(g, s))) return st;
     const long long P = (long long)B * h * w;
     const int threads = 256;
     const long long chunk = std::max(64LL, (P + 4 * 148 - 1) / (4 * 148));
-    k_bias_grad<<<(int)((P + chunk - 1) / chunk), threads, threads * sizeof(float), s>>>(
-        dz, u->grad + u->boff[l], P, L.co, chunk);
+    const int blocks = (int)((P + chunk - 1) / chunk);
+    CFM_ARG_CHECK((long long)blocks * L.co <= GPART_FLOATS, "bias-gradient partials");
+    k_bias_grad<<<blocks, threads, threads * sizeof(float), s>>>(dz, u->grad + u->boff[l], P, L.co, chunk,
+                                                                 u->gpart, u->gcount + 2);
     CFM_CUDA_TRY(cudaGetLastError());
     return CFM_OK;
 }
@@ -645,8 +703,11 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
     // cout
     {
         const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
-        k_thin_wgrad<float, bf16><<<(int)((P0 + chunk - 1) / chunk), 320, 0, s>>>(
-            dout, a.g0, 1, 32, u->grad + u->woff[8], u->grad + u->boff[8], B, H, W, chunk);
+        const int blocks = (int)((P0 + chunk - 1) / chunk);
+        CFM_ARG_CHECK((long long)blocks * (9 * 32 + 1) <= GPART_FLOATS, "thin-gradient partials");
+        k_thin_wgrad<float, bf16><<<blocks, 320, 0, s>>>(dout, a.g0, 1, 32, u->grad + u->woff[8],
+                                                         u->grad + u->boff[8], B, H, W, chunk, u->gpart,
+                                                         u->gcount + 0);
         CFM_CUDA_TRY(cudaGetLastError());
         k_cout_bwd<<<grid_for(P0), 256, 0, s>>>(dout, u->theta + u->woff[8], a.g0, a.dz_g0, B, H, W);
         CFM_CUDA_TRY(cudaGetLastError());
@@ -681,8 +742,11 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
     // cin
     {
         const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
-        k_thin_wgrad<bf16, float><<<(int)((P0 + chunk - 1) / chunk), 608, 0, s>>>(
-            a.dz_h0, x, 32, 2, u->grad + u->woff[0], u->grad + u->boff[0], B, H, W, chunk);
+        const int blocks = (int)((P0 + chunk - 1) / chunk);
+        CFM_ARG_CHECK((long long)blocks * (9 * 32 * 2 + 32) <= GPART_FLOATS, "thin-gradient partials");
+        k_thin_wgrad<bf16, float><<<blocks, 608, 0, s>>>(a.dz_h0, x, 32, 2, u->grad + u->woff[0],
+                                                         u->grad + u->boff[0], B, H, W, chunk, u->gpart,
+                                                         u->gcount + 1);
         CFM_CUDA_TRY(cudaGetLastError());
     }
     return CFM_OK;

@@ -25,8 +25,10 @@
 //    (KC consecutive x of one row per step).  A rows come from x-shifted
 //    channel-major copies of the layer input (XT_dx[img][c][y][x] =
 //    X[img][y][x + dx - 1][c]; the y shift is a TMA coordinate), B rows from
-//    the channel-major output gradient.  Tiles split K; the epilogue adds
-//    its partial tile to dW[tap][co][ci] (FP32 atomics).
+//    the channel-major output gradient.  Tiles split K; the epilogue stores
+//    its partial tile in a workspace [split][tap][ci][co] and
+//    tc_wgrad_reduce adds the splits to dW[tap][co][ci] in split order, so
+//    the gradient is the same on every run.
 //
 // Persistent CTAs (one or two per SM, as the host plan says), 6 warps: warp
 // 0 issues TMA (one elected lane), warp 1 owns TMEM and issues tcgen05.mma
@@ -161,6 +163,7 @@ struct TcConvParams {
     const __nv_bfloat16 *mask;  // [B][H][W][N]; zero the output where mask <= 0
     __nv_bfloat16 *out;         // [B][H][W][N]
     float *dw;                  // [9][Cout][Cin]
+    float *wpart;               // wgrad partial tiles [ksplit][9][Cin][Cout] (FP32)
     int *err;
     unsigned long long budget_ns;
 };
@@ -508,15 +511,17 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                 const int tap = g * p.taps_per_tile + j;
                 const int ci = ct * p.ci_rows + row % p.ci_rows;
                 const bool in = j < p.taps_per_tile && tap < 9 && ci < p.Cin;
-                float *d = p.dw + (size_t)(in ? tap : 0) * p.Cout * p.Cin + ci;
+                // this split's partial row (tap, ci): Cout consecutive floats
+                float *d = p.wpart + (((size_t)(t % p.ksplit) * 9 + (in ? tap : 0)) * p.Cin + ci) * p.Cout;
 #pragma unroll 1
                 for (int c = 0; c < N; c += 16) {
                     float acc[16];
                     tmem_ld16(tbase + c, acc);
-                    if (in) {
+                    if (in && c + 16 <= p.Cout) {
+                        float4 *d4 = reinterpret_cast<float4 *>(d + c);
 #pragma unroll
-                        for (int jj = 0; jj < 16; ++jj)
-                            if (c + jj < p.Cout) atomicAdd(d + (size_t)(c + jj) * p.Cin, acc[jj]);
+                        for (int q = 0; q < 4; ++q)
+                            d4[q] = make_float4(acc[4 * q], acc[4 * q + 1], acc[4 * q + 2], acc[4 * q + 3]);
                     }
                 }
             }
@@ -537,6 +542,25 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
 }  // namespace cfm
 
 namespace cfm {
+
+// Weight-gradient splits of tc_conv_kernel: dw[tap][co][ci] += the sum of
+// part[s][tap][ci][co] over s = 0, 1, ..., ksplit - 1 in that order (the
+// same sum on every run).  One thread per element, in the partials' order
+// (coalesced reads).
+__global__ void tc_wgrad_reduce(const float *part, int ksplit, int Cin, int Cout, float *dw) {
+    pdl_enter();
+    const long long n = 9LL * Cin * Cout;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int co = (int)(e % Cout);
+        const long long r = e / Cout;
+        const int ci = (int)(r % Cin), tap = (int)(r / Cin);
+        float v = 0.f;
+        for (int sp = 0; sp < ksplit; ++sp) v += part[(size_t)sp * n + e];
+        float *d = dw + ((size_t)tap * Cout + co) * Cin + ci;
+        *d += v;
+    }
+}
 
 // Split-K reduction and epilogue of tc_conv_kernel: out[p][c] =
 // act(sum_j ws[j][p][c] + bias[c]) [* (mask > 0)], the partials summed in

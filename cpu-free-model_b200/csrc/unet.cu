@@ -238,10 +238,32 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     return launch(kc, a.Cout, ma, mh, ma, mb, p, s);
 }
 
+namespace {
+
+// K splits of a weight gradient: about two tiles per SM, each split at
+// least four K steps.
+long long wgrad_ksplit(int B, int H, int W, int Cin, int num_sms) {
+    const int kc = W % 64 == 0 ? 64 : 32;
+    const int ci_rows = std::min(Cin, 128);
+    const int taps_per_tile = 128 / ci_rows;
+    const long long base = (long long)((9 + taps_per_tile - 1) / taps_per_tile) * (Cin / ci_rows);
+    const long long total_k = (long long)B * H * (W / kc);
+    long long ks = (2LL * num_sms + base - 1) / base;
+    return std::max(1LL, std::min(ks, total_k / 4 > 0 ? total_k / 4 : 1));
+}
+
+}  // namespace
+
+long long tc_wgrad_ws_floats(int B, int H, int W, int Cin, int Cout, int num_sms) {
+    return wgrad_ksplit(B, H, W, Cin, num_sms) * 9LL * Cin * Cout;
+}
+
 int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     CFM_ARG_CHECK(a.Cin % 32 == 0 && a.Cin <= 256, "Cin must be a multiple of 32, at most 256");
     CFM_ARG_CHECK(a.Cout == 32 || a.Cout == 64 || a.Cout == 128 || a.Cout == 256, "Cout");
     CFM_ARG_CHECK(a.W % 32 == 0, "W must be a multiple of 32");
+    const long long per_split = 9LL * a.Cin * a.Cout;
+    CFM_ARG_CHECK(a.ws && a.ws_floats >= per_split, "weight-gradient workspace too small");
     const int kc = a.W % 64 == 0 ? 64 : 32;
     TcConvParams p{};
     p.mode = 1;
@@ -260,11 +282,11 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     int st = current_device_info(&di);
     if (st) return st;
     const long long base = (long long)p.tap_groups * p.ci_tiles;
-    long long ks = (2LL * di.num_sms + base - 1) / base;
-    ks = std::max(1LL, std::min(ks, p.total_k / 4 > 0 ? p.total_k / 4 : 1));
+    const long long ks = std::min(wgrad_ksplit(a.B, a.H, a.W, a.Cin, di.num_sms), a.ws_floats / per_split);
     p.ksplit = (int)ks;
     p.ntiles = (int)(base * ks);
     p.dw = a.dw;
+    p.wpart = a.ws;
     p.err = a.err;
     p.budget_ns = barrier_timeout_ns();
     CUtensorMap m0, m1, m2, mb;
@@ -281,7 +303,11 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
                               (cuuint64_t)a.Cout * a.H * a.W * 2};
     const cuuint32_t bb[4] = {(cuuint32_t)kc, 1, (cuuint32_t)a.Cout, 1};
     if ((st = encode_map(&mb, a.dzt, 4, db, sb, bb, kc * 2))) return st;
-    return launch(kc, a.Cout, m0, m1, m2, mb, p, s);
+    if ((st = launch(kc, a.Cout, m0, m1, m2, mb, p, s))) return st;
+    const int blocks = (int)std::min<long long>((per_split + 255) / 256, (long long)di.num_sms * 4);
+    CFM_CUDA_TRY(launch_pdl(tc_wgrad_reduce, dim3(blocks), dim3(256), 0, s, (const float *)a.ws, p.ksplit,
+                            a.Cin, a.Cout, a.dw));
+    return CFM_OK;
 }
 
 }  // namespace cfm
@@ -380,7 +406,12 @@ int cfm_tc_conv3x3_wgrad(int B, int H, int W, int Cin, int Cout, const unsigned 
     int st = nhwc_to_chw(dx, xt0, xt1, xt2, B, H, W, Cin, 3, 0);
     if (st) return st;
     if ((st = nhwc_to_chw(ddz, nullptr, dzt, nullptr, B, H, W, Cout, 1, 0))) return st;
-    WgradArgs a{{xt0, xt1, xt2}, dzt, ddw, derr, B, H, W, Cin, Cout};
+    DeviceInfo di;
+    if ((st = current_device_info(&di))) return st;
+    const long long wsn = tc_wgrad_ws_floats(B, H, W, Cin, Cout, di.num_sms);
+    float *dws;
+    CFM_CUDA_TRY(d.get(&dws, (size_t)wsn));
+    WgradArgs a{{xt0, xt1, xt2}, dzt, ddw, derr, B, H, W, Cin, Cout, dws, wsn};
     if ((st = tc_conv_wgrad(a, 0))) return st;
     CFM_CUDA_TRY(cudaDeviceSynchronize());
     if ((st = finish_err(derr))) return st;

@@ -397,8 +397,11 @@ int cfm_unet_train_varcoef(cfm_unet *net, int nsys, int snaps, unsigned long lon
  * held-out variable-coefficient system (cfm_varcoef_problem with `seed`, the
  * training systems' size) is solved to 1e-8 by FPCG (the defaults with a
  * network) with the network as it trains, after every `every` epochs and
- * after the last; training ends with the parameters of the fastest solve.
- * every = 0 (default) keeps the last epoch's. */
+ * after the last; training ends with the parameters of the solve that took
+ * the fewest iterations (ties: the earlier epoch).  every = 0 (default)
+ * keeps the last epoch's.  Training is deterministic: every gradient, loss
+ * and data sum is added in a fixed order, so the same seeds give the same
+ * parameters and the same kept epoch on every run. */
 int cfm_unet_set_validation(cfm_unet *net, unsigned long long seed, int every);
 /* The kept checkpoint of the last training: epochs trained (-1: no
  * validation) and its FPCG time on the validation system (ms). */

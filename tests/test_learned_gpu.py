@@ -154,3 +154,24 @@ def test_validation_keeps_a_checkpoint():
     net.set_validation(0, 0)
     net.train_varcoef(6, 3, 40, 2, 4, 1e-3, smooth=4, coarsen=2)
     assert net.validation()[0] == -1
+
+
+def test_training_is_deterministic():
+    """Two trainings from the same seeds give bit-identical parameters, the
+    same losses, the same kept checkpoint and the same FPCG iteration count:
+    the weight gradients (tensor-core and thin layers), bias gradients, loss
+    sums and training-data scalings all add their partial sums in a fixed
+    order, and the checkpoint is chosen by iteration count."""
+    runs = []
+    for _ in range(2):
+        net = cfm.UNet(64, 256, max_batch=4, seed=3)
+        net.set_validation(1000, 1)
+        info = net.train_varcoef(6, 3, 40, 3, 4, 1e-3, smooth=4, coarsen=2)
+        k, f = cfm.varcoef_problem((128, 512), 1001)
+        _, st = cfm.FPCG(cfm.Stencil(k), k, net, maxiter=20000, tol=1e-8).solve(f)
+        runs.append((net.params(), info["loss_first"], info["loss_last"], net.validation()[0],
+                     st.iterations, st.residual))
+        net.close()
+    a, b = runs
+    np.testing.assert_array_equal(a[0], b[0])
+    assert a[1:] == b[1:]

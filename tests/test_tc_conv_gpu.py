@@ -67,3 +67,6 @@ def test_tc_conv_weight_gradient(B, H, W, Cin, Cout):
     ref = wgrad_ref(x.astype(np.float64), dz.astype(np.float64))
     scale = np.sqrt(B * H * W)
     assert np.max(np.abs(got - ref)) <= 1e-4 * scale, np.max(np.abs(got - ref)) / scale
+    # the K splits are added in split order: a second call gives the same bits
+    again = cfm.tc_conv3x3_wgrad(cfm.to_bf16_bits(x), cfm.to_bf16_bits(dz)).astype(np.float64)
+    np.testing.assert_array_equal(again, got)
