@@ -15,12 +15,22 @@ from the previous grid, which does not change the work.  Metric: GLUP/s
          against MEASURED_PEAKS.json's copy bandwidth.
   cpu_baseline  the oracle's FP64 sweep loop (C/OpenMP) on the host cores.
 
+  secondary  (one GPU, after the timed regions; --no-secondary skips it) the
+         other configurations measured in the same run, each with its own
+         CPU baseline from the oracle on the host cores: config 1 (2D 1024^2
+         FP64, 1000 sweeps, final-grid L2 norm), config 3 (CG on 128^3
+         Poisson to 1e-8: standard, pipelined, FP32 with FP64 reliable
+         updates) and config 4 (512^2 variable-coefficient system to 1e-8:
+         plain FP64 persistent and pipelined CG, Jacobi-smoothed and learned
+         flexible PCG, the network trained first and its time stated).
+
 --gpus N runs N independent replicas (one per GPU, no data exchange; weak
 scaling); rank 0 prints the JSON line.  --impl reference times the host
 restatement of the reference's single-GPU sweep (the reference ships no CPU
 Jacobi of its own) on the host cores with the same metric.
 
 Other workloads (--workload, one JSON line each, same keys):
+  jacobi2d   config 1: the 1024^2 FP64 2D problem, 1000 sweeps (on chip).
   jacobi3d_fp32  the same 512^3 problem in FP32 (8 B/LUP) and its error after
              100 sweeps against the FP64 (bit-exact) result.
   cg128      CG on the 128^3 7-point Poisson CSR system to a true relative
@@ -65,8 +75,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["jacobi3d", "jacobi3d_fp32", "cg128", "varcoef512", "unet", "unet_train",
-                                           "batch256", "cpufree"],
+    ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--workload", choices=["jacobi3d", "jacobi2d", "jacobi3d_fp32", "cg128", "varcoef512", "unet",
+                                           "unet_train", "batch256", "cpufree"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -96,7 +107,68 @@ def line(metric, value, unit, args, ms, config, higher=True, extra=None, dtype="
     print(json.dumps(d), flush=True)
 
 
-def workload_cg128(args, cfm):
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def measure_jacobi2d(steps, warmup, cfm, cpu=True):
+    """Config 1: 1024^2 FP64, 1000 sweeps of the reference 2D problem (x
+    columns sin(2 pi y/(ny-1)), periodic y), 16 MiB per grid, so it runs on
+    chip.  GLUP/s of the resident (PERKS-style) and persistent kernels, the
+    final grid's L2 norm, and the oracle's sweep loop as the CPU baseline."""
+    import numpy as np
+    n2, it = 1024, 1000
+    lup = (n2 - 2) ** 2 * it
+    peak, kind = peak_hbm()
+    res, grid = {}, None
+    for impl, name in ((cfm.JACOBI_RESIDENT, "resident"), (cfm.JACOBI_PERSISTENT, "persistent")):
+        with cfm.Jacobi(2, n2, n2, 1, cfm.FP64, 1, impl) as j:
+            j.load_problem(cfm.PROBLEM_REF)
+            j.run(it)
+            g = j.download()
+            if grid is None:
+                grid = g
+            same = bool(np.array_equal(g, grid))
+            for _ in range(warmup):
+                j.run(it)
+            ts = [j.run(it).seconds for _ in range(steps)]
+        t = statistics.median(ts)
+        res[name] = {"ms": t * 1e3, "glups": lup / t * 1e-9, "us_per_sweep": t / it * 1e6,
+                     "hbm_equivalent_frac": 16.0 * lup / t * 1e-9 / peak, "same_grid_as_first": same}
+    out = {"workload": "jacobi2d5p_1024^2_fp64_1000_sweeps", "impls": res,
+           "best": max(res, key=lambda k: res[k]["glups"]),
+           "final_l2_norm": float(np.sqrt(np.sum(grid.astype(np.longdouble) ** 2))),
+           "timing": "median of steps, CUDA events around one 1000-sweep launch (grid on chip)",
+           "peak_hbm_gbs": peak, "peak_kind": kind}
+    if cpu:
+        oracle = _oracle()
+        a = oracle.jacobi2d_init(n2, n2, np.float64)
+        t0 = time.perf_counter()
+        want = oracle.jacobi2d(a, it)
+        tc = time.perf_counter() - t0
+        out["matches_oracle_bitexact"] = bool(np.array_equal(grid, want))
+        out["cpu_baseline"] = {"value": lup / tc * 1e-9, "unit": "GLUP/s", "cores": oracle.max_threads(),
+                               "kind": "port", "sample": "the whole 1000-sweep solve (oracle call, OpenMP)"}
+    return out
+
+
+def workload_jacobi2d(args, cfm):
+    r = measure_jacobi2d(args.steps, args.warmup, cfm, cpu=not args.no_cpu_baseline)
+    best = r["impls"][r["best"]]
+    extra = {"roofline": {"bound": "on-chip (HBM-equivalent bytes)", "achieved": 16.0 * best["glups"],
+                          "peak": r["peak_hbm_gbs"], "unit": "GB/s", "frac": best["hbm_equivalent_frac"],
+                          "peak_kind": r["peak_kind"]}}
+    if "cpu_baseline" in r:
+        extra["cpu_baseline"] = r["cpu_baseline"]
+    line("Jacobi 2d5p 1024^2 FP64 GLUP/s", best["glups"], "GLUP/s", args, best["ms"], r, extra=extra)
+
+
+def measure_cg128(steps, warmup, cfm, cpu=True):
+    """Config 3: CG on the 128^3 7-point Poisson CSR system to a true
+    relative residual of 1e-8, three persistent kernels; the oracle's FP64 CG
+    (C/OpenMP) on the host cores as the CPU baseline."""
     rowptr, col, val = cfm.poisson3d(128)
     A = cfm.CSR(rowptr, col, val)
     b = A.spmv(cfm.uniform(0, A.n))
@@ -105,21 +177,39 @@ def workload_cg128(args, cfm):
     for impl, name in ((cfm.CG_PERSISTENT, "standard"), (cfm.CG_PERSISTENT_PIPELINED, "pipelined"),
                        (cfm.CG_MIXED, "fp32_cg_fp64_reliable_updates")):
         cg = cfm.CG(A, impl, 20000, 1e-8)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             cg.solve(b)
         ts = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             x, st = cg.solve(b)
             ts.append(st.seconds)
+        cg.close()
         t = statistics.median(ts)
         res[name] = {"ms": t * 1e3, "iterations": st.iterations, "refinements": st.refinements,
                      "true_relres": st.residual, "algorithmic_gbs": st.bytes / t * 1e-9,
                      "hbm_frac": st.bytes / t * 1e-9 / peak}
-    best = min(res, key=lambda k: res[k]["ms"])
-    line("CG 128^3 Poisson CSR time to 1e-8 FP64 true relative residual", res[best]["ms"], "ms", args,
-         res[best]["ms"], {"workload": "cg_poisson7_128^3_csr_tol1e-8", "n": A.n, "nnz": len(val),
-                           "best": best, "impls": res, "timing": "median of steps, CUDA events, H2D of b and D2H of x included",
-                           "peak_hbm_gbs": peak, "peak_kind": kind}, higher=False)
+    A.close()
+    out = {"workload": "cg_poisson7_128^3_csr_tol1e-8", "n": A.n, "nnz": len(val), "impls": res,
+           "best": min(res, key=lambda k: res[k]["ms"]),
+           "timing": "median of steps, CUDA events, H2D of b and D2H of x included",
+           "peak_hbm_gbs": peak, "peak_kind": kind}
+    if cpu:
+        oracle = _oracle()
+        t0 = time.perf_counter()
+        _, _, it, rr = oracle.cg(rowptr, col, val, b, 20000, 1e-8)
+        tc = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": tc * 1e3, "unit": "ms", "cores": oracle.max_threads(), "kind": "port",
+                               "iterations": it, "true_relres": rr,
+                               "sample": "one whole FP64 CG solve to 1e-8 (oracle call, OpenMP)"}
+    return out
+
+
+def workload_cg128(args, cfm):
+    r = measure_cg128(args.steps, args.warmup, cfm, cpu=not args.no_cpu_baseline)
+    best = r["impls"][r["best"]]
+    extra = {"cpu_baseline": r["cpu_baseline"]} if "cpu_baseline" in r else None
+    line("CG 128^3 Poisson CSR time to 1e-8 FP64 true relative residual", best["ms"], "ms", args,
+         best["ms"], r, higher=False, extra=extra)
 
 
 def workload_jacobi3d_fp32(args, cfm):
@@ -166,18 +256,21 @@ def workload_jacobi3d_fp32(args, cfm):
          dtype="f32")
 
 
-def workload_varcoef512(args, cfm):
-    import numpy as np
+def measure_varcoef512(steps, warmup, cfm, cpu=True, variants=((8, 2), (8, 3), (8, 4), (8, 1), (4, 1))):
+    """Config 4: the 512^2 variable-coefficient system to 1e-8.  Plain FP64
+    persistent and pipelined CG, Jacobi-smoothed FPCG, and learned FPCG (the
+    network trained here first; its training time is reported); the oracle's
+    plain FP64 CG on the stencil operator as the CPU baseline."""
     N = 512
     k, f = cfm.varcoef_problem((N, N), 0)
     S = cfm.Stencil(k)
     out = {}
 
     def timed(solver):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             solver()
         ts, st = [], None
-        for _ in range(args.steps):
+        for _ in range(steps):
             x, st = solver()
             ts.append(st.seconds)
         return statistics.median(ts), st
@@ -195,9 +288,11 @@ def workload_varcoef512(args, cfm):
     # (256^2), trained here on plain-CG pairs of 100 fresh 512^2 systems
     net = cfm.UNet(N // 2, N // 2, max_batch=8, seed=7)
     net.set_validation(1000, 1)  # keep the checkpoint fastest on a held-out system (not this one)
+    t0 = time.perf_counter()
     info = net.train_varcoef(100, 19, 1000, 16, 8, 1e-3, smooth=4, coarsen=2)
+    info["wall_s"] = time.perf_counter() - t0
     info["kept_epoch"], info["validation_ms"] = net.validation()
-    for m, per in ((8, 2), (8, 3), (8, 4), (8, 1), (4, 1)):
+    for m, per in variants:
         fl = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, truncation=m, net_period=per)
         t, st = timed(lambda: fl.solve(f))
         out[f"fpcg_learned_m{m}_p{per}"] = {"ms": t * 1e3, "iterations": st.iterations,
@@ -206,15 +301,54 @@ def workload_varcoef512(args, cfm):
     head = out["fpcg_learned_m8_p2"]  # the defaults with a network
     head.update({"training": info, "training_pairs": 100 * 20, "network_grid": [N // 2, N // 2],
                  "forward_ms_b1": net.time_forward(1, 20)})
+    net.close()
     base = out["plain_fp64_persistent_cg"]["ms"]
-    line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual, learned FPCG", head["ms"],
-         "ms", args, head["ms"],
-         {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_m8_p2",
-          "speedup_vs_plain_persistent_cg": base / head["ms"],
-          "speedup_jacobi_only_vs_plain": base / out["fpcg_jacobi4"]["ms"], "solvers": out,
-          "precision": "FP64 Krylov recurrences and dots, FP32 smoothing, BF16 network (FP32 accumulate)",
-          "timing": "median of steps, CUDA events around the whole solve incl. H2D b / D2H x"},
-         higher=False)
+    fastest_plain = min(base, out["plain_fp64_pipelined_cg"]["ms"])
+    r = {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_m8_p2",
+         "ms": head["ms"],
+         "speedup_vs_plain_persistent_cg": base / head["ms"],
+         "speedup_vs_fastest_plain_cg": fastest_plain / head["ms"],
+         "speedup_jacobi_only_vs_plain": base / out["fpcg_jacobi4"]["ms"], "solvers": out,
+         "precision": "FP64 Krylov recurrences and dots, FP32 smoothing, BF16 network (FP32 accumulate)",
+         "timing": "median of steps, CUDA events around the whole solve incl. H2D b / D2H x"}
+    if cpu:
+        oracle = _oracle()
+        c = cfm.varcoef_coeffs(k)
+        t0 = time.perf_counter()
+        _, _, it, _, rr = oracle.krylov_stencil(2, (N, N, 1), c, f.ravel(), 0, 50000, 1e-8)
+        tc = time.perf_counter() - t0
+        r["cpu_baseline"] = {"value": tc * 1e3, "unit": "ms", "cores": oracle.max_threads(), "kind": "port",
+                             "iterations": it, "true_relres": rr,
+                             "sample": "one whole plain FP64 CG solve to 1e-8 (oracle call, OpenMP)"}
+    return r
+
+
+def workload_varcoef512(args, cfm):
+    r = measure_varcoef512(args.steps, args.warmup, cfm, cpu=not args.no_cpu_baseline)
+    extra = {"cpu_baseline": r["cpu_baseline"]} if "cpu_baseline" in r else None
+    line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual, learned FPCG", r["ms"],
+         "ms", args, r["ms"], r, higher=False, extra=extra)
+
+
+def secondary(cfm):
+    """The other configurations in the default run (rank 0, one GPU): short
+    repeats (3 timed after 1 warm-up), each with its CPU baseline."""
+    out, t0 = {}, time.perf_counter()
+    for name, fn in (("config1_jacobi2d_1024_fp64", lambda: measure_jacobi2d(3, 1, cfm)),
+                     ("config3_cg_poisson128", lambda: measure_cg128(3, 1, cfm)),
+                     ("config4_varcoef512", lambda: measure_varcoef512(3, 1, cfm, variants=((8, 2),)))):
+        t1 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # one failing config must not hide the headline
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = time.perf_counter() - t1
+    v = out.get("config4_varcoef512", {})
+    if "ms" in v:
+        out["learned_fpcg_vs_plain_fp64_cg"] = v["speedup_vs_plain_persistent_cg"]
+        out["learned_fpcg_vs_fastest_plain_cg"] = v["speedup_vs_fastest_plain_cg"]
+    out["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def workload_unet(args, cfm):
@@ -374,7 +508,8 @@ def workload_batch256(args, cfm):
 def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
-    {"cg128": workload_cg128, "jacobi3d_fp32": workload_jacobi3d_fp32, "varcoef512": workload_varcoef512,
+    {"cg128": workload_cg128, "jacobi2d": workload_jacobi2d, "jacobi3d_fp32": workload_jacobi3d_fp32,
+     "varcoef512": workload_varcoef512,
      "unet": workload_unet, "unet_train": workload_unet_train, "cpufree": workload_cpufree,
      "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
@@ -613,6 +748,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
+    if rank == 0 and world == 1 and not args.no_secondary:
+        line["secondary"] = secondary(cfm)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
