@@ -298,18 +298,28 @@ def measure_varcoef512(steps, warmup, cfm, cpu=True, variants=((8, 2), (8, 3), (
         out[f"fpcg_learned_m{m}_p{per}"] = {"ms": t * 1e3, "iterations": st.iterations,
                                             "true_relres": st.residual, "fallback": st.refinements,
                                             "truncation": m, "network_every": per}
-    head = out["fpcg_learned_m8_p2"]  # the defaults with a network
+        fl.close()
+    # learned + mixed: the defaults with FP32 Krylov vectors and FP64 reliable updates
+    fm = cfm.FPCG(S, k, net, maxiter=20000, tol=1e-8, precision=cfm.FP32)
+    t, st = timed(lambda: fm.solve(f))
+    out["fpcg_learned_mixed_m8_p2"] = {"ms": t * 1e3, "iterations": st.iterations, "true_relres": st.residual,
+                                       "fallback": st.refinements, "reliable_updates": fm.reliable_updates(),
+                                       "truncation": 8, "network_every": 2, "delta": 0.1}
+    fm.close()
+    head = out["fpcg_learned_mixed_m8_p2"]  # learned + mixed, the configuration the target names
     head.update({"training": info, "training_pairs": 100 * 20, "network_grid": [N // 2, N // 2],
                  "forward_ms_b1": net.time_forward(1, 20)})
     net.close()
     base = out["plain_fp64_persistent_cg"]["ms"]
     fastest_plain = min(base, out["plain_fp64_pipelined_cg"]["ms"])
-    r = {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_m8_p2",
+    r = {"workload": "varcoef2d_512^2_grf_sigma1_corr16_tol1e-8", "solver": "fpcg_learned_mixed_m8_p2",
          "ms": head["ms"],
          "speedup_vs_plain_persistent_cg": base / head["ms"],
          "speedup_vs_fastest_plain_cg": fastest_plain / head["ms"],
          "speedup_jacobi_only_vs_plain": base / out["fpcg_jacobi4"]["ms"], "solvers": out,
-         "precision": "FP64 Krylov recurrences and dots, FP32 smoothing, BF16 network (FP32 accumulate)",
+         "learned_fp64_krylov_ms": out["fpcg_learned_m8_p2"]["ms"],
+         "precision": "FP32 Krylov vectors with FP64 reliable updates, FP64 dots / alpha / beta / true "
+                      "residual; FP32 smoothing; BF16 network (FP32 accumulate)",
          "timing": "median of steps, CUDA events around the whole solve incl. H2D b / D2H x"}
     if cpu:
         oracle = _oracle()
@@ -326,7 +336,7 @@ def measure_varcoef512(steps, warmup, cfm, cpu=True, variants=((8, 2), (8, 3), (
 def workload_varcoef512(args, cfm):
     r = measure_varcoef512(args.steps, args.warmup, cfm, cpu=not args.no_cpu_baseline)
     extra = {"cpu_baseline": r["cpu_baseline"]} if "cpu_baseline" in r else None
-    line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual, learned FPCG", r["ms"],
+    line("512^2 variable-coefficient time to 1e-8 FP64 true relative residual, learned + mixed FPCG", r["ms"],
          "ms", args, r["ms"], r, higher=False, extra=extra)
 
 

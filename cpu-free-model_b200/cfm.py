@@ -88,6 +88,8 @@ _SIGS = {
     "cfm_fpcg_set_network_period": (_c.c_int, [_vp, _c.c_int]),
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
+    "cfm_fpcg_set_precision": (_c.c_int, [_vp, _c.c_int, _c.c_double]),
+    "cfm_fpcg_reliable_updates": (_c.c_int, [_vp]),
     "cfm_batch_create": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cfm_batch_destroy": (None, [_vp]),
     "cfm_batch_set_plan": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
@@ -584,7 +586,8 @@ class UNet:
 class FPCG:
     """Flexible PCG with the network as preconditioner (cfm_fpcg)."""
 
-    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None, net_period=None):
+    def __init__(self, S, k, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None, net_period=None,
+                 precision=None, delta=0.1):
         self.S, self.net = S, net
         self.k = np.ascontiguousarray(k, np.float64)
         h = ctypes.c_void_p()
@@ -598,6 +601,17 @@ class FPCG:
             check("cfm_fpcg_set_truncation", lib.cfm_fpcg_set_truncation(self.h, truncation))
         if net_period is not None:
             check("cfm_fpcg_set_network_period", lib.cfm_fpcg_set_network_period(self.h, net_period))
+        if precision is not None:
+            self.set_precision(precision, delta)
+
+    def set_precision(self, precision, delta=0.1):
+        """FP64, or FP32 Krylov vectors with FP64 reliable updates (delta: the
+        residual drop that triggers one)."""
+        check("cfm_fpcg_set_precision", lib.cfm_fpcg_set_precision(self.h, precision, delta))
+
+    def reliable_updates(self):
+        """FP64 reliable updates of the last solve (mixed precision)."""
+        return lib.cfm_fpcg_reliable_updates(self.h)
 
     def close(self):
         if getattr(self, "h", None):

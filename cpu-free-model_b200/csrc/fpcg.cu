@@ -292,7 +292,8 @@ enum : int {
 // slots (slot j mod (m + 1)).
 constexpr int FP_MAX_TRUNC = 8;
 constexpr int FP_RES_BLOCKS = 256;  // grid of the true-residual pass
-constexpr int FP_NSLOT = FP_ZS + FP_MAX_TRUNC;
+constexpr int FP_TT = FP_ZS + FP_MAX_TRUNC;  // |b - A x|^2 of a reliable update (mixed)
+constexpr int FP_NSLOT = FP_TT + 1;
 
 struct FpState {
     double ps[FP_MAX_TRUNC + 1];  // <p_j, s_j> by ring slot
@@ -302,6 +303,11 @@ struct FpState {
     long long best_k;    // iteration of best_rr
     int done;            // 1 converged, 2 stalled / capped
     int pad;
+    // mixed precision: largest |r32|^2 since the last reliable update, the
+    // parity of the FP64 iterate / FP32 correction buffers, a reliable update
+    // waiting for k_fp_pre, and the updates so far
+    double gmax;
+    int par, pending, updates, pad2;
 };
 
 struct FpArgs {
@@ -324,6 +330,15 @@ struct FpArgs {
     const float *we32, *wn32, *dg32, *wd32;  // FP32 operator and omega / dg for the smoothing
     int pstride;       // partial-sum slot stride: max(ntiles, ntiles2)
     int smooth;
+    // mixed precision: the Krylov vectors in FP32 (residual r32,
+    // preconditioned residual z32, direction rings), the iterate in FP64 as
+    // xm + dm (FP64 iterate at the last reliable update + FP32 steps since),
+    // both double-buffered by the update parity in FpState
+    int mixed;
+    double delta2;  // a reliable update when |r32|^2 < delta^2 max |r32|^2 since the last
+    float *r32, *z32, *pring32, *sring32;
+    double *xm[2];
+    float *dm[2];
 };
 
 
@@ -362,7 +377,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
         const double bi = a.b[i];
         a.x[i] = 0.0;
         a.r[i] = bi;
-        bb = bi * bi;
+        bb = __dmul_rn(bi, bi);
     }
     bb = block_sum(bb, sm);
     if (threadIdx.x == 0) {
@@ -431,7 +446,7 @@ __device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
         int i;
         const bool in = fp_inside(t, a, row, col, &i);
         const int l = row * t.R + col;
-        t.r()[l] = in ? (float)a.r[i] : 0.f;
+        t.r()[l] = in ? (a.mixed ? a.r32[i] : (float)a.r[i]) : 0.f;
         t.we()[l] = in ? a.we32[i] : 0.f;
         t.wn()[l] = in ? a.wn32[i] : 0.f;
         t.dg()[l] = in ? a.dg32[i] : 1.f;
@@ -486,6 +501,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
     if (blockIdx.x == 0) {
         const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
         const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);
+        const double tt = a.mixed ? sum_partials(fslot(a, FP_TT), a.ntiles, sm) : 0.0;
         if (threadIdx.x == 0) {
             FpState *st = a.st;
             if (tick) st->k += 1;
@@ -495,7 +511,17 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
                 st->target = target;
             }
             if (st->k <= a.maxiter) a.hist[st->k] = sqrt(rr);
-            if (sqrt(rr) <= target) st->done = 1;
+            if (!a.mixed) {
+                if (sqrt(rr) <= target) st->done = 1;
+            } else if (st->pending) {  // a reliable update ran: the FP64 true residual judges
+                st->par ^= 1;
+                st->pending = 0;
+                st->updates += 1;
+                st->gmax = rr;
+                if (sqrt(tt) <= target) st->done = 1;
+            } else if (rr > st->gmax) {
+                st->gmax = rr;
+            }
             if (rr < st->best_rr) {
                 st->best_rr = rr;
                 st->best_k = st->k;
@@ -570,8 +596,9 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
         const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
         t.z0()[row * t.R + col] =
             fp_inside(t, a, row, col, &i)
-                ? (float)(c != 0.0 ? a.za[i] + c * (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)]
-                                   : a.za[i])
+                ? __double2float_rn(c != 0.0 ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)],
+                                                        a.za[i])
+                                             : a.za[i])
                 : 0.f;
     }
     __syncthreads();
@@ -583,18 +610,22 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
     double zi = 0;
     if (in) {
         zi = (double)z[l];
-        a.z[i] = zi;
+        if (a.mixed) a.z32[i] = z[l];
+        else a.z[i] = zi;
     }
     const int k = (int)a.st->k;
     const int nj = min(a.m, k);
     if (nj > 0) {
         __shared__ double smm[33 * FP_MAX_TRUNC];
-        __shared__ const double *sj[FP_MAX_TRUNC];
-        if (threadIdx.x < nj) sj[threadIdx.x] = a.sring + (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
+        __shared__ size_t sj[FP_MAX_TRUNC];  // ring slot offsets of s_{k-1-j}
+        if (threadIdx.x < nj) sj[threadIdx.x] = (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
         __syncthreads();
         double v[FP_MAX_TRUNC];
 #pragma unroll
-        for (int j = 0; j < FP_MAX_TRUNC; ++j) v[j] = (j < nj && in) ? zi * sj[j][i] : 0.0;
+        for (int j = 0; j < FP_MAX_TRUNC; ++j)
+            v[j] = (j < nj && in) ? (a.mixed ? xprod(z[l], a.sring32[sj[j] + i])
+                                             : __dmul_rn(zi, a.sring[sj[j] + i]))
+                                  : 0.0;
         block_sum_multi(v, nj, smm);
         if (threadIdx.x < nj) fslot(a, FP_ZS + threadIdx.x)[blockIdx.x] = v[threadIdx.x];
     }
@@ -629,13 +660,13 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
         const float *y = a.out;  // z = P y on this grid: z[j] = y[cell(j)]
         const float *yrow = y + cy * a.ncx;
         const double zi = (double)yrow[cx];
-        double t = o.dg[i] * zi;
-        if (ix > 0) t -= o.we[i - 1] * (double)yrow[(ix - 1) >> sh];
-        if (ix < nx - 1) t -= o.we[i] * (double)yrow[(ix + 1) >> sh];
-        if (iy > 0) t -= o.wn[i - nx] * (double)y[((iy - 1) >> sh) * a.ncx + cx];
-        if (iy < o.ny - 1) t -= o.wn[i] * (double)y[((iy + 1) >> sh) * a.ncx + cx];
-        yr = zi * a.r1[i];
-        yay = zi * t;
+        double t = __dmul_rn(o.dg[i], zi);
+        if (ix > 0) t = __fma_rn(-o.we[i - 1], (double)yrow[(ix - 1) >> sh], t);
+        if (ix < nx - 1) t = __fma_rn(-o.we[i], (double)yrow[(ix + 1) >> sh], t);
+        if (iy > 0) t = __fma_rn(-o.wn[i - nx], (double)y[((iy - 1) >> sh) * a.ncx + cx], t);
+        if (iy < o.ny - 1) t = __fma_rn(-o.wn[i], (double)y[((iy + 1) >> sh) * a.ncx + cx], t);
+        yr = __dmul_rn(zi, a.r1[i]);
+        yay = __dmul_rn(zi, t);
     }
     yr = block_sum(yr, sm);
     yay = block_sum(yay, sm);
@@ -676,10 +707,19 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
     FP_ROW;
     double pr = 0;
     if (i < a.n) {
-        double pi = a.z[i];
-        for (int j = 0; j < nj; ++j) pi -= beta[j] * pj[j][i];
-        a.pring[(size_t)(k % a.ring) * a.n + i] = pi;
-        pr = pi * a.r[i];
+        if (a.mixed) {  // FP32 direction, beta rounded to FP32
+            float pi = a.z32[i];
+            for (int j = 0; j < nj; ++j)
+                pi = __fmaf_rn(-__double2float_rn(beta[j]),
+                               a.pring32[(size_t)((k - 1 - j) % a.ring) * a.n + i], pi);
+            a.pring32[(size_t)(k % a.ring) * a.n + i] = pi;
+            pr = xprod(pi, a.r32[i]);
+        } else {
+            double pi = a.z[i];
+            for (int j = 0; j < nj; ++j) pi = __fma_rn(-beta[j], pj[j][i], pi);
+            a.pring[(size_t)(k % a.ring) * a.n + i] = pi;
+            pr = __dmul_rn(pi, a.r[i]);
+        }
     }
     pr = block_sum(pr, sm);
     if (threadIdx.x == 0) fslot(a, FP_PR)[blockIdx.x] = pr;
@@ -698,7 +738,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
     if (i < a.n) {
         const double si = a.op.apply(p, i);
         a.sring[(size_t)slot * a.n + i] = si;
-        ps = p[i] * si;
+        ps = __dmul_rn(p[i], si);
     }
     ps = block_sum(ps, sm);
     if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
@@ -716,14 +756,144 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     FP_ROW;
     double rr = 0;
     if (i < a.n) {
-        a.x[i] += alpha * a.pring[(size_t)slot * a.n + i];
-        const double rn = a.r[i] - alpha * a.sring[(size_t)slot * a.n + i];
+        a.x[i] = __fma_rn(alpha, a.pring[(size_t)slot * a.n + i], a.x[i]);
+        const double rn = __fma_rn(-alpha, a.sring[(size_t)slot * a.n + i], a.r[i]);
         a.r[i] = rn;
-        rr = rn * rn;
+        rr = __dmul_rn(rn, rn);
     }
     rr = block_sum(rr, sm);
     if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+}
+
+// ------------------------------------------------- mixed-precision kernels
+// x = 0 (FP64 iterate and FP32 correction of parity 0), r32 = fl32(b);
+// partials |b|^2 (FP64) and |r32|^2.
+__global__ void __launch_bounds__(CG_TILE) k_fpm_init(FpArgs a, double tol) {
+    __shared__ double sm[33];
+    FP_ROW;
+    double bb = 0, rr = 0;
+    if (i < a.n) {
+        const double bi = a.b[i];
+        const float ri = __double2float_rn(bi);
+        a.xm[0][i] = 0.0;
+        a.dm[0][i] = 0.f;
+        a.r32[i] = ri;
+        bb = __dmul_rn(bi, bi);
+        rr = xprod(ri, ri);
+    }
+    bb = block_sum(bb, sm);
+    rr = block_sum(rr, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_BB)[blockIdx.x] = bb;
+        fslot(a, FP_RR)[blockIdx.x] = rr;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->k = 0;
+        a.st->done = 0;
+        a.st->best_rr = 1e300;
+        a.st->best_k = 0;
+        for (int j = 0; j <= FP_MAX_TRUNC; ++j) a.st->ps[j] = 0;
+        a.st->target = -tol;
+        a.st->gmax = 0.0;
+        a.st->par = 0;
+        a.st->pending = 0;
+        a.st->updates = 0;
+    }
+}
+
+// s32 = A p32 with the FP32 operator; partial <p32, s32> (FP64 sum of the
+// exact FP32 products).
+__global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
+    pdl_enter();
+    __shared__ double sm[33];
+    const int slot = (int)a.st->k % a.ring;
+    const float *p = a.pring32 + (size_t)slot * a.n;
+    FP_ROW;
+    double ps = 0;
+    if (i < a.n) {
+        const float si = a.op.apply32(p, i);
+        a.sring32[(size_t)slot * a.n + i] = si;
+        ps = xprod(p[i], si);
+    }
+    ps = block_sum(ps, sm);
+    if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
+}
+
+// alpha = <p, r> / <p, s> (FP64, applied rounded to FP32); d += alpha p,
+// r32 -= alpha s (FP32); partial |r32|^2.
+__global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
+    pdl_enter();
+    __shared__ double sm[33];
+    const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
+    const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
+    const int slot = (int)a.st->k % a.ring;
+    const float af = __double2float_rn(ps != 0.0 ? pr / ps : 0.0);
+    float *d = a.dm[a.st->par];
+    FP_ROW;
+    double rr = 0;
+    if (i < a.n) {
+        d[i] = __fmaf_rn(af, a.pring32[(size_t)slot * a.n + i], d[i]);
+        const float rn = __fmaf_rn(-af, a.sring32[(size_t)slot * a.n + i], a.r32[i]);
+        a.r32[i] = rn;
+        rr = xprod(rn, rn);
+    }
+    rr = block_sum(rr, sm);
+    if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+}
+
+// Reliable update, when |r32|^2 has reached tol^2 |b|^2 or fallen below
+// delta^2 times its largest value since the last update (every block sums
+// the same partials in the same order, so all decide alike; otherwise they
+// return at once): x' = x + d in FP64 into
+// the other parity's buffer, d' = 0, t = b - A x' (FP64, A x' from x + d on
+// the fly, so no grid barrier), r32 = fl32(t); partials |t|^2 and |r32|^2.
+// k_fp_pre flips the parity and judges convergence by |t|.
+__global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
+    pdl_enter();
+    __shared__ double sm[33];
+    const double g = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
+    const FpState *st = a.st;
+    const double target = st->target;
+    if (!(g <= target * target || g < a.delta2 * st->gmax)) return;
+    const int par = st->par;
+    const double *x = a.xm[par];
+    const float *d = a.dm[par];
+    FP_ROW;
+    double tt = 0, rr = 0;
+    if (i < a.n) {
+        const StencilOp<2> &o = a.op;
+        const int nx = o.nx, iy = i / nx, ix = i - iy * nx;
+        auto xv = [&](int j) { return __dadd_rn(x[j], (double)d[j]); };
+        const double xi = xv(i);
+        double t = __dmul_rn(o.dg[i], xi);
+        if (ix > 0) t = __fma_rn(-o.we[i - 1], xv(i - 1), t);
+        if (ix < nx - 1) t = __fma_rn(-o.we[i], xv(i + 1), t);
+        if (iy > 0) t = __fma_rn(-o.wn[i - nx], xv(i - nx), t);
+        if (iy < o.ny - 1) t = __fma_rn(-o.wn[i], xv(i + nx), t);
+        const double ti = __dsub_rn(a.b[i], t);
+        const float ri = __double2float_rn(ti);
+        a.xm[par ^ 1][i] = xi;
+        a.dm[par ^ 1][i] = 0.f;
+        a.r32[i] = ri;
+        tt = __dmul_rn(ti, ti);
+        rr = xprod(ri, ri);
+    }
+    tt = block_sum(tt, sm);
+    rr = block_sum(rr, sm);
+    if (threadIdx.x == 0) {
+        fslot(a, FP_TT)[blockIdx.x] = tt;
+        fslot(a, FP_RR)[blockIdx.x] = rr;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->pending = 1;
+}
+
+// The result of a mixed solve: x = xm + dm of the current parity (FP64).
+__global__ void k_fpm_finish(FpArgs a, const FpState *st) {
+    const int par = st->par;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        a.x[i] = __dadd_rn(a.xm[par][i], (double)a.dm[par][i]);
 }
 
 // t = b - A x, |t|^2 into acc[0] (the judged true residual; grid sum in
@@ -793,6 +963,13 @@ struct cfm_fpcg {
     cudaGraphExec_t exec = nullptr;
     bool conditional = false;
     long long last_k = 0;
+    // mixed precision (cfm_fpcg_set_precision): r32 z32 | FP32 rings (2 (m + 1) n)
+    // | FP32 corrections (2 n) and FP64 iterates (2 n) by update parity
+    int mixed = 0;
+    double delta = 0.1;
+    float *vec32 = nullptr, *ring32 = nullptr;
+    double *xm = nullptr;
+    int last_updates = 0;
 };
 
 namespace {
@@ -832,10 +1009,26 @@ FpArgs fp_args(cfm_fpcg *h) {
         a.wn32 = c32 + n;
         a.dg32 = c32 + 3 * n;
         a.wd32 = h->wd32;
+        a.op.we32 = c32;  // the operator's FP32 apply (mixed precision)
+        a.op.wn32 = c32 + n;
+        a.op.wt32 = c32 + 2 * n;
+        a.op.dg32 = c32 + 3 * n;
     }
     a.tx2 = h->tx2;
     a.pstride = h->pstride;
     a.smooth = h->smooth;
+    a.mixed = h->mixed;
+    a.delta2 = h->delta * h->delta;
+    if (h->mixed) {
+        a.r32 = h->vec32;
+        a.z32 = h->vec32 + n;
+        a.dm[0] = h->vec32 + 2 * n;
+        a.dm[1] = h->vec32 + 3 * n;
+        a.pring32 = h->ring32;
+        a.sring32 = h->ring32 + (size_t)(h->m + 1) * n;
+        a.xm[0] = h->xm;
+        a.xm[1] = h->xm + n;
+    }
     return a;
 }
 
@@ -871,9 +1064,34 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
 }
 
 int fp_iteration(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, bool use_net) {
-    CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-    CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+    if (h->mixed) {
+        CFM_CUDA_TRY(launch_pdl(k_fpm_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fpm_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fpm_reliable, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+    } else {
+        CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+    }
     return fp_precond_dir(h, a, cond, set_cond, 1, use_net);
+}
+
+// Drops the captured iteration graph (it holds buffer addresses and the
+// kernel sequence); the next solve builds it again.
+void drop_graph(cfm_fpcg *h) {
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->exec = nullptr;
+    h->graph = nullptr;
+    h->conditional = false;
+}
+
+// FP32 rings of the mixed solve for truncation m.
+int alloc_ring32(cfm_fpcg *h, int m) {
+    float *r = nullptr;
+    CFM_CUDA_TRY(cudaMalloc(&r, sizeof(float) * 2 * (m + 1) * (size_t)h->n));
+    cudaFree(h->ring32);
+    h->ring32 = r;
+    return CFM_OK;
 }
 
 // One pass of the device loop: h->net_every iterations, the network in the
@@ -1028,6 +1246,9 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     cudaFree(h->acc);
     cudaFree(h->rslots);
     cudaFree(h->rcount);
+    cudaFree(h->vec32);
+    cudaFree(h->ring32);
+    cudaFree(h->xm);
     cudaFree(h->st);
     cudaFree(h->hist);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1046,15 +1267,46 @@ int cfm_fpcg_set_truncation(cfm_fpcg *h, int m) {
     CFM_CUDA_TRY(cudaMalloc(&ring, sizeof(double) * 2 * (m + 1) * (size_t)h->n));
     cudaFree(h->ring);
     h->ring = ring;
+    if (h->mixed) {
+        const int st = alloc_ring32(h, m);
+        if (st) return st;
+    }
     h->m = m;
     // the captured iteration graph holds the old ring: build it again
-    if (h->exec) cudaGraphExecDestroy(h->exec);
-    if (h->graph) cudaGraphDestroy(h->graph);
-    h->exec = nullptr;
-    h->graph = nullptr;
-    h->conditional = false;
+    drop_graph(h);
     return CFM_OK;
 }
+
+int cfm_fpcg_set_precision(cfm_fpcg *h, int precision, double delta) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(precision == CFM_FP64 || precision == CFM_FP32, "precision");
+    CFM_ARG_CHECK(delta > 0.0 && delta < 1.0, "delta must be in (0, 1)");
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const int mixed = precision == CFM_FP32;
+    if (mixed && !h->vec32) {
+        const size_t n = h->n;
+        float *v = nullptr;
+        double *xm = nullptr;
+        CFM_CUDA_TRY(cudaMalloc(&v, sizeof(float) * 4 * n));
+        if (cudaMalloc(&xm, sizeof(double) * 2 * n) != cudaSuccess) {
+            cudaFree(v);
+            cudaGetLastError();
+            set_error("mixed-precision buffers: out of device memory");
+            return CFM_OUT_OF_MEMORY;
+        }
+        h->vec32 = v;
+        h->xm = xm;
+        const int st = alloc_ring32(h, h->m);
+        if (st) return st;
+    }
+    if (mixed != h->mixed || delta != h->delta) drop_graph(h);
+    h->mixed = mixed;
+    h->delta = delta;
+    return CFM_OK;
+}
+
+int cfm_fpcg_reliable_updates(const cfm_fpcg *h) { return h ? h->last_updates : -1; }
 
 int cfm_fpcg_set_network_period(cfm_fpcg *h, int every) {
     clear_error();
@@ -1090,7 +1342,10 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     }
     int launches = 0;
     CFM_CUDA_TRY(cudaEventRecord(h->ev0, s));
-    k_fp_init<<<h->ntiles, CG_TILE, 0, s>>>(a, h->tol);
+    if (h->mixed)
+        k_fpm_init<<<h->ntiles, CG_TILE, 0, s>>>(a, h->tol);
+    else
+        k_fp_init<<<h->ntiles, CG_TILE, 0, s>>>(a, h->tol);
     CFM_CUDA_TRY(cudaGetLastError());
     if ((st = fp_precond_dir(h, a, 0, 0, 0))) return st;
     launches += 2;
@@ -1107,6 +1362,11 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
             if (hs.done) break;
         }
     }
+    if (h->mixed) {  // x = FP64 iterate + the FP32 steps since the last update
+        k_fpm_finish<<<256, 256, 0, s>>>(a, h->st);
+        CFM_CUDA_TRY(cudaGetLastError());
+        ++launches;
+    }
     CFM_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
     // FP64 true residual; plain persistent CG finishes if FPCG fell short
     CFM_CUDA_TRY(cudaMemsetAsync(h->acc, 0, sizeof(double) * 2, s));
@@ -1116,6 +1376,7 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     CFM_CUDA_TRY(cudaStreamSynchronize(s));
     if (h->net && (st = unet_check_err(h->net->u))) return st;
     h->last_k = hs.k;
+    h->last_updates = h->mixed ? hs.updates : 0;
     const double bnorm = hs.target / h->tol;
     double tnorm = std::sqrt(acc[0]);
     int fallback = 0;

@@ -432,6 +432,21 @@ int cfm_fpcg_set_truncation(cfm_fpcg *h, int m);
 /* Apply the network in one of every `every` iterations (1..8; default 2
  * with a network); the others use the smoothing alone (c = 0). */
 int cfm_fpcg_set_network_period(cfm_fpcg *h, int every);
+/* Precision of the Krylov iteration.  CFM_FP64 (default): FP64 vectors,
+ * recurrences and dots.  CFM_FP32: mixed precision with FP64 reliable
+ * updates -- the residual, directions, A p and the correction are FP32 and
+ * A p uses the FP32 coefficients; dots are FP64 sums of the exact FP32
+ * products and alpha, beta are FP64 (applied rounded to FP32); the iterate is
+ * x = x64 + d32.  When |r32| reaches tol |b| or falls below delta times its
+ * largest value since the last update, x64 += d32 in FP64, d32 = 0 and r32 is
+ * replaced by fl32(b - A x64) from the FP64 true residual, which alone
+ * decides convergence; the directions are kept (the reliable-update scheme
+ * of CFM_CG_MIXED).  The preconditioner is unchanged (FP32 smoothing, BF16
+ * network); plain FP64 CG stays the fallback.  No counterpart in the
+ * reference (its CG is FP64 only). */
+int cfm_fpcg_set_precision(cfm_fpcg *h, int precision, double delta);
+/* FP64 reliable updates of the last solve (0 in FP64 mode). */
+int cfm_fpcg_reliable_updates(const cfm_fpcg *h);
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
 /* Recursive residual norms |r_k| of the last solve, one per iteration from
  * k = 0 (at most max_n; *n_out = the count).  net == NULL in

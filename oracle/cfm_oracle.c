@@ -800,3 +800,288 @@ int orc_krylov_stencil(int dims, int nx, int ny, int nz, const double *we, const
     free(A.we32); free(A.wn32); free(A.wt32); free(A.dg32);
     return st;
 }
+
+/* ------------------------------------------------------------------ FPCG */
+
+/* Flexible PCG on the 2D variable-coefficient stencil, the device loop of
+ * the learned-preconditioner solver (csrc/fpcg.cu) with the identity in
+ * place of the network, step for step: truncated FCG(m), the preconditioner
+ * z = J(z0 + c P R r1) (z0 = J(0) by `smooth` damped Jacobi sweeps in FP32,
+ * r1 = r - A z0, R the f x f block mean, P its piecewise-constant
+ * prolongation, c = <P y, r1> / <P y, A P y>), FP64 Krylov vectors or
+ * (mixed) FP32 ones with FP64 reliable updates.  Dots are the GPU's trees:
+ * rows in 1024-row tiles, the smoothing kernels' dots in 32 x 32-cell tiles.
+ * Has no reference counterpart (the reference's CG is unpreconditioned). */
+#define FPO_TILE 32
+#define FPO_STALL 200
+#define FPO_OMEGA 0.8
+
+typedef struct {
+    int nx, ny, n, f, ncx, nc, smooth, m, ring, mixed, tx2, nt1, nt2;
+    const double *we, *wn, *dg, *b;
+    orc_op A;  /* FP64 and FP32 operator */
+    float *wd;
+    double delta2, *scr, *part1, *part2;
+} fpo_ctx;
+
+/* 1024-row tile partials of v, summed as the GPU's partial slots. */
+static double fpo_sum1(fpo_ctx *c, const double *v) {
+    for (int t = 0; t < c->nt1; ++t) {
+        double pr[ORC_TILE];
+        for (int l = 0; l < ORC_TILE; ++l) {
+            const long long i = (long long)t * ORC_TILE + l;
+            pr[l] = i < c->n ? v[i] : 0.0;
+        }
+        c->part1[t] = tile_sum(pr);
+    }
+    return partials_sum(c->part1, c->nt1);
+}
+
+/* 32 x 32-cell tile partials of v (cells in row-major order within a tile,
+ * tiles row-major), summed as the GPU's partial slots. */
+static double fpo_sum2(fpo_ctx *c, const double *v) {
+    for (int t = 0; t < c->nt2; ++t) {
+        const int x0 = (t % c->tx2) * FPO_TILE, y0 = (t / c->tx2) * FPO_TILE;
+        double pr[ORC_TILE];
+        for (int ly = 0; ly < FPO_TILE; ++ly)
+            for (int lx = 0; lx < FPO_TILE; ++lx) {
+                const int gx = x0 + lx, gy = y0 + ly;
+                pr[ly * FPO_TILE + lx] = (gx < c->nx && gy < c->ny) ? v[(size_t)gy * c->nx + gx] : 0.0;
+            }
+        c->part2[t] = tile_sum(pr);
+    }
+    return partials_sum(c->part2, c->nt2);
+}
+
+/* `sweeps` damped Jacobi sweeps in FP32 on A z = r from z (in place). */
+static void fpo_sweeps(fpo_ctx *c, const float *r, float *z, float *tmp, int sweeps) {
+    for (int s = 0; s < sweeps; ++s) {
+        op_apply32(&c->A, z, tmp, 1);
+        for (int i = 0; i < c->n; ++i) tmp[i] = fmaf(c->wd[i], r[i] - tmp[i], z[i]);
+        memcpy(z, tmp, sizeof(float) * c->n);
+    }
+}
+
+typedef struct {
+    double ps[9], target, best_rr, gmax;
+    long long k, best_k;
+    int done, par, pending, updates;
+} fpo_state;
+
+int orc_fpcg2d(int nx, int ny, const double *we, const double *wn, const double *dg,
+               const double *b, int f, int smooth, int m, int mixed, double delta, int maxiter,
+               double tol, double *x, long long *iters, int *updates, int *done_out) {
+    if (nx < 1 || ny < 1 || !we || !wn || !dg || !b || !x || (f != 1 && f != 2) || nx % f ||
+        ny % f || smooth < 0 || smooth > 8 || m < 1 || m > 8 || maxiter < 1)
+        return 1;
+    fpo_ctx c;
+    memset(&c, 0, sizeof(c));
+    c.nx = nx; c.ny = ny; c.n = nx * ny; c.f = f; c.ncx = nx / f; c.nc = c.n / (f * f);
+    c.smooth = smooth; c.m = m; c.ring = m + 1; c.mixed = mixed;
+    c.we = we; c.wn = wn; c.dg = dg; c.b = b;
+    c.delta2 = delta * delta;
+    c.tx2 = (nx + FPO_TILE - 1) / FPO_TILE;
+    c.nt1 = (c.n + ORC_TILE - 1) / ORC_TILE;
+    c.nt2 = c.tx2 * ((ny + FPO_TILE - 1) / FPO_TILE);
+    const size_t n = (size_t)c.n;
+    stencil_op(&c.A, 2, nx, ny, 1, we, wn, NULL, dg);
+    c.A.we32 = to_f32(we, n);
+    c.A.wn32 = to_f32(wn, n);
+    c.A.dg32 = to_f32(dg, n);
+    c.wd = (float *)malloc(sizeof(float) * n);
+    for (size_t i = 0; i < n; ++i) c.wd[i] = (float)(FPO_OMEGA / (double)c.A.dg32[i]);
+    c.scr = (double *)malloc(sizeof(double) * n * 3);
+    c.part1 = (double *)malloc(sizeof(double) * c.nt1);
+    c.part2 = (double *)malloc(sizeof(double) * c.nt2);
+    double *r = (double *)calloc(n, sizeof(double)), *z = (double *)calloc(n, sizeof(double));
+    double *za = (double *)calloc(n, sizeof(double)), *r1 = (double *)calloc(n, sizeof(double));
+    double *pring = (double *)calloc(n * c.ring, sizeof(double));
+    double *sring = (double *)calloc(n * c.ring, sizeof(double));
+    float *r32 = (float *)calloc(n, sizeof(float)), *z32 = (float *)calloc(n, sizeof(float));
+    float *p32 = (float *)calloc(n * c.ring, sizeof(float)), *s32 = (float *)calloc(n * c.ring, sizeof(float));
+    float *d32[2] = {(float *)calloc(n, sizeof(float)), (float *)calloc(n, sizeof(float))};
+    double *xm[2] = {(double *)calloc(n, sizeof(double)), (double *)calloc(n, sizeof(double))};
+    float *rf = (float *)malloc(sizeof(float) * n), *zf = (float *)malloc(sizeof(float) * n);
+    float *tf = (float *)malloc(sizeof(float) * n), *yv = (float *)malloc(sizeof(float) * c.nc);
+    double *v1 = c.scr, *v2 = c.scr + n, *v3 = c.scr + 2 * n;
+    fpo_state S;
+    memset(&S, 0, sizeof(S));
+    double RR, BB, TT = 0.0, PR = 0.0;
+    double ZS[8];
+
+    /* init (k_fp_init / k_fpm_init) */
+    for (size_t i = 0; i < n; ++i) {
+        x[i] = 0.0;
+        v1[i] = b[i] * b[i];
+        if (mixed) {
+            r32[i] = (float)b[i];
+            v2[i] = (double)r32[i] * (double)r32[i];
+        } else {
+            r[i] = b[i];
+            v2[i] = v1[i];
+        }
+    }
+    BB = fpo_sum1(&c, v1);
+    RR = fpo_sum1(&c, v2);
+    S.best_rr = 1e300;
+    S.target = -tol;
+
+    int first = 1;
+    for (;;) {
+        if (!first) {
+            /* s = A p; <p, s> (k_fp_spmv / k_fpm_spmv) */
+            const int slot = (int)(S.k % c.ring);
+            double *p = pring + (size_t)slot * n, *sv = sring + (size_t)slot * n;
+            float *pf = p32 + (size_t)slot * n, *sf = s32 + (size_t)slot * n;
+            if (mixed) {
+                op_apply32(&c.A, pf, sf, 1);
+                for (size_t i = 0; i < n; ++i) v1[i] = (double)pf[i] * (double)sf[i];
+            } else {
+                op_apply(&c.A, p, sv, 1);
+                for (size_t i = 0; i < n; ++i) v1[i] = p[i] * sv[i];
+            }
+            const double ps = fpo_sum1(&c, v1);
+            /* alpha = <p, r> / <p, s>; updates (k_fp_update / k_fpm_update) */
+            const double alpha = ps != 0.0 ? PR / ps : 0.0;
+            if (mixed) {
+                const float af = (float)alpha;
+                float *d = d32[S.par];
+                for (size_t i = 0; i < n; ++i) {
+                    d[i] = fmaf(af, pf[i], d[i]);
+                    r32[i] = fmaf(-af, sf[i], r32[i]);
+                    v1[i] = (double)r32[i] * (double)r32[i];
+                }
+            } else {
+                for (size_t i = 0; i < n; ++i) {
+                    x[i] = fma(alpha, p[i], x[i]);
+                    r[i] = fma(-alpha, sv[i], r[i]);
+                    v1[i] = r[i] * r[i];
+                }
+            }
+            RR = fpo_sum1(&c, v1);
+            S.ps[slot] = ps;
+            /* reliable update (k_fpm_reliable) */
+            if (mixed && (RR <= S.target * S.target || RR < c.delta2 * S.gmax)) {
+                const double *xo = xm[S.par];
+                const float *d = d32[S.par];
+                for (size_t i = 0; i < n; ++i) v3[i] = xo[i] + (double)d[i];
+                op_apply(&c.A, v3, v2, 1);
+                for (size_t i = 0; i < n; ++i) {
+                    const double ti = b[i] - v2[i];
+                    r32[i] = (float)ti;
+                    xm[S.par ^ 1][i] = v3[i];
+                    d32[S.par ^ 1][i] = 0.f;
+                    v1[i] = ti * ti;
+                    v2[i] = (double)r32[i] * (double)r32[i];
+                }
+                TT = fpo_sum1(&c, v1);
+                RR = fpo_sum1(&c, v2);
+                S.pending = 1;
+            }
+        }
+        /* k_fp_pre: state, z0 = J(0), r1 = r - A z0, R r1 */
+        if (!first) S.k += 1;
+        if (S.target < 0) S.target = -S.target * sqrt(BB);
+        if (!mixed) {
+            if (sqrt(RR) <= S.target) S.done = 1;
+        } else if (S.pending) {
+            S.par ^= 1;
+            S.pending = 0;
+            S.updates += 1;
+            S.gmax = RR;
+            if (sqrt(TT) <= S.target) S.done = 1;
+        } else if (RR > S.gmax) {
+            S.gmax = RR;
+        }
+        if (RR < S.best_rr) {
+            S.best_rr = RR;
+            S.best_k = S.k;
+        } else if (S.k - S.best_k > FPO_STALL) {
+            S.done = 2;
+        }
+        if (S.k >= maxiter && !S.done) S.done = 2;
+        for (size_t i = 0; i < n; ++i) {
+            rf[i] = mixed ? r32[i] : (float)r[i];
+            zf[i] = smooth > 0 ? c.wd[i] * rf[i] : 0.f;
+        }
+        if (smooth > 1) fpo_sweeps(&c, rf, zf, tf, smooth - 1);
+        op_apply32(&c.A, zf, tf, 1);
+        for (size_t i = 0; i < n; ++i) {
+            r1[i] = (double)(rf[i] - tf[i]);
+            za[i] = (double)zf[i];
+        }
+        for (int ic = 0; ic < c.nc; ++ic) {  /* R r1 (the identity in place of the network) */
+            const int cx = ic % c.ncx, cy = ic / c.ncx;
+            double sum = 0;
+            for (int dy = 0; dy < f; ++dy)
+                for (int dx = 0; dx < f; ++dx) sum += r1[(size_t)(cy * f + dy) * nx + cx * f + dx];
+            yv[ic] = (float)(sum / (f * f));
+        }
+        /* k_fp_ydots: <P y, r1>, <P y, A P y> */
+        for (int i = 0; i < c.n; ++i) {
+            const int ix = i % nx, iy = i / nx, cx = ix / f, cy = iy / f;
+            const double zi = (double)yv[cy * c.ncx + cx];
+            double t = dg[i] * zi;
+            if (ix > 0) t = fma(-we[i - 1], (double)yv[cy * c.ncx + (ix - 1) / f], t);
+            if (ix < nx - 1) t = fma(-we[i], (double)yv[cy * c.ncx + (ix + 1) / f], t);
+            if (iy > 0) t = fma(-wn[i - nx], (double)yv[((iy - 1) / f) * c.ncx + cx], t);
+            if (iy < ny - 1) t = fma(-wn[i], (double)yv[((iy + 1) / f) * c.ncx + cx], t);
+            v1[i] = zi * r1[i];
+            v2[i] = zi * t;
+        }
+        const double yr = fpo_sum1(&c, v1), yay = fpo_sum1(&c, v2);
+        /* k_fp_post: z = J(z0 + c P y); <z, s_j> */
+        const double cc = yay > 0 ? yr / yay : 0.0;
+        for (int i = 0; i < c.n; ++i) {
+            const int ix = i % nx, iy = i / nx;
+            const double yi = (double)yv[(iy / f) * c.ncx + ix / f];
+            zf[i] = (float)(cc != 0.0 ? fma(cc, yi, za[i]) : za[i]);
+        }
+        fpo_sweeps(&c, rf, zf, tf, smooth);
+        for (size_t i = 0; i < n; ++i) {
+            z[i] = (double)zf[i];
+            z32[i] = zf[i];
+        }
+        const int k = (int)S.k, nj = k < m ? k : m;
+        for (int j = 0; j < nj; ++j) {
+            const size_t off = (size_t)((k - 1 - j) % c.ring) * n;
+            for (size_t i = 0; i < n; ++i)
+                v1[i] = mixed ? (double)z32[i] * (double)s32[off + i] : z[i] * sring[off + i];
+            ZS[j] = fpo_sum2(&c, v1);
+        }
+        /* k_fp_dir: p_k = z - sum_j beta_j p_{k-1-j}; <p, r> */
+        double beta[8];
+        for (int j = 0; j < nj; ++j) {
+            const double ps = S.ps[(k - 1 - j) % c.ring];
+            beta[j] = ps != 0.0 ? ZS[j] / ps : 0.0;
+        }
+        const size_t out = (size_t)(k % c.ring) * n;
+        for (size_t i = 0; i < n; ++i) {
+            if (mixed) {
+                float pi = z32[i];
+                for (int j = 0; j < nj; ++j)
+                    pi = fmaf(-(float)beta[j], p32[(size_t)((k - 1 - j) % c.ring) * n + i], pi);
+                p32[out + i] = pi;
+                v1[i] = (double)pi * (double)r32[i];
+            } else {
+                double pi = z[i];
+                for (int j = 0; j < nj; ++j) pi = fma(-beta[j], pring[(size_t)((k - 1 - j) % c.ring) * n + i], pi);
+                pring[out + i] = pi;
+                v1[i] = pi * r[i];
+            }
+        }
+        PR = fpo_sum1(&c, v1);
+        if (!first && S.done) break;
+        first = 0;
+    }
+    if (mixed)
+        for (size_t i = 0; i < n; ++i) x[i] = xm[S.par][i] + (double)d32[S.par][i];
+    if (iters) *iters = S.k;
+    if (updates) *updates = S.updates;
+    if (done_out) *done_out = S.done;
+    free(c.A.we32); free(c.A.wn32); free(c.A.dg32); free(c.wd); free(c.scr); free(c.part1);
+    free(c.part2); free(r); free(z); free(za); free(r1); free(pring); free(sring); free(r32);
+    free(z32); free(p32); free(s32); free(d32[0]); free(d32[1]); free(xm[0]); free(xm[1]);
+    free(rf); free(zf); free(tf); free(yv);
+    return 0;
+}

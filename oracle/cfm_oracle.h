@@ -85,6 +85,18 @@ int orc_krylov_stencil(int dims, int nx, int ny, int nz, const double *we, const
                        int maxiter, double tol, int inner_maxiter, double inner_tol, double *x,
                        long long *iters, int *restarts, double *relres, int threads);
 
+/* Flexible PCG on the 2D variable-coefficient stencil (the learned-
+ * preconditioner solver's device loop, csrc/fpcg.cu) with the identity in
+ * place of the network: truncated FCG(m), z = J(z0 + c P R r1) with `smooth`
+ * FP32 Jacobi sweeps and f x f coarse cells (f = 1 or 2); FP64 Krylov
+ * vectors (mixed = 0) or FP32 ones with FP64 reliable updates at residual
+ * drop `delta` (mixed = 1).  x0 = 0.  Returns 0 / 1 bad arguments; iters,
+ * updates (FP64 reliable updates) and done (1 converged, 2 stalled / capped)
+ * optional. */
+int orc_fpcg2d(int nx, int ny, const double *we, const double *wn, const double *dg,
+               const double *b, int f, int smooth, int m, int mixed, double delta, int maxiter,
+               double tol, double *x, long long *iters, int *updates, int *done);
+
 int orc_max_threads(void);
 
 #ifdef __cplusplus

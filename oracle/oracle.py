@@ -49,6 +49,9 @@ def _load():
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = ctypes.c_int
+    lib.orc_fpcg2d.argtypes = [_i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _i, ctypes.c_double, _i,
+                               ctypes.c_double, _vp, _vp, _vp, _vp]
+    lib.orc_fpcg2d.restype = _i
     lib.orc_dot.argtypes = [ctypes.c_longlong, _vp, _vp, _i]
     lib.orc_dot.restype = ctypes.c_double
     lib.orc_jacobi3d_bench_f64.argtypes = [_i, _i, _i, _i, _i]
@@ -194,6 +197,20 @@ def krylov_stencil(dims, shape, c, b, method, maxiter, tol, inner_maxiter=0, inn
                                 inner_tol, _p(x), ctypes.byref(it), ctypes.byref(rs),
                                 ctypes.byref(rr), threads)
     return x, st, it.value, rs.value, rr.value
+
+
+def fpcg2d(shape, c, b, smooth, m, mixed=False, delta=0.1, maxiter=20000, tol=1e-8, f=1):
+    """FPCG restatement (identity in place of the network) on the 2D stencil
+    with coefficients c = (we, wn, wt, dg).  Returns (x, iterations,
+    reliable updates, done)."""
+    we, wn, _, dg = _coeffs(c)
+    nx, ny = shape
+    bb = np.ascontiguousarray(b, np.float64).reshape(-1)
+    x = np.empty(nx * ny)
+    it, up, dn = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+    assert lib.orc_fpcg2d(nx, ny, _p(we), _p(wn), _p(dg), _p(bb), f, smooth, m, int(mixed), delta,
+                          maxiter, tol, _p(x), ctypes.byref(it), ctypes.byref(up), ctypes.byref(dn)) == 0
+    return x, it.value, up.value, dn.value
 
 
 # ------------------------------------------------------ the reference itself

@@ -262,3 +262,41 @@ def test_oracle_mixed_independent_of_threads():
             for t in (1, 3)]
     np.testing.assert_array_equal(runs[0][0], runs[1][0])
     assert runs[0][1:4] == runs[1][1:4]
+
+
+# ------------------------------------------------------------------ FPCG
+def test_oracle_fpcg_restatement_converges_and_mixed_keeps_the_count():
+    """The FPCG restatement (identity in place of the network) reaches 1e-8
+    and agrees with plain CG's solution; its mixed form (FP32 Krylov
+    vectors, FP64 reliable updates) takes about the FP64 form's iterations
+    and as accurate a solution."""
+    import cfm
+    for shape, seed in (((96, 64), 3), ((60, 100), 4)):
+        ny, nx = shape
+        k, f = cfm.varcoef_problem(shape, seed)
+        c = cfm.varcoef_coeffs(k)
+        xs, st, its, _, _ = oracle.krylov_stencil(2, (nx, ny, 1), c, f.ravel(), 0, 50000, 1e-11)
+        assert st == 0
+        x64, it64, up64, d64 = oracle.fpcg2d((nx, ny), c, f, 4, 1, False)
+        x32, it32, up32, d32 = oracle.fpcg2d((nx, ny), c, f, 4, 1, True)
+        assert d64 == d32 == 1 and up64 == 0 and up32 >= 1
+        assert it64 < 0.25 * its  # smoothing + coarse correction beat plain CG
+        assert abs(it32 - it64) <= max(2, 0.1 * it64)
+        for x in (x64, x32):
+            assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-6
+            r = f.ravel() - oracle.stencil_apply(2, (nx, ny, 1), c, x)
+            assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(f)
+
+
+def test_oracle_fpcg_truncation_and_bad_arguments():
+    import cfm
+    k, f = cfm.varcoef_problem((64, 64), 5)
+    c = cfm.varcoef_coeffs(k)
+    _, it1, _, _ = oracle.fpcg2d((64, 64), c, f, 2, 1, False)
+    _, it8, _, _ = oracle.fpcg2d((64, 64), c, f, 2, 8, False)
+    assert it8 <= it1 + 2  # a linear preconditioner: FCG(8) ~ the one-term recurrence
+    we, wn, _, dg = (np.ascontiguousarray(a, np.float64) for a in c)
+    x = np.empty(64 * 64)
+    p = oracle._p
+    assert oracle.lib.orc_fpcg2d(64, 64, p(we), p(wn), p(dg), p(np.ascontiguousarray(f.ravel())), 3, 2, 1,
+                                 0, 0.1, 100, 1e-8, p(x), None, None, None) == 1  # f must be 1 or 2
