@@ -503,16 +503,80 @@ def workload_batch256(args, cfm):
         t_plain += sp.seconds
         it_plain.append(sp.iterations)
     n = len(systems)
+    learned = batch_learned(args, cfm, systems, methods["pcg_fp32_fp64_reliable_updates_delta0.1"], smooth)
+    if learned.get("ms") and learned["ms"] < methods[best]["ms"]:
+        best, t = "learned_split", learned["ms"] * 1e-3
     line("256 uneven variable-coefficient systems to 1e-8: aggregate solves/s", n / t, "solves/s", args,
          t * 1e3, {"workload": "batch_192x2d_64..512_64x3d_32..128_varcoef_tol1e-8",
                    "systems": n, "cells": int(sum(k.size for k, _ in systems)),
-                   "method": best, "methods": methods,
+                   "method": best, "methods": methods, "learned": learned,
                    "iterations_plain": {"min": int(min(it_plain)), "median": float(np.median(it_plain)),
                                         "max": int(max(it_plain))},
                    "plain_one_solve_per_launch_ms": t_plain * 1e3,
                    "speedup_vs_one_plain_solve_per_launch": t_plain / t,
                    "generation_s": gen_s, "peak_hbm_gbs": peak, "peak_kind": kind,
                    "launch": "one cooperative launch in a CUDA graph per step; 4 damped-Jacobi sweeps"})
+
+
+def batch_learned(args, cfm, systems, poly, smooth, side_min=256):
+    """Config 5 with the learned preconditioner: the network of config 4
+    (trained here on 100 fresh 512^2 systems, its 256^2 grid x 2) solves the
+    2D members of side >= side_min together in one FPCG device loop (each
+    member in the 512^2 frame, learned + mixed precision, the network at
+    batch up to 64), the other members (smaller 2D, all 3D) run in the
+    persistent Jacobi-polynomial mixed-precision kernel; both back to back on
+    one stream, timed together."""
+    import numpy as np
+    N2 = 512
+    big = [i for i, (k, _) in enumerate(systems) if k.ndim == 2 and min(k.shape) >= side_min]
+    rest = [i for i in range(len(systems)) if i not in big]
+    net = cfm.UNet(N2 // 2, N2 // 2, max_batch=64, seed=7)
+    net.set_validation(1000, 1)
+    t0 = time.perf_counter()
+    info = net.train_varcoef(100, 19, 1000, 16, 8, 1e-3, smooth=smooth, coarsen=2)
+    info["wall_s"] = time.perf_counter() - t0
+    info["kept_epoch"], info["validation_ms"] = net.validation()
+    FB = cfm.FPCGBatch([systems[i][0] for i in big], net, maxiter=20000, tol=1e-8, precision=cfm.FP32)
+    fb = [systems[i][1] for i in big]
+    B = cfm.Batch([systems[i] for i in rest])
+    B.set_solver(smooth=smooth, maxiter=20000, tol=1e-8)
+    B.set_precision(cfm.FP32, 0, 0.1)
+    B.autotune()
+    for _ in range(args.warmup):
+        FB.solve(fb)
+        B.solve()
+    ts, tl, tp = [], [], []
+    for _ in range(args.steps):
+        _, it_l, st_l, rr_l, sl = FB.solve(fb)
+        it_p, st_p, rr_p, sp = B.solve()
+        tl.append(sl.seconds)
+        tp.append(sp.seconds)
+        ts.append(sl.seconds + sp.seconds)
+    t = statistics.median(ts)
+    poly_it = poly["per_system_iterations"]
+    it_all = [0] * len(systems)
+    for j, i in enumerate(big):
+        it_all[i] = int(it_l[j])
+    for j, i in enumerate(rest):
+        it_all[i] = int(it_p[j])
+    out = {"ms": t * 1e3, "solves_per_s": len(systems) / t,
+           "learned_members": len(big), "polynomial_members": len(rest), "side_min": side_min,
+           "learned_ms": statistics.median(tl), "polynomial_ms": statistics.median(tp),
+           "all_converged": bool((st_l == cfm.OK).all() and (st_p == cfm.OK).all()),
+           "max_true_relres": float(max(rr_l.max(), rr_p.max())),
+           "learned_iterations": [int(v) for v in it_l],
+           "same_members_polynomial_iterations": [int(poly_it[i]) for i in big],
+           "learned_over_polynomial_iterations": float(np.sum(it_l) / max(1, sum(poly_it[i] for i in big))),
+           "reliable_updates_learned": FB.reliable_updates(), "per_system_iterations": it_all,
+           "training": info, "network_batch": 64,
+           "precision": "learned members: FP32 Krylov vectors + FP64 reliable updates, BF16 network; "
+                        "others: FP32 PCG + FP64 reliable updates"}
+    out["learned_ms"] *= 1e3
+    out["polynomial_ms"] *= 1e3
+    FB.close()
+    B.close()
+    net.close()
+    return out
 
 
 def main_workload(args):

@@ -90,6 +90,8 @@ _SIGS = {
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
     "cfm_fpcg_set_precision": (_c.c_int, [_vp, _c.c_int, _c.c_double]),
     "cfm_fpcg_reliable_updates": (_c.c_int, [_vp]),
+    "cfm_fpcg_create_batch": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
+    "cfm_fpcg_solve_batch": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cfm_batch_create": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "cfm_batch_destroy": (None, [_vp]),
     "cfm_batch_set_plan": (_c.c_int, [_vp, _c.c_int, _vp, _vp]),
@@ -632,6 +634,50 @@ class FPCG:
         st = Stats()
         check("cfm_fpcg_solve", lib.cfm_fpcg_solve(self.h, _ptr(b), _ptr(x), ctypes.byref(st)), allowed)
         return x, st
+
+
+class FPCGBatch(FPCG):
+    """A batch of 2D systems [(k, b) or k] solved together by the FPCG device
+    loop (cfm_fpcg_create_batch): each member embedded in the network's frame
+    (or, without a network, the largest member's), its own scalars and stop."""
+
+    def __init__(self, ks, net, maxiter=5000, tol=1e-8, smooth=None, truncation=None, net_period=None,
+                 precision=None, delta=0.1):
+        self.net, self.maxiter = net, maxiter
+        self.ks = [np.ascontiguousarray(k, np.float64) for k in ks]
+        self.shapes = [k.shape for k in self.ks]
+        nx = np.array([sh[1] for sh in self.shapes], np.int32)
+        ny = np.array([sh[0] for sh in self.shapes], np.int32)
+        kp = (ctypes.c_void_p * len(self.ks))(*[k.ctypes.data for k in self.ks])
+        if smooth is None:
+            smooth = getattr(net, "smooth", 0) if net is not None else 0
+        h = ctypes.c_void_p()
+        check("cfm_fpcg_create_batch", lib.cfm_fpcg_create_batch(len(self.ks), _ptr(nx), _ptr(ny), kp,
+                                                                 None if net is None else net.h, smooth,
+                                                                 maxiter, tol, ctypes.byref(h)))
+        self.h = h
+        if truncation is not None:
+            check("cfm_fpcg_set_truncation", lib.cfm_fpcg_set_truncation(self.h, truncation))
+        if net_period is not None:
+            check("cfm_fpcg_set_network_period", lib.cfm_fpcg_set_network_period(self.h, net_period))
+        if precision is not None:
+            self.set_precision(precision, delta)
+
+    def solve(self, bs, allowed=(OK, NOT_CONVERGED)):
+        """bs: one right-hand side per member (its shape).  Returns (xs,
+        iterations, status, true relative residuals, stats)."""
+        M = len(self.ks)
+        bs = [np.ascontiguousarray(b, np.float64).reshape(sh) for b, sh in zip(bs, self.shapes)]
+        xs = [np.empty(sh) for sh in self.shapes]
+        bp = (ctypes.c_void_p * M)(*[b.ctypes.data for b in bs])
+        xp = (ctypes.c_void_p * M)(*[x.ctypes.data for x in xs])
+        it = np.empty(M, np.int64)
+        stt = np.empty(M, np.int32)
+        rr = np.empty(M)
+        st = Stats()
+        check("cfm_fpcg_solve_batch", lib.cfm_fpcg_solve_batch(self.h, bp, xp, _ptr(it), _ptr(stt), _ptr(rr),
+                                                               ctypes.byref(st)), allowed)
+        return xs, it, stt, rr, st
 
 
 class Batch:

@@ -339,7 +339,65 @@ struct FpArgs {
     float *r32, *z32, *pring32, *sring32;
     double *xm[2];
     float *dm[2];
+    // batches (cfm_fpcg_create_batch): member y = blockIdx.y of every launch
+    // works on its slice of each per-member array (n cells, the nx x ny
+    // frame; direction ring slots sstride = nmem n apart), and only cells
+    // inside its extent (mx, my from ext[y]) take the network's correction
+    int nmem;
+    long long sstride;
+    const int2 *ext;
+    int mx, my;
 };
+
+// Offsets every per-member pointer of `a` to member blockIdx.y (nothing for
+// member 0 and for a single system) and sets the member's extent.
+__device__ __forceinline__ void fp_member(FpArgs &a) {
+    const int y = blockIdx.y;
+    if (a.ext) {
+        a.mx = a.ext[y].x;
+        a.my = a.ext[y].y;
+    }
+    if (y == 0) return;
+    const size_t o = (size_t)y * a.n;
+    a.op.we += o;
+    a.op.wn += o;
+    a.op.dg += o;
+    a.op.we32 += o;
+    a.op.wn32 += o;
+    a.op.dg32 += o;
+    a.we32 += o;
+    a.wn32 += o;
+    a.dg32 += o;
+    a.wd32 += o;
+    a.b += o;
+    a.x += o;
+    a.r += o;
+    a.z += o;
+    a.za += o;
+    a.r1 += o;
+    a.pring += o;
+    a.sring += o;
+    a.xin += (size_t)y * 2 * a.nc;
+    a.out += (size_t)y * a.nc;
+    a.part += (size_t)y * FP_NSLOT * a.pstride;
+    a.st += y;
+    a.hist += (size_t)y * (a.maxiter + 1);
+    if (a.mixed) {
+        a.r32 += o;
+        a.z32 += o;
+        a.pring32 += o;
+        a.sring32 += o;
+        a.xm[0] += o;
+        a.xm[1] += o;
+        a.dm[0] += o;
+        a.dm[1] += o;
+    }
+}
+
+// In a batch, the kernels of a converged member return at once.
+#define FP_MEMBER(a)                                  \
+    fp_member(a);                                     \
+    if (a.nmem > 1 && a.st->done) return
 
 
 __device__ __forceinline__ double *fslot(const FpArgs &a, int s) { return a.part + (size_t)s * a.pstride; }
@@ -370,6 +428,7 @@ __device__ void block_sum_multi(double *v, int nv, double *sm) {
 
 // x = 0, r = b; partials |b|^2, |r|^2.
 __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
+    fp_member(a);
     __shared__ double sm[33];
     FP_ROW;
     double bb = 0;
@@ -496,6 +555,7 @@ __device__ float *fp_sweeps(const FpTile &t, const FpArgs &a, float *cur, float 
 // scales it by 1 / rms(r1) itself).
 __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int net_next) {
     pdl_enter();
+    FP_MEMBER(a);
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
     if (blockIdx.x == 0) {
@@ -581,6 +641,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
 // with the partials <z_k, s_{k-1-j}> (j < min(k, m)) of the orthogonalisation.
 __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
     pdl_enter();
+    FP_MEMBER(a);
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
     double c = 0.0;  // without the network's y this iteration: smoothing alone
@@ -596,9 +657,9 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
         const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
         t.z0()[row * t.R + col] =
             fp_inside(t, a, row, col, &i)
-                ? __double2float_rn(c != 0.0 ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)],
-                                                        a.za[i])
-                                             : a.za[i])
+                ? __double2float_rn(c != 0.0 && gx < a.mx && gy < a.my
+                                        ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)], a.za[i])
+                                        : a.za[i])
                 : 0.f;
     }
     __syncthreads();
@@ -618,7 +679,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
     if (nj > 0) {
         __shared__ double smm[33 * FP_MAX_TRUNC];
         __shared__ size_t sj[FP_MAX_TRUNC];  // ring slot offsets of s_{k-1-j}
-        if (threadIdx.x < nj) sj[threadIdx.x] = (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
+        if (threadIdx.x < nj) sj[threadIdx.x] = (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.sstride;
         __syncthreads();
         double v[FP_MAX_TRUNC];
 #pragma unroll
@@ -642,7 +703,8 @@ __global__ void k_fp_wd(const float *dg32, float *wd32, int n) {
 // Identity in place of the network: out = R(r1) (unscaled; c absorbs the scale).
 __global__ void k_fp_identity(FpArgs a) {
     pdl_enter();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x)
+    const long long nall = (long long)a.nc * a.nmem;  // every member's coarse cells, one after the other
+    for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < nall; i += gridDim.x * blockDim.x)
         a.out[i] = a.xin[2 * i];
 }
 
@@ -650,6 +712,7 @@ __global__ void k_fp_identity(FpArgs a) {
 // (FP32 values, applied in FP64).
 __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     FP_ROW;
     double yr = 0, yay = 0;
@@ -659,12 +722,17 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
         const int sh = a.fsh, cx = ix >> sh, cy = iy >> sh;
         const float *y = a.out;  // z = P y on this grid: z[j] = y[cell(j)]
         const float *yrow = y + cy * a.ncx;
-        const double zi = (double)yrow[cx];
+        // P y inside the member's extent (the whole grid for one system), 0 outside
+        const int mx = a.mx, my = a.my;
+        auto pv = [&](int jx, int jy) {
+            return (jx < mx && jy < my) ? (double)y[(jy >> sh) * a.ncx + (jx >> sh)] : 0.0;
+        };
+        const double zi = (ix < mx && iy < my) ? (double)yrow[cx] : 0.0;
         double t = __dmul_rn(o.dg[i], zi);
-        if (ix > 0) t = __fma_rn(-o.we[i - 1], (double)yrow[(ix - 1) >> sh], t);
-        if (ix < nx - 1) t = __fma_rn(-o.we[i], (double)yrow[(ix + 1) >> sh], t);
-        if (iy > 0) t = __fma_rn(-o.wn[i - nx], (double)y[((iy - 1) >> sh) * a.ncx + cx], t);
-        if (iy < o.ny - 1) t = __fma_rn(-o.wn[i], (double)y[((iy + 1) >> sh) * a.ncx + cx], t);
+        if (ix > 0) t = __fma_rn(-o.we[i - 1], pv(ix - 1, iy), t);
+        if (ix < nx - 1) t = __fma_rn(-o.we[i], pv(ix + 1, iy), t);
+        if (iy > 0) t = __fma_rn(-o.wn[i - nx], pv(ix, iy - 1), t);
+        if (iy < o.ny - 1) t = __fma_rn(-o.wn[i], pv(ix, iy + 1), t);
         yr = __dmul_rn(zi, a.r1[i]);
         yay = __dmul_rn(zi, t);
     }
@@ -682,11 +750,12 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
 __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond,
                                                     int set_cond) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const int k = (int)a.st->k;
     const int nj = min(a.m, k);
     __shared__ const double *pj[FP_MAX_TRUNC];
-    if (threadIdx.x < nj) pj[threadIdx.x] = a.pring + (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.n;
+    if (threadIdx.x < nj) pj[threadIdx.x] = a.pring + (size_t)((k - 1 - (int)threadIdx.x) % a.ring) * a.sstride;
     double beta[FP_MAX_TRUNC];
     if (nj > 0) {
         __shared__ double smm[33 * FP_MAX_TRUNC];
@@ -711,13 +780,13 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
             float pi = a.z32[i];
             for (int j = 0; j < nj; ++j)
                 pi = __fmaf_rn(-__double2float_rn(beta[j]),
-                               a.pring32[(size_t)((k - 1 - j) % a.ring) * a.n + i], pi);
-            a.pring32[(size_t)(k % a.ring) * a.n + i] = pi;
+                               a.pring32[(size_t)((k - 1 - j) % a.ring) * a.sstride + i], pi);
+            a.pring32[(size_t)(k % a.ring) * a.sstride + i] = pi;
             pr = xprod(pi, a.r32[i]);
         } else {
             double pi = a.z[i];
             for (int j = 0; j < nj; ++j) pi = __fma_rn(-beta[j], pj[j][i], pi);
-            a.pring[(size_t)(k % a.ring) * a.n + i] = pi;
+            a.pring[(size_t)(k % a.ring) * a.sstride + i] = pi;
             pr = __dmul_rn(pi, a.r[i]);
         }
     }
@@ -730,14 +799,15 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
 // s_k = A p_k; partial <p_k, s_k>.
 __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const int slot = (int)a.st->k % a.ring;
-    const double *p = a.pring + (size_t)slot * a.n;
+    const double *p = a.pring + (size_t)slot * a.sstride;
     FP_ROW;
     double ps = 0;
     if (i < a.n) {
         const double si = a.op.apply(p, i);
-        a.sring[(size_t)slot * a.n + i] = si;
+        a.sring[(size_t)slot * a.sstride + i] = si;
         ps = __dmul_rn(p[i], si);
     }
     ps = block_sum(ps, sm);
@@ -748,6 +818,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
 // <p_k, s_k> kept in the ring for the orthogonalisations to come.
 __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
@@ -756,8 +827,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
     FP_ROW;
     double rr = 0;
     if (i < a.n) {
-        a.x[i] = __fma_rn(alpha, a.pring[(size_t)slot * a.n + i], a.x[i]);
-        const double rn = __fma_rn(-alpha, a.sring[(size_t)slot * a.n + i], a.r[i]);
+        a.x[i] = __fma_rn(alpha, a.pring[(size_t)slot * a.sstride + i], a.x[i]);
+        const double rn = __fma_rn(-alpha, a.sring[(size_t)slot * a.sstride + i], a.r[i]);
         a.r[i] = rn;
         rr = __dmul_rn(rn, rn);
     }
@@ -770,6 +841,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
 // x = 0 (FP64 iterate and FP32 correction of parity 0), r32 = fl32(b);
 // partials |b|^2 (FP64) and |r32|^2.
 __global__ void __launch_bounds__(CG_TILE) k_fpm_init(FpArgs a, double tol) {
+    fp_member(a);
     __shared__ double sm[33];
     FP_ROW;
     double bb = 0, rr = 0;
@@ -806,14 +878,15 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_init(FpArgs a, double tol) {
 // exact FP32 products).
 __global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const int slot = (int)a.st->k % a.ring;
-    const float *p = a.pring32 + (size_t)slot * a.n;
+    const float *p = a.pring32 + (size_t)slot * a.sstride;
     FP_ROW;
     double ps = 0;
     if (i < a.n) {
         const float si = a.op.apply32(p, i);
-        a.sring32[(size_t)slot * a.n + i] = si;
+        a.sring32[(size_t)slot * a.sstride + i] = si;
         ps = xprod(p[i], si);
     }
     ps = block_sum(ps, sm);
@@ -824,6 +897,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
 // r32 -= alpha s (FP32); partial |r32|^2.
 __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
@@ -833,8 +907,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
     FP_ROW;
     double rr = 0;
     if (i < a.n) {
-        d[i] = __fmaf_rn(af, a.pring32[(size_t)slot * a.n + i], d[i]);
-        const float rn = __fmaf_rn(-af, a.sring32[(size_t)slot * a.n + i], a.r32[i]);
+        d[i] = __fmaf_rn(af, a.pring32[(size_t)slot * a.sstride + i], d[i]);
+        const float rn = __fmaf_rn(-af, a.sring32[(size_t)slot * a.sstride + i], a.r32[i]);
         a.r32[i] = rn;
         rr = xprod(rn, rn);
     }
@@ -852,6 +926,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
 // k_fp_pre flips the parity and judges convergence by |t|.
 __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
     pdl_enter();
+    FP_MEMBER(a);
     __shared__ double sm[33];
     const double g = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
     const FpState *st = a.st;
@@ -889,11 +964,45 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.st->pending = 1;
 }
 
-// The result of a mixed solve: x = xm + dm of the current parity (FP64).
+// The result of a mixed solve: x = xm + dm of the current parity (FP64), for
+// every member (each with its own parity).
 __global__ void k_fpm_finish(FpArgs a, const FpState *st) {
-    const int par = st->par;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+    const long long nall = (long long)a.n * a.nmem;
+    for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < nall; i += gridDim.x * blockDim.x) {
+        const int par = st[i / a.n].par;
         a.x[i] = __dadd_rn(a.xm[par][i], (double)a.dm[par][i]);
+    }
+}
+
+// Loop condition of a batch: go on while any member is not done.
+__global__ void k_fpb_cond(const FpState *st, int nmem, cudaGraphConditionalHandle cond) {
+    pdl_enter();
+    int open = 0;
+    for (int y = threadIdx.x; y < nmem; y += blockDim.x) open |= st[y].done == 0;
+    open = __any_sync(0xffffffffu, open);
+    if (threadIdx.x == 0) cudaGraphSetConditional(cond, open ? 1u : 0u);
+}
+
+// Per-member FP64 true residual t = b - A x, |t|^2 into acc[y] (grid sums in
+// block order: slots of gridDim.x doubles and one counter per member).
+__global__ void k_fpb_true_res(FpArgs a, double *t, double *acc, double *slots, unsigned int *count) {
+    fp_member(a);
+    const int y = blockIdx.y;
+    t += (size_t)y * a.n;
+    __shared__ double red[32];
+    double q = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const double ti = a.b[i] - a.op.apply(a.x, i);
+        t[i] = ti;
+        q += ti * ti;
+    }
+    for (int o = 16; o; o >>= 1) q += __shfl_xor_sync(CG_FULL, q, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = q;
+    __syncthreads();
+    double v = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) v += red[w];
+    ordered_grid_sum<1>(&v, slots + (size_t)y * gridDim.x, blockIdx.x, gridDim.x, count + y, acc + y, false);
 }
 
 // t = b - A x, |t|^2 into acc[0] (the judged true residual; grid sum in
@@ -970,27 +1079,49 @@ struct cfm_fpcg {
     float *vec32 = nullptr, *ring32 = nullptr;
     double *xm = nullptr;
     int last_updates = 0;
+    // a batch (cfm_fpcg_create_batch): nmem members, each embedded in the
+    // nx x ny frame; every per-member array holds nmem slices of n (vector
+    // k of FP_NVEC at k n nmem), the coefficients we | wn | wt | dg likewise
+    int nmem = 1;
+    double *c64b = nullptr;
+    float *c32b = nullptr;
+    int2 *ext = nullptr;         // member extents (device)
+    double *cells = nullptr;     // member cell counts (device; the network's input scale)
+    std::vector<int2> ext_h;
 };
 
 namespace {
 
 FpArgs fp_args(cfm_fpcg *h) {
     FpArgs a{};
-    const size_t n = h->n;
-    a.op = op2(h->S);
+    const size_t n = h->n, N = n * h->nmem;  // N: one vector of every member
+    const double *c64 = h->c64b ? h->c64b : stencil_coeffs(h->S);    // we | wn | wt | dg
+    const float *c32 = h->c32b ? h->c32b : stencil_coeffs32(h->S);
+    a.op.nx = h->nx;
+    a.op.ny = h->ny;
+    a.op.nz = 1;
+    a.op.we = c64;
+    a.op.wn = c64 + N;
+    a.op.wt = c64 + 2 * N;
+    a.op.dg = c64 + 3 * N;
     a.n = h->n;
     a.ntiles = h->ntiles;
     a.x = h->vec;
-    a.r = h->vec + n;
-    a.z = h->vec + 2 * n;
-    a.b = h->vec + 3 * n;
-    a.za = h->vec + 6 * n;
-    a.r1 = h->vec + 7 * n;
+    a.r = h->vec + N;
+    a.z = h->vec + 2 * N;
+    a.b = h->vec + 3 * N;
+    a.za = h->vec + 6 * N;
+    a.r1 = h->vec + 7 * N;
     static_assert(FP_NVEC == 8, "x r z b t d za r1");
     a.m = h->m;
     a.ring = h->m + 1;
     a.pring = h->ring;
-    a.sring = h->ring + (size_t)(h->m + 1) * n;
+    a.sring = h->ring + (size_t)(h->m + 1) * N;
+    a.nmem = h->nmem;
+    a.sstride = (long long)N;
+    a.ext = h->ext;
+    a.mx = h->nx;
+    a.my = h->ny;
     a.xin = h->xin;
     a.out = h->out;
     a.part = h->part;
@@ -1003,17 +1134,14 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.ncx = h->nx / h->coarsen;
     a.nc = h->nc;
     a.ntiles2 = h->ntiles2;
-    {
-        const float *c32 = stencil_coeffs32(h->S);  // we | wn | wt | dg
-        a.we32 = c32;
-        a.wn32 = c32 + n;
-        a.dg32 = c32 + 3 * n;
-        a.wd32 = h->wd32;
-        a.op.we32 = c32;  // the operator's FP32 apply (mixed precision)
-        a.op.wn32 = c32 + n;
-        a.op.wt32 = c32 + 2 * n;
-        a.op.dg32 = c32 + 3 * n;
-    }
+    a.we32 = c32;
+    a.wn32 = c32 + N;
+    a.dg32 = c32 + 3 * N;
+    a.wd32 = h->wd32;
+    a.op.we32 = c32;  // the operator's FP32 apply (mixed precision)
+    a.op.wn32 = c32 + N;
+    a.op.wt32 = c32 + 2 * N;
+    a.op.dg32 = c32 + 3 * N;
     a.tx2 = h->tx2;
     a.pstride = h->pstride;
     a.smooth = h->smooth;
@@ -1021,13 +1149,13 @@ FpArgs fp_args(cfm_fpcg *h) {
     a.delta2 = h->delta * h->delta;
     if (h->mixed) {
         a.r32 = h->vec32;
-        a.z32 = h->vec32 + n;
-        a.dm[0] = h->vec32 + 2 * n;
-        a.dm[1] = h->vec32 + 3 * n;
+        a.z32 = h->vec32 + N;
+        a.dm[0] = h->vec32 + 2 * N;
+        a.dm[1] = h->vec32 + 3 * N;
         a.pring32 = h->ring32;
-        a.sring32 = h->ring32 + (size_t)(h->m + 1) * n;
+        a.sring32 = h->ring32 + (size_t)(h->m + 1) * N;
         a.xm[0] = h->xm;
-        a.xm[1] = h->xm + n;
+        a.xm[1] = h->xm + N;
     }
     return a;
 }
@@ -1042,35 +1170,46 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
                    bool use_net = true) {
     cudaStream_t s = h->stream;
     const int net_next = !(h->net && !use_net);
-    CFM_CUDA_TRY(launch_pdl(k_fp_pre, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(std::max(h->smooth, 1)), s,
-                            a, tick, net_next));
+    const int M = h->nmem;
+    CFM_CUDA_TRY(launch_pdl(k_fp_pre, dim3(h->ntiles2, M), dim3(CG_TILE), fp_smem_bytes(std::max(h->smooth, 1)),
+                            s, a, tick, net_next));
     if (!net_next) {
         // smoothing alone this iteration: no r1, no network, c = 0
-        CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 0));
-        CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
+        CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2, M), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 0));
+        CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles, M), dim3(CG_TILE), 0, s, a, cond, set_cond));
         return CFM_OK;
     }
     if (h->net) {
-        const UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride, h->ntiles2, (double)h->n};
-        int st = unet_forward(h->net->u, 1, h->xin, h->out, s, &sc);
-        if (st) return st;
+        // the members in chunks of the network's largest batch; image z of a
+        // chunk scales its input by its own member's |r1| partials and cells
+        const long long mstride = (long long)FP_NSLOT * a.pstride;
+        for (int m0 = 0; m0 < M; m0 += h->net->maxB) {
+            const int B = std::min(h->net->maxB, M - m0);
+            UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride + (size_t)m0 * mstride, h->ntiles2, (double)h->n};
+            sc.part_stride = mstride;
+            sc.cells_img = h->cells ? h->cells + m0 : nullptr;
+            int st = unet_forward(h->net->u, B, h->xin + (size_t)m0 * 2 * h->nc, h->out + (size_t)m0 * h->nc, s,
+                                  &sc);
+            if (st) return st;
+        }
     } else {
         CFM_CUDA_TRY(launch_pdl(k_fp_identity, dim3(256), dim3(256), 0, s, a));
     }
-    CFM_CUDA_TRY(launch_pdl(k_fp_ydots, dim3(h->ntiles), dim3(CG_TILE), 0, s, a));
-    CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 1));
-    CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles), dim3(CG_TILE), 0, s, a, cond, set_cond));
+    CFM_CUDA_TRY(launch_pdl(k_fp_ydots, dim3(h->ntiles, M), dim3(CG_TILE), 0, s, a));
+    CFM_CUDA_TRY(launch_pdl(k_fp_post, dim3(h->ntiles2, M), dim3(CG_TILE), fp_smem_bytes(h->smooth), s, a, 1));
+    CFM_CUDA_TRY(launch_pdl(k_fp_dir, dim3(h->ntiles, M), dim3(CG_TILE), 0, s, a, cond, set_cond));
     return CFM_OK;
 }
 
 int fp_iteration(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, bool use_net) {
+    const dim3 g(h->ntiles, h->nmem);
     if (h->mixed) {
-        CFM_CUDA_TRY(launch_pdl(k_fpm_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-        CFM_CUDA_TRY(launch_pdl(k_fpm_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-        CFM_CUDA_TRY(launch_pdl(k_fpm_reliable, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fpm_spmv, g, dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fpm_update, g, dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fpm_reliable, g, dim3(CG_TILE), 0, h->stream, a));
     } else {
-        CFM_CUDA_TRY(launch_pdl(k_fp_spmv, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
-        CFM_CUDA_TRY(launch_pdl(k_fp_update, dim3(h->ntiles), dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fp_spmv, g, dim3(CG_TILE), 0, h->stream, a));
+        CFM_CUDA_TRY(launch_pdl(k_fp_update, g, dim3(CG_TILE), 0, h->stream, a));
     }
     return fp_precond_dir(h, a, cond, set_cond, 1, use_net);
 }
@@ -1088,7 +1227,7 @@ void drop_graph(cfm_fpcg *h) {
 // FP32 rings of the mixed solve for truncation m.
 int alloc_ring32(cfm_fpcg *h, int m) {
     float *r = nullptr;
-    CFM_CUDA_TRY(cudaMalloc(&r, sizeof(float) * 2 * (m + 1) * (size_t)h->n));
+    CFM_CUDA_TRY(cudaMalloc(&r, sizeof(float) * 2 * (m + 1) * (size_t)h->n * h->nmem));
     cudaFree(h->ring32);
     h->ring32 = r;
     return CFM_OK;
@@ -1098,10 +1237,13 @@ int alloc_ring32(cfm_fpcg *h, int m) {
 // first (a converged system may take up to net_every - 1 extra iterations,
 // which only lower its residual further).
 int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    const bool batch = h->nmem > 1;
     for (int j = 0; j < h->net_every; ++j) {
-        const int st = fp_iteration(h, a, cond, set_cond && j == h->net_every - 1, j == 0);
+        const int st = fp_iteration(h, a, cond, set_cond && !batch && j == h->net_every - 1, j == 0);
         if (st) return st;
     }
+    if (set_cond && batch)  // a batch goes on while any member is open
+        CFM_CUDA_TRY(launch_pdl(k_fpb_cond, dim3(1), dim3(32), 0, h->stream, (const FpState *)h->st, h->nmem, cond));
     return CFM_OK;
 }
 
@@ -1151,6 +1293,68 @@ int build_graph(cfm_fpcg *h) {
 
 extern "C" {
 
+}  // extern "C"
+
+namespace {
+
+// Handle fields and device buffers of `nmem` systems on an nx x ny grid
+// (frame); the coefficients, omega / dg and the network's log k channel are
+// set by the caller.
+int fp_setup(cfm_fpcg *h, int nx, int ny, int f, cfm_unet *net, int smooth, int maxiter, double tol,
+             int nmem) {
+    h->coarsen = f;
+    h->nc = (nx / f) * (ny / f);
+    h->smooth = smooth;
+    h->net = net;
+    h->nx = nx;
+    h->ny = ny;
+    h->n = nx * ny;
+    h->nmem = nmem;
+    h->ntiles = (h->n + CG_TILE - 1) / CG_TILE;
+    h->tx2 = (nx + FP_TILE - 1) / FP_TILE;
+    h->ntiles2 = h->tx2 * ((ny + FP_TILE - 1) / FP_TILE);
+    h->pstride = std::max(h->ntiles, h->ntiles2);
+    h->maxiter = maxiter;
+    h->tol = tol;
+    const size_t N = (size_t)h->n * nmem;
+    // a linear SPD preconditioner (Jacobi alone) needs no more than the
+    // one-term recurrence; the network's nonlinear one gains from a deeper one
+    h->m = net ? FP_MAX_TRUNC : 1;
+    h->net_every = net ? 2 : 1;  // network every other iteration (smoothing alone in between)
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * N)) != cudaSuccess ||
+        (e = cudaMalloc(&h->ring, sizeof(double) * 2 * (h->m + 1) * N)) != cudaSuccess ||
+        (e = cudaMalloc(&h->wd32, sizeof(float) * N)) != cudaSuccess ||
+        (e = cudaMalloc(&h->xin, sizeof(float) * 2 * (size_t)h->nc * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->out, sizeof(float) * (size_t)h->nc * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * (size_t)h->pstride * nmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
+        (e = cudaMalloc(&h->acc, sizeof(double) * std::max(4, nmem))) != cudaSuccess ||
+        (e = cudaMalloc(&h->rslots, sizeof(double) * FP_RES_BLOCKS * (size_t)nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->rcount, sizeof(unsigned int) * nmem)) != cudaSuccess ||
+        (e = cudaMemset(h->rcount, 0, sizeof(unsigned int) * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->st, sizeof(FpState) * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1) * (size_t)nmem)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("FPCG buffers: %s", cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+    }
+    return CFM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, int smooth,
                     int maxiter, double tol, cfm_fpcg **out) {
     clear_error();
@@ -1170,52 +1374,17 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
         CFM_ARG_CHECK(smooth == net->smooth, "smooth must equal the sweeps the network was trained with");
     }
     cfm_fpcg *h = new cfm_fpcg();
-    h->coarsen = f;
-    h->nc = (nx / f) * (ny / f);
-    h->smooth = smooth;
     h->S = S;
-    h->net = net;
-    h->nx = nx;
-    h->ny = ny;
-    h->n = nx * ny;
-    h->ntiles = (h->n + CG_TILE - 1) / CG_TILE;
-    h->tx2 = (nx + FP_TILE - 1) / FP_TILE;
-    h->ntiles2 = h->tx2 * ((ny + FP_TILE - 1) / FP_TILE);
-    h->pstride = std::max(h->ntiles, h->ntiles2);
-    h->maxiter = maxiter;
-    h->tol = tol;
+    int st = fp_setup(h, nx, ny, f, net, smooth, maxiter, tol, 1);
+    if (st) {
+        cfm_fpcg_destroy(h);
+        return st;
+    }
     const size_t n = h->n;
-    cudaError_t e;
-    std::vector<double> kk(k_host, k_host + n);
     double *kd = nullptr;
-    // a linear SPD preconditioner (Jacobi alone) needs no more than the
-    // one-term recurrence; the network's nonlinear one gains from a deeper one
-    h->m = net ? FP_MAX_TRUNC : 1;
-    h->net_every = net ? 2 : 1;  // network every other iteration (smoothing alone in between)
-    if ((e = cudaMalloc(&h->vec, sizeof(double) * FP_NVEC * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->ring, sizeof(double) * 2 * (h->m + 1) * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->wd32, sizeof(float) * n)) != cudaSuccess ||
-        (e = cudaMalloc(&h->xin, sizeof(float) * 2 * h->nc)) != cudaSuccess ||
-        (e = cudaMalloc(&h->out, sizeof(float) * h->nc)) != cudaSuccess ||
-        (e = cudaMalloc(&h->part, sizeof(double) * FP_NSLOT * h->pstride)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_fp_pre, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_fp_post, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
-        (e = cudaMalloc(&h->acc, sizeof(double) * 4)) != cudaSuccess ||
-        (e = cudaMalloc(&h->rslots, sizeof(double) * FP_RES_BLOCKS)) != cudaSuccess ||
-        (e = cudaMalloc(&h->rcount, sizeof(unsigned int))) != cudaSuccess ||
-        (e = cudaMemset(h->rcount, 0, sizeof(unsigned int))) != cudaSuccess ||
-        (e = cudaMalloc(&h->st, sizeof(FpState))) != cudaSuccess ||
-        (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1))) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess ||
-        (e = cudaMalloc(&kd, sizeof(double) * n)) != cudaSuccess ||
-        (e = cudaMemcpy(kd, kk.data(), sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&kd, sizeof(double) * n)) != cudaSuccess ||
+        (e = cudaMemcpy(kd, k_host, sizeof(double) * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
         cudaFree(kd);
         cfm_fpcg_destroy(h);
         CFM_CUDA_TRY(e);
@@ -1225,6 +1394,105 @@ int cfm_fpcg_create(const cfm_stencil *S, const double *k_host, cfm_unet *net, i
     e = cudaDeviceSynchronize();
     cudaFree(kd);
     if (e != cudaSuccess) {
+        cfm_fpcg_destroy(h);
+        CFM_CUDA_TRY(e);
+    }
+    *out = h;
+    return CFM_OK;
+}
+
+int cfm_fpcg_create_batch(int nmem, const int *nx, const int *ny, const double *const *k_host, cfm_unet *net,
+                          int smooth, int maxiter, double tol, cfm_fpcg **out) {
+    clear_error();
+    CFM_ARG_CHECK(out && nx && ny && k_host && nmem >= 1, "arguments");
+    *out = nullptr;
+    CFM_ARG_CHECK(tol > 0 && maxiter > 0, "tol, maxiter");
+    CFM_ARG_CHECK(smooth >= 0 && smooth <= FP_MAX_SMOOTH, "smooth must be in [0, 8]");
+    const int f = net ? net->coarsen : 1;
+    int FX = 0, FY = 0;  // the frame
+    if (net) {
+        int H = 0, W = 0;
+        unet_shape(net->u, &H, &W);
+        FX = W * f;
+        FY = H * f;
+        CFM_ARG_CHECK(smooth == net->smooth, "smooth must equal the sweeps the network was trained with");
+    } else {
+        for (int m = 0; m < nmem; ++m) {
+            FX = std::max(FX, nx[m]);
+            FY = std::max(FY, ny[m]);
+        }
+    }
+    for (int m = 0; m < nmem; ++m) {
+        CFM_ARG_CHECK(k_host[m] && nx[m] >= 1 && ny[m] >= 1, "member arguments");
+        CFM_ARG_CHECK(nx[m] <= FX && ny[m] <= FY, "a member is larger than the network's grid times its factor");
+    }
+    CFM_ARG_CHECK((double)FX * FY * nmem < 1.5e9, "batch too large");
+    cfm_fpcg *h = new cfm_fpcg();
+    int st = fp_setup(h, FX, FY, f, net, smooth, maxiter, tol, nmem);
+    if (st) {
+        cfm_fpcg_destroy(h);
+        return st;
+    }
+    // Frame coefficients: each member at the frame's origin, its faces to
+    // the padding zero and the padding's diagonal 1, so the padding is an
+    // identity block that stays at zero (b = 0 there and the network's
+    // correction is kept inside the member).  FP32 copies rounded to nearest.
+    const size_t n = h->n, N = n * nmem;
+    std::vector<double> c(4 * N, 0.0);
+    std::vector<float> xin(2 * (size_t)h->nc * nmem, 0.f);
+    std::vector<double> cells(nmem);
+    h->ext_h.resize(nmem);
+    for (int m = 0; m < nmem; ++m) {
+        const int mx = nx[m], my = ny[m];
+        const size_t mn = (size_t)mx * my;
+        std::vector<double> we(mn), wn(mn), wt(mn), dg(mn);
+        if ((st = cfm_varcoef_coeffs(2, mx, my, 1, k_host[m], we.data(), wn.data(), wt.data(), dg.data()))) {
+            cfm_fpcg_destroy(h);
+            return st;
+        }
+        double *fwe = c.data() + m * n, *fwn = c.data() + N + m * n, *fdg = c.data() + 3 * N + m * n;
+        for (size_t i = 0; i < n; ++i) fdg[i] = 1.0;
+        for (int y = 0; y < my; ++y)
+            for (int x = 0; x < mx; ++x) {
+                const size_t src = (size_t)y * mx + x, dst = (size_t)y * FX + x;
+                fwe[dst] = x < mx - 1 ? we[src] : 0.0;
+                fwn[dst] = y < my - 1 ? wn[src] : 0.0;
+                fdg[dst] = dg[src];
+            }
+        // the network's second channel: block-mean log k (k = 1 in the padding)
+        const int ncx = FX / f;
+        for (int ic = 0; ic < h->nc; ++ic) {
+            const int cx = ic % ncx, cy = ic / ncx;
+            double sum = 0;
+            for (int dy = 0; dy < f; ++dy)
+                for (int dx = 0; dx < f; ++dx) {
+                    const int gx = cx * f + dx, gy = cy * f + dy;
+                    if (gx < mx && gy < my) sum += std::log(k_host[m][(size_t)gy * mx + gx]);
+                }
+            xin[2 * ((size_t)m * h->nc + ic) + 1] = (float)(sum / (f * f));
+        }
+        h->ext_h[m] = make_int2(mx, my);
+        cells[m] = (double)mn;
+    }
+    std::vector<float> c32(4 * N);
+    for (size_t i = 0; i < 4 * N; ++i) c32[i] = (float)c[i];
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->c64b, sizeof(double) * 4 * N)) != cudaSuccess ||
+        (e = cudaMalloc(&h->c32b, sizeof(float) * 4 * N)) != cudaSuccess ||
+        (e = cudaMalloc(&h->ext, sizeof(int2) * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->cells, sizeof(double) * nmem)) != cudaSuccess ||
+        (e = cudaMemcpy(h->c64b, c.data(), sizeof(double) * 4 * N, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->c32b, c32.data(), sizeof(float) * 4 * N, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->ext, h->ext_h.data(), sizeof(int2) * nmem, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->cells, cells.data(), sizeof(double) * nmem, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->xin, xin.data(), sizeof(float) * xin.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("batch upload: %s", cudaGetErrorString(e));
+        cfm_fpcg_destroy(h);
+        return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
+    }
+    k_fp_wd<<<1024, 256>>>(h->c32b + 3 * N, h->wd32, (int)N);
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
         cfm_fpcg_destroy(h);
         CFM_CUDA_TRY(e);
     }
@@ -1249,6 +1517,10 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     cudaFree(h->vec32);
     cudaFree(h->ring32);
     cudaFree(h->xm);
+    cudaFree(h->c64b);
+    cudaFree(h->c32b);
+    cudaFree(h->ext);
+    cudaFree(h->cells);
     cudaFree(h->st);
     cudaFree(h->hist);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1264,7 +1536,7 @@ int cfm_fpcg_set_truncation(cfm_fpcg *h, int m) {
     if (m == h->m) return CFM_OK;
     CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     double *ring = nullptr;
-    CFM_CUDA_TRY(cudaMalloc(&ring, sizeof(double) * 2 * (m + 1) * (size_t)h->n));
+    CFM_CUDA_TRY(cudaMalloc(&ring, sizeof(double) * 2 * (m + 1) * (size_t)h->n * h->nmem));
     cudaFree(h->ring);
     h->ring = ring;
     if (h->mixed) {
@@ -1285,7 +1557,7 @@ int cfm_fpcg_set_precision(cfm_fpcg *h, int precision, double delta) {
     CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
     const int mixed = precision == CFM_FP32;
     if (mixed && !h->vec32) {
-        const size_t n = h->n;
+        const size_t n = (size_t)h->n * h->nmem;
         float *v = nullptr;
         double *xm = nullptr;
         CFM_CUDA_TRY(cudaMalloc(&v, sizeof(float) * 4 * n));
@@ -1327,6 +1599,7 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     const cfm::NvtxRange nvtx_range("cfm_fpcg_solve");
     clear_error();
     CFM_ARG_CHECK(h && b_host && x_host, "null argument");
+    CFM_ARG_CHECK(h->nmem == 1, "a batch handle: use cfm_fpcg_solve_batch");
     const size_t n = h->n;
     FpArgs a = fp_args(h);
     cudaStream_t s = h->stream;
@@ -1415,6 +1688,104 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
 }
 
 // |r| before each preconditioner application of the last solve (k + 1 values).
+int cfm_fpcg_solve_batch(cfm_fpcg *h, const double *const *b_host, double *const *x_host, long long *iters,
+                         int *status, double *relres, cfm_stats *stats) {
+    const cfm::NvtxRange nvtx_range("cfm_fpcg_solve_batch");
+    clear_error();
+    CFM_ARG_CHECK(h && b_host && x_host, "null argument");
+    const int M = h->nmem;
+    for (int m = 0; m < M; ++m) CFM_ARG_CHECK(b_host[m] && x_host[m], "null member vector");
+    const size_t n = h->n, N = n * M;
+    FpArgs a = fp_args(h);
+    cudaStream_t s = h->stream;
+    double *b = h->vec + 3 * N, *t = h->vec + 4 * N;
+    // right-hand sides into the frames (zero in the padding)
+    std::vector<double> frame(N, 0.0);
+    for (int m = 0; m < M; ++m) {
+        const int mx = h->ext_h[m].x, my = h->ext_h[m].y;
+        for (int y = 0; y < my; ++y)
+            std::memcpy(frame.data() + m * n + (size_t)y * h->nx, b_host[m] + (size_t)y * mx, sizeof(double) * mx);
+    }
+    CFM_CUDA_TRY(cudaMemcpyAsync(b, frame.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    if (h->net) CFM_CUDA_TRY(cudaMemsetAsync(unet_err(h->net->u), 0, sizeof(int), s));
+    int st = 0;
+    if (!h->exec) {
+        if (h->net && (st = unet_forward(h->net->u, 1, h->xin, h->out, s))) return st;
+        CFM_CUDA_TRY(cudaStreamSynchronize(s));
+        if ((st = build_graph(h))) return st;
+    }
+    int launches = 0;
+    CFM_CUDA_TRY(cudaEventRecord(h->ev0, s));
+    if (h->mixed)
+        k_fpm_init<<<dim3(h->ntiles, M), CG_TILE, 0, s>>>(a, h->tol);
+    else
+        k_fp_init<<<dim3(h->ntiles, M), CG_TILE, 0, s>>>(a, h->tol);
+    CFM_CUDA_TRY(cudaGetLastError());
+    if ((st = fp_precond_dir(h, a, 0, 0, 0))) return st;
+    launches += 2;
+    std::vector<FpState> hs(M);
+    if (h->conditional) {
+        CFM_CUDA_TRY(cudaGraphLaunch(h->exec, s));
+        ++launches;
+    } else {
+        for (;;) {
+            CFM_CUDA_TRY(cudaGraphLaunch(h->exec, s));
+            ++launches;
+            CFM_CUDA_TRY(cudaMemcpyAsync(hs.data(), h->st, sizeof(FpState) * M, cudaMemcpyDeviceToHost, s));
+            CFM_CUDA_TRY(cudaStreamSynchronize(s));
+            bool open = false;
+            for (const FpState &q : hs) open |= q.done == 0;
+            if (!open) break;
+        }
+    }
+    if (h->mixed) {
+        k_fpm_finish<<<1024, 256, 0, s>>>(a, h->st);
+        CFM_CUDA_TRY(cudaGetLastError());
+        ++launches;
+    }
+    k_fpb_true_res<<<dim3(FP_RES_BLOCKS, M), 256, 0, s>>>(a, t, h->acc, h->rslots, h->rcount);
+    CFM_CUDA_TRY(cudaGetLastError());
+    ++launches;
+    CFM_CUDA_TRY(cudaMemcpyAsync(frame.data(), a.x, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+    std::vector<double> acc(M);
+    CFM_CUDA_TRY(cudaMemcpyAsync(acc.data(), h->acc, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+    CFM_CUDA_TRY(cudaMemcpyAsync(hs.data(), h->st, sizeof(FpState) * M, cudaMemcpyDeviceToHost, s));
+    CFM_CUDA_TRY(cudaEventRecord(h->ev1, s));
+    CFM_CUDA_TRY(cudaEventSynchronize(h->ev1));
+    if (h->net && (st = unet_check_err(h->net->u))) return st;
+    float ms = 0;
+    CFM_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    int worst = CFM_OK, updates = 0;
+    long long kmax = 0;
+    for (int m = 0; m < M; ++m) {
+        const int mx = h->ext_h[m].x, my = h->ext_h[m].y;
+        for (int y = 0; y < my; ++y)
+            std::memcpy(x_host[m] + (size_t)y * mx, frame.data() + m * n + (size_t)y * h->nx, sizeof(double) * mx);
+        const double bnorm = hs[m].target / h->tol;
+        const double rr = bnorm > 0 ? std::sqrt(acc[m]) / bnorm : std::sqrt(acc[m]);
+        const int sm = (hs[m].done == 1 && rr <= h->tol) ? CFM_OK : CFM_NOT_CONVERGED;
+        if (iters) iters[m] = hs[m].k;
+        if (status) status[m] = sm;
+        if (relres) relres[m] = rr;
+        if (sm != CFM_OK) worst = sm;
+        kmax = std::max(kmax, hs[m].k);
+        updates += hs[m].updates;
+    }
+    h->last_updates = h->mixed ? updates : 0;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->seconds = ms * 1e-3;
+        stats->iterations = kmax;
+        stats->h2d_bytes = 8.0 * N;
+        stats->d2h_bytes = 8.0 * N;
+        stats->launches = launches;
+        stats->status = worst;
+        stats->refinements = h->last_updates;
+    }
+    if (worst != CFM_OK) set_error("some members did not reach the tolerance");
+    return worst;
+}
+
 int cfm_fpcg_history(cfm_fpcg *h, double *out, long long max_n, long long *n_out) {
     CFM_ARG_CHECK(h && out && n_out, "null argument");
     const long long n = std::min(max_n, std::min(h->last_k + 1, h->maxiter + 1));

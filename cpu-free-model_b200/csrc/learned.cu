@@ -85,14 +85,16 @@ __global__ void __launch_bounds__(256, 2) k_cin_fwd(const float *x, const float 
     float sc = 1.f;
     if (in_scale.part) {
         __shared__ double red[8];
+        const double *part = in_scale.part + blockIdx.z * in_scale.part_stride;
+        const double cells = in_scale.cells_img ? in_scale.cells_img[blockIdx.z] : in_scale.cells;
         double acc = 0;
-        for (int j = threadIdx.x; j < in_scale.nparts; j += blockDim.x) acc += in_scale.part[j];
+        for (int j = threadIdx.x; j < in_scale.nparts; j += blockDim.x) acc += part[j];
         for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
         __syncthreads();
         double tot = 0;
         for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) tot += red[wi];
-        sc = tot > 0 ? (float)sqrt(in_scale.cells / tot) : 0.f;
+        sc = tot > 0 ? (float)sqrt(cells / tot) : 0.f;
     }
     const int q = threadIdx.x & 7, c0 = q * 4, grp = threadIdx.x >> 3;  // 32 groups per block
     float wr[9][8];  // [t][(c - c0) * 2 + in]
@@ -659,7 +661,7 @@ int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
     CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + PXB * CIN_SPAN * 32 - 1) / (PXB * CIN_SPAN * 32), H, B), dim3(256),
                             0, s, x, (const float *)(u->theta + u->woff[0]),
                             (const float *)(u->theta + u->boff[0]), a.h0, H, W,
-                            in_scale ? *in_scale : UNetInputScale{nullptr, 0, 0.0}));
+                            in_scale ? *in_scale : UNetInputScale{}));
     int h = H, w = W;
     CFM_CUDA_TRY(launch_pdl(k_pool<32>, row_grid(w / 2 * 4, h / 2, B), dim3(256), 0, s, (const bf16 *)a.h0,
                             a.p1, h / 2, w / 2));

@@ -33,6 +33,10 @@ struct UNetInputScale {
     const double *part;
     int nparts;
     double cells;
+    // a batch: image z reads part + z part_stride and, when cells_img is
+    // given, takes cells_img[z] cells
+    long long part_stride = 0;
+    const double *cells_img = nullptr;
 };
 // x FP32 [B][H][W][2] -> out FP32 [B][H][W] (device pointers).
 int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,

@@ -447,6 +447,27 @@ int cfm_fpcg_set_network_period(cfm_fpcg *h, int every);
 int cfm_fpcg_set_precision(cfm_fpcg *h, int precision, double delta);
 /* FP64 reliable updates of the last solve (0 in FP64 mode). */
 int cfm_fpcg_reliable_updates(const cfm_fpcg *h);
+/* A batch of independent 2D variable-coefficient systems solved together
+ * by the same device loop: member m has cells nx[m] x ny[m] and
+ * coefficients k_host[m] (built as cfm_varcoef_coeffs does).  Every member
+ * is embedded at the origin of one frame -- the network's grid times its
+ * factor, or with net == NULL the largest member -- whose padding is a
+ * decoupled identity block with zero right-hand side, so it stays zero; the
+ * network runs on all members' frames at once (in chunks of its largest
+ * batch) and its correction is kept inside each member.  Each member has its
+ * own scalars, convergence test and iteration count; converged members stop
+ * while the others go on (one conditional graph).  Precision, truncation and
+ * network period are set as for one system.  No counterpart in the
+ * reference. */
+int cfm_fpcg_create_batch(int nmem, const int *nx, const int *ny, const double *const *k_host,
+                          cfm_unet *net, int smooth, int maxiter, double tol, cfm_fpcg **out);
+/* Solves member m for b_host[m] into x_host[m] (row-major nx[m] x ny[m]);
+ * per-member iterations, status (CFM_OK when the FP64 true relative residual
+ * reached tol) and true relative residual (each optional).  Returns CFM_OK or
+ * CFM_NOT_CONVERGED if any member did not converge.  stats: the whole
+ * batch (seconds, the largest iteration count, launches). */
+int cfm_fpcg_solve_batch(cfm_fpcg *h, const double *const *b_host, double *const *x_host,
+                         long long *iters, int *status, double *relres, cfm_stats *st);
 int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats *st);
 /* Recursive residual norms |r_k| of the last solve, one per iteration from
  * k = 0 (at most max_n; *n_out = the count).  net == NULL in
