@@ -34,6 +34,7 @@ _SIGS = {
     "cfm_jacobi_destroy": (None, [_vp]),
     "cfm_jacobi_set_stream": (_c.c_int, [_vp, _vp]),
     "cfm_jacobi_set_boundary": (_c.c_int, [_vp, _c.c_int]),
+    "cfm_jacobi_set_dataflow": (_c.c_int, [_vp, _c.c_int]),
     "cfm_jacobi_load_problem": (_c.c_int, [_vp, _c.c_int]),
     "cfm_jacobi_upload": (_c.c_int, [_vp, _vp]),
     "cfm_jacobi_download": (_c.c_int, [_vp, _vp]),
@@ -238,6 +239,11 @@ class Jacobi:
 
     def set_stream(self, stream_handle):
         check("cfm_jacobi_set_stream", lib.cfm_jacobi_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def set_dataflow(self, on):
+        """3D TMA pipeline: order sweeps by unit neighbourhoods (True) or by a
+        grid barrier per sweep (False)."""
+        check("cfm_jacobi_set_dataflow", lib.cfm_jacobi_set_dataflow(self.h, int(on)))
 
     def set_boundary(self, boundary):
         """BOUNDARY_DIRICHLET (fixed x columns) or, 2D only, BOUNDARY_MIRROR

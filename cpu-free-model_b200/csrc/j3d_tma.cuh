@@ -14,6 +14,21 @@
 // global memory.  A stage is released (mbarrier arrive, one per consumer warp)
 // after the last step that reads it, so up to STAGES planes are in flight per
 // block.  All mbarrier and grid-barrier waits are bounded.
+//
+// Sweeps are ordered either by a grid barrier after each sweep (udone null)
+// or, with udone (one counter per unit, zero at launch), by the units'
+// neighbourhoods alone: when the consumers of a block finish unit u of
+// sweep t they set udone[u] = t + 1 (release, after a consumer-only barrier
+// that also ORs their error flags), and the producer loads unit u of sweep
+// t only after every unit of its 3 x 3 x 3 neighbourhood -- chunks and
+// tiles at distance one, z chunks wrapping around and y tiles too when y is
+// periodic, since those write the periodic images u reads -- has reached t
+// (27 lanes poll one neighbour each; bounded).  Those neighbours are all of
+// u's readers and writers in sweep t - 1, so both the values u reads and
+// the cells it overwrites are settled, and a block that finishes a sweep
+// early goes straight on with its next unit instead of waiting for the
+// slowest block.  Every wait is on an earlier sweep, so the units complete
+// in (sweep, unit) order at worst and the waits cannot form a cycle.
 #pragma once
 
 #include "barrier.cuh"
@@ -47,6 +62,29 @@ struct TmaGeom {
     static constexpr int THREADS = 32 * (CW + 1);
 };
 
+// Consumer-warp barrier (named barrier 1, `nthreads` threads) that also
+// returns the OR of every participant's `pred`.
+__device__ __forceinline__ int bar_red_or(int nthreads, int pred) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.s32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(pred), "r"(nthreads)
+        : "memory");
+    return r;
+}
+
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ double tma_add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float tma_add(float a, float b) { return __fadd_rn(a, b); }
 
@@ -56,7 +94,8 @@ __device__ __forceinline__ float tma_mul(float a, float b) { return __fmul_rn(a,
 template <typename T, int CW, int RPW, int STAGES, bool PY>
 __global__ void __launch_bounds__(32 * (CW + 1))
     j3d_tma_kernel(const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1,
-                   T *g0, T *g1, int nx, int ny, int nz, int niter, int zchunk, BarrierState *bar) {
+                   T *g0, T *g1, int nx, int ny, int nz, int niter, int zchunk, BarrierState *bar,
+                   unsigned int *udone) {
     using G = TmaGeom<T, CW, RPW, STAGES>;
     using V = typename Vec16<T>::type;
     constexpr int VN = G::VN, TX = G::TX, BXW = G::BXW, TY = G::TY;
@@ -89,15 +128,51 @@ __global__ void __launch_bounds__(32 * (CW + 1))
     const T c6 = T(1) / T(6);
     unsigned k = 0;  // plane loads issued (producer) / consumed (consumers) so far
 
+    int cerr = 0;  // consumers: an error seen by any consumer warp (dataflow order)
     for (int it = 0; it < niter; ++it) {
         const CUtensorMap *tm = (it & 1) ? &tm1 : &tm0;
         T *out = (it & 1) ? g0 : g1;
         if (warp == CW) {
             // ---------------------------------------------------- producer
-            if (lane == 0) {
-                fence_proxy_async_global();
-                for (long long u = blockIdx.x; u < U && !s_err; u += NB) {
-                    const int ch = (int)(u / ntiles), tile = (int)(u - ch * ntiles);
+            if (lane == 0) fence_proxy_async_global();
+            for (long long u = blockIdx.x; u < U; u += NB) {
+                if (__shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)&s_err : 0, 0)) break;
+                const int ch = (int)(u / ntiles), tile = (int)(u - ch * ntiles);
+                if (udone && it > 0) {
+                    // the unit's neighbourhood must have finished sweep it - 1
+                    const int tx = tile % ntx, ty = tile / ntx;
+                    long long nb = -1;
+                    if (lane < 27) {
+                        int c2 = ch + lane / 9 - 1, y2 = ty + (lane / 3) % 3 - 1;
+                        const int x2 = tx + lane % 3 - 1;
+                        c2 = c2 < 0 ? nch - 1 : (c2 >= nch ? 0 : c2);
+                        bool valid = x2 >= 0 && x2 < ntx;
+                        if (PY) y2 = y2 < 0 ? nty - 1 : (y2 >= nty ? 0 : y2);
+                        else valid = valid && y2 >= 0 && y2 < nty;
+                        if (valid) nb = (long long)c2 * ntiles + (long long)y2 * ntx + x2;
+                    }
+                    const unsigned long long t0 = global_ns();
+                    bool waited_out = false;
+                    for (;;) {
+                        const bool ready = nb < 0 || ld_relaxed_u32(udone + nb) >= (unsigned)it;
+                        if (__all_sync(0xffffffffu, ready)) break;
+                        const bool stop = lane == 0 && (global_ns() - t0 > budget || ld_relaxed_i32(&bar->error));
+                        if (__shfl_sync(0xffffffffu, stop, 0)) {
+                            waited_out = true;
+                            break;
+                        }
+                    }
+                    if (waited_out) {
+                        if (lane == 0) {
+                            if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = 3000000 + it;
+                            s_err = 1;
+                        }
+                        break;
+                    }
+                    __threadfence();  // acquire the neighbours' stores ...
+                    if (lane == 0) fence_proxy_async_global();  // ... for the TMA reads below
+                }
+                if (lane == 0) {
                     const int x0 = (tile % ntx) * TX, y0 = 1 + (tile / ntx) * TY;
                     const int z0 = 1 + ch * zchunk, z1 = min(z0 + zchunk, nz - 1);
                     for (int z = z0 - 1; z <= z1; ++z) {
@@ -112,8 +187,10 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                         ++k;
                     }
                 }
+                __syncwarp();
             }
             __syncwarp();
+            if (udone && __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)&s_err : 0, 0)) break;
         } else {
             // ---------------------------------------------------- consumers
             for (long long u = blockIdx.x; u < U; u += NB) {
@@ -250,7 +327,20 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[scur]);
-                if (!ok) {
+                if (udone) {
+                    // the unit's stores, then one consumer barrier: publish
+                    // the unit, or leave together if any consumer failed
+                    __threadfence();
+                    cerr = bar_red_or(32 * CW, !ok);
+                    if (!cerr && warp == 0 && lane == 0) st_release_gpu_u32(udone + u, (unsigned)(it + 1));
+                    if (cerr) {
+                        if (!ok && lane == 0) {
+                            if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = 2000000 + it;
+                            s_err = 1;
+                        }
+                        break;
+                    }
+                } else if (!ok) {
                     if (lane == 0) {
                         if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = 2000000 + it;
                         s_err = 1;
@@ -258,8 +348,9 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                     break;
                 }
             }
+            if (cerr) break;
         }
-        if (it + 1 < niter) {
+        if (!udone && it + 1 < niter) {
             if (!grid_barrier(bar, gridDim.x, it)) break;
         }
     }

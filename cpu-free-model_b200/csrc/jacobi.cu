@@ -577,6 +577,7 @@ struct TmaConfig {
     CUtensorMap map[2], xmap[2];
     const void *fn = nullptr;
     int var = 0, sweeps = 1, blocks = 0, zchunk = 0, threads = 0;
+    long long units = 0;
     size_t smem = 0;
 };
 }  // namespace cfm
@@ -605,6 +606,13 @@ struct cfm_jacobi {
     size_t smem_optin = 0;
     // 2D: the mirror x boundary of the reference's PERKS comparator
     bool mirror = false;
+    // 3D TMA pipeline: sweeps ordered by unit neighbourhoods (true) or a
+    // grid barrier per sweep (the default: measured 3% faster at 512^3, the
+    // lockstep keeps the halo rows that neighbouring tiles share in L2); the
+    // per-unit counters and their capacity
+    bool dataflow = false;
+    unsigned int *udone = nullptr;
+    long long udone_cap = 0;
 };
 
 namespace {
@@ -750,6 +758,19 @@ int build_tma(cfm_jacobi *h, int var, int zchunk, TmaConfig *c) {
     } else {
         c->zchunk = pick_zchunk(ntiles, p.nz - 2, &c->blocks);
     }
+    // one completion counter per unit for the neighbourhood-ordered sweeps
+    const long long U = units_of(ntiles, p.nz - 2, c->zchunk);
+    if (V.sweeps == 1 && U > h->udone_cap) {
+        unsigned int *q = nullptr;
+        CFM_CUDA_TRY(cudaMalloc(&q, sizeof(unsigned int) * U));
+        if (h->udone) {
+            cudaStreamSynchronize(h->stream);
+            cudaFree(h->udone);
+        }
+        h->udone = q;
+        h->udone_cap = U;
+    }
+    c->units = U;
     c->var = var;
     c->sweeps = V.sweeps;
     c->threads = threads;
@@ -1032,8 +1053,10 @@ int launch_tma(cfm_jacobi *h, const TmaConfig &c, int count, int *launches) {
                         &g0, &g1, (void *)&p.nx, (void *)&p.ny, (void *)&p.nz, &n, &zc, &h->bar};
         CFM_CUDA_TRY(launch_cooperative(c.fn, dim3(c.blocks), dim3(c.threads), args, c.smem, h->stream));
     } else {
+        unsigned int *ud = h->dataflow && count > 1 ? h->udone : nullptr;
+        if (ud) CFM_CUDA_TRY(cudaMemsetAsync(ud, 0, sizeof(unsigned int) * c.units, h->stream));
         void *args[] = {(void *)&c.map[cu], (void *)&c.map[cu ^ 1], &g0, &g1, (void *)&p.nx, (void *)&p.ny,
-                        (void *)&p.nz, &n, &zc, &h->bar};
+                        (void *)&p.nz, &n, &zc, &h->bar, &ud};
         CFM_CUDA_TRY(launch_cooperative(c.fn, dim3(c.blocks), dim3(c.threads), args, c.smem, h->stream));
     }
     h->cur ^= (count & 1);
@@ -1215,6 +1238,7 @@ void cfm_jacobi_destroy(cfm_jacobi *h) {
     if (h->bar) cudaFree(h->bar);
     if (h->xbuf) cudaFree(h->xbuf);
     if (h->flags) cudaFree(h->flags);
+    if (h->udone) cudaFree(h->udone);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1249,6 +1273,12 @@ int cfm_jacobi_set_boundary(cfm_jacobi *h, int boundary) {
     h->mirror = m;
     // the sweep kernel changes: its occupancy and work units set the grid
     return choose_launch(h);
+}
+
+int cfm_jacobi_set_dataflow(cfm_jacobi *h, int on) {
+    CFM_ARG_CHECK(h, "handle is null");
+    h->dataflow = on != 0;
+    return CFM_OK;
 }
 
 int cfm_jacobi_load_problem(cfm_jacobi *h, int problem) {

@@ -135,6 +135,24 @@ def test_jacobi3d_config2_fp64_100_sweeps_bitexact(config2_fp64):
     np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize("dataflow", [False, True])
+@pytest.mark.parametrize("shape,py,niter", [((96, 40, 64), 1, 7), ((70, 33, 128), 0, 5), ((34, 130, 64), 1, 12),
+                                            ((18, 9, 16), 1, 4)])
+def test_jacobi3d_sweep_order_same_grid(dataflow, shape, py, niter):
+    """The TMA pipeline with a grid barrier per sweep and with the units'
+    neighbourhood order (no grid barrier) give the oracle's grid, including
+    the periodic images across z chunks and y tiles."""
+    for prec in PRECS:
+        a = rand_grid(shape, cfm.np_dtype(prec), 17)
+        nz, ny, nx = shape
+        with cfm.Jacobi(3, nx, ny, nz, prec, py, cfm.JACOBI_PERSISTENT) as j:
+            j.set_dataflow(dataflow)
+            j.upload(a)
+            st = j.run(niter)
+            np.testing.assert_array_equal(j.download(), oracle.jacobi3d(a, niter, py))
+            assert st.status == cfm.OK
+
+
 def test_jacobi3d_config2_fp32_100_sweeps(config2_fp64):
     """Config 2's FP32 variant: 512^3, 100 sweeps, bit for bit against the FP32
     oracle, and within 1.5e-6 (max-abs and relative L2) of the FP64 grid."""
