@@ -147,6 +147,11 @@ struct Vals32 {
 };
 
 // ------------------------------------------------------------- operators
+// CSR entries per row whose loads a thread issues together (CsrOp::apply2_t,
+// the FP64 passes): 4 and 8 both took standard CG on 128^3 Poisson from
+// 26.4 to 25.5 ms (bit-identical); the same form in the FP32 passes was no
+// faster (20.1-20.9 against 19.9-20.2 ms), so those keep one entry per step.
+constexpr int CSR_Q = 4;
 struct CsrOp {
     const int *rowptr, *col;
     const double *val;
@@ -178,15 +183,32 @@ struct CsrOp {
             e2 = rowptr[i2 + 1];
         }
         T a1 = T(0), a2 = T(0);
+        // CSR_Q entries of each row per step: all their col / val loads,
+        // then all their x gathers, then the FMAs in entry order (the sum is
+        // the one-entry-at-a-time one, bit for bit), so up to 4 CSR_Q
+        // independent loads are in flight per thread instead of two chains
         while (j1 < e1 || j2 < e2) {
-            if (j1 < e1) {
-                a1 = fma_rn(v[j1], x[col[j1]], a1);
-                ++j1;
+            int c1[CSR_Q], c2[CSR_Q];
+            T w1[CSR_Q], w2[CSR_Q], g1[CSR_Q], g2[CSR_Q];
+#pragma unroll
+            for (int q = 0; q < CSR_Q; ++q) {
+                c1[q] = j1 + q < e1 ? col[j1 + q] : -1;
+                c2[q] = j2 + q < e2 ? col[j2 + q] : -1;
+                w1[q] = j1 + q < e1 ? v[j1 + q] : T(0);
+                w2[q] = j2 + q < e2 ? v[j2 + q] : T(0);
             }
-            if (j2 < e2) {
-                a2 = fma_rn(v[j2], x[col[j2]], a2);
-                ++j2;
+#pragma unroll
+            for (int q = 0; q < CSR_Q; ++q) {
+                g1[q] = c1[q] >= 0 ? x[c1[q]] : T(0);
+                g2[q] = c2[q] >= 0 ? x[c2[q]] : T(0);
             }
+#pragma unroll
+            for (int q = 0; q < CSR_Q; ++q) {
+                if (c1[q] >= 0) a1 = fma_rn(w1[q], g1[q], a1);
+                if (c2[q] >= 0) a2 = fma_rn(w2[q], g2[q], a2);
+            }
+            j1 += CSR_Q;
+            j2 += CSR_Q;
         }
         y1 = a1;
         y2 = a2;
