@@ -494,6 +494,150 @@ __global__ void __launch_bounds__(1024, 1)
         for (int x = tid; x < nx; x += nth) final_out[x] = cur[(size_t)h * nx + x];
 }
 
+// The resident kernel with two sweeps per exchange (halo two rows deep): the
+// band lives in shared memory with two halo rows on each side (h + 4 rows,
+// twice).  The first sweep runs alone (the initial halo rows need not be
+// periodic images yet) and ends with an exchange of the block's first two
+// and last two rows; from then on each period is sweep A over rows r0 - 1 ..
+// r1 (the extra row on each side computed from the deeper halo, with the
+// same inputs and arithmetic as the neighbour that owns it, so the same
+// bits) and sweep B over the block's own rows r0 .. r1 - 1, then one
+// exchange; an odd last sweep runs alone.  Half the neighbour handshakes of
+// j2d_resident_kernel for 2 / h more computed rows.  Needs h >= 2.
+template <typename T, bool MIRROR>
+__global__ void __launch_bounds__(1024, 1)
+    j2d_resident2_kernel(const T *in, T *final_out, int nx, int ny, int niter, T *xbuf,
+                         unsigned int *flags, BarrierState *bar) {
+    extern __shared__ __align__(16) unsigned char j2d_smem[];
+    const int B = gridDim.x, b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const int nrows = ny - 2;
+    const int r0 = 1 + (int)((long long)b * nrows / B);
+    const int r1 = 1 + (int)((long long)(b + 1) * nrows / B);
+    const int h = r1 - r0;  // >= 2
+    const int up_blk = (b + B - 1) % B, dn_blk = (b + 1) % B;
+    // local row l of the band is global row r0 - 2 + l; own rows are 2 .. h + 1
+    const size_t band = (size_t)(h + 4) * nx;
+    T *cur = reinterpret_cast<T *>(j2d_smem);
+    T *nxt = cur + band;
+    // initial rows r0 - 1 .. r1 (local 1 .. h + 2) in both copies
+    for (size_t i = tid; i < (size_t)(h + 2) * nx; i += nth) {
+        const T v = in[(size_t)(r0 - 1) * nx + i];
+        cur[nx + i] = v;
+        nxt[nx + i] = v;
+    }
+    __syncthreads();
+    __shared__ int s_ok;
+    const int x0 = MIRROR ? 0 : 1;
+    const int inner = MIRROR ? nx : nx - 2;
+    const int dr = nth / inner, dx = nth % inner;
+    // rows [ra, rb) (local) of dst from src
+    auto sweep_rows = [&](const T *src, T *dst, int ra, int rb) {
+        if (ra >= rb) return;
+        int r = ra + tid / inner, x = x0 + tid % inner;
+        for (; r < rb; r += dr, x += dx) {
+            if (x >= x0 + inner) {
+                x -= inner;
+                ++r;
+                if (r >= rb) break;
+            }
+            const T *c = src + (size_t)r * nx + x;
+            T v;
+            if (MIRROR)
+                v = quarter<T>(add_rn(add_rn(add_rn(c[nx], c[-nx]), c[x < nx - 1 ? 1 : 0]),
+                                      c[x > 0 ? -1 : 0]));
+            else
+                v = quarter<T>(add_rn(add_rn(add_rn(c[1], c[-1]), c[nx]), c[-nx]));
+            dst[(size_t)r * nx + x] = v;
+        }
+    };
+    // The block's own rows of one sweep src -> dst: first its two edge rows
+    // at each end, published (full rows) to exchange slot `e`; then, when
+    // `publish`, the block's counter; then the inner rows; then, when
+    // `publish`, the neighbours' rows into dst's halo rows.  Returns false
+    // when a wait ran out.
+    auto own_sweep = [&](const T *src, T *dst, unsigned e, bool publish) -> bool {
+        const int ea = min(4, h + 2), eb = max(ea, h);
+        sweep_rows(src, dst, 2, ea);
+        sweep_rows(src, dst, eb, h + 2);
+        if (!publish) {
+            sweep_rows(src, dst, ea, eb);
+            return true;
+        }
+        __syncthreads();
+        T *xb = xbuf + ((size_t)(e & 1) * B + b) * 4 * nx;  // first two, last two rows
+        for (int i = tid; i < 2 * nx; i += nth) {
+            __stcg(xb + i, dst[2 * (size_t)nx + i]);
+            __stcg(xb + 2 * nx + i, dst[(size_t)h * nx + i]);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release_u32(flags + b, e);
+        }
+        sweep_rows(src, dst, ea, eb);
+        if (tid == 0) {
+            int ok = 1;
+            const unsigned long long t0 = global_ns();
+            const unsigned long long budget = bar->timeout_ns;
+            while (ld_acquire_u32(flags + up_blk) < e || ld_acquire_u32(flags + dn_blk) < e) {
+                if (ld_relaxed_i32(&bar->error)) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > budget) {
+                    if (atomicCAS(&bar->error, 0, 1) == 0) bar->where = (int)e;
+                    ok = 0;
+                    break;
+                }
+            }
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return false;
+        const T *up = xbuf + ((size_t)(e & 1) * B + up_blk) * 4 * nx + 2 * nx;  // its last two rows
+        const T *dn = xbuf + ((size_t)(e & 1) * B + dn_blk) * 4 * nx;           // its first two rows
+        for (int i = tid; i < 2 * nx; i += nth) {
+            dst[i] = __ldcg(up + i);
+            dst[(size_t)(h + 2) * nx + i] = __ldcg(dn + i);
+        }
+        __syncthreads();
+        return true;
+    };
+    int t = 0;
+    unsigned e = 0;  // exchanges so far
+    if (niter > 0) {  // the first sweep alone, from the initial halo rows
+        if (!own_sweep(cur, nxt, ++e, niter > 1)) return;
+        T *tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+        t = 1;
+    }
+    while (t < niter) {
+        if (niter - t >= 2) {
+            sweep_rows(cur, nxt, 1, h + 3);  // sweep A: own rows and one more each side
+            __syncthreads();
+            if (!own_sweep(nxt, cur, ++e, t + 2 < niter)) return;  // sweep B, back into cur
+            t += 2;
+        } else {
+            if (!own_sweep(cur, nxt, ++e, false)) return;
+            __syncthreads();
+            T *tmp = cur;
+            cur = nxt;
+            nxt = tmp;
+            t += 1;
+        }
+    }
+    __syncthreads();
+    // write the band back; the owners of rows 1 and ny-2 also write their
+    // periodic images (full rows)
+    for (size_t i = tid; i < (size_t)h * nx; i += nth) final_out[(size_t)r0 * nx + i] = cur[2 * nx + i];
+    if (r0 == 1)
+        for (int x = tid; x < nx; x += nth) final_out[(size_t)(ny - 1) * nx + x] = cur[2 * nx + x];
+    if (r1 == ny - 1)
+        for (int x = tid; x < nx; x += nth) final_out[x] = cur[(size_t)(h + 1) * nx + x];
+}
+
 // Cells on the edges of the box (two or more coordinates on the boundary) are
 // neither read nor written by a sweep.  The reference's full-row/plane halo
 // copies leave each such cell equal to its periodic image after the first
@@ -598,6 +742,7 @@ struct cfm_jacobi {
     unsigned int *flags = nullptr;
     int res_blocks = 0;
     size_t res_smem = 0;
+    bool res_two = false;  // two sweeps per exchange (j2d_resident2_kernel)
     bool resident = false;
     // 3D TMA pipeline: the chosen shape, and (for a two-sweep shape) the
     // one-sweep shape that does the last sweep of an odd count
@@ -848,7 +993,14 @@ const void *sweep_fn_any(const cfm_jacobi_params &p, bool images, bool mirror) {
                                    : sweep_fn<float>(p, images, mirror);
 }
 
-const void *resident_fn(const cfm_jacobi_params &p, bool mirror) {
+const void *resident_fn(const cfm_jacobi_params &p, bool mirror, bool two) {
+    if (two) {
+        if (p.precision == CFM_FP64)
+            return mirror ? (const void *)j2d_resident2_kernel<double, true>
+                          : (const void *)j2d_resident2_kernel<double, false>;
+        return mirror ? (const void *)j2d_resident2_kernel<float, true>
+                      : (const void *)j2d_resident2_kernel<float, false>;
+    }
     if (p.precision == CFM_FP64)
         return mirror ? (const void *)j2d_resident_kernel<double, true>
                       : (const void *)j2d_resident_kernel<double, false>;
@@ -930,19 +1082,25 @@ int choose_launch(cfm_jacobi *h) {
         if (need < h->blocks) h->blocks = (int)std::max(1LL, need);
     }
     if (p.dims == 2 && p.impl == CFM_JACOBI_RESIDENT) {
-        // One 1024-thread block per SM, each holding its band (+2 halo rows)
-        // twice in shared memory; used only when that fits on chip.
-        const int B = std::min(di.num_sms, p.ny - 2);
-        const int hmax = (p.ny - 2 + B - 1) / B;
-        const size_t smem = 2 * (size_t)(hmax + 2) * p.nx * h->esize;
-        const void *rfn = resident_fn(p, h->mirror);
-        if (smem <= di.smem_optin) {
+        // One 1024-thread block per SM, each holding its band twice in shared
+        // memory; used only when that fits on chip.  Preferred: two sweeps
+        // per exchange (bands of >= 2 rows plus 2 halo rows each side), else
+        // one (any band, 1 halo row each side).
+        h->resident = false;
+        for (int two = 1; two >= 0 && !h->resident; --two) {
+            const int B = std::min(di.num_sms, two ? (p.ny - 2) / 2 : p.ny - 2);
+            if (B < 1) continue;
+            const int hmax = (p.ny - 2 + B - 1) / B;
+            const size_t smem = 2 * (size_t)(hmax + (two ? 4 : 2)) * p.nx * h->esize;
+            const void *rfn = resident_fn(p, h->mirror, two != 0);
+            if (smem > di.smem_optin) continue;
             CFM_CUDA_TRY(cudaFuncSetAttribute(rfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem));
             int rper = 0;
             CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper, rfn, 1024, smem));
             if (rper >= 1) {
                 h->resident = true;
+                h->res_two = two != 0;
                 h->res_blocks = B;
                 h->res_smem = smem;
             }
@@ -1034,7 +1192,7 @@ int resident2d(cfm_jacobi *h, int niter, int *launches) {
     int n = niter;
     void *args[] = {(void *)&in, &fin, (void *)&p.nx, (void *)&p.ny, &n, &h->xbuf, &h->flags,
                     &h->bar};
-    const void *fn = resident_fn(p, h->mirror);
+    const void *fn = resident_fn(p, h->mirror, h->res_two);
     CFM_CUDA_TRY(launch_cooperative(fn, dim3(h->res_blocks), dim3(1024), args, h->res_smem,
                                     h->stream));
     h->cur ^= (niter & 1);
@@ -1208,7 +1366,8 @@ int cfm_jacobi_create(const cfm_jacobi_params *p, cfm_jacobi **out) {
     if (h->p.impl == CFM_JACOBI_PERSISTENT || h->p.impl == CFM_JACOBI_RESIDENT)
         if ((st = setup_tma(h, default_tma_variant()))) return fail(st);
     if (h->resident) {
-        const size_t xbytes = 2 * (size_t)h->res_blocks * 2 * h->p.nx * h->esize;
+        // exchange rows: 2 parities x blocks x 4 rows (the first and last two)
+        const size_t xbytes = 2 * (size_t)h->res_blocks * 4 * h->p.nx * h->esize;
         if ((e = cudaMalloc(&h->xbuf, xbytes)) != cudaSuccess ||
             (e = cudaMalloc(&h->flags, sizeof(unsigned int) * h->res_blocks)) != cudaSuccess) {
             set_error("exchange buffers: %s", cudaGetErrorString(e));
