@@ -650,6 +650,27 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def same_box_copy_gbs(torch):
+    """Copy bandwidth of this box, measured like the driver's peak (1 Gi BF16
+    elements, b.copy_(a), read + write bytes, best of 10, CUDA events): the
+    context for the roofline fraction, whose denominator stays the driver's
+    measured peak."""
+    a = torch.empty(1 << 30, dtype=torch.bfloat16, device="cuda")
+    b = torch.empty_like(a)
+    a.fill_(1.0)
+    best = 0.0
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.copy_(a)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * a.numel() * 2 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
 def cpu_baseline():
     """Oracle FP64 sweep loop on the host cores, sized to ~10 s."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -849,6 +870,10 @@ def main():
                 "results_equal": e2e_same},
         "gpu_launches": launches,
     }
+    if rank == 0 and world == 1:
+        box = same_box_copy_gbs(torch)
+        line["roofline"]["same_box_copy_gbs"] = box
+        line["roofline"]["frac_of_same_box_copy"] = achieved / box
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if rank == 0 and world == 1 and not args.no_secondary:

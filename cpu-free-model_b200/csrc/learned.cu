@@ -256,36 +256,58 @@ __global__ void k_cout_bwd(const float *dout, const float *w, const bf16 *g0, bf
     }
 }
 
-// Cross-block sums that come out the same on every run.  Every block has
-// stored its `ne` partial sums at part[blockIdx.x * ne + e]; the last block
-// to arrive (counted on *count) adds them in block order, b = 0, 1, ...,
-// hands each total to dst(e, total) and re-arms *count for the next launch.
-// Called by every thread of the block.
-template <class Dst>
-__device__ void add_partials_in_block_order(const float *part, int ne, unsigned int *count, Dst dst) {
-    __shared__ int s_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(count, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        float v = 0.f;
-        for (unsigned int b = 0; b < gridDim.x; ++b) v += __ldcg(part + (size_t)b * ne + e);
-        dst(e, v);
+// Cross-block sums that come out the same on every run: a kernel stores its
+// blocks' partial sums part[b][e] (nb blocks, ne entries) and
+// k_partials_reduce adds them in a fixed order.  A 256-thread block takes 16
+// entries and splits the nb blocks into 16 chunks, one thread per (entry,
+// chunk); a chunk is summed with four accumulators (block b into b mod 4,
+// combined as (a0 + a1) + (a2 + a3)), then the 16 chunks are added in order.
+// The totals go to dw[e] (e < nw) and db[e - nw] (+=).
+constexpr int PR_ENTRIES = 16, PR_CHUNKS = 16;
+__global__ void __launch_bounds__(PR_ENTRIES * PR_CHUNKS)
+    k_partials_reduce(const float *part, int nb, int ne, int nw, float *dw, float *db) {
+    __shared__ float sc[PR_ENTRIES * PR_CHUNKS];
+    const int el = threadIdx.x % PR_ENTRIES, q = threadIdx.x / PR_ENTRIES;
+    const int e = blockIdx.x * PR_ENTRIES + el;
+    float v = 0.f;
+    if (e < ne) {
+        const int b0 = (int)((long long)q * nb / PR_CHUNKS), b1 = (int)((long long)(q + 1) * nb / PR_CHUNKS);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        int b = b0;
+        for (; b + 3 < b1; b += 4) {
+            a0 += part[(size_t)b * ne + e];
+            a1 += part[(size_t)(b + 1) * ne + e];
+            a2 += part[(size_t)(b + 2) * ne + e];
+            a3 += part[(size_t)(b + 3) * ne + e];
+        }
+        for (; b < b1; ++b) a0 += part[(size_t)b * ne + e];
+        v = (a0 + a1) + (a2 + a3);
     }
-    if (threadIdx.x == 0) *count = 0;
+    sc[threadIdx.x] = v;
+    __syncthreads();
+    if (q == 0 && e < ne) {
+        float t = 0.f;
+        for (int c = 0; c < PR_CHUNKS; ++c) t += sc[c * PR_ENTRIES + el];
+        if (e < nw) dw[e] += t;
+        else db[e - nw] += t;
+    }
 }
 
-// Weight and bias gradient of a thin layer: per block, the sums over its
-// chunk of pixels, dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci] and
-// db[co] += sum_p g[p][co], then the blocks' sums added in block order.
-// `g` is FP32 (cout: one channel) or BF16 (cin: 32 channels); `in` FP32
-// (cin: the network input) or BF16 (cout: g0).
+int partials_reduce(const float *part, int nb, int ne, int nw, float *dw, float *db, cudaStream_t s) {
+    k_partials_reduce<<<(ne + PR_ENTRIES - 1) / PR_ENTRIES, PR_ENTRIES * PR_CHUNKS, 0, s>>>(part, nb, ne, nw, dw,
+                                                                                             db);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return CFM_OK;
+}
+
+// Weight and bias gradient of a thin layer, per block the sums over its
+// chunk of pixels of dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci] and
+// db[co] += sum_p g[p][co], into part[block][entry] (k_partials_reduce adds
+// them up).  `g` is FP32 (cout: one channel) or BF16 (cin: 32 channels);
+// `in` FP32 (cin: the network input) or BF16 (cout: g0).
 template <typename GT, typename IT>
-__global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, float *dw, float *db,
-                             int B, int H, int W, long long chunk, float *part, unsigned int *count) {
+__global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, int B, int H, int W,
+                             long long chunk, float *part) {
     const int nw = 9 * co_n * ci_n, ne = nw + co_n;
     const long long P = (long long)B * H * W;
     const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
@@ -294,12 +316,17 @@ __global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, floa
         if (e < nw) {
             const int t = e / (co_n * ci_n), co = (e / ci_n) % co_n, ci = e % ci_n;
             const int sy = t / 3 - 1, sx = t % 3 - 1;
+            const long long sq = (long long)sy * W + sx;
+            // (xx, yy) of pixel p, stepped along with p (no division per pixel).
+            int xx = (int)(p0 % W), yy = (int)((p0 / W) % H);
             for (long long p = p0; p < p1; ++p) {
-                const int xx = (int)(p % W), yy = (int)((p / W) % H);
                 const int y = yy + sy, xq = xx + sx;
-                if (y < 0 || y >= H || xq < 0 || xq >= W) continue;
-                const long long q = p + (long long)sy * W + sx;
-                acc += (float)g[p * co_n + co] * (float)in[q * ci_n + ci];
+                if (y >= 0 && y < H && xq >= 0 && xq < W)
+                    acc += (float)g[p * co_n + co] * (float)in[(p + sq) * ci_n + ci];
+                if (++xx == W) {
+                    xx = 0;
+                    if (++yy == H) yy = 0;
+                }
             }
         } else {
             const int co = e - nw;
@@ -307,10 +334,6 @@ __global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, floa
         }
         part[(size_t)blockIdx.x * ne + e] = acc;
     }
-    add_partials_in_block_order(part, ne, count, [&](int e, float v) {
-        if (e < nw) dw[e] += v;
-        else db[e - nw] += v;
-    });
 }
 
 // 2x2 mean pool, NHWC, 8 channels per thread; (h, w) is the pooled size.
@@ -400,9 +423,8 @@ __global__ void k_skip_pool_mask(const bf16 *dskip, const bf16 *dpool, const bf1
 }
 
 // db[c] += sum_p dz[p][c] (NHWC BF16): block-local sums over a chunk of
-// pixels, then the blocks' sums added in block order.
-__global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long long chunk, float *part,
-                            unsigned int *count) {
+// pixels into part[block][c] (k_partials_reduce adds them up).
+__global__ void k_bias_grad(const bf16 *dz, long long P, int C, long long chunk, float *part) {
     extern __shared__ float red[];  // [blockDim.x]
     const int c = threadIdx.x % C, lane_p = threadIdx.x / C, np = blockDim.x / C;
     const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
@@ -415,7 +437,6 @@ __global__ void k_bias_grad(const bf16 *dz, float *db, long long P, int C, long 
         for (int j = 0; j < np; ++j) s += red[j * C + threadIdx.x];
         part[(size_t)blockIdx.x * C + threadIdx.x] = s;
     }
-    add_partials_in_block_order(part, C, count, [&](int c, float v) { db[c] += v; });
 }
 
 // BF16 weights [9][co][ci] and their tap-flipped transposes [9][ci][co]
@@ -478,7 +499,6 @@ struct UNetImpl {
     // added in block order by the last block (deterministic), and the
     // arrival counters of those reductions
     float *gpart = nullptr;
-    unsigned int *gcount = nullptr;
     long long adam_t = 0;
     std::vector<void *> allocs;
 };
@@ -546,7 +566,6 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     }
     if (!st) st = dalloc(u, &u->ws, (size_t)u->ws_floats);
     if (!st) st = dalloc(u, &u->gpart, (size_t)GPART_FLOATS);
-    if (!st) st = dalloc(u, &u->gcount, 4);
     for (int l = 0; l < UNET_NLAYERS; ++l)
         if (UNET_LAYERS[l].tc) {
             const size_t n = 9 * (size_t)UNET_LAYERS[l].co * UNET_LAYERS[l].ci;
@@ -571,8 +590,7 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     if ((e = cudaMemset(u->theta, 0, o * 4)) != cudaSuccess ||
         (e = cudaMemset(u->m, 0, o * 4)) != cudaSuccess ||
         (e = cudaMemset(u->v, 0, o * 4)) != cudaSuccess ||
-        (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess ||
-        (e = cudaMemset(u->gcount, 0, 4 * sizeof(unsigned int))) != cudaSuccess) {
+        (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess) {
         unet_destroy(u);
         CFM_CUDA_TRY(e);
     }
@@ -644,10 +662,9 @@ int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, i
     const long long chunk = std::max(64LL, (P + 4 * 148 - 1) / (4 * 148));
     const int blocks = (int)((P + chunk - 1) / chunk);
     CFM_ARG_CHECK((long long)blocks * L.co <= GPART_FLOATS, "bias-gradient partials");
-    k_bias_grad<<<blocks, threads, threads * sizeof(float), s>>>(dz, u->grad + u->boff[l], P, L.co, chunk,
-                                                                 u->gpart, u->gcount + 2);
+    k_bias_grad<<<blocks, threads, threads * sizeof(float), s>>>(dz, P, L.co, chunk, u->gpart);
     CFM_CUDA_TRY(cudaGetLastError());
-    return CFM_OK;
+    return partials_reduce(u->gpart, blocks, L.co, 0, nullptr, u->grad + u->boff[l], s);
 }
 
 }  // namespace
@@ -707,10 +724,11 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
         const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
         const int blocks = (int)((P0 + chunk - 1) / chunk);
         CFM_ARG_CHECK((long long)blocks * (9 * 32 + 1) <= GPART_FLOATS, "thin-gradient partials");
-        k_thin_wgrad<float, bf16><<<blocks, 320, 0, s>>>(dout, a.g0, 1, 32, u->grad + u->woff[8],
-                                                         u->grad + u->boff[8], B, H, W, chunk, u->gpart,
-                                                         u->gcount + 0);
+        k_thin_wgrad<float, bf16><<<blocks, 320, 0, s>>>(dout, a.g0, 1, 32, B, H, W, chunk, u->gpart);
         CFM_CUDA_TRY(cudaGetLastError());
+        if ((st = partials_reduce(u->gpart, blocks, 9 * 32 + 1, 9 * 32, u->grad + u->woff[8], u->grad + u->boff[8],
+                                  s)))
+            return st;
         k_cout_bwd<<<grid_for(P0), 256, 0, s>>>(dout, u->theta + u->woff[8], a.g0, a.dz_g0, B, H, W);
         CFM_CUDA_TRY(cudaGetLastError());
     }
@@ -746,10 +764,11 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
         const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
         const int blocks = (int)((P0 + chunk - 1) / chunk);
         CFM_ARG_CHECK((long long)blocks * (9 * 32 * 2 + 32) <= GPART_FLOATS, "thin-gradient partials");
-        k_thin_wgrad<bf16, float><<<blocks, 608, 0, s>>>(a.dz_h0, x, 32, 2, u->grad + u->woff[0],
-                                                         u->grad + u->boff[0], B, H, W, chunk, u->gpart,
-                                                         u->gcount + 1);
+        k_thin_wgrad<bf16, float><<<blocks, 608, 0, s>>>(a.dz_h0, x, 32, 2, B, H, W, chunk, u->gpart);
         CFM_CUDA_TRY(cudaGetLastError());
+        if ((st = partials_reduce(u->gpart, blocks, 9 * 32 * 2 + 32, 9 * 32 * 2, u->grad + u->woff[0],
+                                  u->grad + u->boff[0], s)))
+            return st;
     }
     return CFM_OK;
 }

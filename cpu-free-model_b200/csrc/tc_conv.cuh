@@ -544,9 +544,10 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
 namespace cfm {
 
 // Weight-gradient splits of tc_conv_kernel: dw[tap][co][ci] += the sum of
-// part[s][tap][ci][co] over s = 0, 1, ..., ksplit - 1 in that order (the
-// same sum on every run).  One thread per element, in the partials' order
-// (coalesced reads).
+// part[s][tap][ci][co] over the splits s, in a fixed order (the same sum on
+// every run): split s into accumulator s mod 4, combined as (a0 + a1) +
+// (a2 + a3).  One thread per element, in the partials' order (coalesced
+// reads).
 __global__ void tc_wgrad_reduce(const float *part, int ksplit, int Cin, int Cout, float *dw) {
     pdl_enter();
     const long long n = 9LL * Cin * Cout;
@@ -555,10 +556,17 @@ __global__ void tc_wgrad_reduce(const float *part, int ksplit, int Cin, int Cout
         const int co = (int)(e % Cout);
         const long long r = e / Cout;
         const int ci = (int)(r % Cin), tap = (int)(r / Cin);
-        float v = 0.f;
-        for (int sp = 0; sp < ksplit; ++sp) v += part[(size_t)sp * n + e];
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        int sp = 0;
+        for (; sp + 3 < ksplit; sp += 4) {
+            a0 += part[(size_t)sp * n + e];
+            a1 += part[(size_t)(sp + 1) * n + e];
+            a2 += part[(size_t)(sp + 2) * n + e];
+            a3 += part[(size_t)(sp + 3) * n + e];
+        }
+        for (; sp < ksplit; ++sp) a0 += part[(size_t)sp * n + e];
         float *d = dw + ((size_t)tap * Cout + co) * Cin + ci;
-        *d += v;
+        *d += (a0 + a1) + (a2 + a3);
     }
 }
 

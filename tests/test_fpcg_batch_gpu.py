@@ -78,3 +78,32 @@ def test_learned_batch_of_uneven_members(coarse_net, mixed):
         assert np.linalg.norm(x.ravel() - xs_cg) / np.linalg.norm(xs_cg) < 1e-5
         _, st_j = cfm.FPCG(S, k, None, maxiter=20000, tol=1e-8, smooth=4).solve(f)
         assert it < st_j.iterations
+
+
+def test_config5_shaped_subset_learned_split(coarse_net):
+    """A config-5-shaped subset (2D sides 64..512, 3D sides 32..128, log-
+    uniform, per-system seeds) solved as the bench does with the learned
+    preconditioner: the 2D members of side >= 256 in the batched learned +
+    mixed FPCG, the others in the persistent mixed polynomial kernel (its
+    blocks per system from the autotuner).  Every member reaches the FP64
+    true residual 1e-8, and the learned members take fewer iterations than
+    the polynomial preconditioner gives them."""
+    systems = cfm.uneven_systems(10, 4, seed=11)
+    big = [i for i, (k, _) in enumerate(systems) if k.ndim == 2 and min(k.shape) >= 256]
+    rest = [i for i in range(len(systems)) if i not in big]
+    assert big and rest
+    FB = cfm.FPCGBatch([systems[i][0] for i in big], coarse_net, maxiter=20000, tol=1e-8, precision=cfm.FP32)
+    xs, it_l, st_l, rr_l, _ = FB.solve([systems[i][1] for i in big])
+    B = cfm.Batch([systems[i] for i in rest])
+    B.set_solver(smooth=4, maxiter=20000, tol=1e-8)
+    B.set_precision(cfm.FP32, 0, 0.1)
+    assert B.autotune() > 0
+    it_p, st_p, rr_p, _ = B.solve()
+    assert (st_l == cfm.OK).all() and (rr_l <= 1e-8).all()
+    assert (st_p == cfm.OK).all() and (rr_p <= 1e-8 * 1.5).all()
+    P = cfm.Batch([systems[i] for i in big])  # the same members with the polynomial
+    P.set_solver(smooth=4, maxiter=20000, tol=1e-8)
+    it_poly, st_poly, _, _ = P.solve()
+    assert (st_poly == cfm.OK).all()
+    print(f"learned {list(it_l)} vs polynomial {list(it_poly)}")
+    assert (it_l < it_poly).all()
