@@ -482,7 +482,6 @@ struct UNetBuffers {
     // backward
     bf16 *dz_g0, *du0, *dz_g1, *du1, *dz_g2, *du2, *dz_g3, *dz_h3, *dp3, *dz_h2, *dp2, *dz_h1,
         *dp1, *dz_h0;
-    bf16 *xt[3], *dzt;
 };
 
 struct UNetImpl {
@@ -580,8 +579,6 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     A(&a.dz_g2, L2 * 64); A(&a.du2, L2 * 128); A(&a.dz_g3, L3 * 128); A(&a.dz_h3, L3 * 256);
     A(&a.dp3, L3 * 128); A(&a.dz_h2, L2 * 128); A(&a.dp2, L2 * 64); A(&a.dz_h1, L1 * 64);
     A(&a.dp1, L1 * 32); A(&a.dz_h0, L0 * 32);
-    for (int d = 0; d < 3; ++d) A(&a.xt[d], L0 * 32);
-    A(&a.dzt, L0 * 32);
     if (st) {
         unet_destroy(u);
         return st;
@@ -650,13 +647,9 @@ int conv_bwd_data(UNetImpl *u, int l, const bf16 *dz, const bf16 *mask, bf16 *dx
 int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, int h, int w,
                      cudaStream_t s) {
     const UNetLayer &L = UNET_LAYERS[l];
-    UNetBuffers &a = u->a;
-    int st = nhwc_to_chw(x, a.xt[0], a.xt[1], a.xt[2], B, h, w, L.ci, 3, s);
+    WgradArgs g{x, dz, u->grad + u->woff[l], u->err, B, h, w, L.ci, L.co, u->ws, u->ws_floats};
+    int st = tc_conv_wgrad(g, s);
     if (st) return st;
-    if ((st = nhwc_to_chw(dz, nullptr, a.dzt, nullptr, B, h, w, L.co, 1, s))) return st;
-    WgradArgs g{{a.xt[0], a.xt[1], a.xt[2]}, a.dzt, u->grad + u->woff[l], u->err, B, h, w, L.ci, L.co,
-                u->ws, u->ws_floats};
-    if ((st = tc_conv_wgrad(g, s))) return st;
     const long long P = (long long)B * h * w;
     const int threads = 256;
     const long long chunk = std::max(64LL, (P + 4 * 148 - 1) / (4 * 148));

@@ -22,11 +22,13 @@
 //    BF16 store NHWC (lane pairs write whole 32-byte sectors).
 //  weight gradient:
 //    m = (tap of a tap group, input channel), n = output channel, k = pixels
-//    (KC consecutive x of one row per step).  A rows come from x-shifted
-//    channel-major copies of the layer input (XT_dx[img][c][y][x] =
-//    X[img][y][x + dx - 1][c]; the y shift is a TMA coordinate), B rows from
-//    the channel-major output gradient.  Tiles split K; the epilogue stores
-//    its partial tile in a workspace [split][tap][ci][co] and
+//    (KC consecutive x of one row per step).  Both operands are MN-major
+//    (channels contiguous), read straight from the NHWC tensors: per tap
+//    and block of 64 (or 32) channels one box of KC pixels of the layer
+//    input at (c0, x + dx - 1, y + dy - 1, img), whose zero fill outside
+//    the image is the padding, and per 64 (32) output channels one box of
+//    the output gradient at (c0, x, y, img).  Tiles split K; the epilogue
+//    stores its partial tile in a workspace [split][tap][ci][co] and
 //    tc_wgrad_reduce adds the splits to dW[tap][co][ci] in split order, so
 //    the gradient is the same on every run.
 //
@@ -127,12 +129,27 @@ __device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major,
-// N >> 3 at bits 17-22, M >> 4 at bits 24-28 (M = 128).
-template <int N>
+// Shared-memory matrix descriptor of an MN-major, swizzled operand tile:
+// rows of SW bytes (SW / 2 channels, SW = 64 or 128) along K, 8-row groups
+// `sbo` bytes apart, blocks of SW / 2 channels along M (or N) `lbo` bytes
+// apart.  Field positions as in kmajor_desc.
+__device__ __forceinline__ uint64_t mnmajor_desc(uint32_t saddr, int sw, uint32_t lbo, uint32_t sbo) {
+    const uint64_t layout = sw == 128 ? 2 : 4;
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= layout << 61;
+    return d;
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28 (M = 128); A and B K-major, or both MN-major
+// (bits 15 and 16).
+template <int N, bool MN = false>
 __host__ __device__ constexpr uint32_t idesc_bf16_m128() {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-           ((uint32_t)(128 >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | (MN ? (1u << 15) | (1u << 16) : 0u) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
 
 struct TcConvParams {
@@ -151,6 +168,7 @@ struct TcConvParams {
     long long ws_floats;  // capacity of ws (0: no split)
     // wgrad mode tiling
     int ci_rows, ci_tiles, taps_per_tile, tap_groups, ksplit;
+    int a_cb, b_cb;     // channels of one operand box (64, or 32 for 32-channel tensors)
     long long total_k;  // B * H * (W / KC)
     // shared-memory plan
     int stages;       // operand ring depth
@@ -204,8 +222,7 @@ __device__ __forceinline__ void store16_pairs(__nv_bfloat16 *pix_even, __nv_bflo
 template <int KC, int N>
 __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
     tc_conv_kernel(const __grid_constant__ CUtensorMap mapA0, const __grid_constant__ CUtensorMap mapA1,
-                   const __grid_constant__ CUtensorMap mapA2, const __grid_constant__ CUtensorMap mapB,
-                   TcConvParams p) {
+                   const __grid_constant__ CUtensorMap mapB, TcConvParams p) {
     constexpr int SW = KC * 2;              // bytes of one operand row (the swizzle span)
     constexpr int BTAP = N * SW;            // one weight tile (N rows)
     constexpr uint32_t TMEM_COLS = tc_tmem_cols<N>();
@@ -317,21 +334,24 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                     } else {
                         const long long kq = k0 + q;
                         const int xchunks = p.W / KC;
-                        const int xc = (int)(kq % xchunks);
+                        const int px0 = (int)(kq % xchunks) * KC;
                         const long long r2 = kq / xchunks;
                         const int y = (int)(r2 % p.H), im = (int)(r2 / p.H);
                         int ntap = 9 - g * p.taps_per_tile;
                         if (ntap > p.taps_per_tile) ntap = p.taps_per_tile;
                         const unsigned bytes = (unsigned)ntap * p.ci_rows * KC * 2 + (unsigned)BTAP;
                         mbar_arrive_expect_tx(&full[st], bytes);
+                        const int nab = p.ci_rows / p.a_cb;
+                        const int abox = KC * p.a_cb * 2, bbox = KC * p.b_cb * 2;
                         for (int j = 0; j < ntap; ++j) {
                             const int tap = g * p.taps_per_tile + j;
                             const int dy = tap / 3, dx = tap % 3;
-                            const CUtensorMap *m = dx == 0 ? &mapA0 : (dx == 1 ? &mapA1 : &mapA2);
-                            tma_load_4d(a_dst + j * p.ci_rows * KC * 2, m, xc * KC, y + dy - 1,
-                                        ct * p.ci_rows, im, &full[st]);
+                            for (int b = 0; b < nab; ++b)
+                                tma_load_4d(a_dst + (j * nab + b) * abox, &mapA0, ct * p.ci_rows + b * p.a_cb,
+                                            px0 + dx - 1, y + dy - 1, im, &full[st]);
                         }
-                        tma_load_4d(b_dst, &mapB, xc * KC, y, 0, im, &full[st]);
+                        for (int b = 0; b < N / p.b_cb; ++b)
+                            tma_load_4d(b_dst + b * bbox, &mapB, b * p.b_cb, px0, y, im, &full[st]);
                     }
                 }
             }
@@ -346,6 +366,7 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
         // ------------------------------------------------------------ MMA
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16_m128<N>();
+            constexpr uint32_t idesc_mn = idesc_bf16_m128<N, true>();
             const uint32_t wres_addr = smem_u32(wres);
             bool ok = true;
             if (use_wres && !mbar_wait_bounded(wbar, 0, budget)) {
@@ -394,6 +415,14 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                                 umma_bf16(d_tmem, kmajor_desc<SW>(a0 + kk * 32), kmajor_desc<SW>(b0 + kk * 32),
                                           idesc, (q > q0 || dx > 0 || kk > 0) ? 1u : 0u);
                         }
+                    } else if (!conv) {
+                        // MN-major: a K step of 16 pixels is 16 rows of each box
+                        const uint32_t ra = p.a_cb * 2, rb = p.b_cb * 2;
+#pragma unroll
+                        for (int kk = 0; kk < KC / 16; ++kk)
+                            umma_bf16(d_tmem, mnmajor_desc(a_addr + kk * 16 * ra, ra, KC * ra, 8 * ra),
+                                      mnmajor_desc(b_addr + kk * 16 * rb, rb, KC * rb, 8 * rb), idesc_mn,
+                                      (q > q0 || kk > 0) ? 1u : 0u);
                     } else {
                         uint32_t b0 = b_addr;
                         if (use_wres) {

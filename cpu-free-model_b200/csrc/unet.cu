@@ -1,6 +1,5 @@
 // Tensor-core 3x3 convolutions (tc_conv.cuh) on the host side: tensor maps,
-// launch shapes, the channel-major transposes the weight gradient reads,
-// and C-ABI entry points that run one convolution on host buffers (the
+// launch shapes, and C-ABI entry points that run one convolution on host buffers (the
 // parity tests drive the kernels through them).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -92,8 +91,8 @@ int plan_kc_n(TcConvParams &p, int num_sms, int *cps_out) {
 }
 
 template <int KC, int N>
-int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
-                const CUtensorMap &b, TcConvParams p, cudaStream_t s) {
+int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b, TcConvParams p,
+                cudaStream_t s) {
     static std::once_flag once[64];
     static cudaError_t attr_err[64];
     int dev = 0;
@@ -116,7 +115,7 @@ int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap 
     // (the occupancy query under-reports two CTAs of ~110 KB; the plan keeps
     // 2 x (dynamic + static + 1 KB reserved) inside the SM's 228 KB)
     const int grid = std::min(p.ntiles, di.num_sms * cps);
-    CFM_CUDA_TRY(launch_pdl(tc_conv_kernel<KC, N>, dim3(grid), dim3(192), smem, s, a0, a1, a2, b, p));
+    CFM_CUDA_TRY(launch_pdl(tc_conv_kernel<KC, N>, dim3(grid), dim3(192), smem, s, a0, a1, b, p));
     if (p.mode == 0 && p.csplit > 1) {
         const long long npix = (long long)p.B * p.H * p.W;
         const long long items = npix * (N / 8);
@@ -128,66 +127,25 @@ int launch_kc_n(const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap 
 }
 
 template <int KC>
-int launch_kc(int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
-              const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
+int launch_kc(int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b,
+              const TcConvParams &p, cudaStream_t s) {
     switch (n) {
-        case 32: return launch_kc_n<KC, 32>(a0, a1, a2, b, p, s);
-        case 64: return launch_kc_n<KC, 64>(a0, a1, a2, b, p, s);
-        case 128: return launch_kc_n<KC, 128>(a0, a1, a2, b, p, s);
-        case 256: return launch_kc_n<KC, 256>(a0, a1, a2, b, p, s);
+        case 32: return launch_kc_n<KC, 32>(a0, a1, b, p, s);
+        case 64: return launch_kc_n<KC, 64>(a0, a1, b, p, s);
+        case 128: return launch_kc_n<KC, 128>(a0, a1, b, p, s);
+        case 256: return launch_kc_n<KC, 256>(a0, a1, b, p, s);
         default: set_error("unsupported channel count %d", n); return CFM_UNSUPPORTED;
     }
 }
 
-int launch(int kc, int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &a2,
-           const CUtensorMap &b, const TcConvParams &p, cudaStream_t s) {
-    return kc == 64 ? launch_kc<64>(n, a0, a1, a2, b, p, s) : launch_kc<32>(n, a0, a1, a2, b, p, s);
+int launch(int kc, int n, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b,
+           const TcConvParams &p, cudaStream_t s) {
+    return kc == 64 ? launch_kc<64>(n, a0, a1, b, p, s) : launch_kc<32>(n, a0, a1, b, p, s);
 }
 
 bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
 }  // namespace
-
-// Channel-major copies of an NHWC tensor: out_d[img][c][y][x] =
-// in[img][y][x + d - 1][c] (zero outside) for d = 0 .. nshift - 1 when
-// nshift == 3, or the plain transpose (d = 1 only) when nshift == 1.
-// A block moves 64 pixels of one row (plus one halo pixel each side)
-// through shared memory: reads and writes are both contiguous.
-__global__ void k_nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1,
-                              __nv_bfloat16 *o2, int B, int H, int W, int C, int nshift) {
-    extern __shared__ __nv_bfloat16 tsm[];  // [66][C]
-    const int xt = blockIdx.x, y = blockIdx.y, img = blockIdx.z;
-    const int x0 = xt * 64;
-    const size_t row = ((size_t)img * H + y) * W;
-    for (int e = threadIdx.x; e < 66 * C; e += blockDim.x) {
-        const int px = e / C, c = e % C;
-        const int x = x0 - 1 + px;
-        tsm[e] = (x >= 0 && x < W) ? in[(row + x) * C + c] : __float2bfloat16_rn(0.f);
-    }
-    __syncthreads();
-    const size_t plane = (size_t)H * W;
-    for (int e = threadIdx.x; e < 64 * C; e += blockDim.x) {
-        const int c = e / 64, xx = e % 64, x = x0 + xx;
-        if (x >= W) continue;
-        const size_t o = ((size_t)img * C + c) * plane + (size_t)y * W + x;
-        if (nshift == 3) {
-            o0[o] = tsm[(xx + 0) * C + c];
-            o1[o] = tsm[(xx + 1) * C + c];
-            o2[o] = tsm[(xx + 2) * C + c];
-        } else {
-            o1[o] = tsm[(xx + 1) * C + c];
-        }
-    }
-}
-
-int nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1, __nv_bfloat16 *o2,
-                int B, int H, int W, int C, int nshift, cudaStream_t s) {
-    const size_t smem = 66 * (size_t)C * sizeof(__nv_bfloat16);
-    dim3 grid((W + 63) / 64, H, B);
-    k_nhwc_to_chw<<<grid, 256, smem, s>>>(in, o0, o1, o2, B, H, W, C, nshift);
-    CFM_CUDA_TRY(cudaGetLastError());
-    return CFM_OK;
-}
 
 int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     CFM_ARG_CHECK(a.Cin % 32 == 0 && a.Cin <= 256, "Cin must be a multiple of 32, at most 256");
@@ -235,7 +193,7 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     const cuuint64_t sb[2] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.Cout * a.Cin * 2};
     const cuuint32_t bb[3] = {(cuuint32_t)kc, (cuuint32_t)a.Cout, 1};
     if ((st = encode_map(&mb, a.w, 3, db, sb, bb, kc * 2))) return st;
-    return launch(kc, a.Cout, ma, mh, ma, mb, p, s);
+    return launch(kc, a.Cout, ma, mh, mb, p, s);
 }
 
 namespace {
@@ -246,7 +204,8 @@ long long wgrad_ksplit(int B, int H, int W, int Cin, int num_sms) {
     const int kc = W % 64 == 0 ? 64 : 32;
     const int ci_rows = std::min(Cin, 128);
     const int taps_per_tile = 128 / ci_rows;
-    const long long base = (long long)((9 + taps_per_tile - 1) / taps_per_tile) * (Cin / ci_rows);
+    const long long base =
+        (long long)((9 + taps_per_tile - 1) / taps_per_tile) * ((Cin + ci_rows - 1) / ci_rows);
     const long long total_k = (long long)B * H * (W / kc);
     long long ks = (2LL * num_sms + base - 1) / base;
     return std::max(1LL, std::min(ks, total_k / 4 > 0 ? total_k / 4 : 1));
@@ -274,7 +233,7 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     p.Cin = a.Cin;
     p.Cout = a.Cout;
     p.ci_rows = std::min(a.Cin, 128);
-    p.ci_tiles = a.Cin / p.ci_rows;
+    p.ci_tiles = (a.Cin + p.ci_rows - 1) / p.ci_rows;  // a partial last tile reads zero fill
     p.taps_per_tile = 128 / p.ci_rows;
     p.tap_groups = (9 + p.taps_per_tile - 1) / p.taps_per_tile;
     p.total_k = (long long)a.B * a.H * (a.W / kc);
@@ -289,21 +248,21 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     p.wpart = a.ws;
     p.err = a.err;
     p.budget_ns = barrier_timeout_ns();
-    CUtensorMap m0, m1, m2, mb;
-    const cuuint64_t da[4] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.Cin, (cuuint64_t)a.B};
-    const cuuint64_t sa[3] = {(cuuint64_t)a.W * 2, (cuuint64_t)a.H * a.W * 2,
-                              (cuuint64_t)a.Cin * a.H * a.W * 2};
-    const cuuint32_t ba[4] = {(cuuint32_t)kc, 1, (cuuint32_t)p.ci_rows, 1};
-    if ((st = encode_map(&m0, a.xt[0], 4, da, sa, ba, kc * 2)) ||
-        (st = encode_map(&m1, a.xt[1], 4, da, sa, ba, kc * 2)) ||
-        (st = encode_map(&m2, a.xt[2], 4, da, sa, ba, kc * 2)))
-        return st;
-    const cuuint64_t db[4] = {(cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.Cout, (cuuint64_t)a.B};
-    const cuuint64_t sb[3] = {(cuuint64_t)a.W * 2, (cuuint64_t)a.H * a.W * 2,
-                              (cuuint64_t)a.Cout * a.H * a.W * 2};
-    const cuuint32_t bb[4] = {(cuuint32_t)kc, 1, (cuuint32_t)a.Cout, 1};
-    if ((st = encode_map(&mb, a.dzt, 4, db, sb, bb, kc * 2))) return st;
-    if ((st = launch(kc, a.Cout, m0, m1, m2, mb, p, s))) return st;
+    p.a_cb = a.Cin % 64 == 0 ? 64 : 32;  // divides ci_rows
+    p.b_cb = std::min(a.Cout, 64);
+    // NHWC maps; a box is a_cb (b_cb) channels of KC pixels of one row
+    CUtensorMap mx, mz;
+    const cuuint64_t da[4] = {(cuuint64_t)a.Cin, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
+    const cuuint64_t sa[3] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.W * a.Cin * 2,
+                              (cuuint64_t)a.H * a.W * a.Cin * 2};
+    const cuuint32_t ba[4] = {(cuuint32_t)p.a_cb, (cuuint32_t)kc, 1, 1};
+    if ((st = encode_map(&mx, a.x, 4, da, sa, ba, p.a_cb * 2))) return st;
+    const cuuint64_t db[4] = {(cuuint64_t)a.Cout, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
+    const cuuint64_t sb[3] = {(cuuint64_t)a.Cout * 2, (cuuint64_t)a.W * a.Cout * 2,
+                              (cuuint64_t)a.H * a.W * a.Cout * 2};
+    const cuuint32_t bb[4] = {(cuuint32_t)p.b_cb, (cuuint32_t)kc, 1, 1};
+    if ((st = encode_map(&mz, a.dz, 4, db, sb, bb, p.b_cb * 2))) return st;
+    if ((st = launch(kc, a.Cout, mx, mx, mz, p, s))) return st;
     const int blocks = (int)std::min<long long>((per_split + 255) / 256, (long long)di.num_sms * 4);
     CFM_CUDA_TRY(launch_pdl(tc_wgrad_reduce, dim3(blocks), dim3(256), 0, s, (const float *)a.ws, p.ksplit,
                             a.Cin, a.Cout, a.dw));
@@ -388,30 +347,24 @@ int cfm_tc_conv3x3_wgrad(int B, int H, int W, int Cin, int Cout, const unsigned 
     const size_t nx = (size_t)B * H * W * Cin, nz = (size_t)B * H * W * Cout,
                  nw = (size_t)9 * Cout * Cin;
     DevBufs d;
-    __nv_bfloat16 *dx, *ddz, *xt0, *xt1, *xt2, *dzt;
+    __nv_bfloat16 *dx, *ddz;
     float *ddw;
     int *derr;
     CFM_CUDA_TRY(d.get(&dx, nx));
     CFM_CUDA_TRY(d.get(&ddz, nz));
-    CFM_CUDA_TRY(d.get(&xt0, nx));
-    CFM_CUDA_TRY(d.get(&xt1, nx));
-    CFM_CUDA_TRY(d.get(&xt2, nx));
-    CFM_CUDA_TRY(d.get(&dzt, nz));
     CFM_CUDA_TRY(d.get(&ddw, nw));
     CFM_CUDA_TRY(d.get(&derr, 1));
     CFM_CUDA_TRY(cudaMemcpy(dx, x, nx * 2, cudaMemcpyHostToDevice));
     CFM_CUDA_TRY(cudaMemcpy(ddz, dz, nz * 2, cudaMemcpyHostToDevice));
     CFM_CUDA_TRY(cudaMemset(ddw, 0, nw * 4));
     CFM_CUDA_TRY(cudaMemset(derr, 0, sizeof(int)));
-    int st = nhwc_to_chw(dx, xt0, xt1, xt2, B, H, W, Cin, 3, 0);
-    if (st) return st;
-    if ((st = nhwc_to_chw(ddz, nullptr, dzt, nullptr, B, H, W, Cout, 1, 0))) return st;
     DeviceInfo di;
-    if ((st = current_device_info(&di))) return st;
+    int st = current_device_info(&di);
+    if (st) return st;
     const long long wsn = tc_wgrad_ws_floats(B, H, W, Cin, Cout, di.num_sms);
     float *dws;
     CFM_CUDA_TRY(d.get(&dws, (size_t)wsn));
-    WgradArgs a{{xt0, xt1, xt2}, dzt, ddw, derr, B, H, W, Cin, Cout, dws, wsn};
+    WgradArgs a{dx, ddz, ddw, derr, B, H, W, Cin, Cout, dws, wsn};
     if ((st = tc_conv_wgrad(a, 0))) return st;
     CFM_CUDA_TRY(cudaDeviceSynchronize());
     if ((st = finish_err(derr))) return st;

@@ -28,12 +28,12 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s);
 constexpr long long TC_WS_FLOATS = 4LL << 20;
 
 // dw[tap][co][ci] += sum over pixels of dz[p][co] * x[p + shift(tap)][ci],
-// from the channel-major copies xt[d] (x shifted by d - 1 in x) and dzt.
-// The K (pixel) range is split over CTAs; the splits' partial tiles go to
-// the workspace `ws` and are added in split order (deterministic).
+// x and dz NHWC BF16 (zero outside the image).  The K (pixel) range is
+// split over CTAs; the splits' partial tiles go to the workspace `ws` and
+// are added in split order (deterministic).
 struct WgradArgs {
-    const __nv_bfloat16 *xt[3];
-    const __nv_bfloat16 *dzt;
+    const __nv_bfloat16 *x;
+    const __nv_bfloat16 *dz;
     float *dw;
     int *err;
     int B, H, W, Cin, Cout;
@@ -44,9 +44,5 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s);
 // Workspace (floats) the widest K split of that weight gradient uses on a
 // device with `num_sms` SMs.
 long long tc_wgrad_ws_floats(int B, int H, int W, int Cin, int Cout, int num_sms);
-
-// Channel-major copies of an NHWC tensor (see k_nhwc_to_chw).
-int nhwc_to_chw(const __nv_bfloat16 *in, __nv_bfloat16 *o0, __nv_bfloat16 *o1, __nv_bfloat16 *o2,
-                int B, int H, int W, int C, int nshift, cudaStream_t s);
 
 }  // namespace cfm

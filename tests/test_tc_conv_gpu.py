@@ -58,7 +58,8 @@ def test_tc_conv_forward(B, H, W, Cin, Cout, act):
 
 @pytest.mark.parametrize("B,H,W,Cin,Cout", [
     (1, 8, 64, 32, 32), (2, 16, 64, 64, 128), (1, 4, 128, 128, 64), (1, 4, 64, 256, 256),
-    (1, 2, 32, 32, 64), (2, 32, 256, 64, 32)])
+    (1, 2, 32, 32, 64), (2, 32, 256, 64, 32), (1, 8, 64, 128, 256), (2, 4, 96, 64, 64),
+    (1, 4, 64, 96, 32), (1, 4, 32, 160, 64)])
 def test_tc_conv_weight_gradient(B, H, W, Cin, Cout):
     rng = np.random.default_rng(B + H + W + Cin + 7 * Cout)
     x = bf16_round(rng.normal(size=(B, H, W, Cin)).astype(np.float32))
