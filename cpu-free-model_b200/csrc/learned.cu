@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "cfm_internal.h"
@@ -300,40 +301,121 @@ int partials_reduce(const float *part, int nb, int ne, int nw, float *dw, float 
     return CFM_OK;
 }
 
-// Weight and bias gradient of a thin layer, per block the sums over its
-// chunk of pixels of dw[t][co][ci] += sum_p g[p][co] in[p + s_t][ci] and
-// db[co] += sum_p g[p][co], into part[block][entry] (k_partials_reduce adds
-// them up).  `g` is FP32 (cout: one channel) or BF16 (cin: 32 channels);
-// `in` FP32 (cin: the network input) or BF16 (cout: g0).
-template <typename GT, typename IT>
-__global__ void k_thin_wgrad(const GT *g, const IT *in, int co_n, int ci_n, int B, int H, int W,
-                             long long chunk, float *part) {
-    const int nw = 9 * co_n * ci_n, ne = nw + co_n;
-    const long long P = (long long)B * H * W;
-    const long long p0 = blockIdx.x * chunk, p1 = min(P, p0 + chunk);
-    for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-        float acc = 0.f;
-        if (e < nw) {
-            const int t = e / (co_n * ci_n), co = (e / ci_n) % co_n, ci = e % ci_n;
-            const int sy = t / 3 - 1, sx = t % 3 - 1;
-            const long long sq = (long long)sy * W + sx;
-            // (xx, yy) of pixel p, stepped along with p (no division per pixel).
-            int xx = (int)(p0 % W), yy = (int)((p0 / W) % H);
-            for (long long p = p0; p < p1; ++p) {
-                const int y = yy + sy, xq = xx + sx;
-                if (y >= 0 && y < H && xq >= 0 && xq < W)
-                    acc += (float)g[p * co_n + co] * (float)in[(p + sq) * ci_n + ci];
-                if (++xx == W) {
-                    xx = 0;
-                    if (++yy == H) yy = 0;
-                }
-            }
-        } else {
-            const int co = e - nw;
-            for (long long p = p0; p < p1; ++p) acc += (float)g[p * co_n + co];
-        }
-        part[(size_t)blockIdx.x * ne + e] = acc;
+// N consecutive values of a BF16 or FP32 row as FP32 (one 8-byte load for
+// four BF16 or two FP32; the address is a multiple of N elements).
+template <typename T, int N>
+__device__ __forceinline__ void load_row(const T *src, float *v) {
+    if constexpr (std::is_same<T, float>::value && N == 2) {
+        const float2 q = *reinterpret_cast<const float2 *>(src);
+        v[0] = q.x, v[1] = q.y;
+    } else if constexpr (std::is_same<T, bf16>::value && N == 4) {
+        const uint2 q = *reinterpret_cast<const uint2 *>(src);
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+        const float2 a = __bfloat1622float2(h[0]), b = __bfloat1622float2(h[1]);
+        v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = (float)src[i];
     }
+}
+
+// Weight and bias gradient of a thin layer (the 2 -> 32 input layer and
+// the 32 -> 1 output layer, FP32 on the CUDA cores):
+//   dw[t][co][ci] = sum_p g[p][co] in[p + s_t][ci],   db[co] = sum_p g[p][co]
+// with `in` zero outside the image.  Warp w of a block owns CO_T output and
+// CI_T input channels (group w of (CO_N / CO_T) x (CI_N / CI_T) = 8) for
+// all nine taps; lane l takes pixels l, l + 32, ... of the block's chunk of
+// 32-pixel groups (each inside one row: W is a multiple of 32).  The lanes'
+// sums are combined by a fixed xor butterfly and the block's sums go to
+// part[block][entry], entry (t CO_N + co) CI_N + ci, then 9 CO_N CI_N + co
+// for the bias (k_partials_reduce adds the blocks up).
+template <typename GT, typename IT, int CO_N, int CI_N, int CO_T, int CI_T>
+__global__ void __launch_bounds__(256, 2)
+    k_thin_wgrad(const GT *g, const IT *in, int H, int W, long long ngroups, long long gchunk, float *part) {
+    static_assert((CO_N / CO_T) * (CI_N / CI_T) == 8, "eight warps, one channel group each");
+    constexpr int NW = 9 * CO_N * CI_N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int co0 = (warp / (CI_N / CI_T)) * CO_T, ci0 = (warp % (CI_N / CI_T)) * CI_T;
+    float acc[9][CO_T][CI_T], bacc[CO_T];
+#pragma unroll
+    for (int t = 0; t < 9; ++t)
+#pragma unroll
+        for (int i = 0; i < CO_T; ++i)
+#pragma unroll
+            for (int j = 0; j < CI_T; ++j) acc[t][i][j] = 0.f;
+#pragma unroll
+    for (int i = 0; i < CO_T; ++i) bacc[i] = 0.f;
+    const long long g0 = blockIdx.x * gchunk, g1 = min(ngroups, g0 + gchunk);
+    const int gpr = W / 32;
+    int x = (int)(g0 % gpr) * 32 + lane;
+    int y = (int)((g0 / gpr) % H);
+    for (long long gi = g0; gi < g1; ++gi) {
+        const long long p = gi * 32 + lane;
+        float gv[CO_T];
+        load_row<GT, CO_T>(g + p * CO_N + co0, gv);
+#pragma unroll
+        for (int i = 0; i < CO_T; ++i) bacc[i] += gv[i];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int sy = t / 3 - 1, sx = t % 3 - 1;
+            float iv[CI_T];
+            if (y + sy >= 0 && y + sy < H && x + sx >= 0 && x + sx < W) {
+                load_row<IT, CI_T>(in + (p + (long long)sy * W + sx) * CI_N + ci0, iv);
+            } else {
+#pragma unroll
+                for (int j = 0; j < CI_T; ++j) iv[j] = 0.f;
+            }
+#pragma unroll
+            for (int i = 0; i < CO_T; ++i)
+#pragma unroll
+                for (int j = 0; j < CI_T; ++j) acc[t][i][j] = __fmaf_rn(gv[i], iv[j], acc[t][i][j]);
+        }
+        x += 32;  // the whole group moves to the next row together
+        if (x >= W) {
+            x -= W;
+            if (++y == H) y = 0;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 9; ++t)
+#pragma unroll
+        for (int i = 0; i < CO_T; ++i)
+#pragma unroll
+            for (int j = 0; j < CI_T; ++j)
+#pragma unroll
+                for (int o = 16; o; o >>= 1) acc[t][i][j] += __shfl_xor_sync(0xffffffffu, acc[t][i][j], o);
+#pragma unroll
+    for (int i = 0; i < CO_T; ++i)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) bacc[i] += __shfl_xor_sync(0xffffffffu, bacc[i], o);
+    if (lane == 0) {
+        float *dst = part + (size_t)blockIdx.x * (NW + CO_N);
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int i = 0; i < CO_T; ++i)
+#pragma unroll
+                for (int j = 0; j < CI_T; ++j) dst[(t * CO_N + co0 + i) * CI_N + ci0 + j] = acc[t][i][j];
+        if (ci0 == 0)
+#pragma unroll
+            for (int i = 0; i < CO_T; ++i) dst[NW + co0 + i] = bacc[i];
+    }
+}
+
+// Launch of k_thin_wgrad over all B H W pixels (about two blocks per SM)
+// and the fixed-order sum of its blocks into dw and db.
+template <typename GT, typename IT, int CO_N, int CI_N, int CO_T, int CI_T>
+int thin_wgrad(const GT *g, const IT *in, int B, int H, int W, float *part, float *dw, float *db,
+               cudaStream_t s) {
+    CFM_ARG_CHECK(W % 32 == 0, "thin-layer gradient: W must be a multiple of 32");
+    const long long ngroups = (long long)B * H * W / 32;
+    const long long gchunk = std::max(1LL, (ngroups + 2 * 148 - 1) / (2 * 148));
+    const int blocks = (int)((ngroups + gchunk - 1) / gchunk);
+    constexpr int NE = 9 * CO_N * CI_N + CO_N;
+    CFM_ARG_CHECK((long long)blocks * NE <= GPART_FLOATS, "thin-gradient partials");
+    k_thin_wgrad<GT, IT, CO_N, CI_N, CO_T, CI_T><<<blocks, 256, 0, s>>>(g, in, H, W, ngroups, gchunk, part);
+    CFM_CUDA_TRY(cudaGetLastError());
+    return partials_reduce(part, blocks, NE, 9 * CO_N * CI_N, dw, db, s);
 }
 
 // 2x2 mean pool, NHWC, 8 channels per thread; (h, w) is the pooled size.
@@ -714,13 +796,8 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
     const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
     // cout
     {
-        const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
-        const int blocks = (int)((P0 + chunk - 1) / chunk);
-        CFM_ARG_CHECK((long long)blocks * (9 * 32 + 1) <= GPART_FLOATS, "thin-gradient partials");
-        k_thin_wgrad<float, bf16><<<blocks, 320, 0, s>>>(dout, a.g0, 1, 32, B, H, W, chunk, u->gpart);
-        CFM_CUDA_TRY(cudaGetLastError());
-        if ((st = partials_reduce(u->gpart, blocks, 9 * 32 + 1, 9 * 32, u->grad + u->woff[8], u->grad + u->boff[8],
-                                  s)))
+        if ((st = thin_wgrad<float, bf16, 1, 32, 1, 4>(dout, a.g0, B, H, W, u->gpart, u->grad + u->woff[8],
+                                                       u->grad + u->boff[8], s)))
             return st;
         k_cout_bwd<<<grid_for(P0), 256, 0, s>>>(dout, u->theta + u->woff[8], a.g0, a.dz_g0, B, H, W);
         CFM_CUDA_TRY(cudaGetLastError());
@@ -754,13 +831,8 @@ int unet_backward(UNetImpl *u, int B, const float *x, const float *dout, cudaStr
     k_skip_pool_mask<<<grid_for(P0 * 4), 256, 0, s>>>(a.du0, a.dp1, a.h0, a.dz_h0, B, H1, W1, 32);
     // cin
     {
-        const long long chunk = std::max(256LL, (P0 + 2 * 148 - 1) / (2 * 148));
-        const int blocks = (int)((P0 + chunk - 1) / chunk);
-        CFM_ARG_CHECK((long long)blocks * (9 * 32 * 2 + 32) <= GPART_FLOATS, "thin-gradient partials");
-        k_thin_wgrad<bf16, float><<<blocks, 608, 0, s>>>(a.dz_h0, x, 32, 2, B, H, W, chunk, u->gpart);
-        CFM_CUDA_TRY(cudaGetLastError());
-        if ((st = partials_reduce(u->gpart, blocks, 9 * 32 * 2 + 32, 9 * 32 * 2, u->grad + u->woff[0],
-                                  u->grad + u->boff[0], s)))
+        if ((st = thin_wgrad<bf16, float, 32, 2, 4, 2>(a.dz_h0, x, B, H, W, u->gpart, u->grad + u->woff[0],
+                                                       u->grad + u->boff[0], s)))
             return st;
     }
     return CFM_OK;
