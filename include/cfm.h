@@ -370,8 +370,9 @@ int cfm_unet_forward_host(cfm_unet *net, int B, const float *in, float *out);
 /* Forward, then the gradient of sum(out * dout) with respect to the
  * parameters into grad (cfm_unet_num_params floats). */
 int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *dout, float *grad);
-/* Device time of one forward pass of batch B on device-resident buffers
- * (mean over `iters` after a warm-up; CUDA events). */
+/* Device time of one forward pass of batch B on device-resident buffers:
+ * one pass captured in a CUDA graph (as a solver's graph runs it), replayed
+ * `iters` times back to back after a warm-up; CUDA events. */
 int cfm_unet_time_forward(cfm_unet *net, int B, int iters, double *ms_per_forward);
 /* Device time of one training step at batch B (forward, the backward pass
  * of sum(out * dout) with its weight gradients, one Adam step at lr 1e-4)
