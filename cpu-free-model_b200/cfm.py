@@ -78,6 +78,7 @@ _SIGS = {
     "cfm_unet_gradient_host": (_c.c_int, [_vp, _c.c_int, _vp, _vp, _vp]),
     "cfm_unet_activation_host": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_time_forward": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
+    "cfm_unet_set_forward_mode": (_c.c_int, [_vp, _c.c_int]),
     "cfm_unet_time_train_step": (_c.c_int, [_vp, _c.c_int, _c.c_int, _vp]),
     "cfm_unet_train_varcoef": (_c.c_int, [_vp, _c.c_int, _c.c_int, _c.c_ulonglong, _c.c_int, _c.c_int,
                                           _c.c_float, _c.c_int, _c.c_int, _vp, _vp, _vp, _vp]),
@@ -496,6 +497,10 @@ def tc_conv3x3_wgrad(x_bits, dz_bits):
     return dw
 
 
+# U-Net forward pass (cfm_unet_set_forward_mode)
+UNET_FORWARD_AUTO, UNET_FORWARD_LAYERS, UNET_FORWARD_PERSISTENT = 0, 1, 2
+
+
 class UNet:
     """The learned preconditioner's network (cfm_unet)."""
 
@@ -570,6 +575,12 @@ class UNet:
         """What a network restored with set_params was trained for."""
         check("cfm_unet_set_training_info", lib.cfm_unet_set_training_info(self.h, smooth, coarsen))
         self.smooth, self.coarsen = smooth, coarsen
+
+    def set_forward_mode(self, mode):
+        """UNET_FORWARD_LAYERS (one kernel per layer), UNET_FORWARD_PERSISTENT
+        (one persistent kernel) or UNET_FORWARD_AUTO (per layer, the faster);
+        same outputs bit for bit."""
+        check("cfm_unet_set_forward_mode", lib.cfm_unet_set_forward_mode(self.h, mode))
 
     def time_forward(self, B=1, iters=20):
         ms = ctypes.c_double()

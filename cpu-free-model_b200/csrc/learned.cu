@@ -401,6 +401,10 @@ struct UNetImpl {
     // added in block order by the last block (deterministic), and the
     // arrival counters of those reductions
     float *gpart = nullptr;
+    // grid barrier of the persistent forward, and which forward runs
+    // (CFM_UNET_FORWARD_AUTO / _LAYERS / _PERSISTENT)
+    UfBarrier *bar = nullptr;
+    int fwd_mode = 0;
     long long adam_t = 0;
     std::vector<void *> allocs;
 };
@@ -422,6 +426,15 @@ int dalloc(UNetImpl *u, T **p, size_t count) {
 }
 
 }  // namespace
+
+// Clears the persistent forward's barrier (counters, error word) and sets
+// its wait budget.
+int unet_reset_barrier(UNetImpl *u) {
+    UfBarrier b{};
+    b.timeout_ns = barrier_timeout_ns();
+    CFM_CUDA_TRY(cudaMemcpy(u->bar, &b, sizeof(b), cudaMemcpyHostToDevice));
+    return CFM_OK;
+}
 
 int unet_create(int H, int W, int maxB, UNetImpl **out) {
     CFM_ARG_CHECK(out, "null argument");
@@ -452,6 +465,7 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
     if (!st) st = dalloc(u, &u->m, o);
     if (!st) st = dalloc(u, &u->v, o);
     if (!st) st = dalloc(u, &u->err, 1);
+    if (!st) st = dalloc(u, &u->bar, 1);
     // the split-K workspace: the forward split's TC_WS_FLOATS or the widest
     // weight-gradient split of any tensor-core layer at the largest batch
     u->ws_floats = TC_WS_FLOATS;
@@ -493,6 +507,10 @@ int unet_create(int H, int W, int maxB, UNetImpl **out) {
         (e = cudaMemset(u->err, 0, sizeof(int))) != cudaSuccess) {
         unet_destroy(u);
         CFM_CUDA_TRY(e);
+    }
+    if ((st = unet_reset_barrier(u))) {
+        unet_destroy(u);
+        return st;
     }
     *out = u;
     return CFM_OK;
@@ -565,12 +583,56 @@ int conv_bwd_weights(UNetImpl *u, int l, const bf16 *x, const bf16 *dz, int B, i
 
 }  // namespace
 
+// The persistent forward (one cooperative launch, unet_fused.cuh) with the
+// per-layer kernels' buffers and plans.
+int forward_persistent(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
+                       const UNetInputScale *in_scale) {
+    UNetBuffers &a = u->a;
+    const int H = u->H, W = u->W;
+    FusedForwardArgs f{};
+    f.B = B;
+    f.H = H;
+    f.W = W;
+    f.x = x;
+    f.out = out;
+    f.in_scale = in_scale ? *in_scale : UNetInputScale{};
+    f.cin_w = u->theta + u->woff[0];
+    f.cin_b = u->theta + u->boff[0];
+    f.cout_w = u->theta + u->woff[8];
+    f.cout_b = u->theta + u->boff[8];
+    f.h0 = a.h0;
+    f.p1 = a.p1;
+    f.h1 = a.h1;
+    f.p2 = a.p2;
+    f.h2 = a.h2;
+    f.p3 = a.p3;
+    const bf16 *in[7] = {a.p1, a.p2, a.p3, a.h3, a.u2, a.u1, a.u0};
+    bf16 *o[7] = {a.h1, a.h2, a.h3, a.g3, a.g2, a.g1, a.g0};
+    for (int l = 0; l < 7; ++l) {
+        const UNetLayer &L = UNET_LAYERS[l + 1];
+        const int h = H >> L.level, w = W >> L.level;
+        f.conv[l] = ConvArgs{in[l], u->wb[l + 1], u->theta + u->boff[l + 1], nullptr, o[l], u->err, B, h, w,
+                             L.ci, L.co, 1};
+        f.conv[l].ws = u->ws;
+        f.conv[l].ws_floats = TC_WS_FLOATS;
+    }
+    f.skip[3] = a.h2;  // d3: u2 = up(g3) + h2
+    f.uout[3] = a.u2;
+    f.skip[4] = a.h1;  // d2: u1 = up(g2) + h1
+    f.uout[4] = a.u1;
+    f.skip[5] = a.h0;  // d1: u0 = up(g1) + h0
+    f.uout[5] = a.u0;
+    f.bar = u->bar;
+    return unet_forward_fused(f, s);
+}
+
 int unet_forward(UNetImpl *u, int B, const float *x, float *out, cudaStream_t s,
                  const UNetInputScale *in_scale) {
     CFM_ARG_CHECK(B >= 1 && B <= u->maxB, "batch");
     UNetBuffers &a = u->a;
     const int H = u->H, W = u->W;
     int st;
+    if (u->fwd_mode == CFM_UNET_FORWARD_PERSISTENT) return forward_persistent(u, B, x, out, s, in_scale);
     CFM_CUDA_TRY(launch_pdl(k_cin_fwd, dim3((W + PXB * CIN_SPAN * 32 - 1) / (PXB * CIN_SPAN * 32), H, B), dim3(256),
                             0, s, x, (const float *)(u->theta + u->woff[0]),
                             (const float *)(u->theta + u->boff[0]), a.h0, H, W,
@@ -671,9 +733,16 @@ int unet_adam(UNetImpl *u, float lr, float scale, cudaStream_t s) {
 
 int unet_check_err(UNetImpl *u) {
     int herr = 0;
+    UfBarrier b{};
     CFM_CUDA_TRY(cudaMemcpy(&herr, u->err, sizeof(int), cudaMemcpyDeviceToHost));
+    CFM_CUDA_TRY(cudaMemcpy(&b, u->bar, sizeof(b), cudaMemcpyDeviceToHost));
     if (herr) {
         set_error("unet: a tensor-core pipeline wait timed out (site %d)", herr);
+        return CFM_BARRIER_TIMEOUT;
+    }
+    if (b.error) {
+        set_error("unet: a grid barrier of the persistent forward timed out (barrier %d)", b.where);
+        unet_reset_barrier(u);
         return CFM_BARRIER_TIMEOUT;
     }
     return CFM_OK;
@@ -801,6 +870,16 @@ int cfm_unet_gradient_host(cfm_unet *h, int B, const float *in, const float *dou
 
 // Device time of one forward pass on the net's own input buffer (whatever it
 // holds), averaged over `iters` passes after one warm-up: CUDA events.
+int cfm_unet_set_forward_mode(cfm_unet *h, int mode) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(mode == CFM_UNET_FORWARD_AUTO || mode == CFM_UNET_FORWARD_LAYERS ||
+                      mode == CFM_UNET_FORWARD_PERSISTENT,
+                  "mode must be CFM_UNET_FORWARD_AUTO, _LAYERS or _PERSISTENT");
+    h->u->fwd_mode = mode;
+    return CFM_OK;
+}
+
 int cfm_unet_time_forward(cfm_unet *h, int B, int iters, double *ms_per_forward) {
     clear_error();
     CFM_ARG_CHECK(h && ms_per_forward && iters >= 1, "arguments");

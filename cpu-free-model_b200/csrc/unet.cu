@@ -11,6 +11,7 @@
 
 #include "cfm_internal.h"
 #include "tc_conv.cuh"
+#include "unet_fused.cuh"
 #include "unet_internal.h"
 
 namespace cfm {
@@ -147,13 +148,18 @@ bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
 }  // namespace
 
-int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
+namespace {
+
+// The parameters of a convolution pass before its launch plan: tiling (a
+// 128-pixel tile is bx x by), channel chunk, halo or per-tap staging, the
+// epilogue and the split-K workspace.
+int conv_fwd_params(const ConvArgs &a, TcConvParams &p, int *kc_out) {
     CFM_ARG_CHECK(a.Cin % 32 == 0 && a.Cin <= 256, "Cin must be a multiple of 32, at most 256");
     CFM_ARG_CHECK(a.Cout == 32 || a.Cout == 64 || a.Cout == 128 || a.Cout == 256, "Cout");
     CFM_ARG_CHECK(a.W % 128 == 0 || (pow2(a.W) && a.W <= 128), "W: a power of two or a multiple of 128");
     CFM_ARG_CHECK(a.H >= 1 && a.B >= 1, "H, B");
     const int kc = a.Cin % 64 == 0 ? 64 : 32;
-    TcConvParams p{};
+    p = TcConvParams{};
     p.mode = 0;
     p.B = a.B;
     p.H = a.H;
@@ -177,23 +183,144 @@ int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
     p.ws_floats = a.ws ? a.ws_floats : 0;
     p.csplit = 1;
     p.budget_ns = barrier_timeout_ns();
-    CUtensorMap ma, mb;
+    *kc_out = kc;
+    return CFM_OK;
+}
+
+// Its tensor maps: per-tap boxes (bx x by pixels), halo boxes (130 pixels of
+// one row; the per-tap map when the tile is narrower) and the weights.
+int conv_fwd_maps(const ConvArgs &a, const TcConvParams &p, int kc, CUtensorMap *ma, CUtensorMap *mh,
+                  CUtensorMap *mb) {
     const cuuint64_t da[4] = {(cuuint64_t)a.Cin, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
     const cuuint64_t sa[3] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.W * a.Cin * 2,
                               (cuuint64_t)a.H * a.W * a.Cin * 2};
     const cuuint32_t ba[4] = {(cuuint32_t)kc, (cuuint32_t)p.bx, (cuuint32_t)p.by, 1};
-    int st = encode_map(&ma, a.x, 4, da, sa, ba, kc * 2);
+    int st = encode_map(ma, a.x, 4, da, sa, ba, kc * 2);
     if (st) return st;
-    CUtensorMap mh = ma;  // halo boxes: 130 pixels of one row
+    *mh = *ma;
     if (p.halo) {
         const cuuint32_t bh[4] = {(cuuint32_t)kc, (cuuint32_t)TC_HALO_ROWS, 1, 1};
-        if ((st = encode_map(&mh, a.x, 4, da, sa, bh, kc * 2))) return st;
+        if ((st = encode_map(mh, a.x, 4, da, sa, bh, kc * 2))) return st;
     }
     const cuuint64_t db[3] = {(cuuint64_t)a.Cin, (cuuint64_t)a.Cout, 9};
     const cuuint64_t sb[2] = {(cuuint64_t)a.Cin * 2, (cuuint64_t)a.Cout * a.Cin * 2};
     const cuuint32_t bb[3] = {(cuuint32_t)kc, (cuuint32_t)a.Cout, 1};
-    if ((st = encode_map(&mb, a.w, 3, db, sb, bb, kc * 2))) return st;
+    return encode_map(mb, a.w, 3, db, sb, bb, kc * 2);
+}
+
+template <int KC>
+int plan_kc(int n, TcConvParams &p, int num_sms, int *cps) {
+    switch (n) {
+        case 32: return plan_kc_n<KC, 32>(p, num_sms, cps);
+        case 64: return plan_kc_n<KC, 64>(p, num_sms, cps);
+        case 128: return plan_kc_n<KC, 128>(p, num_sms, cps);
+        case 256: return plan_kc_n<KC, 256>(p, num_sms, cps);
+        default: set_error("unsupported channel count %d", n); return CFM_UNSUPPORTED;
+    }
+}
+
+}  // namespace
+
+int tc_conv_fwd(const ConvArgs &a, cudaStream_t s) {
+    TcConvParams p;
+    int kc = 0;
+    int st = conv_fwd_params(a, p, &kc);
+    if (st) return st;
+    CUtensorMap ma, mh, mb;
+    if ((st = conv_fwd_maps(a, p, kc, &ma, &mh, &mb))) return st;
     return launch(kc, a.Cout, ma, mh, mb, p, s);
+}
+
+int unet_forward_fused(const FusedForwardArgs &f, cudaStream_t s) {
+    DeviceInfo di;
+    int st = current_device_info(&di);
+    if (st) return st;
+    UfParams p{};
+    UfMaps m;
+    int slot = 0;
+    for (int l = 0; l < UF_CONVS; ++l) {
+        const ConvArgs &a = f.conv[l];
+        TcConvParams tp;
+        int kc = 0, cps = 1;
+        if ((st = conv_fwd_params(a, tp, &kc))) return st;
+        CUtensorMap ma, mh, mb;
+        if ((st = conv_fwd_maps(a, tp, kc, &ma, &mh, &mb))) return st;
+        // the per-layer launch plan: the same staging and split-K, so the
+        // same K order and partial sums
+        if ((st = kc == 64 ? plan_kc<64>(a.Cout, tp, di.num_sms, &cps) : plan_kc<32>(a.Cout, tp, di.num_sms, &cps)))
+            return st;
+        UfConv &L = p.conv[l];
+        L.H = a.H;
+        L.W = a.W;
+        L.N = a.Cout;
+        L.kc = kc;
+        L.bx = tp.bx;
+        L.by = tp.by;
+        L.tiles_x = tp.tiles_x;
+        L.tiles_y = tp.tiles_y;
+        L.nch = tp.nch;
+        L.halo = tp.halo;
+        L.ksteps = tp.ksteps;
+        L.csplit = tp.csplit;
+        L.ntiles = tp.ntiles;
+        L.a_region = tp.a_region;
+        L.bias = a.bias;
+        L.relu = a.relu;
+        L.out = a.out;
+        L.ws = a.ws;
+        L.skip = f.skip[l];
+        L.uout = f.uout[l];
+        m.a[l] = tp.halo ? mh : ma;
+        m.b[l] = mb;
+        const int b_stage = (tp.halo ? 3 : 1) * a.Cout * kc * 2;
+        slot = std::max(slot, round1k(tp.a_region + b_stage));
+    }
+    int stages = 2;
+    while (stages < 16 && uf_smem_bytes(stages + 1, slot) <= (size_t)TC_SMEM_MAX) ++stages;
+    if (uf_smem_bytes(stages, slot) > (size_t)TC_SMEM_MAX) {
+        set_error("persistent U-Net forward: a %d-byte ring slot leaves no two-stage ring", slot);
+        return CFM_UNSUPPORTED;
+    }
+    p.B = f.B;
+    p.H = f.H;
+    p.W = f.W;
+    p.x = f.x;
+    p.out = f.out;
+    p.in_scale = f.in_scale;
+    p.cin_w = f.cin_w;
+    p.cin_b = f.cin_b;
+    p.cout_w = f.cout_w;
+    p.cout_b = f.cout_b;
+    p.h0 = f.h0;
+    p.p1 = f.p1;
+    p.h1 = f.h1;
+    p.p2 = f.p2;
+    p.h2 = f.h2;
+    p.p3 = f.p3;
+    p.stages = stages;
+    p.slot_bytes = slot;
+    p.err = f.conv[0].err;
+    p.bar = f.bar;
+    p.budget_ns = barrier_timeout_ns();
+    // at least 120 KB: one CTA per SM, so that its 512-column TMEM
+    // allocation never waits for another CTA's
+    const size_t smem = std::max<size_t>(uf_smem_bytes(stages, slot), 120 * 1024);
+    static std::once_flag once[64];
+    static cudaError_t attr_err[64];
+    std::call_once(once[di.device & 63], [&] {
+        attr_err[di.device & 63] =
+            cudaFuncSetAttribute(unet_fused_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_MAX);
+    });
+    CFM_CUDA_TRY(attr_err[di.device & 63]);
+    int per_sm = 0;
+    CFM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, unet_fused_fwd, UF_THREADS, smem));
+    if (per_sm != 1) {
+        set_error("persistent U-Net forward: %d CTAs per SM (needs exactly one)", per_sm);
+        return CFM_UNSUPPORTED;
+    }
+    void *args[] = {(void *)&m, (void *)&p};
+    CFM_CUDA_TRY(launch_cooperative((const void *)unet_fused_fwd, dim3(di.num_sms), dim3(UF_THREADS), args, smem, s));
+    return CFM_OK;
 }
 
 namespace {

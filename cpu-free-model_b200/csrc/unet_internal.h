@@ -5,6 +5,9 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "cfm_internal.h"
+#include "learned_internal.h"
+
 namespace cfm {
 
 // out = act(conv3x3(x, w) + bias) [* (mask > 0)], NHWC BF16, padding 1.
@@ -26,6 +29,35 @@ struct ConvArgs {
 int tc_conv_fwd(const ConvArgs &a, cudaStream_t s);
 // Split-K workspace a net keeps for its convolutions (floats).
 constexpr long long TC_WS_FLOATS = 4LL << 20;
+
+// Grid barrier state of the persistent forward (uf_grid_sync).
+struct UfBarrier {
+    unsigned long long count;  // arrivals, a multiple of the grid between passes
+    int error;                 // set by a wait that ran out of budget (or a pipeline timeout)
+    int where;                 // barrier index of the first timeout
+    unsigned long long timeout_ns;
+};
+
+// The whole U-Net forward as one persistent cooperative kernel
+// (unet_fused.cuh): conv[0..6] are the tensor-core layers e1 e2 e3 d3 d2 d1
+// d0 as tc_conv_fwd would run them (their outputs h1 h2 h3 g3 g2 g1 g0);
+// skip[l] / uout[l], when set, fold the following upsample-and-add into
+// layer l (uout = up(out) + skip at twice the resolution).  The output and
+// every activation are bit-identical to the per-layer kernels.
+// CFM_UNSUPPORTED when a layer's staging does not fit the shared ring.
+struct FusedForwardArgs {
+    int B, H, W;
+    const float *x;
+    float *out;
+    UNetInputScale in_scale;
+    const float *cin_w, *cin_b, *cout_w, *cout_b;
+    __nv_bfloat16 *h0, *p1, *h1, *p2, *h2, *p3;
+    ConvArgs conv[7];
+    const __nv_bfloat16 *skip[7];
+    __nv_bfloat16 *uout[7];
+    UfBarrier *bar;  // zeroed before the first pass
+};
+int unet_forward_fused(const FusedForwardArgs &f, cudaStream_t s);
 
 // dw[tap][co][ci] += sum over pixels of dz[p][co] * x[p + shift(tap)][ci],
 // x and dz NHWC BF16 (zero outside the image).  The K (pixel) range is

@@ -374,6 +374,23 @@ int cfm_unet_gradient_host(cfm_unet *net, int B, const float *in, const float *d
  * one pass captured in a CUDA graph (as a solver's graph runs it), replayed
  * `iters` times back to back after a warm-up; CUDA events. */
 int cfm_unet_time_forward(cfm_unet *net, int B, int iters, double *ms_per_forward);
+/* Which forward pass the network runs (no counterpart in the reference,
+ * whose solver has no learned preconditioner):
+ *   CFM_UNET_FORWARD_LAYERS      one kernel per layer (19 launches, PDL);
+ *   CFM_UNET_FORWARD_PERSISTENT  one persistent cooperative kernel that walks
+ *                                the layers behind bounded grid barriers;
+ *   CFM_UNET_FORWARD_AUTO        (default) the per-layer kernels, which
+ *                                measured faster at every size tried.
+ * Both give bit-identical outputs.  The persistent pass fails with
+ * CFM_UNSUPPORTED when a layer's staging does not fit its shared ring.  A
+ * solver that captured the forward in its graph keeps the pass it captured
+ * until it builds the graph again. */
+enum {
+    CFM_UNET_FORWARD_AUTO = 0,
+    CFM_UNET_FORWARD_LAYERS = 1,
+    CFM_UNET_FORWARD_PERSISTENT = 2
+};
+int cfm_unet_set_forward_mode(cfm_unet *net, int mode);
 /* Device time of one training step at batch B (forward, the backward pass
  * of sum(out * dout) with its weight gradients, one Adam step at lr 1e-4)
  * on fixed synthetic inputs, averaged over `iters` steps after one warm-up
