@@ -459,12 +459,20 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_init(FpArgs a, double tol) {
 // FP_TILE x FP_TILE tiles held in shared memory with a halo as wide as the
 // sweeps need, so that all sweeps of one application (and what surrounds
 // them) take one launch: each sweep shrinks the valid region by one cell,
-// cells outside the grid are never read (the Dirichlet apply skips them),
 // and the arithmetic is the operator's (A u)_i = dg u_i - we_{i-1} u_{i-1} -
-// we_i u_{i+1} - wn_{i-nx} u_{i-nx} - wn_i u_{i+nx}, in that order.
+// we_i u_{i+1} - wn_{i-nx} u_{i-nx} - wn_i u_{i+nx}, in that order.  The
+// region holds we = wn = r = u = 0, dg = 1 and wd = 0 outside the grid, and
+// the face coefficients of the grid's last column and row are 0, so the
+// apply needs no boundary test: a term across the boundary adds -0 * 0 or
+// -0 * u, which leaves the sum unchanged (up to the sign of a zero), and a
+// sweep leaves the cells outside the grid at 0.  A thread visits the region
+// cells threadIdx.x + j blockDim.x, j < FP_MAXC, in every loop (no division
+// inside the sweeps: each cell's margin is computed once).
 constexpr int FP_TILE = 32;  // one thread per tile cell: FP_TILE^2 = CG_TILE threads
 static_assert(FP_TILE * FP_TILE == CG_TILE, "one thread per tile cell");
 constexpr int FP_MAX_SMOOTH = 8;
+constexpr int FP_MAXC = 3;  // region cells per thread: (FP_TILE + 2 FP_MAX_SMOOTH)^2 <= FP_MAXC CG_TILE
+static_assert((FP_TILE + 2 * FP_MAX_SMOOTH) * (FP_TILE + 2 * FP_MAX_SMOOTH) <= FP_MAXC * CG_TILE, "region cells");
 
 // Region arrays [R * R] each, region-local, one after the other in shared
 // memory: r, z0, z1, we, wn, dg, wd = omega / dg (addressed from one base
@@ -481,19 +489,17 @@ struct FpTile {
     __device__ __forceinline__ float *wd() const { return d + 6 * RR; }
 };
 
-// Region cells are visited as (row, column) by warps over rows and lanes
-// over columns: no integer division in the loops.
-#define FP_FOR_SQUARE(m, side, row, col)                                                   \
-    for (int row = (m) + (int)(threadIdx.x >> 5); row < (m) + (side); row += (int)(blockDim.x >> 5)) \
-        for (int col = (m) + (int)(threadIdx.x & 31); col < (m) + (side); col += 32)
-
 __device__ __forceinline__ bool fp_inside(const FpTile &t, const FpArgs &a, int row, int col, int *gi) {
     const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
     *gi = gy * a.op.nx + gx;
     return gx >= 0 && gx < a.op.nx && gy >= 0 && gy < a.op.ny;
 }
 
-__device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
+// Loads the region (r and the operator, zero outside the grid) and sets
+// z0[l] = init(l, row, col, inside, global index, wd[l], r[l]) for every
+// region cell; the margins of this thread's cells go to mg[].
+template <class Init>
+__device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem, int *mg, Init init) {
     FpTile t;
     t.x0 = (blockIdx.x % a.tx2) * FP_TILE;
     t.y0 = (blockIdx.x / a.tx2) * FP_TILE;
@@ -501,43 +507,52 @@ __device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem) {
     t.R = FP_TILE + 2 * H;
     t.d = reinterpret_cast<float *>(smem);
     t.RR = t.R * t.R;
-    FP_FOR_SQUARE(0, t.R, row, col) {
+#pragma unroll
+    for (int j = 0; j < FP_MAXC; ++j) {
+        const int l = threadIdx.x + j * CG_TILE;
+        mg[j] = -1;
+        if (l >= t.RR) continue;
+        const int row = l / t.R, col = l - row * t.R;
+        mg[j] = min(min(row, col), min(t.R - 1 - row, t.R - 1 - col));
         int i;
         const bool in = fp_inside(t, a, row, col, &i);
-        const int l = row * t.R + col;
-        t.r()[l] = in ? (a.mixed ? a.r32[i] : (float)a.r[i]) : 0.f;
+        const float r = in ? (a.mixed ? a.r32[i] : (float)a.r[i]) : 0.f;
+        const float wd = in ? a.wd32[i] : 0.f;
+        t.r()[l] = r;
         t.we()[l] = in ? a.we32[i] : 0.f;
         t.wn()[l] = in ? a.wn32[i] : 0.f;
         t.dg()[l] = in ? a.dg32[i] : 1.f;
-        t.wd()[l] = in ? a.wd32[i] : 0.f;
+        t.wd()[l] = wd;
+        t.z0()[l] = init(l, row, col, in, i, wd, r);
     }
     return t;
 }
 
-// (A u) at region cell (row, col) of a global cell (gx, gy) inside the grid,
-// its neighbours in the region.
-__device__ __forceinline__ float fp_apply(const FpTile &t, const FpArgs &a, const float *u, int row, int col) {
-    const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row, l = row * t.R + col;
+// (A u) at region cell l (not on the region's outer ring); no boundary test
+// (see above).
+__device__ __forceinline__ float fp_apply(const FpTile &t, const float *u, int l) {
     const float *we = t.we(), *wn = t.wn();
     float v = __fmul_rn(t.dg()[l], u[l]);
-    if (gx > 0) v = __fmaf_rn(-we[l - 1], u[l - 1], v);
-    if (gx < a.op.nx - 1) v = __fmaf_rn(-we[l], u[l + 1], v);
-    if (gy > 0) v = __fmaf_rn(-wn[l - t.R], u[l - t.R], v);
-    if (gy < a.op.ny - 1) v = __fmaf_rn(-wn[l], u[l + t.R], v);
+    v = __fmaf_rn(-we[l - 1], u[l - 1], v);
+    v = __fmaf_rn(-we[l], u[l + 1], v);
+    v = __fmaf_rn(-wn[l - t.R], u[l - t.R], v);
+    v = __fmaf_rn(-wn[l], u[l + t.R], v);
     return v;
 }
 
 // `sweeps` damped Jacobi sweeps on A z = r, z += (omega / dg) (r - A z),
 // starting from *cur (valid at margin m0 of the region); returns the buffer
-// holding the result, valid at margin m0 + sweeps.
-__device__ float *fp_sweeps(const FpTile &t, const FpArgs &a, float *cur, float *nxt, int m0, int sweeps) {
+// holding the result, valid at margin m0 + sweeps.  Sweep s updates the
+// cells of margin >= m0 + s + 1 only, so it reads only cells the previous
+// sweep (or the start) wrote.
+__device__ float *fp_sweeps(const FpTile &t, const int *mg, float *cur, float *nxt, int m0, int sweeps) {
     for (int s = 0; s < sweeps; ++s) {
-        const int m = m0 + s + 1, side = t.R - 2 * m;
-        FP_FOR_SQUARE(m, side, row, col) {
-            int i;
-            if (!fp_inside(t, a, row, col, &i)) continue;
-            const int l = row * t.R + col;
-            const float res = t.r()[l] - fp_apply(t, a, cur, row, col);
+        const int m = m0 + s + 1;
+#pragma unroll
+        for (int j = 0; j < FP_MAXC; ++j) {
+            if (mg[j] < m) continue;
+            const int l = threadIdx.x + j * CG_TILE;
+            const float res = t.r()[l] - fp_apply(t, cur, l);
             nxt[l] = __fmaf_rn(t.wd()[l], res, cur[l]);
         }
         __syncthreads();
@@ -592,15 +607,14 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
         }
     }
     const int H = a.smooth > 0 ? a.smooth : 1;
-    FpTile t = fp_tile(a, H, fp_smem);
-    __syncthreads();
+    int mg[FP_MAXC];
     // sweep 1 from zero is pointwise: z = (omega / dg) r on the whole region
-    FP_FOR_SQUARE(0, t.R, row, col) {
-        const int l = row * t.R + col;
-        t.z0()[l] = a.smooth > 0 ? t.wd()[l] * t.r()[l] : 0.f;
-    }
+    const int smooth = a.smooth;
+    FpTile t = fp_tile(a, H, fp_smem, mg, [&](int, int, int, bool, int, float wd, float r) {
+        return smooth > 0 ? wd * r : 0.f;
+    });
     __syncthreads();
-    const float *z = a.smooth > 1 ? fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth - 1) : t.z0();
+    const float *z = a.smooth > 1 ? fp_sweeps(t, mg, t.z0(), t.z1(), 0, a.smooth - 1) : t.z0();
     // this thread's tile cell
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
@@ -612,7 +626,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
     }
     double q = 0;
     if (in) {
-        const double v = (double)(t.r()[l] - fp_apply(t, a, z, row, col));
+        const double v = (double)(t.r()[l] - fp_apply(t, z, l));
         a.r1[i] = v;
         a.za[i] = (double)z[l];
         q = v * v;
@@ -651,19 +665,17 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
         c = yay > 0 ? yr / yay : 0.0;
     }
     const int H = a.smooth;
-    FpTile t = fp_tile(a, H, fp_smem);
-    FP_FOR_SQUARE(0, t.R, row, col) {
-        int i;
-        const int gx = t.x0 - t.H + col, gy = t.y0 - t.H + row;
-        t.z0()[row * t.R + col] =
-            fp_inside(t, a, row, col, &i)
-                ? __double2float_rn(c != 0.0 && gx < a.mx && gy < a.my
-                                        ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)], a.za[i])
-                                        : a.za[i])
-                : 0.f;
-    }
+    int mg[FP_MAXC];
+    const int x0 = (blockIdx.x % a.tx2) * FP_TILE - H, y0 = (blockIdx.x / a.tx2) * FP_TILE - H;
+    FpTile t = fp_tile(a, H, fp_smem, mg, [&](int, int row, int col, bool in, int i, float, float) {
+        const int gx = x0 + col, gy = y0 + row;
+        return in ? __double2float_rn(c != 0.0 && gx < a.mx && gy < a.my
+                                          ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)], a.za[i])
+                                          : a.za[i])
+                  : 0.f;
+    });
     __syncthreads();
-    const float *z = fp_sweeps(t, a, t.z0(), t.z1(), 0, a.smooth);
+    const float *z = fp_sweeps(t, mg, t.z0(), t.z1(), 0, a.smooth);
     const int lx = threadIdx.x & (FP_TILE - 1), ly = threadIdx.x / FP_TILE;
     const int row = H + ly, col = H + lx, l = row * t.R + col;
     int i;
