@@ -33,6 +33,7 @@ int current_device_info(DeviceInfo *out);
 
 // Device-side state of one grid barrier; see barrier.cuh.
 struct BarrierState {
+    // count (low) and gen (high) are updated as one 64-bit word
     unsigned int count;   // arrivals in the current generation
     unsigned int gen;     // generation, bumped by the last arrival
     int error;            // set to 1 by a wait that ran out of budget

@@ -92,12 +92,6 @@ struct UfParams {
 // last-arriver round trip.  The count stays a multiple of the grid between
 // passes because every CTA arrives at every barrier; after a timed-out wait
 // (error set) the host resets the whole struct before the next pass.
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
 // All threads of every CTA call it; true when every CTA arrived.
 __device__ __forceinline__ bool uf_grid_sync(UfBarrier *b, unsigned long long &target, int site) {
     __shared__ int s_ok;
