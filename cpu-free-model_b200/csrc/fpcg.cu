@@ -852,6 +852,12 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
 // ------------------------------------------------- mixed-precision kernels
 // x = 0 (FP64 iterate and FP32 correction of parity 0), r32 = fl32(b);
 // partials |b|^2 (FP64) and |r32|^2.
+// The parity buffers of a mixed solve, chosen by a select rather than an
+// index into the argument struct (a runtime index would copy the whole
+// struct into local memory on every thread).
+__device__ __forceinline__ double *fp_xm(const FpArgs &a, int par) { return par ? a.xm[1] : a.xm[0]; }
+__device__ __forceinline__ float *fp_dm(const FpArgs &a, int par) { return par ? a.dm[1] : a.dm[0]; }
+
 __global__ void __launch_bounds__(CG_TILE) k_fpm_init(FpArgs a, double tol) {
     fp_member(a);
     __shared__ double sm[33];
@@ -915,7 +921,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
     const int slot = (int)a.st->k % a.ring;
     const float af = __double2float_rn(ps != 0.0 ? pr / ps : 0.0);
-    float *d = a.dm[a.st->par];
+    float *d = fp_dm(a, a.st->par);
     FP_ROW;
     double rr = 0;
     if (i < a.n) {
@@ -945,8 +951,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
     const double target = st->target;
     if (!(g <= target * target || g < a.delta2 * st->gmax)) return;
     const int par = st->par;
-    const double *x = a.xm[par];
-    const float *d = a.dm[par];
+    const double *x = fp_xm(a, par);
+    const float *d = fp_dm(a, par);
     FP_ROW;
     double tt = 0, rr = 0;
     if (i < a.n) {
@@ -961,8 +967,8 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
         if (iy < o.ny - 1) t = __fma_rn(-o.wn[i], xv(i + nx), t);
         const double ti = __dsub_rn(a.b[i], t);
         const float ri = __double2float_rn(ti);
-        a.xm[par ^ 1][i] = xi;
-        a.dm[par ^ 1][i] = 0.f;
+        fp_xm(a, par ^ 1)[i] = xi;
+        fp_dm(a, par ^ 1)[i] = 0.f;
         a.r32[i] = ri;
         tt = __dmul_rn(ti, ti);
         rr = xprod(ri, ri);
@@ -982,7 +988,7 @@ __global__ void k_fpm_finish(FpArgs a, const FpState *st) {
     const long long nall = (long long)a.n * a.nmem;
     for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < nall; i += gridDim.x * blockDim.x) {
         const int par = st[i / a.n].par;
-        a.x[i] = __dadd_rn(a.xm[par][i], (double)a.dm[par][i]);
+        a.x[i] = __dadd_rn(fp_xm(a, par)[i], (double)fp_dm(a, par)[i]);
     }
 }
 
