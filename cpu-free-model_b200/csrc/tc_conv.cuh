@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                 int img = 0, y0 = 0, x0 = 0, g = 0, ct = 0;
                 long long k0 = 0;
                 int q0 = 0, q1 = 0;
+                int wxc = 0, wy = 0, wim = 0;  // wgrad: x chunk, row and image of the next K step
                 if (conv) {
                     const int pt = t / p.csplit, sp = t % p.csplit;
                     const int tx = pt % p.tiles_x, rest = pt / p.tiles_x;
@@ -309,6 +310,11 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                     g = rest / p.ci_tiles;
                     k0 = p.total_k * s / p.ksplit;
                     q1 = (int)(p.total_k * ((t % p.ksplit) + 1) / p.ksplit - k0);
+                    const int xchunks = p.W / KC;
+                    wxc = (int)(k0 % xchunks);
+                    const long long r2 = k0 / xchunks;
+                    wy = (int)(r2 % p.H);
+                    wim = (int)(r2 / p.H);
                 }
                 for (int q = q0; q < q1; ++q, ++it) {
                     const int st = it % STAGES;
@@ -332,11 +338,14 @@ __global__ void __launch_bounds__(192, N <= 128 ? 2 : 1)
                         tma_load_4d(a_dst, &mapA0, ch * KC, x0 + dx - 1, y0 + dy - 1, img, &full[st]);
                         if (!use_wres) tma_load_3d(b_dst, &mapB, ch * KC, 0, tap, &full[st]);
                     } else {
-                        const long long kq = k0 + q;
-                        const int xchunks = p.W / KC;
-                        const int px0 = (int)(kq % xchunks) * KC;
-                        const long long r2 = kq / xchunks;
-                        const int y = (int)(r2 % p.H), im = (int)(r2 / p.H);
+                        const int px0 = wxc * KC, y = wy, im = wim;
+                        if (++wxc == p.W / KC) {  // step along the row, then rows, then images
+                            wxc = 0;
+                            if (++wy == p.H) {
+                                wy = 0;
+                                ++wim;
+                            }
+                        }
                         int ntap = 9 - g * p.taps_per_tile;
                         if (ntap > p.taps_per_tile) ntap = p.taps_per_tile;
                         const unsigned bytes = (unsigned)ntap * p.ci_rows * KC * 2 + (unsigned)BTAP;

@@ -66,7 +66,9 @@ int plan_kc_n(TcConvParams &p, int num_sms, int *cps_out) {
     p.a_region = conv && p.halo ? round1k(136 * SW) : 128 * SW;
     const int b_stage = conv && p.halo ? 3 * BTAP : BTAP;
     const int wbytes = conv ? round1k(9 * p.nch * BTAP) : 0;
-    const int cps = (2 * tc_tmem_cols<N>() <= 512 && p.ntiles >= 2 * num_sms) ? 2 : 1;
+    // (a weight gradient's split is planned for up to two tiles per SM)
+    const int cps =
+        (2 * tc_tmem_cols<N>() <= 512 && p.ntiles >= (conv ? 2 * num_sms : num_sms + 1)) ? 2 : 1;
     // per-CTA dynamic shared memory (the SM has 228 KB; 1 KB per CTA is reserved)
     const int budget = cps == 2 ? TC_SMEM_MAX / 2 : TC_SMEM_MAX;
     const int overhead = 1024 + 8 * 8 + 16;
@@ -325,8 +327,8 @@ int unet_forward_fused(const FusedForwardArgs &f, cudaStream_t s) {
 
 namespace {
 
-// K splits of a weight gradient: about two tiles per SM, each split at
-// least four K steps.
+// K splits of a weight gradient: at most two tiles per SM (so that no CTA
+// runs a tile more than the others), each split at least four K steps.
 long long wgrad_ksplit(int B, int H, int W, int Cin, int num_sms) {
     const int kc = W % 64 == 0 ? 64 : 32;
     const int ci_rows = std::min(Cin, 128);
@@ -334,7 +336,7 @@ long long wgrad_ksplit(int B, int H, int W, int Cin, int num_sms) {
     const long long base =
         (long long)((9 + taps_per_tile - 1) / taps_per_tile) * ((Cin + ci_rows - 1) / ci_rows);
     const long long total_k = (long long)B * H * (W / kc);
-    long long ks = (2LL * num_sms + base - 1) / base;
+    long long ks = 2LL * num_sms / base;
     return std::max(1LL, std::min(ks, total_k / 4 > 0 ? total_k / 4 : 1));
 }
 
