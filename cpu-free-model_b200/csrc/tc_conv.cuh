@@ -583,28 +583,42 @@ namespace cfm {
 
 // Weight-gradient splits of tc_conv_kernel: dw[tap][co][ci] += the sum of
 // part[s][tap][ci][co] over the splits s, in a fixed order (the same sum on
-// every run): split s into accumulator s mod 4, combined as (a0 + a1) +
-// (a2 + a3).  One thread per element, in the partials' order (coalesced
-// reads).
-__global__ void tc_wgrad_reduce(const float *part, int ksplit, int Cin, int Cout, float *dw) {
+// every run).  A block takes WR_ENTRIES consecutive partial entries and
+// splits the ksplit splits into WR_CHUNKS chunks, one thread per (entry,
+// chunk): a chunk is summed with four accumulators (split s into s mod 4,
+// combined as (a0 + a1) + (a2 + a3)), then the chunks are added in order.
+// Reads are coalesced over the entries of a split.
+constexpr int WR_ENTRIES = 32, WR_CHUNKS = 8;
+__global__ void __launch_bounds__(WR_ENTRIES * WR_CHUNKS)
+    tc_wgrad_reduce(const float *part, int ksplit, int Cin, int Cout, float *dw) {
     pdl_enter();
+    __shared__ float sc[WR_CHUNKS][WR_ENTRIES];
     const long long n = 9LL * Cin * Cout;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int co = (int)(e % Cout);
-        const long long r = e / Cout;
-        const int ci = (int)(r % Cin), tap = (int)(r / Cin);
+    const int el = threadIdx.x % WR_ENTRIES, q = threadIdx.x / WR_ENTRIES;
+    const long long e = (long long)blockIdx.x * WR_ENTRIES + el;
+    float v = 0.f;
+    if (e < n) {
+        const int s0 = ksplit * q / WR_CHUNKS, s1 = ksplit * (q + 1) / WR_CHUNKS;
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-        int sp = 0;
-        for (; sp + 3 < ksplit; sp += 4) {
+        int sp = s0;
+        for (; sp + 3 < s1; sp += 4) {
             a0 += part[(size_t)sp * n + e];
             a1 += part[(size_t)(sp + 1) * n + e];
             a2 += part[(size_t)(sp + 2) * n + e];
             a3 += part[(size_t)(sp + 3) * n + e];
         }
-        for (; sp < ksplit; ++sp) a0 += part[(size_t)sp * n + e];
-        float *d = dw + ((size_t)tap * Cout + co) * Cin + ci;
-        *d += (a0 + a1) + (a2 + a3);
+        for (; sp < s1; ++sp) a0 += part[(size_t)sp * n + e];
+        v = (a0 + a1) + (a2 + a3);
+    }
+    sc[q][el] = v;
+    __syncthreads();
+    if (q == 0 && e < n) {
+        float t = 0.f;
+        for (int c = 0; c < WR_CHUNKS; ++c) t += sc[c][el];
+        const int co = (int)(e % Cout);
+        const long long r = e / Cout;
+        const int ci = (int)(r % Cin), tap = (int)(r / Cin);
+        dw[((size_t)tap * Cout + co) * Cin + ci] += t;
     }
 }
 

@@ -392,9 +392,9 @@ int tc_conv_wgrad(const WgradArgs &a, cudaStream_t s) {
     const cuuint32_t bb[4] = {(cuuint32_t)p.b_cb, (cuuint32_t)kc, 1, 1};
     if ((st = encode_map(&mz, a.dz, 4, db, sb, bb, p.b_cb * 2))) return st;
     if ((st = launch(kc, a.Cout, mx, mx, mz, p, s))) return st;
-    const int blocks = (int)std::min<long long>((per_split + 255) / 256, (long long)di.num_sms * 4);
-    CFM_CUDA_TRY(launch_pdl(tc_wgrad_reduce, dim3(blocks), dim3(256), 0, s, (const float *)a.ws, p.ksplit,
-                            a.Cin, a.Cout, a.dw));
+    const int blocks = (int)((per_split + WR_ENTRIES - 1) / WR_ENTRIES);
+    CFM_CUDA_TRY(launch_pdl(tc_wgrad_reduce, dim3(blocks), dim3(WR_ENTRIES * WR_CHUNKS), 0, s,
+                            (const float *)a.ws, p.ksplit, a.Cin, a.Cout, a.dw));
     return CFM_OK;
 }
 
