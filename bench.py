@@ -823,10 +823,10 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     torch.cuda.synchronize()
-    threads = [threading.Thread(target=e2e_worker, args=(k,)) for k in range(len(handles))]
-    for th in threads:
+    workers = [threading.Thread(target=e2e_worker, args=(k,)) for k in range(len(handles))]
+    for th in workers:
         th.start()
-    for th in threads:
+    for th in workers:
         th.join()
     torch.cuda.synchronize()
     e1.record()
