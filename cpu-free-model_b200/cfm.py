@@ -91,6 +91,7 @@ _SIGS = {
     "cfm_fpcg_solve": (_c.c_int, [_vp, _vp, _vp, _vp]),
     "cfm_fpcg_history": (_c.c_int, [_vp, _vp, _c.c_longlong, _vp]),
     "cfm_fpcg_set_precision": (_c.c_int, [_vp, _c.c_int, _c.c_double]),
+    "cfm_fpcg_set_device_loop": (_c.c_int, [_vp, _c.c_int]),
     "cfm_fpcg_reliable_updates": (_c.c_int, [_vp]),
     "cfm_fpcg_create_batch": (_c.c_int, [_c.c_int, _vp, _vp, _vp, _vp, _c.c_int, _c.c_int, _c.c_double, _vp]),
     "cfm_fpcg_solve_batch": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
@@ -627,6 +628,11 @@ class FPCG:
         """FP64, or FP32 Krylov vectors with FP64 reliable updates (delta: the
         residual drop that triggers one)."""
         check("cfm_fpcg_set_precision", lib.cfm_fpcg_set_precision(self.h, precision, delta))
+
+    def set_device_loop(self, on):
+        """0 (default): one kernel per phase; 1: a single system's iterations
+        between network applications in one persistent launch (same values)."""
+        check("cfm_fpcg_set_device_loop", lib.cfm_fpcg_set_device_loop(self.h, int(on)))
 
     def reliable_updates(self):
         """FP64 reliable updates of the last solve (mixed precision)."""

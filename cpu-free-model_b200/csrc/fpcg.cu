@@ -499,10 +499,10 @@ __device__ __forceinline__ bool fp_inside(const FpTile &t, const FpArgs &a, int 
 // z0[l] = init(l, row, col, inside, global index, wd[l], r[l]) for every
 // region cell; the margins of this thread's cells go to mg[].
 template <class Init>
-__device__ FpTile fp_tile(const FpArgs &a, int H, unsigned char *smem, int *mg, Init init) {
+__device__ FpTile fp_tile(const FpArgs &a, int bx, int H, unsigned char *smem, int *mg, Init init) {
     FpTile t;
-    t.x0 = (blockIdx.x % a.tx2) * FP_TILE;
-    t.y0 = (blockIdx.x / a.tx2) * FP_TILE;
+    t.x0 = (bx % a.tx2) * FP_TILE;
+    t.y0 = (bx / a.tx2) * FP_TILE;
     t.H = H;
     t.R = FP_TILE + 2 * H;
     t.d = reinterpret_cast<float *>(smem);
@@ -568,12 +568,11 @@ __device__ float *fp_sweeps(const FpTile &t, const int *mg, float *cur, float *n
 // and, when the network follows (`net_next`), r1 = r - A z0, partial
 // |r1|^2, and the network input channel 0 = R(r1) (f x f means; the network
 // scales it by 1 / rms(r1) itself).
-__global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int net_next) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_pre_blk(const FpArgs &a, int bx, int tick, int net_next) {
+    __syncthreads();  // a previous call on this block has read its shared tile
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
-    if (blockIdx.x == 0) {
+    if (bx == 0) {
         const double rr = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
         const double bb = sum_partials(fslot(a, FP_BB), a.ntiles, sm);
         const double tt = a.mixed ? sum_partials(fslot(a, FP_TT), a.ntiles, sm) : 0.0;
@@ -610,7 +609,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
     int mg[FP_MAXC];
     // sweep 1 from zero is pointwise: z = (omega / dg) r on the whole region
     const int smooth = a.smooth;
-    FpTile t = fp_tile(a, H, fp_smem, mg, [&](int, int, int, bool, int, float wd, float r) {
+    FpTile t = fp_tile(a, bx, H, fp_smem, mg, [&](int, int, int, bool, int, float wd, float r) {
         return smooth > 0 ? wd * r : 0.f;
     });
     __syncthreads();
@@ -632,7 +631,7 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
         q = v * v;
     }
     q = block_sum(q, sm);  // (its barriers also order the r1 stores before the restriction)
-    if (threadIdx.x == 0) fslot(a, FP_R1)[blockIdx.x] = q;
+    if (threadIdx.x == 0) fslot(a, FP_R1)[bx] = q;
     // restriction of this tile's cells (f divides FP_TILE and the tile origin)
     const int f = a.f, cs = FP_TILE / f;
     if (threadIdx.x < cs * cs) {
@@ -647,15 +646,19 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int n
         }
     }
 }
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_pre(FpArgs a, int tick, int net_next) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_pre_blk(a, blockIdx.x, tick, net_next);
+}
 
 // End of the preconditioner (one launch): z = `smooth` sweeps starting from
 // z0 + c P y, c = <P y, r1> / <P y, A P y> from the ydots partials (of all
 // multiples of P y, c P y removes the most A-norm error from A d = r1, so the
 // network's correction can only help the smoothed iterate), written to a.z
 // with the partials <z_k, s_{k-1-j}> (j < min(k, m)) of the orthogonalisation.
-__global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_post_blk(const FpArgs &a, int bx, int use_y) {
+    __syncthreads();  // a previous call on this block has read its shared tile
     extern __shared__ __align__(16) unsigned char fp_smem[];
     __shared__ double sm[33];
     double c = 0.0;  // without the network's y this iteration: smoothing alone
@@ -666,8 +669,8 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
     }
     const int H = a.smooth;
     int mg[FP_MAXC];
-    const int x0 = (blockIdx.x % a.tx2) * FP_TILE - H, y0 = (blockIdx.x / a.tx2) * FP_TILE - H;
-    FpTile t = fp_tile(a, H, fp_smem, mg, [&](int, int row, int col, bool in, int i, float, float) {
+    const int x0 = (bx % a.tx2) * FP_TILE - H, y0 = (bx / a.tx2) * FP_TILE - H;
+    FpTile t = fp_tile(a, bx, H, fp_smem, mg, [&](int, int row, int col, bool in, int i, float, float) {
         const int gx = x0 + col, gy = y0 + row;
         return in ? __double2float_rn(c != 0.0 && gx < a.mx && gy < a.my
                                           ? __fma_rn(c, (double)a.out[(gy >> a.fsh) * a.ncx + (gx >> a.fsh)], a.za[i])
@@ -700,8 +703,13 @@ __global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
                                              : __dmul_rn(zi, a.sring[sj[j] + i]))
                                   : 0.0;
         block_sum_multi(v, nj, smm);
-        if (threadIdx.x < nj) fslot(a, FP_ZS + threadIdx.x)[blockIdx.x] = v[threadIdx.x];
+        if (threadIdx.x < nj) fslot(a, FP_ZS + threadIdx.x)[bx] = v[threadIdx.x];
     }
+}
+__global__ void __launch_bounds__(CG_TILE, 2) k_fp_post(FpArgs a, int use_y) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_post_blk(a, blockIdx.x, use_y);
 }
 
 size_t fp_smem_bytes(int H) { return 7 * sizeof(float) * (size_t)(FP_TILE + 2 * H) * (FP_TILE + 2 * H); }
@@ -722,11 +730,9 @@ __global__ void k_fp_identity(FpArgs a) {
 
 // Partials <z, r1> and <z, A z> of the prolongated network output z = P y
 // (FP32 values, applied in FP64).
-__global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_ydots_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double yr = 0, yay = 0;
     if (i < a.n) {
         const StencilOp<2> &o = a.op;
@@ -751,18 +757,20 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
     yr = block_sum(yr, sm);
     yay = block_sum(yay, sm);
     if (threadIdx.x == 0) {
-        fslot(a, FP_YR)[blockIdx.x] = yr;
-        fslot(a, FP_YAY)[blockIdx.x] = yay;
+        fslot(a, FP_YR)[bx] = yr;
+        fslot(a, FP_YAY)[bx] = yay;
     }
+}
+__global__ void __launch_bounds__(CG_TILE) k_fp_ydots(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_ydots_blk(a, blockIdx.x);
 }
 
 // p_k = z_k - sum_j (<z_k, s_j> / <p_j, s_j>) p_j over the last min(k, m)
 // directions (into ring slot k mod (m + 1)), partial <p_k, r_k>, and the
 // loop condition.
-__global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond,
-                                                    int set_cond) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_dir_blk(const FpArgs &a, int bx, cudaGraphConditionalHandle cond, int set_cond) {
     __shared__ double sm[33];
     const int k = (int)a.st->k;
     const int nj = min(a.m, k);
@@ -785,7 +793,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
         }
     }
     __syncthreads();  // pj
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double pr = 0;
     if (i < a.n) {
         if (a.mixed) {  // FP32 direction, beta rounded to FP32
@@ -803,19 +811,22 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphCondition
         }
     }
     pr = block_sum(pr, sm);
-    if (threadIdx.x == 0) fslot(a, FP_PR)[blockIdx.x] = pr;
-    if (set_cond && blockIdx.x == 0 && threadIdx.x == 0)
+    if (threadIdx.x == 0) fslot(a, FP_PR)[bx] = pr;
+    if (set_cond && bx == 0 && threadIdx.x == 0)
         cudaGraphSetConditional(cond, a.st->done ? 0u : 1u);
+}
+__global__ void __launch_bounds__(CG_TILE) k_fp_dir(FpArgs a, cudaGraphConditionalHandle cond, int set_cond) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_dir_blk(a, blockIdx.x, cond, set_cond);
 }
 
 // s_k = A p_k; partial <p_k, s_k>.
-__global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_spmv_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
     const int slot = (int)a.st->k % a.ring;
     const double *p = a.pring + (size_t)slot * a.sstride;
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double ps = 0;
     if (i < a.n) {
         const double si = a.op.apply(p, i);
@@ -823,20 +834,23 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
         ps = __dmul_rn(p[i], si);
     }
     ps = block_sum(ps, sm);
-    if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
+    if (threadIdx.x == 0) fslot(a, FP_PS)[bx] = ps;
+}
+__global__ void __launch_bounds__(CG_TILE) k_fp_spmv(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_spmv_blk(a, blockIdx.x);
 }
 
 // alpha = <p_k, r_k> / <p_k, s_k>; x += alpha p_k; r -= alpha s_k; |r|^2;
 // <p_k, s_k> kept in the ring for the orthogonalisations to come.
-__global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fp_update_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
     const int slot = (int)a.st->k % a.ring;
     const double alpha = ps != 0.0 ? pr / ps : 0.0;
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double rr = 0;
     if (i < a.n) {
         a.x[i] = __fma_rn(alpha, a.pring[(size_t)slot * a.sstride + i], a.x[i]);
@@ -845,8 +859,13 @@ __global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
         rr = __dmul_rn(rn, rn);
     }
     rr = block_sum(rr, sm);
-    if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+    if (threadIdx.x == 0) fslot(a, FP_RR)[bx] = rr;
+    if (bx == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+}
+__global__ void __launch_bounds__(CG_TILE) k_fp_update(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fp_update_blk(a, blockIdx.x);
 }
 
 // ------------------------------------------------- mixed-precision kernels
@@ -894,13 +913,11 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_init(FpArgs a, double tol) {
 
 // s32 = A p32 with the FP32 operator; partial <p32, s32> (FP64 sum of the
 // exact FP32 products).
-__global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fpm_spmv_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
     const int slot = (int)a.st->k % a.ring;
     const float *p = a.pring32 + (size_t)slot * a.sstride;
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double ps = 0;
     if (i < a.n) {
         const float si = a.op.apply32(p, i);
@@ -908,21 +925,24 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
         ps = xprod(p[i], si);
     }
     ps = block_sum(ps, sm);
-    if (threadIdx.x == 0) fslot(a, FP_PS)[blockIdx.x] = ps;
+    if (threadIdx.x == 0) fslot(a, FP_PS)[bx] = ps;
+}
+__global__ void __launch_bounds__(CG_TILE) k_fpm_spmv(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fpm_spmv_blk(a, blockIdx.x);
 }
 
 // alpha = <p, r> / <p, s> (FP64, applied rounded to FP32); d += alpha p,
 // r32 -= alpha s (FP32); partial |r32|^2.
-__global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fpm_update_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
     const double ps = sum_partials(fslot(a, FP_PS), a.ntiles, sm);
     const double pr = sum_partials(fslot(a, FP_PR), a.ntiles, sm);
     const int slot = (int)a.st->k % a.ring;
     const float af = __double2float_rn(ps != 0.0 ? pr / ps : 0.0);
     float *d = fp_dm(a, a.st->par);
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double rr = 0;
     if (i < a.n) {
         d[i] = __fmaf_rn(af, a.pring32[(size_t)slot * a.sstride + i], d[i]);
@@ -931,8 +951,13 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
         rr = xprod(rn, rn);
     }
     rr = block_sum(rr, sm);
-    if (threadIdx.x == 0) fslot(a, FP_RR)[blockIdx.x] = rr;
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+    if (threadIdx.x == 0) fslot(a, FP_RR)[bx] = rr;
+    if (bx == 0 && threadIdx.x == 0) a.st->ps[slot] = ps;
+}
+__global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fpm_update_blk(a, blockIdx.x);
 }
 
 // Reliable update, when |r32|^2 has reached tol^2 |b|^2 or fallen below
@@ -942,9 +967,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_update(FpArgs a) {
 // the other parity's buffer, d' = 0, t = b - A x' (FP64, A x' from x + d on
 // the fly, so no grid barrier), r32 = fl32(t); partials |t|^2 and |r32|^2.
 // k_fp_pre flips the parity and judges convergence by |t|.
-__global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
-    pdl_enter();
-    FP_MEMBER(a);
+__device__ __forceinline__ void k_fpm_reliable_blk(const FpArgs &a, int bx) {
     __shared__ double sm[33];
     const double g = sum_partials(fslot(a, FP_RR), a.ntiles, sm);
     const FpState *st = a.st;
@@ -953,7 +976,7 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
     const int par = st->par;
     const double *x = fp_xm(a, par);
     const float *d = fp_dm(a, par);
-    FP_ROW;
+    const int i = bx * CG_TILE + threadIdx.x;
     double tt = 0, rr = 0;
     if (i < a.n) {
         const StencilOp<2> &o = a.op;
@@ -976,10 +999,72 @@ __global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
     tt = block_sum(tt, sm);
     rr = block_sum(rr, sm);
     if (threadIdx.x == 0) {
-        fslot(a, FP_TT)[blockIdx.x] = tt;
-        fslot(a, FP_RR)[blockIdx.x] = rr;
+        fslot(a, FP_TT)[bx] = tt;
+        fslot(a, FP_RR)[bx] = rr;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.st->pending = 1;
+    if (bx == 0 && threadIdx.x == 0) a.st->pending = 1;
+}
+__global__ void __launch_bounds__(CG_TILE) k_fpm_reliable(FpArgs a) {
+    pdl_enter();
+    FP_MEMBER(a);
+    k_fpm_reliable_blk(a, blockIdx.x);
+}
+
+// ------------------------------------------------------ single-system device loop
+// The phases of one or more FPCG iterations of a single system in one
+// cooperative launch, a grid barrier between phases instead of a kernel
+// boundary: each phase walks its blocks (row tiles, or smoothing tiles for
+// pre / post) as virtual blocks of the persistent grid and runs the same
+// block body as its kernel, so the arithmetic, and every result, is the
+// per-kernel path's.  The network runs between two such launches.
+enum FpPhaseCode : int {
+    FPP_SPMV,
+    FPP_UPDATE,
+    FPP_MSPMV,
+    FPP_MUPDATE,
+    FPP_MRELIABLE,
+    FPP_PRE,       // x: tick, y: net_next
+    FPP_IDENTITY,  // the network's stand-in without a network: y = R r1
+    FPP_YDOTS,
+    FPP_POST,      // x: use_y
+    FPP_DIR        // x: set the loop condition
+};
+struct FpOp {
+    int code, x, y;
+};
+constexpr int FP_MAX_OPS = 48;
+struct FpProgram {
+    int n;
+    FpOp op[FP_MAX_OPS];
+};
+
+__global__ void __launch_bounds__(CG_TILE, 2)
+    k_fp_loop(const FpArgs a, const FpProgram pg, BarrierState *bar, cudaGraphConditionalHandle cond) {
+    for (int s = 0; s < pg.n; ++s) {
+        const int code = pg.op[s].code, ox = pg.op[s].x, oy = pg.op[s].y;
+        if (code == FPP_IDENTITY) {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.nc;
+                 i += (long long)gridDim.x * blockDim.x)
+                a.out[i] = a.xin[2 * i];
+        } else {
+            const int nvb = (code == FPP_PRE || code == FPP_POST) ? a.ntiles2 : a.ntiles;
+            for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+                switch (code) {
+                    case FPP_SPMV: k_fp_spmv_blk(a, vb); break;
+                    case FPP_UPDATE: k_fp_update_blk(a, vb); break;
+                    case FPP_MSPMV: k_fpm_spmv_blk(a, vb); break;
+                    case FPP_MUPDATE: k_fpm_update_blk(a, vb); break;
+                    case FPP_MRELIABLE: k_fpm_reliable_blk(a, vb); break;
+                    case FPP_PRE: k_fp_pre_blk(a, vb, ox, oy); break;
+                    case FPP_YDOTS: k_fp_ydots_blk(a, vb); break;
+                    case FPP_POST: k_fp_post_blk(a, vb, ox); break;
+                    case FPP_DIR: k_fp_dir_blk(a, vb, cond, ox); break;
+                    default: break;
+                }
+            }
+        }
+        if (s + 1 < pg.n && !grid_barrier(bar, gridDim.x, s)) return;
+    }
 }
 
 // The result of a mixed solve: x = xm + dm of the current parity (FP64), for
@@ -1106,6 +1191,12 @@ struct cfm_fpcg {
     int2 *ext = nullptr;         // member extents (device)
     double *cells = nullptr;     // member cell counts (device; the network's input scale)
     std::vector<int2> ext_h;
+    // single-system device loop (k_fp_loop, cfm_fpcg_set_device_loop): off
+    // by default (slower than the per-phase kernels chained by programmatic
+    // dependent launch); its grid (0: unavailable) and barrier
+    int loop = 0;
+    int loop_grid = 0;
+    BarrierState *bar = nullptr;
 };
 
 namespace {
@@ -1184,6 +1275,24 @@ FpArgs fp_args(cfm_fpcg *h) {
 // rms(r1), log k) (or the identity), k_fp_ydots (<P y, r1>, <P y, A P y>),
 // k_fp_post (z = `smooth` sweeps from z0 + c P y, <z, r>, <z, r_old>) and
 // k_fp_dir (beta, p, the loop condition).
+// The network on R r1 of every member: the members in chunks of the
+// network's largest batch; image z of a chunk scales its input by its own
+// member's |r1| partials and cells.
+int fp_network(cfm_fpcg *h, const FpArgs &a) {
+    const int M = h->nmem;
+    const long long mstride = (long long)FP_NSLOT * a.pstride;
+    for (int m0 = 0; m0 < M; m0 += h->net->maxB) {
+        const int B = std::min(h->net->maxB, M - m0);
+        UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride + (size_t)m0 * mstride, h->ntiles2, (double)h->n};
+        sc.part_stride = mstride;
+        sc.cells_img = h->cells ? h->cells + m0 : nullptr;
+        const int st = unet_forward(h->net->u, B, h->xin + (size_t)m0 * 2 * h->nc, h->out + (size_t)m0 * h->nc,
+                                    h->stream, &sc);
+        if (st) return st;
+    }
+    return CFM_OK;
+}
+
 int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond, int tick,
                    bool use_net = true) {
     cudaStream_t s = h->stream;
@@ -1198,18 +1307,8 @@ int fp_precond_dir(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond
         return CFM_OK;
     }
     if (h->net) {
-        // the members in chunks of the network's largest batch; image z of a
-        // chunk scales its input by its own member's |r1| partials and cells
-        const long long mstride = (long long)FP_NSLOT * a.pstride;
-        for (int m0 = 0; m0 < M; m0 += h->net->maxB) {
-            const int B = std::min(h->net->maxB, M - m0);
-            UNetInputScale sc{a.part + (size_t)FP_R1 * a.pstride + (size_t)m0 * mstride, h->ntiles2, (double)h->n};
-            sc.part_stride = mstride;
-            sc.cells_img = h->cells ? h->cells + m0 : nullptr;
-            int st = unet_forward(h->net->u, B, h->xin + (size_t)m0 * 2 * h->nc, h->out + (size_t)m0 * h->nc, s,
-                                  &sc);
-            if (st) return st;
-        }
+        const int st = fp_network(h, a);
+        if (st) return st;
     } else {
         CFM_CUDA_TRY(launch_pdl(k_fp_identity, dim3(256), dim3(256), 0, s, a));
     }
@@ -1254,7 +1353,53 @@ int alloc_ring32(cfm_fpcg *h, int m) {
 // One pass of the device loop: h->net_every iterations, the network in the
 // first (a converged system may take up to net_every - 1 extra iterations,
 // which only lower its residual further).
+// One device-loop launch of the program's phases (none: nothing).
+int fp_loop_launch(cfm_fpcg *h, const FpArgs &a, FpProgram &pg, cudaGraphConditionalHandle cond) {
+    if (pg.n == 0) return CFM_OK;
+    void *args[] = {(void *)&a, (void *)&pg, (void *)&h->bar, (void *)&cond};
+    CFM_CUDA_TRY(launch_cooperative((const void *)k_fp_loop, dim3(h->loop_grid), dim3(CG_TILE), args,
+                                    fp_smem_bytes(std::max(h->smooth, 1)), h->stream));
+    pg.n = 0;
+    return CFM_OK;
+}
+
+// The iterations of fp_body as device-loop launches: the phases of
+// fp_iteration in order, a launch boundary only where the network runs
+// (or where the program is full).
+int fp_body_loop(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    FpProgram pg{};
+    int st;
+    auto add = [&](int code, int x, int y) -> int {
+        if (pg.n == FP_MAX_OPS) {
+            const int e = fp_loop_launch(h, a, pg, cond);
+            if (e) return e;
+        }
+        pg.op[pg.n++] = FpOp{code, x, y};
+        return CFM_OK;
+    };
+    for (int j = 0; j < h->net_every; ++j) {
+        const int set = set_cond && j == h->net_every - 1;
+        const int net_next = !(h->net && j != 0);
+        if ((st = add(h->mixed ? FPP_MSPMV : FPP_SPMV, 0, 0)) || (st = add(h->mixed ? FPP_MUPDATE : FPP_UPDATE, 0, 0)))
+            return st;
+        if (h->mixed && (st = add(FPP_MRELIABLE, 0, 0))) return st;
+        if ((st = add(FPP_PRE, 1, net_next))) return st;
+        if (!net_next) {
+            if ((st = add(FPP_POST, 0, 0)) || (st = add(FPP_DIR, set, 0))) return st;
+            continue;
+        }
+        if (h->net) {
+            if ((st = fp_loop_launch(h, a, pg, cond)) || (st = fp_network(h, a))) return st;
+        } else if ((st = add(FPP_IDENTITY, 0, 0))) {
+            return st;
+        }
+        if ((st = add(FPP_YDOTS, 0, 0)) || (st = add(FPP_POST, 1, 0)) || (st = add(FPP_DIR, set, 0))) return st;
+    }
+    return fp_loop_launch(h, a, pg, cond);
+}
+
 int fp_body(cfm_fpcg *h, const FpArgs &a, cudaGraphConditionalHandle cond, int set_cond) {
+    if (h->nmem == 1 && h->loop && h->loop_grid > 0) return fp_body_loop(h, a, cond, set_cond);
     const bool batch = h->nmem > 1;
     for (int j = 0; j < h->net_every; ++j) {
         const int st = fp_iteration(h, a, cond, set_cond && !batch && j == h->net_every - 1, j == 0);
@@ -1359,6 +1504,11 @@ int fp_setup(cfm_fpcg *h, int nx, int ny, int f, cfm_unet *net, int smooth, int 
         (e = cudaMalloc(&h->rcount, sizeof(unsigned int) * nmem)) != cudaSuccess ||
         (e = cudaMemset(h->rcount, 0, sizeof(unsigned int) * nmem)) != cudaSuccess ||
         (e = cudaMalloc(&h->st, sizeof(FpState) * nmem)) != cudaSuccess ||
+        (e = cudaMalloc(&h->bar, sizeof(BarrierState))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_loop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)fp_smem_bytes(FP_MAX_SMOOTH))) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_fp_loop, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess ||
         (e = cudaMalloc(&h->hist, sizeof(double) * (maxiter + 1) * (size_t)nmem)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
@@ -1366,6 +1516,15 @@ int fp_setup(cfm_fpcg *h, int nx, int ny, int f, cfm_unet *net, int smooth, int 
         set_error("FPCG buffers: %s", cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? CFM_OUT_OF_MEMORY : CFM_CUDA_ERROR;
     }
+    // the device loop's grid: every block co-resident (its grid barriers)
+    DeviceInfo di;
+    int per_sm = 0;
+    if (current_device_info(&di) == CFM_OK &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fp_loop, CG_TILE,
+                                                      fp_smem_bytes(std::max(smooth, 1))) == cudaSuccess &&
+        per_sm > 0)
+        h->loop_grid = std::min(std::max(h->ntiles, h->ntiles2), per_sm * di.num_sms);
+    cudaGetLastError();
     return CFM_OK;
 }
 
@@ -1540,6 +1699,7 @@ void cfm_fpcg_destroy(cfm_fpcg *h) {
     cudaFree(h->ext);
     cudaFree(h->cells);
     cudaFree(h->st);
+    cudaFree(h->bar);
     cudaFree(h->hist);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1564,6 +1724,17 @@ int cfm_fpcg_set_truncation(cfm_fpcg *h, int m) {
     h->m = m;
     // the captured iteration graph holds the old ring: build it again
     drop_graph(h);
+    return CFM_OK;
+}
+
+int cfm_fpcg_set_device_loop(cfm_fpcg *h, int on) {
+    clear_error();
+    CFM_ARG_CHECK(h, "null argument");
+    CFM_ARG_CHECK(on == 0 || on == 1, "on must be 0 or 1");
+    if (on == h->loop) return CFM_OK;
+    CFM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->loop = on;
+    drop_graph(h);  // the captured iteration is the other form
     return CFM_OK;
 }
 
@@ -1631,6 +1802,11 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
         CFM_CUDA_TRY(cudaStreamSynchronize(s));
         if ((st = build_graph(h))) return st;
     }
+    {  // the device loop's barrier: counters and error word cleared, wait budget set
+        BarrierState bs{};
+        bs.timeout_ns = barrier_timeout_ns();
+        CFM_CUDA_TRY(cudaMemcpyAsync(h->bar, &bs, sizeof(bs), cudaMemcpyHostToDevice, s));
+    }
     int launches = 0;
     CFM_CUDA_TRY(cudaEventRecord(h->ev0, s));
     if (h->mixed)
@@ -1666,6 +1842,14 @@ int cfm_fpcg_solve(cfm_fpcg *h, const double *b_host, double *x_host, cfm_stats 
     CFM_CUDA_TRY(cudaMemcpyAsync(acc, h->acc, sizeof(double), cudaMemcpyDeviceToHost, s));
     CFM_CUDA_TRY(cudaStreamSynchronize(s));
     if (h->net && (st = unet_check_err(h->net->u))) return st;
+    {
+        BarrierState bs{};
+        CFM_CUDA_TRY(cudaMemcpy(&bs, h->bar, sizeof(bs), cudaMemcpyDeviceToHost));
+        if (bs.error) {
+            set_error("FPCG device loop: grid barrier %d timed out", bs.where);
+            return CFM_BARRIER_TIMEOUT;
+        }
+    }
     h->last_k = hs.k;
     h->last_updates = h->mixed ? hs.updates : 0;
     const double bnorm = hs.target / h->tol;

@@ -474,6 +474,16 @@ int cfm_fpcg_set_network_period(cfm_fpcg *h, int every);
 int cfm_fpcg_set_precision(cfm_fpcg *h, int precision, double delta);
 /* FP64 reliable updates of the last solve (0 in FP64 mode). */
 int cfm_fpcg_reliable_updates(const cfm_fpcg *h);
+/* How a single system's iterations run on the device.  on = 0 (default):
+ * one kernel per phase, chained by programmatic dependent launch inside the
+ * solver's CUDA graph.  on = 1: the solver kernels between two network
+ * applications run as one persistent cooperative launch that walks the
+ * phases behind bounded grid barriers (the persistent-kernel idea of the
+ * reference's CPU-free CG, CG/src/single-stream/standard.cu:158-299,
+ * applied to FPCG).  Both compute the same values bit for bit; on B200 the
+ * per-phase kernels measured faster (512^2: 38 against 48 ms for
+ * Jacobi-smoothed FPCG).  Batches always use the per-phase kernels. */
+int cfm_fpcg_set_device_loop(cfm_fpcg *h, int on);
 /* A batch of independent 2D variable-coefficient systems solved together
  * by the same device loop: member m has cells nx[m] x ny[m] and
  * coefficients k_host[m] (built as cfm_varcoef_coeffs does).  Every member
