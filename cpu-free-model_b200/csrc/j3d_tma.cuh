@@ -11,9 +11,9 @@
 // and VN consecutive points per lane (one 16-byte vector); they keep the z-1
 // and z values of their points in registers, read the z+1 plane and the
 // N/S/E/W neighbours from shared memory, and store the new values straight to
-// global memory.  A stage is released (mbarrier arrive, one per consumer warp)
-// after the last step that reads it, so up to STAGES planes are in flight per
-// block.  All mbarrier and grid-barrier waits are bounded.
+// global memory.  A stage is released (a proxy fence by every consumer lane,
+// then one mbarrier arrive per consumer warp) after the last step that reads
+// it, so up to STAGES planes are in flight per block.  All mbarrier and grid-barrier waits are bounded.
 //
 // Sweeps are ordered either by a grid barrier after each sweep (udone null)
 // or, with udone (one counter per unit, zero at launch), by the units'
@@ -221,6 +221,7 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                         const V v = *reinterpret_cast<const V *>(pp + own0 + j * BXW);
                         memcpy(prev[j], &v, sizeof(v));
                     }
+                    fence_proxy_async_shared();  // reads of the slot before its refill
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[s]);
                     ++k;
@@ -258,6 +259,7 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                         wl[j] = pc[j * BXW - 1];
                         er[j] = pc[j * BXW + VN];
                     }
+                    fence_proxy_async_shared();  // reads of the slot before its refill
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[scur]);
                     const bool zspecial = (z == 1) || (z == nz - 2);
@@ -325,6 +327,7 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                     }
                     scur = snx;
                 }
+                fence_proxy_async_shared();  // reads of the slot before its refill
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[scur]);
                 if (udone) {

@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(32 * (CW + 1))
                             }
                         }
                     }
+                    fence_proxy_async_shared();  // reads of the stages before their refill
                     consumers_sync<CW>();
                     // stages no later window reads: all three before a fresh
                     // window (or after the last), else the oldest

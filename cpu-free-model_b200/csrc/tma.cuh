@@ -59,6 +59,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     return true;
 }
 
+// Orders this thread's earlier generic-proxy accesses to the CTA's shared
+// memory before later async-proxy (TMA) accesses to it.  A consumer of a
+// TMA-filled ring slot runs it after its last read of the slot and before
+// the arrive that lets the producer refill the slot; without it the refill
+// was seen, under heavy memory traffic, by reads that precede the arrive in
+// program order.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // Orders this thread's generic-proxy view of global memory before its later
 // async-proxy (TMA) reads.
 __device__ __forceinline__ void fence_proxy_async_global() {
