@@ -76,8 +76,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
-    ap.add_argument("--workload", choices=["jacobi3d", "jacobi2d", "jacobi3d_fp32", "cg128", "varcoef512", "unet",
-                                           "unet_train", "batch256", "cpufree"],
+    ap.add_argument("--workload", choices=["jacobi3d", "jacobi2d", "jacobi3d_fp32", "cg128", "varcoef512", "fpcg512",
+                                           "unet", "unet_train", "batch256", "cpufree"],
                     default="jacobi3d")
     return ap.parse_args()
 
@@ -340,6 +340,37 @@ def workload_varcoef512(args, cfm):
          "ms", args, r["ms"], r, higher=False, extra=extra)
 
 
+def workload_fpcg512(args, cfm):
+    """The preconditioner's solver kernels without the network: Jacobi-
+    smoothed FPCG (4 FP32 sweeps before and after) on the config-4 512^2
+    system to 1e-8, FP64 and mixed Krylov vectors, one kernel per phase and
+    the device loop (no training: a quick case for the solver kernels)."""
+    N = 512
+    k, f = cfm.varcoef_problem((N, N), 0)
+    S = cfm.Stencil(k)
+    res = {}
+    for prec, pname in ((cfm.FP64, "fp64"), (cfm.FP32, "mixed")):
+        for loop in (0, 1):
+            fp = cfm.FPCG(S, k, None, maxiter=20000, tol=1e-8, smooth=4, precision=prec)
+            fp.set_device_loop(loop)
+            for _ in range(max(args.warmup, 1)):
+                fp.solve(f)
+            ts = []
+            for _ in range(max(args.steps, 3)):
+                x, st = fp.solve(f)
+                ts.append(st.seconds)
+            fp.close()
+            t = statistics.median(ts)
+            res[f"{pname}_{'device_loop' if loop else 'kernels'}"] = {
+                "ms": t * 1e3, "iterations": st.iterations, "us_per_iteration": t * 1e6 / st.iterations,
+                "true_relres": st.residual}
+    best = min(res, key=lambda q: res[q]["ms"])
+    line("512^2 variable-coefficient time to 1e-8, Jacobi-smoothed FPCG", res[best]["ms"], "ms", args,
+         res[best]["ms"], {"workload": "varcoef2d_512^2_fpcg_jacobi4_tol1e-8", "best": best, "solvers": res,
+                           "timing": "median of steps, CUDA events around the whole solve incl. H2D b / D2H x"},
+         higher=False, dtype="f64")
+
+
 def secondary(cfm):
     """The other configurations in the default run (rank 0, one GPU): short
     repeats (3 timed after 1 warm-up), each with its CPU baseline."""
@@ -583,7 +614,7 @@ def main_workload(args):
     import torch  # noqa: F401  (device plumbing only)
     import cfm
     {"cg128": workload_cg128, "jacobi2d": workload_jacobi2d, "jacobi3d_fp32": workload_jacobi3d_fp32,
-     "varcoef512": workload_varcoef512,
+     "varcoef512": workload_varcoef512, "fpcg512": workload_fpcg512,
      "unet": workload_unet, "unet_train": workload_unet_train, "cpufree": workload_cpufree,
      "batch256": workload_batch256}[args.workload](args, cfm)
     return 0
@@ -796,22 +827,25 @@ def main():
 
     # ---- end-to-end through the C ABI with pinned host buffers: every step
     # copies its grid in from host memory, sweeps, and copies the result
-    # out (cfm_jacobi_run_host).  Two handles with the same tuned shape run
-    # on two host threads, so one step's copies overlap the other handle's
-    # sweeps; the timed region spans all steps of both, between two idle
-    # points of the device (CUDA events with a synchronize on each side).
+    # out (cfm_jacobi_run_host).  Three handles with the same tuned shape run
+    # on three host threads, so one step's copies overlap another handle's
+    # sweeps (a step is ~18 ms in, ~36 ms of sweeps, ~18 ms out: with two
+    # handles the copies of one barely fit in the other's sweeps, with three
+    # the sweeps run back to back; measured 171 / 311 / 326 / 294 GLUP/s
+    # for 1 / 2 / 3 / 4 handles); the timed region spans all steps of all,
+    # between two idle points of the device (CUDA events with a synchronize
+    # on each side).
     import threading
     os.environ["CFM_J3D_TMA_VARIANT"] = str(best if best >= 0 else 0)
     os.environ["CFM_J3D_ZCHUNK"] = str(zchunk)
-    j2 = cfm.Jacobi(3, N, N, N, cfm.FP64, 1, cfm.JACOBI_PERSISTENT)
+    handles = [j] + [cfm.Jacobi(3, N, N, N, cfm.FP64, 1, cfm.JACOBI_PERSISTENT) for _ in range(2)]
     del os.environ["CFM_J3D_TMA_VARIANT"], os.environ["CFM_J3D_ZCHUNK"]
-    handles = [j, j2]
     host_in = torch.from_numpy(j.problem_host(cfm.PROBLEM_CONFIG).reshape(-1)).pin_memory()
     host_out = [torch.empty_like(host_in).pin_memory() for _ in handles]
-    last = [None, None]
+    last = [None] * len(handles)
     for k, hk in enumerate(handles):  # warm the copy path
         last[k] = hk.run_host(NITER, host_in, host_out[k])
-    per_thread = max(2, args.steps // 4)
+    per_thread = max(4, args.steps // 2)
     e2e_steps = per_thread * len(handles)
 
     def e2e_worker(k):
@@ -834,10 +868,10 @@ def main():
     barrier()
     e2e_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3)
     h2d, d2h = last[0].h2d_bytes, last[0].d2h_bytes
-    e2e_same = bool(torch.equal(host_out[0], host_out[1]))
+    e2e_same = all(bool(torch.equal(host_out[0], o)) for o in host_out[1:])
     clk = clocks.stop()
-    j.close()
-    j2.close()
+    for hk in handles:
+        hk.close()
 
     lup_step = NITER * LUP_PER_SWEEP
     value = whole_job_rate(world, args.steps, lup_step, t_dev) / 1e9
@@ -865,8 +899,8 @@ def main():
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": "GLUP/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                "how": "cfm_jacobi_run_host on 2 handles x 2 host threads (copies of one step overlap "
-                       "the other's sweeps); CUDA events between idle points",
+                "how": "cfm_jacobi_run_host on 3 handles x 3 host threads (copies of one step overlap "
+                       "another's sweeps); CUDA events between idle points",
                 "results_equal": e2e_same},
         "gpu_launches": launches,
     }
